@@ -47,10 +47,12 @@ class Poisson:
     def source(self, x, uq, param, t):
         ng = x.shape[0]
         s = np.zeros((ng, 1))
+        # same literals and operation order as exasim_b200/models/poisson{2,3}d/HdgSource.cpp
         if self.nd == 2:
-            s[:, 0] = np.sin(x[:, 0] * PI) * np.sin(x[:, 1] * PI) * (2 * PI * PI)
+            s[:, 0] = np.sin(x[:, 0] * 3.141592653589793) * np.sin(x[:, 1] * 3.141592653589793) * 1.973920880217872E+1
         else:
-            s[:, 0] = 3 * (PI * PI) * np.sin(PI * x[:, 0]) * np.sin(PI * x[:, 1]) * np.sin(PI * x[:, 2])
+            s[:, 0] = (np.sin(x[:, 0] * 3.141592653589793) * np.sin(x[:, 1] * 3.141592653589793)
+                       * np.sin(x[:, 2] * 3.141592653589793) * 2.960881320326807E+1)
         return s, np.zeros((ng, 1, self.nc))
 
     def fbou(self, ib, x, uq, uh, n, tau, param, t):
