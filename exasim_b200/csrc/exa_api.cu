@@ -1,0 +1,583 @@
+// Context setup from Exasim's input blobs and the C ABI of the solver
+// (declarations and reference citations: include/exasim_b200.h).
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "exa_solver.cuh"
+#include "../../include/exasim_b200.h"
+
+namespace {
+
+// Exasim *.bin layout: [lsize, nsize(lsize), part_0(nsize[0]), part_1(nsize[1]), ...]
+struct Blob {
+  std::vector<long long> nsize;
+  std::vector<const double*> part;
+  bool ok = false;
+};
+
+Blob split_blob(const double* a, long long n) {
+  Blob b;
+  if (!a || n < 1) return b;
+  const long long ls = (long long)a[0];
+  if (ls < 1 || 1 + ls > n) return b;
+  long long o = 1 + ls;
+  for (long long i = 0; i < ls; ++i) {
+    const long long s = (long long)a[1 + i];
+    if (s < 0 || o + s > n) return b;
+    b.nsize.push_back(s);
+    b.part.push_back(a + o);
+    o += s;
+  }
+  b.ok = true;
+  return b;
+}
+
+template <class T>
+int dev_upload(ExaCtx& c, T** dst, const T* src, size_t count) {
+  if (count == 0) {
+    *dst = nullptr;
+    return EXA_OK;
+  }
+  void* p = nullptr;
+  cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+  if (e != cudaSuccess) {
+    exa_set_error("cudaMalloc of %zu bytes failed: %s", count * sizeof(T), cudaGetErrorString(e));
+    return EXA_ERR_NOMEM;
+  }
+  c.allocs.push_back(p);
+  *dst = (T*)p;
+  if (src) EXA_CUDA(cudaMemcpy(p, src, count * sizeof(T), cudaMemcpyHostToDevice));
+  return EXA_OK;
+}
+
+template <class T>
+int dev_alloc(ExaCtx& c, T** dst, size_t count) {
+  EXA_TRY(dev_upload<T>(c, dst, nullptr, count));
+  if (count) EXA_CUDA(cudaMemset(*dst, 0, count * sizeof(T)));
+  return EXA_OK;
+}
+
+std::vector<int> to_int(const double* p, long long n) {
+  std::vector<int> v((size_t)n);
+  for (long long i = 0; i < n; ++i) v[(size_t)i] = (int)llround(p[i]);
+  return v;
+}
+
+}  // namespace
+
+int exa_ctx_init(ExaCtx& c, const double* app, long long napp, const double* master, long long nmaster,
+                 const double* mesh, long long nmesh, const double* sol, long long nsol, int device) {
+  Blob A = split_blob(app, napp), M = split_blob(master, nmaster), Me = split_blob(mesh, nmesh),
+       S = split_blob(sol, nsol);
+  if (!A.ok || !M.ok || !Me.ok || !S.ok) {
+    exa_set_error("malformed input blob (app %d, master %d, mesh %d, sol %d)", A.ok, M.ok, Me.ok, S.ok);
+    return EXA_ERR_ARG;
+  }
+  if (A.nsize.size() < 9 || M.nsize.size() < 15 || Me.nsize.size() < 28 || S.nsize.size() < 3) {
+    exa_set_error("input blobs are shorter than Exasim's formats");
+    return EXA_ERR_ARG;
+  }
+  // ---- app.bin (readappstruct, readbinaryfiles.cpp:65-152; setcommonstruct, setstructs.cpp:45-200)
+  const double* nd_app = A.part[0];
+  const double* flag = A.part[1];
+  const double* prob = A.part[2];
+  ExaDims& P = c.P;
+  const int mpiprocs = (int)nd_app[0];
+  P.nc = (int)nd_app[5];
+  P.ncu = (int)nd_app[6];
+  P.ncq = (int)nd_app[7];
+  P.nco = (int)nd_app[9];
+  P.ncx = (int)nd_app[11];
+  P.ncw = (int)nd_app[13];
+  c.tdep = (int)flag[0];
+  c.wave = (int)flag[1];
+  c.ortho = (int)flag[5];
+  c.preconditioner = (int)flag[6];
+  c.tdfunc = (int)flag[10];
+  c.sourcefunc = (int)flag[11];
+  c.modelnumber = (int)flag[12];
+  const int spatial = (int)prob[0];
+  c.torder = (int)prob[3];
+  c.nstage = (int)prob[4];
+  c.newton_maxit = (int)prob[13];
+  c.gmres_maxit = (int)prob[14];
+  c.restart = (int)prob[15];
+  c.RBdim = (int)prob[16];
+  c.ppdegree = A.nsize[2] > 27 ? (int)prob[27] : 0;
+  const int coupled = A.nsize[2] > 28 ? (int)prob[28] : 0;
+  c.h_uinf.assign(A.part[3], A.part[3] + A.nsize[3]);
+  c.dt.assign(A.part[4], A.part[4] + A.nsize[4]);
+  const double* factor = A.part[5];
+  c.h_param.assign(A.part[6], A.part[6] + A.nsize[6]);
+  const double* solvers = A.part[7];
+  if (A.nsize[7] < 2 || A.nsize[8] < 1) {
+    exa_set_error("app.bin lacks solver parameters or tau");
+    return EXA_ERR_ARG;
+  }
+  c.newton_tol = solvers[0];
+  c.gmres_tol = solvers[1];
+  c.time0 = (c.tdep == 1 && A.nsize[5] > 0) ? factor[0] : 0.0;
+  c.time = c.time0;
+  if (spatial != 1) { exa_set_error("only the HDG discretization (problem[0]=1) is on this path"); return EXA_ERR_UNSUPPORTED; }
+  if (mpiprocs > 1) { exa_set_error("multi-rank inputs: this solver runs one GPU per mesh"); return EXA_ERR_UNSUPPORTED; }
+  if (P.nco > 0 || P.ncw > 0) { exa_set_error("odg/wdg fields (nco=%d, ncw=%d) are outside the HDG hot path", P.nco, P.ncw); return EXA_ERR_UNSUPPORTED; }
+  if (c.wave) { exa_set_error("wave (ModelW) problems are not supported"); return EXA_ERR_UNSUPPORTED; }
+  if (coupled > 0) { exa_set_error("coupled interfaces are not supported"); return EXA_ERR_UNSUPPORTED; }
+  if (c.RBdim > 0) { exa_set_error("reduced-basis initial guess (RBdim=%d) is not supported; set RBdim = 0", c.RBdim); return EXA_ERR_UNSUPPORTED; }
+  if (c.ppdegree > 1) { exa_set_error("polynomial preconditioner (ppdegree=%d) is not supported", c.ppdegree); return EXA_ERR_UNSUPPORTED; }
+  if (c.preconditioner != 0 && c.preconditioner != 1) { exa_set_error("preconditioner %d: only block Jacobi (0) and elemental additive Schwarz (1)", c.preconditioner); return EXA_ERR_UNSUPPORTED; }
+  if (c.restart < 1 || c.gmres_maxit < 1) { exa_set_error("GMRES restart/iterations must be positive"); return EXA_ERR_ARG; }
+
+  // ---- master.bin (readmasterstruct, readbinaryfiles.cpp:208-268)
+  const double* mnd = M.part[0];
+  P.nd = (int)mnd[0];
+  c.elemtype = (int)mnd[1];
+  c.porder = (int)mnd[3];
+  P.npe = (int)mnd[5];
+  P.npf = (int)mnd[6];
+  P.nge = (int)mnd[7];
+  P.ngf = (int)mnd[8];
+  if (P.ncx != P.nd) { exa_set_error("ncx (%d) differs from the dimension (%d)", P.ncx, P.nd); return EXA_ERR_UNSUPPORTED; }
+  if (P.nc != P.ncu && P.nc != P.ncu * (P.nd + 1)) { exa_set_error("nc=%d is neither ncu nor ncu*(nd+1)", P.nc); return EXA_ERR_UNSUPPORTED; }
+  if ((long long)M.nsize[1] != (long long)P.nge * P.npe * (P.nd + 1) || (long long)M.nsize[3] != (long long)P.ngf * P.npf * P.nd) {
+    exa_set_error("master.bin shape tables do not match its sizes");
+    return EXA_ERR_ARG;
+  }
+
+  // ---- mesh.bin (readmeshstruct, readbinaryfiles.cpp:321-409)
+  const double* mdims = Me.part[0];
+  P.ne = (int)mdims[1];
+  P.nfe = (int)mdims[4];
+  P.ndf = P.npf * P.nfe;
+  P.n = P.npe * P.ncu;
+  P.m = P.ncu * P.ndf;
+  if (Me.nsize[23] != (long long)P.npf * P.nfe || Me.nsize[24] != (long long)P.nfe * P.ne) {
+    exa_set_error("mesh.bin perm/bf sizes do not match the master element");
+    return EXA_ERR_ARG;
+  }
+  std::vector<int> perm = to_int(Me.part[23], Me.nsize[23]);
+  std::vector<int> bfv = to_int(Me.part[24], Me.nsize[24]);
+  ExaConn conn;
+  if (Me.nsize[1] == 0) {
+    if (Me.nsize[26] != (long long)P.ne * ((c.elemtype == 0) ? P.nd + 1 : (1 << P.nd))) {
+      exa_set_error("mesh.bin has neither connectivity nor element vertex lists");
+      return EXA_ERR_ARG;
+    }
+    std::vector<int> t = to_int(Me.part[26], Me.nsize[26]);
+    const int nf = exa_build_connectivity(t.data(), bfv.data(), perm.data(), M.part[12], P.nd, c.elemtype, P.ne,
+                                          P.npe, P.npf, conn);
+    if (nf < 0) { exa_set_error("mesh connectivity is wrong (unmatched face)"); return EXA_ERR_MESH; }
+  } else {
+    // pre-connected mesh: f2e [4,nf], elemcon [npf*nfe, ne]; interior faces are the fblks with code 0
+    conn.nf = (int)mdims[2];
+    conn.nfe = P.nfe;
+    conn.f2e = to_int(Me.part[21], Me.nsize[21]);
+    conn.elemcon = to_int(Me.part[22], Me.nsize[22]);
+    conn.nf0 = 0;
+    for (long long j = 0; j + 2 < Me.nsize[3]; j += 3)
+      if ((int)Me.part[3][j + 2] == 0) conn.nf0 += (int)Me.part[3][j + 1] - (int)Me.part[3][j] + 1;
+    if ((long long)conn.f2e.size() != 4LL * conn.nf || (long long)conn.elemcon.size() != (long long)P.ndf * P.ne) {
+      exa_set_error("mesh.bin f2e/elemcon sizes are inconsistent");
+      return EXA_ERR_ARG;
+    }
+  }
+  P.nf = conn.nf;
+  P.nf0 = conn.nf0;
+
+  // ---- sol.bin (readsolstruct, readbinaryfiles.cpp:499-618)
+  if (S.nsize[1] != (long long)P.npe * P.ncx * P.ne) { exa_set_error("sol.bin xdg size mismatch"); return EXA_ERR_ARG; }
+  c.h_xdg.assign(S.part[1], S.part[1] + S.nsize[1]);
+
+  // ---- device
+  c.device = device;
+  EXA_CUDA(cudaSetDevice(device));
+  EXA_CUDA(cudaStreamCreateWithFlags(&c.st, cudaStreamNonBlocking));
+  EXA_TRY(dev_upload(c, &c.shapegt, M.part[1], (size_t)M.nsize[1]));
+  EXA_TRY(dev_upload(c, &c.shapegw, M.part[2], (size_t)M.nsize[2]));
+  EXA_TRY(dev_upload(c, &c.shapfgt, M.part[3], (size_t)M.nsize[3]));
+  EXA_TRY(dev_upload(c, &c.shapfgw, M.part[4], (size_t)M.nsize[4]));
+  EXA_TRY(dev_upload(c, &c.perm, perm.data(), perm.size()));
+  EXA_TRY(dev_upload(c, &c.bf, bfv.data(), bfv.size()));
+  EXA_TRY(dev_upload(c, &c.f2e, conn.f2e.data(), conn.f2e.size()));
+  EXA_TRY(dev_upload(c, &c.elemcon, conn.elemcon.data(), conn.elemcon.size()));
+  EXA_TRY(dev_upload(c, &c.xdg, S.part[1], (size_t)S.nsize[1]));
+  std::vector<double> one_zero(1, 0.0);
+  EXA_TRY(dev_upload(c, &c.uinf, c.h_uinf.empty() ? one_zero.data() : c.h_uinf.data(), std::max<size_t>(1, c.h_uinf.size())));
+  EXA_TRY(dev_upload(c, &c.param, c.h_param.empty() ? one_zero.data() : c.h_param.data(), std::max<size_t>(1, c.h_param.size())));
+  EXA_TRY(dev_upload(c, &c.tau, A.part[8], (size_t)A.nsize[8]));
+  const size_t ne = P.ne;
+  EXA_TRY(dev_alloc(c, &c.elemg, ne * P.elemg_stride()));
+  EXA_TRY(dev_alloc(c, &c.faceg, ne * P.nfe * P.faceg_stride()));
+  EXA_TRY(exa_k_geometry(P, c.shapegt, c.shapfgt, c.perm, c.xdg, c.elemg, c.faceg, c.st));
+
+  // solution: udg from sol.bin (full or u only) or the model's initial condition; uhat from sol.bin or u
+  EXA_TRY(dev_alloc(c, &c.udg, ne * P.npe * P.nc));
+  EXA_TRY(dev_alloc(c, &c.uh, (size_t)c.ndofuhat()));
+  EXA_TRY(dev_alloc(c, &c.sdg, ne * P.npe * P.ncu));
+  {
+    std::vector<double> u(ne * P.npe * P.nc, 0.0);
+    const long long nu = S.nsize.size() > 2 ? S.nsize[2] : 0;
+    if (nu == (long long)ne * P.npe * P.nc) {
+      std::memcpy(u.data(), S.part[2], sizeof(double) * u.size());
+    } else if (nu == (long long)ne * P.npe * P.ncu) {
+      for (size_t e = 0; e < ne; ++e)
+        for (int k = 0; k < P.ncu; ++k)
+          for (int i = 0; i < P.npe; ++i) u[i + P.npe * k + P.npe * P.nc * e] = S.part[2][i + P.npe * k + P.npe * P.ncu * e];
+    } else if (nu == 0) {
+      EXA_TRY(exa_model_init_udg(c, u.data()));
+    } else {
+      exa_set_error("sol.bin udg size %lld matches neither npe*nc*ne nor npe*ncu*ne", nu);
+      return EXA_ERR_ARG;
+    }
+    EXA_CUDA(cudaMemcpy(c.udg, u.data(), sizeof(double) * u.size(), cudaMemcpyHostToDevice));
+    const long long nuh = S.nsize.size() > 5 ? S.nsize[5] : 0;
+    if (nuh == c.ndofuhat()) {
+      EXA_CUDA(cudaMemcpy(c.uh, S.part[5], sizeof(double) * nuh, cudaMemcpyHostToDevice));
+    } else {
+      EXA_TRY(exa_k_face_nodes(P, c.f2e, c.perm, c.udg, c.uh, c.st));
+    }
+  }
+
+  // q-equation matrices Minv*C, Minv*E (qequation.cpp:66-338)
+  if (P.ncq > 0) {
+    double *mass = nullptr, *cw = nullptr, *ew = nullptr;
+    EXA_TRY(dev_alloc(c, &mass, ne * P.npe * P.npe));
+    EXA_TRY(dev_alloc(c, &cw, ne * P.npe * P.npe * P.nd));
+    EXA_TRY(dev_alloc(c, &ew, ne * P.npe * P.ndf * P.nd));
+    EXA_TRY(dev_alloc(c, &c.MC, ne * P.npe * P.npe * P.nd));
+    EXA_TRY(dev_alloc(c, &c.ME, ne * P.npe * P.ndf * P.nd));
+    EXA_TRY(dev_alloc(c, &c.d_flag, 4));
+    EXA_TRY(exa_k_qmats(P, c.shapegt, c.shapegw, c.shapfgt, c.shapfgw, c.perm, c.elemg, c.faceg, mass, cw, ew, c.st));
+    EXA_TRY(exa_inverse(mass, P.npe, (long long)P.npe * P.npe, P.ne, c.d_flag, c.st));
+    GemmBatch g{};
+    g.M = P.npe; g.N = P.npe; g.K = P.npe; g.alpha = 1.0; g.beta = 0.0;
+    g.A = mass; g.lda = P.npe; g.sA = (long long)P.npe * P.npe; g.sA2 = 0;
+    g.B = cw; g.ldb = P.npe; g.sB = (long long)P.npe * P.npe * P.nd; g.sB2 = (long long)P.npe * P.npe;
+    g.C = c.MC; g.ldc = P.npe; g.sC = (long long)P.npe * P.npe * P.nd; g.sC2 = (long long)P.npe * P.npe;
+    g.batch = P.ne; g.batch2 = P.nd;
+    EXA_TRY(exa_gemm(g, c.st));
+    g.N = P.ndf;
+    g.B = ew; g.sB = (long long)P.npe * P.ndf * P.nd; g.sB2 = (long long)P.npe * P.ndf;
+    g.C = c.ME; g.sC = (long long)P.npe * P.ndf * P.nd; g.sC2 = (long long)P.npe * P.ndf;
+    EXA_TRY(exa_gemm(g, c.st));
+    EXA_CUDA(cudaStreamSynchronize(c.st));
+    int flag_h = 0;
+    EXA_CUDA(cudaMemcpy(&flag_h, c.d_flag, sizeof(int), cudaMemcpyDeviceToHost));
+    if (flag_h) { exa_set_error("singular element mass matrix"); return EXA_ERR_SINGULAR; }
+  } else {
+    EXA_TRY(dev_alloc(c, &c.d_flag, 4));
+  }
+
+  // condensed system and workspace
+  const size_t n = P.n, m = P.m, nqn = (size_t)P.npe * P.nd * P.ncu;
+  EXA_TRY(dev_alloc(c, &c.H, ne * m * m));
+  EXA_TRY(dev_alloc(c, &c.F, ne * n * m));
+  EXA_TRY(dev_alloc(c, &c.Ru, ne * n));
+  EXA_TRY(dev_alloc(c, &c.Rh, ne * m));
+  const size_t N = (size_t)c.ndofuhat();
+  EXA_TRY(dev_alloc(c, &c.b, N));
+  if (c.preconditioner == 0)
+    EXA_TRY(dev_alloc(c, &c.Pc, (size_t)P.ncu * P.npf * P.ncu * P.npf * P.nf));
+  else
+    EXA_TRY(dev_alloc(c, &c.Pc, ne * m * m));
+  // element chunk: bounded workspace (about 8 GB at most)
+  const size_t per_elem = sizeof(double) * (n * n + n * nqn + n * m + m * n + m * nqn +
+                                            (size_t)P.nge * (P.nd + 1) * P.ncu * P.nc + n);
+  size_t cap = (size_t)8 << 30;
+  c.neb = (int)std::max<size_t>(1, std::min<size_t>(std::min<size_t>(ne, cap / per_elem), 65535));
+  const size_t nb = c.neb;
+  EXA_TRY(dev_alloc(c, &c.wD, nb * n * n));
+  EXA_TRY(dev_alloc(c, &c.wB, std::max<size_t>(1, nb * n * nqn)));
+  EXA_TRY(dev_alloc(c, &c.wF, nb * n * m));
+  EXA_TRY(dev_alloc(c, &c.wK, nb * m * n));
+  EXA_TRY(dev_alloc(c, &c.wG, std::max<size_t>(1, nb * m * nqn)));
+  EXA_TRY(dev_alloc(c, &c.wRg, nb * P.nge * (P.nd + 1) * P.ncu * P.nc));
+  EXA_TRY(dev_alloc(c, &c.wRu, nb * n));
+  EXA_TRY(dev_alloc(c, &c.V, N * (size_t)(c.restart + 1)));
+  EXA_TRY(dev_alloc(c, &c.x, N));
+  EXA_TRY(dev_alloc(c, &c.r, N));
+  EXA_TRY(dev_alloc(c, &c.w, N));
+  EXA_TRY(dev_alloc(c, &c.we, ne * m));
+  EXA_TRY(dev_alloc(c, &c.du, ne * n));
+  const int VB = exa_vec_blocks();
+  EXA_TRY(dev_alloc(c, &c.part_a, VB));
+  EXA_TRY(dev_alloc(c, &c.part_b, VB));
+  EXA_TRY(dev_alloc(c, &c.part_m, (size_t)VB * (c.restart + 1)));
+  const size_t n1 = c.restart + 1;
+  EXA_TRY(dev_alloc(c, &c.hess, n1 * c.restart));
+  EXA_TRY(dev_alloc(c, &c.gs, n1));
+  EXA_TRY(dev_alloc(c, &c.gcs, n1));
+  EXA_TRY(dev_alloc(c, &c.gsn, n1));
+  EXA_TRY(dev_alloc(c, &c.scal, 16));
+  if (c.tdep) {
+    EXA_TRY(dev_alloc(c, &c.udgprev, ne * n));
+    EXA_TRY(dev_alloc(c, &c.utmp, ne * n));
+  }
+  EXA_CUDA(cudaMallocHost((void**)&c.pinned, sizeof(double) * (n1 * (n1 + 2) + 64)));
+  EXA_CUDA(cudaStreamSynchronize(c.st));
+  return EXA_OK;
+}
+
+void exa_ctx_free(ExaCtx& c) {
+  if (c.device >= 0) cudaSetDevice(c.device);
+  for (void* p : c.allocs) cudaFree(p);
+  c.allocs.clear();
+  if (c.pinned) cudaFreeHost(c.pinned);
+  c.pinned = nullptr;
+  if (c.st) cudaStreamDestroy(c.st);
+  c.st = nullptr;
+}
+
+// ==================================================================================
+// C ABI
+// ==================================================================================
+struct exa_ctx {
+  ExaCtx c;
+};
+
+namespace {
+
+struct FieldRef {
+  double* p;
+  long long n;
+};
+
+bool field(ExaCtx& c, const char* name, FieldRef& f) {
+  const ExaDims& P = c.P;
+  const long long ne = P.ne, n = P.n, m = P.m, N = c.ndofuhat();
+  const std::string s(name ? name : "");
+  if (s == "udg") f = {c.udg, (long long)P.npe * P.nc * ne};
+  else if (s == "uh") f = {c.uh, N};
+  else if (s == "H") f = {c.H, m * m * ne};
+  else if (s == "F") f = {c.F, n * m * ne};
+  else if (s == "Ru") f = {c.Ru, n * ne};
+  else if (s == "Rh") f = {c.Rh, m * ne};
+  else if (s == "b") f = {c.b, N};
+  else if (s == "x") f = {c.x, N};
+  else if (s == "sdg") f = {c.sdg, n * ne};
+  else if (s == "P") f = {c.Pc, c.preconditioner == 0 ? (long long)P.ncu * P.npf * P.ncu * P.npf * P.nf : m * m * ne};
+  else if (s == "MinvC") f = {c.MC, P.ncq > 0 ? (long long)P.npe * P.npe * P.nd * ne : 0};
+  else if (s == "MinvE") f = {c.ME, P.ncq > 0 ? (long long)P.npe * P.ndf * P.nd * ne : 0};
+  else if (s == "elemg") f = {c.elemg, (long long)P.elemg_stride() * ne};
+  else if (s == "faceg") f = {c.faceg, (long long)P.faceg_stride() * P.nfe * ne};
+  else return false;
+  return true;
+}
+
+int guard(exa_ctx* h) {
+  if (!h) {
+    exa_set_error("null context");
+    return EXA_ERR_ARG;
+  }
+  cudaError_t e = cudaSetDevice(h->c.device);
+  if (e != cudaSuccess) {
+    exa_set_error("cudaSetDevice(%d): %s", h->c.device, cudaGetErrorString(e));
+    return EXA_ERR_CUDA;
+  }
+  return EXA_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* exa_last_error(void) { return exa_get_error(); }
+
+int exa_create(const double* app, long long napp, const double* master, long long nmaster, const double* mesh,
+               long long nmesh, const double* sol, long long nsol, int device, exa_ctx** out) {
+  if (!out) {
+    exa_set_error("null output handle");
+    return EXA_ERR_ARG;
+  }
+  *out = nullptr;
+  exa_ctx* h = new exa_ctx();
+  int s = exa_ctx_init(h->c, app, napp, master, nmaster, mesh, nmesh, sol, nsol, device);
+  if (s != EXA_OK) {
+    exa_ctx_free(h->c);
+    delete h;
+    return s;
+  }
+  *out = h;
+  return EXA_OK;
+}
+
+void exa_destroy(exa_ctx* h) {
+  if (!h) return;
+  exa_ctx_free(h->c);
+  delete h;
+}
+
+int exa_sizes(exa_ctx* h, long long* out) {
+  EXA_TRY(guard(h));
+  const ExaDims& P = h->c.P;
+  const long long v[16] = {P.ne, P.nf, P.nf0, P.npe, P.npf, P.nfe, P.nc, P.ncu, P.nd,
+                           P.n,  P.m,  h->c.ndofuhat(), P.nge, P.ngf, h->c.neb, h->c.preconditioner};
+  for (int i = 0; i < 16; ++i) out[i] = v[i];
+  return EXA_OK;
+}
+
+int exa_get_field(exa_ctx* h, const char* name, double* host, long long n) {
+  EXA_TRY(guard(h));
+  FieldRef f{};
+  if (!field(h->c, name, f) || !host || n != f.n) {
+    exa_set_error("get_field('%s'): unknown name or size %lld != %lld", name ? name : "", n, f.n);
+    return EXA_ERR_ARG;
+  }
+  EXA_CUDA(cudaStreamSynchronize(h->c.st));
+  if (n) EXA_CUDA(cudaMemcpy(host, f.p, sizeof(double) * n, cudaMemcpyDeviceToHost));
+  return EXA_OK;
+}
+
+int exa_set_field(exa_ctx* h, const char* name, const double* host, long long n) {
+  EXA_TRY(guard(h));
+  FieldRef f{};
+  if (!field(h->c, name, f) || !host || n != f.n) {
+    exa_set_error("set_field('%s'): unknown name or size %lld != %lld", name ? name : "", n, f.n);
+    return EXA_ERR_ARG;
+  }
+  EXA_CUDA(cudaStreamSynchronize(h->c.st));
+  if (n) EXA_CUDA(cudaMemcpy(f.p, host, sizeof(double) * n, cudaMemcpyHostToDevice));
+  return EXA_OK;
+}
+
+int exa_field_ptr(exa_ctx* h, const char* name, double** dev, long long* n) {
+  EXA_TRY(guard(h));
+  FieldRef f{};
+  if (!field(h->c, name, f) || !dev || !n) {
+    exa_set_error("field_ptr('%s'): unknown name", name ? name : "");
+    return EXA_ERR_ARG;
+  }
+  *dev = f.p;
+  *n = f.n;
+  return EXA_OK;
+}
+
+int exa_get_connectivity(exa_ctx* h, int* f2e, int* elemcon) {
+  EXA_TRY(guard(h));
+  const ExaDims& P = h->c.P;
+  if (f2e) EXA_CUDA(cudaMemcpy(f2e, h->c.f2e, sizeof(int) * 4 * (size_t)P.nf, cudaMemcpyDeviceToHost));
+  if (elemcon) EXA_CUDA(cudaMemcpy(elemcon, h->c.elemcon, sizeof(int) * (size_t)P.ndf * P.ne, cudaMemcpyDeviceToHost));
+  return EXA_OK;
+}
+
+int exa_set_time(exa_ctx* h, double time, double dtfactor) {
+  EXA_TRY(guard(h));
+  h->c.time = time;
+  h->c.dtfactor = dtfactor;
+  return EXA_OK;
+}
+
+int exa_assemble(exa_ctx* h) {
+  EXA_TRY(guard(h));
+  return exa_drv_assemble(h->c);
+}
+
+int exa_residual(exa_ctx* h, double* norm) {
+  EXA_TRY(guard(h));
+  EXA_TRY(exa_drv_residual(h->c, norm));
+  EXA_CUDA(cudaStreamSynchronize(h->c.st));
+  return EXA_OK;
+}
+
+int exa_matvec(exa_ctx* h, const double* v, double* w) {
+  EXA_TRY(guard(h));
+  EXA_TRY(exa_drv_matvec(h->c, v, w));
+  EXA_CUDA(cudaStreamSynchronize(h->c.st));
+  return EXA_OK;
+}
+
+int exa_precond(exa_ctx* h, const double* v, double* w) {
+  EXA_TRY(guard(h));
+  if (v == w) {
+    exa_set_error("precond: input and output must differ");
+    return EXA_ERR_ARG;
+  }
+  EXA_TRY(exa_drv_precond(h->c, v, w));
+  EXA_CUDA(cudaStreamSynchronize(h->c.st));
+  return EXA_OK;
+}
+
+int exa_gmres(exa_ctx* h, int* iters, double* relerr) {
+  EXA_TRY(guard(h));
+  int it = 0;
+  double re = 0.0;
+  EXA_TRY(exa_drv_gmres(h->c, &it, &re));
+  if (iters) *iters = it;
+  if (relerr) *relerr = re;
+  return EXA_OK;
+}
+
+int exa_getq(exa_ctx* h) {
+  EXA_TRY(guard(h));
+  EXA_TRY(exa_drv_getq(h->c));
+  EXA_CUDA(cudaStreamSynchronize(h->c.st));
+  return EXA_OK;
+}
+
+int exa_newton(exa_ctx* h, int* iters, double* norm) {
+  EXA_TRY(guard(h));
+  int it = 0;
+  double nr = 0.0;
+  int s = exa_drv_newton(h->c, &it, &nr);
+  if (iters) *iters = it;
+  if (norm) *norm = nr;
+  EXA_CUDA(cudaStreamSynchronize(h->c.st));
+  return s;
+}
+
+int exa_dirk(exa_ctx* h, int nsteps, int* newton_iters, int max_out) {
+  EXA_TRY(guard(h));
+  return exa_drv_dirk(h->c, nsteps, newton_iters, max_out);
+}
+
+int exa_solve(exa_ctx* h, const double* udg_in, const double* uh_in, double* udg_out, double* uh_out, int* iters,
+              double* norm) {
+  EXA_TRY(guard(h));
+  ExaCtx& c = h->c;
+  const size_t nu = (size_t)c.P.npe * c.P.nc * c.P.ne, nh = (size_t)c.ndofuhat();
+  if (udg_in) EXA_CUDA(cudaMemcpyAsync(c.udg, udg_in, sizeof(double) * nu, cudaMemcpyHostToDevice, c.st));
+  if (uh_in) EXA_CUDA(cudaMemcpyAsync(c.uh, uh_in, sizeof(double) * nh, cudaMemcpyHostToDevice, c.st));
+  int it = 0;
+  double nr = 0.0;
+  int s = exa_drv_newton(c, &it, &nr);
+  if (iters) *iters = it;
+  if (norm) *norm = nr;
+  if (s != EXA_OK) return s;
+  if (udg_out) EXA_CUDA(cudaMemcpyAsync(udg_out, c.udg, sizeof(double) * nu, cudaMemcpyDeviceToHost, c.st));
+  if (uh_out) EXA_CUDA(cudaMemcpyAsync(uh_out, c.uh, sizeof(double) * nh, cudaMemcpyDeviceToHost, c.st));
+  EXA_CUDA(cudaStreamSynchronize(c.st));
+  return EXA_OK;
+}
+
+int exa_stats(exa_ctx* h, long long* out) {
+  EXA_TRY(guard(h));
+  out[0] = h->c.last_gmres_iters;
+  out[1] = h->c.last_newton_iters;
+  out[2] = h->c.total_gmres_iters;
+  out[3] = 0;
+  return EXA_OK;
+}
+
+int exa_synchronize(exa_ctx* h) {
+  EXA_TRY(guard(h));
+  EXA_CUDA(cudaStreamSynchronize(h->c.st));
+  return EXA_OK;
+}
+
+}  // extern "C"
+
+extern "C" int exa_connectivity_host(const int* t, const int* bf, const int* perm, const double* xpf, int dim,
+                                     int elemtype, int ne, int npe, int npf, int* f2e, int* elemcon, int* nf0) {
+  ExaConn conn;
+  const int nf = exa_build_connectivity(t, bf, perm, xpf, dim, elemtype, ne, npe, npf, conn);
+  if (nf < 0) {
+    exa_set_error("mesh connectivity is wrong (unmatched face)");
+    return -EXA_ERR_MESH;
+  }
+  std::memcpy(f2e, conn.f2e.data(), sizeof(int) * conn.f2e.size());
+  std::memcpy(elemcon, conn.elemcon.data(), sizeof(int) * conn.elemcon.size());
+  *nf0 = conn.nf0;
+  return nf;
+}

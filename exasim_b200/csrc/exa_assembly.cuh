@@ -1,0 +1,464 @@
+// HDG element assembly kernels, templated on the pointwise model (device functions
+// produced by exasim_b200/modelc.py from Exasim's generated sources).  Included once by
+// each model's translation unit.
+//
+// Reference steps (backend/Discretization/uequation.cpp):
+//   volume   :45-203   uq at quadrature points, Source/Flux with Jacobians, the DIRK
+//                      term, ApplyXxJac, then Ru (Gauss2Node with shapegw) and D, B
+//                      (Gauss2Node with shapegw x shapegt, negated)
+//   faces    :206-557  (uhat, q) at face points, numerical flux f(uhat,q).n + tau(u-uhat)
+//                      for Ru, D, B, F on every face; boundary faces replace the flux by
+//                      Fbou for the trace rows Rh, K, G, H
+//   residual :790-1088 the same without Jacobians (Flux/Source/Fbouonly)
+// One block per element; all of an element's faces are handled by the same block in
+// sequence, so face contributions accumulate into D, B and Ru without atomics.
+#pragma once
+#include "exa_kernels.cuh"
+
+struct AsmArgs {
+  ExaDims P;
+  const double *shapegt, *shapegw, *shapfgt, *shapfgw;
+  const int *perm, *elemcon, *bf;
+  const double *elemg, *faceg;
+  const double *uinf, *param, *tau;
+  const double *udg, *uh, *sdg;
+  double time, dtfactor;
+  int tdep, tdfunc, sourcefunc, modelnumber;
+  int e0;  // first element of the chunk; per-chunk outputs are indexed from it
+};
+
+// ----------------------------------------------------------------------------------
+// volume: quadrature-point values, Ru (volume part) and the Jacobian integrands rgJ
+// rgJ per element: [nge, nd+1, ncu, nc]
+// ----------------------------------------------------------------------------------
+template <class Mdl, bool JAC>
+__global__ void vol_points_kernel(AsmArgs A, double* Ru, double* rgJ) {
+  extern __shared__ double sm[];
+  const ExaDims& P = A.P;
+  const int le = blockIdx.x, e = A.e0 + le;
+  const int npe = P.npe, nge = P.nge, nc = P.nc, ncu = P.ncu, nd = P.nd, ncx = P.ncx;
+  double* un = sm;                       // npe*nc
+  double* ug = un + npe * nc;            // nge*nc
+  double* xg = ug + nge * nc;            // nge*ncx
+  double* sg = xg + nge * ncx;           // nge*ncu
+  double* fg = sg + nge * ncu;           // nge*ncu*nd
+  double* sdgg = fg + nge * ncu * nd;    // nge*ncu
+  double* td = sdgg + nge * ncu;         // nge*ncu
+  double* rgR = td + nge * ncu;          // nge*(nd+1)*ncu
+  double* sJ = rgR + nge * (nd + 1) * ncu;  // nge*ncu*nc      (JAC)
+  double* fJ = sJ + nge * ncu * nc;         // nge*ncu*nd*nc   (JAC)
+
+  const double* eg = A.elemg + (long long)e * P.elemg_stride();
+  const double* Xx = eg + nge * ncx;
+  const double* jac = Xx + nge * nd * nd;
+  const double* U = A.udg + (long long)e * npe * nc;
+  for (int t = threadIdx.x; t < npe * nc; t += blockDim.x) un[t] = U[t];
+  for (int t = threadIdx.x; t < nge * ncx; t += blockDim.x) xg[t] = eg[t];
+  for (int t = threadIdx.x; t < nge * ncu * nd; t += blockDim.x) fg[t] = 0.0;
+  for (int t = threadIdx.x; t < nge * ncu; t += blockDim.x) sg[t] = 0.0;
+  if (JAC) {
+    for (int t = threadIdx.x; t < nge * ncu * nc; t += blockDim.x) sJ[t] = 0.0;
+    for (int t = threadIdx.x; t < nge * ncu * nd * nc; t += blockDim.x) fJ[t] = 0.0;
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < nge * nc; t += blockDim.x) {
+    const int g = t % nge, c = t / nge;
+    double s = 0.0;
+    for (int j = 0; j < npe; ++j) s = fma(A.shapegt[g + nge * j], un[j + npe * c], s);
+    ug[t] = s;
+  }
+  if (A.tdep) {
+    const double* S = A.sdg + (long long)e * npe * ncu;
+    for (int t = threadIdx.x; t < nge * ncu; t += blockDim.x) {
+      const int g = t % nge, k = t / nge;
+      double s = 0.0;
+      for (int j = 0; j < npe; ++j) s = fma(A.shapegt[g + nge * j], S[j + npe * k], s);
+      sdgg[t] = s;
+    }
+  }
+  __syncthreads();
+  for (int g = threadIdx.x; g < nge; g += blockDim.x) {
+    if (JAC) {
+      Mdl::source(g, sg, sJ, nullptr, xg, ug, nullptr, nullptr, A.uinf, A.param, A.time, A.modelnumber, nge, nc,
+                  ncu, nd, ncx, P.nco, P.ncw);
+      Mdl::flux(g, fg, fJ, nullptr, xg, ug, nullptr, nullptr, A.uinf, A.param, A.time, A.modelnumber, nge, nc, ncu,
+                nd, ncx, P.nco, P.ncw);
+    } else {
+      if (!A.tdep || A.sourcefunc == 1)
+        Mdl::source_only(g, sg, xg, ug, nullptr, nullptr, A.uinf, A.param, A.time, A.modelnumber, nge, nc, ncu, nd,
+                         ncx, P.nco, P.ncw);
+      Mdl::flux_only(g, fg, xg, ug, nullptr, nullptr, A.uinf, A.param, A.time, A.modelnumber, nge, nc, ncu, nd, ncx,
+                     P.nco, P.ncw);
+    }
+    if (A.tdep) {
+      if (A.tdfunc == 1)
+        Mdl::tdfunc(g, td, xg, ug, nullptr, nullptr, A.uinf, A.param, A.time, A.modelnumber, nge, nc, ncu, nd, ncx,
+                    P.nco, P.ncw);
+      else
+        for (int k = 0; k < ncu; ++k) td[g + nge * k] = 1.0;
+    }
+  }
+  __syncthreads();
+  if (A.tdep) {
+    // s += (sdg - dtfactor*u) * Tdfunc ; ds/du -= dtfactor * Tdfunc  (uequation.cpp:126-151)
+    for (int t = threadIdx.x; t < nge * ncu; t += blockDim.x) {
+      double f = 1.0 * sdgg[t] + (-A.dtfactor) * ug[t];
+      if (JAC || A.tdfunc == 1) f = 1.0 * f * td[t];
+      sg[t] = 1.0 * sg[t] + 1.0 * f;
+      if (JAC) {
+        const int g = t % nge, k = t / nge;
+        sJ[g + nge * k + nge * ncu * k] += (-A.dtfactor) * td[t];
+      }
+    }
+    __syncthreads();
+  }
+  // ApplyXxJac (kokkosimpl.h:2105-2159)
+  for (int t = threadIdx.x; t < nge * ncu; t += blockDim.x) {
+    const int g = t % nge, k = t / nge;
+    rgR[g + nge * (nd + 1) * k] = sg[t] * jac[g];
+    for (int mm = 0; mm < nd; ++mm) {
+      double s = fg[g + nge * k] * Xx[g + nge * (nd * mm)];
+      for (int j = 1; j < nd; ++j) s += fg[g + nge * (k + ncu * j)] * Xx[g + nge * (j + nd * mm)];
+      rgR[g + nge * (1 + mm) + nge * (nd + 1) * k] = s;
+    }
+  }
+  if (JAC) {
+    double* R = rgJ + (long long)le * nge * (nd + 1) * ncu * nc;
+    for (int t = threadIdx.x; t < nge * ncu * nc; t += blockDim.x) {
+      const int g = t % nge, k = (t / nge) % ncu, c = t / (nge * ncu);
+      const long long base = (long long)nge * (nd + 1) * (k + ncu * c);
+      R[g + base] = sJ[t] * jac[g];
+      for (int mm = 0; mm < nd; ++mm) {
+        double s = fJ[g + nge * (k + ncu * nd * c)] * Xx[g + nge * (nd * mm)];
+        for (int j = 1; j < nd; ++j) s += fJ[g + nge * (k + ncu * j + ncu * nd * c)] * Xx[g + nge * (j + nd * mm)];
+        R[g + nge * (1 + mm) + base] = s;
+      }
+    }
+  }
+  __syncthreads();
+  // Ru(i,k) = sum_{g,d} shapegw[i,g,d] rgR[g,d,k]
+  const int K = nge * (nd + 1);
+  for (int t = threadIdx.x; t < npe * ncu; t += blockDim.x) {
+    const int i = t % npe, k = t / npe;
+    double s = 0.0;
+    for (int q = 0; q < K; ++q) s = fma(A.shapegw[i + npe * q], rgR[q + K * k], s);
+    Ru[(long long)le * P.n + t] = s;
+  }
+}
+
+template <bool JAC>
+inline size_t vol_points_smem(const ExaDims& P) {
+  size_t s = (size_t)P.npe * P.nc + (size_t)P.nge * (P.nc + P.ncx + P.ncu + P.ncu * P.nd + 2 * P.ncu +
+                                                      (P.nd + 1) * P.ncu);
+  if (JAC) s += (size_t)P.nge * P.ncu * P.nc * (1 + P.nd);
+  return s * sizeof(double);
+}
+
+// ----------------------------------------------------------------------------------
+// D and B volume blocks: for each (k, c) pair,
+//   M[i, j] = - sum_g ( sum_d shapegw[i,g,d] rgJ[g,d,k,c] ) shapegt[g,j]
+// (the reference contracts shapegw x shapegt over (g,d) in one GEMM; summing over d
+// first is the same sum with fewer products).  c < ncu goes to D[(i,k),(j,c)],
+// c = ncu + nq + ncu*d goes to B[(i,k), j + npe*d + npe*nd*nq].
+// Grid: (tiles, elements, ncu*nc); 64x64 tiles as exa_gemm.
+// ----------------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) vol_mat_kernel(ExaDims P, const double* shapegw, const double* shapegt,
+                                                      const double* rgJ, double* D, double* B) {
+  constexpr int TMv = 64, TNv = 64, TKv = 16;
+  __shared__ double As[TKv][TMv + 1];
+  __shared__ double Bs[TKv][TNv + 1];
+  const int npe = P.npe, nge = P.nge, nd = P.nd, ncu = P.ncu, n = P.n;
+  const int tiles = (npe + TMv - 1) / TMv;
+  const int tm = blockIdx.x % tiles, tn = blockIdx.x / tiles;
+  const int le = blockIdx.y, kc = blockIdx.z;
+  const int k = kc % ncu, c = kc / ncu;
+  const double* R = rgJ + (long long)le * nge * (nd + 1) * ncu * P.nc + (long long)nge * (nd + 1) * kc;
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  const int r0 = tm * TMv, c0 = tn * TNv;
+  double acc[4][4];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
+  for (int g0 = 0; g0 < nge; g0 += TKv) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int t = threadIdx.x + 256 * q;
+      const int r = t & 63, kk = t >> 6;
+      const int gi = r0 + r, gg = g0 + kk;
+      double v = 0.0;
+      if (gi < npe && gg < nge)
+        for (int d = 0; d <= nd; ++d) v = fma(shapegw[gi + npe * gg + npe * nge * d], R[gg + nge * d], v);
+      As[kk][r] = v;
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int t = threadIdx.x + 256 * q;
+      const int kk = t & 15, cc = t >> 4;
+      const int gg = g0 + kk, gj = c0 + cc;
+      Bs[kk][cc] = (gg < nge && gj < npe) ? shapegt[gg + nge * gj] : 0.0;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < TKv; ++kk) {
+      double av[4], bv[4];
+#pragma unroll
+      for (int a = 0; a < 4; ++a) av[a] = As[kk][ty + 16 * a];
+#pragma unroll
+      for (int b = 0; b < 4; ++b) bv[b] = Bs[kk][tx + 16 * b];
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) acc[a][b] = fma(av[a], bv[b], acc[a][b]);
+    }
+    __syncthreads();
+  }
+  double* out;
+  long long col0, ld = n;
+  if (c < ncu) {
+    out = D + (long long)le * n * n;
+    col0 = (long long)npe * c;
+  } else {
+    const int qc = c - ncu, nq = qc % ncu, d = qc / ncu;
+    out = B + (long long)le * n * npe * nd * ncu;
+    col0 = (long long)npe * d + (long long)npe * nd * nq;
+  }
+#pragma unroll
+  for (int a = 0; a < 4; ++a) {
+    const int i = r0 + ty + 16 * a;
+    if (i >= npe) continue;
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      const int j = c0 + tx + 16 * b;
+      if (j >= npe) continue;
+      out[(i + npe * k) + ld * (col0 + j)] = -acc[a][b];
+    }
+  }
+}
+
+// ----------------------------------------------------------------------------------
+// faces.  Per element face l (processed in order by the whole block):
+//   uhat, (u, q) at the face nodes (elemcon / perm), then at the face points;
+//   numerical flux fh = f(uhat, q).n + tau (u - uhat) and its derivatives
+//   (FhatDriver, backend/Model/ModelDrivers.cpp:789-849), times the face jacobian;
+//   interior formula into Ru, D, B, F; trace rows (Fbou on boundary faces) into
+//   Rh, K, G, H (uequation.cpp:300-487, kokkosimpl.h:1650-1730).
+// JAC = false computes Ru and Rh only (RuEquationElemFaceBlock, uequation.cpp:883-1077).
+// F, K, G, H must be zero on entry; Ru holds the volume part.
+// ----------------------------------------------------------------------------------
+template <class Mdl, bool JAC>
+__global__ void face_kernel(AsmArgs A, double* Ru, double* Rh, double* D, double* B, double* F, double* K,
+                            double* G, double* H) {
+  extern __shared__ double sm[];
+  const ExaDims& P = A.P;
+  const int le = blockIdx.x, e = A.e0 + le;
+  const int npe = P.npe, npf = P.npf, ngf = P.ngf, nc = P.nc, ncu = P.ncu, nd = P.nd, ncx = P.ncx;
+  const int nfe = P.nfe, ndf = P.ndf, n = P.n, m = P.m;
+  const int nqn = npe * nd * ncu;  // columns of B and G
+  double* uhn = sm;                   // npf*ncu
+  double* un = uhn + npf * ncu;       // npf*nc
+  double* uhg = un + npf * nc;        // ngf*ncu
+  double* ugq = uhg + ngf * ncu;      // ngf*nc   (u, q)
+  double* uqh = ugq + ngf * nc;       // ngf*nc   (uhat, q)
+  double* fg = uqh + ngf * nc;        // ngf*ncu*nd
+  double* fh = fg + ngf * ncu * nd;   // ngf*ncu
+  double* fb = fh + ngf * ncu;        // ngf*ncu
+  double* fJ = fb + ngf * ncu;        // ngf*ncu*nd*nc   (JAC)
+  double* fh_uq = fJ + ngf * ncu * nd * nc;  // ngf*ncu*nc
+  double* fh_uh = fh_uq + ngf * ncu * nc;    // ngf*ncu*ncu
+  double* fb_uq = fh_uh + ngf * ncu * ncu;   // ngf*ncu*nc
+  double* fb_uh = fb_uq + ngf * ncu * nc;    // ngf*ncu*ncu
+  __shared__ int s_ib;
+
+  const double* U = A.udg + (long long)e * npe * nc;
+  double* Rue = Ru + (long long)le * n;
+  double* Rhe = Rh + (long long)le * m;
+  const double tau0 = A.tau[0];
+  for (int l = 0; l < nfe; ++l) {
+    const double* fgeo = A.faceg + ((long long)e * nfe + l) * P.faceg_stride();
+    const double* xg = fgeo;
+    const double* nl = fgeo + ngf * ncx;
+    const double* jac = nl + ngf * nd;
+    const int* pl = A.perm + npf * l;
+    if (threadIdx.x == 0) s_ib = A.bf[l + nfe * e];
+    for (int t = threadIdx.x; t < npf * ncu; t += blockDim.x) {
+      const int a = t % npf, k = t / npf;
+      uhn[t] = A.uh[k + ncu * (long long)A.elemcon[a + npf * l + ndf * e]];
+    }
+    for (int t = threadIdx.x; t < npf * nc; t += blockDim.x) {
+      const int a = t % npf, c = t / npf;
+      un[t] = U[pl[a] + npe * c];
+    }
+    for (int t = threadIdx.x; t < ngf * ncu * nd; t += blockDim.x) fg[t] = 0.0;
+    if (JAC)
+      for (int t = threadIdx.x; t < ngf * ncu * nd * nc; t += blockDim.x) fJ[t] = 0.0;
+    for (int t = threadIdx.x; t < ngf * ncu; t += blockDim.x) fb[t] = 0.0;
+    if (JAC) {
+      for (int t = threadIdx.x; t < ngf * ncu * nc; t += blockDim.x) fb_uq[t] = 0.0;
+      for (int t = threadIdx.x; t < ngf * ncu * ncu; t += blockDim.x) fb_uh[t] = 0.0;
+    }
+    __syncthreads();
+    const int ib = s_ib;
+    for (int t = threadIdx.x; t < ngf * ncu; t += blockDim.x) {
+      const int g = t % ngf, k = t / ngf;
+      double s = 0.0;
+      for (int a = 0; a < npf; ++a) s = fma(A.shapfgt[g + ngf * a], uhn[a + npf * k], s);
+      uhg[t] = s;
+    }
+    for (int t = threadIdx.x; t < ngf * nc; t += blockDim.x) {
+      const int g = t % ngf, c = t / ngf;
+      double s = 0.0;
+      for (int a = 0; a < npf; ++a) s = fma(A.shapfgt[g + ngf * a], un[a + npf * c], s);
+      ugq[t] = s;
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < ngf * nc; t += blockDim.x) uqh[t] = (t < ngf * ncu) ? uhg[t] : ugq[t];
+    __syncthreads();
+    for (int g = threadIdx.x; g < ngf; g += blockDim.x) {
+      if (JAC) {
+        Mdl::flux(g, fg, fJ, nullptr, xg, uqh, nullptr, nullptr, A.uinf, A.param, A.time, A.modelnumber, ngf, nc, ncu,
+                  nd, ncx, P.nco, P.ncw);
+        if (ib > 0)
+          Mdl::fbou(g, fb, fb_uq, nullptr, fb_uh, xg, ugq, nullptr, nullptr, uhg, nl, A.tau, A.uinf, A.param, A.time,
+                    A.modelnumber, ib, ngf, nc, ncu, nd, ncx, P.nco, P.ncw);
+      } else {
+        Mdl::flux_only(g, fg, xg, uqh, nullptr, nullptr, A.uinf, A.param, A.time, A.modelnumber, ngf, nc, ncu, nd, ncx,
+                       P.nco, P.ncw);
+        if (ib > 0)
+          Mdl::fbou_only(g, fb, xg, ugq, nullptr, nullptr, uhg, nl, A.tau, A.uinf, A.param, A.time, A.modelnumber, ib,
+                         ngf, nc, ncu, nd, ncx, P.nco, P.ncw);
+      }
+    }
+    __syncthreads();
+    // f.n, derivatives, stabilisation, face jacobian (FluxDotNormal, AddStabilization1,
+    // columnwiseMultiply)
+    for (int t = threadIdx.x; t < ngf * ncu; t += blockDim.x) {
+      const int g = t % ngf, k = t / ngf;
+      double s = fg[g + ngf * k] * nl[g];
+      for (int d = 1; d < nd; ++d) s += fg[g + ngf * (k + ncu * d)] * nl[g + ngf * d];
+      s += tau0 * (ugq[t] - uhg[t]);
+      fh[t] = s * jac[g];
+      if (ib > 0) fb[t] = fb[t] * jac[g];
+      if (JAC) {
+        for (int c = 0; c < nc; ++c) {
+          double v = fJ[g + ngf * (k + ncu * nd * c)] * nl[g];
+          for (int d = 1; d < nd; ++d) v += fJ[g + ngf * (k + ncu * d + ncu * nd * c)] * nl[g + ngf * d];
+          if (c < ncu) {
+            double vh = v, vu = 0.0;
+            if (c == k) {
+              vu += tau0;
+              vh -= tau0;
+            }
+            fh_uh[g + ngf * (k + ncu * c)] = vh * jac[g];
+            fh_uq[g + ngf * (k + ncu * c)] = vu * jac[g];
+          } else {
+            fh_uq[g + ngf * (k + ncu * c)] = v * jac[g];
+          }
+          if (ib > 0) {
+            fb_uq[g + ngf * (k + ncu * c)] *= jac[g];
+            if (c < ncu) fb_uh[g + ngf * (k + ncu * c)] *= jac[g];
+          }
+        }
+      }
+    }
+    __syncthreads();
+    const double* fT = (ib > 0) ? fb : fh;
+    // Ru -= shapfgw . fh at this face's element nodes; Rh = -shapfgw . fT
+    for (int t = threadIdx.x; t < npf * ncu; t += blockDim.x) {
+      const int a = t % npf, k = t / npf;
+      double s = 0.0, r = 0.0;
+      for (int g = 0; g < ngf; ++g) {
+        s = fma(A.shapfgw[a + npf * g], fh[g + ngf * k], s);
+        r = fma(A.shapfgw[a + npf * g], fT[g + ngf * k], r);
+      }
+      Rue[pl[a] + npe * k] -= s;
+      Rhe[k + ncu * (a + npf * l)] = -r;
+    }
+    if (JAC) {
+      const double* fT_uq = (ib > 0) ? fb_uq : fh_uq;
+      const double* fT_uh = (ib > 0) ? fb_uh : fh_uh;
+      double* De = D + (long long)le * n * n;
+      double* Be = B + (long long)le * n * nqn;
+      double* Fe = F + (long long)le * n * m;
+      double* Ke = K + (long long)le * m * n;
+      double* Ge = G + (long long)le * m * nqn;
+      double* He = H + (long long)le * m * m;
+      for (int t = threadIdx.x; t < npf * npf * ncu * nc; t += blockDim.x) {
+        const int a = t % npf, b = (t / npf) % npf, k = (t / (npf * npf)) % ncu, c = t / (npf * npf * ncu);
+        double vq = 0.0, vT = 0.0, vh = 0.0, vTh = 0.0;
+        for (int g = 0; g < ngf; ++g) {
+          const double w = A.shapfgw[a + npf * g] * A.shapfgt[g + ngf * b];
+          vq = fma(w, fh_uq[g + ngf * (k + ncu * c)], vq);
+          vT = fma(w, fT_uq[g + ngf * (k + ncu * c)], vT);
+          if (c < ncu) {
+            vh = fma(w, fh_uh[g + ngf * (k + ncu * c)], vh);
+            vTh = fma(w, fT_uh[g + ngf * (k + ncu * c)], vTh);
+          }
+        }
+        const int row_e = pl[a] + npe * k;           // element row (i,k)
+        const int row_t = k + ncu * (a + npf * l);   // trace row (k, jf)
+        if (c < ncu) {
+          De[row_e + (long long)n * (pl[b] + npe * c)] += vq;
+          Fe[row_e + (long long)n * (c + ncu * (b + npf * l))] = vh;
+          Ke[row_t + (long long)m * (pl[b] + npe * c)] = vT;
+          He[row_t + (long long)m * (c + ncu * (b + npf * l))] = vTh;
+        } else {
+          const int qc = c - ncu, nq = qc % ncu, d = qc / ncu;
+          const long long col = pl[b] + (long long)npe * d + (long long)npe * nd * nq;
+          Be[row_e + (long long)n * col] += vq;
+          Ge[row_t + (long long)m * col] = vT;
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
+inline size_t face_smem(const ExaDims& P, bool jac) {
+  size_t s = (size_t)P.npf * (P.ncu + P.nc) + (size_t)P.ngf * (P.ncu + 2 * P.nc + P.ncu * P.nd + 2 * P.ncu);
+  if (jac) s += (size_t)P.ngf * P.ncu * (P.nd * P.nc + 2 * P.nc + 2 * P.ncu);
+  return s * sizeof(double);
+}
+
+// Binds a generated model namespace to the argument roles the kernels use
+// (Exasim's DefaultModel functors, backend/Model/modeltemplate.hpp:377-457).
+#define EXA_BIND_MODEL(NS)                                                                                      \
+  struct ExaModel {                                                                                             \
+    __device__ static void flux(size_t i, double* f, double* J1, double* J2, const double* x, const double* uq,  \
+                                const double* v, const double* w, const double* eta, const double* mu,          \
+                                double t, int mn, int N, int a, int b, int c, int d, int e, int h) {           \
+      NS::HdgFlux_pt(i, f, J1, J2, x, uq, v, w, eta, mu, t, mn, N, a, b, c, d, e, h);                            \
+    }                                                                                                           \
+    __device__ static void source(size_t i, double* f, double* J1, double* J2, const double* x, const double* uq, \
+                                  const double* v, const double* w, const double* eta, const double* mu,        \
+                                  double t, int mn, int N, int a, int b, int c, int d, int e, int h) {         \
+      NS::HdgSource_pt(i, f, J1, J2, x, uq, v, w, eta, mu, t, mn, N, a, b, c, d, e, h);                          \
+    }                                                                                                           \
+    __device__ static void flux_only(size_t i, double* f, const double* x, const double* uq, const double* v,    \
+                                     const double* w, const double* eta, const double* mu, double t, int mn,    \
+                                     int N, int a, int b, int c, int d, int e, int h) {                         \
+      NS::KokkosFlux_pt(i, f, x, uq, v, w, eta, mu, t, mn, N, a, b, c, d, e, h);                                 \
+    }                                                                                                           \
+    __device__ static void source_only(size_t i, double* f, const double* x, const double* uq, const double* v,  \
+                                       const double* w, const double* eta, const double* mu, double t, int mn,  \
+                                       int N, int a, int b, int c, int d, int e, int h) {                       \
+      NS::KokkosSource_pt(i, f, x, uq, v, w, eta, mu, t, mn, N, a, b, c, d, e, h);                               \
+    }                                                                                                           \
+    __device__ static void tdfunc(size_t i, double* f, const double* x, const double* uq, const double* v,       \
+                                  const double* w, const double* eta, const double* mu, double t, int mn, int N, \
+                                  int a, int b, int c, int d, int e, int h) {                                   \
+      NS::KokkosTdfunc_pt(i, f, x, uq, v, w, eta, mu, t, mn, N, a, b, c, d, e, h);                               \
+    }                                                                                                           \
+    __device__ static void fbou(size_t i, double* f, double* J1, double* J2, double* J3, const double* x,        \
+                                const double* uq, const double* v, const double* w, const double* uh,           \
+                                const double* nl, const double* tau, const double* eta, const double* mu,       \
+                                double t, int mn, int ib, int N, int a, int b, int c, int d, int e, int h) {   \
+      NS::HdgFbou_pt(i, f, J1, J2, J3, x, uq, v, w, uh, nl, tau, eta, mu, t, mn, ib, N, a, b, c, d, e, h);       \
+    }                                                                                                           \
+    __device__ static void fbou_only(size_t i, double* f, const double* x, const double* uq, const double* v,    \
+                                     const double* w, const double* uh, const double* nl, const double* tau,    \
+                                     const double* eta, const double* mu, double t, int mn, int ib, int N,     \
+                                     int a, int b, int c, int d, int e, int h) {                                \
+      NS::HdgFbouonly_pt(i, f, x, uq, v, w, uh, nl, tau, eta, mu, t, mn, ib, N, a, b, c, d, e, h);               \
+    }                                                                                                           \
+  };

@@ -1,0 +1,348 @@
+// Linear-system, Krylov, Newton and DIRK drivers on top of the device kernels.
+// The control flow is Exasim's (references at each function); all vectors stay on
+// the device, and the host reads one scalar per GMRES iteration (the Givens residual)
+// as the reference does with its host-side Givens rotations.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "exa_solver.cuh"
+
+int exa_drv_norm(ExaCtx& c, const double* x, long long n, double* out) {
+  EXA_TRY(exa_dot_partials(x, x, n, c.part_a, c.st));
+  EXA_TRY(exa_reduce_partials(c.part_a, c.scal + 15, 1, c.st));
+  EXA_CUDA(cudaMemcpyAsync(c.pinned, c.scal + 15, sizeof(double), cudaMemcpyDeviceToHost, c.st));
+  EXA_CUDA(cudaStreamSynchronize(c.st));
+  *out = c.pinned[0];
+  return EXA_OK;
+}
+
+// hdgAssembleRHS + preconditioner setup (discretization.cpp:483-573, matvec.cpp:103-217)
+int exa_drv_build_precond(ExaCtx& c) {
+  const ExaDims& P = c.P;
+  if (c.preconditioner == 0) {
+    EXA_TRY(exa_k_bj_build(P, c.f2e, c.elemcon, c.H, c.Pc, c.st));
+    const int ncf = P.ncu * P.npf;
+    EXA_TRY(exa_inverse(c.Pc, ncf, (long long)ncf * ncf, P.nf, c.d_flag, c.st));
+  } else {
+    EXA_TRY(exa_k_eas_build(P, c.f2e, c.elemcon, c.H, c.Pc, c.st));
+    EXA_TRY(exa_inverse(c.Pc, P.m, (long long)P.m * P.m, P.ne, c.d_flag, c.st));
+  }
+  return EXA_OK;
+}
+
+int exa_drv_assemble(ExaCtx& c) {
+  EXA_CUDA(cudaMemsetAsync(c.d_flag, 0, sizeof(int), c.st));
+  EXA_TRY(exa_model_assemble(c, true));
+  EXA_TRY(exa_k_scatter(c.P, c.f2e, c.elemcon, c.Rh, c.b, c.st));
+  EXA_TRY(exa_drv_build_precond(c));
+  int flag = 0;
+  EXA_CUDA(cudaMemcpyAsync(c.pinned, c.d_flag, sizeof(int), cudaMemcpyDeviceToHost, c.st));
+  EXA_CUDA(cudaStreamSynchronize(c.st));
+  std::memcpy(&flag, c.pinned, sizeof(int));
+  if (flag) {
+    exa_set_error("singular element or preconditioner block during assembly");
+    return EXA_ERR_SINGULAR;
+  }
+  return EXA_OK;
+}
+
+// hdgAssembleResidual: Ru, Rh, b; norm = |b| + |Ru| (solution.cpp:148-157)
+int exa_drv_residual(ExaCtx& c, double* norm) {
+  EXA_TRY(exa_model_assemble(c, false));
+  EXA_TRY(exa_k_scatter(c.P, c.f2e, c.elemcon, c.Rh, c.b, c.st));
+  if (norm) {
+    double nb = 0.0, nr = 0.0;
+    EXA_TRY(exa_drv_norm(c, c.b, c.ndofuhat(), &nb));
+    EXA_TRY(exa_drv_norm(c, c.Ru, (long long)c.P.n * c.P.ne, &nr));
+    *norm = nb + nr;
+  }
+  return EXA_OK;
+}
+
+// w = A v (hdgMatVec, matvec.cpp:240-389)
+int exa_drv_matvec(ExaCtx& c, const double* v, double* w) {
+  EXA_TRY(exa_k_elem_matvec(c.P, c.elemcon, c.H, v, c.we, c.st));
+  EXA_TRY(exa_k_scatter(c.P, c.f2e, c.elemcon, c.we, w, c.st));
+  return EXA_OK;
+}
+
+// w = P v (ApplyPreconditioner, preconditioner.cpp:273-295); v and w may not alias
+int exa_drv_precond(ExaCtx& c, const double* v, double* w) {
+  if (c.preconditioner == 0) return exa_k_bj_apply(c.P, c.Pc, v, w, c.st);
+  EXA_TRY(exa_k_elem_matvec(c.P, c.elemcon, c.Pc, v, c.we, c.st));
+  return exa_k_scatter(c.P, c.f2e, c.elemcon, c.we, w, c.st);
+}
+
+int exa_drv_getq(ExaCtx& c) {
+  if (c.P.ncq == 0) return EXA_OK;
+  return exa_k_getq(c.P, c.elemcon, c.MC, c.ME, c.uh, c.udg, c.st);
+}
+
+namespace {
+
+// cpuBackSolve (backend/Common/cpuimpl.h:198-208)
+void back_solve(double* y, const double* H, const double* s, int i, int n) {
+  for (int j = i; j >= 0; j--) y[j] = s[j];
+  for (int j = i; j >= 0; j--) {
+    y[j] = y[j] / H[j + n * j];
+    for (int k = j - 1; k >= 0; k--) y[k] = y[k] - H[k + n * j] * y[j];
+  }
+}
+
+}  // namespace
+
+// GMRES (gmres.cpp:361-597): restarted, left-preconditioned, MGS (flag 0) or CGS (flag 1).
+// Solves A x = b for the current system; x starts at zero (no reduced basis).
+int exa_drv_gmres(ExaCtx& c, int* iters_out, double* relerr_out) {
+  const long long N = c.ndofuhat();
+  const int nrest = c.restart, maxit = c.gmres_maxit, n1 = nrest + 1;
+  double nrmb = 0.0, nrmr = 0.0;
+  EXA_CUDA(cudaMemsetAsync(c.x, 0, sizeof(double) * N, c.st));
+  EXA_TRY(exa_drv_norm(c, c.b, N, &nrmb));
+  if (nrmb < c.newton_tol) {
+    *iters_out = 0;
+    *relerr_out = 0.0;
+    return EXA_OK;
+  }
+  nrmr = nrmb;  // x = 0: r = b
+  const double tol = std::min(0.1, c.gmres_tol * (nrmb / nrmr));
+  EXA_TRY(exa_drv_precond(c, c.b, c.r));
+  EXA_TRY(exa_drv_norm(c, c.r, N, &nrmb));
+  nrmr = nrmb;
+  // device copy of nrmb for the Givens kernel
+  double* d_nrmb = c.scal + 14;
+  double* d_relerr = c.scal + 13;
+  c.pinned[0] = nrmb;
+  EXA_CUDA(cudaMemcpyAsync(d_nrmb, c.pinned, sizeof(double), cudaMemcpyHostToDevice, c.st));
+  std::vector<double> ybuf(n1);
+  int j = 0;
+  double relerr = 1.0;
+  double* yd = c.part_m;  // device copy of the back-solve result (part_m holds >= restart+1 doubles)
+  while (j < maxit) {
+    EXA_TRY(exa_scale(c.V, c.r, 1.0 / nrmr, N, c.st));
+    std::vector<double> s0(n1, 0.0);
+    s0[0] = nrmr;
+    std::copy(s0.begin(), s0.end(), c.pinned);
+    EXA_CUDA(cudaMemcpyAsync(c.gs, c.pinned, sizeof(double) * n1, cudaMemcpyHostToDevice, c.st));
+    int i = 0;
+    for (i = 0; i < nrest && j < maxit; i++, j++) {
+      double* vi = c.V + (long long)i * N;
+      double* vn = c.V + (long long)(i + 1) * N;
+      double* hcol = c.hess + (long long)n1 * i;
+      EXA_TRY(exa_drv_matvec(c, vi, c.w));
+      EXA_TRY(exa_drv_precond(c, c.w, vn));
+      if (c.ortho == 0) {
+        EXA_TRY(exa_dot_partials(vn, c.V, N, c.part_a, c.st));
+        double* pin = c.part_a;
+        double* pout = c.part_b;
+        for (int k = 1; k <= i; ++k) {
+          EXA_TRY(exa_mgs_step(vn, c.V + (long long)(k - 1) * N, c.V + (long long)k * N, pin, pout, hcol + k - 1, N, c.st));
+          std::swap(pin, pout);
+        }
+        EXA_TRY(exa_mgs_step(vn, c.V + (long long)i * N, nullptr, pin, pout, hcol + i, N, c.st));
+        EXA_TRY(exa_mgs_finish(vn, vn, pout, hcol + i + 1, N, c.st));
+      } else {
+        EXA_TRY(exa_cgs(vn, c.V, hcol, c.part_m, N, i + 1, c.st));
+        EXA_TRY(exa_dot_partials(vn, vn, N, c.part_a, c.st));
+        EXA_TRY(exa_mgs_finish(vn, vn, c.part_a, hcol + i + 1, N, c.st));
+      }
+      EXA_TRY(exa_givens(hcol, c.gs, c.gcs, c.gsn, i, d_nrmb, d_relerr, c.st));
+      EXA_CUDA(cudaMemcpyAsync(c.pinned, d_relerr, sizeof(double), cudaMemcpyDeviceToHost, c.st));
+      EXA_CUDA(cudaStreamSynchronize(c.st));
+      relerr = c.pinned[0];
+      if (relerr < tol) {
+        // UpdateSolution (gmres.cpp:132-137)
+        double* hh = c.pinned;
+        double* ss = hh + (size_t)n1 * nrest;
+        EXA_CUDA(cudaMemcpyAsync(hh, c.hess, sizeof(double) * n1 * nrest, cudaMemcpyDeviceToHost, c.st));
+        EXA_CUDA(cudaMemcpyAsync(ss, c.gs, sizeof(double) * n1, cudaMemcpyDeviceToHost, c.st));
+        EXA_CUDA(cudaStreamSynchronize(c.st));
+        back_solve(ybuf.data(), hh, ss, i, n1);
+        EXA_CUDA(cudaMemcpyAsync(yd, ybuf.data(), sizeof(double) * (i + 1), cudaMemcpyHostToDevice, c.st));
+        EXA_TRY(exa_gemv_add(c.x, c.V, yd, N, i + 1, c.st));
+        EXA_CUDA(cudaStreamSynchronize(c.st));
+        *iters_out = j + 1;
+        *relerr_out = relerr;
+        return EXA_OK;
+      }
+    }
+    {
+      double* hh = c.pinned;
+      double* ss = hh + (size_t)n1 * nrest;
+      EXA_CUDA(cudaMemcpyAsync(hh, c.hess, sizeof(double) * n1 * nrest, cudaMemcpyDeviceToHost, c.st));
+      EXA_CUDA(cudaMemcpyAsync(ss, c.gs, sizeof(double) * n1, cudaMemcpyDeviceToHost, c.st));
+      EXA_CUDA(cudaStreamSynchronize(c.st));
+      back_solve(ybuf.data(), hh, ss, i - 1, n1);
+      EXA_CUDA(cudaMemcpyAsync(yd, ybuf.data(), sizeof(double) * i, cudaMemcpyHostToDevice, c.st));
+      EXA_TRY(exa_gemv_add(c.x, c.V, yd, N, i, c.st));
+    }
+    // r = P (b - A x)
+    EXA_TRY(exa_drv_matvec(c, c.x, c.w));
+    EXA_TRY(exa_axpby(c.w, c.b, 1.0, -1.0, N, c.st));
+    EXA_TRY(exa_drv_precond(c, c.w, c.r));
+    EXA_TRY(exa_drv_norm(c, c.r, N, &nrmr));
+    relerr = nrmr / nrmb;
+    if (relerr < tol) {
+      *iters_out = j;
+      *relerr_out = relerr;
+      return EXA_OK;
+    }
+  }
+  *iters_out = j;
+  *relerr_out = relerr;
+  return EXA_OK;  // not converged: the reference warns and continues (gmres.cpp:586-594)
+}
+
+// NewtonSolver (solution.cpp:125-243)
+int exa_drv_newton(ExaCtx& c, int* iters_out, double* norm_out) {
+  const ExaDims& P = c.P;
+  const long long N = c.ndofuhat();
+  double nrmr = 0.0;
+  EXA_TRY(exa_drv_getq(c));
+  EXA_TRY(exa_drv_residual(c, &nrmr));
+  c.total_gmres_iters = 0;
+  for (int it = 0; it < c.newton_maxit; ++it) {
+    EXA_TRY(exa_drv_assemble(c));
+    int gi = 0;
+    double ge = 0.0;
+    EXA_TRY(exa_drv_gmres(c, &gi, &ge));
+    c.last_gmres_iters = gi;
+    c.last_gmres_relerr = ge;
+    c.total_gmres_iters += gi;
+    double alpha = 1.0;
+    // u += alpha x; uhat = u; du = Ru + DinvF x; udg(u) += alpha du
+    EXA_TRY(exa_axpby(c.uh, c.x, alpha, 1.0, N, c.st));
+    EXA_TRY(exa_k_dudg(P, c.elemcon, c.F, c.Ru, c.x, c.du, c.st));
+    EXA_TRY(exa_k_udg_update(P, c.udg, c.du, alpha, c.st));
+    EXA_TRY(exa_drv_getq(c));
+    const double nrm0 = nrmr;
+    EXA_TRY(exa_drv_residual(c, &nrmr));
+    if (nrmr > nrm0 && nrmr > 1.0e6) {
+      exa_set_error("Residual norm increases more than 1e6 (%g -> %g)", nrm0, nrmr);
+      *iters_out = it + 1;
+      *norm_out = nrmr;
+      return EXA_ERR_NOTCONV;
+    }
+    while ((nrmr > nrm0 && alpha > 0.1) || std::isnan(nrmr)) {
+      alpha = alpha / 2.0;
+      EXA_TRY(exa_axpby(c.uh, c.x, -alpha, 1.0, N, c.st));
+      EXA_TRY(exa_k_udg_update(P, c.udg, c.du, -alpha, c.st));
+      EXA_TRY(exa_drv_getq(c));
+      EXA_TRY(exa_drv_residual(c, &nrmr));
+      if (alpha < 1e-12) break;
+    }
+    c.last_newton_iters = it + 1;
+    if (std::isnan(nrmr)) {
+      exa_set_error("Newton residual is NaN");
+      *iters_out = it + 1;
+      *norm_out = nrmr;
+      return EXA_ERR_NAN;
+    }
+    if (nrmr < c.newton_tol) {
+      *iters_out = it + 1;
+      *norm_out = nrmr;
+      return EXA_OK;
+    }
+  }
+  *iters_out = c.newton_maxit;
+  *norm_out = nrmr;
+  return EXA_OK;
+}
+
+namespace {
+// DIRK tables (timestepcoeff.cpp:35-104): c, d (column-major nstage x nstage), t
+bool dirk_coeff(int nstage, int torder, std::vector<double>& cc, std::vector<double>& d, std::vector<double>& t) {
+  if (nstage == 1 && torder == 1) { cc = {1.0}; d = {1.0}; t = {1.0}; return true; }
+  if (nstage == 1 && torder == 2) { cc = {2.0}; d = {2.0}; t = {0.5}; return true; }
+  if (nstage == 2 && torder == 2) {
+    d = {3.414213562373096, -8.242640687119289, 0.0, 3.414213562373096}; cc = {0.0, 1.0};
+    t = {0.292893218813452, 1.0}; return true;
+  }
+  if (nstage == 2 && torder == 3) {
+    d = {1.267949192431123, 0.928203230275509, 0.0, 1.267949192431123}; cc = {1.098076211353316, 0.633974596215561};
+    t = {0.788675134594813, 0.211324865405187}; return true;
+  }
+  if (nstage == 3 && torder == 3) {
+    d = {2.294280360323567, -1.484721005721436, -8.556127801733982, 0.0, 2.294280360323568, 3.391748836909791,
+         0.0, 0.0, 2.294280360323567};
+    cc = {0.0, 0.0, 1.0}; t = {0.435866521500000, 0.717933260750000, 1.000000000000000}; return true;
+  }
+  if (nstage == 3 && torder == 4) {
+    d = {0.935822227524088, 0.497940606760015, -0.345865915800969, 0.0, 0.935822227524088, 2.867525668568206,
+         0.0, 0.0, 0.935822227524088};
+    cc = {0.445622407287714, 1.064177772475912, 0.120614758428183};
+    t = {1.068579021301629, 0.500000000000000, -0.068579021301629}; return true;
+  }
+  return false;
+}
+
+__global__ void extract_u_kernel(ExaDims P, const double* udg, double* u) {
+  const long long N = (long long)P.n * P.ne;
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < N; idx += (long long)gridDim.x * blockDim.x)
+    u[idx] = udg[idx % P.n + (long long)P.npe * P.nc * (idx / P.n)];
+}
+__global__ void insert_u_kernel(ExaDims P, double* udg, const double* u) {
+  const long long N = (long long)P.n * P.ne;
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < N; idx += (long long)gridDim.x * blockDim.x)
+    udg[idx % P.n + (long long)P.npe * P.nc * (idx / P.n)] = u[idx];
+}
+}  // namespace
+
+// DIRK time stepping around Newton (exasim.hpp:413-482, previoussolutions.cpp:23-45,
+// updatesource.cpp:32-80, updatesolution.cpp:118-140)
+int exa_drv_dirk(ExaCtx& c, int nsteps, int* its_out, int max_out) {
+  if (!c.tdep) { exa_set_error("app.bin is not time dependent"); return EXA_ERR_ARG; }
+  std::vector<double> cc, d, t;
+  if (!dirk_coeff(c.nstage, c.torder, cc, d, t)) { exa_set_error("DIRK(%d,%d) is not tabulated", c.nstage, c.torder); return EXA_ERR_UNSUPPORTED; }
+  const ExaDims& P = c.P;
+  const int S = c.nstage;
+  const long long Nu = (long long)P.n * P.ne;
+  const int blocks = 1024;
+  int count = 0;
+  for (int istep = 0; istep < nsteps; ++istep) {
+    if (istep >= (int)c.dt.size()) { exa_set_error("step %d beyond the dt list", istep); return EXA_ERR_ARG; }
+    const double dt = c.dt[istep];
+    double csum = 1.0;
+    for (int j = 0; j < S; ++j) csum -= cc[j];
+    extract_u_kernel<<<blocks, 256, 0, c.st>>>(P, c.udg, c.udgprev);
+    EXA_LAUNCH_CHECK();
+    EXA_TRY(exa_scale(c.utmp, c.udgprev, csum, Nu, c.st));
+    for (int j = 0; j < S; ++j) {
+      c.time = c.time0 + dt * t[j];
+      c.dtfactor = d[j * S + j] / dt;
+      // sdg from the stage history (UpdateSourceDIRK)
+      extract_u_kernel<<<blocks, 256, 0, c.st>>>(P, c.udg, c.du);
+      EXA_LAUNCH_CHECK();
+      if (j == 0) {
+        EXA_TRY(exa_scale(c.sdg, c.du, d[0] / dt, Nu, c.st));
+      } else if (j == 1) {
+        const double sc = (d[1] + d[S + 1]) / d[0];
+        EXA_TRY(exa_axpby(c.sdg, c.du, -d[1] / dt, sc, Nu, c.st));
+      } else if (j == 2) {
+        const double sc = d[2] / d[1];
+        const double pc = d[2] + d[S + 2] + d[2 * S + 2] - sc * (d[1] + d[S + 1]);
+        EXA_TRY(exa_axpby(c.sdg, c.du, -d[S + 2] / dt, sc, Nu, c.st));
+        EXA_TRY(exa_axpby(c.sdg, c.udgprev, pc / dt, 1.0, Nu, c.st));
+      } else {
+        exa_set_error("DIRK with more than 3 stages");
+        return EXA_ERR_UNSUPPORTED;
+      }
+      int its = 0;
+      double nrm = 0.0;
+      EXA_TRY(exa_drv_newton(c, &its, &nrm));
+      if (its_out && count < max_out) its_out[count] = its;
+      ++count;
+      // utmp += c_j u
+      extract_u_kernel<<<blocks, 256, 0, c.st>>>(P, c.udg, c.du);
+      EXA_LAUNCH_CHECK();
+      EXA_TRY(exa_axpby(c.utmp, c.du, cc[j], 1.0, Nu, c.st));
+    }
+    insert_u_kernel<<<blocks, 256, 0, c.st>>>(P, c.udg, c.utmp);
+    EXA_LAUNCH_CHECK();
+    c.time0 = c.time0 + dt;
+  }
+  EXA_CUDA(cudaStreamSynchronize(c.st));
+  return EXA_OK;
+}

@@ -1,0 +1,398 @@
+// Model-independent HDG kernels: geometry at quadrature points, the q-equation
+// element matrices, and the trace-space operations of the Krylov solver (gather /
+// scatter through the face connectivity, condensed matvec, block-Jacobi and
+// elemental additive-Schwarz preconditioners, Newton update of the element unknowns).
+// Every kernel maps one element (or one face) to one block, so the element-to-face
+// assembly needs no atomics: the first element of a face writes, the second adds,
+// as Exasim's PutElementFaceNodes pair does (backend/Common/kokkosimpl.h:1032-1065).
+#include "exa_kernels.cuh"
+
+namespace {
+
+// ----------------------------------------------------------------------------------
+// geometry (backend/Discretization/geometry.cpp:44-222, kokkosimpl.h:2321-2415)
+// elemg per element: xg [nge, ncx] | Xx [nge, nd*nd] | jac [nge]
+// faceg per element face: xg [ngf, ncx] | nl [ngf, nd] | jac [ngf]
+// ----------------------------------------------------------------------------------
+__global__ void elem_geom_kernel(ExaDims P, const double* shapegt, const double* xdg, double* elemg) {
+  const int e = blockIdx.x;
+  const int nge = P.nge, npe = P.npe, nd = P.nd, ncx = P.ncx;
+  const double* x = xdg + (long long)e * npe * ncx;
+  double* out = elemg + (long long)e * P.elemg_stride();
+  for (int g = threadIdx.x; g < nge; g += blockDim.x) {
+    double J[3][3];  // J[c][r] = d x_c / d xi_r
+    for (int c = 0; c < ncx; ++c) {
+      double s = 0.0;
+      for (int j = 0; j < npe; ++j) s += shapegt[g + nge * j] * x[j + npe * c];
+      out[g + nge * c] = s;
+    }
+    for (int c = 0; c < nd; ++c)
+      for (int r = 0; r < nd; ++r) {
+        double s = 0.0;
+        for (int j = 0; j < npe; ++j) s += shapegt[g + nge * j + nge * npe * (1 + r)] * x[j + npe * c];
+        J[c][r] = s;
+      }
+    double* Xx = out + nge * ncx;
+    double* jac = Xx + nge * nd * nd;
+    if (nd == 1) {
+      jac[g] = J[0][0];
+      Xx[g] = 1.0;
+    } else if (nd == 2) {
+      const double J11 = J[0][0], J12 = J[1][0], J21 = J[0][1], J22 = J[1][1];
+      jac[g] = J11 * J22 - J12 * J21;
+      Xx[g + nge * 0] = J22;    // Xx11
+      Xx[g + nge * 1] = -J21;   // Xx21 = jac * dxi/dy
+      Xx[g + nge * 2] = -J12;   // Xx12 = jac * deta/dx
+      Xx[g + nge * 3] = J11;    // Xx22
+    } else {
+      const double J11 = J[0][0], J12 = J[1][0], J13 = J[2][0];
+      const double J21 = J[0][1], J22 = J[1][1], J23 = J[2][1];
+      const double J31 = J[0][2], J32 = J[1][2], J33 = J[2][2];
+      jac[g] = J11 * J22 * J33 - J11 * J32 * J23 + J21 * J32 * J13 - J21 * J12 * J33 + J31 * J12 * J23 -
+               J31 * J22 * J13;
+      Xx[g + nge * 0] = J22 * J33 - J23 * J32;
+      Xx[g + nge * 1] = J23 * J31 - J21 * J33;
+      Xx[g + nge * 2] = J21 * J32 - J22 * J31;
+      Xx[g + nge * 3] = J13 * J32 - J12 * J33;
+      Xx[g + nge * 4] = J11 * J33 - J13 * J31;
+      Xx[g + nge * 5] = J12 * J31 - J11 * J32;
+      Xx[g + nge * 6] = J12 * J23 - J13 * J22;
+      Xx[g + nge * 7] = J13 * J21 - J11 * J23;
+      Xx[g + nge * 8] = J11 * J22 - J12 * J21;
+    }
+  }
+}
+
+__global__ void face_geom_kernel(ExaDims P, const double* shapfgt, const int* perm, const double* xdg,
+                                 double* faceg) {
+  const int e = blockIdx.x;
+  const int ngf = P.ngf, npf = P.npf, npe = P.npe, nd = P.nd, ncx = P.ncx;
+  const double* x = xdg + (long long)e * npe * ncx;
+  for (int t = threadIdx.x; t < ngf * P.nfe; t += blockDim.x) {
+    const int g = t % ngf, l = t / ngf;
+    double* out = faceg + ((long long)e * P.nfe + l) * P.faceg_stride();
+    double* nl = out + ngf * ncx;
+    double* jac = nl + ngf * nd;
+    for (int c = 0; c < ncx; ++c) {
+      double s = 0.0;
+      for (int a = 0; a < npf; ++a) s += shapfgt[g + ngf * a] * x[perm[a + npf * l] + npe * c];
+      out[g + ngf * c] = s;
+    }
+    if (nd == 1) {
+      jac[g] = 1.0;
+      nl[g] = (l % 2 == 0) ? -1.0 : 1.0;   // FaceGeom1D + FixNormal1D
+      continue;
+    }
+    double T[3][2];  // T[c][r] = d x_c / d s_r along the face
+    for (int c = 0; c < nd; ++c)
+      for (int r = 0; r < nd - 1; ++r) {
+        double s = 0.0;
+        for (int a = 0; a < npf; ++a) s += shapfgt[g + ngf * a + ngf * npf * (1 + r)] * x[perm[a + npf * l] + npe * c];
+        T[c][r] = s;
+      }
+    if (nd == 2) {
+      const double Jx = T[0][0], Jy = T[1][0];
+      const double j = sqrt(Jx * Jx + Jy * Jy);
+      jac[g] = j;
+      nl[g] = Jy / j;
+      nl[g + ngf] = -Jx / j;
+    } else {
+      const double a1 = T[0][0], a2 = T[1][0], a3 = T[2][0];
+      const double b1 = T[0][1], b2 = T[1][1], b3 = T[2][1];
+      const double n1 = a2 * b3 - a3 * b2, n2 = a3 * b1 - a1 * b3, n3 = a1 * b2 - a2 * b1;
+      const double j = sqrt(n1 * n1 + n2 * n2 + n3 * n3);
+      jac[g] = j;
+      nl[g] = n1 / j;
+      nl[g + ngf] = n2 / j;
+      nl[g + 2 * ngf] = n3 / j;
+    }
+  }
+}
+
+// ----------------------------------------------------------------------------------
+// q-equation element matrices before the mass inverse (qequation.cpp:66-170, 255-338):
+//   mass[a,b]      = sum_g (w0[a,g] t0[g,b]) jac[g]
+//   cw[a,b,d]      = sum_r sum_g (w_{1+r}[a,g] t0[g,b]) Xx[g, d + nd r]   (terms added per r)
+//   ew[perm[a,l], (b,l), d] = sum_g (wf0[a,g] tf0[g,b]) (nl_d[g] jac[g])
+// ----------------------------------------------------------------------------------
+__global__ void qmats_kernel(ExaDims P, const double* shapegt, const double* shapegw, const double* shapfgt,
+                             const double* shapfgw, const int* perm, const double* elemg, const double* faceg,
+                             double* mass, double* cw, double* ew) {
+  const int e = blockIdx.x;
+  const int npe = P.npe, nge = P.nge, nd = P.nd, npf = P.npf, ngf = P.ngf, ndf = P.ndf;
+  const double* eg = elemg + (long long)e * P.elemg_stride();
+  const double* Xx = eg + nge * P.ncx;
+  const double* jac = Xx + nge * nd * nd;
+  double* M = mass + (long long)e * npe * npe;
+  double* C = cw + (long long)e * npe * npe * nd;
+  double* E = ew + (long long)e * npe * ndf * nd;
+  for (int t = threadIdx.x; t < npe * npe; t += blockDim.x) {
+    const int a = t % npe, b = t / npe;
+    double s = 0.0;
+    for (int g = 0; g < nge; ++g) s += (shapegw[a + npe * g] * shapegt[g + nge * b]) * jac[g];
+    M[t] = s;
+    for (int d = 0; d < nd; ++d) {
+      double acc = 0.0;
+      for (int r = 0; r < nd; ++r) {
+        double sr = 0.0;
+        for (int g = 0; g < nge; ++g)
+          sr += (shapegw[a + npe * g + npe * nge * (1 + r)] * shapegt[g + nge * b]) * Xx[g + nge * (d + nd * r)];
+        acc = (r == 0) ? sr : acc + sr;
+      }
+      C[t + npe * npe * d] = acc;
+    }
+  }
+  for (int t = threadIdx.x; t < npe * ndf * nd; t += blockDim.x) E[t] = 0.0;
+  __syncthreads();
+  for (int t = threadIdx.x; t < npf * npf * P.nfe * nd; t += blockDim.x) {
+    const int a = t % npf, b = (t / npf) % npf, l = (t / (npf * npf)) % P.nfe, d = t / (npf * npf * P.nfe);
+    const double* fg = faceg + ((long long)e * P.nfe + l) * P.faceg_stride();
+    const double* nl = fg + ngf * P.ncx;
+    const double* fj = nl + ngf * nd;
+    double s = 0.0;
+    for (int g = 0; g < ngf; ++g) s += (shapfgw[a + npf * g] * shapfgt[g + ngf * b]) * ((1.0 * nl[g + ngf * d]) * fj[g]);
+    E[perm[a + npf * l] + npe * (b + npf * l) + npe * ndf * d] = s;
+  }
+}
+
+// ----------------------------------------------------------------------------------
+// trace-space gather / scatter and operators
+// ----------------------------------------------------------------------------------
+// w (face vector [ncu, npf, nf]) from element vectors we ([ncu, npf, nfe] per element):
+// the face's first element writes, the second adds (interior faces only).
+__global__ void scatter_kernel(ExaDims P, const int* f2e, const int* elemcon, const double* we, double* w) {
+  const int ncu = P.ncu, npf = P.npf, m = P.m;
+  const long long N = (long long)ncu * npf * P.nf;
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < N; idx += (long long)gridDim.x * blockDim.x) {
+    const int k = idx % ncu;
+    const long long q = idx / ncu;
+    const int a = q % npf;
+    const int f = q / npf;
+    const int e1 = f2e[4 * f], l1 = f2e[4 * f + 1], e2 = f2e[4 * f + 2], l2 = f2e[4 * f + 3];
+    double v = we[(long long)e1 * m + k + ncu * (a + npf * l1)];
+    if (f < P.nf0 && e2 >= 0) {
+      const int ii = elemcon[a + npf * l2 + P.ndf * e2] - npf * f;
+      v += we[(long long)e2 * m + k + ncu * (ii + npf * l2)];
+    }
+    w[idx] = v;
+  }
+}
+
+// we_e = A_e * gather(v), A_e = H (matvec) or the additive-Schwarz inverse blocks
+__global__ void elem_matvec_kernel(ExaDims P, const int* elemcon, const double* A, const double* v, double* we) {
+  extern __shared__ double ve[];
+  const int e = blockIdx.x, m = P.m, ncu = P.ncu;
+  for (int r = threadIdx.x; r < m; r += blockDim.x) ve[r] = v[r % ncu + ncu * (long long)elemcon[r / ncu + P.ndf * e]];
+  __syncthreads();
+  const double* Ae = A + (long long)e * m * m;
+  for (int r = threadIdx.x; r < m; r += blockDim.x) {
+    double s = 0.0;
+    for (int c = 0; c < m; ++c) s = fma(Ae[r + (long long)m * c], ve[c], s);
+    we[(long long)e * m + r] = s;
+  }
+}
+
+// block-Jacobi blocks per face from the condensed element matrices (kokkosimpl.h:1067-1111)
+__global__ void bj_build_kernel(ExaDims P, const int* f2e, const int* elemcon, const double* H, double* BE) {
+  const int ncu = P.ncu, npf = P.npf, ncf = ncu * npf, m = P.m;
+  const long long N = (long long)ncf * ncf * P.nf;
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < N; idx += (long long)gridDim.x * blockDim.x) {
+    const int r = idx % ncf;
+    const long long q = idx / ncf;
+    const int c = q % ncf;
+    const int f = q / ncf;
+    const int e1 = f2e[4 * f], l1 = f2e[4 * f + 1], e2 = f2e[4 * f + 2], l2 = f2e[4 * f + 3];
+    double v = H[(long long)e1 * m * m + (r + ncf * l1) + (long long)m * (c + ncf * l1)];
+    if (f < P.nf0 && e2 >= 0) {
+      const int dm = r % ncu + ncu * (elemcon[r / ncu + npf * l2 + P.ndf * e2] - npf * f);
+      const int dn = c % ncu + ncu * (elemcon[c / ncu + npf * l2 + P.ndf * e2] - npf * f);
+      v += H[(long long)e2 * m * m + (dm + ncf * l2) + (long long)m * (dn + ncf * l2)];
+    }
+    BE[idx] = v;
+  }
+}
+
+// elemental additive Schwarz: both elements of an interior face get the sum of their
+// face blocks (kokkosimpl.h:1113-1143); BE starts as a copy of H.
+__global__ void eas_build_kernel(ExaDims P, const int* f2e, const int* elemcon, const double* H, double* BE) {
+  const int ncu = P.ncu, npf = P.npf, ncf = ncu * npf, m = P.m;
+  const long long N = (long long)ncf * ncf * P.nf;
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < N; idx += (long long)gridDim.x * blockDim.x) {
+    const int r = idx % ncf;
+    const long long q = idx / ncf;
+    const int c = q % ncf;
+    const int f = q / ncf;
+    const int e1 = f2e[4 * f], l1 = f2e[4 * f + 1], e2 = f2e[4 * f + 2], l2 = f2e[4 * f + 3];
+    if (e2 < 0) continue;
+    const int dm = r % ncu + ncu * (elemcon[r / ncu + npf * l2 + P.ndf * e2] - npf * f);
+    const int dn = c % ncu + ncu * (elemcon[c / ncu + npf * l2 + P.ndf * e2] - npf * f);
+    const long long i1 = (long long)e1 * m * m + (r + ncf * l1) + (long long)m * (c + ncf * l1);
+    const long long i2 = (long long)e2 * m * m + (dm + ncf * l2) + (long long)m * (dn + ncf * l2);
+    const double tm = H[i1] + H[i2];
+    BE[i1] = tm;
+    BE[i2] = tm;
+  }
+}
+
+__global__ void bj_apply_kernel(ExaDims P, const double* BE, const double* x, double* y) {
+  const int ncf = P.ncu * P.npf;
+  const long long N = (long long)ncf * P.nf;
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < N; idx += (long long)gridDim.x * blockDim.x) {
+    const int r = idx % ncf;
+    const long long f = idx / ncf;
+    const double* A = BE + f * ncf * ncf;
+    const double* xf = x + f * ncf;
+    double s = 0.0;
+    for (int c = 0; c < ncf; ++c) s = fma(A[r + ncf * c], xf[c], s);
+    y[idx] = s;
+  }
+}
+
+// du_e = Ru_e + DinvF_e gather(x) (matvec.cpp:219-238); udg(:, 0:ncu, e) += alpha du_e
+__global__ void dudg_kernel(ExaDims P, const int* elemcon, const double* DinvF, const double* Ru, const double* x,
+                            double* du) {
+  extern __shared__ double ve[];
+  const int e = blockIdx.x, m = P.m, n = P.n, ncu = P.ncu;
+  for (int r = threadIdx.x; r < m; r += blockDim.x) ve[r] = x[r % ncu + ncu * (long long)elemcon[r / ncu + P.ndf * e]];
+  __syncthreads();
+  const double* A = DinvF + (long long)e * n * m;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    double s = 0.0;
+    for (int c = 0; c < m; ++c) s = fma(A[i + (long long)n * c], ve[c], s);
+    du[(long long)e * n + i] = Ru[(long long)e * n + i] + s;
+  }
+}
+
+__global__ void udg_update_kernel(ExaDims P, double* udg, const double* du, double alpha) {
+  const long long N = (long long)P.n * P.ne;
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < N; idx += (long long)gridDim.x * blockDim.x) {
+    const long long e = idx / P.n;
+    const int ik = idx % P.n;  // i + npe*k
+    udg[ik + (long long)P.npe * P.nc * e] += alpha * du[idx];
+  }
+}
+
+// q = MinvC u - MinvE uhat per dimension (qequation.cpp:372-470)
+__global__ void getq_kernel(ExaDims P, const int* elemcon, const double* MC, const double* ME, const double* uh,
+                            double* udg) {
+  extern __shared__ double sm[];
+  const int e = blockIdx.x, npe = P.npe, ncu = P.ncu, ndf = P.ndf, nd = P.nd, nc = P.nc;
+  double* u = sm;               // [npe, ncu]
+  double* uhe = sm + npe * ncu; // [ndf, ncu]
+  double* U = udg + (long long)e * npe * nc;
+  for (int t = threadIdx.x; t < npe * ncu; t += blockDim.x) u[t] = U[t];
+  for (int t = threadIdx.x; t < ndf * ncu; t += blockDim.x) {
+    const int jf = t % ndf, k = t / ndf;
+    uhe[t] = uh[k + ncu * (long long)elemcon[jf + ndf * e]];
+  }
+  __syncthreads();
+  const double* C = MC + (long long)e * npe * npe * nd;
+  const double* E = ME + (long long)e * npe * ndf * nd;
+  for (int t = threadIdx.x; t < npe * ncu * nd; t += blockDim.x) {
+    const int i = t % npe, k = (t / npe) % ncu, d = t / (npe * ncu);
+    double s = 0.0;
+    for (int j = 0; j < npe; ++j) s = fma(C[i + npe * j + npe * npe * d], u[j + npe * k], s);
+    double r = 0.0;
+    for (int j = 0; j < ndf; ++j) r = fma(E[i + npe * j + npe * ndf * d], uhe[j + ndf * k], r);
+    U[i + npe * (ncu + k + ncu * d)] = s - r;
+  }
+}
+
+// uh from the first element of each face (kokkosimpl.h:901-915)
+__global__ void face_nodes_kernel(ExaDims P, const int* f2e, const int* perm, const double* udg, double* uh) {
+  const long long N = (long long)P.ncu * P.npf * P.nf;
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < N; idx += (long long)gridDim.x * blockDim.x) {
+    const int k = idx % P.ncu;
+    const long long q = idx / P.ncu;
+    const int a = q % P.npf;
+    const int f = q / P.npf;
+    const int e1 = f2e[4 * f], l1 = f2e[4 * f + 1];
+    uh[idx] = udg[perm[a + P.npf * l1] + P.npe * k + (long long)P.npe * P.nc * e1];
+  }
+}
+
+int grid_for(long long n) {
+  long long b = (n + 255) / 256;
+  return (int)(b < 4096 ? (b > 0 ? b : 1) : 4096);
+}
+
+}  // namespace
+
+int exa_k_geometry(const ExaDims& P, const double* shapegt, const double* shapfgt, const int* perm,
+                   const double* xdg, double* elemg, double* faceg, cudaStream_t st) {
+  elem_geom_kernel<<<P.ne, 128, 0, st>>>(P, shapegt, xdg, elemg);
+  EXA_LAUNCH_CHECK();
+  face_geom_kernel<<<P.ne, 128, 0, st>>>(P, shapfgt, perm, xdg, faceg);
+  EXA_LAUNCH_CHECK();
+  return EXA_OK;
+}
+
+int exa_k_qmats(const ExaDims& P, const double* shapegt, const double* shapegw, const double* shapfgt,
+                const double* shapfgw, const int* perm, const double* elemg, const double* faceg, double* mass,
+                double* cw, double* ew, cudaStream_t st) {
+  qmats_kernel<<<P.ne, 256, 0, st>>>(P, shapegt, shapegw, shapfgt, shapfgw, perm, elemg, faceg, mass, cw, ew);
+  EXA_LAUNCH_CHECK();
+  return EXA_OK;
+}
+
+int exa_k_scatter(const ExaDims& P, const int* f2e, const int* elemcon, const double* we, double* w, cudaStream_t st) {
+  scatter_kernel<<<grid_for((long long)P.ncu * P.npf * P.nf), 256, 0, st>>>(P, f2e, elemcon, we, w);
+  EXA_LAUNCH_CHECK();
+  return EXA_OK;
+}
+
+int exa_k_elem_matvec(const ExaDims& P, const int* elemcon, const double* A, const double* v, double* we,
+                      cudaStream_t st) {
+  int th = P.m <= 64 ? 64 : (P.m <= 128 ? 128 : 256);
+  elem_matvec_kernel<<<P.ne, th, P.m * sizeof(double), st>>>(P, elemcon, A, v, we);
+  EXA_LAUNCH_CHECK();
+  return EXA_OK;
+}
+
+int exa_k_bj_build(const ExaDims& P, const int* f2e, const int* elemcon, const double* H, double* BE, cudaStream_t st) {
+  const long long ncf = (long long)P.ncu * P.npf;
+  bj_build_kernel<<<grid_for(ncf * ncf * P.nf), 256, 0, st>>>(P, f2e, elemcon, H, BE);
+  EXA_LAUNCH_CHECK();
+  return EXA_OK;
+}
+
+int exa_k_eas_build(const ExaDims& P, const int* f2e, const int* elemcon, const double* H, double* BE, cudaStream_t st) {
+  EXA_CUDA(cudaMemcpyAsync(BE, H, sizeof(double) * (size_t)P.m * P.m * P.ne, cudaMemcpyDeviceToDevice, st));
+  const long long ncf = (long long)P.ncu * P.npf;
+  eas_build_kernel<<<grid_for(ncf * ncf * P.nf), 256, 0, st>>>(P, f2e, elemcon, H, BE);
+  EXA_LAUNCH_CHECK();
+  return EXA_OK;
+}
+
+int exa_k_bj_apply(const ExaDims& P, const double* BE, const double* x, double* y, cudaStream_t st) {
+  bj_apply_kernel<<<grid_for((long long)P.ncu * P.npf * P.nf), 256, 0, st>>>(P, BE, x, y);
+  EXA_LAUNCH_CHECK();
+  return EXA_OK;
+}
+
+int exa_k_dudg(const ExaDims& P, const int* elemcon, const double* DinvF, const double* Ru, const double* x,
+               double* du, cudaStream_t st) {
+  dudg_kernel<<<P.ne, 128, P.m * sizeof(double), st>>>(P, elemcon, DinvF, Ru, x, du);
+  EXA_LAUNCH_CHECK();
+  return EXA_OK;
+}
+
+int exa_k_udg_update(const ExaDims& P, double* udg, const double* du, double alpha, cudaStream_t st) {
+  udg_update_kernel<<<grid_for((long long)P.n * P.ne), 256, 0, st>>>(P, udg, du, alpha);
+  EXA_LAUNCH_CHECK();
+  return EXA_OK;
+}
+
+int exa_k_getq(const ExaDims& P, const int* elemcon, const double* MC, const double* ME, const double* uh,
+               double* udg, cudaStream_t st) {
+  size_t smem = sizeof(double) * ((size_t)P.npe * P.ncu + (size_t)P.ndf * P.ncu);
+  getq_kernel<<<P.ne, 128, smem, st>>>(P, elemcon, MC, ME, uh, udg);
+  EXA_LAUNCH_CHECK();
+  return EXA_OK;
+}
+
+int exa_k_face_nodes(const ExaDims& P, const int* f2e, const int* perm, const double* udg, double* uh, cudaStream_t st) {
+  face_nodes_kernel<<<grid_for((long long)P.ncu * P.npf * P.nf), 256, 0, st>>>(P, f2e, perm, udg, uh);
+  EXA_LAUNCH_CHECK();
+  return EXA_OK;
+}

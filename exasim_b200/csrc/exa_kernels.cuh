@@ -1,0 +1,30 @@
+// Sizes shared by the HDG kernels and their host-side launchers.
+#pragma once
+#include "exa_common.cuh"
+
+struct ExaDims {
+  int nd, ncu, nc, ncq, ncx, nco, ncw;   // dimension and field components
+  int npe, npf, nge, ngf, nfe, ndf;       // nodes / quadrature points per element and face
+  int n, m;                               // n = npe*ncu (element block), m = ncu*npf*nfe (trace block)
+  int ne, nf, nf0;                        // elements, faces, interior faces
+  __host__ __device__ int elemg_stride() const { return nge * (ncx + nd * nd + 1); }
+  __host__ __device__ int faceg_stride() const { return ngf * (ncx + nd + 1); }
+};
+
+int exa_k_geometry(const ExaDims& P, const double* shapegt, const double* shapfgt, const int* perm,
+                   const double* xdg, double* elemg, double* faceg, cudaStream_t st);
+int exa_k_qmats(const ExaDims& P, const double* shapegt, const double* shapegw, const double* shapfgt,
+                const double* shapfgw, const int* perm, const double* elemg, const double* faceg, double* mass,
+                double* cw, double* ew, cudaStream_t st);
+int exa_k_scatter(const ExaDims& P, const int* f2e, const int* elemcon, const double* we, double* w, cudaStream_t st);
+int exa_k_elem_matvec(const ExaDims& P, const int* elemcon, const double* A, const double* v, double* we,
+                      cudaStream_t st);
+int exa_k_bj_build(const ExaDims& P, const int* f2e, const int* elemcon, const double* H, double* BE, cudaStream_t st);
+int exa_k_eas_build(const ExaDims& P, const int* f2e, const int* elemcon, const double* H, double* BE, cudaStream_t st);
+int exa_k_bj_apply(const ExaDims& P, const double* BE, const double* x, double* y, cudaStream_t st);
+int exa_k_dudg(const ExaDims& P, const int* elemcon, const double* DinvF, const double* Ru, const double* x,
+               double* du, cudaStream_t st);
+int exa_k_udg_update(const ExaDims& P, double* udg, const double* du, double alpha, cudaStream_t st);
+int exa_k_getq(const ExaDims& P, const int* elemcon, const double* MC, const double* ME, const double* uh,
+               double* udg, cudaStream_t st);
+int exa_k_face_nodes(const ExaDims& P, const int* f2e, const int* perm, const double* udg, double* uh, cudaStream_t st);

@@ -1,0 +1,167 @@
+// Model-specific translation unit: instantiates the assembly kernels for one
+// generated model (header produced by exasim_b200/modelc.py, selected at build time
+// with -DEXA_MODEL_HEADER="..." -DEXA_MODEL_NS=exa_model_<name>) and runs the
+// element-block loop of hdgAssembleLinearSystem / hdgAssembleResidual
+// (backend/Discretization/uequation.cpp:778-787, 1080-1088).
+#include <vector>
+
+#include "exa_assembly.cuh"
+#include "exa_solver.cuh"
+#include EXA_MODEL_HEADER
+
+EXA_BIND_MODEL(EXA_MODEL_NS)
+
+namespace {
+
+AsmArgs make_args(const ExaCtx& c, int e0) {
+  AsmArgs A{};
+  A.P = c.P;
+  A.shapegt = c.shapegt; A.shapegw = c.shapegw; A.shapfgt = c.shapfgt; A.shapfgw = c.shapfgw;
+  A.perm = c.perm; A.elemcon = c.elemcon; A.bf = c.bf;
+  A.elemg = c.elemg; A.faceg = c.faceg;
+  A.uinf = c.uinf; A.param = c.param; A.tau = c.tau;
+  A.udg = c.udg; A.uh = c.uh; A.sdg = c.sdg;
+  A.time = c.time; A.dtfactor = c.dtfactor;
+  A.tdep = c.tdep; A.tdfunc = c.tdfunc; A.sourcefunc = c.sourcefunc; A.modelnumber = c.modelnumber;
+  A.e0 = e0;
+  return A;
+}
+
+int smem_attr(const void* fn, size_t bytes) {
+  if (bytes > 48 * 1024) EXA_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+  if (bytes > 227 * 1024) {
+    exa_set_error("element tile needs %zu bytes of shared memory", bytes);
+    return EXA_ERR_UNSUPPORTED;
+  }
+  return EXA_OK;
+}
+
+// Schur condensation of one chunk (uequation.cpp:559-775): q-elimination, D^-1, DinvF,
+// Ru <- D^-1 Ru, H += K DinvF, Rh -= K Ru.
+int schur_chunk(ExaCtx& c, int e0, int nb) {
+  const ExaDims& P = c.P;
+  const int n = P.n, m = P.m, npe = P.npe, nd = P.nd, ncu = P.ncu, ndf = P.ndf;
+  const long long nqn = (long long)npe * nd * ncu;
+  double* Hc = c.H + (long long)e0 * m * m;
+  if (P.ncq > 0) {
+    const double* MC = c.MC + (long long)e0 * npe * npe * nd;
+    const double* ME = c.ME + (long long)e0 * npe * ndf * nd;
+    for (int d = 0; d < nd; ++d) {
+      GemmBatch g{};
+      g.batch = nb; g.batch2 = ncu;
+      g.K = npe; g.beta = 1.0;
+      // D(:, j + npe*nq) += B(:, k + npe*d + npe*nd*nq) MinvC_d
+      g.M = n; g.N = npe; g.alpha = 1.0;
+      g.A = c.wB + (long long)n * npe * d; g.lda = n; g.sA = (long long)n * nqn; g.sA2 = (long long)n * npe * nd;
+      g.B = MC + (long long)npe * npe * d; g.ldb = npe; g.sB = (long long)npe * npe * nd; g.sB2 = 0;
+      g.C = c.wD; g.ldc = n; g.sC = (long long)n * n; g.sC2 = (long long)n * npe;
+      EXA_TRY(exa_gemm(g, c.st));
+      // F(:, b + ncu*jf) -= B(:, k + npe*d + npe*nd*b) MinvE_d
+      g.N = ndf; g.alpha = -1.0;
+      g.B = ME + (long long)npe * ndf * d; g.ldb = npe; g.sB = (long long)npe * ndf * nd;
+      g.C = c.wF; g.ldc = (long long)n * ncu; g.sC = (long long)n * m; g.sC2 = n;
+      EXA_TRY(exa_gemm(g, c.st));
+      // K(:, j + npe*nq) += G(:, k + npe*d + npe*nd*nq) MinvC_d
+      g.M = m; g.N = npe; g.alpha = 1.0;
+      g.A = c.wG + (long long)m * npe * d; g.lda = m; g.sA = (long long)m * nqn; g.sA2 = (long long)m * npe * nd;
+      g.B = MC + (long long)npe * npe * d; g.ldb = npe; g.sB = (long long)npe * npe * nd;
+      g.C = c.wK; g.ldc = m; g.sC = (long long)m * n; g.sC2 = (long long)m * npe;
+      EXA_TRY(exa_gemm(g, c.st));
+      // H(:, b + ncu*jf) -= G(:, k + npe*d + npe*nd*b) MinvE_d
+      g.N = ndf; g.alpha = -1.0;
+      g.B = ME + (long long)npe * ndf * d; g.ldb = npe; g.sB = (long long)npe * ndf * nd;
+      g.C = Hc; g.ldc = (long long)m * ncu; g.sC = (long long)m * m; g.sC2 = m;
+      EXA_TRY(exa_gemm(g, c.st));
+    }
+  }
+  EXA_TRY(exa_inverse(c.wD, n, (long long)n * n, nb, c.d_flag, c.st));
+  GemmBatch g{};
+  g.batch = nb; g.batch2 = 1;
+  // DinvF = -Dinv F
+  g.M = n; g.N = m; g.K = n; g.alpha = -1.0; g.beta = 0.0;
+  g.A = c.wD; g.lda = n; g.sA = (long long)n * n;
+  g.B = c.wF; g.ldb = n; g.sB = (long long)n * m;
+  g.C = c.F + (long long)e0 * n * m; g.ldc = n; g.sC = (long long)n * m;
+  EXA_TRY(exa_gemm(g, c.st));
+  // Ru = Dinv Ru
+  double* Ruc = c.Ru + (long long)e0 * n;
+  EXA_CUDA(cudaMemcpyAsync(c.wRu, Ruc, sizeof(double) * (size_t)n * nb, cudaMemcpyDeviceToDevice, c.st));
+  g.N = 1; g.alpha = 1.0;
+  g.B = c.wRu; g.ldb = n; g.sB = n;
+  g.C = Ruc; g.ldc = n; g.sC = n;
+  EXA_TRY(exa_gemm(g, c.st));
+  // H += K DinvF
+  g.M = m; g.N = m; g.K = n; g.alpha = 1.0; g.beta = 1.0;
+  g.A = c.wK; g.lda = m; g.sA = (long long)m * n;
+  g.B = c.F + (long long)e0 * n * m; g.ldb = n; g.sB = (long long)n * m;
+  g.C = Hc; g.ldc = m; g.sC = (long long)m * m;
+  EXA_TRY(exa_gemm(g, c.st));
+  // Rh -= K Ru
+  g.N = 1; g.alpha = -1.0;
+  g.B = Ruc; g.ldb = n; g.sB = n;
+  g.C = c.Rh + (long long)e0 * m; g.ldc = m; g.sC = m;
+  EXA_TRY(exa_gemm(g, c.st));
+  return EXA_OK;
+}
+
+}  // namespace
+
+int exa_model_assemble(ExaCtx& c, bool jacobian) {
+  const ExaDims& P = c.P;
+  const int n = P.n, m = P.m;
+  const long long nqn = (long long)P.npe * P.nd * P.ncu;
+  const size_t vs = jacobian ? vol_points_smem<true>(P) : vol_points_smem<false>(P);
+  const size_t fs = face_smem(P, jacobian);
+  if (jacobian) {
+    EXA_TRY(smem_attr((const void*)vol_points_kernel<ExaModel, true>, vs));
+    EXA_TRY(smem_attr((const void*)face_kernel<ExaModel, true>, fs));
+  } else {
+    EXA_TRY(smem_attr((const void*)vol_points_kernel<ExaModel, false>, vs));
+    EXA_TRY(smem_attr((const void*)face_kernel<ExaModel, false>, fs));
+  }
+  const int tpb_v = P.nge <= 64 ? 64 : (P.nge <= 128 ? 128 : 256);
+  const int tpb_f = 128;
+  for (int e0 = 0; e0 < P.ne; e0 += c.neb) {
+    const int nb = std::min(c.neb, P.ne - e0);
+    AsmArgs A = make_args(c, e0);
+    double* Ruc = c.Ru + (long long)e0 * n;
+    double* Rhc = c.Rh + (long long)e0 * m;
+    if (jacobian) {
+      vol_points_kernel<ExaModel, true><<<nb, tpb_v, vs, c.st>>>(A, Ruc, c.wRg);
+      EXA_LAUNCH_CHECK();
+      const int tiles = exa_ceil_div(P.npe, 64);
+      dim3 grid(tiles * tiles, nb, P.ncu * P.nc);
+      vol_mat_kernel<<<grid, 256, 0, c.st>>>(P, c.shapegw, c.shapegt, c.wRg, c.wD, c.wB);
+      EXA_LAUNCH_CHECK();
+      double* Hc = c.H + (long long)e0 * m * m;
+      EXA_CUDA(cudaMemsetAsync(c.wF, 0, sizeof(double) * (size_t)nb * n * m, c.st));
+      EXA_CUDA(cudaMemsetAsync(c.wK, 0, sizeof(double) * (size_t)nb * m * n, c.st));
+      if (nqn > 0 && P.ncq > 0) EXA_CUDA(cudaMemsetAsync(c.wG, 0, sizeof(double) * (size_t)nb * m * nqn, c.st));
+      EXA_CUDA(cudaMemsetAsync(Hc, 0, sizeof(double) * (size_t)nb * m * m, c.st));
+      face_kernel<ExaModel, true><<<nb, tpb_f, fs, c.st>>>(A, Ruc, Rhc, c.wD, c.wB, c.wF, c.wK, c.wG, Hc);
+      EXA_LAUNCH_CHECK();
+      EXA_TRY(schur_chunk(c, e0, nb));
+    } else {
+      vol_points_kernel<ExaModel, false><<<nb, tpb_v, vs, c.st>>>(A, Ruc, nullptr);
+      EXA_LAUNCH_CHECK();
+      face_kernel<ExaModel, false><<<nb, tpb_f, fs, c.st>>>(A, Ruc, Rhc, nullptr, nullptr, nullptr, nullptr, nullptr,
+                                                           nullptr);
+      EXA_LAUNCH_CHECK();
+    }
+  }
+  return EXA_OK;
+}
+
+// initial u from the model's cpuInitu at the element nodes (readsolstruct, readbinaryfiles.cpp:546-556)
+int exa_model_init_udg(ExaCtx& c, double* host_udg) {
+  const ExaDims& P = c.P;
+  const int np = P.npe * P.ne;
+  std::vector<double> f((size_t)np * P.nc, 0.0);
+  EXA_MODEL_NS::cpuInitu(f.data(), c.h_xdg.data(), c.h_uinf.data(), c.h_param.data(), c.modelnumber, np, P.ncx,
+                         P.nc, P.npe, P.ne);
+  for (int e = 0; e < P.ne; ++e)
+    for (int k = 0; k < P.ncu; ++k)
+      for (int i = 0; i < P.npe; ++i)
+        host_udg[i + P.npe * k + P.npe * P.nc * e] = f[i + P.npe * k + (size_t)P.npe * P.nc * e];
+  return EXA_OK;
+}

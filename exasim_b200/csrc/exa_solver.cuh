@@ -1,0 +1,73 @@
+// Host-side solver context: inputs parsed from Exasim's app/master/mesh/sol blobs,
+// device-resident mesh, master, solution and condensed system, and the workspace of
+// the assembly and Krylov loops.  The drivers mirror Exasim's call structure:
+//   hdgAssembleLinearSystem / hdgAssembleResidual (discretization.cpp:483-592),
+//   GMRES (gmres.cpp:361-597), NewtonSolver (solution.cpp:125-243), DIRK stepping
+//   (exasim.hpp:413-482).
+#pragma once
+#include <string>
+#include <vector>
+
+#include "exa_kernels.cuh"
+#include "exa_conn.h"
+
+struct ExaCtx {
+  ExaDims P{};
+  int device = 0;
+  cudaStream_t st = nullptr;
+  // app flags (app.bin flag/problem/solversparam, setstructs.cpp:45-322)
+  int tdep = 0, wave = 0, preconditioner = 0, ortho = 0, tdfunc = 1, sourcefunc = 1, modelnumber = 0;
+  int newton_maxit = 20, gmres_maxit = 200, restart = 25, torder = 1, nstage = 1, ppdegree = 0, RBdim = 0;
+  double newton_tol = 1e-6, gmres_tol = 1e-3, time0 = 0.0;
+  std::vector<double> dt;
+  int elemtype = 0, porder = 0;
+  // host copies needed by the host-side initial condition
+  std::vector<double> h_xdg, h_uinf, h_param;
+  // device data
+  double *shapegt = nullptr, *shapegw = nullptr, *shapfgt = nullptr, *shapfgw = nullptr;
+  int *perm = nullptr, *elemcon = nullptr, *f2e = nullptr, *bf = nullptr;
+  double *xdg = nullptr, *elemg = nullptr, *faceg = nullptr, *uinf = nullptr, *param = nullptr, *tau = nullptr;
+  double *udg = nullptr, *uh = nullptr, *sdg = nullptr;
+  double *MC = nullptr, *ME = nullptr;
+  double *H = nullptr, *F = nullptr, *Ru = nullptr, *Rh = nullptr, *b = nullptr, *Pc = nullptr;
+  // assembly workspace for a chunk of `neb` elements
+  int neb = 0;
+  double *wD = nullptr, *wB = nullptr, *wF = nullptr, *wK = nullptr, *wG = nullptr, *wRg = nullptr, *wRu = nullptr;
+  // Krylov / Newton workspace
+  double *V = nullptr, *x = nullptr, *r = nullptr, *w = nullptr, *we = nullptr, *du = nullptr;
+  double *part_a = nullptr, *part_b = nullptr, *part_m = nullptr, *hess = nullptr, *gs = nullptr, *gcs = nullptr,
+         *gsn = nullptr, *scal = nullptr, *udgprev = nullptr, *utmp = nullptr;
+  int* d_flag = nullptr;
+  double* pinned = nullptr;  // small host staging buffer
+  // state
+  double time = 0.0, dtfactor = 0.0;
+  int nf_total = 0;
+  std::vector<void*> allocs;
+  // statistics of the last solve
+  int last_gmres_iters = 0, last_newton_iters = 0, total_gmres_iters = 0;
+  double last_gmres_relerr = 0.0;
+  long long kernel_launches = 0;
+
+  long long ndofuhat() const { return (long long)P.ncu * P.npf * P.nf; }
+};
+
+// setup and teardown (exa_api.cu)
+int exa_ctx_init(ExaCtx& c, const double* app, long long napp, const double* master, long long nmaster,
+                 const double* mesh, long long nmesh, const double* sol, long long nsol, int device);
+void exa_ctx_free(ExaCtx& c);
+
+// model-specific steps (instantiated per model)
+int exa_model_assemble(ExaCtx& c, bool jacobian);
+int exa_model_init_udg(ExaCtx& c, double* host_udg);
+
+// model-independent drivers (exa_drivers.cu)
+int exa_drv_assemble(ExaCtx& c);
+int exa_drv_residual(ExaCtx& c, double* norm);
+int exa_drv_matvec(ExaCtx& c, const double* v, double* w);
+int exa_drv_precond(ExaCtx& c, const double* v, double* w);
+int exa_drv_build_precond(ExaCtx& c);
+int exa_drv_gmres(ExaCtx& c, int* iters, double* relerr);
+int exa_drv_getq(ExaCtx& c);
+int exa_drv_newton(ExaCtx& c, int* iters, double* norm);
+int exa_drv_dirk(ExaCtx& c, int nsteps, int* newton_iters_out, int max_out);
+int exa_drv_norm(ExaCtx& c, const double* x, long long n, double* out);

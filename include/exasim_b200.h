@@ -1,0 +1,91 @@
+/* C ABI of the B200 HDG solver (libexasim_b200_<model>.so).
+ *
+ * One shared library per PDE model, as Exasim builds one libpdemodel<backend>.so per
+ * model (backend/Model/libpdemodel.hpp).  A context owns all device memory: mesh,
+ * master element, solution (udg, uhat) and the condensed HDG system.  Pointers named
+ * *_dev are CUDA device pointers; every other pointer is host memory owned by the caller.
+ * Every function returns 0 on success or an ExaStatus code (1 bad argument,
+ * 2 unsupported input, 3 CUDA error, 4 singular block, 5 mesh error, 6 not converged,
+ * 7 NaN residual, 8 out of device memory); exa_last_error() describes the last failure.
+ * The reference prints and exits instead (backend/Common/common.h:527-555).
+ * One host thread per context; calls are synchronous unless noted.
+ *
+ * Array layouts are Exasim's (column-major):  udg [npe, nc, ne], uhat [ncu, npf, nf].
+ */
+#ifndef EXASIM_B200_H
+#define EXASIM_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct exa_ctx exa_ctx;
+
+/* Message of the last failed call (thread-unsafe static buffer). */
+const char* exa_last_error(void);
+
+/* Build a context from the four input files Exasim's preprocessor writes
+ * (datain/app.bin, master.bin, mesh.bin, sol.bin), passed as their float64 words.
+ * Replaces CDiscretization's constructor: readInput (backend/Discretization/readbinaryfiles.cpp:625),
+ * buildConn for raw element lists (connectivity.cpp:1212), compGeometry (geometry.cpp:87-222),
+ * qEquation (qequation.cpp:365) and the HDG allocations (discretization.cpp:245-428). */
+int exa_create(const double* app, long long napp, const double* master, long long nmaster,
+               const double* mesh, long long nmesh, const double* sol, long long nsol, int device,
+               exa_ctx** out);
+void exa_destroy(exa_ctx* ctx);
+
+/* out[16] = {ne, nf, nf0, npe, npf, nfe, nc, ncu, nd, n=npe*ncu, m=ncu*npf*nfe,
+ *            ndofuhat, nge, ngf, element chunk, preconditioner} */
+int exa_sizes(exa_ctx* ctx, long long* out);
+
+/* Host copies of named device arrays: "udg", "uh", "H", "F" (D^-1 F after assembly),
+ * "Ru", "Rh", "b", "x", "sdg", "P" (preconditioner), "MinvC", "MinvE", "elemg", "faceg".
+ * n must equal the array length. */
+int exa_get_field(exa_ctx* ctx, const char* name, double* host, long long n);
+int exa_set_field(exa_ctx* ctx, const char* name, const double* host, long long n);
+/* Device pointer and length of a named array (zero-copy access, e.g. from torch). */
+int exa_field_ptr(exa_ctx* ctx, const char* name, double** dev, long long* n);
+/* f2e [4, nf] and elemcon [npf*nfe, ne] (0-based), either may be NULL. */
+int exa_get_connectivity(exa_ctx* ctx, int* f2e, int* elemcon);
+
+/* Current time and DIRK factor d_jj/dt used by time-dependent assembly (UpdateSourceDIRK,
+ * backend/Solution/updatesource.cpp:32-50). */
+int exa_set_time(exa_ctx* ctx, double time, double dtfactor);
+
+/* hdgAssembleLinearSystem (backend/Discretization/discretization.cpp:483-573): element
+ * residuals and Jacobians (uequation.cpp:45-557), static condensation (:559-775),
+ * RHS b (matvec.cpp:103) and the preconditioner (matvec.cpp:119-217). */
+int exa_assemble(exa_ctx* ctx);
+/* hdgAssembleResidual (discretization.cpp:576-592); *norm = |b| + |Ru| (solution.cpp:148-157). */
+int exa_residual(exa_ctx* ctx, double* norm);
+/* w = A v, hdgMatVec (matvec.cpp:240-389); device vectors of length ndofuhat. */
+int exa_matvec(exa_ctx* ctx, const double* v_dev, double* w_dev);
+/* w = P v, ApplyPreconditioner (Preconditioning/preconditioner.cpp:273-295); v != w. */
+int exa_precond(exa_ctx* ctx, const double* v_dev, double* w_dev);
+/* Solve A x = b by restarted GMRES (Solver/gmres.cpp:361-597); x is field "x". */
+int exa_gmres(exa_ctx* ctx, int* iters, double* relerr);
+/* q from u and uhat, hdgGetQ (qequation.cpp:372-484). */
+int exa_getq(exa_ctx* ctx);
+/* Damped Newton on the HDG residual, NewtonSolver (Solution/solution.cpp:125-243). */
+int exa_newton(exa_ctx* ctx, int* iters, double* norm);
+/* nsteps DIRK steps around Newton (Main/exasim.hpp:413-482); newton_iters[0..max_out) receives
+ * the Newton count of each stage. */
+int exa_dirk(exa_ctx* ctx, int nsteps, int* newton_iters, int max_out);
+/* One Newton solve from host buffers: copies udg/uhat in (NULL keeps the current state),
+ * solves, copies them out (NULL skips).  The end-to-end form of exa_newton. */
+int exa_solve(exa_ctx* ctx, const double* udg_in, const double* uh_in, double* udg_out,
+              double* uh_out, int* iters, double* norm);
+/* Face connectivity of a raw element list on the host, buildConn / connectivity()
+ * (backend/Discretization/connectivity.cpp:426-497, 1212-1385): t [nve, ne] 0-based vertices,
+ * bf [nfe, ne] boundary codes, perm [npf, nfe], xpf [npf, dim-1]; f2e (4*nfe*ne ints) and
+ * elemcon (npf*nfe*ne ints) receive the result.  Returns nf (>= 0) or a negated status. */
+int exa_connectivity_host(const int* t, const int* bf, const int* perm, const double* xpf, int dim,
+                          int elemtype, int ne, int npe, int npf, int* f2e, int* elemcon, int* nf0);
+/* out[4] = {last GMRES iterations, last Newton iterations, GMRES iterations of the last solve, 0} */
+int exa_stats(exa_ctx* ctx, long long* out);
+int exa_synchronize(exa_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

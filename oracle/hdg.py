@@ -230,10 +230,10 @@ class HDGOracle:
         elif nd == 2:
             J11, J12, J21, J22 = J[:, 0, 0], J[:, 1, 0], J[:, 0, 1], J[:, 1, 1]
             jac = J11 * J22 - J12 * J21
-            Xx[:, 0] = J22
-            Xx[:, 2] = -J21
-            Xx[:, 1] = -J12
-            Xx[:, 3] = J11
+            Xx[:, 0] = J22        # Xx11
+            Xx[:, 1] = -J21       # Xx21 = jac * dxi/dy
+            Xx[:, 2] = -J12       # Xx12 = jac * deta/dx
+            Xx[:, 3] = J11        # Xx22
         else:
             J11, J12, J13 = J[:, 0, 0], J[:, 1, 0], J[:, 2, 0]
             J21, J22, J23 = J[:, 0, 1], J[:, 1, 1], J[:, 2, 1]
