@@ -2,8 +2,11 @@
 reference's own golden solution).  Every call goes through the C ABI.
 
 Tolerances (FP64 plain form):
-  * assembled element blocks H, Rh, D^-1 F, Ru, RHS b, preconditioner blocks, matvec,
-    q matrices: max |gpu - oracle| <= 1e-12 * max |oracle| (relative to the array's scale)
+  * assembled blocks H, Rh, RHS b, preconditioner blocks, matvec: max |gpu - oracle| <=
+    1e-12 * max |oracle| (relative to the array's scale)
+  * arrays that pass through the explicit element inverse alone (D^-1 F, D^-1 Ru) and the
+    q matrices (Minv C, Minv E): 1e-11, since Gauss-Jordan and LAPACK getrf+getri round
+    differently by about cond(D) * eps (cond(D) ~ 1e3 on these meshes)
   * solutions after GMRES to tolerance tol: |uh - uh_oracle| / |uh_oracle| <= 1e3 * tol
 """
 import os
@@ -18,6 +21,7 @@ from tests.cases import poisson3d_datain
 
 pytestmark = pytest.mark.gpu
 ASM_TOL = 1e-12
+INV_TOL = 1e-11
 
 
 @pytest.fixture(scope="module", autouse=True)
@@ -45,7 +49,8 @@ def check_assembly(s: HDGSolver, o: HDGOracle, tol=ASM_TOL):
     o.build_precond()
     errs["P"] = rel(s.get("P"), o.P)
     for k, v in errs.items():
-        assert v < tol, (k, v, errs)
+        assert v < (INV_TOL if k in ("F", "Ru") else tol), (k, v, errs)
+    print("assembly parity (max rel err):", {k: float(f"{v:.2e}") for k, v in errs.items()})
     return errs
 
 
@@ -76,8 +81,8 @@ def test_geometry_and_q_matrices(poisson2d_case):
     assert rel(xg, o.xg) < ASM_TOL and rel(Xx, o.Xx) < ASM_TOL and rel(jac, o.jac) < ASM_TOL
     MC = s.get("MinvC").reshape(o.npe, o.npe, nd, ne, order="F")
     ME = s.get("MinvE").reshape(o.npe, o.npf * o.nfe, nd, ne, order="F")
-    assert rel(MC, np.transpose(o.MinvC, (0, 1, 3, 2))) < 1e-11
-    assert rel(ME, np.transpose(o.MinvE, (0, 1, 3, 2))) < 1e-11
+    assert rel(MC, np.transpose(o.MinvC, (0, 1, 3, 2))) < INV_TOL
+    assert rel(ME, np.transpose(o.MinvE, (0, 1, 3, 2))) < INV_TOL
     s.close()
 
 
