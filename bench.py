@@ -1,0 +1,335 @@
+"""Benchmark: HDG Newton solves/s on the 3D convection-diffusion workload.
+
+Workload (one GPU): HDG p=4 on a 16^3 hexahedral mesh of the unit cube (4096 elements,
+125 nodes each, 326,400 trace unknowns), velocity (1, 0.5, 0.25), kappa = 0.01,
+Gaussian source at the centre (sigma 0.1), u = 0 on the boundary, DIRK(3,3) with
+dt = 0.01.  One step = one DIRK-stage Newton solve: source update, assembly with
+static condensation, block-Jacobi GMRES(50) to a relative residual of 1e-8, Newton
+update and residual check (plain FP64 form).  Inputs are seeded synthetic data with
+the configuration's shapes.  With --gpus N (torchrun) every rank solves its own
+replica: the path has no data-path collective, so scaling is weak.
+
+Prints one JSON line.  `--impl reference` times the CPU restatement of the reference
+path (numpy + LAPACK on the host cores) on a bounded sample of the workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = "HDG Newton solves/s (DIRK-stage solve, ||r||/||r0|| <= 1e-8), plain FP64"
+CFG_N, CFG_P = 16, 4
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=CFG_N, help="elements per cube edge")
+    ap.add_argument("--e2e-steps", type=int, default=None)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def config(n):
+    return {"workload": f"3D convection-diffusion HDG p={CFG_P}, {n}^3 hexahedra ({n ** 3} elements), "
+                        "DIRK(3,3) dt=0.01, block-Jacobi GMRES(50) to 1e-8",
+            "elements": n ** 3, "porder": CFG_P, "ndofuhat": 25 * (3 * n * n * (n + 1)),
+            "step": "one DIRK-stage Newton solve",
+            "l2": "inputs larger than L2 (condensed blocks H 737 MB, D^-1 F 614 MB per solve at 16^3)",
+            "parallelism": "replicas (one independent solve per GPU)"}
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples while the timed region runs."""
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+                for k, nm in enumerate(names):
+                    if r[5 + k].lower() in ("active", "1"):
+                        reasons.add(nm)
+            except (ValueError, IndexError):
+                continue
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f), "measured"
+    except (OSError, ValueError):
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+def make_case(tmp, n):
+    from exasim_b200 import cases
+    d = os.path.join(tmp, "datain")
+    # 20 DIRK steps of dt = 0.01 (the configuration); stages beyond them wrap around
+    cases.convdiff3d_hex(d, n=n, porder=CFG_P, nsteps=20, dt=0.01)
+    return d
+
+
+def _oracle_case(tmp, n):
+    from oracle.hdg import HDGOracle
+    from oracle.models import MODELS
+    from exasim_b200 import cases
+    d = os.path.join(tmp, f"cpu_datain_{n}")
+    cases.convdiff3d_hex(d, n=n, porder=CFG_P, nsteps=20, dt=0.01)
+    return HDGOracle(d, MODELS["convdiff3d"]())
+
+
+def _oracle_stage_times(o, nsolves):
+    """Wall time of each DIRK-stage Newton solve of the oracle (stages of successive steps)."""
+    times = []
+
+    def hook(istep, j, _o):
+        times.append(time.perf_counter())
+
+    t0 = time.perf_counter()
+    times.append(t0)
+    o.dirk_solve(nsteps=(nsolves + 2) // 3, on_stage=hook)
+    d = np.diff(times)
+    return list(d[:nsolves])
+
+
+SAMPLE_N = 4
+
+
+def cpu_baseline_sample(tmp, full_n):
+    """Oracle (numpy + LAPACK, all host threads) on a 4^3 sub-problem of the same physics:
+    DIRK(3,3) stage Newton solves; solves/s scaled by element count to the full mesh."""
+    o = _oracle_case(tmp, SAMPLE_N)
+    per = _oracle_stage_times(o, 3)
+    per_solve = statistics.median(per)
+    scale = (SAMPLE_N ** 3) / float(full_n ** 3)
+    return {"value": scale / per_solve, "unit": "solves/s", "cores": os.cpu_count(), "kind": "port",
+            "sample": f"oracle/hdg.py (numpy + LAPACK, {os.cpu_count()} host threads): DIRK(3,3) stage "
+                      f"Newton solves on the {SAMPLE_N}^3 sub-mesh ({SAMPLE_N ** 3} of {full_n ** 3} elements), "
+                      f"{per_solve:.2f} s per solve, scaled by element count"}
+
+
+def run_reference(args):
+    """The reference path's CPU restatement (the reference itself is not built here), one
+    DIRK-stage solve on the 4^3 sub-mesh per step, reported scaled to the full mesh."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    with tempfile.TemporaryDirectory() as tmp:
+        o = _oracle_case(tmp, SAMPLE_N)
+        if args.warmup > 0:
+            _oracle_stage_times(o, 1)
+        steps = max(1, min(args.steps, 45))
+        per = _oracle_stage_times(o, steps)
+        scale = (SAMPLE_N ** 3) / float(args.n ** 3)
+        v = scale * len(per) / sum(per)
+        sample = (f"oracle/hdg.py (numpy + LAPACK, {os.cpu_count()} host threads): {len(per)} DIRK(3,3) stage "
+                  f"Newton solves on the {SAMPLE_N}^3 sub-mesh ({SAMPLE_N ** 3} of {args.n ** 3} elements), "
+                  "solves/s scaled by element count")
+        line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "solves/s", "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / v,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (seeded mesh and source of the configuration's shape)", "config": config(args.n),
+                "latency_ms": {"p50": float(np.percentile(per, 50)) * 1000.0 / scale,
+                               "p99": float(np.percentile(per, 99)) * 1000.0 / scale},
+                "cpu_baseline": {"value": v, "unit": "solves/s", "cores": os.cpu_count(), "kind": "port",
+                                 "sample": sample},
+                "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    from exasim_b200 import HDGSolver, load_library, build as B
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    if rank == 0:
+        B.build(["convdiff3d"])
+    if world > 1:
+        dist.barrier()
+    lib = load_library("convdiff3d")
+    with tempfile.TemporaryDirectory() as tmp:
+        d = make_case(tmp, args.n)
+        s = HDGSolver(d, "convdiff3d", device=local)
+        stream = torch.cuda.ExternalStream(s.stream(), device=local)
+        ndt, S = 20, 3
+        k = [0]
+
+        def stage():
+            istep, j = divmod(k[0], S)
+            its, nrm = s.DIRKStage(istep % ndt, j)
+            k[0] += 1
+            return its
+
+        for _ in range(args.warmup):
+            stage()
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+        gmres = []
+        l0 = lib.exa_launch_count()
+        with ClockSampler(local) as clk:
+            torch.cuda.synchronize()
+            ev[0].record(stream)
+            for i in range(args.steps):
+                stage()
+                gmres.append(s.stats()["gmres_total"])
+                ev[i + 1].record(stream)
+            torch.cuda.synchronize()
+        launches = lib.exa_launch_count() - l0
+        per = [ev[i].elapsed_time(ev[i + 1]) for i in range(args.steps)]
+        total_ms = ev[0].elapsed_time(ev[args.steps])
+        t = torch.tensor([total_ms], dtype=torch.float64, device=f"cuda:{local}")
+        if world > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+        value = world * args.steps / (total_ms / 1000.0)
+
+        # end-to-end: the same stage solve through the C ABI from pinned host buffers
+        nu, nh, ns = s.field_size("udg"), s.field_size("uh"), s.field_size("sdg")
+        h_udg = torch.from_numpy(s.get("udg")).pin_memory().numpy()
+        h_uh = torch.from_numpy(s.get("uh")).pin_memory().numpy()
+        h_sdg = torch.from_numpy(s.get("sdg")).pin_memory().numpy()
+        o_udg = torch.empty(nu, dtype=torch.float64).pin_memory().numpy()
+        o_uh = torch.empty(nh, dtype=torch.float64).pin_memory().numpy()
+        ne2e = args.e2e_steps or max(3, min(args.steps, 10))
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(ne2e):
+            s.set("sdg", h_sdg)
+            s.solve(h_udg, h_uh, o_udg, o_uh)
+        torch.cuda.synchronize()
+        e2e_s = time.perf_counter() - t0
+        e2e = {"value": world * ne2e / e2e_s, "unit": "solves/s", "steps": ne2e,
+               "h2d_bytes_per_step": 8 * (nu + nh + ns), "d2h_bytes_per_step": 8 * (nu + nh)}
+
+        # dominant kernels timed alone on the solver's stream
+        roof = kernel_rooflines(s, stream, torch)
+        out = None
+        if rank == 0:
+            clocks = clk.summary()
+            out = {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+                   "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+                   "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                   "data": "synthetic (seeded mesh and source of the configuration's shape)",
+                   "config": config(args.n),
+                   "latency_ms": {"p50": float(np.percentile(per, 50)), "p99": float(np.percentile(per, 99))},
+                   "gmres_iters_per_solve": float(np.mean(gmres)), "gpu_launches": int(launches),
+                   "clocks": clocks, "e2e": e2e}
+            out.update(roof)
+            if not args.no_cpu_baseline and world == 1:
+                out["cpu_baseline"] = {k: v for k, v in cpu_baseline_sample(tmp, args.n).items()
+                                       if k != "per_solve_s_sample"}
+            print(json.dumps(out), flush=True)
+        s.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def kernel_rooflines(s, stream, torch):
+    """Time the trace-space matvec (reads every condensed block H once) and one assembly
+    alone on the solver's stream with CUDA events."""
+    peaks, src = measured_peaks()
+    sz = s.sizes
+    ne, m, N = sz["ne"], sz["m"], sz["ndofuhat"]
+    v = torch.randn(N, dtype=torch.float64, device=f"cuda:{torch.cuda.current_device()}")
+    w = torch.empty_like(v)
+    torch.cuda.synchronize()
+    for _ in range(3):
+        s.evalMatVec(v.data_ptr(), w.data_ptr())
+    reps = 20
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(reps):
+        s.evalMatVec(v.data_ptr(), w.data_ptr())
+    e1.record(stream)
+    torch.cuda.synchronize()
+    mv_ms = e0.elapsed_time(e1) / reps
+    # algorithmic bytes: H once (8 m^2 ne), gathered input and element output (16 m ne), face vector (16 N)
+    mv_bytes = 8 * m * m * ne + 16 * (m * ne + N)
+    achieved = mv_bytes / (mv_ms * 1e-3) / 1e9
+    e0.record(stream)
+    for _ in range(2):
+        s.hdgAssembleLinearSystem()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    asm_ms = e0.elapsed_time(e1) / 2
+    return {"roofline": {"kernel": "condensed matvec (elem_matvec_kernel + scatter_kernel)", "bound": "hbm",
+                         "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                         "frac": achieved / peaks["hbm_gbs"], "peak_source": src,
+                         "algorithmic_bytes_per_launch": mv_bytes, "ms_per_launch": mv_ms, "traffic": None},
+            "phase_ms": {"assembly": asm_ms, "matvec": mv_ms}}
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

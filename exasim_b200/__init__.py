@@ -65,6 +65,9 @@ def load_library(model: str) -> ctypes.CDLL:
         "exa_stats": ([P, PLL], I),
         "exa_synchronize": ([P], I),
         "exa_connectivity_host": ([P, P, P, P, I, I, I, I, I, P, P, PI], I),
+        "exa_dirk_stage": ([P, I, I, PI, PD], I),
+        "exa_stream": ([P, ctypes.POINTER(P)], I),
+        "exa_launch_count": ([], LL),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
@@ -179,6 +182,16 @@ class HDGSolver:
         its = np.zeros(max(1, nsteps * 8), dtype=np.int32)
         self._check(self.lib.exa_dirk(self.h, nsteps, _ptr(its), its.size))
         return its
+
+    def DIRKStage(self, istep: int, stage: int):
+        it, nrm = ctypes.c_int(), ctypes.c_double()
+        self._check(self.lib.exa_dirk_stage(self.h, istep, stage, ctypes.byref(it), ctypes.byref(nrm)))
+        return it.value, nrm.value
+
+    def stream(self) -> int:
+        p = ctypes.c_void_p()
+        self._check(self.lib.exa_stream(self.h, ctypes.byref(p)))
+        return int(p.value or 0)
 
     def solve(self, udg: Optional[np.ndarray] = None, uh: Optional[np.ndarray] = None,
               udg_out: Optional[np.ndarray] = None, uh_out: Optional[np.ndarray] = None):

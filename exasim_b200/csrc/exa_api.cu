@@ -532,6 +532,19 @@ int exa_dirk(exa_ctx* h, int nsteps, int* newton_iters, int max_out) {
   return exa_drv_dirk(h->c, nsteps, newton_iters, max_out);
 }
 
+int exa_dirk_stage(exa_ctx* h, int istep, int stage, int* iters, double* norm) {
+  EXA_TRY(guard(h));
+  EXA_TRY(exa_drv_dirk_stage(h->c, istep, stage, iters, norm));
+  EXA_CUDA(cudaStreamSynchronize(h->c.st));
+  return EXA_OK;
+}
+
+int exa_stream(exa_ctx* h, void** stream) {
+  EXA_TRY(guard(h));
+  *stream = (void*)h->c.st;
+  return EXA_OK;
+}
+
 int exa_solve(exa_ctx* h, const double* udg_in, const double* uh_in, double* udg_out, double* uh_out, int* iters,
               double* norm) {
   EXA_TRY(guard(h));

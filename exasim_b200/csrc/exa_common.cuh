@@ -47,8 +47,13 @@ const char* exa_get_error();
     if (s_ != EXA_OK) return s_;    \
   } while (0)
 
+// Every kernel launch site ends with EXA_LAUNCH_CHECK(), which also counts the launch
+// (exa_launch_count() in the C ABI).
+void exa_count_launch();
+
 #define EXA_LAUNCH_CHECK()                                                          \
   do {                                                                              \
+    exa_count_launch();                                                             \
     cudaError_t e_ = cudaGetLastError();                                            \
     if (e_ != cudaSuccess) {                                                        \
       exa_set_error("%s:%d launch: %s", __FILE__, __LINE__, cudaGetErrorString(e_)); \

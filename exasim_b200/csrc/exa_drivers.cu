@@ -290,58 +290,72 @@ __global__ void insert_u_kernel(ExaDims P, double* udg, const double* u) {
 }
 }  // namespace
 
-// DIRK time stepping around Newton (exasim.hpp:413-482, previoussolutions.cpp:23-45,
-// updatesource.cpp:32-80, updatesolution.cpp:118-140)
-int exa_drv_dirk(ExaCtx& c, int nsteps, int* its_out, int max_out) {
+// One DIRK stage around Newton (exasim.hpp:413-482): PreviousSolutions at stage 0
+// (previoussolutions.cpp:23-45), UpdateSourceDIRK (updatesource.cpp:32-80), the Newton
+// solve, and the stage accumulation of UpdateSolution (updatesolution.cpp:118-140).
+// `time0` is the time at the start of step `istep`.
+int exa_drv_dirk_stage(ExaCtx& c, int istep, int j, int* its_out, double* norm_out) {
   if (!c.tdep) { exa_set_error("app.bin is not time dependent"); return EXA_ERR_ARG; }
   std::vector<double> cc, d, t;
   if (!dirk_coeff(c.nstage, c.torder, cc, d, t)) { exa_set_error("DIRK(%d,%d) is not tabulated", c.nstage, c.torder); return EXA_ERR_UNSUPPORTED; }
+  if (istep < 0 || istep >= (int)c.dt.size()) { exa_set_error("step %d beyond the dt list", istep); return EXA_ERR_ARG; }
+  if (j < 0 || j >= c.nstage) { exa_set_error("stage %d out of range", j); return EXA_ERR_ARG; }
   const ExaDims& P = c.P;
   const int S = c.nstage;
   const long long Nu = (long long)P.n * P.ne;
   const int blocks = 1024;
-  int count = 0;
-  for (int istep = 0; istep < nsteps; ++istep) {
-    if (istep >= (int)c.dt.size()) { exa_set_error("step %d beyond the dt list", istep); return EXA_ERR_ARG; }
-    const double dt = c.dt[istep];
+  const double dt = c.dt[istep];
+  if (j == 0) {
     double csum = 1.0;
-    for (int j = 0; j < S; ++j) csum -= cc[j];
+    for (int k = 0; k < S; ++k) csum -= cc[k];
     extract_u_kernel<<<blocks, 256, 0, c.st>>>(P, c.udg, c.udgprev);
     EXA_LAUNCH_CHECK();
     EXA_TRY(exa_scale(c.utmp, c.udgprev, csum, Nu, c.st));
-    for (int j = 0; j < S; ++j) {
-      c.time = c.time0 + dt * t[j];
-      c.dtfactor = d[j * S + j] / dt;
-      // sdg from the stage history (UpdateSourceDIRK)
-      extract_u_kernel<<<blocks, 256, 0, c.st>>>(P, c.udg, c.du);
-      EXA_LAUNCH_CHECK();
-      if (j == 0) {
-        EXA_TRY(exa_scale(c.sdg, c.du, d[0] / dt, Nu, c.st));
-      } else if (j == 1) {
-        const double sc = (d[1] + d[S + 1]) / d[0];
-        EXA_TRY(exa_axpby(c.sdg, c.du, -d[1] / dt, sc, Nu, c.st));
-      } else if (j == 2) {
-        const double sc = d[2] / d[1];
-        const double pc = d[2] + d[S + 2] + d[2 * S + 2] - sc * (d[1] + d[S + 1]);
-        EXA_TRY(exa_axpby(c.sdg, c.du, -d[S + 2] / dt, sc, Nu, c.st));
-        EXA_TRY(exa_axpby(c.sdg, c.udgprev, pc / dt, 1.0, Nu, c.st));
-      } else {
-        exa_set_error("DIRK with more than 3 stages");
-        return EXA_ERR_UNSUPPORTED;
-      }
-      int its = 0;
-      double nrm = 0.0;
-      EXA_TRY(exa_drv_newton(c, &its, &nrm));
-      if (its_out && count < max_out) its_out[count] = its;
-      ++count;
-      // utmp += c_j u
-      extract_u_kernel<<<blocks, 256, 0, c.st>>>(P, c.udg, c.du);
-      EXA_LAUNCH_CHECK();
-      EXA_TRY(exa_axpby(c.utmp, c.du, cc[j], 1.0, Nu, c.st));
-    }
+  }
+  c.time = c.time0 + dt * t[j];
+  c.dtfactor = d[j * S + j] / dt;
+  extract_u_kernel<<<blocks, 256, 0, c.st>>>(P, c.udg, c.du);
+  EXA_LAUNCH_CHECK();
+  if (j == 0) {
+    EXA_TRY(exa_scale(c.sdg, c.du, d[0] / dt, Nu, c.st));
+  } else if (j == 1) {
+    const double sc = (d[1] + d[S + 1]) / d[0];
+    EXA_TRY(exa_axpby(c.sdg, c.du, -d[1] / dt, sc, Nu, c.st));
+  } else if (j == 2) {
+    const double sc = d[2] / d[1];
+    const double pc = d[2] + d[S + 2] + d[2 * S + 2] - sc * (d[1] + d[S + 1]);
+    EXA_TRY(exa_axpby(c.sdg, c.du, -d[S + 2] / dt, sc, Nu, c.st));
+    EXA_TRY(exa_axpby(c.sdg, c.udgprev, pc / dt, 1.0, Nu, c.st));
+  } else {
+    exa_set_error("DIRK with more than 3 stages");
+    return EXA_ERR_UNSUPPORTED;
+  }
+  int its = 0;
+  double nrm = 0.0;
+  EXA_TRY(exa_drv_newton(c, &its, &nrm));
+  if (its_out) *its_out = its;
+  if (norm_out) *norm_out = nrm;
+  extract_u_kernel<<<blocks, 256, 0, c.st>>>(P, c.udg, c.du);
+  EXA_LAUNCH_CHECK();
+  EXA_TRY(exa_axpby(c.utmp, c.du, cc[j], 1.0, Nu, c.st));
+  if (j == S - 1) {
     insert_u_kernel<<<blocks, 256, 0, c.st>>>(P, c.udg, c.utmp);
     EXA_LAUNCH_CHECK();
     c.time0 = c.time0 + dt;
+  }
+  return EXA_OK;
+}
+
+// nsteps DIRK steps (exasim.hpp:413-482)
+int exa_drv_dirk(ExaCtx& c, int nsteps, int* its_out, int max_out) {
+  int count = 0;
+  for (int istep = 0; istep < nsteps; ++istep) {
+    for (int j = 0; j < c.nstage; ++j) {
+      int its = 0;
+      EXA_TRY(exa_drv_dirk_stage(c, istep, j, &its, nullptr));
+      if (its_out && count < max_out) its_out[count] = its;
+      ++count;
+    }
   }
   EXA_CUDA(cudaStreamSynchronize(c.st));
   return EXA_OK;

@@ -13,7 +13,13 @@
 
 #include "exa_common.cuh"
 
+#include <atomic>
+
 static char g_err[1024] = "";
+static std::atomic<long long> g_launches{0};
+
+void exa_count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+extern "C" long long exa_launch_count(void) { return g_launches.load(); }
 
 void exa_set_error(const char* fmt, ...) {
   va_list ap;

@@ -70,4 +70,5 @@ int exa_drv_gmres(ExaCtx& c, int* iters, double* relerr);
 int exa_drv_getq(ExaCtx& c);
 int exa_drv_newton(ExaCtx& c, int* iters, double* norm);
 int exa_drv_dirk(ExaCtx& c, int nsteps, int* newton_iters_out, int max_out);
+int exa_drv_dirk_stage(ExaCtx& c, int istep, int stage, int* its_out, double* norm_out);
 int exa_drv_norm(ExaCtx& c, const double* x, long long n, double* out);

@@ -71,6 +71,12 @@ int exa_newton(exa_ctx* ctx, int* iters, double* norm);
 /* nsteps DIRK steps around Newton (Main/exasim.hpp:413-482); newton_iters[0..max_out) receives
  * the Newton count of each stage. */
 int exa_dirk(exa_ctx* ctx, int nsteps, int* newton_iters, int max_out);
+/* One DIRK stage of step istep (0-based, < number of dt entries): source update from the
+ * stage history (updatesource.cpp:32-80), Newton solve, stage accumulation
+ * (updatesolution.cpp:118-140); the last stage of a step advances the time. */
+int exa_dirk_stage(exa_ctx* ctx, int istep, int stage, int* iters, double* norm);
+/* The CUDA stream the context launches on (cudaStream_t), for events and interop. */
+int exa_stream(exa_ctx* ctx, void** stream);
 /* One Newton solve from host buffers: copies udg/uhat in (NULL keeps the current state),
  * solves, copies them out (NULL skips).  The end-to-end form of exa_newton. */
 int exa_solve(exa_ctx* ctx, const double* udg_in, const double* uh_in, double* udg_out,
@@ -84,6 +90,8 @@ int exa_connectivity_host(const int* t, const int* bf, const int* perm, const do
 /* out[4] = {last GMRES iterations, last Newton iterations, GMRES iterations of the last solve, 0} */
 int exa_stats(exa_ctx* ctx, long long* out);
 int exa_synchronize(exa_ctx* ctx);
+/* Number of CUDA kernels this library has launched since it was loaded (all contexts). */
+long long exa_launch_count(void);
 
 #ifdef __cplusplus
 }
