@@ -594,3 +594,20 @@ extern "C" int exa_connectivity_host(const int* t, const int* bf, const int* per
   *nf0 = conn.nf0;
   return nf;
 }
+
+// Batched FP64 primitives on device pointers (the kernels the assembly uses).
+extern "C" int exa_dgemm_batched(int M, int N, int K, double alpha, const double* A, long long lda, long long sA,
+                                 const double* B, long long ldb, long long sB, double beta, double* C, long long ldc,
+                                 long long sC, int batch, void* stream) {
+  GemmBatch g{};
+  g.M = M; g.N = N; g.K = K; g.alpha = alpha; g.beta = beta;
+  g.A = A; g.lda = lda; g.sA = sA; g.sA2 = 0;
+  g.B = B; g.ldb = ldb; g.sB = sB; g.sB2 = 0;
+  g.C = C; g.ldc = ldc; g.sC = sC; g.sC2 = 0;
+  g.batch = batch; g.batch2 = 1;
+  return exa_gemm(g, (cudaStream_t)stream);
+}
+
+extern "C" int exa_dinverse_batched(double* A, int n, long long stride, int batch, int* info_dev, void* stream) {
+  return exa_inverse(A, n, stride, batch, info_dev, (cudaStream_t)stream);
+}

@@ -30,86 +30,258 @@ void exa_set_error(const char* fmt, ...) {
 const char* exa_get_error() { return g_err; }
 
 // ----------------------------------------------------------------------------------
-// batched GEMM: 64x64 output tile per block, 256 threads, 4x4 accumulators per thread
-// (rows ty + 16*a, cols tx + 16*b so shared-memory reads are conflict free), K staged
-// through shared memory in chunks of 16.
+// batched GEMM.  256 threads in a 16 x 16 grid; each thread accumulates a TM x TN
+// register block (rows ty + 16*a, cols tx + 16*b), so a block tile is (16 TM) x (16 TN)
+// and every k step costs TM + TN shared-memory reads for TM*TN FMAs.  The tile shape
+// is picked per call to fit the element blocks (125 -> 128, 150 -> 160) with little
+// padding.  K advances in chunks of 8 through double-buffered shared memory.
 // ----------------------------------------------------------------------------------
 namespace {
-constexpr int TM = 64, TN = 64, TK = 16;
+constexpr int GK = 8;
 
-__global__ void __launch_bounds__(256) gemm_kernel(GemmBatch g) {
-  __shared__ double As[TK][TM + 1];
-  __shared__ double Bs[TK][TN + 1];
-  const int tilesM = (g.M + TM - 1) / TM;
+template <int TM, int TN>
+__global__ void __launch_bounds__(256, 1) gemm_kernel(GemmBatch g) {
+  constexpr int BM = 16 * TM, BN = 16 * TN;
+  __shared__ double As[2][GK][BM];
+  __shared__ double Bs[2][GK][BN + 1];
+  const int tilesM = (g.M + BM - 1) / BM;
   const int tm = blockIdx.x % tilesM, tn = blockIdx.x / tilesM;
   const long long b1 = blockIdx.y, b2 = blockIdx.z;
   const double* A = g.A + b1 * g.sA + b2 * g.sA2;
   const double* B = g.B + b1 * g.sB + b2 * g.sB2;
   double* C = g.C + b1 * g.sC + b2 * g.sC2;
-  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-  const int r0 = tm * TM, c0 = tn * TN;
-  double acc[4][4];
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  const int r0 = tm * BM, c0 = tn * BN;
+  double acc[TM][TN];
 #pragma unroll
-  for (int a = 0; a < 4; ++a)
+  for (int a = 0; a < TM; ++a)
 #pragma unroll
-    for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
-
-  for (int k0 = 0; k0 < g.K; k0 += TK) {
-    // A tile: 64 rows x 16 k, element t -> (row t%64, k t/64), coalesced along rows
+    for (int b = 0; b < TN; ++b) acc[a][b] = 0.0;
+  const int nk = (g.K + GK - 1) / GK;
+  // register staging of the next chunk
+  double ra[(BM * GK + 255) / 256], rb[(BN * GK + 255) / 256];
+  auto load = [&](int kc) {
+    const int k0 = kc * GK;
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      int t = threadIdx.x + 256 * q;
-      int r = t & 63, k = t >> 6;
-      int gr = r0 + r, gk = k0 + k;
-      As[k][r] = (gr < g.M && gk < g.K) ? A[gr + g.lda * gk] : 0.0;
+    for (int q = 0; q < (BM * GK + 255) / 256; ++q) {
+      const int t = tid + 256 * q;
+      const int r = t % BM, k = t / BM;
+      const int gr = r0 + r, gk = k0 + k;
+      ra[q] = (k < GK && gr < g.M && gk < g.K) ? A[gr + g.lda * gk] : 0.0;
     }
-    // B tile: 16 k x 64 cols, element t -> (k t%16, col t/16), coalesced along k
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      int t = threadIdx.x + 256 * q;
-      int k = t & 15, c = t >> 4;
-      int gk = k0 + k, gc = c0 + c;
-      Bs[k][c] = (gk < g.K && gc < g.N) ? B[gk + g.ldb * gc] : 0.0;
+    for (int q = 0; q < (BN * GK + 255) / 256; ++q) {
+      const int t = tid + 256 * q;
+      const int k = t % GK, c = t / GK;
+      const int gk = k0 + k, gc = c0 + c;
+      rb[q] = (c < BN && gk < g.K && gc < g.N) ? B[gk + g.ldb * gc] : 0.0;
     }
-    __syncthreads();
+  };
+  auto store = [&](int buf) {
 #pragma unroll
-    for (int k = 0; k < TK; ++k) {
-      double av[4], bv[4];
-#pragma unroll
-      for (int a = 0; a < 4; ++a) av[a] = As[k][ty + 16 * a];
-#pragma unroll
-      for (int b = 0; b < 4; ++b) bv[b] = Bs[k][tx + 16 * b];
-#pragma unroll
-      for (int a = 0; a < 4; ++a)
-#pragma unroll
-        for (int b = 0; b < 4; ++b) acc[a][b] = fma(av[a], bv[b], acc[a][b]);
+    for (int q = 0; q < (BM * GK + 255) / 256; ++q) {
+      const int t = tid + 256 * q;
+      const int r = t % BM, k = t / BM;
+      if (k < GK) As[buf][k][r] = ra[q];
     }
+#pragma unroll
+    for (int q = 0; q < (BN * GK + 255) / 256; ++q) {
+      const int t = tid + 256 * q;
+      const int k = t % GK, c = t / GK;
+      if (c < BN) Bs[buf][k][c] = rb[q];
+    }
+  };
+  load(0);
+  store(0);
+  __syncthreads();
+  for (int kc = 0; kc < nk; ++kc) {
+    const int buf = kc & 1;
+    if (kc + 1 < nk) load(kc + 1);
+#pragma unroll
+    for (int k = 0; k < GK; ++k) {
+      double av[TM], bv[TN];
+#pragma unroll
+      for (int a = 0; a < TM; ++a) av[a] = As[buf][k][ty + 16 * a];
+#pragma unroll
+      for (int b = 0; b < TN; ++b) bv[b] = Bs[buf][k][tx + 16 * b];
+#pragma unroll
+      for (int a = 0; a < TM; ++a)
+#pragma unroll
+        for (int b = 0; b < TN; ++b) acc[a][b] = fma(av[a], bv[b], acc[a][b]);
+    }
+    if (kc + 1 < nk) store(buf ^ 1);
     __syncthreads();
   }
 #pragma unroll
-  for (int a = 0; a < 4; ++a) {
-    int gr = r0 + ty + 16 * a;
+  for (int a = 0; a < TM; ++a) {
+    const int gr = r0 + ty + 16 * a;
     if (gr >= g.M) continue;
 #pragma unroll
-    for (int b = 0; b < 4; ++b) {
-      int gc = c0 + tx + 16 * b;
+    for (int b = 0; b < TN; ++b) {
+      const int gc = c0 + tx + 16 * b;
       if (gc >= g.N) continue;
       double* p = C + gr + g.ldc * gc;
-      double v = g.alpha * acc[a][b];
+      const double v = g.alpha * acc[a][b];
       *p = (g.beta == 0.0) ? v : v + g.beta * (*p);
     }
   }
+}
+
+// C = alpha A x + beta C for N = 1: one warp per output row block
+__global__ void gemv_batch_kernel(GemmBatch g) {
+  const long long b1 = blockIdx.y, b2 = blockIdx.z;
+  const double* A = g.A + b1 * g.sA + b2 * g.sA2;
+  const double* x = g.B + b1 * g.sB + b2 * g.sB2;
+  double* C = g.C + b1 * g.sC + b2 * g.sC2;
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < g.M; r += gridDim.x * blockDim.x) {
+    double s = 0.0;
+    for (int k = 0; k < g.K; ++k) s = fma(A[r + g.lda * k], x[k], s);
+    const double v = g.alpha * s;
+    C[r] = (g.beta == 0.0) ? v : v + g.beta * C[r];
+  }
+}
+
+// ----------------------------------------------------------------------------------
+// FP64 tensor-core (DMMA, mma.sync m8n8k4 f64) batched GEMM.  A warp owns a
+// (8 TI) x (8 TJ) block of C held as TI*TJ 8x8 accumulator fragments; the CTA is a
+// WM x WN grid of warps.  A and B tiles go through double-buffered shared memory in
+// chunks of 8 along K, stored k-major with a row stride of 4 (mod 16) doubles so the
+// fragment loads of a half-warp hit distinct banks.
+// Fragment layout (PTX ISA, m8n8k4 .f64): a0 = A[lane/4][lane%4], b0 = B[lane%4][lane/4],
+// c0/c1 = C[lane/4][2 (lane%4) + 0/1].
+// ----------------------------------------------------------------------------------
+constexpr int DK = 8;
+
+__device__ __forceinline__ void dmma(double& c0, double& c1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+               : "+d"(c0), "+d"(c1)
+               : "d"(a), "d"(b));
+}
+
+template <int TI, int TJ, int WM, int WN>
+__global__ void __launch_bounds__(32 * WM * WN) dmma_gemm_kernel(GemmBatch g) {
+  constexpr int BM = 8 * TI * WM, BN = 8 * TJ * WN, NT = 32 * WM * WN;
+  constexpr int SA = BM + 4 + ((16 - (BM + 4) % 16) + 4) % 16, SB = BN + 4 + ((16 - (BN + 4) % 16) + 4) % 16;
+  __shared__ double As[2][DK][SA];
+  __shared__ double Bs[2][DK][SB];
+  const int tilesM = (g.M + BM - 1) / BM;
+  const int tm = blockIdx.x % tilesM, tn = blockIdx.x / tilesM;
+  const long long b1 = blockIdx.y, b2 = blockIdx.z;
+  const double* A = g.A + b1 * g.sA + b2 * g.sA2;
+  const double* B = g.B + b1 * g.sB + b2 * g.sB2;
+  double* C = g.C + b1 * g.sC + b2 * g.sC2;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int wm = warp % WM, wn = warp / WM;
+  const int r0 = tm * BM, c0 = tn * BN;
+  const int gq = lane >> 2, tq = lane & 3;
+  double acc[TI][TJ][2];
+#pragma unroll
+  for (int i = 0; i < TI; ++i)
+#pragma unroll
+    for (int j = 0; j < TJ; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+  constexpr int LA = (BM * DK + NT - 1) / NT, LB = (BN * DK + NT - 1) / NT;
+  double ra[LA], rb[LB];
+  const int nk = (g.K + DK - 1) / DK;
+  auto load = [&](int kc) {
+    const int k0 = kc * DK;
+#pragma unroll
+    for (int q = 0; q < LA; ++q) {
+      const int t = tid + NT * q;
+      const int r = t % BM, k = t / BM;
+      const int gr = r0 + r, gk = k0 + k;
+      ra[q] = (k < DK && gr < g.M && gk < g.K) ? A[gr + g.lda * gk] : 0.0;
+    }
+#pragma unroll
+    for (int q = 0; q < LB; ++q) {
+      const int t = tid + NT * q;
+      const int k = t % DK, c = t / DK;
+      const int gk = k0 + k, gc = c0 + c;
+      rb[q] = (c < BN && gk < g.K && gc < g.N) ? B[gk + g.ldb * gc] : 0.0;
+    }
+  };
+  auto store = [&](int buf) {
+#pragma unroll
+    for (int q = 0; q < LA; ++q) {
+      const int t = tid + NT * q;
+      const int r = t % BM, k = t / BM;
+      if (k < DK) As[buf][k][r] = ra[q];
+    }
+#pragma unroll
+    for (int q = 0; q < LB; ++q) {
+      const int t = tid + NT * q;
+      const int k = t % DK, c = t / DK;
+      if (c < BN) Bs[buf][k][c] = rb[q];
+    }
+  };
+  load(0);
+  store(0);
+  __syncthreads();
+  const int wr = wm * 8 * TI, wc = wn * 8 * TJ;
+  for (int kc = 0; kc < nk; ++kc) {
+    const int buf = kc & 1;
+    if (kc + 1 < nk) load(kc + 1);
+#pragma unroll
+    for (int k4 = 0; k4 < DK; k4 += 4) {
+      double af[TI], bf[TJ];
+#pragma unroll
+      for (int i = 0; i < TI; ++i) af[i] = As[buf][k4 + tq][wr + 8 * i + gq];
+#pragma unroll
+      for (int j = 0; j < TJ; ++j) bf[j] = Bs[buf][k4 + tq][wc + 8 * j + gq];
+#pragma unroll
+      for (int i = 0; i < TI; ++i)
+#pragma unroll
+        for (int j = 0; j < TJ; ++j) dmma(acc[i][j][0], acc[i][j][1], af[i], bf[j]);
+    }
+    if (kc + 1 < nk) store(buf ^ 1);
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < TI; ++i) {
+    const int gr = r0 + wr + 8 * i + gq;
+    if (gr >= g.M) continue;
+#pragma unroll
+    for (int j = 0; j < TJ; ++j)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int gc = c0 + wc + 8 * j + 2 * tq + h;
+        if (gc >= g.N) continue;
+        double* p = C + gr + g.ldc * gc;
+        const double v = g.alpha * acc[i][j][h];
+        *p = (g.beta == 0.0) ? v : v + g.beta * (*p);
+      }
+  }
+}
+
+template <int TI, int TJ, int WM, int WN>
+int launch_dmma(const GemmBatch& g, cudaStream_t st) {
+  constexpr int BM = 8 * TI * WM, BN = 8 * TJ * WN;
+  dim3 grid((unsigned)(exa_ceil_div(g.M, BM) * exa_ceil_div(g.N, BN)), (unsigned)g.batch, (unsigned)g.batch2);
+  dmma_gemm_kernel<TI, TJ, WM, WN><<<grid, 32 * WM * WN, 0, st>>>(g);
+  EXA_LAUNCH_CHECK();
+  return EXA_OK;
+}
+
+int tiles_cost(int M, int N, int bm, int bn) {
+  return ((M + bm - 1) / bm) * bm * ((N + bn - 1) / bn) * bn;
+}
+
+template <int TM, int TN>
+int launch_gemm(const GemmBatch& g, cudaStream_t st) {
+  constexpr int BM = 16 * TM, BN = 16 * TN;
+  dim3 grid((unsigned)(exa_ceil_div(g.M, BM) * exa_ceil_div(g.N, BN)), (unsigned)g.batch, (unsigned)g.batch2);
+  gemm_kernel<TM, TN><<<grid, 256, 0, st>>>(g);
+  EXA_LAUNCH_CHECK();
+  return EXA_OK;
 }
 }  // namespace
 
 int exa_gemm(const GemmBatch& g, cudaStream_t st) {
   if (g.M <= 0 || g.N <= 0 || g.batch <= 0 || g.batch2 <= 0) return EXA_OK;
-  if (g.batch > 65535 * 1024 || g.batch2 > 65535) {
-    exa_set_error("gemm batch too large (%d, %d)", g.batch, g.batch2);
+  if (g.batch2 > 65535) {
+    exa_set_error("gemm second batch dimension too large (%d)", g.batch2);
     return EXA_ERR_ARG;
   }
-  dim3 grid((unsigned)(exa_ceil_div(g.M, TM) * exa_ceil_div(g.N, TN)), (unsigned)g.batch, (unsigned)g.batch2);
-  if (grid.y > 65535) {
+  if (g.batch > 65535) {
     // split the first batch dimension into chunks the grid can hold
     for (int b0 = 0; b0 < g.batch; b0 += 65535) {
       GemmBatch h = g;
@@ -121,111 +293,185 @@ int exa_gemm(const GemmBatch& g, cudaStream_t st) {
     }
     return EXA_OK;
   }
-  gemm_kernel<<<grid, 256, 0, st>>>(g);
-  EXA_LAUNCH_CHECK();
-  return EXA_OK;
+  if (g.N == 1) {
+    dim3 grid((unsigned)exa_ceil_div(g.M, 128), (unsigned)g.batch, (unsigned)g.batch2);
+    gemv_batch_kernel<<<grid, 128, 0, st>>>(g);
+    EXA_LAUNCH_CHECK();
+    return EXA_OK;
+  }
+  // tensor-core tiles sized to the element blocks: warp tiles of 32 or 40 rows/columns
+  // cover 125 -> 128 and 150 -> 160 with little padding; tiny blocks use 32 x 32 CTAs
+  if (g.M <= 40 && g.N <= 40) return launch_dmma<2, 2, 2, 2>(g, st);
+  const int cand[4][2] = {{4, 4}, {4, 5}, {5, 4}, {5, 5}};
+  int best = 0;
+  long long bc = -1;
+  for (int i = 0; i < 4; ++i) {
+    const long long c = tiles_cost(g.M, g.N, 8 * cand[i][0] * 4, 8 * cand[i][1] * 2);
+    if (bc < 0 || c < bc) { bc = c; best = i; }
+  }
+  switch (best) {
+    case 0: return launch_dmma<4, 4, 4, 2>(g, st);
+    case 1: return launch_dmma<4, 5, 4, 2>(g, st);
+    case 2: return launch_dmma<5, 4, 4, 2>(g, st);
+    default: return launch_dmma<5, 5, 4, 2>(g, st);
+  }
 }
 
 // ----------------------------------------------------------------------------------
-// batched explicit inverse (Gauss-Jordan, partial pivoting, column swaps undone at the
-// end).  Exasim forms the same explicit inverse with getrf + getri
-// (backend/Common/pblas.h:163-260); the pivot choice (largest magnitude, first on ties)
-// matches LAPACK's partial pivoting.
+// batched explicit inverse.  Exasim forms the explicit inverse of each element block
+// with getrf + getri (backend/Common/pblas.h:163-260).  Here: Gauss-Jordan exchange
+// steps with partial pivoting (pivot = largest magnitude among the rows not yet used,
+// first on ties), one block per matrix, the matrix held in registers: thread (tx, ty)
+// of a 16 x 32 grid owns rows ty + 32*a and columns tx + 16*b.  Rows are never swapped
+// physically; the pivot order is recorded and undone when the result is written, which
+// gives the same pivots and arithmetic as swapping.  Each exchange at pivot (p, k):
+//   a_pk <- 1/a_pk,  a_pj <- a_pj / a_pk,  a_ik <- -a_ik / a_pk,  a_ij <- a_ij - a_ik a_pj / a_pk.
 // ----------------------------------------------------------------------------------
 namespace {
 constexpr int INV_MAX_N = 160;
 
-__global__ void __launch_bounds__(512) inverse_kernel(double* Aall, int n, long long stride, int* flag) {
-  extern __shared__ double sm[];
-  double* A = sm;                                  // n x n, column-major
-  __shared__ int ipiv[INV_MAX_N];
-  __shared__ double s_d;
-  __shared__ int s_p;
+template <int RR, int RC>
+__global__ void __launch_bounds__(512, 1) inverse_kernel(double* Aall, int n, long long stride, int* flag) {
+  // double-buffered pivot column / pivot row: step k uses buffer k&1, so one barrier
+  // after publishing the column and one after publishing the row suffice per step
+  __shared__ double colk[2][INV_MAX_N];
+  __shared__ double rowp[2][INV_MAX_N];
+  __shared__ int perm[INV_MAX_N];   // perm[k] = pivot row of step k
   double* G = Aall + (long long)blockIdx.x * stride;
-  const int nn = n * n;
-  for (int t = threadIdx.x; t < nn; t += blockDim.x) A[t] = G[t];
-  __syncthreads();
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int k = 0; k < n; ++k) {
-    if (warp == 0) {
-      double best = -1.0;
-      int bi = n;
-      for (int i = k + lane; i < n; i += 32) {
-        double v = fabs(A[i + n * k]);
-        if (v > best) { best = v; bi = i; }
-      }
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;   // 16 x 32
+  const int lane = threadIdx.x & 31;
+  double a[RR][RC];
 #pragma unroll
-      for (int off = 16; off > 0; off >>= 1) {
-        double ob = __shfl_down_sync(0xffffffffu, best, off);
-        int oi = __shfl_down_sync(0xffffffffu, bi, off);
-        if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
-      }
-      if (lane == 0) {
-        if (!(best > 0.0)) { atomicExch(flag, 1); bi = k; }
-        s_p = bi;
-        ipiv[k] = bi;
-      }
+  for (int i = 0; i < RR; ++i)
+#pragma unroll
+    for (int j = 0; j < RC; ++j) {
+      const int r = ty + 32 * i, c = tx + 16 * j;
+      a[i][j] = (r < n && c < n) ? G[r + (long long)n * c] : 0.0;
+    }
+  unsigned used = 0u;  // bit q: row lane + 32 q already pivoted (identical in every warp)
+  bool singular = false;
+  for (int k = 0; k < n; ++k) {
+    const int buf = k & 1;
+    const int kb = k >> 4, kt = k & 15;
+    if (tx == kt) {
+#pragma unroll
+      for (int j = 0; j < RC; ++j)
+        if (j == kb) {
+#pragma unroll
+          for (int i = 0; i < RR; ++i) {
+            const int r = ty + 32 * i;
+            if (r < n) colk[buf][r] = a[i][j];
+          }
+        }
     }
     __syncthreads();
-    const int p = s_p;
-    if (p != k) {
-      for (int j = threadIdx.x; j < n; j += blockDim.x) {
-        double t = A[k + n * j];
-        A[k + n * j] = A[p + n * j];
-        A[p + n * j] = t;
+    // every warp finds the pivot (largest |a_rk| over unused rows, first on ties)
+    double best = -1.0;
+    int bi = n;
+#pragma unroll
+    for (int q = 0; q < (INV_MAX_N + 31) / 32; ++q) {
+      const int r = lane + 32 * q;
+      if (r < n && !((used >> q) & 1u)) {
+        const double v = fabs(colk[buf][r]);
+        if (v > best) { best = v; bi = r; }
       }
     }
-    __syncthreads();
-    if (threadIdx.x == 0) s_d = 1.0 / A[k + n * k];
-    __syncthreads();
-    const double d = s_d;
-    for (int j = threadIdx.x; j < n; j += blockDim.x) A[k + n * j] = (j == k) ? d : A[k + n * j] * d;
-    __syncthreads();
-    // rank-1 update of every entry off row k and column k
-    for (int t = threadIdx.x; t < nn; t += blockDim.x) {
-      int i = t % n, j = t / n;
-      if (i != k && j != k) A[t] -= A[i + n * k] * A[k + n * j];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      const double ob = __shfl_xor_sync(0xffffffffu, best, off);
+      const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
+      if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
+    }
+    if (!(best > 0.0) || bi >= n) {
+      singular = true;
+      // continue on the first unused row so the block still terminates
+      bi = n;
+      for (int r = 0; r < n; ++r) {
+        const int owner = r & 31, q = r >> 5;
+        const unsigned u = __shfl_sync(0xffffffffu, used, owner);
+        if (!((u >> q) & 1u)) { bi = r; break; }
+      }
+      if (bi >= n) bi = 0;
+    }
+    const int p = bi;
+    if (lane == (p & 31)) used |= 1u << (p >> 5);
+    const double d = 1.0 / colk[buf][p];
+    if (threadIdx.x == 0) perm[k] = p;
+    const int pa = p >> 5, pt = p & 31;
+    if (ty == pt) {
+#pragma unroll
+      for (int i = 0; i < RR; ++i)
+        if (i == pa) {
+#pragma unroll
+          for (int j = 0; j < RC; ++j) {
+            const int c = tx + 16 * j;
+            const double v = (c == k) ? d : a[i][j] * d;
+            a[i][j] = v;
+            if (c < n) rowp[buf][c] = v;
+          }
+        }
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < n; i += blockDim.x)
-      if (i != k) A[i + n * k] = -A[i + n * k] * d;
-    __syncthreads();
+    double fv[RR], rv[RC];
+#pragma unroll
+    for (int i = 0; i < RR; ++i) {
+      const int r = ty + 32 * i;
+      fv[i] = (r < n) ? colk[buf][r] : 0.0;
+    }
+#pragma unroll
+    for (int j = 0; j < RC; ++j) {
+      const int c = tx + 16 * j;
+      rv[j] = (c < n) ? rowp[buf][c] : 0.0;
+    }
+#pragma unroll
+    for (int i = 0; i < RR; ++i) {
+      const int r = ty + 32 * i;
+      if (r == p) continue;
+#pragma unroll
+      for (int j = 0; j < RC; ++j) {
+        const int c = tx + 16 * j;
+        a[i][j] = (c == k) ? -fv[i] * d : a[i][j] - fv[i] * rv[j];
+      }
+    }
   }
-  for (int k = n - 1; k >= 0; --k) {
-    const int p = ipiv[k];
-    if (p != k) {
-      for (int i = threadIdx.x; i < n; i += blockDim.x) {
-        double t = A[i + n * k];
-        A[i + n * k] = A[i + n * p];
-        A[i + n * p] = t;
-      }
+  if (singular && threadIdx.x == 0) atomicExch(flag, 1);
+  // element (r, c) of the exchanged tableau is inverse(pos[r], perm[c]) with pos = perm^-1
+  __shared__ int pos[INV_MAX_N];
+  __syncthreads();
+  for (int t = threadIdx.x; t < n; t += blockDim.x) pos[perm[t]] = t;
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < RR; ++i)
+#pragma unroll
+    for (int j = 0; j < RC; ++j) {
+      const int r = ty + 32 * i, c = tx + 16 * j;
+      if (r < n && c < n) G[pos[r] + (long long)n * perm[c]] = a[i][j];
     }
-    __syncthreads();
-  }
-  for (int t = threadIdx.x; t < nn; t += blockDim.x) G[t] = A[t];
+}
+
+template <int RR, int RC>
+int launch_inverse(double* A, int n, long long stride, int batch, int* d_flag, cudaStream_t st) {
+  inverse_kernel<RR, RC><<<batch, 512, 0, st>>>(A, n, stride, d_flag);
+  EXA_LAUNCH_CHECK();
+  return EXA_OK;
 }
 }  // namespace
 
 int exa_inverse(double* A, int n, long long stride, int batch, int* d_flag, cudaStream_t st) {
   if (batch <= 0) return EXA_OK;
   if (n > INV_MAX_N || n <= 0) {
-    exa_set_error("dense inverse of order %d exceeds the shared-memory kernel limit %d", n, INV_MAX_N);
+    exa_set_error("dense inverse of order %d exceeds the register kernel limit %d", n, INV_MAX_N);
     return EXA_ERR_UNSUPPORTED;
   }
-  size_t smem = (size_t)n * n * sizeof(double);
-  static bool attr_set = false;
-  if (!attr_set) {
-    EXA_CUDA(cudaFuncSetAttribute(inverse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  INV_MAX_N * INV_MAX_N * (int)sizeof(double)));
-    attr_set = true;
-  }
-  int threads = n * n >= 4096 ? 512 : (n * n >= 1024 ? 256 : 128);
-  for (int b0 = 0; b0 < batch; b0 += 1 << 30) {
-    int nb = batch - b0;
-    inverse_kernel<<<nb, threads, smem, st>>>(A + (long long)b0 * stride, n, stride, d_flag);
-    EXA_LAUNCH_CHECK();
-  }
-  return EXA_OK;
+  const int rr = (n + 31) / 32, rc = (n + 15) / 16;
+  // rows per thread 1..5, columns per thread 1..10
+  if (rr <= 1 && rc <= 2) return launch_inverse<1, 2>(A, n, stride, batch, d_flag, st);
+  if (rr <= 1 && rc <= 4) return launch_inverse<1, 4>(A, n, stride, batch, d_flag, st);
+  if (rr <= 2 && rc <= 4) return launch_inverse<2, 4>(A, n, stride, batch, d_flag, st);
+  if (rr <= 2 && rc <= 6) return launch_inverse<2, 6>(A, n, stride, batch, d_flag, st);
+  if (rr <= 3 && rc <= 6) return launch_inverse<3, 6>(A, n, stride, batch, d_flag, st);
+  if (rr <= 4 && rc <= 8) return launch_inverse<4, 8>(A, n, stride, batch, d_flag, st);
+  return launch_inverse<5, 10>(A, n, stride, batch, d_flag, st);
 }
 
 // ----------------------------------------------------------------------------------

@@ -90,6 +90,15 @@ int exa_connectivity_host(const int* t, const int* bf, const int* perm, const do
 /* out[4] = {last GMRES iterations, last Newton iterations, GMRES iterations of the last solve, 0} */
 int exa_stats(exa_ctx* ctx, long long* out);
 int exa_synchronize(exa_ctx* ctx);
+/* Batched FP64 building blocks on device pointers, enqueued on `stream` (cudaStream_t, may
+ * be NULL): C_b = alpha A_b B_b + beta C_b (column-major, batch strides sA, sB, sC) as used for
+ * Exasim's PGEMNMStridedBached (backend/Common/pblas.h:695); and the in-place explicit
+ * inverse of `batch` n x n blocks `stride` doubles apart (pblas.h:163 Inverse), n <= 160,
+ * *info_dev set non-zero on a zero pivot. */
+int exa_dgemm_batched(int M, int N, int K, double alpha, const double* A, long long lda, long long sA,
+                      const double* B, long long ldb, long long sB, double beta, double* C, long long ldc,
+                      long long sC, int batch, void* stream);
+int exa_dinverse_batched(double* A, int n, long long stride, int batch, int* info_dev, void* stream);
 /* Number of CUDA kernels this library has launched since it was loaded (all contexts). */
 long long exa_launch_count(void);
 
