@@ -2,10 +2,11 @@
 // Gauss-Jordan inverse, and the deterministic vector reductions used by GMRES.
 //
 // Exasim runs these steps through cuBLAS (DgemmStridedBatched, DgetrfBatched +
-// DgetriBatched, Ddot/Daxpy/Dscal: backend/Common/pblas.h:163-734).  Here they are
-// plain SIMT kernels: the element blocks (n, m <= a few hundred) are too small for
-// tensor-core tiles in FP64, and the reductions stay on the device so the Krylov loop
-// only synchronises once per iteration.
+// DgetriBatched, Ddot/Daxpy/Dscal: backend/Common/pblas.h:163-734).  Here the GEMM runs
+// on the FP64 tensor cores (DMMA) with CTA tiles sized to the element blocks (n, m of a
+// few hundred), the inverse keeps each block in registers across a 512-thread CTA, and
+// the reductions stay on the device so the Krylov loop only synchronises once per
+// iteration.
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
