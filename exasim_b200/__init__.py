@@ -70,6 +70,7 @@ def load_library(model: str) -> ctypes.CDLL:
         "exa_launch_count": ([], LL),
         "exa_dgemm_batched": ([I, I, I, D, P, LL, LL, P, LL, LL, D, P, LL, LL, I, P], I),
         "exa_dinverse_batched": ([P, I, LL, I, P, P], I),
+        "exa_dnrm2_cols_fixed": ([P, LL, LL, I, P, P], I),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)

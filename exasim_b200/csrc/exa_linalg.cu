@@ -694,3 +694,104 @@ int exa_cgs(double* w, const double* V, double* hcol, double* part, long long n,
   EXA_LAUNCH_CHECK();
   return EXA_OK;
 }
+
+// ----------------------------------------------------------------------------------
+// Column 2-norms with fixed scratch (exa_dnrm2_cols_fixed in the C ABI).
+//
+// The Krylov norms above take their per-block partial sums from memory that a solver
+// context allocates when it is created.  This variant serves callers that hold no
+// context and may not allocate device memory where they call it: code running inside
+// another framework's memory pool, which has already reserved the free device memory so
+// a cudaMalloc there can fail, and step loops that cannot afford the device-wide
+// synchronisation that cudaFree performs.  Its partial sums live in the file-scope
+// device array below, a fixed 151,552 bytes (COLNRM_MAXCOLS x VB doubles), so it handles
+// at most COLNRM_MAXCOLS columns per call and rejects more with EXA_ERR_ARG.
+//
+// Nothing in the scratch has to start at zero: the first kernel overwrites every
+// partial of the columns it handles before the second kernel reads them.  The array is
+// one per device and per loaded library, so two calls whose kernels can overlap (on
+// different streams without an ordering event, or from several host threads) race on
+// it; calls on the same device must be ordered, e.g. issued on one stream.
+//
+// The arithmetic (grid-stride sums of squares per block, then the partials added in
+// block order) is that of the context's norm, so both give the same bits.
+// ----------------------------------------------------------------------------------
+#include <mutex>
+
+namespace {
+constexpr int COLNRM_MAXCOLS = 64;
+constexpr int COLNRM_MAXDEV = 64;
+}  // namespace
+
+static __device__ __align__(256) double g_colnrm_scratch[COLNRM_MAXCOLS * VB];
+
+namespace {
+std::mutex g_colnrm_mu;
+double* g_colnrm_ptr[COLNRM_MAXDEV] = {};
+
+// part[j * VB + block] = sum over this block's share of column j of x(i)^2
+__global__ void __launch_bounds__(VT) colnrm_partial_kernel(const double* X, long long n, long long ldx,
+                                                             double* part) {
+  const int j = blockIdx.y;
+  const double* x = X + ldx * j;
+  double v = 0.0;
+  for (long long i = blockIdx.x * (long long)VT + threadIdx.x; i < n; i += (long long)VB * VT) v = fma(x[i], x[i], v);
+  double s = block_sum(v);
+  if (threadIdx.x == 0) part[j * VB + blockIdx.x] = s;
+}
+
+// out[j] = sqrt(sum of column j's VB partials), one block per column
+__global__ void __launch_bounds__(VT) colnrm_finish_kernel(const double* part, double* out) {
+  double s = sum_partials(part + blockIdx.x * VB);
+  if (threadIdx.x == 0) out[blockIdx.x] = sqrt(s);
+}
+
+// Device address of this device's scratch, looked up on the first call made with that
+// device current and cached afterwards.
+int colnrm_scratch(double** out) {
+  int dev = 0;
+  EXA_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= COLNRM_MAXDEV) {
+    exa_set_error("exa_dnrm2_cols_fixed: device ordinal %d outside the %d devices it keeps scratch for", dev,
+                  COLNRM_MAXDEV);
+    return EXA_ERR_ARG;
+  }
+  std::lock_guard<std::mutex> lock(g_colnrm_mu);
+  if (!g_colnrm_ptr[dev]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_colnrm_scratch);
+    if (e != cudaSuccess || p == nullptr) {
+      exa_set_error("exa_dnrm2_cols_fixed: scratch address lookup failed: %s", cudaGetErrorString(e));
+      return EXA_ERR_CUDA;
+    }
+    g_colnrm_ptr[dev] = static_cast<double*>(p);
+  }
+  *out = g_colnrm_ptr[dev];
+  return EXA_OK;
+}
+}  // namespace
+
+extern "C" int exa_dnrm2_cols_fixed(const double* X, long long n, long long ldx, int ncols, double* out_dev,
+                                    void* stream) {
+  if (ncols < 1 || ncols > COLNRM_MAXCOLS) {
+    exa_set_error("exa_dnrm2_cols_fixed: ncols = %d, but its fixed scratch holds 1 to %d columns per call", ncols,
+                  COLNRM_MAXCOLS);
+    return EXA_ERR_ARG;
+  }
+  if (n < 0 || (ncols > 1 && ldx < n)) {
+    exa_set_error("exa_dnrm2_cols_fixed: bad sizes n = %lld, ldx = %lld", n, ldx);
+    return EXA_ERR_ARG;
+  }
+  if (out_dev == nullptr || (n > 0 && X == nullptr)) {
+    exa_set_error("exa_dnrm2_cols_fixed: null pointer");
+    return EXA_ERR_ARG;
+  }
+  double* part = nullptr;
+  EXA_TRY(colnrm_scratch(&part));
+  cudaStream_t st = (cudaStream_t)stream;
+  colnrm_partial_kernel<<<dim3(VB, ncols), VT, 0, st>>>(X, n, ldx, part);
+  EXA_LAUNCH_CHECK();
+  colnrm_finish_kernel<<<ncols, VT, 0, st>>>(part, out_dev);
+  EXA_LAUNCH_CHECK();
+  return EXA_OK;
+}

@@ -101,6 +101,17 @@ int exa_dgemm_batched(int M, int N, int K, double alpha, const double* A, long l
 int exa_dinverse_batched(double* A, int n, long long stride, int batch, int* info_dev, void* stream);
 /* Number of CUDA kernels this library has launched since it was loaded (all contexts). */
 long long exa_launch_count(void);
+/* Euclidean norms of `ncols` device columns of length n, column j at X + j*ldx, written to
+ * out_dev[0..ncols) on `stream` (cudaStream_t, may be NULL) without allocating anything.
+ * No counterpart in the reference: it exists for callers that cannot allocate device memory
+ * at the call (a host framework's memory pool owns the free memory, or the step loop cannot
+ * take cudaFree's device-wide synchronisation).  Its partial sums live in one fixed device
+ * array per device (64 columns x 296 blocks of doubles, 151,552 bytes); ncols > 64 returns
+ * EXA_ERR_ARG (1).  The first call on each device, with that device current, looks up the
+ * array's address (which can load this library's device code), so make it before any stream
+ * capture starts.  Nothing needs zeroing beforehand.  Calls whose kernels can overlap (other
+ * streams with no ordering, several host threads) race on the shared array: order them. */
+int exa_dnrm2_cols_fixed(const double* X, long long n, long long ldx, int ncols, double* out_dev, void* stream);
 
 #ifdef __cplusplus
 }

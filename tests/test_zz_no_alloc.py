@@ -1,0 +1,62 @@
+"""The fixed-scratch column-norm entry point (exa_dnrm2_cols_fixed), called through the C
+ABI.  Its norms must reproduce the residual norm that exa_residual reports (|b| + |Ru|,
+computed with the context's own allocated partials), on two calls in a row, and it must
+refuse more columns than its fixed scratch holds.  The file sorts last so the entry point
+also runs after every other GPU test of the session."""
+import ctypes
+
+import numpy as np
+import pytest
+
+from exasim_b200 import HDGSolver, build as B, cases
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-14
+
+
+def test_fixed_scratch_norms_match_residual_norm(tmp_path):
+    import torch
+    B.build(["poisson2d"])
+    d = str(tmp_path / "datain")
+    cases.poisson2d_tri(d, n=4)
+    s = HDGSolver(d, "poisson2d")
+    L = s.lib
+    st = ctypes.c_void_p(s.stream())
+    torch.cuda.set_device(0)
+    nrm = s.hdgAssembleResidual()
+    b, nb = s.field_ptr("b")
+    ru, nru = s.field_ptr("Ru")
+    out = torch.full((4,), -1.0, dtype=torch.float64, device="cuda")
+    results = []
+    for _ in range(2):
+        for k, (p, n) in enumerate(((b, nb), (ru, nru))):
+            rc = L.exa_dnrm2_cols_fixed(ctypes.c_void_p(p), n, n, 1, ctypes.c_void_p(out.data_ptr() + 8 * k), st)
+            assert rc == 0, L.exa_last_error().decode()
+        assert L.exa_synchronize(s.h) == 0
+        v = out.cpu().numpy()
+        results.append(v[0] + v[1])
+    assert results[0] == results[1]
+    assert abs(results[0] - nrm) <= TOL * nrm, (results, nrm)
+    # several columns in one call: the field copies side by side, against numpy
+    X = torch.zeros((3, nru), dtype=torch.float64, device="cuda")
+    ru_host = s.get("Ru")
+    for j in range(3):
+        X[j].copy_(torch.from_numpy(ru_host * (j + 1)))
+    torch.cuda.synchronize()
+    for _ in range(2):
+        out.fill_(-1.0)
+        torch.cuda.synchronize()
+        rc = L.exa_dnrm2_cols_fixed(ctypes.c_void_p(X.data_ptr()), nru, nru, 3, ctypes.c_void_p(out.data_ptr()),
+                                    None)
+        assert rc == 0, L.exa_last_error().decode()
+        torch.cuda.synchronize()
+        got = out.cpu().numpy()[:3]
+        ref = np.linalg.norm(ru_host) * np.arange(1, 4)
+        assert np.abs(got - ref).max() <= TOL * ref.max() * 10, (got, ref)
+        assert out.cpu().numpy()[3] == -1.0
+    # more columns than the fixed scratch holds: refused on the host, nothing launched
+    before = L.exa_launch_count()
+    rc = L.exa_dnrm2_cols_fixed(ctypes.c_void_p(X.data_ptr()), 1, 1, 65, ctypes.c_void_p(out.data_ptr()), None)
+    assert rc == 1 and "65" in L.exa_last_error().decode()
+    assert L.exa_launch_count() == before
+    s.close()
