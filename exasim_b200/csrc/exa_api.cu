@@ -255,12 +255,14 @@ int exa_ctx_init(ExaCtx& c, const double* app, long long napp, const double* mas
     g.M = P.npe; g.N = P.npe; g.K = P.npe; g.alpha = 1.0; g.beta = 0.0;
     g.A = mass; g.lda = P.npe; g.sA = (long long)P.npe * P.npe; g.sA2 = 0;
     g.B = cw; g.ldb = P.npe; g.sB = (long long)P.npe * P.npe * P.nd; g.sB2 = (long long)P.npe * P.npe;
-    g.C = c.MC; g.ldc = P.npe; g.sC = (long long)P.npe * P.npe * P.nd; g.sC2 = (long long)P.npe * P.npe;
+    // stored with rows (l, d) stacked: MinvC(l, d, j) = MC[l + npe*d + npe*nd*j], so the Schur
+    // q-elimination contracts over (l, d) in one GEMM per block
+    g.C = c.MC; g.ldc = (long long)P.npe * P.nd; g.sC = (long long)P.npe * P.npe * P.nd; g.sC2 = P.npe;
     g.batch = P.ne; g.batch2 = P.nd;
     EXA_TRY(exa_gemm(g, c.st));
     g.N = P.ndf;
     g.B = ew; g.sB = (long long)P.npe * P.ndf * P.nd; g.sB2 = (long long)P.npe * P.ndf;
-    g.C = c.ME; g.sC = (long long)P.npe * P.ndf * P.nd; g.sC2 = (long long)P.npe * P.ndf;
+    g.C = c.ME; g.sC = (long long)P.npe * P.ndf * P.nd; g.sC2 = P.npe;
     EXA_TRY(exa_gemm(g, c.st));
     EXA_CUDA(cudaStreamSynchronize(c.st));
     int flag_h = 0;

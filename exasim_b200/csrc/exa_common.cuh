@@ -10,7 +10,7 @@
 //   K    [m, n]     per element   row (k,jf) = k + ncu*jf
 //   H    [m, m]     per element
 //   B    [n, npe*nd*ncu], G [m, npe*nd*ncu]: column (j, d, n) = j + npe*d + npe*nd*n
-//   MinvC [npe, npe, nd], MinvE [npe, ndf, nd] per element
+//   MinvC [npe, nd, npe], MinvE [npe, nd, ndf] per element (dimension next to the row)
 #pragma once
 #include <cstddef>
 #include <cstdint>

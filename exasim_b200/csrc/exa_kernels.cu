@@ -291,9 +291,12 @@ __global__ void getq_kernel(ExaDims P, const int* elemcon, const double* MC, con
   for (int t = threadIdx.x; t < npe * ncu * nd; t += blockDim.x) {
     const int i = t % npe, k = (t / npe) % ncu, d = t / (npe * ncu);
     double s = 0.0;
-    for (int j = 0; j < npe; ++j) s = fma(C[i + npe * j + npe * npe * d], u[j + npe * k], s);
+    const double* Cd = C + i + npe * d;
+    const double* Ed = E + i + npe * d;
+    const int ld = npe * nd;
+    for (int j = 0; j < npe; ++j) s = fma(Cd[ld * j], u[j + npe * k], s);
     double r = 0.0;
-    for (int j = 0; j < ndf; ++j) r = fma(E[i + npe * j + npe * ndf * d], uhe[j + ndf * k], r);
+    for (int j = 0; j < ndf; ++j) r = fma(Ed[ld * j], uhe[j + ndf * k], r);
     U[i + npe * (ncu + k + ncu * d)] = s - r;
   }
 }

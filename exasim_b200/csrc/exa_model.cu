@@ -46,33 +46,34 @@ int schur_chunk(ExaCtx& c, int e0, int nb) {
   if (P.ncq > 0) {
     const double* MC = c.MC + (long long)e0 * npe * npe * nd;
     const double* ME = c.ME + (long long)e0 * npe * ndf * nd;
-    for (int d = 0; d < nd; ++d) {
-      GemmBatch g{};
-      g.batch = nb; g.batch2 = ncu;
-      g.K = npe; g.beta = 1.0;
-      // D(:, j + npe*nq) += B(:, k + npe*d + npe*nd*nq) MinvC_d
-      g.M = n; g.N = npe; g.alpha = 1.0;
-      g.A = c.wB + (long long)n * npe * d; g.lda = n; g.sA = (long long)n * nqn; g.sA2 = (long long)n * npe * nd;
-      g.B = MC + (long long)npe * npe * d; g.ldb = npe; g.sB = (long long)npe * npe * nd; g.sB2 = 0;
-      g.C = c.wD; g.ldc = n; g.sC = (long long)n * n; g.sC2 = (long long)n * npe;
-      EXA_TRY(exa_gemm(g, c.st));
-      // F(:, b + ncu*jf) -= B(:, k + npe*d + npe*nd*b) MinvE_d
-      g.N = ndf; g.alpha = -1.0;
-      g.B = ME + (long long)npe * ndf * d; g.ldb = npe; g.sB = (long long)npe * ndf * nd;
-      g.C = c.wF; g.ldc = (long long)n * ncu; g.sC = (long long)n * m; g.sC2 = n;
-      EXA_TRY(exa_gemm(g, c.st));
-      // K(:, j + npe*nq) += G(:, k + npe*d + npe*nd*nq) MinvC_d
-      g.M = m; g.N = npe; g.alpha = 1.0;
-      g.A = c.wG + (long long)m * npe * d; g.lda = m; g.sA = (long long)m * nqn; g.sA2 = (long long)m * npe * nd;
-      g.B = MC + (long long)npe * npe * d; g.ldb = npe; g.sB = (long long)npe * npe * nd;
-      g.C = c.wK; g.ldc = m; g.sC = (long long)m * n; g.sC2 = (long long)m * npe;
-      EXA_TRY(exa_gemm(g, c.st));
-      // H(:, b + ncu*jf) -= G(:, k + npe*d + npe*nd*b) MinvE_d
-      g.N = ndf; g.alpha = -1.0;
-      g.B = ME + (long long)npe * ndf * d; g.ldb = npe; g.sB = (long long)npe * ndf * nd;
-      g.C = Hc; g.ldc = (long long)m * ncu; g.sC = (long long)m * m; g.sC2 = m;
-      EXA_TRY(exa_gemm(g, c.st));
-    }
+    // contraction over the stacked (l, d) rows of MinvC / MinvE (K = npe*nd), one GEMM per
+    // block and per trace component b (batch2 = ncu)
+    const long long kq = (long long)npe * nd;
+    GemmBatch g{};
+    g.batch = nb; g.batch2 = ncu;
+    g.K = (int)kq; g.beta = 1.0;
+    // D(:, j + npe*b) += sum_(l,d) B(:, l + npe*d + npe*nd*b) MinvC(l, d, j)
+    g.M = n; g.N = npe; g.alpha = 1.0;
+    g.A = c.wB; g.lda = n; g.sA = (long long)n * nqn; g.sA2 = (long long)n * kq;
+    g.B = MC; g.ldb = kq; g.sB = kq * npe; g.sB2 = 0;
+    g.C = c.wD; g.ldc = n; g.sC = (long long)n * n; g.sC2 = (long long)n * npe;
+    EXA_TRY(exa_gemm(g, c.st));
+    // F(:, b + ncu*jf) -= sum_(l,d) B(:, l + npe*d + npe*nd*b) MinvE(l, d, jf)
+    g.N = ndf; g.alpha = -1.0;
+    g.B = ME; g.ldb = kq; g.sB = kq * ndf;
+    g.C = c.wF; g.ldc = (long long)n * ncu; g.sC = (long long)n * m; g.sC2 = n;
+    EXA_TRY(exa_gemm(g, c.st));
+    // K(:, j + npe*b) += sum_(l,d) G(:, l + npe*d + npe*nd*b) MinvC(l, d, j)
+    g.M = m; g.N = npe; g.alpha = 1.0;
+    g.A = c.wG; g.lda = m; g.sA = (long long)m * nqn; g.sA2 = (long long)m * kq;
+    g.B = MC; g.ldb = kq; g.sB = kq * npe;
+    g.C = c.wK; g.ldc = m; g.sC = (long long)m * n; g.sC2 = (long long)m * npe;
+    EXA_TRY(exa_gemm(g, c.st));
+    // H(:, b + ncu*jf) -= sum_(l,d) G(:, l + npe*d + npe*nd*b) MinvE(l, d, jf)
+    g.N = ndf; g.alpha = -1.0;
+    g.B = ME; g.ldb = kq; g.sB = kq * ndf;
+    g.C = Hc; g.ldc = (long long)m * ncu; g.sC = (long long)m * m; g.sC2 = m;
+    EXA_TRY(exa_gemm(g, c.st));
   }
   EXA_TRY(exa_inverse(c.wD, n, (long long)n * n, nb, c.d_flag, c.st));
   GemmBatch g{};

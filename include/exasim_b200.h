@@ -40,7 +40,8 @@ int exa_sizes(exa_ctx* ctx, long long* out);
 
 /* Host copies of named device arrays: "udg", "uh", "H", "F" (D^-1 F after assembly),
  * "Ru", "Rh", "b", "x", "sdg", "P" (preconditioner), "MinvC", "MinvE", "elemg", "faceg".
- * n must equal the array length. */
+ * n must equal the array length.  MinvC and MinvE hold, per element, Minv*C_d and Minv*E_d
+ * with the dimension index next to the row index: [npe, nd, npe] and [npe, nd, npf*nfe]. */
 int exa_get_field(exa_ctx* ctx, const char* name, double* host, long long n);
 int exa_set_field(exa_ctx* ctx, const char* name, const double* host, long long n);
 /* Device pointer and length of a named array (zero-copy access, e.g. from torch). */

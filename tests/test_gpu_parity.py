@@ -79,10 +79,11 @@ def test_geometry_and_q_matrices(poisson2d_case):
     Xx = eg[nge * nd:nge * (nd + nd * nd)].reshape(nge, nd * nd, ne, order="F")
     jac = eg[nge * (nd + nd * nd):].reshape(nge, ne, order="F")
     assert rel(xg, o.xg) < ASM_TOL and rel(Xx, o.Xx) < ASM_TOL and rel(jac, o.jac) < ASM_TOL
-    MC = s.get("MinvC").reshape(o.npe, o.npe, nd, ne, order="F")
-    ME = s.get("MinvE").reshape(o.npe, o.npf * o.nfe, nd, ne, order="F")
-    assert rel(MC, np.transpose(o.MinvC, (0, 1, 3, 2))) < INV_TOL
-    assert rel(ME, np.transpose(o.MinvE, (0, 1, 3, 2))) < INV_TOL
+    # stored per element as [npe, nd, npe] and [npe, nd, ndf] (rows (l, d) stacked)
+    MC = s.get("MinvC").reshape(o.npe, nd, o.npe, ne, order="F")
+    ME = s.get("MinvE").reshape(o.npe, nd, o.npf * o.nfe, ne, order="F")
+    assert rel(MC, np.transpose(o.MinvC, (0, 3, 1, 2))) < INV_TOL
+    assert rel(ME, np.transpose(o.MinvE, (0, 3, 1, 2))) < INV_TOL
     s.close()
 
 
