@@ -227,6 +227,7 @@ def run_ours(args):
             dist.barrier()
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
         gmres = []
+        s.profile(True)  # per-phase CUDA events on the solver's stream, read after the timed region
         l0 = lib.exa_launch_count()
         with ClockSampler(local) as clk:
             torch.cuda.synchronize()
@@ -237,6 +238,8 @@ def run_ours(args):
                 ev[i + 1].record(stream)
             torch.cuda.synchronize()
         launches = lib.exa_launch_count() - l0
+        s.profile(False)
+        prof = s.profile_read()
         per = [ev[i].elapsed_time(ev[i + 1]) for i in range(args.steps)]
         total_ms = ev[0].elapsed_time(ev[args.steps])
         t = torch.tensor([total_ms], dtype=torch.float64, device=f"cuda:{local}")
@@ -263,8 +266,8 @@ def run_ours(args):
         e2e = {"value": world * ne2e / e2e_s, "unit": "solves/s", "steps": ne2e,
                "h2d_bytes_per_step": 8 * (nu + nh + ns), "d2h_bytes_per_step": 8 * (nu + nh)}
 
-        # dominant kernels timed alone on the solver's stream
-        roof = kernel_rooflines(s, stream, torch)
+        # the dominant kernel from the live phase timers; the matvec timed alone
+        roof = kernel_rooflines(s, stream, torch, prof, args.steps)
         out = None
         if rank == 0:
             clocks = clk.summary()
@@ -288,12 +291,54 @@ def run_ours(args):
     return 0
 
 
-def kernel_rooflines(s, stream, torch):
-    """Time the trace-space matvec (reads every condensed block H once) and one assembly
-    alone on the solver's stream with CUDA events."""
+# DRAM traffic of the four q-elimination GEMM launches of one assembly, from one ncu capture
+# (dram__bytes_read.sum + dram__bytes_write.sum) on the 10^3-element mesh of this workload:
+# 4.458 GB for 1000 elements; it scales with the element count (each element's blocks are
+# read once), so per launch and element it is 4.458e9 / 1000 / 4 bytes.
+QELIM_TRAFFIC_PER_ELEMENT_LAUNCH = 4.458e9 / 1000 / 4
+
+
+def fp64_gemm_peak(torch):
+    """cuBLAS DGEMM at 8192^3 on this GPU, in TFLOP/s (the FP64 tensor-core reference)."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn_like(a)
+    for _ in range(2):
+        a @ b
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(4):
+        a @ b
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / 4
+    del a, b
+    torch.cuda.empty_cache()
+    return 2.0 * n ** 3 / (ms * 1e-3) / 1e12
+
+
+def kernel_rooflines(s, stream, torch, prof, steps):
+    """roofline: the q-elimination GEMMs (dmma_gemm_kernel, the largest share of a solve),
+    from the phase timers recorded inside the timed region.  matvec_roofline: the trace-space
+    matvec (reads every condensed block H once) timed alone on the solver's stream."""
     peaks, src = measured_peaks()
     sz = s.sizes
     ne, m, N = sz["ne"], sz["m"], sz["ndofuhat"]
+    q_ms, q_regions, q_flops = prof["qelim"]
+    gemm_launches = 4 * q_regions  # four GEMMs per q-elimination region
+    peak64 = fp64_gemm_peak(torch)
+    ms_launch = q_ms / max(gemm_launches, 1)
+    achieved = q_flops / max(gemm_launches, 1) / (ms_launch * 1e-3) / 1e12 if q_ms > 0 else 0.0
+    roofline = {"kernel": "dmma_gemm_kernel (q-elimination GEMMs: D += B MinvC, F -= B MinvE, K += G MinvC, "
+                          "H -= G MinvE; FP64 tensor cores)",
+                "bound": "tensor", "achieved": achieved, "peak": peak64, "unit": "TFLOP/s",
+                "frac": achieved / peak64,
+                "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (MEASURED_PEAKS.json has no FP64 figure)",
+                "algorithmic_flops_per_launch": q_flops / max(gemm_launches, 1), "ms_per_launch": ms_launch,
+                "launches": gemm_launches,
+                "traffic": QELIM_TRAFFIC_PER_ELEMENT_LAUNCH * ne,
+                "traffic_source": "ncu dram bytes of the same launches on a 10^3 mesh, scaled by element count"}
     v = torch.randn(N, dtype=torch.float64, device=f"cuda:{torch.cuda.current_device()}")
     w = torch.empty_like(v)
     torch.cuda.synchronize()
@@ -310,18 +355,20 @@ def kernel_rooflines(s, stream, torch):
     mv_ms = e0.elapsed_time(e1) / reps
     # algorithmic bytes: H once (8 m^2 ne), gathered input and element output (16 m ne), face vector (16 N)
     mv_bytes = 8 * m * m * ne + 16 * (m * ne + N)
-    achieved = mv_bytes / (mv_ms * 1e-3) / 1e9
-    e0.record(stream)
-    for _ in range(2):
-        s.hdgAssembleLinearSystem()
-    e1.record(stream)
-    torch.cuda.synchronize()
-    asm_ms = e0.elapsed_time(e1) / 2
-    return {"roofline": {"kernel": "condensed matvec (elem_matvec_kernel + scatter_kernel)", "bound": "hbm",
-                         "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                         "frac": achieved / peaks["hbm_gbs"], "peak_source": src,
-                         "algorithmic_bytes_per_launch": mv_bytes, "ms_per_launch": mv_ms, "traffic": None},
-            "phase_ms": {"assembly": asm_ms, "matvec": mv_ms}}
+    mv = mv_bytes / (mv_ms * 1e-3) / 1e9
+    phases = {}
+    for k, (ms, cnt, fl) in prof.items():
+        if cnt == 0:
+            continue
+        d = {"ms_per_solve": ms / steps, "regions": cnt}
+        if fl > 0:
+            d["tflops"] = fl / (ms * 1e-3) / 1e12
+        phases[k] = d
+    return {"roofline": roofline,
+            "matvec_roofline": {"kernel": "condensed matvec (elem_matvec_kernel + scatter_kernel)", "bound": "hbm",
+                                "achieved": mv, "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": mv / peaks["hbm_gbs"],
+                                "peak_source": src, "algorithmic_bytes_per_launch": mv_bytes, "ms_per_launch": mv_ms},
+            "phases": phases}
 
 
 def main():

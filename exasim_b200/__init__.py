@@ -71,6 +71,8 @@ def load_library(model: str) -> ctypes.CDLL:
         "exa_dgemm_batched": ([I, I, I, D, P, LL, LL, P, LL, LL, D, P, LL, LL, I, P], I),
         "exa_dinverse_batched": ([P, I, LL, I, P, P], I),
         "exa_dnrm2_cols_fixed": ([P, LL, LL, I, P, P], I),
+        "exa_profile": ([P, I], I),
+        "exa_profile_read": ([P, I, PD, PLL, PD], I),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
@@ -204,6 +206,20 @@ class HDGSolver:
         self._check(self.lib.exa_solve(self.h, P(udg), P(uh), P(udg_out), P(uh_out), ctypes.byref(it),
                                        ctypes.byref(nrm)))
         return it.value, nrm.value
+
+    PHASES = ("volume", "face", "qelim", "inverse", "schur", "precond_build", "matvec", "precond_apply",
+              "orthogonalize", "getq", "residual")
+
+    def profile(self, enable: bool):
+        """Start (resetting the totals) or stop the per-phase device timers."""
+        self._check(self.lib.exa_profile(self.h, 1 if enable else 0))
+
+    def profile_read(self):
+        """{phase: (ms, timed regions, algorithmic GEMM FLOPs)} accumulated since profile(True)."""
+        n = len(self.PHASES)
+        ms, cnt, fl = (ctypes.c_double * n)(), (ctypes.c_longlong * n)(), (ctypes.c_double * n)()
+        self._check(self.lib.exa_profile_read(self.h, n, ms, cnt, fl))
+        return {p: (float(ms[i]), int(cnt[i]), float(fl[i])) for i, p in enumerate(self.PHASES)}
 
     def stats(self):
         s = (ctypes.c_longlong * 4)()

@@ -324,6 +324,8 @@ int exa_ctx_init(ExaCtx& c, const double* app, long long napp, const double* mas
 
 void exa_ctx_free(ExaCtx& c) {
   if (c.device >= 0) cudaSetDevice(c.device);
+  if (c.st) cudaStreamSynchronize(c.st);
+  exa_prof_free(c);
   for (void* p : c.allocs) cudaFree(p);
   c.allocs.clear();
   if (c.pinned) cudaFreeHost(c.pinned);
@@ -563,6 +565,26 @@ int exa_solve(exa_ctx* h, const double* udg_in, const double* uh_in, double* udg
   if (udg_out) EXA_CUDA(cudaMemcpyAsync(udg_out, c.udg, sizeof(double) * nu, cudaMemcpyDeviceToHost, c.st));
   if (uh_out) EXA_CUDA(cudaMemcpyAsync(uh_out, c.uh, sizeof(double) * nh, cudaMemcpyDeviceToHost, c.st));
   EXA_CUDA(cudaStreamSynchronize(c.st));
+  return EXA_OK;
+}
+
+int exa_profile(exa_ctx* h, int enable) {
+  EXA_TRY(guard(h));
+  return exa_prof_enable(h->c, enable);
+}
+
+int exa_profile_read(exa_ctx* h, int nphase, double* ms, long long* count, double* flops) {
+  EXA_TRY(guard(h));
+  if (nphase < 0 || nphase > EXA_NPHASE) {
+    exa_set_error("profile: nphase = %d, at most %d phases", nphase, (int)EXA_NPHASE);
+    return EXA_ERR_ARG;
+  }
+  EXA_TRY(exa_prof_flush(h->c));
+  for (int i = 0; i < nphase; ++i) {
+    if (ms) ms[i] = h->c.prof.ms[i];
+    if (count) count[i] = h->c.prof.count[i];
+    if (flops) flops[i] = h->c.prof.flops[i];
+  }
   return EXA_OK;
 }
 

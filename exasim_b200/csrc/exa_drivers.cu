@@ -9,6 +9,68 @@
 
 #include "exa_solver.cuh"
 
+// ---- phase profile: a pool of event pairs, summed into per-phase totals when read or full
+namespace {
+constexpr int PROF_SLOTS = 2048;
+}
+
+int exa_prof_flush(ExaCtx& c) {
+  ExaProf& p = c.prof;
+  if (p.used == 0) return EXA_OK;
+  EXA_CUDA(cudaStreamSynchronize(c.st));
+  for (int i = 0; i < p.used; ++i) {
+    float ms = 0.0f;
+    EXA_CUDA(cudaEventElapsedTime(&ms, p.ev[2 * i], p.ev[2 * i + 1]));
+    p.ms[p.phase[i]] += ms;
+    p.count[p.phase[i]] += 1;
+  }
+  p.used = 0;
+  return EXA_OK;
+}
+
+int exa_prof_enable(ExaCtx& c, int on) {
+  ExaProf& p = c.prof;
+  if (on) {
+    if (p.ev.empty()) {
+      p.ev.resize(2 * PROF_SLOTS);
+      p.phase.resize(PROF_SLOTS);
+      for (auto& e : p.ev) EXA_CUDA(cudaEventCreate(&e));
+    }
+    EXA_TRY(exa_prof_flush(c));
+    for (int i = 0; i < EXA_NPHASE; ++i) p.ms[i] = 0.0, p.count[i] = 0, p.flops[i] = 0.0;
+    p.on = true;
+  } else {
+    EXA_TRY(exa_prof_flush(c));
+    p.on = false;
+  }
+  return EXA_OK;
+}
+
+void exa_prof_free(ExaCtx& c) {
+  for (auto& e : c.prof.ev) cudaEventDestroy(e);
+  c.prof.ev.clear();
+  c.prof.on = false;
+  c.prof.used = 0;
+}
+
+// Profiling is best effort: a failed event record leaves the slot unused and the solver
+// call unaffected.
+ExaProfScope::ExaProfScope(ExaCtx& ctx, int phase) : c(ctx) {
+  ExaProf& p = c.prof;
+  if (!p.on) return;
+  if (p.used == PROF_SLOTS && exa_prof_flush(c) != EXA_OK) return;
+  if (cudaEventRecord(p.ev[2 * p.used], c.st) != cudaSuccess) return;
+  slot = p.used++;
+  p.phase[slot] = phase;
+}
+
+ExaProfScope::~ExaProfScope() {
+  if (slot >= 0 && cudaEventRecord(c.prof.ev[2 * slot + 1], c.st) != cudaSuccess) {
+    // drop the unfinished slot if it is the last one, otherwise time it to the next record
+    if (slot == c.prof.used - 1) c.prof.used--;
+  }
+}
+
 int exa_drv_norm(ExaCtx& c, const double* x, long long n, double* out) {
   EXA_TRY(exa_dot_partials(x, x, n, c.part_a, c.st));
   EXA_TRY(exa_reduce_partials(c.part_a, c.scal + 15, 1, c.st));
@@ -21,6 +83,7 @@ int exa_drv_norm(ExaCtx& c, const double* x, long long n, double* out) {
 // hdgAssembleRHS + preconditioner setup (discretization.cpp:483-573, matvec.cpp:103-217)
 int exa_drv_build_precond(ExaCtx& c) {
   const ExaDims& P = c.P;
+  ExaProfScope ps(c, EXA_PH_PRECOND_BUILD);
   if (c.preconditioner == 0) {
     EXA_TRY(exa_k_bj_build(P, c.f2e, c.elemcon, c.H, c.Pc, c.st));
     const int ncf = P.ncu * P.npf;
@@ -63,6 +126,7 @@ int exa_drv_residual(ExaCtx& c, double* norm) {
 
 // w = A v (hdgMatVec, matvec.cpp:240-389)
 int exa_drv_matvec(ExaCtx& c, const double* v, double* w) {
+  ExaProfScope ps(c, EXA_PH_MATVEC);
   EXA_TRY(exa_k_elem_matvec(c.P, c.elemcon, c.H, v, c.we, c.st));
   EXA_TRY(exa_k_scatter(c.P, c.f2e, c.elemcon, c.we, w, c.st));
   return EXA_OK;
@@ -70,6 +134,7 @@ int exa_drv_matvec(ExaCtx& c, const double* v, double* w) {
 
 // w = P v (ApplyPreconditioner, preconditioner.cpp:273-295); v and w may not alias
 int exa_drv_precond(ExaCtx& c, const double* v, double* w) {
+  ExaProfScope ps(c, EXA_PH_PRECOND_APPLY);
   if (c.preconditioner == 0) return exa_k_bj_apply(c.P, c.Pc, v, w, c.st);
   EXA_TRY(exa_k_elem_matvec(c.P, c.elemcon, c.Pc, v, c.we, c.st));
   return exa_k_scatter(c.P, c.f2e, c.elemcon, c.we, w, c.st);
@@ -77,6 +142,7 @@ int exa_drv_precond(ExaCtx& c, const double* v, double* w) {
 
 int exa_drv_getq(ExaCtx& c) {
   if (c.P.ncq == 0) return EXA_OK;
+  ExaProfScope ps(c, EXA_PH_GETQ);
   return exa_k_getq(c.P, c.elemcon, c.MC, c.ME, c.uh, c.udg, c.st);
 }
 
@@ -133,6 +199,7 @@ int exa_drv_gmres(ExaCtx& c, int* iters_out, double* relerr_out) {
       double* hcol = c.hess + (long long)n1 * i;
       EXA_TRY(exa_drv_matvec(c, vi, c.w));
       EXA_TRY(exa_drv_precond(c, c.w, vn));
+      ExaProfScope ps_ortho(c, EXA_PH_ORTHO);
       if (c.ortho == 0) {
         EXA_TRY(exa_dot_partials(vn, c.V, N, c.part_a, c.st));
         double* pin = c.part_a;

@@ -44,6 +44,9 @@ int schur_chunk(ExaCtx& c, int e0, int nb) {
   const long long nqn = (long long)npe * nd * ncu;
   double* Hc = c.H + (long long)e0 * m * m;
   if (P.ncq > 0) {
+    ExaProfScope ps(c, EXA_PH_QELIM);
+    // four GEMMs per trace component with K = npe*nd: (n + m) rows x (npe + ndf) columns in all
+    exa_prof_flops(c, EXA_PH_QELIM, 2.0 * nb * ncu * (double)npe * nd * (double)(n + m) * (npe + ndf));
     const double* MC = c.MC + (long long)e0 * npe * npe * nd;
     const double* ME = c.ME + (long long)e0 * npe * ndf * nd;
     // contraction over the stacked (l, d) rows of MinvC / MinvE (K = npe*nd), one GEMM per
@@ -75,7 +78,12 @@ int schur_chunk(ExaCtx& c, int e0, int nb) {
     g.C = Hc; g.ldc = (long long)m * ncu; g.sC = (long long)m * m; g.sC2 = m;
     EXA_TRY(exa_gemm(g, c.st));
   }
-  EXA_TRY(exa_inverse(c.wD, n, (long long)n * n, nb, c.d_flag, c.st));
+  {
+    ExaProfScope ps(c, EXA_PH_INVERSE);
+    EXA_TRY(exa_inverse(c.wD, n, (long long)n * n, nb, c.d_flag, c.st));
+  }
+  ExaProfScope ps(c, EXA_PH_SCHUR);
+  exa_prof_flops(c, EXA_PH_SCHUR, 2.0 * nb * ((double)n * n * m + (double)n * n + (double)m * m * n + (double)m * n));
   GemmBatch g{};
   g.batch = nb; g.batch2 = 1;
   // DinvF = -Dinv F
@@ -128,21 +136,28 @@ int exa_model_assemble(ExaCtx& c, bool jacobian) {
     double* Ruc = c.Ru + (long long)e0 * n;
     double* Rhc = c.Rh + (long long)e0 * m;
     if (jacobian) {
-      vol_points_kernel<ExaModel, true><<<nb, tpb_v, vs, c.st>>>(A, Ruc, c.wRg);
-      EXA_LAUNCH_CHECK();
-      const int tiles = exa_ceil_div(P.npe, 64);
-      dim3 grid(tiles * tiles, nb, P.ncu * P.nc);
-      vol_mat_kernel<<<grid, 256, 0, c.st>>>(P, c.shapegw, c.shapegt, c.wRg, c.wD, c.wB);
-      EXA_LAUNCH_CHECK();
+      {
+        ExaProfScope ps(c, EXA_PH_VOLUME);
+        vol_points_kernel<ExaModel, true><<<nb, tpb_v, vs, c.st>>>(A, Ruc, c.wRg);
+        EXA_LAUNCH_CHECK();
+        const int tiles = exa_ceil_div(P.npe, 64);
+        dim3 grid(tiles * tiles, nb, P.ncu * P.nc);
+        vol_mat_kernel<<<grid, 256, 0, c.st>>>(P, c.shapegw, c.shapegt, c.wRg, c.wD, c.wB);
+        EXA_LAUNCH_CHECK();
+      }
       double* Hc = c.H + (long long)e0 * m * m;
-      EXA_CUDA(cudaMemsetAsync(c.wF, 0, sizeof(double) * (size_t)nb * n * m, c.st));
-      EXA_CUDA(cudaMemsetAsync(c.wK, 0, sizeof(double) * (size_t)nb * m * n, c.st));
-      if (nqn > 0 && P.ncq > 0) EXA_CUDA(cudaMemsetAsync(c.wG, 0, sizeof(double) * (size_t)nb * m * nqn, c.st));
-      EXA_CUDA(cudaMemsetAsync(Hc, 0, sizeof(double) * (size_t)nb * m * m, c.st));
-      face_kernel<ExaModel, true><<<nb, tpb_f, fs, c.st>>>(A, Ruc, Rhc, c.wD, c.wB, c.wF, c.wK, c.wG, Hc);
-      EXA_LAUNCH_CHECK();
+      {
+        ExaProfScope ps(c, EXA_PH_FACE);
+        EXA_CUDA(cudaMemsetAsync(c.wF, 0, sizeof(double) * (size_t)nb * n * m, c.st));
+        EXA_CUDA(cudaMemsetAsync(c.wK, 0, sizeof(double) * (size_t)nb * m * n, c.st));
+        if (nqn > 0 && P.ncq > 0) EXA_CUDA(cudaMemsetAsync(c.wG, 0, sizeof(double) * (size_t)nb * m * nqn, c.st));
+        EXA_CUDA(cudaMemsetAsync(Hc, 0, sizeof(double) * (size_t)nb * m * m, c.st));
+        face_kernel<ExaModel, true><<<nb, tpb_f, fs, c.st>>>(A, Ruc, Rhc, c.wD, c.wB, c.wF, c.wK, c.wG, Hc);
+        EXA_LAUNCH_CHECK();
+      }
       EXA_TRY(schur_chunk(c, e0, nb));
     } else {
+      ExaProfScope ps(c, EXA_PH_RESIDUAL);
       vol_points_kernel<ExaModel, false><<<nb, tpb_v, vs, c.st>>>(A, Ruc, nullptr);
       EXA_LAUNCH_CHECK();
       face_kernel<ExaModel, false><<<nb, tpb_f, fs, c.st>>>(A, Ruc, Rhc, nullptr, nullptr, nullptr, nullptr, nullptr,

@@ -11,6 +11,23 @@
 #include "exa_kernels.cuh"
 #include "exa_conn.h"
 
+// Device time by solver phase (exa_profile / exa_profile_read in the C ABI): CUDA event
+// pairs recorded on the context stream around each phase, summed when read.
+enum ExaPhase {
+  EXA_PH_VOLUME = 0, EXA_PH_FACE, EXA_PH_QELIM, EXA_PH_INVERSE, EXA_PH_SCHUR, EXA_PH_PRECOND_BUILD,
+  EXA_PH_MATVEC, EXA_PH_PRECOND_APPLY, EXA_PH_ORTHO, EXA_PH_GETQ, EXA_PH_RESIDUAL, EXA_NPHASE
+};
+
+struct ExaProf {
+  bool on = false;
+  std::vector<cudaEvent_t> ev;  // two per slot: start, end
+  std::vector<int> phase;       // phase of each slot
+  int used = 0;
+  double ms[EXA_NPHASE] = {};
+  long long count[EXA_NPHASE] = {};
+  double flops[EXA_NPHASE] = {};
+};
+
 struct ExaCtx {
   ExaDims P{};
   int device = 0;
@@ -47,6 +64,7 @@ struct ExaCtx {
   int last_gmres_iters = 0, last_newton_iters = 0, total_gmres_iters = 0;
   double last_gmres_relerr = 0.0;
   long long kernel_launches = 0;
+  ExaProf prof;
 
   long long ndofuhat() const { return (long long)P.ncu * P.npf * P.nf; }
 };
@@ -72,3 +90,18 @@ int exa_drv_newton(ExaCtx& c, int* iters, double* norm);
 int exa_drv_dirk(ExaCtx& c, int nsteps, int* newton_iters_out, int max_out);
 int exa_drv_dirk_stage(ExaCtx& c, int istep, int stage, int* its_out, double* norm_out);
 int exa_drv_norm(ExaCtx& c, const double* x, long long n, double* out);
+
+// phase profile (exa_drivers.cu)
+int exa_prof_enable(ExaCtx& c, int on);
+int exa_prof_flush(ExaCtx& c);
+void exa_prof_free(ExaCtx& c);
+inline void exa_prof_flops(ExaCtx& c, int phase, double f) {
+  if (c.prof.on) c.prof.flops[phase] += f;
+}
+// Records the start event on construction and the end event on destruction.
+struct ExaProfScope {
+  ExaCtx& c;
+  int slot = -1;
+  ExaProfScope(ExaCtx& ctx, int phase);
+  ~ExaProfScope();
+};

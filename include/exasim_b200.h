@@ -88,6 +88,17 @@ int exa_solve(exa_ctx* ctx, const double* udg_in, const double* uh_in, double* u
  * elemcon (npf*nfe*ne ints) receive the result.  Returns nf (>= 0) or a negated status. */
 int exa_connectivity_host(const int* t, const int* bf, const int* perm, const double* xpf, int dim,
                           int elemtype, int ne, int npe, int npf, int* f2e, int* elemcon, int* nf0);
+/* Device time by solver phase, from CUDA events recorded on the context stream around each
+ * phase (the reference prints its own phase timers instead, e.g. Solver/ptcsolver.cpp:361).
+ * exa_profile(ctx, 1) resets the totals and starts recording; exa_profile(ctx, 0) stops.
+ * Phases: 0 volume assembly, 1 face assembly, 2 q-elimination GEMMs, 3 element inverse,
+ * 4 Schur GEMMs, 5 preconditioner build, 6 matvec, 7 preconditioner apply,
+ * 8 Gram-Schmidt + Givens, 9 q recovery, 10 residual-only assembly.
+ * exa_profile_read fills ms, count (timed regions) and flops (algorithmic FLOPs of the GEMM
+ * phases 2 and 4, 0 elsewhere) for the first nphase (<= 11) phases; any may be NULL.  It
+ * synchronises the context stream. */
+int exa_profile(exa_ctx* ctx, int enable);
+int exa_profile_read(exa_ctx* ctx, int nphase, double* ms, long long* count, double* flops);
 /* out[4] = {last GMRES iterations, last Newton iterations, GMRES iterations of the last solve, 0} */
 int exa_stats(exa_ctx* ctx, long long* out);
 int exa_synchronize(exa_ctx* ctx);
