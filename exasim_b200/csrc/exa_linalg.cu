@@ -30,105 +30,8 @@ void exa_set_error(const char* fmt, ...) {
 }
 const char* exa_get_error() { return g_err; }
 
-// ----------------------------------------------------------------------------------
-// batched GEMM.  256 threads in a 16 x 16 grid; each thread accumulates a TM x TN
-// register block (rows ty + 16*a, cols tx + 16*b), so a block tile is (16 TM) x (16 TN)
-// and every k step costs TM + TN shared-memory reads for TM*TN FMAs.  The tile shape
-// is picked per call to fit the element blocks (125 -> 128, 150 -> 160) with little
-// padding.  K advances in chunks of 8 through double-buffered shared memory.
-// ----------------------------------------------------------------------------------
 namespace {
-constexpr int GK = 8;
-
-template <int TM, int TN>
-__global__ void __launch_bounds__(256, 1) gemm_kernel(GemmBatch g) {
-  constexpr int BM = 16 * TM, BN = 16 * TN;
-  __shared__ double As[2][GK][BM];
-  __shared__ double Bs[2][GK][BN + 1];
-  const int tilesM = (g.M + BM - 1) / BM;
-  const int tm = blockIdx.x % tilesM, tn = blockIdx.x / tilesM;
-  const long long b1 = blockIdx.y, b2 = blockIdx.z;
-  const double* A = g.A + b1 * g.sA + b2 * g.sA2;
-  const double* B = g.B + b1 * g.sB + b2 * g.sB2;
-  double* C = g.C + b1 * g.sC + b2 * g.sC2;
-  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
-  const int r0 = tm * BM, c0 = tn * BN;
-  double acc[TM][TN];
-#pragma unroll
-  for (int a = 0; a < TM; ++a)
-#pragma unroll
-    for (int b = 0; b < TN; ++b) acc[a][b] = 0.0;
-  const int nk = (g.K + GK - 1) / GK;
-  // register staging of the next chunk
-  double ra[(BM * GK + 255) / 256], rb[(BN * GK + 255) / 256];
-  auto load = [&](int kc) {
-    const int k0 = kc * GK;
-#pragma unroll
-    for (int q = 0; q < (BM * GK + 255) / 256; ++q) {
-      const int t = tid + 256 * q;
-      const int r = t % BM, k = t / BM;
-      const int gr = r0 + r, gk = k0 + k;
-      ra[q] = (k < GK && gr < g.M && gk < g.K) ? A[gr + g.lda * gk] : 0.0;
-    }
-#pragma unroll
-    for (int q = 0; q < (BN * GK + 255) / 256; ++q) {
-      const int t = tid + 256 * q;
-      const int k = t % GK, c = t / GK;
-      const int gk = k0 + k, gc = c0 + c;
-      rb[q] = (c < BN && gk < g.K && gc < g.N) ? B[gk + g.ldb * gc] : 0.0;
-    }
-  };
-  auto store = [&](int buf) {
-#pragma unroll
-    for (int q = 0; q < (BM * GK + 255) / 256; ++q) {
-      const int t = tid + 256 * q;
-      const int r = t % BM, k = t / BM;
-      if (k < GK) As[buf][k][r] = ra[q];
-    }
-#pragma unroll
-    for (int q = 0; q < (BN * GK + 255) / 256; ++q) {
-      const int t = tid + 256 * q;
-      const int k = t % GK, c = t / GK;
-      if (c < BN) Bs[buf][k][c] = rb[q];
-    }
-  };
-  load(0);
-  store(0);
-  __syncthreads();
-  for (int kc = 0; kc < nk; ++kc) {
-    const int buf = kc & 1;
-    if (kc + 1 < nk) load(kc + 1);
-#pragma unroll
-    for (int k = 0; k < GK; ++k) {
-      double av[TM], bv[TN];
-#pragma unroll
-      for (int a = 0; a < TM; ++a) av[a] = As[buf][k][ty + 16 * a];
-#pragma unroll
-      for (int b = 0; b < TN; ++b) bv[b] = Bs[buf][k][tx + 16 * b];
-#pragma unroll
-      for (int a = 0; a < TM; ++a)
-#pragma unroll
-        for (int b = 0; b < TN; ++b) acc[a][b] = fma(av[a], bv[b], acc[a][b]);
-    }
-    if (kc + 1 < nk) store(buf ^ 1);
-    __syncthreads();
-  }
-#pragma unroll
-  for (int a = 0; a < TM; ++a) {
-    const int gr = r0 + ty + 16 * a;
-    if (gr >= g.M) continue;
-#pragma unroll
-    for (int b = 0; b < TN; ++b) {
-      const int gc = c0 + tx + 16 * b;
-      if (gc >= g.N) continue;
-      double* p = C + gr + g.ldc * gc;
-      const double v = g.alpha * acc[a][b];
-      *p = (g.beta == 0.0) ? v : v + g.beta * (*p);
-    }
-  }
-}
-
-// C = alpha A x + beta C for N = 1: one warp per output row block
+// C = alpha A x + beta C for N = 1: one thread per output row
 __global__ void gemv_batch_kernel(GemmBatch g) {
   const long long b1 = blockIdx.y, b2 = blockIdx.z;
   const double* A = g.A + b1 * g.sA + b2 * g.sA2;
@@ -145,13 +48,23 @@ __global__ void gemv_batch_kernel(GemmBatch g) {
 // ----------------------------------------------------------------------------------
 // FP64 tensor-core (DMMA, mma.sync m8n8k4 f64) batched GEMM.  A warp owns a
 // (8 TI) x (8 TJ) block of C held as TI*TJ 8x8 accumulator fragments; the CTA is a
-// WM x WN grid of warps.  A and B tiles go through double-buffered shared memory in
-// chunks of 8 along K, stored k-major with a row stride of 4 (mod 16) doubles so the
-// fragment loads of a half-warp hit distinct banks.
+// WM x WN grid of warps, one CTA tile of one batch entry per block.  A and B stream
+// through a GST-stage ring of shared-memory buffers, GK deep along K, filled with
+// cp.async (8-byte copies, zero-filled outside the matrix) so no registers stage the
+// loads and up to GST-1 chunks are in flight while one is multiplied.  Tiles are stored
+// k-major with a row stride of 4 (mod 16) doubles: the fragment loads of each half-warp
+// and the cp.async writes of four consecutive k by four columns hit distinct banks.
 // Fragment layout (PTX ISA, m8n8k4 .f64): a0 = A[lane/4][lane%4], b0 = B[lane%4][lane/4],
 // c0/c1 = C[lane/4][2 (lane%4) + 0/1].
 // ----------------------------------------------------------------------------------
-constexpr int DK = 8;
+constexpr int GK = 16, GST = 3;
+
+__host__ __device__ constexpr int dmma_stride(int w) { return (w + 15) / 16 * 16 + 4; }
+
+template <int TI, int TJ, int WM, int WN>
+constexpr size_t dmma_smem() {
+  return sizeof(double) * (size_t)GST * GK * (dmma_stride(8 * TI * WM) + dmma_stride(8 * TJ * WN));
+}
 
 __device__ __forceinline__ void dmma(double& c0, double& c1, double a, double b) {
   asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
@@ -159,12 +72,23 @@ __device__ __forceinline__ void dmma(double& c0, double& c1, double a, double b)
                : "d"(a), "d"(b));
 }
 
+// 8-byte asynchronous copy global -> shared; src_bytes = 0 writes zeros and reads nothing
+__device__ __forceinline__ void cp_async8(double* dst, const double* src, int src_bytes) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(src), "r"(src_bytes));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
 template <int TI, int TJ, int WM, int WN>
-__global__ void __launch_bounds__(32 * WM * WN) dmma_gemm_kernel(GemmBatch g) {
+__global__ void __launch_bounds__(32 * WM * WN, 2) dmma_gemm_kernel(GemmBatch g) {
   constexpr int BM = 8 * TI * WM, BN = 8 * TJ * WN, NT = 32 * WM * WN;
-  constexpr int SA = BM + 4 + ((16 - (BM + 4) % 16) + 4) % 16, SB = BN + 4 + ((16 - (BN + 4) % 16) + 4) % 16;
-  __shared__ double As[2][DK][SA];
-  __shared__ double Bs[2][DK][SB];
+  constexpr int SA = dmma_stride(BM), SB = dmma_stride(BN);
+  constexpr int LA = (BM * GK + NT - 1) / NT, LB = (BN * GK + NT - 1) / NT;
+  extern __shared__ __align__(16) double dsm[];
+  double* As = dsm;                    // [GST][GK][SA]
+  double* Bs = dsm + GST * GK * SA;    // [GST][GK][SB]
   const int tilesM = (g.M + BM - 1) / BM;
   const int tm = blockIdx.x % tilesM, tn = blockIdx.x / tilesM;
   const long long b1 = blockIdx.y, b2 = blockIdx.z;
@@ -180,62 +104,62 @@ __global__ void __launch_bounds__(32 * WM * WN) dmma_gemm_kernel(GemmBatch g) {
   for (int i = 0; i < TI; ++i)
 #pragma unroll
     for (int j = 0; j < TJ; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
-  constexpr int LA = (BM * DK + NT - 1) / NT, LB = (BN * DK + NT - 1) / NT;
-  double ra[LA], rb[LB];
-  const int nk = (g.K + DK - 1) / DK;
-  auto load = [&](int kc) {
-    const int k0 = kc * DK;
+  const int nk = (g.K + GK - 1) / GK;
+  // stage s <- K chunk kc.  A: consecutive threads take consecutive rows (contiguous in
+  // global and in shared memory).  B: groups of four threads take four consecutive k of
+  // one column (one 32-byte sector), the next group the next column.
+  auto load = [&](int s, int kc) {
+    const int k0 = kc * GK;
+    double* as = As + s * GK * SA;
+    double* bs = Bs + s * GK * SB;
 #pragma unroll
     for (int q = 0; q < LA; ++q) {
       const int t = tid + NT * q;
       const int r = t % BM, k = t / BM;
-      const int gr = r0 + r, gk = k0 + k;
-      ra[q] = (k < DK && gr < g.M && gk < g.K) ? A[gr + g.lda * gk] : 0.0;
+      if (k < GK) {
+        const int gr = r0 + r, gk = k0 + k;
+        const bool in = gr < g.M && gk < g.K;
+        cp_async8(as + k * SA + r, in ? A + gr + g.lda * gk : A, in ? 8 : 0);
+      }
     }
 #pragma unroll
     for (int q = 0; q < LB; ++q) {
       const int t = tid + NT * q;
-      const int k = t % DK, c = t / DK;
-      const int gk = k0 + k, gc = c0 + c;
-      rb[q] = (c < BN && gk < g.K && gc < g.N) ? B[gk + g.ldb * gc] : 0.0;
+      const int rest = t >> 2, c = rest % BN, k = (t & 3) + 4 * (rest / BN);
+      if (k < GK) {
+        const int gk = k0 + k, gc = c0 + c;
+        const bool in = gk < g.K && gc < g.N;
+        cp_async8(bs + k * SB + c, in ? B + gk + g.ldb * gc : B, in ? 8 : 0);
+      }
     }
   };
-  auto store = [&](int buf) {
 #pragma unroll
-    for (int q = 0; q < LA; ++q) {
-      const int t = tid + NT * q;
-      const int r = t % BM, k = t / BM;
-      if (k < DK) As[buf][k][r] = ra[q];
-    }
-#pragma unroll
-    for (int q = 0; q < LB; ++q) {
-      const int t = tid + NT * q;
-      const int k = t % DK, c = t / DK;
-      if (c < BN) Bs[buf][k][c] = rb[q];
-    }
-  };
-  load(0);
-  store(0);
-  __syncthreads();
+  for (int s = 0; s < GST - 1; ++s) {
+    if (s < nk) load(s, s);
+    cp_async_commit();
+  }
   const int wr = wm * 8 * TI, wc = wn * 8 * TJ;
   for (int kc = 0; kc < nk; ++kc) {
-    const int buf = kc & 1;
-    if (kc + 1 < nk) load(kc + 1);
+    cp_async_wait<GST - 2>();
+    __syncthreads();  // chunk kc visible to all; the buffer of chunk kc-1 is free
+    if (kc + GST - 1 < nk) load((kc + GST - 1) % GST, kc + GST - 1);
+    cp_async_commit();
+    const double* as = As + (kc % GST) * GK * SA;
+    const double* bs = Bs + (kc % GST) * GK * SB;
 #pragma unroll
-    for (int k4 = 0; k4 < DK; k4 += 4) {
+    for (int k4 = 0; k4 < GK; k4 += 4) {
       double af[TI], bf[TJ];
 #pragma unroll
-      for (int i = 0; i < TI; ++i) af[i] = As[buf][k4 + tq][wr + 8 * i + gq];
+      for (int i = 0; i < TI; ++i) af[i] = as[(k4 + tq) * SA + wr + 8 * i + gq];
 #pragma unroll
-      for (int j = 0; j < TJ; ++j) bf[j] = Bs[buf][k4 + tq][wc + 8 * j + gq];
+      for (int j = 0; j < TJ; ++j) bf[j] = bs[(k4 + tq) * SB + wc + 8 * j + gq];
 #pragma unroll
       for (int i = 0; i < TI; ++i)
 #pragma unroll
         for (int j = 0; j < TJ; ++j) dmma(acc[i][j][0], acc[i][j][1], af[i], bf[j]);
     }
-    if (kc + 1 < nk) store(buf ^ 1);
-    __syncthreads();
   }
+  cp_async_wait<0>();
 #pragma unroll
   for (int i = 0; i < TI; ++i) {
     const int gr = r0 + wr + 8 * i + gq;
@@ -256,23 +180,18 @@ __global__ void __launch_bounds__(32 * WM * WN) dmma_gemm_kernel(GemmBatch g) {
 template <int TI, int TJ, int WM, int WN>
 int launch_dmma(const GemmBatch& g, cudaStream_t st) {
   constexpr int BM = 8 * TI * WM, BN = 8 * TJ * WN;
+  constexpr size_t smem = dmma_smem<TI, TJ, WM, WN>();
+  static_assert(smem <= 227 * 1024, "GEMM tile exceeds shared memory");
+  auto kern = dmma_gemm_kernel<TI, TJ, WM, WN>;
+  EXA_CUDA(cudaFuncSetAttribute((const void*)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   dim3 grid((unsigned)(exa_ceil_div(g.M, BM) * exa_ceil_div(g.N, BN)), (unsigned)g.batch, (unsigned)g.batch2);
-  dmma_gemm_kernel<TI, TJ, WM, WN><<<grid, 32 * WM * WN, 0, st>>>(g);
+  kern<<<grid, 32 * WM * WN, smem, st>>>(g);
   EXA_LAUNCH_CHECK();
   return EXA_OK;
 }
 
-int tiles_cost(int M, int N, int bm, int bn) {
-  return ((M + bm - 1) / bm) * bm * ((N + bn - 1) / bn) * bn;
-}
-
-template <int TM, int TN>
-int launch_gemm(const GemmBatch& g, cudaStream_t st) {
-  constexpr int BM = 16 * TM, BN = 16 * TN;
-  dim3 grid((unsigned)(exa_ceil_div(g.M, BM) * exa_ceil_div(g.N, BN)), (unsigned)g.batch, (unsigned)g.batch2);
-  gemm_kernel<TM, TN><<<grid, 256, 0, st>>>(g);
-  EXA_LAUNCH_CHECK();
-  return EXA_OK;
+long long tiles_cost(int M, int N, int bm, int bn) {
+  return (long long)((M + bm - 1) / bm) * bm * ((N + bn - 1) / bn) * bn;
 }
 }  // namespace
 
@@ -300,21 +219,20 @@ int exa_gemm(const GemmBatch& g, cudaStream_t st) {
     EXA_LAUNCH_CHECK();
     return EXA_OK;
   }
-  // tensor-core tiles sized to the element blocks: warp tiles of 32 or 40 rows/columns
-  // cover 125 -> 128 and 150 -> 160 with little padding; tiny blocks use 32 x 32 CTAs
+  // CTA tiles sized to the element blocks: 128 x 64, 128 x 80 and 160 x 32 cover
+  // 125 -> 128 and 150 -> 160 with little padding; tiny blocks use 32 x 32 CTAs
   if (g.M <= 40 && g.N <= 40) return launch_dmma<2, 2, 2, 2>(g, st);
-  const int cand[4][2] = {{4, 4}, {4, 5}, {5, 4}, {5, 5}};
+  const int cand[3][2] = {{128, 64}, {128, 80}, {160, 32}};
   int best = 0;
   long long bc = -1;
-  for (int i = 0; i < 4; ++i) {
-    const long long c = tiles_cost(g.M, g.N, 8 * cand[i][0] * 4, 8 * cand[i][1] * 2);
+  for (int i = 0; i < 3; ++i) {
+    const long long c = tiles_cost(g.M, g.N, cand[i][0], cand[i][1]);
     if (bc < 0 || c < bc) { bc = c; best = i; }
   }
   switch (best) {
     case 0: return launch_dmma<4, 4, 4, 2>(g, st);
     case 1: return launch_dmma<4, 5, 4, 2>(g, st);
-    case 2: return launch_dmma<5, 4, 4, 2>(g, st);
-    default: return launch_dmma<5, 5, 4, 2>(g, st);
+    default: return launch_dmma<5, 2, 4, 2>(g, st);
   }
 }
 
