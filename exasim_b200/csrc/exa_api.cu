@@ -6,6 +6,7 @@
 #include <vector>
 
 #include "exa_solver.cuh"
+#include "exa_umma.cuh"
 #include "../../include/exasim_b200.h"
 
 namespace {
@@ -630,6 +631,20 @@ extern "C" int exa_dgemm_batched(int M, int N, int K, double alpha, const double
   g.C = C; g.ldc = ldc; g.sC = sC; g.sC2 = 0;
   g.batch = batch; g.batch2 = 1;
   return exa_gemm(g, (cudaStream_t)stream);
+}
+
+extern "C" int exa_gemm_tf32_batched(int M, int N, int K, double alpha, const void* A, int a_f64, long long lda,
+                                     long long sA, const void* B, int b_f64, long long ldb, long long sB,
+                                     double beta, void* C, int c_f64, long long ldc, long long sC, int batch,
+                                     int* flag_dev, void* stream) {
+  UGemm g{};
+  g.M = M; g.N = N; g.K = K; g.alpha = alpha; g.beta = beta;
+  g.A = A; g.ta = a_f64 ? EXA_T_F64 : EXA_T_F32; g.lda = lda; g.sA = sA; g.sA2 = 0;
+  g.B = B; g.tb = b_f64 ? EXA_T_F64 : EXA_T_F32; g.ldb = ldb; g.sB = sB; g.sB2 = 0;
+  g.Cin = C; g.tci = c_f64 ? EXA_T_F64 : EXA_T_F32; g.ldci = ldc; g.sCi = sC; g.sCi2 = 0;
+  g.C = C; g.tco = g.tci; g.ldc = ldc; g.sC = sC; g.sC2 = 0;
+  g.batch = batch; g.batch2 = 1;
+  return exa_gemm_tf32(g, flag_dev, (cudaStream_t)stream);
 }
 
 extern "C" int exa_dinverse_batched(double* A, int n, long long stride, int batch, int* info_dev, void* stream) {

@@ -111,6 +111,14 @@ int exa_dgemm_batched(int M, int N, int K, double alpha, const double* A, long l
                       const double* B, long long ldb, long long sB, double beta, double* C, long long ldc,
                       long long sC, int batch, void* stream);
 int exa_dinverse_batched(double* A, int n, long long stride, int batch, int* info_dev, void* stream);
+/* C_b = alpha A_b B_b + beta C_b on the TF32 tensor cores (tcgen05) with FP32 accumulation,
+ * the product the mixed-precision form uses for PGEMNMStridedBached (pblas.h:695).  Each of
+ * A, B and C is FP32 or FP64 (a_f64, b_f64, c_f64); the instantiated combinations are all
+ * FP32, and FP64 A with FP32 B and C.  N <= 256.  *flag_dev is set to 2 if a wait inside the
+ * kernel ran out (the result is then not valid). */
+int exa_gemm_tf32_batched(int M, int N, int K, double alpha, const void* A, int a_f64, long long lda, long long sA,
+                          const void* B, int b_f64, long long ldb, long long sB, double beta, void* C, int c_f64,
+                          long long ldc, long long sC, int batch, int* flag_dev, void* stream);
 /* Number of CUDA kernels this library has launched since it was loaded (all contexts). */
 long long exa_launch_count(void);
 /* Euclidean norms of `ncols` device columns of length n, column j at X + j*ldx, written to
