@@ -73,6 +73,8 @@ def load_library(model: str) -> ctypes.CDLL:
         "exa_dnrm2_cols_fixed": ([P, LL, LL, I, P, P], I),
         "exa_gemm_tf32_batched": ([I, I, I, D, P, I, LL, LL, P, I, LL, LL, D, P, I, LL, LL, I, P, P], I),
         "exa_profile": ([P, I], I),
+        "exa_set_precision": ([P, I, D, D], I),
+        "exa_last_residual": ([P, PD, PD], I),
         "exa_profile_read": ([P, I, PD, PLL, PD], I),
     }
     for name, (args, res) in sig.items():
@@ -207,6 +209,16 @@ class HDGSolver:
         self._check(self.lib.exa_solve(self.h, P(udg), P(uh), P(udg_out), P(uh_out), ctypes.byref(it),
                                        ctypes.byref(nrm)))
         return it.value, nrm.value
+
+    def set_precision(self, mode: int, inner_tol: float = 1e-4, rtol: float = 0.0):
+        """0: plain FP64.  1: FP32/TF32 element elimination with FP64 residual refinement."""
+        self._check(self.lib.exa_set_precision(self.h, int(mode), float(inner_tol), float(rtol)))
+
+    def last_residual(self):
+        """(initial, final) residual norm |b| + |Ru| of the last Newton solve."""
+        a, b = ctypes.c_double(), ctypes.c_double()
+        self._check(self.lib.exa_last_residual(self.h, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
 
     PHASES = ("volume", "face", "qelim", "inverse", "schur", "precond_build", "matvec", "precond_apply",
               "orthogonalize", "getq", "residual")

@@ -323,6 +323,38 @@ int exa_ctx_init(ExaCtx& c, const double* app, long long napp, const double* mas
   return EXA_OK;
 }
 
+// Switch between the plain FP64 form (0) and the mixed-precision form (1).  The FP32
+// arrays of the mixed form are allocated on the first switch to it and kept afterwards.
+int exa_ctx_set_precision(ExaCtx& c, int mode) {
+  if (mode != 0 && mode != 1) {
+    exa_set_error("precision mode %d: 0 (FP64) or 1 (FP32/TF32 elimination with FP64 refinement)", mode);
+    return EXA_ERR_ARG;
+  }
+  if (mode == 1 && c.H32 == nullptr) {
+    const ExaDims& P = c.P;
+    const size_t ne = P.ne, n = P.n, m = P.m, nb = c.neb;
+    if (P.ncq > 0) {
+      EXA_TRY(dev_alloc(c, &c.MC32, ne * P.npe * P.npe * P.nd));
+      EXA_TRY(dev_alloc(c, &c.ME32, ne * P.npe * P.ndf * P.nd));
+      EXA_TRY(exa_k_to_f32(c.MC, c.MC32, (long long)(ne * P.npe * P.npe * P.nd), c.st));
+      EXA_TRY(exa_k_to_f32(c.ME, c.ME32, (long long)(ne * P.npe * P.ndf * P.nd), c.st));
+    }
+    EXA_TRY(dev_alloc(c, &c.H32, ne * m * m));
+    EXA_TRY(dev_alloc(c, &c.F32, ne * n * m));
+    EXA_TRY(dev_alloc(c, &c.K32, ne * m * n));
+    EXA_TRY(dev_alloc(c, &c.Dinv32, ne * n * n));
+    EXA_TRY(dev_alloc(c, &c.wF32, nb * n * m));
+    if (c.preconditioner == 0)
+      EXA_TRY(dev_alloc(c, &c.Pc32, (size_t)P.ncu * P.npf * P.ncu * P.npf * P.nf));
+    else
+      EXA_TRY(dev_alloc(c, &c.Pc32, ne * m * m));
+    c.d_uflag = c.d_flag + 1;
+    EXA_CUDA(cudaStreamSynchronize(c.st));
+  }
+  c.precision = mode;
+  return EXA_OK;
+}
+
 void exa_ctx_free(ExaCtx& c) {
   if (c.device >= 0) cudaSetDevice(c.device);
   if (c.st) cudaStreamSynchronize(c.st);
@@ -347,6 +379,7 @@ namespace {
 struct FieldRef {
   double* p;
   long long n;
+  float* p32 = nullptr;  // FP32 arrays of the mixed-precision form (p is null then)
 };
 
 bool field(ExaCtx& c, const char* name, FieldRef& f) {
@@ -367,6 +400,10 @@ bool field(ExaCtx& c, const char* name, FieldRef& f) {
   else if (s == "MinvE") f = {c.ME, P.ncq > 0 ? (long long)P.npe * P.ndf * P.nd * ne : 0};
   else if (s == "elemg") f = {c.elemg, (long long)P.elemg_stride() * ne};
   else if (s == "faceg") f = {c.faceg, (long long)P.faceg_stride() * P.nfe * ne};
+  else if (s == "H32" && c.H32) f = {nullptr, m * m * ne, c.H32};
+  else if (s == "F32" && c.F32) f = {nullptr, n * m * ne, c.F32};
+  else if (s == "K32" && c.K32) f = {nullptr, m * n * ne, c.K32};
+  else if (s == "Dinv32" && c.Dinv32) f = {nullptr, n * n * ne, c.Dinv32};
   else return false;
   return true;
 }
@@ -431,7 +468,13 @@ int exa_get_field(exa_ctx* h, const char* name, double* host, long long n) {
     return EXA_ERR_ARG;
   }
   EXA_CUDA(cudaStreamSynchronize(h->c.st));
-  if (n) EXA_CUDA(cudaMemcpy(host, f.p, sizeof(double) * n, cudaMemcpyDeviceToHost));
+  if (n && f.p32) {
+    std::vector<float> t((size_t)n);
+    EXA_CUDA(cudaMemcpy(t.data(), f.p32, sizeof(float) * n, cudaMemcpyDeviceToHost));
+    for (long long i = 0; i < n; ++i) host[i] = t[(size_t)i];
+  } else if (n) {
+    EXA_CUDA(cudaMemcpy(host, f.p, sizeof(double) * n, cudaMemcpyDeviceToHost));
+  }
   return EXA_OK;
 }
 
@@ -443,7 +486,12 @@ int exa_set_field(exa_ctx* h, const char* name, const double* host, long long n)
     return EXA_ERR_ARG;
   }
   EXA_CUDA(cudaStreamSynchronize(h->c.st));
-  if (n) EXA_CUDA(cudaMemcpy(f.p, host, sizeof(double) * n, cudaMemcpyHostToDevice));
+  if (n && f.p32) {
+    std::vector<float> t(host, host + n);
+    EXA_CUDA(cudaMemcpy(f.p32, t.data(), sizeof(float) * n, cudaMemcpyHostToDevice));
+  } else if (n) {
+    EXA_CUDA(cudaMemcpy(f.p, host, sizeof(double) * n, cudaMemcpyHostToDevice));
+  }
   return EXA_OK;
 }
 
@@ -454,7 +502,7 @@ int exa_field_ptr(exa_ctx* h, const char* name, double** dev, long long* n) {
     exa_set_error("field_ptr('%s'): unknown name", name ? name : "");
     return EXA_ERR_ARG;
   }
-  *dev = f.p;
+  *dev = f.p32 ? reinterpret_cast<double*>(f.p32) : f.p;
   *n = f.n;
   return EXA_OK;
 }
@@ -566,6 +614,25 @@ int exa_solve(exa_ctx* h, const double* udg_in, const double* uh_in, double* udg
   if (udg_out) EXA_CUDA(cudaMemcpyAsync(udg_out, c.udg, sizeof(double) * nu, cudaMemcpyDeviceToHost, c.st));
   if (uh_out) EXA_CUDA(cudaMemcpyAsync(uh_out, c.uh, sizeof(double) * nh, cudaMemcpyDeviceToHost, c.st));
   EXA_CUDA(cudaStreamSynchronize(c.st));
+  return EXA_OK;
+}
+
+int exa_set_precision(exa_ctx* h, int mode, double inner_tol, double rtol) {
+  EXA_TRY(guard(h));
+  if (!(inner_tol > 0.0 && inner_tol < 1.0) || !(rtol >= 0.0 && rtol < 1.0)) {
+    exa_set_error("set_precision: inner_tol must lie in (0, 1) and rtol in [0, 1)");
+    return EXA_ERR_ARG;
+  }
+  EXA_TRY(exa_ctx_set_precision(h->c, mode));
+  h->c.mixed_inner_tol = inner_tol;
+  h->c.mixed_rtol = rtol;
+  return EXA_OK;
+}
+
+int exa_last_residual(exa_ctx* h, double* initial, double* final_norm) {
+  EXA_TRY(guard(h));
+  if (initial) *initial = h->c.last_norm0;
+  if (final_norm) *final_norm = h->c.last_norm;
   return EXA_OK;
 }
 

@@ -79,6 +79,7 @@ int exa_gemm(const GemmBatch& g, cudaStream_t st);
 // doubles apart (Gauss-Jordan with partial pivoting in shared memory).  Sets
 // *d_flag (device int) non-zero when a pivot is exactly zero.
 int exa_inverse(double* A, int n, long long stride, int batch, int* d_flag, cudaStream_t st);
+int exa_inverse(float* A, int n, long long stride, int batch, int* d_flag, cudaStream_t st);
 
 // Vector kernels for the Krylov solver.  Reductions are deterministic: each block
 // writes a partial sum and consumers reduce the partial array in a fixed order.

@@ -84,6 +84,18 @@ int exa_drv_norm(ExaCtx& c, const double* x, long long n, double* out) {
 int exa_drv_build_precond(ExaCtx& c) {
   const ExaDims& P = c.P;
   ExaProfScope ps(c, EXA_PH_PRECOND_BUILD);
+  if (c.precision == 1) {
+    // mixed form: blocks from the FP32 condensed matrix, inverted in FP32
+    if (c.preconditioner == 0) {
+      const int ncf = P.ncu * P.npf;
+      EXA_TRY(exa_k_bj_build(P, c.f2e, c.elemcon, c.H32, c.Pc32, c.st));
+      EXA_TRY(exa_inverse(c.Pc32, ncf, (long long)ncf * ncf, P.nf, c.d_flag, c.st));
+    } else {
+      EXA_TRY(exa_k_eas_build(P, c.f2e, c.elemcon, c.H32, c.Pc32, c.st));
+      EXA_TRY(exa_inverse(c.Pc32, P.m, (long long)P.m * P.m, P.ne, c.d_flag, c.st));
+    }
+    return EXA_OK;
+  }
   if (c.preconditioner == 0) {
     EXA_TRY(exa_k_bj_build(P, c.f2e, c.elemcon, c.H, c.Pc, c.st));
     const int ncf = P.ncu * P.npf;
@@ -96,15 +108,20 @@ int exa_drv_build_precond(ExaCtx& c) {
 }
 
 int exa_drv_assemble(ExaCtx& c) {
-  EXA_CUDA(cudaMemsetAsync(c.d_flag, 0, sizeof(int), c.st));
+  // d_flag[0]: zero pivot in an inverse; d_flag[1]: a tensor-core kernel's wait ran out
+  EXA_CUDA(cudaMemsetAsync(c.d_flag, 0, 2 * sizeof(int), c.st));
   EXA_TRY(exa_model_assemble(c, true));
   EXA_TRY(exa_k_scatter(c.P, c.f2e, c.elemcon, c.Rh, c.b, c.st));
   EXA_TRY(exa_drv_build_precond(c));
-  int flag = 0;
-  EXA_CUDA(cudaMemcpyAsync(c.pinned, c.d_flag, sizeof(int), cudaMemcpyDeviceToHost, c.st));
+  int flag[2] = {0, 0};
+  EXA_CUDA(cudaMemcpyAsync(c.pinned, c.d_flag, 2 * sizeof(int), cudaMemcpyDeviceToHost, c.st));
   EXA_CUDA(cudaStreamSynchronize(c.st));
-  std::memcpy(&flag, c.pinned, sizeof(int));
-  if (flag) {
+  std::memcpy(flag, c.pinned, 2 * sizeof(int));
+  if (flag[1]) {
+    exa_set_error("tensor-core element elimination: a wait inside the kernel ran out");
+    return EXA_ERR_CUDA;
+  }
+  if (flag[0]) {
     exa_set_error("singular element or preconditioner block during assembly");
     return EXA_ERR_SINGULAR;
   }
@@ -127,7 +144,10 @@ int exa_drv_residual(ExaCtx& c, double* norm) {
 // w = A v (hdgMatVec, matvec.cpp:240-389)
 int exa_drv_matvec(ExaCtx& c, const double* v, double* w) {
   ExaProfScope ps(c, EXA_PH_MATVEC);
-  EXA_TRY(exa_k_elem_matvec(c.P, c.elemcon, c.H, v, c.we, c.st));
+  if (c.precision == 1)
+    EXA_TRY(exa_k_elem_matvec(c.P, c.elemcon, c.H32, v, c.we, c.st));
+  else
+    EXA_TRY(exa_k_elem_matvec(c.P, c.elemcon, c.H, v, c.we, c.st));
   EXA_TRY(exa_k_scatter(c.P, c.f2e, c.elemcon, c.we, w, c.st));
   return EXA_OK;
 }
@@ -135,6 +155,11 @@ int exa_drv_matvec(ExaCtx& c, const double* v, double* w) {
 // w = P v (ApplyPreconditioner, preconditioner.cpp:273-295); v and w may not alias
 int exa_drv_precond(ExaCtx& c, const double* v, double* w) {
   ExaProfScope ps(c, EXA_PH_PRECOND_APPLY);
+  if (c.precision == 1) {
+    if (c.preconditioner == 0) return exa_k_bj_apply(c.P, c.Pc32, v, w, c.st);
+    EXA_TRY(exa_k_elem_matvec(c.P, c.elemcon, c.Pc32, v, c.we, c.st));
+    return exa_k_scatter(c.P, c.f2e, c.elemcon, c.we, w, c.st);
+  }
   if (c.preconditioner == 0) return exa_k_bj_apply(c.P, c.Pc, v, w, c.st);
   EXA_TRY(exa_k_elem_matvec(c.P, c.elemcon, c.Pc, v, c.we, c.st));
   return exa_k_scatter(c.P, c.f2e, c.elemcon, c.we, w, c.st);
@@ -264,11 +289,13 @@ int exa_drv_gmres(ExaCtx& c, int* iters_out, double* relerr_out) {
 
 // NewtonSolver (solution.cpp:125-243)
 int exa_drv_newton(ExaCtx& c, int* iters_out, double* norm_out) {
+  if (c.precision == 1) return exa_drv_newton_mixed(c, iters_out, norm_out);
   const ExaDims& P = c.P;
   const long long N = c.ndofuhat();
   double nrmr = 0.0;
   EXA_TRY(exa_drv_getq(c));
   EXA_TRY(exa_drv_residual(c, &nrmr));
+  c.last_norm0 = nrmr;
   c.total_gmres_iters = 0;
   for (int it = 0; it < c.newton_maxit; ++it) {
     EXA_TRY(exa_drv_assemble(c));
@@ -310,11 +337,91 @@ int exa_drv_newton(ExaCtx& c, int* iters_out, double* norm_out) {
     if (nrmr < c.newton_tol) {
       *iters_out = it + 1;
       *norm_out = nrmr;
+      c.last_norm = nrmr;
       return EXA_OK;
     }
   }
   *iters_out = c.newton_maxit;
   *norm_out = nrmr;
+  c.last_norm = nrmr;
+  return EXA_OK;
+}
+
+// Condensed right-hand side of the mixed form from the FP64 residual (Ru, Rh) of the
+// current state: Ru <- D^-1 Ru and Rh <- Rh - K Ru with the FP32 factors of the last
+// assembly, then b = scatter(Rh).
+int exa_drv_condense_mixed(ExaCtx& c) {
+  const ExaDims& P = c.P;
+  const int n = P.n, m = P.m;
+  EXA_CUDA(cudaMemcpyAsync(c.wRu, c.Ru, sizeof(double) * (size_t)n * P.ne, cudaMemcpyDeviceToDevice, c.st));
+  EXA_TRY(exa_k_gemv32(n, n, P.ne, 1.0, c.Dinv32, (long long)n * n, c.wRu, n, 0.0, c.Ru, n, c.st));
+  EXA_TRY(exa_k_gemv32(m, n, P.ne, -1.0, c.K32, (long long)m * n, c.Ru, n, 1.0, c.Rh, m, c.st));
+  return exa_k_scatter(P, c.f2e, c.elemcon, c.Rh, c.b, c.st);
+}
+
+// Mixed-precision Newton solve: one assembly of the FP32 Jacobian blocks, then steps
+//   solve A32 x = b (GMRES to mixed_inner_tol), uhat += x, u += D^-1 Ru + D^-1 F x,
+//   FP64 residual, FP64 condensed right-hand side through the FP32 factors,
+// until the FP64 residual norm |b| + |Ru| (solution.cpp:148-157) has dropped by the target
+// ratio (mixed_rtol, or the GMRES tolerance when it is 0).  The FP64 residual at every
+// step makes the FP32 solve an iterative refinement of the FP64 Newton step.
+int exa_drv_newton_mixed(ExaCtx& c, int* iters_out, double* norm_out) {
+  const ExaDims& P = c.P;
+  const long long N = c.ndofuhat();
+  const double rtol = c.mixed_rtol > 0.0 ? c.mixed_rtol : c.gmres_tol;
+  double nrmr = 0.0;
+  EXA_TRY(exa_drv_getq(c));
+  EXA_TRY(exa_drv_residual(c, &nrmr));
+  const double nrm0 = nrmr;
+  c.last_norm0 = nrm0;
+  c.total_gmres_iters = 0;
+  if (!(nrm0 > 0.0)) {
+    *iters_out = 0;
+    *norm_out = nrm0;
+    c.last_norm = nrm0;
+    return std::isnan(nrm0) ? EXA_ERR_NAN : EXA_OK;
+  }
+  EXA_TRY(exa_drv_assemble(c));
+  const double gtol = c.gmres_tol;
+  int it = 0;
+  for (it = 0; it < c.mixed_maxit; ++it) {
+    int gi = 0;
+    double ge = 0.0;
+    // the inner solves see the small right-hand sides of late steps: no absolute cut-off
+    const double ntol = c.newton_tol;
+    c.gmres_tol = c.mixed_inner_tol;
+    c.newton_tol = 0.0;
+    const int st = exa_drv_gmres(c, &gi, &ge);
+    c.gmres_tol = gtol;
+    c.newton_tol = ntol;
+    EXA_TRY(st);
+    c.last_gmres_iters = gi;
+    c.last_gmres_relerr = ge;
+    c.total_gmres_iters += gi;
+    EXA_TRY(exa_axpby(c.uh, c.x, 1.0, 1.0, N, c.st));
+    EXA_TRY(exa_k_dudg(P, c.elemcon, c.F32, c.Ru, c.x, c.du, c.st));
+    EXA_TRY(exa_k_udg_update(P, c.udg, c.du, 1.0, c.st));
+    EXA_TRY(exa_drv_getq(c));
+    EXA_TRY(exa_drv_residual(c, &nrmr));
+    c.last_newton_iters = it + 1;
+    if (std::isnan(nrmr)) {
+      exa_set_error("mixed-precision refinement: residual is NaN");
+      *iters_out = it + 1;
+      *norm_out = nrmr;
+      c.last_norm = nrmr;
+      return EXA_ERR_NAN;
+    }
+    if (nrmr <= rtol * nrm0) break;
+    EXA_TRY(exa_drv_condense_mixed(c));
+  }
+  *iters_out = std::min(it + 1, c.mixed_maxit);
+  *norm_out = nrmr;
+  c.last_norm = nrmr;
+  if (nrmr > rtol * nrm0) {
+    exa_set_error("mixed-precision refinement stopped at residual ratio %.3e after %d steps", nrmr / nrm0,
+                  c.mixed_maxit);
+    return EXA_ERR_NOTCONV;
+  }
   return EXA_OK;
 }
 

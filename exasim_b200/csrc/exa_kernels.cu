@@ -179,21 +179,23 @@ __global__ void scatter_kernel(ExaDims P, const int* f2e, const int* elemcon, co
 }
 
 // we_e = A_e * gather(v), A_e = H (matvec) or the additive-Schwarz inverse blocks
-__global__ void elem_matvec_kernel(ExaDims P, const int* elemcon, const double* A, const double* v, double* we) {
+template <typename T>
+__global__ void elem_matvec_kernel(ExaDims P, const int* elemcon, const T* A, const double* v, double* we) {
   extern __shared__ double ve[];
   const int e = blockIdx.x, m = P.m, ncu = P.ncu;
   for (int r = threadIdx.x; r < m; r += blockDim.x) ve[r] = v[r % ncu + ncu * (long long)elemcon[r / ncu + P.ndf * e]];
   __syncthreads();
-  const double* Ae = A + (long long)e * m * m;
+  const T* Ae = A + (long long)e * m * m;
   for (int r = threadIdx.x; r < m; r += blockDim.x) {
     double s = 0.0;
-    for (int c = 0; c < m; ++c) s = fma(Ae[r + (long long)m * c], ve[c], s);
+    for (int c = 0; c < m; ++c) s = fma((double)Ae[r + (long long)m * c], ve[c], s);
     we[(long long)e * m + r] = s;
   }
 }
 
 // block-Jacobi blocks per face from the condensed element matrices (kokkosimpl.h:1067-1111)
-__global__ void bj_build_kernel(ExaDims P, const int* f2e, const int* elemcon, const double* H, double* BE) {
+template <typename T>
+__global__ void bj_build_kernel(ExaDims P, const int* f2e, const int* elemcon, const T* H, T* BE) {
   const int ncu = P.ncu, npf = P.npf, ncf = ncu * npf, m = P.m;
   const long long N = (long long)ncf * ncf * P.nf;
   for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < N; idx += (long long)gridDim.x * blockDim.x) {
@@ -202,19 +204,20 @@ __global__ void bj_build_kernel(ExaDims P, const int* f2e, const int* elemcon, c
     const int c = q % ncf;
     const int f = q / ncf;
     const int e1 = f2e[4 * f], l1 = f2e[4 * f + 1], e2 = f2e[4 * f + 2], l2 = f2e[4 * f + 3];
-    double v = H[(long long)e1 * m * m + (r + ncf * l1) + (long long)m * (c + ncf * l1)];
+    double v = (double)H[(long long)e1 * m * m + (r + ncf * l1) + (long long)m * (c + ncf * l1)];
     if (f < P.nf0 && e2 >= 0) {
       const int dm = r % ncu + ncu * (elemcon[r / ncu + npf * l2 + P.ndf * e2] - npf * f);
       const int dn = c % ncu + ncu * (elemcon[c / ncu + npf * l2 + P.ndf * e2] - npf * f);
-      v += H[(long long)e2 * m * m + (dm + ncf * l2) + (long long)m * (dn + ncf * l2)];
+      v += (double)H[(long long)e2 * m * m + (dm + ncf * l2) + (long long)m * (dn + ncf * l2)];
     }
-    BE[idx] = v;
+    BE[idx] = (T)v;
   }
 }
 
 // elemental additive Schwarz: both elements of an interior face get the sum of their
 // face blocks (kokkosimpl.h:1113-1143); BE starts as a copy of H.
-__global__ void eas_build_kernel(ExaDims P, const int* f2e, const int* elemcon, const double* H, double* BE) {
+template <typename T>
+__global__ void eas_build_kernel(ExaDims P, const int* f2e, const int* elemcon, const T* H, T* BE) {
   const int ncu = P.ncu, npf = P.npf, ncf = ncu * npf, m = P.m;
   const long long N = (long long)ncf * ncf * P.nf;
   for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < N; idx += (long long)gridDim.x * blockDim.x) {
@@ -228,37 +231,39 @@ __global__ void eas_build_kernel(ExaDims P, const int* f2e, const int* elemcon, 
     const int dn = c % ncu + ncu * (elemcon[c / ncu + npf * l2 + P.ndf * e2] - npf * f);
     const long long i1 = (long long)e1 * m * m + (r + ncf * l1) + (long long)m * (c + ncf * l1);
     const long long i2 = (long long)e2 * m * m + (dm + ncf * l2) + (long long)m * (dn + ncf * l2);
-    const double tm = H[i1] + H[i2];
+    const T tm = (T)((double)H[i1] + (double)H[i2]);
     BE[i1] = tm;
     BE[i2] = tm;
   }
 }
 
-__global__ void bj_apply_kernel(ExaDims P, const double* BE, const double* x, double* y) {
+template <typename T>
+__global__ void bj_apply_kernel(ExaDims P, const T* BE, const double* x, double* y) {
   const int ncf = P.ncu * P.npf;
   const long long N = (long long)ncf * P.nf;
   for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < N; idx += (long long)gridDim.x * blockDim.x) {
     const int r = idx % ncf;
     const long long f = idx / ncf;
-    const double* A = BE + f * ncf * ncf;
+    const T* A = BE + f * ncf * ncf;
     const double* xf = x + f * ncf;
     double s = 0.0;
-    for (int c = 0; c < ncf; ++c) s = fma(A[r + ncf * c], xf[c], s);
+    for (int c = 0; c < ncf; ++c) s = fma((double)A[r + ncf * c], xf[c], s);
     y[idx] = s;
   }
 }
 
 // du_e = Ru_e + DinvF_e gather(x) (matvec.cpp:219-238); udg(:, 0:ncu, e) += alpha du_e
-__global__ void dudg_kernel(ExaDims P, const int* elemcon, const double* DinvF, const double* Ru, const double* x,
+template <typename T>
+__global__ void dudg_kernel(ExaDims P, const int* elemcon, const T* DinvF, const double* Ru, const double* x,
                             double* du) {
   extern __shared__ double ve[];
   const int e = blockIdx.x, m = P.m, n = P.n, ncu = P.ncu;
   for (int r = threadIdx.x; r < m; r += blockDim.x) ve[r] = x[r % ncu + ncu * (long long)elemcon[r / ncu + P.ndf * e]];
   __syncthreads();
-  const double* A = DinvF + (long long)e * n * m;
+  const T* A = DinvF + (long long)e * n * m;
   for (int i = threadIdx.x; i < n; i += blockDim.x) {
     double s = 0.0;
-    for (int c = 0; c < m; ++c) s = fma(A[i + (long long)n * c], ve[c], s);
+    for (int c = 0; c < m; ++c) s = fma((double)A[i + (long long)n * c], ve[c], s);
     du[(long long)e * n + i] = Ru[(long long)e * n + i] + s;
   }
 }
@@ -344,7 +349,8 @@ int exa_k_scatter(const ExaDims& P, const int* f2e, const int* elemcon, const do
   return EXA_OK;
 }
 
-int exa_k_elem_matvec(const ExaDims& P, const int* elemcon, const double* A, const double* v, double* we,
+template <typename T>
+int exa_k_elem_matvec(const ExaDims& P, const int* elemcon, const T* A, const double* v, double* we,
                       cudaStream_t st) {
   int th = P.m <= 64 ? 64 : (P.m <= 128 ? 128 : 256);
   elem_matvec_kernel<<<P.ne, th, P.m * sizeof(double), st>>>(P, elemcon, A, v, we);
@@ -352,28 +358,32 @@ int exa_k_elem_matvec(const ExaDims& P, const int* elemcon, const double* A, con
   return EXA_OK;
 }
 
-int exa_k_bj_build(const ExaDims& P, const int* f2e, const int* elemcon, const double* H, double* BE, cudaStream_t st) {
+template <typename T>
+int exa_k_bj_build(const ExaDims& P, const int* f2e, const int* elemcon, const T* H, T* BE, cudaStream_t st) {
   const long long ncf = (long long)P.ncu * P.npf;
   bj_build_kernel<<<grid_for(ncf * ncf * P.nf), 256, 0, st>>>(P, f2e, elemcon, H, BE);
   EXA_LAUNCH_CHECK();
   return EXA_OK;
 }
 
-int exa_k_eas_build(const ExaDims& P, const int* f2e, const int* elemcon, const double* H, double* BE, cudaStream_t st) {
-  EXA_CUDA(cudaMemcpyAsync(BE, H, sizeof(double) * (size_t)P.m * P.m * P.ne, cudaMemcpyDeviceToDevice, st));
+template <typename T>
+int exa_k_eas_build(const ExaDims& P, const int* f2e, const int* elemcon, const T* H, T* BE, cudaStream_t st) {
+  EXA_CUDA(cudaMemcpyAsync(BE, H, sizeof(T) * (size_t)P.m * P.m * P.ne, cudaMemcpyDeviceToDevice, st));
   const long long ncf = (long long)P.ncu * P.npf;
   eas_build_kernel<<<grid_for(ncf * ncf * P.nf), 256, 0, st>>>(P, f2e, elemcon, H, BE);
   EXA_LAUNCH_CHECK();
   return EXA_OK;
 }
 
-int exa_k_bj_apply(const ExaDims& P, const double* BE, const double* x, double* y, cudaStream_t st) {
+template <typename T>
+int exa_k_bj_apply(const ExaDims& P, const T* BE, const double* x, double* y, cudaStream_t st) {
   bj_apply_kernel<<<grid_for((long long)P.ncu * P.npf * P.nf), 256, 0, st>>>(P, BE, x, y);
   EXA_LAUNCH_CHECK();
   return EXA_OK;
 }
 
-int exa_k_dudg(const ExaDims& P, const int* elemcon, const double* DinvF, const double* Ru, const double* x,
+template <typename T>
+int exa_k_dudg(const ExaDims& P, const int* elemcon, const T* DinvF, const double* Ru, const double* x,
                double* du, cudaStream_t st) {
   dudg_kernel<<<P.ne, 128, P.m * sizeof(double), st>>>(P, elemcon, DinvF, Ru, x, du);
   EXA_LAUNCH_CHECK();
@@ -399,3 +409,51 @@ int exa_k_face_nodes(const ExaDims& P, const int* f2e, const int* perm, const do
   EXA_LAUNCH_CHECK();
   return EXA_OK;
 }
+
+namespace {
+__global__ void gemv32_kernel(int M, int K, double alpha, const float* A, long long sA, const double* x,
+                              long long sx, double beta, double* y, long long sy) {
+  extern __shared__ double xs[];
+  const long long e = blockIdx.x;
+  for (int k = threadIdx.x; k < K; k += blockDim.x) xs[k] = x[e * sx + k];
+  __syncthreads();
+  const float* Ae = A + e * sA;
+  for (int r = threadIdx.x; r < M; r += blockDim.x) {
+    double s = 0.0;
+    for (int k = 0; k < K; ++k) s = fma((double)Ae[r + (long long)M * k], xs[k], s);
+    double* yr = y + e * sy + r;
+    *yr = (beta == 0.0) ? alpha * s : alpha * s + beta * *yr;
+  }
+}
+
+__global__ void to_f32_kernel(const double* x, float* y, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    y[i] = (float)x[i];
+}
+}  // namespace
+
+int exa_k_gemv32(int M, int K, int batch, double alpha, const float* A, long long sA, const double* x, long long sx,
+                 double beta, double* y, long long sy, cudaStream_t st) {
+  if (batch <= 0 || M <= 0) return EXA_OK;
+  const int th = M <= 64 ? 64 : (M <= 128 ? 128 : 256);
+  gemv32_kernel<<<batch, th, sizeof(double) * (size_t)(K > 0 ? K : 1), st>>>(M, K, alpha, A, sA, x, sx, beta, y, sy);
+  EXA_LAUNCH_CHECK();
+  return EXA_OK;
+}
+
+int exa_k_to_f32(const double* x, float* y, long long n, cudaStream_t st) {
+  if (n <= 0) return EXA_OK;
+  to_f32_kernel<<<grid_for(n), 256, 0, st>>>(x, y, n);
+  EXA_LAUNCH_CHECK();
+  return EXA_OK;
+}
+
+// block arrays in FP64 (plain form) and FP32 (mixed-precision form)
+#define EXA_INST_BLOCK_KERNELS(T)                                                                              \
+  template int exa_k_elem_matvec<T>(const ExaDims&, const int*, const T*, const double*, double*, cudaStream_t); \
+  template int exa_k_bj_build<T>(const ExaDims&, const int*, const int*, const T*, T*, cudaStream_t);           \
+  template int exa_k_eas_build<T>(const ExaDims&, const int*, const int*, const T*, T*, cudaStream_t);          \
+  template int exa_k_bj_apply<T>(const ExaDims&, const T*, const double*, double*, cudaStream_t);              \
+  template int exa_k_dudg<T>(const ExaDims&, const int*, const T*, const double*, const double*, double*, cudaStream_t);
+EXA_INST_BLOCK_KERNELS(double)
+EXA_INST_BLOCK_KERNELS(float)

@@ -17,13 +17,25 @@ int exa_k_qmats(const ExaDims& P, const double* shapegt, const double* shapegw, 
                 const double* shapfgw, const int* perm, const double* elemg, const double* faceg, double* mass,
                 double* cw, double* ew, cudaStream_t st);
 int exa_k_scatter(const ExaDims& P, const int* f2e, const int* elemcon, const double* we, double* w, cudaStream_t st);
-int exa_k_elem_matvec(const ExaDims& P, const int* elemcon, const double* A, const double* v, double* we,
+// block kernels, T = double (plain form) or float (mixed-precision form); vectors stay FP64
+template <typename T>
+int exa_k_elem_matvec(const ExaDims& P, const int* elemcon, const T* A, const double* v, double* we,
                       cudaStream_t st);
-int exa_k_bj_build(const ExaDims& P, const int* f2e, const int* elemcon, const double* H, double* BE, cudaStream_t st);
-int exa_k_eas_build(const ExaDims& P, const int* f2e, const int* elemcon, const double* H, double* BE, cudaStream_t st);
-int exa_k_bj_apply(const ExaDims& P, const double* BE, const double* x, double* y, cudaStream_t st);
-int exa_k_dudg(const ExaDims& P, const int* elemcon, const double* DinvF, const double* Ru, const double* x,
+template <typename T>
+int exa_k_bj_build(const ExaDims& P, const int* f2e, const int* elemcon, const T* H, T* BE, cudaStream_t st);
+template <typename T>
+int exa_k_eas_build(const ExaDims& P, const int* f2e, const int* elemcon, const T* H, T* BE, cudaStream_t st);
+template <typename T>
+int exa_k_bj_apply(const ExaDims& P, const T* BE, const double* x, double* y, cudaStream_t st);
+template <typename T>
+int exa_k_dudg(const ExaDims& P, const int* elemcon, const T* DinvF, const double* Ru, const double* x,
                double* du, cudaStream_t st);
+// y_e = alpha A_e x_e + beta y_e per element e: A_e FP32 [M, K] column-major sA apart,
+// x_e, y_e FP64 sx, sy apart (FP64 accumulation)
+int exa_k_gemv32(int M, int K, int batch, double alpha, const float* A, long long sA, const double* x, long long sx,
+                 double beta, double* y, long long sy, cudaStream_t st);
+// y = (float) x
+int exa_k_to_f32(const double* x, float* y, long long n, cudaStream_t st);
 int exa_k_udg_update(const ExaDims& P, double* udg, const double* du, double alpha, cudaStream_t st);
 int exa_k_getq(const ExaDims& P, const int* elemcon, const double* MC, const double* ME, const double* uh,
                double* udg, cudaStream_t st);

@@ -249,23 +249,28 @@ int exa_gemm(const GemmBatch& g, cudaStream_t st) {
 namespace {
 constexpr int INV_MAX_N = 160;
 
-template <int RR, int RC>
-__global__ void __launch_bounds__(512, 1) inverse_kernel(double* Aall, int n, long long stride, int* flag) {
+template <typename T>
+__device__ __forceinline__ T absval(T x) { return x < T(0) ? -x : x; }
+
+// FP32 blocks (mixed-precision form) need half the registers: two CTAs per SM
+template <typename T, int RR, int RC>
+__global__ void __launch_bounds__(512, sizeof(T) == 4 ? 2 : 1)
+    inverse_kernel(T* Aall, int n, long long stride, int* flag) {
   // double-buffered pivot column / pivot row: step k uses buffer k&1, so one barrier
   // after publishing the column and one after publishing the row suffice per step
-  __shared__ double colk[2][INV_MAX_N];
-  __shared__ double rowp[2][INV_MAX_N];
+  __shared__ T colk[2][INV_MAX_N];
+  __shared__ T rowp[2][INV_MAX_N];
   __shared__ int perm[INV_MAX_N];   // perm[k] = pivot row of step k
-  double* G = Aall + (long long)blockIdx.x * stride;
+  T* G = Aall + (long long)blockIdx.x * stride;
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;   // 16 x 32
   const int lane = threadIdx.x & 31;
-  double a[RR][RC];
+  T a[RR][RC];
 #pragma unroll
   for (int i = 0; i < RR; ++i)
 #pragma unroll
     for (int j = 0; j < RC; ++j) {
       const int r = ty + 32 * i, c = tx + 16 * j;
-      a[i][j] = (r < n && c < n) ? G[r + (long long)n * c] : 0.0;
+      a[i][j] = (r < n && c < n) ? G[r + (long long)n * c] : T(0);
     }
   unsigned used = 0u;  // bit q: row lane + 32 q already pivoted (identical in every warp)
   bool singular = false;
@@ -285,23 +290,23 @@ __global__ void __launch_bounds__(512, 1) inverse_kernel(double* Aall, int n, lo
     }
     __syncthreads();
     // every warp finds the pivot (largest |a_rk| over unused rows, first on ties)
-    double best = -1.0;
+    T best = T(-1);
     int bi = n;
 #pragma unroll
     for (int q = 0; q < (INV_MAX_N + 31) / 32; ++q) {
       const int r = lane + 32 * q;
       if (r < n && !((used >> q) & 1u)) {
-        const double v = fabs(colk[buf][r]);
+        const T v = absval(colk[buf][r]);
         if (v > best) { best = v; bi = r; }
       }
     }
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) {
-      const double ob = __shfl_xor_sync(0xffffffffu, best, off);
+      const T ob = __shfl_xor_sync(0xffffffffu, best, off);
       const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
       if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
     }
-    if (!(best > 0.0) || bi >= n) {
+    if (!(best > T(0)) || bi >= n) {
       singular = true;
       // continue on the first unused row so the block still terminates
       bi = n;
@@ -314,7 +319,7 @@ __global__ void __launch_bounds__(512, 1) inverse_kernel(double* Aall, int n, lo
     }
     const int p = bi;
     if (lane == (p & 31)) used |= 1u << (p >> 5);
-    const double d = 1.0 / colk[buf][p];
+    const T d = T(1) / colk[buf][p];
     if (threadIdx.x == 0) perm[k] = p;
     const int pa = p >> 5, pt = p & 31;
     if (ty == pt) {
@@ -324,23 +329,23 @@ __global__ void __launch_bounds__(512, 1) inverse_kernel(double* Aall, int n, lo
 #pragma unroll
           for (int j = 0; j < RC; ++j) {
             const int c = tx + 16 * j;
-            const double v = (c == k) ? d : a[i][j] * d;
+            const T v = (c == k) ? d : a[i][j] * d;
             a[i][j] = v;
             if (c < n) rowp[buf][c] = v;
           }
         }
     }
     __syncthreads();
-    double fv[RR], rv[RC];
+    T fv[RR], rv[RC];
 #pragma unroll
     for (int i = 0; i < RR; ++i) {
       const int r = ty + 32 * i;
-      fv[i] = (r < n) ? colk[buf][r] : 0.0;
+      fv[i] = (r < n) ? colk[buf][r] : T(0);
     }
 #pragma unroll
     for (int j = 0; j < RC; ++j) {
       const int c = tx + 16 * j;
-      rv[j] = (c < n) ? rowp[buf][c] : 0.0;
+      rv[j] = (c < n) ? rowp[buf][c] : T(0);
     }
 #pragma unroll
     for (int i = 0; i < RR; ++i) {
@@ -368,15 +373,15 @@ __global__ void __launch_bounds__(512, 1) inverse_kernel(double* Aall, int n, lo
     }
 }
 
-template <int RR, int RC>
-int launch_inverse(double* A, int n, long long stride, int batch, int* d_flag, cudaStream_t st) {
-  inverse_kernel<RR, RC><<<batch, 512, 0, st>>>(A, n, stride, d_flag);
+template <typename T, int RR, int RC>
+int launch_inverse(T* A, int n, long long stride, int batch, int* d_flag, cudaStream_t st) {
+  inverse_kernel<T, RR, RC><<<batch, 512, 0, st>>>(A, n, stride, d_flag);
   EXA_LAUNCH_CHECK();
   return EXA_OK;
 }
-}  // namespace
 
-int exa_inverse(double* A, int n, long long stride, int batch, int* d_flag, cudaStream_t st) {
+template <typename T>
+int inverse_dispatch(T* A, int n, long long stride, int batch, int* d_flag, cudaStream_t st) {
   if (batch <= 0) return EXA_OK;
   if (n > INV_MAX_N || n <= 0) {
     exa_set_error("dense inverse of order %d exceeds the register kernel limit %d", n, INV_MAX_N);
@@ -384,13 +389,22 @@ int exa_inverse(double* A, int n, long long stride, int batch, int* d_flag, cuda
   }
   const int rr = (n + 31) / 32, rc = (n + 15) / 16;
   // rows per thread 1..5, columns per thread 1..10
-  if (rr <= 1 && rc <= 2) return launch_inverse<1, 2>(A, n, stride, batch, d_flag, st);
-  if (rr <= 1 && rc <= 4) return launch_inverse<1, 4>(A, n, stride, batch, d_flag, st);
-  if (rr <= 2 && rc <= 4) return launch_inverse<2, 4>(A, n, stride, batch, d_flag, st);
-  if (rr <= 2 && rc <= 6) return launch_inverse<2, 6>(A, n, stride, batch, d_flag, st);
-  if (rr <= 3 && rc <= 6) return launch_inverse<3, 6>(A, n, stride, batch, d_flag, st);
-  if (rr <= 4 && rc <= 8) return launch_inverse<4, 8>(A, n, stride, batch, d_flag, st);
-  return launch_inverse<5, 10>(A, n, stride, batch, d_flag, st);
+  if (rr <= 1 && rc <= 2) return launch_inverse<T, 1, 2>(A, n, stride, batch, d_flag, st);
+  if (rr <= 1 && rc <= 4) return launch_inverse<T, 1, 4>(A, n, stride, batch, d_flag, st);
+  if (rr <= 2 && rc <= 4) return launch_inverse<T, 2, 4>(A, n, stride, batch, d_flag, st);
+  if (rr <= 2 && rc <= 6) return launch_inverse<T, 2, 6>(A, n, stride, batch, d_flag, st);
+  if (rr <= 3 && rc <= 6) return launch_inverse<T, 3, 6>(A, n, stride, batch, d_flag, st);
+  if (rr <= 4 && rc <= 8) return launch_inverse<T, 4, 8>(A, n, stride, batch, d_flag, st);
+  return launch_inverse<T, 5, 10>(A, n, stride, batch, d_flag, st);
+}
+}  // namespace
+
+int exa_inverse(double* A, int n, long long stride, int batch, int* d_flag, cudaStream_t st) {
+  return inverse_dispatch(A, n, stride, batch, d_flag, st);
+}
+
+int exa_inverse(float* A, int n, long long stride, int batch, int* d_flag, cudaStream_t st) {
+  return inverse_dispatch(A, n, stride, batch, d_flag, st);
 }
 
 // ----------------------------------------------------------------------------------

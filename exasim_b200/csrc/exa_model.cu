@@ -7,6 +7,7 @@
 
 #include "exa_assembly.cuh"
 #include "exa_solver.cuh"
+#include "exa_umma.cuh"
 #include EXA_MODEL_HEADER
 
 EXA_BIND_MODEL(EXA_MODEL_NS)
@@ -113,6 +114,91 @@ int schur_chunk(ExaCtx& c, int e0, int nb) {
   return EXA_OK;
 }
 
+// Mixed-precision Schur condensation of one chunk: the same steps as schur_chunk with the
+// products on the TF32 tensor cores (FP32 accumulation) and the results kept in FP32:
+// Dinv32 = D^-1, F32 = -D^-1 F, K32 = K, H32 = H + K D^-1 F.  Ru <- D^-1 Ru and
+// Rh <- Rh - K Ru stay FP64 vectors (FP32 matrices, FP64 accumulation).
+int schur_chunk_mixed(ExaCtx& c, int e0, int nb) {
+  const ExaDims& P = c.P;
+  const int n = P.n, m = P.m, npe = P.npe, nd = P.nd, ncu = P.ncu, ndf = P.ndf;
+  const long long nqn = (long long)npe * nd * ncu;
+  float* D32 = c.Dinv32 + (long long)e0 * n * n;
+  float* K32 = c.K32 + (long long)e0 * m * n;
+  float* H32 = c.H32 + (long long)e0 * m * m;
+  float* F32 = c.F32 + (long long)e0 * n * m;
+  const double* Hc = c.H + (long long)e0 * m * m;
+  if (P.ncq > 0) {
+    ExaProfScope ps(c, EXA_PH_QELIM);
+    exa_prof_flops(c, EXA_PH_QELIM, 2.0 * nb * ncu * (double)npe * nd * (double)(n + m) * (npe + ndf));
+    const long long kq = (long long)npe * nd;
+    const float* MC = c.MC32 + (long long)e0 * npe * npe * nd;
+    const float* ME = c.ME32 + (long long)e0 * npe * ndf * nd;
+    UGemm u{};
+    u.batch = nb; u.batch2 = ncu; u.K = (int)kq; u.beta = 1.0;
+    u.ta = EXA_T_F64; u.tb = EXA_T_F32; u.tci = EXA_T_F64; u.tco = EXA_T_F32;
+    // D(:, j + npe*b) = D + sum_(l,d) B(:, l + npe*d + npe*nd*b) MinvC(l, d, j)
+    u.M = n; u.N = npe; u.alpha = 1.0;
+    u.A = c.wB; u.lda = n; u.sA = (long long)n * nqn; u.sA2 = (long long)n * kq;
+    u.B = MC; u.ldb = kq; u.sB = kq * npe; u.sB2 = 0;
+    u.Cin = c.wD; u.ldci = n; u.sCi = (long long)n * n; u.sCi2 = (long long)n * npe;
+    u.C = D32; u.ldc = n; u.sC = (long long)n * n; u.sC2 = (long long)n * npe;
+    EXA_TRY(exa_gemm_tf32(u, c.d_uflag, c.st));
+    // F(:, b + ncu*jf) = F - sum_(l,d) B(:, l + npe*d + npe*nd*b) MinvE(l, d, jf)
+    u.N = ndf; u.alpha = -1.0;
+    u.B = ME; u.ldb = kq; u.sB = kq * ndf;
+    u.Cin = c.wF; u.ldci = (long long)n * ncu; u.sCi = (long long)n * m; u.sCi2 = n;
+    u.C = c.wF32; u.ldc = (long long)n * ncu; u.sC = (long long)n * m; u.sC2 = n;
+    EXA_TRY(exa_gemm_tf32(u, c.d_uflag, c.st));
+    // K(:, j + npe*b) = K + sum_(l,d) G(:, l + npe*d + npe*nd*b) MinvC(l, d, j)
+    u.M = m; u.N = npe; u.alpha = 1.0;
+    u.A = c.wG; u.lda = m; u.sA = (long long)m * nqn; u.sA2 = (long long)m * kq;
+    u.B = MC; u.ldb = kq; u.sB = kq * npe;
+    u.Cin = c.wK; u.ldci = m; u.sCi = (long long)m * n; u.sCi2 = (long long)m * npe;
+    u.C = K32; u.ldc = m; u.sC = (long long)m * n; u.sC2 = (long long)m * npe;
+    EXA_TRY(exa_gemm_tf32(u, c.d_uflag, c.st));
+    // H(:, b + ncu*jf) = H - sum_(l,d) G(:, l + npe*d + npe*nd*b) MinvE(l, d, jf)
+    u.N = ndf; u.alpha = -1.0;
+    u.B = ME; u.ldb = kq; u.sB = kq * ndf;
+    u.Cin = Hc; u.ldci = (long long)m * ncu; u.sCi = (long long)m * m; u.sCi2 = m;
+    u.C = H32; u.ldc = (long long)m * ncu; u.sC = (long long)m * m; u.sC2 = m;
+    EXA_TRY(exa_gemm_tf32(u, c.d_uflag, c.st));
+  } else {
+    EXA_TRY(exa_k_to_f32(c.wD, D32, (long long)nb * n * n, c.st));
+    EXA_TRY(exa_k_to_f32(c.wF, c.wF32, (long long)nb * n * m, c.st));
+    EXA_TRY(exa_k_to_f32(c.wK, K32, (long long)nb * m * n, c.st));
+    EXA_TRY(exa_k_to_f32(Hc, H32, (long long)nb * m * m, c.st));
+  }
+  {
+    ExaProfScope ps(c, EXA_PH_INVERSE);
+    EXA_TRY(exa_inverse(D32, n, (long long)n * n, nb, c.d_flag, c.st));
+  }
+  ExaProfScope ps(c, EXA_PH_SCHUR);
+  exa_prof_flops(c, EXA_PH_SCHUR, 2.0 * nb * ((double)n * n * m + (double)n * n + (double)m * m * n + (double)m * n));
+  UGemm u{};
+  u.batch = nb; u.batch2 = 1;
+  u.ta = u.tb = u.tci = u.tco = EXA_T_F32;
+  // DinvF = -Dinv F
+  u.M = n; u.N = m; u.K = n; u.alpha = -1.0; u.beta = 0.0;
+  u.A = D32; u.lda = n; u.sA = (long long)n * n;
+  u.B = c.wF32; u.ldb = n; u.sB = (long long)n * m;
+  u.Cin = nullptr;
+  u.C = F32; u.ldc = n; u.sC = (long long)n * m;
+  EXA_TRY(exa_gemm_tf32(u, c.d_uflag, c.st));
+  // H += K DinvF
+  u.M = m; u.N = m; u.K = n; u.alpha = 1.0; u.beta = 1.0;
+  u.A = K32; u.lda = m; u.sA = (long long)m * n;
+  u.B = F32; u.ldb = n; u.sB = (long long)n * m;
+  u.Cin = H32; u.ldci = m; u.sCi = (long long)m * m;
+  u.C = H32; u.ldc = m; u.sC = (long long)m * m;
+  EXA_TRY(exa_gemm_tf32(u, c.d_uflag, c.st));
+  // Ru = Dinv Ru; Rh -= K Ru
+  double* Ruc = c.Ru + (long long)e0 * n;
+  EXA_CUDA(cudaMemcpyAsync(c.wRu, Ruc, sizeof(double) * (size_t)n * nb, cudaMemcpyDeviceToDevice, c.st));
+  EXA_TRY(exa_k_gemv32(n, n, nb, 1.0, D32, (long long)n * n, c.wRu, n, 0.0, Ruc, n, c.st));
+  EXA_TRY(exa_k_gemv32(m, n, nb, -1.0, K32, (long long)m * n, Ruc, n, 1.0, c.Rh + (long long)e0 * m, m, c.st));
+  return EXA_OK;
+}
+
 }  // namespace
 
 int exa_model_assemble(ExaCtx& c, bool jacobian) {
@@ -155,7 +241,7 @@ int exa_model_assemble(ExaCtx& c, bool jacobian) {
         face_kernel<ExaModel, true><<<nb, tpb_f, fs, c.st>>>(A, Ruc, Rhc, c.wD, c.wB, c.wF, c.wK, c.wG, Hc);
         EXA_LAUNCH_CHECK();
       }
-      EXA_TRY(schur_chunk(c, e0, nb));
+      EXA_TRY(c.precision == 1 ? schur_chunk_mixed(c, e0, nb) : schur_chunk(c, e0, nb));
     } else {
       ExaProfScope ps(c, EXA_PH_RESIDUAL);
       vol_points_kernel<ExaModel, false><<<nb, tpb_v, vs, c.st>>>(A, Ruc, nullptr);

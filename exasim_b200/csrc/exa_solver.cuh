@@ -65,6 +65,21 @@ struct ExaCtx {
   double last_gmres_relerr = 0.0;
   long long kernel_launches = 0;
   ExaProf prof;
+  // residual norms of the last Newton / refinement solve: at its start and at its end
+  double last_norm0 = 0.0, last_norm = 0.0;
+
+  // mixed-precision form (exa_set_precision): the element elimination, the condensed
+  // blocks and the preconditioner in FP32 (TF32 tensor-core products, FP32 accumulation);
+  // the residual, the Newton update and GMRES stay FP64 and iterate the FP32 solve to the
+  // FP64 residual tolerance.
+  int precision = 0;              // 0 plain FP64, 1 mixed
+  double mixed_inner_tol = 1e-4;  // GMRES tolerance of each refinement step
+  double mixed_rtol = 0.0;        // target residual ratio of a mixed solve (0: GMRES tolerance)
+  int mixed_maxit = 30;           // refinement steps per mixed solve
+  float *MC32 = nullptr, *ME32 = nullptr;                  // Minv C, Minv E
+  float *H32 = nullptr, *F32 = nullptr, *K32 = nullptr;    // condensed block, D^-1 F, K
+  float *Dinv32 = nullptr, *Pc32 = nullptr, *wF32 = nullptr;
+  int* d_uflag = nullptr;         // tensor-core kernel wait flag
 
   long long ndofuhat() const { return (long long)P.ncu * P.npf * P.nf; }
 };
@@ -90,6 +105,10 @@ int exa_drv_newton(ExaCtx& c, int* iters, double* norm);
 int exa_drv_dirk(ExaCtx& c, int nsteps, int* newton_iters_out, int max_out);
 int exa_drv_dirk_stage(ExaCtx& c, int istep, int stage, int* its_out, double* norm_out);
 int exa_drv_norm(ExaCtx& c, const double* x, long long n, double* out);
+// mixed-precision form (exa_drivers.cu, exa_api.cu)
+int exa_ctx_set_precision(ExaCtx& c, int mode);
+int exa_drv_newton_mixed(ExaCtx& c, int* iters, double* norm);
+int exa_drv_condense_mixed(ExaCtx& c);
 
 // phase profile (exa_drivers.cu)
 int exa_prof_enable(ExaCtx& c, int on);

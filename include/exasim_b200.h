@@ -41,7 +41,10 @@ int exa_sizes(exa_ctx* ctx, long long* out);
 /* Host copies of named device arrays: "udg", "uh", "H", "F" (D^-1 F after assembly),
  * "Ru", "Rh", "b", "x", "sdg", "P" (preconditioner), "MinvC", "MinvE", "elemg", "faceg".
  * n must equal the array length.  MinvC and MinvE hold, per element, Minv*C_d and Minv*E_d
- * with the dimension index next to the row index: [npe, nd, npe] and [npe, nd, npf*nfe]. */
+ * with the dimension index next to the row index: [npe, nd, npe] and [npe, nd, npf*nfe].
+ * After exa_set_precision(ctx, 1, ...) the FP32 arrays "H32", "F32" (D^-1 F), "K32" and
+ * "Dinv32" are available too: exa_get_field/exa_set_field convert them to and from double,
+ * and exa_field_ptr returns their device address (pointing at floats). */
 int exa_get_field(exa_ctx* ctx, const char* name, double* host, long long n);
 int exa_set_field(exa_ctx* ctx, const char* name, const double* host, long long n);
 /* Device pointer and length of a named array (zero-copy access, e.g. from torch). */
@@ -88,6 +91,17 @@ int exa_solve(exa_ctx* ctx, const double* udg_in, const double* uh_in, double* u
  * elemcon (npf*nfe*ne ints) receive the result.  Returns nf (>= 0) or a negated status. */
 int exa_connectivity_host(const int* t, const int* bf, const int* perm, const double* xpf, int dim,
                           int elemtype, int ne, int npe, int npf, int* f2e, int* elemcon, int* nf0);
+/* Precision form of the Newton solves (exa_newton, exa_dirk, exa_dirk_stage, exa_solve).
+ * mode 0: plain FP64 (the reference's arithmetic).  mode 1: mixed precision, with no
+ * counterpart in the reference: the element elimination (q elimination, D^-1, Schur
+ * products) runs on the TF32 tensor cores with FP32 accumulation, and the condensed blocks
+ * and the preconditioner are kept in FP32.  The residual, the Newton update and GMRES stay
+ * FP64: each step solves the FP32 system to inner_tol and recomputes the FP64 residual,
+ * until the FP64 residual norm has dropped by rtol (0: by the GMRES tolerance of app.bin).
+ * The first switch to mode 1 allocates the FP32 arrays. */
+int exa_set_precision(exa_ctx* ctx, int mode, double inner_tol, double rtol);
+/* Residual norm |b| + |Ru| at the start and at the end of the last Newton solve. */
+int exa_last_residual(exa_ctx* ctx, double* initial, double* final_norm);
 /* Device time by solver phase, from CUDA events recorded on the context stream around each
  * phase (the reference prints its own phase timers instead, e.g. Solver/ptcsolver.cpp:361).
  * exa_profile(ctx, 1) resets the totals and starts recording; exa_profile(ctx, 0) stops.
