@@ -72,6 +72,7 @@ def load_library(model: str) -> ctypes.CDLL:
         "exa_dinverse_batched": ([P, I, LL, I, P, P], I),
         "exa_dnrm2_cols_fixed": ([P, LL, LL, I, P, P], I),
         "exa_gemm_tf32_batched": ([I, I, I, D, P, I, LL, LL, P, I, LL, LL, D, P, I, LL, LL, I, P, P], I),
+        "exa_gemm_3xtf32_batched": ([I, I, I, D, P, I, LL, LL, P, I, LL, LL, D, P, LL, LL, I, P, P], I),
         "exa_profile": ([P, I], I),
         "exa_set_precision": ([P, I, D, D], I),
         "exa_last_residual": ([P, PD, PD], I),

@@ -333,17 +333,37 @@ int exa_ctx_set_precision(ExaCtx& c, int mode) {
   if (mode == 1 && c.H32 == nullptr) {
     const ExaDims& P = c.P;
     const size_t ne = P.ne, n = P.n, m = P.m, nb = c.neb;
+    const int kq = P.npe * P.nd;
+    // a packed operand for `count` elements with `per` parts each (batch strides sb = per
+    // parts, sb2 = one part)
+    auto packed = [&](UPacked& u, int R, int K, int TR, size_t count, int per) -> int {
+      const long long sz = exa_pack_size(R, K);
+      u.R = R; u.K = K; u.TR = TR;
+      u.sb = sz * per;
+      u.sb2 = sz;
+      EXA_TRY(dev_alloc(c, &u.hi, (size_t)sz * per * count));
+      EXA_TRY(dev_alloc(c, &u.lo, (size_t)sz * per * count));
+      return EXA_OK;
+    };
+    const int r16m = (P.m + 15) / 16 * 16;
     if (P.ncq > 0) {
-      EXA_TRY(dev_alloc(c, &c.MC32, ne * P.npe * P.npe * P.nd));
-      EXA_TRY(dev_alloc(c, &c.ME32, ne * P.npe * P.ndf * P.nd));
-      EXA_TRY(exa_k_to_f32(c.MC, c.MC32, (long long)(ne * P.npe * P.npe * P.nd), c.st));
-      EXA_TRY(exa_k_to_f32(c.ME, c.ME32, (long long)(ne * P.npe * P.ndf * P.nd), c.st));
+      // Minv C, Minv E as B operands: row j (column of the product), k = (l, d) stacked
+      EXA_TRY(packed(c.MCp, P.npe, kq, (P.npe + 15) / 16 * 16, ne, 1));
+      EXA_TRY(packed(c.MEp, P.ndf, kq, (P.ndf + 15) / 16 * 16, ne, 1));
+      EXA_TRY(exa_pack(c.MC, 1, kq, 1, (long long)kq * P.npe, 0, (int)ne, 1, c.MCp, c.st));
+      EXA_TRY(exa_pack(c.ME, 1, kq, 1, (long long)kq * P.ndf, 0, (int)ne, 1, c.MEp, c.st));
+      // B and G as A operands, one part per trace component b
+      EXA_TRY(packed(c.wBp, P.n, kq, 128, nb, P.ncu));
+      EXA_TRY(packed(c.wGp, P.m, kq, 128, nb, P.ncu));
     }
+    EXA_TRY(packed(c.Dinvp, P.n, P.n, 128, nb, 1));
+    EXA_TRY(packed(c.wFp, P.m, P.n, r16m, nb, 1));
+    EXA_TRY(packed(c.Kp, P.m, P.n, 128, nb, 1));
+    EXA_TRY(packed(c.DinvFp, P.m, P.n, r16m, nb, 1));
     EXA_TRY(dev_alloc(c, &c.H32, ne * m * m));
     EXA_TRY(dev_alloc(c, &c.F32, ne * n * m));
     EXA_TRY(dev_alloc(c, &c.K32, ne * m * n));
     EXA_TRY(dev_alloc(c, &c.Dinv32, ne * n * n));
-    EXA_TRY(dev_alloc(c, &c.wF32, nb * n * m));
     if (c.preconditioner == 0)
       EXA_TRY(dev_alloc(c, &c.Pc32, (size_t)P.ncu * P.npf * P.ncu * P.npf * P.nf));
     else
@@ -712,6 +732,43 @@ extern "C" int exa_gemm_tf32_batched(int M, int N, int K, double alpha, const vo
   g.C = C; g.tco = g.tci; g.ldc = ldc; g.sC = sC; g.sC2 = 0;
   g.batch = batch; g.batch2 = 1;
   return exa_gemm_tf32(g, flag_dev, (cudaStream_t)stream);
+}
+
+// 3xTF32 product through packed copies of A and B (allocated for the call and freed after
+// it, so the call synchronises the stream); C is FP32.
+extern "C" int exa_gemm_3xtf32_batched(int M, int N, int K, double alpha, const void* A, int a_f64, long long lda,
+                                       long long sA, const void* B, int b_f64, long long ldb, long long sB,
+                                       double beta, float* C, long long ldc, long long sC, int batch, int* flag_dev,
+                                       void* stream) {
+  if (M <= 0 || N <= 0 || K <= 0 || batch <= 0 || N > 256) {
+    exa_set_error("3xtf32 gemm: sizes M %d N %d K %d batch %d (N <= 256)", M, N, K, batch);
+    return EXA_ERR_ARG;
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  const long long pa = exa_pack_size(M, K), pb = exa_pack_size(N, K);
+  float* buf = nullptr;
+  EXA_CUDA(cudaMalloc(&buf, sizeof(float) * 2 * (size_t)(pa + pb) * batch));
+  UPacked Ap{buf, buf + pa * batch, pa, 0, M, K, 128};
+  UPacked Bp{buf + 2 * pa * batch, buf + 2 * pa * batch + pb * batch, pb, 0, N, K, (N + 15) / 16 * 16};
+  int s = exa_pack(A, a_f64, 1, lda, sA, 0, batch, 1, Ap, st);
+  if (s == EXA_OK) s = exa_pack(B, b_f64, ldb, 1, sB, 0, batch, 1, Bp, st);
+  if (s == EXA_OK) {
+    UGemmP g{};
+    g.M = M; g.N = N; g.K = K; g.alpha = alpha; g.beta = beta;
+    g.A = Ap; g.B = Bp;
+    g.Cin = C; g.tci = EXA_T_F32; g.ldci = ldc; g.sCi = sC; g.sCi2 = 0;
+    g.C = C; g.tco = EXA_T_F32; g.ldc = ldc; g.sC = sC; g.sC2 = 0;
+    g.nout = 0; g.batch = batch; g.batch2 = 1;
+    s = exa_gemm_3xtf32(g, flag_dev, st);
+  }
+  cudaError_t e = cudaStreamSynchronize(st);
+  cudaFree(buf);
+  if (s != EXA_OK) return s;
+  if (e != cudaSuccess) {
+    exa_set_error("3xtf32 gemm: %s", cudaGetErrorString(e));
+    return EXA_ERR_CUDA;
+  }
+  return EXA_OK;
 }
 
 extern "C" int exa_dinverse_batched(double* A, int n, long long stride, int batch, int* info_dev, void* stream) {

@@ -114,10 +114,12 @@ int schur_chunk(ExaCtx& c, int e0, int nb) {
   return EXA_OK;
 }
 
-// Mixed-precision Schur condensation of one chunk: the same steps as schur_chunk with the
-// products on the TF32 tensor cores (FP32 accumulation) and the results kept in FP32:
-// Dinv32 = D^-1, F32 = -D^-1 F, K32 = K, H32 = H + K D^-1 F.  Ru <- D^-1 Ru and
-// Rh <- Rh - K Ru stay FP64 vectors (FP32 matrices, FP64 accumulation).
+// Mixed-precision Schur condensation of one chunk: the steps of schur_chunk with the
+// products in 3xTF32 on the tensor cores (FP32 accumulation) over operands packed in the
+// tensor-core layout, and the results kept in FP32: Dinv32 = D^-1, F32 = -D^-1 F,
+// K32 = K, H32 = H + K D^-1 F.  The GEMM epilogues write each result both where the
+// solver reads it and packed for the next product.  Ru <- D^-1 Ru and Rh <- Rh - K Ru stay
+// FP64 vectors (FP32 matrices, FP64 accumulation).
 int schur_chunk_mixed(ExaCtx& c, int e0, int nb) {
   const ExaDims& P = c.P;
   const int n = P.n, m = P.m, npe = P.npe, nd = P.nd, ncu = P.ncu, ndf = P.ndf;
@@ -127,46 +129,59 @@ int schur_chunk_mixed(ExaCtx& c, int e0, int nb) {
   float* H32 = c.H32 + (long long)e0 * m * m;
   float* F32 = c.F32 + (long long)e0 * n * m;
   const double* Hc = c.H + (long long)e0 * m * m;
+  auto at = [](UPacked u, long long e) {  // operand of element e of the set
+    u.hi += e * u.sb;
+    u.lo += e * u.sb;
+    return u;
+  };
+  UPackOut toF{c.wFp, 1, 1, 0}, toK{c.Kp, 0, 1, 0};
   if (P.ncq > 0) {
     ExaProfScope ps(c, EXA_PH_QELIM);
     exa_prof_flops(c, EXA_PH_QELIM, 2.0 * nb * ncu * (double)npe * nd * (double)(n + m) * (npe + ndf));
     const long long kq = (long long)npe * nd;
-    const float* MC = c.MC32 + (long long)e0 * npe * npe * nd;
-    const float* ME = c.ME32 + (long long)e0 * npe * ndf * nd;
-    UGemm u{};
+    // B and G per trace component: row r, k = (l, d) at column l + npe*d + npe*nd*b
+    EXA_TRY(exa_pack(c.wB, 1, 1, n, (long long)n * nqn, (long long)n * kq, nb, ncu, c.wBp, c.st));
+    EXA_TRY(exa_pack(c.wG, 1, 1, m, (long long)m * nqn, (long long)m * kq, nb, ncu, c.wGp, c.st));
+    UGemmP u{};
     u.batch = nb; u.batch2 = ncu; u.K = (int)kq; u.beta = 1.0;
-    u.ta = EXA_T_F64; u.tb = EXA_T_F32; u.tci = EXA_T_F64; u.tco = EXA_T_F32;
-    // D(:, j + npe*b) = D + sum_(l,d) B(:, l + npe*d + npe*nd*b) MinvC(l, d, j)
+    u.tci = EXA_T_F64; u.tco = EXA_T_F32;
+    // D(:, j + npe*b) = D + B_b MinvC
     u.M = n; u.N = npe; u.alpha = 1.0;
-    u.A = c.wB; u.lda = n; u.sA = (long long)n * nqn; u.sA2 = (long long)n * kq;
-    u.B = MC; u.ldb = kq; u.sB = kq * npe; u.sB2 = 0;
+    u.A = c.wBp; u.B = at(c.MCp, e0); u.B.sb2 = 0;
     u.Cin = c.wD; u.ldci = n; u.sCi = (long long)n * n; u.sCi2 = (long long)n * npe;
     u.C = D32; u.ldc = n; u.sC = (long long)n * n; u.sC2 = (long long)n * npe;
-    EXA_TRY(exa_gemm_tf32(u, c.d_uflag, c.st));
-    // F(:, b + ncu*jf) = F - sum_(l,d) B(:, l + npe*d + npe*nd*b) MinvE(l, d, jf)
+    u.nout = 0;
+    EXA_TRY(exa_gemm_3xtf32(u, c.d_uflag, c.st));
+    // F(:, b + ncu*jf) = F - B_b MinvE, packed only (B operand of D^-1 F)
     u.N = ndf; u.alpha = -1.0;
-    u.B = ME; u.ldb = kq; u.sB = kq * ndf;
+    u.B = at(c.MEp, e0); u.B.sb2 = 0;
     u.Cin = c.wF; u.ldci = (long long)n * ncu; u.sCi = (long long)n * m; u.sCi2 = n;
-    u.C = c.wF32; u.ldc = (long long)n * ncu; u.sC = (long long)n * m; u.sC2 = n;
-    EXA_TRY(exa_gemm_tf32(u, c.d_uflag, c.st));
-    // K(:, j + npe*b) = K + sum_(l,d) G(:, l + npe*d + npe*nd*b) MinvC(l, d, j)
+    u.C = nullptr;
+    toF.cmul = ncu; toF.cadd = 1;
+    u.out[0] = toF; u.nout = 1;
+    EXA_TRY(exa_gemm_3xtf32(u, c.d_uflag, c.st));
+    // K(:, j + npe*b) = K + G_b MinvC, plain and packed (A operand of K D^-1 F)
     u.M = m; u.N = npe; u.alpha = 1.0;
-    u.A = c.wG; u.lda = m; u.sA = (long long)m * nqn; u.sA2 = (long long)m * kq;
-    u.B = MC; u.ldb = kq; u.sB = kq * npe;
+    u.A = c.wGp; u.B = at(c.MCp, e0); u.B.sb2 = 0;
     u.Cin = c.wK; u.ldci = m; u.sCi = (long long)m * n; u.sCi2 = (long long)m * npe;
     u.C = K32; u.ldc = m; u.sC = (long long)m * n; u.sC2 = (long long)m * npe;
-    EXA_TRY(exa_gemm_tf32(u, c.d_uflag, c.st));
-    // H(:, b + ncu*jf) = H - sum_(l,d) G(:, l + npe*d + npe*nd*b) MinvE(l, d, jf)
+    toK.cmul = 1; toK.cadd = npe;
+    u.out[0] = toK; u.nout = 1;
+    EXA_TRY(exa_gemm_3xtf32(u, c.d_uflag, c.st));
+    // H(:, b + ncu*jf) = H - G_b MinvE
     u.N = ndf; u.alpha = -1.0;
-    u.B = ME; u.ldb = kq; u.sB = kq * ndf;
+    u.B = at(c.MEp, e0); u.B.sb2 = 0;
     u.Cin = Hc; u.ldci = (long long)m * ncu; u.sCi = (long long)m * m; u.sCi2 = m;
     u.C = H32; u.ldc = (long long)m * ncu; u.sC = (long long)m * m; u.sC2 = m;
-    EXA_TRY(exa_gemm_tf32(u, c.d_uflag, c.st));
+    u.nout = 0;
+    EXA_TRY(exa_gemm_3xtf32(u, c.d_uflag, c.st));
   } else {
     EXA_TRY(exa_k_to_f32(c.wD, D32, (long long)nb * n * n, c.st));
-    EXA_TRY(exa_k_to_f32(c.wF, c.wF32, (long long)nb * n * m, c.st));
     EXA_TRY(exa_k_to_f32(c.wK, K32, (long long)nb * m * n, c.st));
     EXA_TRY(exa_k_to_f32(Hc, H32, (long long)nb * m * m, c.st));
+    // F as the B operand of D^-1 F (row = column of F, k = row), K as an A operand
+    EXA_TRY(exa_pack(c.wF, 1, n, 1, (long long)n * m, 0, nb, 1, c.wFp, c.st));
+    EXA_TRY(exa_pack(c.wK, 1, 1, m, (long long)m * n, 0, nb, 1, c.Kp, c.st));
   }
   {
     ExaProfScope ps(c, EXA_PH_INVERSE);
@@ -174,23 +189,24 @@ int schur_chunk_mixed(ExaCtx& c, int e0, int nb) {
   }
   ExaProfScope ps(c, EXA_PH_SCHUR);
   exa_prof_flops(c, EXA_PH_SCHUR, 2.0 * nb * ((double)n * n * m + (double)n * n + (double)m * m * n + (double)m * n));
-  UGemm u{};
+  EXA_TRY(exa_pack(D32, 0, 1, n, (long long)n * n, 0, nb, 1, c.Dinvp, c.st));
+  UGemmP u{};
   u.batch = nb; u.batch2 = 1;
-  u.ta = u.tb = u.tci = u.tco = EXA_T_F32;
-  // DinvF = -Dinv F
+  u.tci = EXA_T_F32; u.tco = EXA_T_F32;
+  // DinvF = -Dinv F: plain (Newton update) and packed (B operand of K DinvF)
   u.M = n; u.N = m; u.K = n; u.alpha = -1.0; u.beta = 0.0;
-  u.A = D32; u.lda = n; u.sA = (long long)n * n;
-  u.B = c.wF32; u.ldb = n; u.sB = (long long)n * m;
+  u.A = c.Dinvp; u.B = c.wFp;
   u.Cin = nullptr;
   u.C = F32; u.ldc = n; u.sC = (long long)n * m;
-  EXA_TRY(exa_gemm_tf32(u, c.d_uflag, c.st));
+  u.out[0] = UPackOut{c.DinvFp, 1, 1, 0}; u.nout = 1;
+  EXA_TRY(exa_gemm_3xtf32(u, c.d_uflag, c.st));
   // H += K DinvF
   u.M = m; u.N = m; u.K = n; u.alpha = 1.0; u.beta = 1.0;
-  u.A = K32; u.lda = m; u.sA = (long long)m * n;
-  u.B = F32; u.ldb = n; u.sB = (long long)n * m;
+  u.A = c.Kp; u.B = c.DinvFp;
   u.Cin = H32; u.ldci = m; u.sCi = (long long)m * m;
   u.C = H32; u.ldc = m; u.sC = (long long)m * m;
-  EXA_TRY(exa_gemm_tf32(u, c.d_uflag, c.st));
+  u.nout = 0;
+  EXA_TRY(exa_gemm_3xtf32(u, c.d_uflag, c.st));
   // Ru = Dinv Ru; Rh -= K Ru
   double* Ruc = c.Ru + (long long)e0 * n;
   EXA_CUDA(cudaMemcpyAsync(c.wRu, Ruc, sizeof(double) * (size_t)n * nb, cudaMemcpyDeviceToDevice, c.st));

@@ -10,6 +10,7 @@
 
 #include "exa_kernels.cuh"
 #include "exa_conn.h"
+#include "exa_umma.cuh"
 
 // Device time by solver phase (exa_profile / exa_profile_read in the C ABI): CUDA event
 // pairs recorded on the context stream around each phase, summed when read.
@@ -76,10 +77,13 @@ struct ExaCtx {
   double mixed_inner_tol = 1e-4;  // GMRES tolerance of each refinement step
   double mixed_rtol = 0.0;        // target residual ratio of a mixed solve (0: GMRES tolerance)
   int mixed_maxit = 30;           // refinement steps per mixed solve
-  float *MC32 = nullptr, *ME32 = nullptr;                  // Minv C, Minv E
   float *H32 = nullptr, *F32 = nullptr, *K32 = nullptr;    // condensed block, D^-1 F, K
-  float *Dinv32 = nullptr, *Pc32 = nullptr, *wF32 = nullptr;
+  float *Dinv32 = nullptr, *Pc32 = nullptr;
   int* d_uflag = nullptr;         // tensor-core kernel wait flag
+  // operands of the 3xTF32 products, packed in the tensor-core layout (hi and lo parts):
+  // Minv C, Minv E as B operands (all elements); per element chunk: B and G (A operands of
+  // the q elimination), D^-1 (A), F (B of D^-1 F), K (A) and D^-1 F (B of K D^-1 F)
+  UPacked MCp{}, MEp{}, wBp{}, wGp{}, Dinvp{}, wFp{}, Kp{}, DinvFp{};
 
   long long ndofuhat() const { return (long long)P.ncu * P.npf * P.nf; }
 };

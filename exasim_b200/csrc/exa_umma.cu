@@ -16,6 +16,7 @@
 //
 // Every wait on an mbarrier is bounded.  A wait that runs out sets *flag (EXA_UMMA_TIMEOUT),
 // waits (bounded again) for the MMAs already issued, frees the tensor memory and returns.
+#include <algorithm>
 #include <cstdint>
 
 #include "exa_common.cuh"
@@ -276,4 +277,270 @@ int exa_gemm_tf32(const UGemm& g, int* flag, cudaStream_t st) {
       exa_set_error("tf32 gemm: operand type combination %d is not instantiated", key);
       return EXA_ERR_UNSUPPORTED;
   }
+}
+
+// ==================================================================================
+// Packed operands and the 3xTF32 GEMM with bulk-copy staging.
+//
+// The register-staged kernel above spends about six instructions per operand element
+// (load, two conversions, address, store) and is bound by instruction issue, not by the
+// tensor cores.  Here the operands arrive pre-packed in the tcgen05 layout (hi and lo
+// TF32 parts), so one thread moves each K chunk into shared memory with cp.async.bulk
+// (completing on the stage's mbarrier through its transaction count), one thread issues
+// the MMAs, and four warps run the epilogue: no per-element staging instructions.
+// ==================================================================================
+namespace {
+
+constexpr int PK = 16;        // K per chunk
+constexpr int PST = 3;        // stages
+constexpr int PNT = 128;      // threads (4 warps: epilogue lanes 0..127)
+
+__host__ __device__ inline long long pack_off(int row, int k, int R, int K, int TR) {
+  const int nkc = (K + PK - 1) / PK;
+  const int t = row / TR, rl = row - t * TR;
+  const int rows_t = (R - t * TR) < TR ? (R - t * TR) : TR;
+  const int ng = (rows_t + 7) / 8;
+  const int kc = k / PK, kl = k - kc * PK;
+  return (long long)t * (TR / 8) * nkc * 128 + (long long)kc * ng * 128 + (rl >> 3) * 128 + (kl >> 2) * 32 +
+         (rl & 7) * 4 + (kl & 3);
+}
+
+__device__ __forceinline__ void split_tf32(double x, float& hi, float& lo) {
+  const uint32_t h = to_tf32((float)x);
+  hi = __uint_as_float(h);
+  lo = __uint_as_float(to_tf32((float)(x - (double)hi)));
+}
+
+template <typename TS>
+__global__ void pack_kernel(const TS* src, long long rs, long long ks, long long sb, long long sb2, int batch2,
+                            long long total, UPacked d) {
+  const int nkc = (d.K + PK - 1) / PK, NG = (d.R + 7) / 8;
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+       idx += (long long)gridDim.x * blockDim.x) {
+    const int w = (int)(idx & 127);
+    long long q = idx >> 7;
+    const int kc = (int)(q % nkc);
+    q /= nkc;
+    const int G = (int)(q % NG);
+    q /= NG;
+    const long long b2 = q % batch2, b1 = q / batch2;
+    const int ki = w >> 5, r8 = (w >> 2) & 7, k4 = w & 3;
+    const int row = 8 * G + r8, k = PK * kc + 4 * ki + k4;
+    double x = 0.0;
+    if (row < d.R && k < d.K) x = (double)src[b1 * sb + b2 * sb2 + row * rs + k * ks];
+    float hi, lo;
+    split_tf32(x, hi, lo);
+    const long long o = b1 * d.sb + b2 * d.sb2 + pack_off(row, k, d.R, d.K, d.TR);
+    d.hi[o] = hi;
+    if (d.lo) d.lo[o] = lo;
+  }
+}
+
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_addr(dst)),
+               "l"(src), "r"(bytes), "r"(smem_addr(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+               : "memory");
+}
+
+template <int NP, typename TCI, typename TCO>
+__global__ void __launch_bounds__(PNT, 1) umma3_kernel(UGemmP g, int* flag) {
+  static_assert(NP % 16 == 0 && NP >= 16 && NP <= 256, "N tile");
+  constexpr int A_B = 16 * 512, B_B = (NP / 8) * 512;     // one part (hi or lo) per stage
+  constexpr int STAGE = 2 * (A_B + B_B);
+  constexpr int TCOLS = NP <= 32 ? 32 : (NP <= 64 ? 64 : (NP <= 128 ? 128 : 256));
+  constexpr uint32_t IDESC = idesc_tf32(UM, NP);
+  extern __shared__ __align__(1024) uint8_t psm[];
+  uint64_t* full = reinterpret_cast<uint64_t*>(psm + PST * STAGE);
+  uint64_t* empty = full + PST;
+  uint64_t* done = empty + PST;
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(done + 1);
+  int* abort_flag = reinterpret_cast<int*>(tslot + 1);
+
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const long long b1 = blockIdx.y, b2 = blockIdx.z;
+  const int tA = blockIdx.x, m0 = tA * UM;
+  const int nkc = (g.K + PK - 1) / PK;
+  const int rowsA = (g.M - m0) < UM ? (g.M - m0) : UM;
+  const int ngA = (rowsA + 7) / 8, ngB = (g.N + 7) / 8;
+  const uint32_t bytesA = (uint32_t)ngA * 512, bytesB = (uint32_t)ngB * 512;
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(tslot)),
+                 "r"(TCOLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (tid == 0) {
+    for (int s = 0; s < PST; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    mbar_init(done, 1);
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tslot;
+
+  const float* Ahi = g.A.hi + b1 * g.A.sb + b2 * g.A.sb2 + (long long)tA * 16 * nkc * 128;
+  const float* Alo = g.A.lo + b1 * g.A.sb + b2 * g.A.sb2 + (long long)tA * 16 * nkc * 128;
+  const float* Bhi = g.B.hi + b1 * g.B.sb + b2 * g.B.sb2;
+  const float* Blo = g.B.lo + b1 * g.B.sb + b2 * g.B.sb2;
+
+  if (warp == 0 && lane == 0) {
+    // producer: chunk kc into stage kc % PST once the MMAs of chunk kc - PST are done
+    for (int kc = 0; kc < nkc; ++kc) {
+      const int s = kc % PST;
+      if (kc >= PST && !mbar_wait(&empty[s], (uint32_t)((kc / PST - 1) & 1))) {
+        atomicExch(abort_flag, 1);
+        break;
+      }
+      uint8_t* st = psm + s * STAGE;
+      mbar_expect_tx(&full[s], 2 * (bytesA + bytesB));
+      bulk_g2s(st, Ahi + (long long)kc * ngA * 128, bytesA, &full[s]);
+      bulk_g2s(st + A_B, Alo + (long long)kc * ngA * 128, bytesA, &full[s]);
+      bulk_g2s(st + 2 * A_B, Bhi + (long long)kc * ngB * 128, bytesB, &full[s]);
+      bulk_g2s(st + 2 * A_B + B_B, Blo + (long long)kc * ngB * 128, bytesB, &full[s]);
+    }
+  } else if (warp == 1 && lane == 0) {
+    // MMA issuer: hi*hi + hi*lo + lo*hi per K step of 8
+    for (int kc = 0; kc < nkc; ++kc) {
+      const int s = kc % PST;
+      if (!mbar_wait(&full[s], (uint32_t)((kc / PST) & 1))) {
+        atomicExch(abort_flag, 1);
+        break;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint32_t a_hi = smem_addr(psm + s * STAGE), a_lo = a_hi + A_B;
+      const uint32_t b_hi = a_hi + 2 * A_B, b_lo = b_hi + B_B;
+#pragma unroll
+      for (int kk = 0; kk < PK / 8; ++kk) {
+        const uint32_t o = kk * 256;
+        umma_tf32(tmem, sdesc(a_hi + o, 128, 512), sdesc(b_hi + o, 128, 512), IDESC, (kc > 0 || kk > 0) ? 1u : 0u);
+        umma_tf32(tmem, sdesc(a_hi + o, 128, 512), sdesc(b_lo + o, 128, 512), IDESC, 1u);
+        umma_tf32(tmem, sdesc(a_lo + o, 128, 512), sdesc(b_hi + o, 128, 512), IDESC, 1u);
+      }
+      umma_commit(&empty[s]);
+    }
+    umma_commit(done);  // tracks every MMA issued above
+  }
+  __syncwarp();
+  const bool fin = mbar_wait(done, 0);
+  const bool ok = __syncthreads_and(fin && *abort_flag == 0);
+  if (!ok && tid == 0) atomicExch(flag, EXA_UMMA_TIMEOUT);
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (ok) {
+    const int r = m0 + 32 * warp + lane;
+    TCO* C = reinterpret_cast<TCO*>(g.C);
+    const TCI* Ci = reinterpret_cast<const TCI*>(g.Cin);
+    if (C) C += b1 * g.sC + b2 * g.sC2;
+    if (Ci) Ci += b1 * g.sCi + b2 * g.sCi2;
+#pragma unroll 1
+    for (int c0 = 0; c0 < NP; c0 += 16) {
+      uint32_t v[16];
+      const uint32_t taddr = tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)c0;
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+          "%14, %15}, [%16];"
+          : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+            "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+          : "r"(taddr));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      if (r < g.M) {
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          const int c = c0 + j;
+          if (c >= g.N) break;
+          double x = g.alpha * (double)__uint_as_float(v[j]);
+          if (g.beta != 0.0) x += g.beta * (double)Ci[r + g.ldci * c];
+          if (C) C[r + g.ldc * c] = (TCO)x;
+          for (int o = 0; o < g.nout; ++o) {
+            const UPackOut& po = g.out[o];
+            const int gc = c * po.cmul + (int)b2 * po.cadd;
+            const long long off = b1 * po.p.sb + (po.as_b ? pack_off(gc, r, po.p.R, po.p.K, po.p.TR)
+                                                          : pack_off(r, gc, po.p.R, po.p.K, po.p.TR));
+            float hi, lo;
+            split_tf32(x, hi, lo);
+            po.p.hi[off] = hi;
+            po.p.lo[off] = lo;
+          }
+        }
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TCOLS) : "memory");
+}
+
+template <int NP, typename TCI, typename TCO>
+int launch_umma3(const UGemmP& g, int* flag, cudaStream_t st) {
+  constexpr size_t smem = (size_t)PST * 2 * (16 * 512 + (NP / 8) * 512) + (2 * PST + 1) * 8 + 16;
+  static_assert(smem <= 227 * 1024, "tile exceeds shared memory");
+  auto kern = umma3_kernel<NP, TCI, TCO>;
+  EXA_CUDA(cudaFuncSetAttribute((const void*)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  EXA_CUDA(cudaFuncSetAttribute((const void*)kern, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                (int)cudaSharedmemCarveoutMaxShared));
+  dim3 grid((unsigned)exa_ceil_div(g.M, UM), (unsigned)g.batch, (unsigned)g.batch2);
+  kern<<<grid, PNT, smem, st>>>(g, flag);
+  EXA_LAUNCH_CHECK();
+  return EXA_OK;
+}
+
+template <typename TCI, typename TCO>
+int umma3_np(const UGemmP& g, int* flag, cudaStream_t st) {
+  if (g.N <= 128) return launch_umma3<128, TCI, TCO>(g, flag, st);
+  if (g.N <= 160) return launch_umma3<160, TCI, TCO>(g, flag, st);
+  return launch_umma3<256, TCI, TCO>(g, flag, st);
+}
+
+}  // namespace
+
+long long exa_pack_size(int R, int K) { return (long long)((R + 7) / 8) * ((K + PK - 1) / PK) * 128; }
+
+int exa_pack(const void* src, int src_f64, long long rs, long long ks, long long sb, long long sb2, int batch,
+             int batch2, const UPacked& d, cudaStream_t st) {
+  if (batch <= 0 || batch2 <= 0 || d.R <= 0 || d.K <= 0) return EXA_OK;
+  if (d.TR % 8 != 0) {
+    exa_set_error("pack: tile height %d is not a multiple of 8", d.TR);
+    return EXA_ERR_ARG;
+  }
+  const long long total = (long long)batch * batch2 * exa_pack_size(d.R, d.K);
+  const int grid = (int)std::min<long long>((total + 255) / 256, 148LL * 32);
+  if (src_f64)
+    pack_kernel<double><<<grid, 256, 0, st>>>((const double*)src, rs, ks, sb, sb2, batch2, total, d);
+  else
+    pack_kernel<float><<<grid, 256, 0, st>>>((const float*)src, rs, ks, sb, sb2, batch2, total, d);
+  EXA_LAUNCH_CHECK();
+  return EXA_OK;
+}
+
+int exa_gemm_3xtf32(const UGemmP& g, int* flag, cudaStream_t st) {
+  if (g.M <= 0 || g.N <= 0 || g.batch <= 0 || g.batch2 <= 0) return EXA_OK;
+  // the kernel locates chunks from M and N, so the packed operands must have exactly those
+  // rows; batch strides keep every chunk on a 16-byte boundary for the bulk copies
+  if (g.K <= 0 || g.N > 256 || g.A.K != g.K || g.B.K != g.K || g.A.TR != UM || g.B.TR < g.N || g.A.R != g.M ||
+      g.B.R != g.N || !g.A.lo || !g.B.lo || g.nout < 0 || g.nout > 2 || (g.beta != 0.0 && !g.Cin) ||
+      (g.A.sb | g.A.sb2 | g.B.sb | g.B.sb2) % 4 != 0) {
+    exa_set_error("3xtf32 gemm: inconsistent operand description (M %d N %d K %d)", g.M, g.N, g.K);
+    return EXA_ERR_ARG;
+  }
+  if (g.batch > 65535 || g.batch2 > 65535) {
+    exa_set_error("3xtf32 gemm: batch dimensions %d x %d exceed the grid", g.batch, g.batch2);
+    return EXA_ERR_ARG;
+  }
+  const bool ci64 = g.tci == EXA_T_F64, co64 = g.tco == EXA_T_F64;
+  if (ci64 && !co64) return umma3_np<double, float>(g, flag, st);
+  if (!ci64 && !co64) return umma3_np<float, float>(g, flag, st);
+  exa_set_error("3xtf32 gemm: FP64 output is not instantiated");
+  return EXA_ERR_UNSUPPORTED;
 }

@@ -23,3 +23,46 @@ struct UGemm {
 
 // *flag (device int) is set to EXA_UMMA_TIMEOUT if a wait inside the kernel ran out.
 int exa_gemm_tf32(const UGemm& g, int* flag, cudaStream_t st);
+
+// ---- packed operands (3xTF32) -------------------------------------------------------
+// An operand X(row, k) with R rows and K reduction values is stored pre-packed in the
+// canonical K-major layout of tcgen05, split into hi = tf32(x) and lo = tf32(x - hi):
+//   tiles of TR rows (128 for A operands; one tile of all N rows for B operands), each
+//   tile as K chunks of 16, each chunk as ceil(rows/8) groups of 8 rows x 16 k, each
+//   group as 4 core matrices of 8 rows x 4 k (128 bytes).  Rows past R and k past K are
+//   zero.  Floats per batch entry: ceil(R/8) * ceil(K/16) * 128 when TR is a multiple of 8.
+struct UPacked {
+  float* hi;
+  float* lo;
+  long long sb, sb2;  // batch strides in floats
+  int R, K, TR;
+};
+long long exa_pack_size(int R, int K);  // floats per batch entry
+
+// Pack X(r, k) = src[b1 sb + b2 sb2 + r rs + k ks] (FP64 or FP32) for b1 < batch, b2 < batch2.
+int exa_pack(const void* src, int src_f64, long long rs, long long ks, long long sb, long long sb2, int batch,
+             int batch2, const UPacked& dst, cudaStream_t st);
+
+// Packed-output description for a GEMM epilogue: C(r, c) is also stored as a packed
+// operand of a later GEMM, either as an A operand (row r, k = global column) or as a B
+// operand (row = global column, k = r).  global column = c * cmul + b2 * cadd; the packed
+// batch index is b1.
+struct UPackOut {
+  UPacked p;
+  int as_b;  // 0: A operand (row r, k col); 1: B operand (row col, k r)
+  int cmul, cadd;
+};
+
+// Cout = alpha A B + beta Cin with A (R = M, tiles of 128) and B (R = N, one tile) packed;
+// the products hi*hi + hi*lo + lo*hi on the TF32 tensor cores, accumulated in FP32.
+// Plain output C (FP32 or FP64, column-major) and up to two packed outputs, each optional.
+struct UGemmP {
+  int M, N, K;
+  double alpha, beta;
+  UPacked A, B;       // batch strides per b1 and b2
+  const void* Cin; int tci; long long ldci, sCi, sCi2;
+  void* C; int tco; long long ldc, sC, sC2;
+  UPackOut out[2]; int nout;
+  int batch, batch2;
+};
+int exa_gemm_3xtf32(const UGemmP& g, int* flag, cudaStream_t st);

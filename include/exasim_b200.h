@@ -125,6 +125,14 @@ int exa_dgemm_batched(int M, int N, int K, double alpha, const double* A, long l
                       const double* B, long long ldb, long long sB, double beta, double* C, long long ldc,
                       long long sC, int batch, void* stream);
 int exa_dinverse_batched(double* A, int n, long long stride, int batch, int* info_dev, void* stream);
+/* C_b = alpha A_b B_b + beta C_b with FP32 C, the products split as hi*hi + hi*lo + lo*hi over
+ * TF32 parts (3xTF32, about FP32 accuracy) on the tcgen05 tensor cores with FP32
+ * accumulation: the product the mixed-precision form uses.  A and B are FP64 or FP32,
+ * column-major.  N <= 256.  The call packs A and B into temporary device buffers (allocated
+ * and freed inside) and synchronises the stream.  *flag_dev as for exa_gemm_tf32_batched. */
+int exa_gemm_3xtf32_batched(int M, int N, int K, double alpha, const void* A, int a_f64, long long lda, long long sA,
+                            const void* B, int b_f64, long long ldb, long long sB, double beta, float* C, long long ldc,
+                            long long sC, int batch, int* flag_dev, void* stream);
 /* C_b = alpha A_b B_b + beta C_b on the TF32 tensor cores (tcgen05) with FP32 accumulation,
  * the product the mixed-precision form uses for PGEMNMStridedBached (pblas.h:695).  Each of
  * A, B and C is FP32 or FP64 (a_f64, b_f64, c_f64); the instantiated combinations are all

@@ -1,9 +1,9 @@
-"""Mixed-precision form (TF32 tensor-core element elimination, FP32 condensed blocks, FP64
+"""Mixed-precision form (3xTF32 tensor-core element elimination, FP32 condensed blocks, FP64
 residual refinement) through the C ABI.
 
 Tolerances:
-  * condensed block H (FP32, from TF32 products): max |H32 - H_oracle| <= 2e-3 max |H_oracle|
-    (TF32 keeps 11 significant bits: 4.9e-4 relative rounding of each operand)
+  * condensed block H (FP32, from 3xTF32 products and an FP32 inverse): max |H32 - H_oracle|
+    <= 1e-4 max |H_oracle| (FP32 rounding amplified by cond(D) ~ 1e3 through D^-1)
   * solution of a mixed solve: relative 2-norm distance to the FP64 solve <= 1e-6, and the
     FP64 residual norm reaches the requested ratio
 """
@@ -54,11 +54,11 @@ def test_mixed_condensed_blocks_close_to_fp64(cd3):
     o.assemble()
     H = s.get("H32")
     err = np.abs(H - o.H.ravel(order="F")).max() / np.abs(o.H).max()
-    assert err < 2e-3, err
+    assert err < 1e-4, err
     s.close()
 
 
-@pytest.mark.parametrize("case", ["convdiff3d"])
+@pytest.mark.parametrize("case", ["poisson2d", "convdiff3d"])
 def test_mixed_newton_matches_fp64(tmp_path, cd3, case):
     if case == "poisson2d":
         d = str(tmp_path / "datain")
