@@ -311,28 +311,32 @@ __device__ __forceinline__ void split_tf32(double x, float& hi, float& lo) {
   lo = __uint_as_float(to_tf32((float)(x - (double)hi)));
 }
 
+// one CTA per batch entry (b1, b2); a pass of 128 threads fills one 8-row x 16-k group
+// (four core matrices, 512 contiguous bytes per part)
 template <typename TS>
-__global__ void pack_kernel(const TS* src, long long rs, long long ks, long long sb, long long sb2, int batch2,
-                            long long total, UPacked d) {
+__global__ void __launch_bounds__(256) pack_kernel(const TS* src, long long rs, long long ks, long long sb,
+                                                   long long sb2, int batch2, UPacked d) {
   const int nkc = (d.K + PK - 1) / PK, NG = (d.R + 7) / 8;
-  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
-       idx += (long long)gridDim.x * blockDim.x) {
-    const int w = (int)(idx & 127);
-    long long q = idx >> 7;
-    const int kc = (int)(q % nkc);
-    q /= nkc;
-    const int G = (int)(q % NG);
-    q /= NG;
-    const long long b2 = q % batch2, b1 = q / batch2;
-    const int ki = w >> 5, r8 = (w >> 2) & 7, k4 = w & 3;
+  const long long b2 = blockIdx.x % batch2, b1 = blockIdx.x / batch2;
+  const TS* X = src + b1 * sb + b2 * sb2;
+  float* hi = d.hi + b1 * d.sb + b2 * d.sb2;
+  float* lo = d.lo ? d.lo + b1 * d.sb + b2 * d.sb2 : nullptr;
+  const int w = threadIdx.x & 127;
+  const int ki = w >> 5, r8 = (w >> 2) & 7, k4 = w & 3;
+  const int npair = NG * nkc;
+  for (int p = threadIdx.x >> 7; p < npair; p += blockDim.x >> 7) {
+    const int G = p / nkc, kc = p - G * nkc;
     const int row = 8 * G + r8, k = PK * kc + 4 * ki + k4;
     double x = 0.0;
-    if (row < d.R && k < d.K) x = (double)src[b1 * sb + b2 * sb2 + row * rs + k * ks];
-    float hi, lo;
-    split_tf32(x, hi, lo);
-    const long long o = b1 * d.sb + b2 * d.sb2 + pack_off(row, k, d.R, d.K, d.TR);
-    d.hi[o] = hi;
-    if (d.lo) d.lo[o] = lo;
+    if (row < d.R && k < d.K) x = (double)X[row * rs + k * ks];
+    float h, l;
+    split_tf32(x, h, l);
+    // tile t of TR rows: groups of earlier tiles are full, this tile has ng groups
+    const int t = (8 * G) / d.TR, g = G - t * (d.TR / 8);
+    const int rows_t = min(d.TR, d.R - t * d.TR), ng = (rows_t + 7) / 8;
+    const long long o = (long long)t * (d.TR / 8) * nkc * 128 + (long long)kc * ng * 128 + g * 128 + w;
+    hi[o] = h;
+    if (lo) lo[o] = l;
   }
 }
 
@@ -439,10 +443,32 @@ __global__ void __launch_bounds__(PNT, 1) umma3_kernel(UGemmP g, int* flag) {
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   if (ok) {
     const int r = m0 + 32 * warp + lane;
+    const bool rv = r < g.M;
     TCO* C = reinterpret_cast<TCO*>(g.C);
     const TCI* Ci = reinterpret_cast<const TCI*>(g.Cin);
     if (C) C += b1 * g.sC + b2 * g.sC2;
     if (Ci) Ci += b1 * g.sCi + b2 * g.sCi2;
+    const bool use_cin = g.beta != 0.0;
+    // per-thread parts of the packed offsets (row r fixed; columns vary)
+    long long pbase[2] = {0, 0};
+    int png[2] = {0, 0};
+#pragma unroll
+    for (int o = 0; o < 2; ++o) {
+      if (o >= g.nout) break;
+      const UPackOut& po = g.out[o];
+      if (po.as_b) {
+        // row = global column, k = r: one tile of ng groups
+        png[o] = (po.p.R + 7) / 8;
+        pbase[o] = b1 * po.p.sb + (long long)(r >> 4) * png[o] * 128 + ((r >> 2) & 3) * 32 + (r & 3);
+      } else {
+        // row = r in tile t, k = global column
+        const int t = r / po.p.TR, rl = r - t * po.p.TR;
+        const int rows_t = min(po.p.TR, po.p.R - t * po.p.TR);
+        const int nkc = (po.p.K + PK - 1) / PK;
+        png[o] = (rows_t + 7) / 8;
+        pbase[o] = b1 * po.p.sb + (long long)t * (po.p.TR / 8) * nkc * 128 + (rl >> 3) * 128 + (rl & 7) * 4;
+      }
+    }
 #pragma unroll 1
     for (int c0 = 0; c0 < NP; c0 += 16) {
       uint32_t v[16];
@@ -453,24 +479,55 @@ __global__ void __launch_bounds__(PNT, 1) umma3_kernel(UGemmP g, int* flag) {
           : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
             "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
           : "r"(taddr));
-      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-      if (r < g.M) {
+      // Cin of the 16 columns first: independent loads in flight together
+      double cin[16];
 #pragma unroll
-        for (int j = 0; j < 16; ++j) {
-          const int c = c0 + j;
-          if (c >= g.N) break;
-          double x = g.alpha * (double)__uint_as_float(v[j]);
-          if (g.beta != 0.0) x += g.beta * (double)Ci[r + g.ldci * c];
-          if (C) C[r + g.ldc * c] = (TCO)x;
-          for (int o = 0; o < g.nout; ++o) {
-            const UPackOut& po = g.out[o];
+      for (int j = 0; j < 16; ++j) {
+        const int c = c0 + j;
+        cin[j] = (use_cin && rv && c < g.N) ? (double)Ci[r + g.ldci * c] : 0.0;
+      }
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      double x[16];
+#pragma unroll
+      for (int j = 0; j < 16; ++j) x[j] = g.alpha * (double)__uint_as_float(v[j]) + g.beta * cin[j];
+      if (!rv) continue;
+      if (C) {
+#pragma unroll
+        for (int j = 0; j < 16; ++j)
+          if (c0 + j < g.N) C[r + g.ldc * (c0 + j)] = (TCO)x[j];
+      }
+#pragma unroll
+      for (int o = 0; o < 2; ++o) {
+        if (o >= g.nout) break;
+        const UPackOut& po = g.out[o];
+        if (!po.as_b && po.cmul == 1 && (po.cadd & 3) == 0) {
+          // A operand, consecutive columns are consecutive k: 4 k of a core-matrix row
+          // are one float4 (the packed K is zero-padded, so whole quads are written)
+#pragma unroll
+          for (int j = 0; j < 16; j += 4) {
+            const int gc = c0 + j + (int)b2 * po.cadd;
+            if (c0 + j >= g.N) break;
+            const long long off = pbase[o] + (long long)(gc >> 4) * png[o] * 128 + ((gc >> 2) & 3) * 32;
+            float4 h, l;
+            split_tf32(c0 + j + 0 < g.N ? x[j + 0] : 0.0, h.x, l.x);
+            split_tf32(c0 + j + 1 < g.N ? x[j + 1] : 0.0, h.y, l.y);
+            split_tf32(c0 + j + 2 < g.N ? x[j + 2] : 0.0, h.z, l.z);
+            split_tf32(c0 + j + 3 < g.N ? x[j + 3] : 0.0, h.w, l.w);
+            *reinterpret_cast<float4*>(po.p.hi + off) = h;
+            *reinterpret_cast<float4*>(po.p.lo + off) = l;
+          }
+        } else {
+#pragma unroll
+          for (int j = 0; j < 16; ++j) {
+            const int c = c0 + j;
+            if (c >= g.N) break;
             const int gc = c * po.cmul + (int)b2 * po.cadd;
-            const long long off = b1 * po.p.sb + (po.as_b ? pack_off(gc, r, po.p.R, po.p.K, po.p.TR)
-                                                          : pack_off(r, gc, po.p.R, po.p.K, po.p.TR));
-            float hi, lo;
-            split_tf32(x, hi, lo);
-            po.p.hi[off] = hi;
-            po.p.lo[off] = lo;
+            const long long off = po.as_b ? pbase[o] + (gc >> 3) * 128 + (gc & 7) * 4
+                                           : pbase[o] + (long long)(gc >> 4) * png[o] * 128 + ((gc >> 2) & 3) * 32 + (gc & 3);
+            float h, l;
+            split_tf32(x[j], h, l);
+            po.p.hi[off] = h;
+            po.p.lo[off] = l;
           }
         }
       }
@@ -514,12 +571,15 @@ int exa_pack(const void* src, int src_f64, long long rs, long long ks, long long
     exa_set_error("pack: tile height %d is not a multiple of 8", d.TR);
     return EXA_ERR_ARG;
   }
-  const long long total = (long long)batch * batch2 * exa_pack_size(d.R, d.K);
-  const int grid = (int)std::min<long long>((total + 255) / 256, 148LL * 32);
+  if ((long long)batch * batch2 > 0x7fffffffLL) {
+    exa_set_error("pack: %d x %d batch entries exceed the grid", batch, batch2);
+    return EXA_ERR_ARG;
+  }
+  const unsigned grid = (unsigned)((long long)batch * batch2);
   if (src_f64)
-    pack_kernel<double><<<grid, 256, 0, st>>>((const double*)src, rs, ks, sb, sb2, batch2, total, d);
+    pack_kernel<double><<<grid, 256, 0, st>>>((const double*)src, rs, ks, sb, sb2, batch2, d);
   else
-    pack_kernel<float><<<grid, 256, 0, st>>>((const float*)src, rs, ks, sb, sb2, batch2, total, d);
+    pack_kernel<float><<<grid, 256, 0, st>>>((const float*)src, rs, ks, sb, sb2, batch2, d);
   EXA_LAUNCH_CHECK();
   return EXA_OK;
 }
@@ -537,6 +597,17 @@ int exa_gemm_3xtf32(const UGemmP& g, int* flag, cudaStream_t st) {
   if (g.batch > 65535 || g.batch2 > 65535) {
     exa_set_error("3xtf32 gemm: batch dimensions %d x %d exceed the grid", g.batch, g.batch2);
     return EXA_ERR_ARG;
+  }
+  for (int o = 0; o < g.nout; ++o) {
+    const UPackOut& po = g.out[o];
+    // B-operand outputs hold all their rows in one tile; A-operand outputs with unit column
+    // step are written in aligned quads of k
+    const bool bad = po.as_b ? (po.p.TR < po.p.R || po.p.K < g.M)
+                             : (po.p.TR != UM || po.p.R < g.M);
+    if (bad || po.p.sb % 4 != 0 || !po.p.hi || !po.p.lo) {
+      exa_set_error("3xtf32 gemm: packed output %d does not fit the product", o);
+      return EXA_ERR_ARG;
+    }
   }
   const bool ci64 = g.tci == EXA_T_F64, co64 = g.tco == EXA_T_F64;
   if (ci64 && !co64) return umma3_np<double, float>(g, flag, st);
