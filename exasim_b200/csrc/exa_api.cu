@@ -53,10 +53,12 @@ int dev_upload(ExaCtx& c, T** dst, const T* src, size_t count) {
   return EXA_OK;
 }
 
+// Zeroed on the context stream: that stream is non-blocking, so a legacy-stream memset
+// would not be ordered before the kernels that later fill the array on it.
 template <class T>
 int dev_alloc(ExaCtx& c, T** dst, size_t count) {
   EXA_TRY(dev_upload<T>(c, dst, nullptr, count));
-  if (count) EXA_CUDA(cudaMemset(*dst, 0, count * sizeof(T)));
+  if (count) EXA_CUDA(cudaMemsetAsync(*dst, 0, count * sizeof(T), c.st));
   return EXA_OK;
 }
 
@@ -356,6 +358,11 @@ int exa_ctx_set_precision(ExaCtx& c, int mode) {
       EXA_TRY(packed(c.wBp, P.n, kq, 128, nb, P.ncu));
       EXA_TRY(packed(c.wGp, P.m, kq, 128, nb, P.ncu));
     }
+    if (exa_vol_mat_tc_fits(P)) {
+      // basis at the Gauss points: row j (node), k = g
+      EXA_TRY(packed(c.Sp, P.npe, P.nge, 128, 1, 1));
+      EXA_TRY(exa_pack(c.shapegt, 1, P.nge, 1, 0, 0, 1, 1, c.Sp, c.st));
+    }
     EXA_TRY(packed(c.Dinvp, P.n, P.n, 128, nb, 1));
     EXA_TRY(packed(c.wFp, P.m, P.n, r16m, nb, 1));
     EXA_TRY(packed(c.Kp, P.m, P.n, 128, nb, 1));
@@ -420,6 +427,9 @@ bool field(ExaCtx& c, const char* name, FieldRef& f) {
   else if (s == "MinvE") f = {c.ME, P.ncq > 0 ? (long long)P.npe * P.ndf * P.nd * ne : 0};
   else if (s == "elemg") f = {c.elemg, (long long)P.elemg_stride() * ne};
   else if (s == "faceg") f = {c.faceg, (long long)P.faceg_stride() * P.nfe * ne};
+  else if (s == "K" && c.neb == P.ne) f = {c.wK, m * n * ne};
+  else if (s == "B" && c.neb == P.ne) f = {c.wB, n * (long long)P.npe * P.nd * P.ncu * ne};
+  else if (s == "Dinv" && c.neb == P.ne) f = {c.wD, n * n * ne};
   else if (s == "H32" && c.H32) f = {nullptr, m * m * ne, c.H32};
   else if (s == "F32" && c.F32) f = {nullptr, n * m * ne, c.F32};
   else if (s == "K32" && c.K32) f = {nullptr, m * n * ne, c.K32};

@@ -179,21 +179,62 @@ __global__ void scatter_kernel(ExaDims P, const int* f2e, const int* elemcon, co
 }
 
 // we_e = A_e * gather(v), A_e = H (matvec) or the additive-Schwarz inverse blocks
-template <typename T>
-__global__ void elem_matvec_kernel(ExaDims P, const int* elemcon, const T* A, const double* v, double* we) {
-  extern __shared__ double ve[];
+// we_e = A_e ve_e per element, ve_e gathered from v through elemcon.  8 warps split the
+// columns (warp w takes c = w, w + 8, ...); lane l keeps the partial sums of rows
+// l + 32 i (i < RI) in registers, so every column is one coalesced load per 32 rows and
+// each thread has RI x 2 independent loads in flight; the 8 partials meet in shared memory.
+template <typename T, int RI>
+__global__ void __launch_bounds__(256) elem_matvec_kernel(ExaDims P, const int* elemcon, const T* A, const double* v,
+                                                          double* we) {
+  extern __shared__ double sm[];
+  double* ve = sm;             // [m]
+  double* part = sm + P.m;     // [8][m]
   const int e = blockIdx.x, m = P.m, ncu = P.ncu;
   for (int r = threadIdx.x; r < m; r += blockDim.x) ve[r] = v[r % ncu + ncu * (long long)elemcon[r / ncu + P.ndf * e]];
   __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const T* Ae = A + (long long)e * m * m;
+  double acc[RI];
+#pragma unroll
+  for (int i = 0; i < RI; ++i) acc[i] = 0.0;
+  int c = warp;
+  for (; c + 8 < m; c += 16) {
+    const T* a0 = Ae + (long long)m * c;
+    const T* a1 = a0 + 8LL * m;
+    const double x0 = ve[c], x1 = ve[c + 8];
+    T y0[RI], y1[RI];
+#pragma unroll
+    for (int i = 0; i < RI; ++i) {
+      const int r = lane + 32 * i;
+      y0[i] = r < m ? a0[r] : T(0);
+      y1[i] = r < m ? a1[r] : T(0);
+    }
+#pragma unroll
+    for (int i = 0; i < RI; ++i) acc[i] = fma((double)y1[i], x1, fma((double)y0[i], x0, acc[i]));
+  }
+  for (; c < m; c += 8) {
+    const T* a0 = Ae + (long long)m * c;
+    const double x0 = ve[c];
+#pragma unroll
+    for (int i = 0; i < RI; ++i) {
+      const int r = lane + 32 * i;
+      if (r < m) acc[i] = fma((double)a0[r], x0, acc[i]);
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < RI; ++i) {
+    const int r = lane + 32 * i;
+    if (r < m) part[warp * m + r] = acc[i];
+  }
+  __syncthreads();
   for (int r = threadIdx.x; r < m; r += blockDim.x) {
     double s = 0.0;
-    for (int c = 0; c < m; ++c) s = fma((double)Ae[r + (long long)m * c], ve[c], s);
+#pragma unroll
+    for (int w = 0; w < 8; ++w) s += part[w * m + r];
     we[(long long)e * m + r] = s;
   }
 }
 
-// block-Jacobi blocks per face from the condensed element matrices (kokkosimpl.h:1067-1111)
 template <typename T>
 __global__ void bj_build_kernel(ExaDims P, const int* f2e, const int* elemcon, const T* H, T* BE) {
   const int ncu = P.ncu, npf = P.npf, ncf = ncu * npf, m = P.m;
@@ -352,8 +393,16 @@ int exa_k_scatter(const ExaDims& P, const int* f2e, const int* elemcon, const do
 template <typename T>
 int exa_k_elem_matvec(const ExaDims& P, const int* elemcon, const T* A, const double* v, double* we,
                       cudaStream_t st) {
-  int th = P.m <= 64 ? 64 : (P.m <= 128 ? 128 : 256);
-  elem_matvec_kernel<<<P.ne, th, P.m * sizeof(double), st>>>(P, elemcon, A, v, we);
+  const size_t smem = sizeof(double) * (size_t)P.m * 9;
+  if (P.m <= 32) elem_matvec_kernel<T, 1><<<P.ne, 256, smem, st>>>(P, elemcon, A, v, we);
+  else if (P.m <= 64) elem_matvec_kernel<T, 2><<<P.ne, 256, smem, st>>>(P, elemcon, A, v, we);
+  else if (P.m <= 128) elem_matvec_kernel<T, 4><<<P.ne, 256, smem, st>>>(P, elemcon, A, v, we);
+  else if (P.m <= 256) elem_matvec_kernel<T, 8><<<P.ne, 256, smem, st>>>(P, elemcon, A, v, we);
+  else if (P.m <= 512) elem_matvec_kernel<T, 16><<<P.ne, 256, smem, st>>>(P, elemcon, A, v, we);
+  else {
+    exa_set_error("matvec: trace block of %d rows exceeds 512", P.m);
+    return EXA_ERR_UNSUPPORTED;
+  }
   EXA_LAUNCH_CHECK();
   return EXA_OK;
 }

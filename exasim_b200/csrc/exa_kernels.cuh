@@ -34,6 +34,12 @@ int exa_k_dudg(const ExaDims& P, const int* elemcon, const T* DinvF, const doubl
 // x_e, y_e FP64 sx, sy apart (FP64 accumulation)
 int exa_k_gemv32(int M, int K, int batch, double alpha, const float* A, long long sA, const double* x, long long sx,
                  double beta, double* y, long long sy, cudaStream_t st);
+// D and B volume blocks on the tcgen05 tensor cores (3xTF32) for the mixed-precision form,
+// with S = shapegt[:, :, 0] packed as a B operand (rows npe, K nge); npe, nge <= 128.
+struct UPacked;
+bool exa_vol_mat_tc_fits(const ExaDims& P);
+int exa_k_vol_mat_tc(const ExaDims& P, const double* shapegw, const UPacked& Sp, const double* rgJ, double* D,
+                     double* B, int nb, int* flag, cudaStream_t st);
 // y = (float) x
 int exa_k_to_f32(const double* x, float* y, long long n, cudaStream_t st);
 int exa_k_udg_update(const ExaDims& P, double* udg, const double* du, double alpha, cudaStream_t st);

@@ -242,10 +242,14 @@ int exa_model_assemble(ExaCtx& c, bool jacobian) {
         ExaProfScope ps(c, EXA_PH_VOLUME);
         vol_points_kernel<ExaModel, true><<<nb, tpb_v, vs, c.st>>>(A, Ruc, c.wRg);
         EXA_LAUNCH_CHECK();
-        const int tiles = exa_ceil_div(P.npe, 64);
-        dim3 grid(tiles * tiles, nb, P.ncu * P.nc);
-        vol_mat_kernel<<<grid, 256, 0, c.st>>>(P, c.shapegw, c.shapegt, c.wRg, c.wD, c.wB);
-        EXA_LAUNCH_CHECK();
+        if (c.precision == 1 && c.Sp.hi) {
+          EXA_TRY(exa_k_vol_mat_tc(P, c.shapegw, c.Sp, c.wRg, c.wD, c.wB, nb, c.d_uflag, c.st));
+        } else {
+          const int tiles = exa_ceil_div(P.npe, 64);
+          dim3 grid(tiles * tiles, nb, P.ncu * P.nc);
+          vol_mat_kernel<<<grid, 256, 0, c.st>>>(P, c.shapegw, c.shapegt, c.wRg, c.wD, c.wB);
+          EXA_LAUNCH_CHECK();
+        }
       }
       double* Hc = c.H + (long long)e0 * m * m;
       {

@@ -84,6 +84,7 @@ struct ExaCtx {
   // Minv C, Minv E as B operands (all elements); per element chunk: B and G (A operands of
   // the q elimination), D^-1 (A), F (B of D^-1 F), K (A) and D^-1 F (B of K D^-1 F)
   UPacked MCp{}, MEp{}, wBp{}, wGp{}, Dinvp{}, wFp{}, Kp{}, DinvFp{};
+  UPacked Sp{};  // shapegt[:, :, 0] as the B operand of the tensor-core volume kernel
 
   long long ndofuhat() const { return (long long)P.ncu * P.npf * P.nf; }
 };

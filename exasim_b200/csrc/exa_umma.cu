@@ -21,6 +21,9 @@
 
 #include "exa_common.cuh"
 #include "exa_umma.cuh"
+#include "exa_tc.cuh"
+
+using namespace exa_tc;
 
 namespace {
 
@@ -28,64 +31,6 @@ constexpr int UM = 128;      // tile rows (tcgen05 M)
 constexpr int UBK = 32;      // K values per stage
 constexpr int UST = 3;       // stages
 constexpr int UNT = 256;     // threads
-constexpr long long WAIT_LIMIT = 1ll << 22;
-
-__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-// shared-memory matrix descriptor: K-major, no swizzle (layout type 0), version 1
-__device__ __forceinline__ uint64_t sdesc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
-  uint64_t d = 0;
-  d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
-  d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
-  d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
-  d |= (uint64_t)1 << 46;
-  return d;
-}
-
-// instruction descriptor, kind::tf32: D FP32, A and B TF32, both K-major, N >> 3, M >> 4
-__host__ __device__ constexpr uint32_t idesc_tf32(int m, int n) {
-  return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(m >> 4) << 24);
-}
-
-__device__ __forceinline__ uint32_t to_tf32(float x) {
-  uint32_t r;
-  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-  return r;
-}
-
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count));
-}
-
-// true once the phase with the given parity has completed; false after WAIT_LIMIT polls
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
-  const uint32_t a = smem_addr(bar);
-  for (long long i = 0; i < WAIT_LIMIT; ++i) {
-    uint32_t done;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(done)
-        : "r"(a), "r"(parity)
-        : "memory");
-    if (done) return true;
-  }
-  return false;
-}
-
-__device__ __forceinline__ void umma_tf32(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
-                                          uint32_t accumulate) {
-  asm volatile(
-      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
-      " tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem_d),
-      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
-      : "memory");
-}
-
-__device__ __forceinline__ void umma_commit(uint64_t* bar) {
-  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_addr(bar))
-               : "memory");
-}
-
 template <typename T>
 __device__ __forceinline__ float ldf(const T* p) { return (float)*p; }
 
@@ -291,25 +236,8 @@ int exa_gemm_tf32(const UGemm& g, int* flag, cudaStream_t st) {
 // ==================================================================================
 namespace {
 
-constexpr int PK = 16;        // K per chunk
-constexpr int PST = 3;        // stages
-constexpr int PNT = 128;      // threads (4 warps: epilogue lanes 0..127)
-
-__host__ __device__ inline long long pack_off(int row, int k, int R, int K, int TR) {
-  const int nkc = (K + PK - 1) / PK;
-  const int t = row / TR, rl = row - t * TR;
-  const int rows_t = (R - t * TR) < TR ? (R - t * TR) : TR;
-  const int ng = (rows_t + 7) / 8;
-  const int kc = k / PK, kl = k - kc * PK;
-  return (long long)t * (TR / 8) * nkc * 128 + (long long)kc * ng * 128 + (rl >> 3) * 128 + (kl >> 2) * 32 +
-         (rl & 7) * 4 + (kl & 3);
-}
-
-__device__ __forceinline__ void split_tf32(double x, float& hi, float& lo) {
-  const uint32_t h = to_tf32((float)x);
-  hi = __uint_as_float(h);
-  lo = __uint_as_float(to_tf32((float)(x - (double)hi)));
-}
+constexpr int PST = 3;    // stages
+constexpr int PNT = 128;  // threads (4 warps: epilogue lanes 0..127)
 
 // one CTA per batch entry (b1, b2); a pass of 128 threads fills one 8-row x 16-k group
 // (four core matrices, 512 contiguous bytes per part)
@@ -338,18 +266,6 @@ __global__ void __launch_bounds__(256) pack_kernel(const TS* src, long long rs, 
     hi[o] = h;
     if (lo) lo[o] = l;
   }
-}
-
-__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
-  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                   smem_addr(dst)),
-               "l"(src), "r"(bytes), "r"(smem_addr(bar))
-               : "memory");
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
-               : "memory");
 }
 
 template <int NP, typename TCI, typename TCO>

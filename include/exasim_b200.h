@@ -42,6 +42,8 @@ int exa_sizes(exa_ctx* ctx, long long* out);
  * "Ru", "Rh", "b", "x", "sdg", "P" (preconditioner), "MinvC", "MinvE", "elemg", "faceg".
  * n must equal the array length.  MinvC and MinvE hold, per element, Minv*C_d and Minv*E_d
  * with the dimension index next to the row index: [npe, nd, npe] and [npe, nd, npf*nfe].
+ * "K", "B" and "Dinv" (the FP64 K and B blocks, and D^-1 after an FP64 assembly) exist when the whole
+ * mesh is one assembly chunk (exa_sizes element chunk == ne).
  * After exa_set_precision(ctx, 1, ...) the FP32 arrays "H32", "F32" (D^-1 F), "K32" and
  * "Dinv32" are available too: exa_get_field/exa_set_field convert them to and from double,
  * and exa_field_ptr returns their device address (pointing at floats). */
