@@ -222,7 +222,7 @@ class HDGSolver:
         return a.value, b.value
 
     PHASES = ("volume", "face", "qelim", "inverse", "schur", "precond_build", "matvec", "precond_apply",
-              "orthogonalize", "getq", "residual")
+              "orthogonalize", "getq", "residual", "pack")
 
     def profile(self, enable: bool):
         """Start (resetting the totals) or stop the per-phase device timers."""

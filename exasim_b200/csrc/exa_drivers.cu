@@ -363,8 +363,9 @@ int exa_drv_condense_mixed(ExaCtx& c) {
 //   solve A32 x = b (GMRES to mixed_inner_tol), uhat += x, u += D^-1 Ru + D^-1 F x,
 //   FP64 residual, FP64 condensed right-hand side through the FP32 factors,
 // until the FP64 residual norm |b| + |Ru| (solution.cpp:148-157) has dropped by the target
-// ratio (mixed_rtol, or the GMRES tolerance when it is 0).  The FP64 residual at every
-// step makes the FP32 solve an iterative refinement of the FP64 Newton step.
+// ratio (mixed_rtol, or the GMRES tolerance when it is 0), or has stopped falling below the
+// absolute Newton tolerance.  The FP64 residual at every step makes the FP32 solve an
+// iterative refinement of the FP64 Newton step.
 int exa_drv_newton_mixed(ExaCtx& c, int* iters_out, double* norm_out) {
   const ExaDims& P = c.P;
   const long long N = c.ndofuhat();
@@ -383,6 +384,7 @@ int exa_drv_newton_mixed(ExaCtx& c, int* iters_out, double* norm_out) {
   }
   EXA_TRY(exa_drv_assemble(c));
   const double gtol = c.gmres_tol;
+  double prev = nrm0;
   int it = 0;
   for (it = 0; it < c.mixed_maxit; ++it) {
     int gi = 0;
@@ -412,12 +414,17 @@ int exa_drv_newton_mixed(ExaCtx& c, int* iters_out, double* norm_out) {
       return EXA_ERR_NAN;
     }
     if (nrmr <= rtol * nrm0) break;
+    // a residual already below the absolute Newton tolerance that no longer falls has
+    // reached the FP64 round-off floor (a solve started from a converged state)
+    const bool floor = nrmr < c.newton_tol && nrmr > 0.5 * prev;
+    prev = nrmr;
+    if (floor) break;
     EXA_TRY(exa_drv_condense_mixed(c));
   }
   *iters_out = std::min(it + 1, c.mixed_maxit);
   *norm_out = nrmr;
   c.last_norm = nrmr;
-  if (nrmr > rtol * nrm0) {
+  if (nrmr > rtol * nrm0 && !(nrmr < c.newton_tol)) {
     exa_set_error("mixed-precision refinement stopped at residual ratio %.3e after %d steps", nrmr / nrm0,
                   c.mixed_maxit);
     return EXA_ERR_NOTCONV;

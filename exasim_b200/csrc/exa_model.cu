@@ -136,12 +136,15 @@ int schur_chunk_mixed(ExaCtx& c, int e0, int nb) {
   };
   UPackOut toF{c.wFp, 1, 1, 0}, toK{c.Kp, 0, 1, 0};
   if (P.ncq > 0) {
+    const long long kq = (long long)npe * nd;
+    {
+      // B and G per trace component: row r, k = (l, d) at column l + npe*d + npe*nd*b
+      ExaProfScope pp(c, EXA_PH_PACK);
+      EXA_TRY(exa_pack(c.wB, 1, 1, n, (long long)n * nqn, (long long)n * kq, nb, ncu, c.wBp, c.st));
+      EXA_TRY(exa_pack(c.wG, 1, 1, m, (long long)m * nqn, (long long)m * kq, nb, ncu, c.wGp, c.st));
+    }
     ExaProfScope ps(c, EXA_PH_QELIM);
     exa_prof_flops(c, EXA_PH_QELIM, 2.0 * nb * ncu * (double)npe * nd * (double)(n + m) * (npe + ndf));
-    const long long kq = (long long)npe * nd;
-    // B and G per trace component: row r, k = (l, d) at column l + npe*d + npe*nd*b
-    EXA_TRY(exa_pack(c.wB, 1, 1, n, (long long)n * nqn, (long long)n * kq, nb, ncu, c.wBp, c.st));
-    EXA_TRY(exa_pack(c.wG, 1, 1, m, (long long)m * nqn, (long long)m * kq, nb, ncu, c.wGp, c.st));
     UGemmP u{};
     u.batch = nb; u.batch2 = ncu; u.K = (int)kq; u.beta = 1.0;
     u.tci = EXA_T_F64; u.tco = EXA_T_F32;
@@ -187,9 +190,12 @@ int schur_chunk_mixed(ExaCtx& c, int e0, int nb) {
     ExaProfScope ps(c, EXA_PH_INVERSE);
     EXA_TRY(exa_inverse(D32, n, (long long)n * n, nb, c.d_flag, c.st));
   }
+  {
+    ExaProfScope pp(c, EXA_PH_PACK);
+    EXA_TRY(exa_pack(D32, 0, 1, n, (long long)n * n, 0, nb, 1, c.Dinvp, c.st));
+  }
   ExaProfScope ps(c, EXA_PH_SCHUR);
   exa_prof_flops(c, EXA_PH_SCHUR, 2.0 * nb * ((double)n * n * m + (double)n * n + (double)m * m * n + (double)m * n));
-  EXA_TRY(exa_pack(D32, 0, 1, n, (long long)n * n, 0, nb, 1, c.Dinvp, c.st));
   UGemmP u{};
   u.batch = nb; u.batch2 = 1;
   u.tci = EXA_T_F32; u.tco = EXA_T_F32;

@@ -109,9 +109,10 @@ int exa_last_residual(exa_ctx* ctx, double* initial, double* final_norm);
  * exa_profile(ctx, 1) resets the totals and starts recording; exa_profile(ctx, 0) stops.
  * Phases: 0 volume assembly, 1 face assembly, 2 q-elimination GEMMs, 3 element inverse,
  * 4 Schur GEMMs, 5 preconditioner build, 6 matvec, 7 preconditioner apply,
- * 8 Gram-Schmidt + Givens, 9 q recovery, 10 residual-only assembly.
+ * 8 Gram-Schmidt + Givens, 9 q recovery, 10 residual-only assembly, 11 packing of tensor-core
+ * operands (mixed-precision form).
  * exa_profile_read fills ms, count (timed regions) and flops (algorithmic FLOPs of the GEMM
- * phases 2 and 4, 0 elsewhere) for the first nphase (<= 11) phases; any may be NULL.  It
+ * phases 2 and 4, 0 elsewhere) for the first nphase (<= 12) phases; any may be NULL.  It
  * synchronises the context stream. */
 int exa_profile(exa_ctx* ctx, int enable);
 int exa_profile_read(exa_ctx* ctx, int nphase, double* ms, long long* count, double* flops);
