@@ -182,7 +182,7 @@ __global__ void scatter_kernel(ExaDims P, const int* f2e, const int* elemcon, co
 // we_e = A_e ve_e per element, ve_e gathered from v through elemcon.  8 warps split the
 // columns (warp w takes c = w, w + 8, ...); lane l keeps the partial sums of rows
 // l + 32 i (i < RI) in registers, so every column is one coalesced load per 32 rows and
-// each thread has RI x 2 independent loads in flight; the 8 partials meet in shared memory.
+// each thread has RI x 4 independent loads in flight; the 8 partials meet in shared memory.
 template <typename T, int RI>
 __global__ void __launch_bounds__(256) elem_matvec_kernel(ExaDims P, const int* elemcon, const T* A, const double* v,
                                                           double* we) {
@@ -198,19 +198,24 @@ __global__ void __launch_bounds__(256) elem_matvec_kernel(ExaDims P, const int* 
 #pragma unroll
   for (int i = 0; i < RI; ++i) acc[i] = 0.0;
   int c = warp;
-  for (; c + 8 < m; c += 16) {
-    const T* a0 = Ae + (long long)m * c;
-    const T* a1 = a0 + 8LL * m;
-    const double x0 = ve[c], x1 = ve[c + 8];
-    T y0[RI], y1[RI];
+  // four columns (c, c + 8, c + 16, c + 24) per step: 4 RI independent loads per thread
+  for (; c + 24 < m; c += 32) {
+    T y[4][RI];
 #pragma unroll
-    for (int i = 0; i < RI; ++i) {
-      const int r = lane + 32 * i;
-      y0[i] = r < m ? a0[r] : T(0);
-      y1[i] = r < m ? a1[r] : T(0);
+    for (int u = 0; u < 4; ++u) {
+      const T* a = Ae + (long long)m * (c + 8 * u);
+#pragma unroll
+      for (int i = 0; i < RI; ++i) {
+        const int r = lane + 32 * i;
+        y[u][i] = r < m ? a[r] : T(0);
+      }
     }
 #pragma unroll
-    for (int i = 0; i < RI; ++i) acc[i] = fma((double)y1[i], x1, fma((double)y0[i], x0, acc[i]));
+    for (int u = 0; u < 4; ++u) {
+      const double x = ve[c + 8 * u];
+#pragma unroll
+      for (int i = 0; i < RI; ++i) acc[i] = fma((double)y[u][i], x, acc[i]);
+    }
   }
   for (; c < m; c += 8) {
     const T* a0 = Ae + (long long)m * c;

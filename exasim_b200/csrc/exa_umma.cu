@@ -239,8 +239,9 @@ namespace {
 constexpr int PST = 3;    // stages
 constexpr int PNT = 128;  // threads (4 warps: epilogue lanes 0..127)
 
-// one CTA per batch entry (b1, b2); a pass of 128 threads fills one 8-row x 16-k group
-// (four core matrices, 512 contiguous bytes per part)
+// one CTA per batch entry (b1, b2); a warp fills one 8-row x 16-k group (four core
+// matrices, 512 contiguous bytes per part): lane (ki, r8) converts the four k of its row in
+// core ki and stores them as one float4 per part
 template <typename TS>
 __global__ void __launch_bounds__(256) pack_kernel(const TS* src, long long rs, long long ks, long long sb,
                                                    long long sb2, int batch2, UPacked d) {
@@ -249,22 +250,27 @@ __global__ void __launch_bounds__(256) pack_kernel(const TS* src, long long rs, 
   const TS* X = src + b1 * sb + b2 * sb2;
   float* hi = d.hi + b1 * d.sb + b2 * d.sb2;
   float* lo = d.lo ? d.lo + b1 * d.sb + b2 * d.sb2 : nullptr;
-  const int w = threadIdx.x & 127;
-  const int ki = w >> 5, r8 = (w >> 2) & 7, k4 = w & 3;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int ki = lane >> 3, r8 = lane & 7;
   const int npair = NG * nkc;
-  for (int p = threadIdx.x >> 7; p < npair; p += blockDim.x >> 7) {
+  for (int p = warp; p < npair; p += blockDim.x >> 5) {
     const int G = p / nkc, kc = p - G * nkc;
-    const int row = 8 * G + r8, k = PK * kc + 4 * ki + k4;
-    double x = 0.0;
-    if (row < d.R && k < d.K) x = (double)X[row * rs + k * ks];
-    float h, l;
-    split_tf32(x, h, l);
+    const int row = 8 * G + r8, k0 = PK * kc + 4 * ki;
+    float4 h, l;
+    float* hp = &h.x;
+    float* lp = &l.x;
+#pragma unroll
+    for (int k4 = 0; k4 < 4; ++k4) {
+      const int k = k0 + k4;
+      const double x = (row < d.R && k < d.K) ? (double)X[row * rs + k * ks] : 0.0;
+      split_tf32(x, hp[k4], lp[k4]);
+    }
     // tile t of TR rows: groups of earlier tiles are full, this tile has ng groups
     const int t = (8 * G) / d.TR, g = G - t * (d.TR / 8);
     const int rows_t = min(d.TR, d.R - t * d.TR), ng = (rows_t + 7) / 8;
-    const long long o = (long long)t * (d.TR / 8) * nkc * 128 + (long long)kc * ng * 128 + g * 128 + w;
-    hi[o] = h;
-    if (lo) lo[o] = l;
+    const long long o = (long long)t * (d.TR / 8) * nkc * 128 + (long long)kc * ng * 128 + g * 128 + ki * 32 + r8 * 4;
+    *reinterpret_cast<float4*>(hi + o) = h;
+    if (lo) *reinterpret_cast<float4*>(lo + o) = l;
   }
 }
 
