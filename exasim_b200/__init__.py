@@ -75,6 +75,7 @@ def load_library(model: str) -> ctypes.CDLL:
         "exa_gemm_3xtf32_batched": ([I, I, I, D, P, I, LL, LL, P, I, LL, LL, D, P, LL, LL, I, P, P], I),
         "exa_profile": ([P, I], I),
         "exa_set_precision": ([P, I, D, D], I),
+        "exa_bilu0_ordering": ([P, I, P, I, I, I, P, I, P, I, P, I, PI], I),
         "exa_last_residual": ([P, PD, PD], I),
         "exa_profile_read": ([P, I, PD, PLL, PD], I),
     }

@@ -4,6 +4,7 @@ Exasim datain/ folders (app, master, mesh, sol .bin) by exasim_b200.inputs.
 * poisson2d_tri : 2D Poisson, p=3 triangles on an n x n grid split into 2n^2 triangles,
                   interior vertices moved by U(-0.05h, 0.05h); block Jacobi; GMRES(50) to 1e-10
                   (examples/Poisson/poisson2d/pdemodel.txt)
+* poisson2d_quad: 2D Poisson on an n x n grid of quadrilaterals (element i + n j)
 * convdiff3d_hex: 3D convection-diffusion, p=4 hexahedra on an n^3 grid of the unit cube,
                   c = (1, 0.5, 0.25), kappa = 0.01, Gaussian source at the centre (sigma 0.1),
                   u = 0 on the boundary, DIRK(3,3) with dt = 0.01; block Jacobi; GMRES(50) to 1e-8
@@ -21,12 +22,12 @@ def _on(axis, value):
     return lambda x: abs(x[axis] - value) < 1e-8
 
 
-def write_case(datain: str, grid: I.Grid, master: I.Master, app: I.PDEApp, exprs, bcs):
+def write_case(datain: str, grid: I.Grid, master: I.Master, app: I.PDEApp, exprs, bcs, cartgridpart=()):
     os.makedirs(datain, exist_ok=True)
     bf = I.assign_bf(grid, exprs, bcs)
     I.write_app_bin(os.path.join(datain, "app.bin"), app)
     I.write_master_bin(os.path.join(datain, "master.bin"), master)
-    I.write_mesh_bin(os.path.join(datain, "mesh.bin"), grid, master, bf, bcs)
+    I.write_mesh_bin(os.path.join(datain, "mesh.bin"), grid, master, bf, bcs, cartgridpart=cartgridpart)
     I.write_sol_bin(os.path.join(datain, "sol.bin"), I.dgnodes(grid, master), nc=app.nc, ncu=app.ncu)
     return datain
 
@@ -42,9 +43,20 @@ def poisson2d_tri(datain: str, n: int = 16, porder: int = 3, seed: int = 0, prec
     return write_case(datain, grid, master, app, exprs, [1, 1, 1, 1])
 
 
+def poisson2d_quad(datain: str, n: int = 16, porder: int = 3, preconditioner: int = 0, gmres_tol: float = 1e-10,
+                   restart: int = 50, ortho: int = 0, cartgridpart=()):
+    grid = I.square_quad_grid(n)
+    master = I.make_master(2, 1, porder, 2 * porder)
+    app = I.PDEApp(nd=2, ncu=1, model="ModelD", preconditioner=preconditioner, NewtonIter=1,
+                   NewtonTol=1e-6, GMRESiter=1000, GMRESrestart=restart, GMREStol=gmres_tol, GMRESortho=ortho,
+                   RBdim=0, ppdegree=1, tau=[1.0], physicsparam=[1.0], externalparam=[0.0, 0.0])
+    exprs = [_on(1, 0.0), _on(0, 1.0), _on(1, 1.0), _on(0, 0.0)]
+    return write_case(datain, grid, master, app, exprs, [1, 1, 1, 1], cartgridpart)
+
+
 def convdiff3d_hex(datain: str, n: int = 16, porder: int = 4, nsteps: int = 20, dt: float = 0.01,
                    preconditioner: int = 0, gmres_tol: float = 1e-8, restart: int = 50, ortho: int = 0,
-                   nstage: int = 3, torder: int = 3):
+                   nstage: int = 3, torder: int = 3, cartgridpart=()):
     grid = I.cube_hex_grid(n)
     master = I.make_master(3, 1, porder, 2 * porder)
     app = I.PDEApp(nd=3, ncu=1, model="ModelD", preconditioner=preconditioner, NewtonIter=20,
@@ -52,4 +64,4 @@ def convdiff3d_hex(datain: str, n: int = 16, porder: int = 4, nsteps: int = 20, 
                    RBdim=0, ppdegree=1, tau=[1.0], torder=torder, nstage=nstage, dt=[dt] * nsteps,
                    physicsparam=[0.01, 1.0, 0.5, 0.25, 0.5, 0.5, 0.5, 0.1], externalparam=[0.0, 0.0])
     exprs = [_on(2, 0.0), _on(2, 1.0), _on(1, 0.0), _on(0, 1.0), _on(1, 1.0), _on(0, 0.0)]
-    return write_case(datain, grid, master, app, exprs, [1, 1, 1, 1, 1, 1])
+    return write_case(datain, grid, master, app, exprs, [1, 1, 1, 1, 1, 1], cartgridpart)

@@ -6,6 +6,7 @@
 #include <vector>
 
 #include "exa_solver.cuh"
+#include "exa_bilu0.h"
 #include "exa_umma.cuh"
 #include "../../include/exasim_b200.h"
 
@@ -130,7 +131,7 @@ int exa_ctx_init(ExaCtx& c, const double* app, long long napp, const double* mas
   if (coupled > 0) { exa_set_error("coupled interfaces are not supported"); return EXA_ERR_UNSUPPORTED; }
   if (c.RBdim > 0) { exa_set_error("reduced-basis initial guess (RBdim=%d) is not supported; set RBdim = 0", c.RBdim); return EXA_ERR_UNSUPPORTED; }
   if (c.ppdegree > 1) { exa_set_error("polynomial preconditioner (ppdegree=%d) is not supported", c.ppdegree); return EXA_ERR_UNSUPPORTED; }
-  if (c.preconditioner != 0 && c.preconditioner != 1) { exa_set_error("preconditioner %d: only block Jacobi (0) and elemental additive Schwarz (1)", c.preconditioner); return EXA_ERR_UNSUPPORTED; }
+  if (c.preconditioner < 0 || c.preconditioner > 2) { exa_set_error("preconditioner %d: block Jacobi (0), elemental additive Schwarz (1) or block ILU(0) on Cartesian sub-domains (2)", c.preconditioner); return EXA_ERR_UNSUPPORTED; }
   if (c.restart < 1 || c.gmres_maxit < 1) { exa_set_error("GMRES restart/iterations must be positive"); return EXA_ERR_ARG; }
 
   // ---- master.bin (readmasterstruct, readbinaryfiles.cpp:208-268)
@@ -205,6 +206,40 @@ int exa_ctx_init(ExaCtx& c, const double* app, long long napp, const double* mas
   EXA_TRY(dev_upload(c, &c.bf, bfv.data(), bfv.size()));
   EXA_TRY(dev_upload(c, &c.f2e, conn.f2e.data(), conn.f2e.size()));
   EXA_TRY(dev_upload(c, &c.elemcon, conn.elemcon.data(), conn.elemcon.size()));
+  if (c.preconditioner == 2) {
+    // block ILU(0) on the Cartesian sub-domains of mesh.bin's cartgridpart (discretization.cpp:296-311)
+    c.cartgridpart = to_int(Me.part[25], Me.nsize[25]);
+    if (c.cartgridpart.empty()) {
+      exa_set_error("block ILU(0) (preconditioner 2) needs cartgridpart in mesh.bin");
+      return EXA_ERR_UNSUPPORTED;
+    }
+    ExaBilu hb;
+    char msg[256] = "";
+    if (exa_bilu_setup(c.cartgridpart.data(), (int)c.cartgridpart.size(), conn.f2e.data(), conn.nf, P.nfe, P.ne, hb,
+                       msg, sizeof(msg)) != 0) {
+      exa_set_error("block ILU(0): %s", msg);
+      return EXA_ERR_UNSUPPORTED;
+    }
+    const int ncf = P.ncu * P.npf;
+    if (ncf > 64 || exa_bilu_apply_smem(ncf, hb.nfse) > 227 * 1024) {
+      exa_set_error("block ILU(0): %d faces of %d rows per sub-domain exceed shared memory", hb.nfse, ncf);
+      return EXA_ERR_UNSUPPORTED;
+    }
+    ExaBiluDev& d = c.bilu;
+    d.nse = hb.nse; d.nfse = hb.nfse; d.nnz = hb.nnz;
+    EXA_TRY(dev_upload(c, &d.row_ptr, hb.row_ptr.data(), hb.row_ptr.size()));
+    EXA_TRY(dev_upload(c, &d.col_ind, hb.col_ind.data(), hb.col_ind.size()));
+    EXA_TRY(dev_upload(c, &d.face, hb.face.data(), hb.face.size()));
+    EXA_TRY(dev_upload(c, &d.row_of, hb.row_of.data(), hb.row_of.size()));
+    EXA_TRY(dev_upload(c, &d.fac_ptr, hb.fac_ptr.data(), hb.fac_ptr.size()));
+    EXA_TRY(dev_upload(c, &d.fac_ji, hb.fac_ji.data(), std::max<size_t>(1, hb.fac_ji.size())));
+    EXA_TRY(dev_upload(c, &d.upd_ptr, hb.upd_ptr.data(), hb.upd_ptr.size()));
+    EXA_TRY(dev_upload(c, &d.upd_jl, hb.upd_jl.data(), std::max<size_t>(1, hb.upd_jl.size())));
+    EXA_TRY(dev_upload(c, &d.upd_il, hb.upd_il.data(), std::max<size_t>(1, hb.upd_il.size())));
+    EXA_TRY(dev_upload(c, &d.gf_ptr, hb.gf_ptr.data(), hb.gf_ptr.size()));
+    EXA_TRY(dev_upload(c, &d.gf_pos, hb.gf_pos.data(), hb.gf_pos.size()));
+    EXA_TRY(dev_alloc(c, &d.out, (size_t)hb.nse * hb.nfse * ncf));
+  }
   EXA_TRY(dev_upload(c, &c.xdg, S.part[1], (size_t)S.nsize[1]));
   std::vector<double> one_zero(1, 0.0);
   EXA_TRY(dev_upload(c, &c.uinf, c.h_uinf.empty() ? one_zero.data() : c.h_uinf.data(), std::max<size_t>(1, c.h_uinf.size())));
@@ -285,6 +320,8 @@ int exa_ctx_init(ExaCtx& c, const double* app, long long napp, const double* mas
   EXA_TRY(dev_alloc(c, &c.b, N));
   if (c.preconditioner == 0)
     EXA_TRY(dev_alloc(c, &c.Pc, (size_t)P.ncu * P.npf * P.ncu * P.npf * P.nf));
+  else if (c.preconditioner == 2)
+    EXA_TRY(dev_alloc(c, &c.Pc, (size_t)P.ncu * P.npf * P.ncu * P.npf * c.bilu.nse * c.bilu.nnz));
   else
     EXA_TRY(dev_alloc(c, &c.Pc, ne * m * m));
   // element chunk: bounded workspace (about 8 GB at most)
@@ -373,6 +410,8 @@ int exa_ctx_set_precision(ExaCtx& c, int mode) {
     EXA_TRY(dev_alloc(c, &c.Dinv32, ne * n * n));
     if (c.preconditioner == 0)
       EXA_TRY(dev_alloc(c, &c.Pc32, (size_t)P.ncu * P.npf * P.ncu * P.npf * P.nf));
+    else if (c.preconditioner == 2)
+      EXA_TRY(dev_alloc(c, &c.Pc32, (size_t)P.ncu * P.npf * P.ncu * P.npf * c.bilu.nse * c.bilu.nnz));
     else
       EXA_TRY(dev_alloc(c, &c.Pc32, ne * m * m));
     c.d_uflag = c.d_flag + 1;
@@ -422,7 +461,10 @@ bool field(ExaCtx& c, const char* name, FieldRef& f) {
   else if (s == "b") f = {c.b, N};
   else if (s == "x") f = {c.x, N};
   else if (s == "sdg") f = {c.sdg, n * ne};
-  else if (s == "P") f = {c.Pc, c.preconditioner == 0 ? (long long)P.ncu * P.npf * P.ncu * P.npf * P.nf : m * m * ne};
+  else if (s == "P")
+    f = {c.Pc, c.preconditioner == 0   ? (long long)P.ncu * P.npf * P.ncu * P.npf * P.nf
+               : c.preconditioner == 2 ? (long long)P.ncu * P.npf * P.ncu * P.npf * c.bilu.nse * c.bilu.nnz
+                                       : m * m * ne};
   else if (s == "MinvC") f = {c.MC, P.ncq > 0 ? (long long)P.npe * P.npe * P.nd * ne : 0};
   else if (s == "MinvE") f = {c.ME, P.ncq > 0 ? (long long)P.npe * P.ndf * P.nd * ne : 0};
   else if (s == "elemg") f = {c.elemg, (long long)P.elemg_stride() * ne};
@@ -715,6 +757,26 @@ extern "C" int exa_connectivity_host(const int* t, const int* bf, const int* per
   std::memcpy(elemcon, conn.elemcon.data(), sizeof(int) * conn.elemcon.size());
   *nf0 = conn.nf0;
   return nf;
+}
+
+extern "C" int exa_bilu0_ordering(const int* cartgridpart, int ncgp, const int* f2e, int nf, int nfe, int ne,
+                                  int* row_ptr, int cap_row_ptr, int* col_ind, int cap_col_ind, int* face,
+                                  int cap_face, int* nse) {
+  ExaBilu b;
+  char msg[256] = "";
+  if (exa_bilu_setup(cartgridpart, ncgp, f2e, nf, nfe, ne, b, msg, sizeof(msg)) != 0) {
+    exa_set_error("block ILU(0): %s", msg);
+    return -EXA_ERR_ARG;
+  }
+  if (b.nfse + 1 > cap_row_ptr || b.nnz > cap_col_ind || (long long)b.nse * b.nfse > cap_face) {
+    exa_set_error("block ILU(0) ordering: output buffers too small");
+    return -EXA_ERR_ARG;
+  }
+  std::memcpy(row_ptr, b.row_ptr.data(), sizeof(int) * b.row_ptr.size());
+  std::memcpy(col_ind, b.col_ind.data(), sizeof(int) * b.col_ind.size());
+  std::memcpy(face, b.face.data(), sizeof(int) * b.face.size());
+  *nse = b.nse;
+  return b.nfse;
 }
 
 // Batched FP64 primitives on device pointers (the kernels the assembly uses).

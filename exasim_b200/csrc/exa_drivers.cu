@@ -84,6 +84,11 @@ int exa_drv_norm(ExaCtx& c, const double* x, long long n, double* out) {
 int exa_drv_build_precond(ExaCtx& c) {
   const ExaDims& P = c.P;
   ExaProfScope ps(c, EXA_PH_PRECOND_BUILD);
+  if (c.preconditioner == 2) {
+    // super-element additive Schwarz with block ILU(0) (matvec.cpp:119-166)
+    if (c.precision == 1) return exa_k_bilu_build(P, c.bilu, c.f2e, c.elemcon, c.H32, c.Pc32, c.d_flag, c.st);
+    return exa_k_bilu_build(P, c.bilu, c.f2e, c.elemcon, c.H, c.Pc, c.d_flag, c.st);
+  }
   if (c.precision == 1) {
     // mixed form: blocks from the FP32 condensed matrix, inverted in FP32
     if (c.preconditioner == 0) {
@@ -155,6 +160,10 @@ int exa_drv_matvec(ExaCtx& c, const double* v, double* w) {
 // w = P v (ApplyPreconditioner, preconditioner.cpp:273-295); v and w may not alias
 int exa_drv_precond(ExaCtx& c, const double* v, double* w) {
   ExaProfScope ps(c, EXA_PH_PRECOND_APPLY);
+  if (c.preconditioner == 2) {
+    if (c.precision == 1) return exa_k_bilu_apply(c.P, c.bilu, c.Pc32, v, w, c.st);
+    return exa_k_bilu_apply(c.P, c.bilu, c.Pc, v, w, c.st);
+  }
   if (c.precision == 1) {
     if (c.preconditioner == 0) return exa_k_bj_apply(c.P, c.Pc32, v, w, c.st);
     EXA_TRY(exa_k_elem_matvec(c.P, c.elemcon, c.Pc32, v, c.we, c.st));

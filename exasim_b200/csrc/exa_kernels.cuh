@@ -40,6 +40,24 @@ struct UPacked;
 bool exa_vol_mat_tc_fits(const ExaDims& P);
 int exa_k_vol_mat_tc(const ExaDims& P, const double* shapegw, const UPacked& Sp, const double* rgJ, double* D,
                      double* B, int nb, int* flag, cudaStream_t st);
+// Block ILU(0) preconditioner on Cartesian sub-domains (Exasim preconditioner = 2): the
+// schedule built on the host (exa_bilu0.h) in device memory, and the sub-domain results.
+struct ExaBiluDev {
+  int nse = 0, nfse = 0, nnz = 0;
+  int *row_ptr = nullptr, *col_ind = nullptr, *face = nullptr, *row_of = nullptr;
+  int *fac_ptr = nullptr, *fac_ji = nullptr, *upd_ptr = nullptr, *upd_jl = nullptr, *upd_il = nullptr;
+  int *gf_ptr = nullptr, *gf_pos = nullptr;
+  double* out = nullptr;  // [nse * nfse, ncf]
+};
+size_t exa_bilu_apply_smem(int ncf, int nfse);
+// blocks from the condensed element matrices H, then the block ILU(0) in place
+template <typename T>
+int exa_k_bilu_build(const ExaDims& P, const ExaBiluDev& b, const int* f2e, const int* elemcon, const T* H, T* BE,
+                     int* flag, cudaStream_t st);
+// w = P x (x and w trace vectors, x != w)
+template <typename T>
+int exa_k_bilu_apply(const ExaDims& P, const ExaBiluDev& b, const T* BE, const double* x, double* w,
+                     cudaStream_t st);
 // y = (float) x
 int exa_k_to_f32(const double* x, float* y, long long n, cudaStream_t st);
 int exa_k_udg_update(const ExaDims& P, double* udg, const double* du, double alpha, cudaStream_t st);

@@ -85,6 +85,9 @@ struct ExaCtx {
   // the q elimination), D^-1 (A), F (B of D^-1 F), K (A) and D^-1 F (B of K D^-1 F)
   UPacked MCp{}, MEp{}, wBp{}, wGp{}, Dinvp{}, wFp{}, Kp{}, DinvFp{};
   UPacked Sp{};  // shapegt[:, :, 0] as the B operand of the tensor-core volume kernel
+  // block ILU(0) on Cartesian sub-domains (preconditioner 2): blocks in Pc / Pc32
+  std::vector<int> cartgridpart;
+  ExaBiluDev bilu;
 
   long long ndofuhat() const { return (long long)P.ncu * P.npf * P.nf; }
 };

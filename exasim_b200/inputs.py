@@ -483,6 +483,20 @@ def square_quad_grid(n: int, L: float = 1.0) -> Grid:
     return Grid(p=p, t=np.array(t, dtype=np.int64).T, elemtype=1)
 
 
+def square_quad_grid(n: int, L: float = 1.0) -> Grid:
+    """Square of n^2 quadrilaterals, element i + n*j (vertices counter-clockwise)."""
+    xs = np.linspace(0.0, L, n + 1)
+    X, Y = np.meshgrid(xs, xs, indexing="ij")
+    p = np.vstack([X.ravel(order="F"), Y.ravel(order="F")])
+    m = n + 1
+    t = []
+    for j in range(n):
+        for i in range(n):
+            v0 = i + m * j
+            t.append([v0, v0 + 1, v0 + 1 + m, v0 + m])
+    return Grid(p=p, t=np.array(t, dtype=np.int64).T, elemtype=1)
+
+
 def cube_hex_grid(n: int, L: float = 1.0) -> Grid:
     """Unit cube of n^3 hexahedra (vertex order of Exasim's hex: bottom face CCW, then top)."""
     xs = np.linspace(0.0, L, n + 1)

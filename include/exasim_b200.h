@@ -116,6 +116,14 @@ int exa_last_residual(exa_ctx* ctx, double* initial, double* final_norm);
  * synchronises the context stream. */
 int exa_profile(exa_ctx* ctx, int enable);
 int exa_profile_read(exa_ctx* ctx, int nphase, double* ms, long long* count, double* flops);
+/* Sub-domain face ordering of the block ILU(0) preconditioner (preconditioner 2) on the host:
+ * the Cartesian partition of cartgridpart ([2, Nx, Ny, Mx, My, opt] or [3, Nx, Ny, Nz, Mx, My,
+ * Mz, opt], gridpartition2d/3d, backend/Common/cpuimpl.h:1332-1496) and the face ordering of a
+ * sub-domain (crs_faceordering, cpuimpl.h:1266-1330) for the face connectivity f2e [4, nf]:
+ * row_ptr [nfse + 1] and col_ind (CRS, diagonal first) and face [nse, nfse] (column-major).
+ * Returns nfse, or a negated status. */
+int exa_bilu0_ordering(const int* cartgridpart, int ncgp, const int* f2e, int nf, int nfe, int ne, int* row_ptr,
+                       int cap_row_ptr, int* col_ind, int cap_col_ind, int* face, int cap_face, int* nse);
 /* out[4] = {last GMRES iterations, last Newton iterations, GMRES iterations of the last solve, 0} */
 int exa_stats(exa_ctx* ctx, long long* out);
 int exa_synchronize(exa_ctx* ctx);

@@ -176,6 +176,8 @@ class HDGOracle:
         self.bf = _F(me[25], (self.nfe, self.ne)).astype(np.int64)
         nve = ns[26] // self.ne
         self.t = _F(me[27], (nve, self.ne)).astype(np.int64)
+        # Cartesian sub-domains for block ILU(0) (readbinaryfiles.cpp:356)
+        self.cartgridpart = me[26].astype(np.int64) if ns[25] > 0 else np.zeros(0, dtype=np.int64)
 
         s = _read_blob(os.path.join(d, "sol.bin"))
         self.xdg = _F(s[2], (npe, self.ncx, self.ne))
@@ -610,13 +612,22 @@ class HDGOracle:
                 BE[:, l2[f], :, l2[f], e2[f]] = sub
             self.P = _inverse(BE.reshape(ncf * nfe, ncf * nfe, self.ne, order="F"))
         else:
-            raise NotImplementedError("block ILU(0) preconditioner")
+            # super-element additive Schwarz with block ILU(0) (matvec.cpp:119-166)
+            from oracle.bilu0 import BlockILU0
+            if self.cartgridpart.size == 0:
+                raise ValueError("block ILU(0) needs cartgridpart in mesh.bin")
+            self.bilu = BlockILU0(self.cartgridpart, self.f2e, self.elemcon, ncu, npf, nfe)
+            m = ncf * nfe
+            self.P = self.bilu.factor(self.bilu.assemble(self.H.reshape(m, m, self.ne, order="F")))
 
     def apply_precond(self, x):
         if self.preconditioner == 0:
             X = x.reshape(self.ncu * self.npf, self.nf, order="F")
             y = np.einsum("ijf,jf->if", self.P, X)
             return y.reshape(x.shape, order="F")
+        if self.preconditioner == 2:
+            X = x.reshape(self.ncu * self.npf, self.nf, order="F")
+            return self.bilu.apply(self.P, X).reshape(x.shape, order="F")
         return self.matvec(x, self.P)
 
     # -------------------------------------------------------------------- GMRES
