@@ -8,6 +8,14 @@ Exasim datain/ folders (app, master, mesh, sol .bin) by exasim_b200.inputs.
 * convdiff3d_hex: 3D convection-diffusion, p=4 hexahedra on an n^3 grid of the unit cube,
                   c = (1, 0.5, 0.25), kappa = 0.01, Gaussian source at the centre (sigma 0.1),
                   u = 0 on the boundary, DIRK(3,3) with dt = 0.01; block Jacobi; GMRES(50) to 1e-8
+* ns2d_tgv_quad : 2D compressible Navier-Stokes, Taylor-Green vortex on the periodic [0, 2 pi]^2,
+                  p=3 quadrilaterals, Mach 0.1, Re 1600, gamma 1.4, Pr 0.72, DIRK(3,3) dt 0.05,
+                  Newton to 1e-8, GMRES(100) with block ILU(0) on 4 x 4-element sub-domains
+* euler3d_vortex_hex: 3D Euler (no q), isentropic vortex of strength 5 on the periodic
+                  [-5, 5]^3, p=3 hexahedra (320 x 320 element blocks), Mach 0.5, DIRK(2,2)
+* cdsin2d_quad  : one request of the served stream: 2D convection-diffusion on the unit square,
+                  kappa, velocity (cos theta, sin theta), source sin(a pi x) sin(b pi y), u = 0,
+                  one Newton step, block Jacobi GMRES
 """
 from __future__ import annotations
 
@@ -65,3 +73,41 @@ def convdiff3d_hex(datain: str, n: int = 16, porder: int = 4, nsteps: int = 20, 
                    physicsparam=[0.01, 1.0, 0.5, 0.25, 0.5, 0.5, 0.5, 0.1], externalparam=[0.0, 0.0])
     exprs = [_on(2, 0.0), _on(2, 1.0), _on(1, 0.0), _on(0, 1.0), _on(1, 1.0), _on(0, 0.0)]
     return write_case(datain, grid, master, app, exprs, [1, 1, 1, 1, 1, 1], cartgridpart)
+
+
+def ns2d_tgv_quad(datain: str, n: int = 64, porder: int = 3, nsteps: int = 10, dt: float = 0.05,
+                  preconditioner: int = 2, block: int = 4, restart: int = 100, gmres_tol: float = 1e-8,
+                  newton_tol: float = 1e-8, mach: float = 0.1, tau: float = 2.0):
+    grid = I.periodic_square_quad_grid(n, 0.0, 2 * np.pi)
+    master = I.make_master(2, 1, porder, 2 * porder)
+    app = I.PDEApp(nd=2, ncu=4, model="ModelD", preconditioner=preconditioner, NewtonIter=20,
+                   NewtonTol=newton_tol, GMRESiter=1000, GMRESrestart=restart, GMREStol=gmres_tol,
+                   RBdim=0, ppdegree=1, tau=[tau], torder=3, nstage=3, dt=[dt] * nsteps,
+                   physicsparam=[1.4, 1600.0, 0.72, mach], externalparam=[0.0, 0.0])
+    cgp = (2, n, n, block, block, 0) if preconditioner == 2 else ()
+    return write_case(datain, grid, master, app, [], [], cgp)
+
+
+def euler3d_vortex_hex(datain: str, n: int = 32, porder: int = 3, nsteps: int = 5, dt: float = 0.05,
+                       preconditioner: int = 0, restart: int = 50, gmres_tol: float = 1e-8,
+                       newton_tol: float = 1e-8, mach: float = 0.5):
+    grid = I.periodic_cube_hex_grid(n, -5.0, 10.0)
+    master = I.make_master(3, 1, porder, 2 * porder)
+    app = I.PDEApp(nd=3, ncu=5, model="ModelC", preconditioner=preconditioner, NewtonIter=20,
+                   NewtonTol=newton_tol, GMRESiter=1000, GMRESrestart=restart, GMREStol=gmres_tol,
+                   RBdim=0, ppdegree=1, tau=[1.0 + 1.0 / mach], torder=2, nstage=2, dt=[dt] * nsteps,
+                   physicsparam=[1.4, mach], externalparam=[0.0, 0.0])
+    return write_case(datain, grid, master, app, [], [])
+
+
+def cdsin2d_quad(datain: str, n: int = 16, porder: int = 3, kappa: float = 0.01, theta: float = 0.0,
+                 a: int = 1, b: int = 1, gmres_tol: float = 1e-8, restart: int = 50, preconditioner: int = 0):
+    grid = I.square_quad_grid(n)
+    master = I.make_master(2, 1, porder, 2 * porder)
+    app = I.PDEApp(nd=2, ncu=1, model="ModelD", preconditioner=preconditioner, NewtonIter=1,
+                   NewtonTol=1e-8, GMRESiter=1000, GMRESrestart=restart, GMREStol=gmres_tol,
+                   RBdim=0, ppdegree=1, tau=[1.0],
+                   physicsparam=[kappa, float(np.cos(theta)), float(np.sin(theta)), float(a), float(b)],
+                   externalparam=[0.0, 0.0])
+    exprs = [_on(1, 0.0), _on(0, 1.0), _on(1, 1.0), _on(0, 0.0)]
+    return write_case(datain, grid, master, app, exprs, [1, 1, 1, 1])

@@ -189,6 +189,15 @@ int exa_ctx_init(ExaCtx& c, const double* app, long long napp, const double* mas
   }
   P.nf = conn.nf;
   P.nf0 = conn.nf0;
+  if (P.n > exa_inverse_max_n()) {
+    exa_set_error("element blocks of order %d exceed the dense inverse's limit %d", P.n, exa_inverse_max_n());
+    return EXA_ERR_UNSUPPORTED;
+  }
+  if ((c.preconditioner == 0 && P.ncu * P.npf > 160) || (c.preconditioner == 1 && P.m > 160)) {
+    exa_set_error("preconditioner %d: its blocks (order %d) exceed 160", c.preconditioner,
+                  c.preconditioner == 0 ? P.ncu * P.npf : P.m);
+    return EXA_ERR_UNSUPPORTED;
+  }
 
   // ---- sol.bin (readsolstruct, readbinaryfiles.cpp:499-618)
   if (S.nsize[1] != (long long)P.npe * P.ncx * P.ne) { exa_set_error("sol.bin xdg size mismatch"); return EXA_ERR_ARG; }
@@ -325,8 +334,9 @@ int exa_ctx_init(ExaCtx& c, const double* app, long long napp, const double* mas
   else
     EXA_TRY(dev_alloc(c, &c.Pc, ne * m * m));
   // element chunk: bounded workspace (about 8 GB at most)
+  const size_t inv_ws = exa_inverse_needs_ws((int)n) ? n * n : 0;
   const size_t per_elem = sizeof(double) * (n * n + n * nqn + n * m + m * n + m * nqn +
-                                            (size_t)P.nge * (P.nd + 1) * P.ncu * P.nc + n);
+                                            (size_t)P.nge * (P.nd + 1) * P.ncu * P.nc + n + inv_ws);
   size_t cap = (size_t)8 << 30;
   c.neb = (int)std::max<size_t>(1, std::min<size_t>(std::min<size_t>(ne, cap / per_elem), 65535));
   const size_t nb = c.neb;
@@ -337,6 +347,7 @@ int exa_ctx_init(ExaCtx& c, const double* app, long long napp, const double* mas
   EXA_TRY(dev_alloc(c, &c.wG, std::max<size_t>(1, nb * m * nqn)));
   EXA_TRY(dev_alloc(c, &c.wRg, nb * P.nge * (P.nd + 1) * P.ncu * P.nc));
   EXA_TRY(dev_alloc(c, &c.wRu, nb * n));
+  if (inv_ws) EXA_TRY(dev_alloc(c, &c.wInv, nb * inv_ws));
   EXA_TRY(dev_alloc(c, &c.V, N * (size_t)(c.restart + 1)));
   EXA_TRY(dev_alloc(c, &c.x, N));
   EXA_TRY(dev_alloc(c, &c.r, N));
@@ -368,6 +379,10 @@ int exa_ctx_set_precision(ExaCtx& c, int mode) {
   if (mode != 0 && mode != 1) {
     exa_set_error("precision mode %d: 0 (FP64) or 1 (FP32/TF32 elimination with FP64 refinement)", mode);
     return EXA_ERR_ARG;
+  }
+  if (mode == 1 && exa_inverse_needs_ws(c.P.n)) {
+    exa_set_error("the FP32 element elimination covers element blocks up to order 160 (this mesh: %d)", c.P.n);
+    return EXA_ERR_UNSUPPORTED;
   }
   if (mode == 1 && c.H32 == nullptr) {
     const ExaDims& P = c.P;
@@ -844,5 +859,16 @@ extern "C" int exa_gemm_3xtf32_batched(int M, int N, int K, double alpha, const 
 }
 
 extern "C" int exa_dinverse_batched(double* A, int n, long long stride, int batch, int* info_dev, void* stream) {
-  return exa_inverse(A, n, stride, batch, info_dev, (cudaStream_t)stream);
+  if (!exa_inverse_needs_ws(n) || batch <= 0) return exa_inverse(A, n, stride, batch, info_dev, (cudaStream_t)stream);
+  if (n > exa_inverse_max_n()) {
+    exa_set_error("dense inverse of order %d exceeds %d", n, exa_inverse_max_n());
+    return EXA_ERR_UNSUPPORTED;
+  }
+  // blocked orders: a temporary workspace of n^2 per matrix, freed after the stream drains
+  cudaStream_t st = (cudaStream_t)stream;
+  double* ws = nullptr;
+  EXA_CUDA(cudaMallocAsync((void**)&ws, sizeof(double) * (size_t)n * n * batch, st));
+  const int s = exa_inverse_ws(A, n, stride, batch, ws, info_dev, st);
+  cudaFreeAsync(ws, st);
+  return s;
 }

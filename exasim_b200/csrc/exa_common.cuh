@@ -80,6 +80,13 @@ int exa_gemm(const GemmBatch& g, cudaStream_t st);
 // *d_flag (device int) non-zero when a pivot is exactly zero.
 int exa_inverse(double* A, int n, long long stride, int batch, int* d_flag, cudaStream_t st);
 int exa_inverse(float* A, int n, long long stride, int batch, int* d_flag, cudaStream_t st);
+// The same for n up to exa_inverse_max_n(): orders above the register kernel's limit
+// (exa_inverse_needs_ws) are inverted blockwise and need ws, n^2 entries per matrix,
+// spaced n^2 apart.
+int exa_inverse_max_n();
+int exa_inverse_needs_ws(int n);
+int exa_inverse_ws(double* A, int n, long long stride, int batch, double* ws, int* d_flag, cudaStream_t st);
+int exa_inverse_ws(float* A, int n, long long stride, int batch, float* ws, int* d_flag, cudaStream_t st);
 
 // Vector kernels for the Krylov solver.  Reductions are deterministic: each block
 // writes a partial sum and consumers reduce the partial array in a fixed order.

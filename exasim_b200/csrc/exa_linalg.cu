@@ -408,6 +408,157 @@ int exa_inverse(float* A, int n, long long stride, int batch, int* d_flag, cudaS
 }
 
 // ----------------------------------------------------------------------------------
+// blocked inverse for INV_MAX_N < n <= 2 INV_MAX_N (e.g. 320 x 320 blocks of 3D Euler at
+// p = 3), by the 2 x 2 block formula with n1 = n/2 rounded up and n2 = n - n1:
+//   X = A11^-1 (Gauss-Jordan, pivoting within the block), W1 = X A12, S = A22 - A21 W1,
+//   Y = S^-1, W3 = A21 X;  inverse = [X + W1 Y W3, -W1 Y; -Y W3, Y].
+// The products run on the FP64 DMMA GEMM (or an FP32 SIMT GEMM for the FP32 blocks).
+// Workspace: n^2 entries per matrix.
+// ----------------------------------------------------------------------------------
+namespace {
+// C(r, c) = alpha sum_k A(r, k) B(k, c) + beta C(r, c), one batch entry per blockIdx.y;
+// 64 x 64 tiles, 256 threads with 4 x 4 outputs each, K in steps of 16 through shared memory
+template <typename T>
+__global__ void __launch_bounds__(256) simt_gemm_kernel(int M, int N, int K, T alpha, T beta, const T* A,
+                                                        long long lda, long long sA, const T* B, long long ldb,
+                                                        long long sB, T* C, long long ldc, long long sC) {
+  __shared__ T as[16][65], bs[16][65];
+  const long long b = blockIdx.y;
+  A += b * sA;
+  B += b * sB;
+  C += b * sC;
+  const int tilesM = (M + 63) / 64;
+  const int r0 = (blockIdx.x % tilesM) * 64, c0 = (blockIdx.x / tilesM) * 64;
+  const int tr = threadIdx.x & 15, tc = threadIdx.x >> 4;
+  T acc[4][4] = {};
+  for (int k0 = 0; k0 < K; k0 += 16) {
+    for (int t = threadIdx.x; t < 16 * 64; t += 256) {
+      const int kk = t >> 6, rr = t & 63;
+      as[kk][rr] = (r0 + rr < M && k0 + kk < K) ? A[(r0 + rr) + lda * (k0 + kk)] : T(0);
+      bs[kk][rr] = (c0 + rr < N && k0 + kk < K) ? B[(k0 + kk) + ldb * (c0 + rr)] : T(0);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < 16; ++kk) {
+      T av[4], bv[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) av[i] = as[kk][tr + 16 * i];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) bv[j] = bs[kk][tc + 16 * j];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] += av[i] * bv[j];
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int r = r0 + tr + 16 * i, c = c0 + tc + 16 * j;
+      if (r < M && c < N) {
+        T* p = C + r + ldc * c;
+        *p = (beta == T(0)) ? alpha * acc[i][j] : alpha * acc[i][j] + beta * (*p);
+      }
+    }
+}
+
+// batched sub-matrix copy: dst(r, c) = src(r, c) for r < R, c < Cn
+template <typename T>
+__global__ void submat_copy_kernel(T* dst, long long ldd, long long sd, const T* src, long long lds, long long ss,
+                                   int R, int Cn) {
+  const long long b = blockIdx.y;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < R * Cn; t += gridDim.x * blockDim.x) {
+    const int r = t % R, c = t / R;
+    dst[b * sd + r + ldd * c] = src[b * ss + r + lds * c];
+  }
+}
+
+template <typename T>
+int bgemm(int M, int N, int K, T alpha, T beta, const T* A, long long lda, long long sA, const T* B, long long ldb,
+          long long sB, T* C, long long ldc, long long sC, int batch, cudaStream_t st) {
+  if constexpr (sizeof(T) == 8) {
+    GemmBatch g{M, N, K, alpha, beta, A, lda, sA, 0, B, ldb, sB, 0, C, ldc, sC, 0, batch, 1};
+    return exa_gemm(g, st);
+  } else {
+    for (int b0 = 0; b0 < batch; b0 += 65535) {
+      const int nb = (batch - b0 < 65535) ? batch - b0 : 65535;
+      dim3 grid((unsigned)(exa_ceil_div(M, 64) * exa_ceil_div(N, 64)), (unsigned)nb);
+      simt_gemm_kernel<T><<<grid, 256, 0, st>>>(M, N, K, alpha, beta, A + b0 * sA, lda, sA, B + b0 * sB, ldb, sB,
+                                                C + b0 * sC, ldc, sC);
+      EXA_LAUNCH_CHECK();
+    }
+    return EXA_OK;
+  }
+}
+
+template <typename T>
+int subcopy(T* dst, long long ldd, long long sd, const T* src, long long lds, long long ss, int R, int Cn, int batch,
+            cudaStream_t st) {
+  for (int b0 = 0; b0 < batch; b0 += 65535) {
+    const int nb = (batch - b0 < 65535) ? batch - b0 : 65535;
+    dim3 grid((unsigned)exa_ceil_div(R * Cn, 256 * 4), (unsigned)nb);
+    submat_copy_kernel<T><<<grid, 256, 0, st>>>(dst + b0 * sd, ldd, sd, src + b0 * ss, lds, ss, R, Cn);
+    EXA_LAUNCH_CHECK();
+  }
+  return EXA_OK;
+}
+
+template <typename T>
+int inverse_blocked(T* A, int n, long long stride, int batch, T* ws, int* d_flag, cudaStream_t st) {
+  const int n1 = (n + 1) / 2, n2 = n - n1;
+  const long long sw = (long long)n * n;
+  T* W0 = ws;                                  // n1 x n1: A11, then X
+  T* W1 = W0 + (long long)n1 * n1;             // n1 x n2: X A12
+  T* W2 = W1 + (long long)n1 * n2;             // n2 x n2: S, then Y
+  T* W3 = W2 + (long long)n2 * n2;             // n2 x n1: A21 X
+  T* A11 = A;
+  T* A21 = A + n1;
+  T* A12 = A + (long long)n * n1;
+  T* A22 = A + n1 + (long long)n * n1;
+  EXA_TRY(subcopy<T>(W0, n1, sw, A11, n, stride, n1, n1, batch, st));
+  EXA_TRY(inverse_dispatch<T>(W0, n1, sw, batch, d_flag, st));
+  EXA_TRY(bgemm<T>(n1, n2, n1, T(1), T(0), W0, n1, sw, A12, n, stride, W1, n1, sw, batch, st));
+  EXA_TRY(bgemm<T>(n2, n2, n1, T(-1), T(1), A21, n, stride, W1, n1, sw, A22, n, stride, batch, st));
+  EXA_TRY(subcopy<T>(W2, n2, sw, A22, n, stride, n2, n2, batch, st));
+  EXA_TRY(inverse_dispatch<T>(W2, n2, sw, batch, d_flag, st));
+  EXA_TRY(bgemm<T>(n2, n1, n1, T(1), T(0), A21, n, stride, W0, n1, sw, W3, n2, sw, batch, st));
+  EXA_TRY(bgemm<T>(n1, n2, n2, T(-1), T(0), W1, n1, sw, W2, n2, sw, A12, n, stride, batch, st));
+  EXA_TRY(subcopy<T>(A11, n, stride, W0, n1, sw, n1, n1, batch, st));
+  EXA_TRY(bgemm<T>(n1, n1, n2, T(-1), T(1), A12, n, stride, W3, n2, sw, A11, n, stride, batch, st));
+  EXA_TRY(bgemm<T>(n2, n1, n2, T(-1), T(0), W2, n2, sw, W3, n2, sw, A21, n, stride, batch, st));
+  EXA_TRY(subcopy<T>(A22, n, stride, W2, n2, sw, n2, n2, batch, st));
+  return EXA_OK;
+}
+
+template <typename T>
+int inverse_ws(T* A, int n, long long stride, int batch, T* ws, int* d_flag, cudaStream_t st) {
+  if (n <= INV_MAX_N || batch <= 0) return inverse_dispatch<T>(A, n, stride, batch, d_flag, st);
+  if (n > 2 * INV_MAX_N) {
+    exa_set_error("dense inverse of order %d exceeds the blocked kernel limit %d", n, 2 * INV_MAX_N);
+    return EXA_ERR_UNSUPPORTED;
+  }
+  if (!ws) {
+    exa_set_error("dense inverse of order %d needs a workspace of n^2 entries per matrix", n);
+    return EXA_ERR_ARG;
+  }
+  return inverse_blocked<T>(A, n, stride, batch, ws, d_flag, st);
+}
+}  // namespace
+
+int exa_inverse_max_n() { return 2 * INV_MAX_N; }
+int exa_inverse_needs_ws(int n) { return n > INV_MAX_N; }
+
+int exa_inverse_ws(double* A, int n, long long stride, int batch, double* ws, int* d_flag, cudaStream_t st) {
+  return inverse_ws<double>(A, n, stride, batch, ws, d_flag, st);
+}
+
+int exa_inverse_ws(float* A, int n, long long stride, int batch, float* ws, int* d_flag, cudaStream_t st) {
+  return inverse_ws<float>(A, n, stride, batch, ws, d_flag, st);
+}
+
+// ----------------------------------------------------------------------------------
 // vector kernels.  A fixed grid of VB blocks (two per SM) covers every vector with a
 // grid-stride loop; each reduction leaves VB partial sums that the consumer kernel
 // adds up in index order, so results do not depend on scheduling.

@@ -81,7 +81,7 @@ int schur_chunk(ExaCtx& c, int e0, int nb) {
   }
   {
     ExaProfScope ps(c, EXA_PH_INVERSE);
-    EXA_TRY(exa_inverse(c.wD, n, (long long)n * n, nb, c.d_flag, c.st));
+    EXA_TRY(exa_inverse_ws(c.wD, n, (long long)n * n, nb, c.wInv, c.d_flag, c.st));
   }
   ExaProfScope ps(c, EXA_PH_SCHUR);
   exa_prof_flops(c, EXA_PH_SCHUR, 2.0 * nb * ((double)n * n * m + (double)n * n + (double)m * m * n + (double)m * n));

@@ -51,6 +51,7 @@ struct ExaCtx {
   // assembly workspace for a chunk of `neb` elements
   int neb = 0;
   double *wD = nullptr, *wB = nullptr, *wF = nullptr, *wK = nullptr, *wG = nullptr, *wRg = nullptr, *wRu = nullptr;
+  double* wInv = nullptr;  // blocked-inverse workspace (n^2 per element) when n exceeds the register kernel
   // Krylov / Newton workspace
   double *V = nullptr, *x = nullptr, *r = nullptr, *w = nullptr, *we = nullptr, *du = nullptr;
   double *part_a = nullptr, *part_b = nullptr, *part_m = nullptr, *hess = nullptr, *gs = nullptr, *gcs = nullptr,

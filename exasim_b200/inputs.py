@@ -419,10 +419,20 @@ def elem_faces(dim: int, elemtype: int) -> np.ndarray:
 
 @dataclass
 class Grid:
-    """``grid.bin`` content: vertices p [nd, np] and elements t [nve, ne] (0-based)."""
+    """``grid.bin`` content: vertices p [nd, np] and elements t [nve, ne] (0-based).
+
+    ``tp``, when set, is t with the vertices of periodic boundaries identified (the vertex on
+    the far side replaced by its image on the near side), as the preprocessor's
+    ``setperiodicfaces`` leaves it (makemesh.cpp:593-760): connectivity is built from tp,
+    so periodic faces join their two elements, while the element nodes (xdg) come from t."""
     p: np.ndarray
     t: np.ndarray
     elemtype: int
+    tp: Optional[np.ndarray] = None
+
+    @property
+    def tconn(self):
+        return self.t if self.tp is None else self.tp
 
     @property
     def nd(self):
@@ -472,18 +482,6 @@ def square_tri_grid(n: int, perturb: float = 0.0, seed: int = 0) -> Grid:
 
 
 def square_quad_grid(n: int, L: float = 1.0) -> Grid:
-    xs = np.linspace(0.0, L, n + 1)
-    X, Y = np.meshgrid(xs, xs, indexing="ij")
-    p = np.vstack([X.ravel(order="F"), Y.ravel(order="F")])
-    t = []
-    for j in range(n):
-        for i in range(n):
-            v0 = i + (n + 1) * j
-            t.append([v0, v0 + 1, v0 + n + 2, v0 + n + 1])
-    return Grid(p=p, t=np.array(t, dtype=np.int64).T, elemtype=1)
-
-
-def square_quad_grid(n: int, L: float = 1.0) -> Grid:
     """Square of n^2 quadrilaterals, element i + n*j (vertices counter-clockwise)."""
     xs = np.linspace(0.0, L, n + 1)
     X, Y = np.meshgrid(xs, xs, indexing="ij")
@@ -495,6 +493,34 @@ def square_quad_grid(n: int, L: float = 1.0) -> Grid:
             v0 = i + m * j
             t.append([v0, v0 + 1, v0 + 1 + m, v0 + m])
     return Grid(p=p, t=np.array(t, dtype=np.int64).T, elemtype=1)
+
+
+def _periodic_ids(t, n, nd):
+    """Structured vertex ids i + (n+1) j (+ (n+1)^2 k) with every coordinate index taken mod n."""
+    m = n + 1
+    idx = [t % m, (t // m) % m] + ([t // (m * m)] if nd == 3 else [])
+    out = np.zeros_like(t)
+    s = 1
+    for k in range(nd):
+        out += (idx[k] % n) * s
+        s *= m
+    return out
+
+
+def periodic_square_quad_grid(n: int, x0: float = 0.0, L: float = 1.0) -> Grid:
+    """n^2 quadrilaterals on [x0, x0+L]^2, periodic in x and y."""
+    g = square_quad_grid(n, L)
+    g.p = g.p + x0
+    g.tp = _periodic_ids(g.t, n, 2)
+    return g
+
+
+def periodic_cube_hex_grid(n: int, x0: float = 0.0, L: float = 1.0) -> Grid:
+    """n^3 hexahedra on [x0, x0+L]^3, periodic in x, y and z."""
+    g = cube_hex_grid(n, L)
+    g.p = g.p + x0
+    g.tp = _periodic_ids(g.t, n, 3)
+    return g
 
 
 def cube_hex_grid(n: int, L: float = 1.0) -> Grid:
@@ -518,7 +544,7 @@ def boundary_faces(grid: Grid) -> np.ndarray:
     nd, et = grid.nd, grid.elemtype
     lf = elem_faces(nd, et)
     nvf, nfe = lf.shape
-    keys = np.sort(grid.t[lf.T.reshape(-1)].reshape(nfe, nvf, grid.ne), axis=1)   # [nfe, nvf, ne]
+    keys = np.sort(grid.tconn[lf.T.reshape(-1)].reshape(nfe, nvf, grid.ne), axis=1)   # [nfe, nvf, ne]
     keys = np.transpose(keys, (2, 0, 1)).reshape(-1, nvf)                      # (e, l) rows
     _, inv, cnt = np.unique(keys, axis=0, return_inverse=True, return_counts=True)
     shared = cnt[inv.ravel()] > 1
@@ -559,7 +585,7 @@ def write_mesh_bin(fn: str, grid: Grid, master: Master, bf: np.ndarray, bcs: Seq
     ndims = np.zeros(20)
     ndims[0] = grid.nd
     ndims[1] = ne
-    ndims[3] = int(grid.t.max()) + 1
+    ndims[3] = int(grid.tconn.max()) + 1
     ndims[4] = master.nfe
     nsize = np.zeros(50)
     nsize[0] = 20
@@ -571,7 +597,7 @@ def write_mesh_bin(fn: str, grid: Grid, master: Master, bf: np.ndarray, bcs: Seq
     nsize[26] = ne * nve
     nsize[27] = len(bcs)
     nsize[28] = 4
-    parts = [ndims, np.arange(ne), [ne], master.perm, bf, list(cartgridpart), grid.t,
+    parts = [ndims, np.arange(ne), [ne], master.perm, bf, list(cartgridpart), grid.tconn,
              list(bcs), [ne, 0, 0, 0]]
     _write_blob(fn, nsize, parts)
 

@@ -1,0 +1,27 @@
+void HdgFbouonly1(dstype* f, const dstype* x, const dstype* uq, const dstype* v, const dstype* w, const dstype* uhat, const dstype* n, const dstype* tau, const dstype* eta, const dstype* mu, const dstype t, const int modelnumber, const int N, const int szx, const int szuq, const int szv, const int szw, const int szuhat, const int szn, const int sztau, const int szeta, const int szmu)
+{
+
+  Kokkos::parallel_for("FbouHdg", N, KOKKOS_LAMBDA(const size_t i) {
+    dstype x0 = x[0*N+i];
+    dstype x1 = x[1*N+i];
+    dstype uq0 = uq[0*N+i];
+    dstype uq1 = uq[1*N+i];
+    dstype uq2 = uq[2*N+i];
+    dstype uhat0 = uhat[0*N+i];
+    dstype n0 = n[0*N+i];
+    dstype n1 = n[1*N+i];
+    dstype tau0 = tau[0];
+    dstype mu0 = mu[0];
+    dstype mu1 = mu[1];
+    dstype mu2 = mu[2];
+    dstype mu3 = mu[3];
+    dstype mu4 = mu[4];
+
+    f[0 * N + i] = -tau0*uhat0;
+  });
+}
+
+void HdgFbouonly(dstype* f, const dstype* xdg, const dstype* udg, const dstype* odg, const dstype* wdg, const dstype* uhg, const dstype* nlg, const dstype* tau, const dstype* uinf, const dstype* param, const dstype time, const int modelnumber, const int ib, const int ng, const int nc, const int ncu, const int nd, const int ncx, const int nco, const int ncw) {
+    if (ib == 1 )
+        HdgFbouonly1(f, xdg, udg, odg, wdg, uhg, nlg, tau, uinf, param, time, modelnumber, ng, nc, ncu, nd, ncx, nco, ncw, nc, ncu, nd);
+}

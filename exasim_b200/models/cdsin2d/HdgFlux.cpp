@@ -1,0 +1,25 @@
+void HdgFlux(dstype* f, dstype* J1, dstype* J2, const dstype* x, const dstype* uq, const dstype* v, const dstype* w, const dstype* eta, const dstype* mu, const dstype t, const int modelnumber, const int N, const int szx, const int szuq, const int szv, const int szw, const int szeta, const int szmu)
+{
+
+  Kokkos::parallel_for("Flux", N, KOKKOS_LAMBDA(const size_t i) {
+    dstype x0 = x[0*N+i];
+    dstype x1 = x[1*N+i];
+    dstype uq0 = uq[0*N+i];
+    dstype uq1 = uq[1*N+i];
+    dstype uq2 = uq[2*N+i];
+    dstype mu0 = mu[0];
+    dstype mu1 = mu[1];
+    dstype mu2 = mu[2];
+    dstype mu3 = mu[3];
+    dstype mu4 = mu[4];
+
+    f[0 * N + i] = mu0*uq1 + mu1*uq0;
+    f[1 * N + i] = mu0*uq2 + mu2*uq0;
+    J1[0 * N + i] = mu1;
+    J1[1 * N + i] = mu2;
+    J1[2 * N + i] = mu0;
+    J1[3 * N + i] = 0;
+    J1[4 * N + i] = 0;
+    J1[5 * N + i] = mu0;
+  });
+}

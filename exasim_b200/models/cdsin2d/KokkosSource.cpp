@@ -1,0 +1,18 @@
+void KokkosSource(dstype* f, const dstype* x, const dstype* uq, const dstype* v, const dstype* w, const dstype* eta, const dstype* mu, const dstype t, const int modelnumber, const int N, const int szx, const int szuq, const int szv, const int szw, const int szeta, const int szmu)
+{
+
+  Kokkos::parallel_for("Source", N, KOKKOS_LAMBDA(const size_t i) {
+    dstype x0 = x[0*N+i];
+    dstype x1 = x[1*N+i];
+    dstype uq0 = uq[0*N+i];
+    dstype uq1 = uq[1*N+i];
+    dstype uq2 = uq[2*N+i];
+    dstype mu0 = mu[0];
+    dstype mu1 = mu[1];
+    dstype mu2 = mu[2];
+    dstype mu3 = mu[3];
+    dstype mu4 = mu[4];
+
+    f[0 * N + i] = sin(M_PI*mu3*x0)*sin(M_PI*mu4*x1);
+  });
+}

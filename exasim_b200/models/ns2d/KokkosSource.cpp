@@ -1,0 +1,29 @@
+void KokkosSource(dstype* f, const dstype* x, const dstype* uq, const dstype* v, const dstype* w, const dstype* eta, const dstype* mu, const dstype t, const int modelnumber, const int N, const int szx, const int szuq, const int szv, const int szw, const int szeta, const int szmu)
+{
+
+  Kokkos::parallel_for("Source", N, KOKKOS_LAMBDA(const size_t i) {
+    dstype x0 = x[0*N+i];
+    dstype x1 = x[1*N+i];
+    dstype uq0 = uq[0*N+i];
+    dstype uq1 = uq[1*N+i];
+    dstype uq2 = uq[2*N+i];
+    dstype uq3 = uq[3*N+i];
+    dstype uq4 = uq[4*N+i];
+    dstype uq5 = uq[5*N+i];
+    dstype uq6 = uq[6*N+i];
+    dstype uq7 = uq[7*N+i];
+    dstype uq8 = uq[8*N+i];
+    dstype uq9 = uq[9*N+i];
+    dstype uq10 = uq[10*N+i];
+    dstype uq11 = uq[11*N+i];
+    dstype mu0 = mu[0];
+    dstype mu1 = mu[1];
+    dstype mu2 = mu[2];
+    dstype mu3 = mu[3];
+
+    f[0 * N + i] = 0;
+    f[1 * N + i] = 0;
+    f[2 * N + i] = 0;
+    f[3 * N + i] = 0;
+  });
+}
