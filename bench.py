@@ -45,8 +45,11 @@ def parse():
     ap.add_argument("--n", type=int, default=CFG_N, help="elements per cube edge")
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--form", default="both", choices=["both", "mixed", "plain"],
+    ap.add_argument("--form", default="both", choices=["both", "mixed", "plain", "served"],
                     help="time both forms (default) or one; one form prints a partial line, for profiling")
+    ap.add_argument("--serve-requests", type=int, default=200,
+                    help="requests per configuration of the served-stream leg (0 skips it)")
+    ap.add_argument("--serve-slots", type=int, default=8)
     return ap.parse_args()
 
 
@@ -277,6 +280,16 @@ def run_ours(args):
         s64 = HDGSolver(d, "convdiff3d", device=local)
         s32 = HDGSolver(d, "convdiff3d", device=local)
         s32.set_precision(1, **MIXED)
+        if args.form == "served":
+            served = run_served(args, local)
+            if rank == 0:
+                print(json.dumps({"metric": METRIC, "form": "served", "served": served}), flush=True)
+            s64.close()
+            s32.close()
+            if world > 1:
+                dist.barrier()
+                dist.destroy_process_group()
+            return 0
         if args.form != "both":
             run_one_form(s32 if args.form == "mixed" else s64, lib, torch, local, args, world, dist, rank)
             s64.close()
@@ -337,6 +350,8 @@ def run_ours(args):
                                   "roofline": roof.pop("plain_roofline")},
                    "phases": phases_of(mixed["prof"], args.steps)}
             out.update(roof)
+            if args.serve_requests > 0 and world == 1:
+                out["served"] = run_served(args, local)
             if not args.no_cpu_baseline and world == 1:
                 out["cpu_baseline"] = {k: v for k, v in cpu_baseline_sample(tmp, args.n).items()
                                        if k != "per_solve_s_sample"}
@@ -359,6 +374,74 @@ def run_one_form(s, lib, torch, local, args, world, dist, rank):
                           "gmres_iters_per_solve": float(np.mean(r["gmres"])),
                           "residual_ratio_max": max(r["ratios"]), "gpu_launches": int(r["launches"]),
                           "clocks": r["clocks"], "phases": phases_of(r["prof"], args.steps)}), flush=True)
+
+
+SERVED_WORKLOAD = ("served stream of 2D convection-diffusion HDG solves: kappa log-uniform [1e-3, 1], unit "
+                   "velocity of uniform direction, p uniform in {2, 3, 4}, n x n quadrilaterals with n uniform in "
+                   "{8..64}, source sin(a pi x) sin(b pi y); plain form: one Newton step, block-Jacobi GMRES(50) "
+                   "to 1e-10; mixed form: FP64 refinement to ||r||/||r0|| <= 1e-8")
+
+
+def run_served(args, device):
+    """The served-stream leg: the same seeded requests solved (a) one at a time in plain FP64,
+    (b) by the server with `slots` overlapping solves in plain FP64 and (c) in the mixed form,
+    each on warm (resident) contexts; then the mixed server under Poisson arrivals at 100/s and
+    1000/s for p50/p99 latency.  Times are host wall-clock from submit to result."""
+    from exasim_b200 import build as B
+    from exasim_b200.serve import CaseCache, Server, stream_requests, with_params
+    B.build(["cdsin2d"])
+    R = args.serve_requests
+    cache = CaseCache()
+    reqs = stream_requests(R, 0.0, seed=2024)
+    blobs = [[with_params(cache.get(n, p)[0], prm)] + cache.get(n, p)[1:] for _, n, p, prm in reqs]
+    budget = 48 << 30
+
+    def saturated(srv, precision):
+        t0 = time.perf_counter()
+        ids = [srv.submit(b, precision=precision, **({"inner_tol": 1e-4, "rtol": 1e-8} if precision else {}))
+               for b in blobs]
+        res = [srv.wait(i) for i in ids]
+        return time.perf_counter() - t0, res
+
+    out = {"workload": SERVED_WORKLOAD, "requests": R, "slots": args.serve_slots, "hbm_budget_bytes": budget}
+    lines = {}
+    for name, slots, precision in (("plain_fp64_one_at_a_time", 1, 0), ("served_plain_fp64", args.serve_slots, 0),
+                                   ("served_mixed", args.serve_slots, 1)):
+        with Server("cdsin2d", device=device, hbm_budget=budget, slots=slots) as srv:
+            saturated(srv, precision)            # warm: every (n, p) context created once
+            wall, res = saturated(srv, precision)
+            st = srv.stats()
+        dofs = [r.uh.size for r in res]
+        lat = [r.latency_ms for r in res]
+        ratio = max((r.residual / r.residual0) if r.residual0 > 0 else 0.0 for r in res)
+        lines[name] = {"solves_per_s": R / wall, "dofs_per_s": sum(dofs) / wall,
+                       "mean_run_ms": float(np.mean([r.run_ms for r in res])),
+                       "gmres_iters_per_solve": float(np.mean([r.gmres for r in res])),
+                       "residual_ratio_max": ratio, "contexts_reused": st["contexts_reused"],
+                       "peak_bytes_held": st["peak_bytes_held"]}
+    base = lines["plain_fp64_one_at_a_time"]["solves_per_s"]
+    for v in lines.values():
+        v["speedup_vs_plain_fp64_one_at_a_time"] = v["solves_per_s"] / base
+    out.update(lines)
+    rates = {}
+    with Server("cdsin2d", device=device, hbm_budget=budget, slots=args.serve_slots) as srv:
+        saturated(srv, 1)
+        for rate in (100.0, 1000.0):
+            arr = stream_requests(R, rate, seed=7)
+            t0 = time.perf_counter()
+            ids = []
+            for (ta, n, p, prm), b in zip(arr, blobs):
+                dt = t0 + ta - time.perf_counter()
+                if dt > 0:
+                    time.sleep(dt)
+                ids.append(srv.submit(b, precision=1, inner_tol=1e-4, rtol=1e-8))
+            res = [srv.wait(i) for i in ids]
+            wall = time.perf_counter() - t0
+            lat = [r.latency_ms for r in res]
+            rates[f"{rate:g}/s"] = {"solves_per_s": R / wall, "latency_ms": {"p50": float(np.percentile(lat, 50)),
+                                                                            "p99": float(np.percentile(lat, 99))}}
+    out["poisson_arrivals_mixed"] = rates
+    return out
 
 
 # DRAM traffic of the four q-elimination GEMM launches of one FP64 assembly, from one ncu

@@ -20,7 +20,8 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 _LIBS: Dict[str, ctypes.CDLL] = {}
 
 STATUS = {0: "ok", 1: "bad argument", 2: "unsupported input", 3: "CUDA error", 4: "singular block",
-          5: "mesh error", 6: "not converged", 7: "NaN residual", 8: "out of device memory"}
+          5: "mesh error", 6: "not converged", 7: "NaN residual", 8: "out of device memory",
+          9: "wait timed out"}
 
 
 class ExaError(RuntimeError):
@@ -78,6 +79,12 @@ def load_library(model: str) -> ctypes.CDLL:
         "exa_bilu0_ordering": ([P, I, P, I, I, I, P, I, P, I, P, I, PI], I),
         "exa_last_residual": ([P, PD, PD], I),
         "exa_profile_read": ([P, I, PD, PLL, PD], I),
+        "exa_server_create": ([I, LL, I, I, ctypes.POINTER(P)], I),
+        "exa_server_submit": ([P, P, LL, P, LL, P, LL, P, LL, I, D, D, PLL], I),
+        "exa_server_wait": ([P, LL, D, PLL, PLL], I),
+        "exa_server_fetch": ([P, LL, P, LL, P, LL, PD], I),
+        "exa_server_stats": ([P, PLL], I),
+        "exa_server_destroy": ([P], None),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)

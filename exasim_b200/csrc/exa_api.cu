@@ -42,15 +42,19 @@ int dev_upload(ExaCtx& c, T** dst, const T* src, size_t count) {
     *dst = nullptr;
     return EXA_OK;
   }
+  // stream-ordered allocation on the context stream: unlike cudaMalloc / cudaFree it does not
+  // synchronize the device, so contexts can come and go while others are solving
   void* p = nullptr;
-  cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+  cudaError_t e = cudaMallocAsync(&p, count * sizeof(T), c.st);
   if (e != cudaSuccess) {
-    exa_set_error("cudaMalloc of %zu bytes failed: %s", count * sizeof(T), cudaGetErrorString(e));
+    exa_set_error("device allocation of %zu bytes failed: %s", count * sizeof(T), cudaGetErrorString(e));
     return EXA_ERR_NOMEM;
   }
   c.allocs.push_back(p);
+  c.alloc_bytes += (long long)(count * sizeof(T));
   *dst = (T*)p;
-  if (src) EXA_CUDA(cudaMemcpy(p, src, count * sizeof(T), cudaMemcpyHostToDevice));
+  // from pageable memory the call returns once the source has been staged
+  if (src) EXA_CUDA(cudaMemcpyAsync(p, src, count * sizeof(T), cudaMemcpyHostToDevice, c.st));
   return EXA_OK;
 }
 
@@ -67,6 +71,39 @@ std::vector<int> to_int(const double* p, long long n) {
   std::vector<int> v((size_t)n);
   for (long long i = 0; i < n; ++i) v[(size_t)i] = (int)llround(p[i]);
   return v;
+}
+
+// udg from sol.bin (full or u only) or the model's initial condition; uhat from sol.bin or
+// from u at the face nodes (readsolstruct, readbinaryfiles.cpp:499-618)
+int init_solution(ExaCtx& c, const Blob& S) {
+  const ExaDims& P = c.P;
+  {
+    std::vector<double> u((size_t)P.ne * P.npe * P.nc, 0.0);
+    const long long nu = S.nsize.size() > 2 ? S.nsize[2] : 0;
+    if (nu == (long long)(size_t)P.ne * P.npe * P.nc) {
+      std::memcpy(u.data(), S.part[2], sizeof(double) * u.size());
+    } else if (nu == (long long)(size_t)P.ne * P.npe * P.ncu) {
+      for (size_t e = 0; e < (size_t)P.ne; ++e)
+        for (int k = 0; k < P.ncu; ++k)
+          for (int i = 0; i < P.npe; ++i) u[i + P.npe * k + P.npe * P.nc * e] = S.part[2][i + P.npe * k + P.npe * P.ncu * e];
+    } else if (nu == 0) {
+      EXA_TRY(exa_model_init_udg(c, u.data()));
+    } else {
+      exa_set_error("sol.bin udg size %lld matches neither npe*nc*ne nor npe*ncu*ne", nu);
+      return EXA_ERR_ARG;
+    }
+    // on the context stream, after the zeroing queued there (pageable sources are staged
+    // before the calls return)
+    EXA_CUDA(cudaMemcpyAsync(c.udg, u.data(), sizeof(double) * u.size(), cudaMemcpyHostToDevice, c.st));
+    const long long nuh = S.nsize.size() > 5 ? S.nsize[5] : 0;
+    if (nuh == c.ndofuhat()) {
+      EXA_CUDA(cudaMemcpyAsync(c.uh, S.part[5], sizeof(double) * nuh, cudaMemcpyHostToDevice, c.st));
+    } else {
+      EXA_TRY(exa_k_face_nodes(P, c.f2e, c.perm, c.udg, c.uh, c.st));
+    }
+  }
+
+  return EXA_OK;
 }
 
 }  // namespace
@@ -263,29 +300,7 @@ int exa_ctx_init(ExaCtx& c, const double* app, long long napp, const double* mas
   EXA_TRY(dev_alloc(c, &c.udg, ne * P.npe * P.nc));
   EXA_TRY(dev_alloc(c, &c.uh, (size_t)c.ndofuhat()));
   EXA_TRY(dev_alloc(c, &c.sdg, ne * P.npe * P.ncu));
-  {
-    std::vector<double> u(ne * P.npe * P.nc, 0.0);
-    const long long nu = S.nsize.size() > 2 ? S.nsize[2] : 0;
-    if (nu == (long long)ne * P.npe * P.nc) {
-      std::memcpy(u.data(), S.part[2], sizeof(double) * u.size());
-    } else if (nu == (long long)ne * P.npe * P.ncu) {
-      for (size_t e = 0; e < ne; ++e)
-        for (int k = 0; k < P.ncu; ++k)
-          for (int i = 0; i < P.npe; ++i) u[i + P.npe * k + P.npe * P.nc * e] = S.part[2][i + P.npe * k + P.npe * P.ncu * e];
-    } else if (nu == 0) {
-      EXA_TRY(exa_model_init_udg(c, u.data()));
-    } else {
-      exa_set_error("sol.bin udg size %lld matches neither npe*nc*ne nor npe*ncu*ne", nu);
-      return EXA_ERR_ARG;
-    }
-    EXA_CUDA(cudaMemcpy(c.udg, u.data(), sizeof(double) * u.size(), cudaMemcpyHostToDevice));
-    const long long nuh = S.nsize.size() > 5 ? S.nsize[5] : 0;
-    if (nuh == c.ndofuhat()) {
-      EXA_CUDA(cudaMemcpy(c.uh, S.part[5], sizeof(double) * nuh, cudaMemcpyHostToDevice));
-    } else {
-      EXA_TRY(exa_k_face_nodes(P, c.f2e, c.perm, c.udg, c.uh, c.st));
-    }
-  }
+  EXA_TRY(init_solution(c, S));
 
   // q-equation matrices Minv*C, Minv*E (qequation.cpp:66-338)
   if (P.ncq > 0) {
@@ -436,12 +451,95 @@ int exa_ctx_set_precision(ExaCtx& c, int mode) {
   return EXA_OK;
 }
 
+// Puts a context back to the start of a new solve of the same mesh and discretization with the
+// physical parameters, tau and initial state of `app` / `sol` (the serving path reuses contexts
+// this way, keeping master, mesh, geometry and q matrices resident).
+int exa_ctx_reset(ExaCtx& c, const double* app, long long napp, const double* sol, long long nsol) {
+  Blob A = split_blob(app, napp), S = split_blob(sol, nsol);
+  if (!A.ok || !S.ok || A.nsize.size() < 9 || S.nsize.size() < 3) {
+    exa_set_error("reset: malformed app or sol blob");
+    return EXA_ERR_ARG;
+  }
+  if ((size_t)A.nsize[6] != c.h_param.size() || A.nsize[8] < 1) {
+    exa_set_error("reset: %lld physical parameters, the context has %zu", A.nsize[6], c.h_param.size());
+    return EXA_ERR_ARG;
+  }
+  EXA_CUDA(cudaSetDevice(c.device));
+  c.h_param.assign(A.part[6], A.part[6] + A.nsize[6]);
+  if (!c.h_param.empty())
+    EXA_CUDA(cudaMemcpyAsync(c.param, c.h_param.data(), sizeof(double) * c.h_param.size(), cudaMemcpyHostToDevice,
+                             c.st));
+  EXA_CUDA(cudaMemcpyAsync(c.tau, A.part[8], sizeof(double) * (size_t)A.nsize[8], cudaMemcpyHostToDevice, c.st));
+  c.time0 = (c.tdep == 1 && A.nsize[5] > 0) ? A.part[5][0] : 0.0;
+  c.time = c.time0;
+  c.dtfactor = 0.0;
+  c.last_gmres_iters = c.last_newton_iters = c.total_gmres_iters = 0;
+  c.last_norm0 = c.last_norm = 0.0;
+  EXA_CUDA(cudaMemsetAsync(c.sdg, 0, sizeof(double) * (size_t)c.P.npe * c.P.ncu * c.P.ne, c.st));
+  EXA_TRY(init_solution(c, S));
+  EXA_CUDA(cudaStreamSynchronize(c.st));
+  return EXA_OK;
+}
+
+// 64-bit FNV-1a over the blobs that fix a context's resident data: master, mesh, sol, and app
+// without its physical parameters and tau (parts 6 and 8), which exa_ctx_reset replaces.
+unsigned long long exa_ctx_key(const double* app, long long napp, const double* master, long long nmaster,
+                               const double* mesh, long long nmesh, const double* sol, long long nsol) {
+  unsigned long long h = 1469598103934665603ULL;
+  auto mix = [&](const void* p, size_t n) {
+    const unsigned char* b = (const unsigned char*)p;
+    for (size_t i = 0; i < n; ++i) {
+      h ^= b[i];
+      h *= 1099511628211ULL;
+    }
+  };
+  Blob A = split_blob(app, napp);
+  if (A.ok) {
+    mix(app, sizeof(double) * (size_t)(1 + A.nsize.size()));  // the part sizes
+    for (size_t i = 0; i < A.part.size(); ++i)
+      if (i != 6 && i != 8) mix(A.part[i], sizeof(double) * (size_t)A.nsize[i]);
+  } else {
+    mix(app, sizeof(double) * (size_t)std::max(0LL, napp));
+  }
+  mix(master, sizeof(double) * (size_t)std::max(0LL, nmaster));
+  mix(mesh, sizeof(double) * (size_t)std::max(0LL, nmesh));
+  mix(sol, sizeof(double) * (size_t)std::max(0LL, nsol));
+  return h;
+}
+
+// Device bytes a context for these blobs will hold (the arrays exa_ctx_init allocates, with
+// nf bounded by ne * nfe), for admission before it exists; 0 for malformed blobs.
+long long exa_ctx_estimate_bytes(const double* app, long long napp, const double* master, long long nmaster,
+                                 const double* mesh, long long nmesh, int precision) {
+  Blob A = split_blob(app, napp), M = split_blob(master, nmaster), Me = split_blob(mesh, nmesh);
+  if (!A.ok || !M.ok || !Me.ok || A.nsize.size() < 9 || M.nsize.size() < 1 || Me.nsize.size() < 1) return 0;
+  const double ncu = A.part[0][6], nc = A.part[0][5], ncq = A.part[0][7];
+  const double restart = A.part[2][15], precond = A.part[1][6];
+  const double nd = M.part[0][0], npe = M.part[0][5], npf = M.part[0][6], nge = M.part[0][7], ngf = M.part[0][8];
+  const double ne = Me.part[0][1], nfe = Me.part[0][4];
+  const double nf = ne * nfe, n = npe * ncu, ndf = npf * nfe, m = ndf * ncu, N = ncu * npf * nf;
+  const double nqn = ncq > 0 ? npe * nd * ncu : 0;
+  double per_elem = m * m + n * m + n + m + npe * nc + npe * ncu + nge * (nd + nd * nd + 1) + nfe * ngf * (2 * nd + 1) +
+                    (ncq > 0 ? npe * npe * nd + npe * ndf * nd + npe * npe * (2 + nd) + npe * ndf * nd : 0) + m + n;
+  per_elem += precond == 1 ? m * m : 0;
+  // element chunk workspace (the whole mesh when it fits in 8 GB)
+  per_elem += n * n + n * nqn + 2 * n * m + m * nqn + nge * (nd + 1) * ncu * nc + n + (n > 160 ? n * n : 0);
+  double words = ne * per_elem + N * (restart + 6) + (precond == 0 ? ncu * npf * ncu * npf * nf : 0);
+  if (precision == 1) words *= 1.75;
+  return (long long)(8.0 * words) + (16LL << 20);
+}
+
 void exa_ctx_free(ExaCtx& c) {
   if (c.device >= 0) cudaSetDevice(c.device);
   if (c.st) cudaStreamSynchronize(c.st);
   exa_prof_free(c);
-  for (void* p : c.allocs) cudaFree(p);
+  for (void* p : c.allocs) {
+    if (c.st) cudaFreeAsync(p, c.st);
+    else cudaFree(p);
+  }
+  if (c.st) cudaStreamSynchronize(c.st);
   c.allocs.clear();
+  c.alloc_bytes = 0;
   if (c.pinned) cudaFreeHost(c.pinned);
   c.pinned = nullptr;
   if (c.st) cudaStreamDestroy(c.st);
@@ -596,6 +694,7 @@ int exa_field_ptr(exa_ctx* h, const char* name, double** dev, long long* n) {
 
 int exa_get_connectivity(exa_ctx* h, int* f2e, int* elemcon) {
   EXA_TRY(guard(h));
+  EXA_CUDA(cudaStreamSynchronize(h->c.st));
   const ExaDims& P = h->c.P;
   if (f2e) EXA_CUDA(cudaMemcpy(f2e, h->c.f2e, sizeof(int) * 4 * (size_t)P.nf, cudaMemcpyDeviceToHost));
   if (elemcon) EXA_CUDA(cudaMemcpy(elemcon, h->c.elemcon, sizeof(int) * (size_t)P.ndf * P.ne, cudaMemcpyDeviceToHost));

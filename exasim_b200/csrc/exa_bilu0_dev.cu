@@ -273,8 +273,7 @@ int exa_k_bilu_build(const ExaDims& P, const ExaBiluDev& b, const int* f2e, cons
                                                        b.nnz, H, BE);
   EXA_LAUNCH_CHECK();
   const size_t smem = sizeof(T) * 4 * (size_t)ncf * ncf;
-  EXA_CUDA(cudaFuncSetAttribute((const void*)bilu_factor_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)smem));
+  EXA_TRY(exa_allow_smem((const void*)bilu_factor_kernel<T>, smem));
   bilu_factor_kernel<T><<<b.nse, 256, smem, st>>>(ncf, b.nse, b.nfse, b.row_ptr, b.fac_ptr, b.fac_ji, b.upd_ptr,
                                                    b.upd_jl, b.upd_il, BE, flag);
   EXA_LAUNCH_CHECK();
@@ -286,8 +285,7 @@ int exa_k_bilu_apply(const ExaDims& P, const ExaBiluDev& b, const T* BE, const d
                      cudaStream_t st) {
   const int ncf = P.ncu * P.npf;
   const size_t smem = exa_bilu_apply_smem(ncf, b.nfse);
-  EXA_CUDA(cudaFuncSetAttribute((const void*)bilu_apply_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)smem));
+  EXA_TRY(exa_allow_smem((const void*)bilu_apply_kernel<T>, smem));
   bilu_apply_kernel<T><<<b.nse, 256, smem, st>>>(ncf, b.nse, b.nfse, b.row_ptr, b.col_ind, b.face, BE, x, b.out);
   EXA_LAUNCH_CHECK();
   bilu_sum_kernel<<<grid_of((long long)ncf * P.nf), 256, 0, st>>>(ncf, P.nf, b.gf_ptr, b.gf_pos, b.out, w);

@@ -27,9 +27,14 @@ enum ExaStatus {
   EXA_ERR_NOTCONV = 6,      // solver stopped without reaching its tolerance
   EXA_ERR_NAN = 7,          // residual norm is NaN
   EXA_ERR_NOMEM = 8,        // device allocation refused
+  EXA_ERR_TIMEOUT = 9,      // a wait ran out before its request finished
 };
 
 void exa_set_error(const char* fmt, ...);
+// Lets `fn` launch with `bytes` of dynamic shared memory.  The attribute is set to the
+// device maximum (227 KB), the same value for every caller, so host threads launching the
+// same kernel with different sizes cannot undo each other's setting.
+int exa_allow_smem(const void* fn, size_t bytes);
 const char* exa_get_error();
 
 #define EXA_CUDA(call)                                                              \

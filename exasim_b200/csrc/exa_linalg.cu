@@ -16,8 +16,18 @@
 
 #include <atomic>
 
-static char g_err[1024] = "";
+static thread_local char g_err[1024] = "";  // per host thread: each context is driven by one thread
 static std::atomic<long long> g_launches{0};
+
+int exa_allow_smem(const void* fn, size_t bytes) {
+  constexpr size_t kMax = 227 * 1024;
+  if (bytes > kMax) {
+    exa_set_error("kernel needs %zu bytes of shared memory, more than %zu", bytes, kMax);
+    return EXA_ERR_UNSUPPORTED;
+  }
+  if (bytes > 48 * 1024) EXA_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMax));
+  return EXA_OK;
+}
 
 void exa_count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 extern "C" long long exa_launch_count(void) { return g_launches.load(); }
@@ -183,7 +193,7 @@ int launch_dmma(const GemmBatch& g, cudaStream_t st) {
   constexpr size_t smem = dmma_smem<TI, TJ, WM, WN>();
   static_assert(smem <= 227 * 1024, "GEMM tile exceeds shared memory");
   auto kern = dmma_gemm_kernel<TI, TJ, WM, WN>;
-  EXA_CUDA(cudaFuncSetAttribute((const void*)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  EXA_TRY(exa_allow_smem((const void*)kern, smem));
   dim3 grid((unsigned)(exa_ceil_div(g.M, BM) * exa_ceil_div(g.N, BN)), (unsigned)g.batch, (unsigned)g.batch2);
   kern<<<grid, 32 * WM * WN, smem, st>>>(g);
   EXA_LAUNCH_CHECK();

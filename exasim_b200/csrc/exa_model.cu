@@ -29,11 +29,7 @@ AsmArgs make_args(const ExaCtx& c, int e0) {
 }
 
 int smem_attr(const void* fn, size_t bytes) {
-  if (bytes > 48 * 1024) EXA_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
-  if (bytes > 227 * 1024) {
-    exa_set_error("element tile needs %zu bytes of shared memory", bytes);
-    return EXA_ERR_UNSUPPORTED;
-  }
+  EXA_TRY(exa_allow_smem(fn, bytes));
   return EXA_OK;
 }
 

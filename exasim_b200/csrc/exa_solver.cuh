@@ -62,6 +62,7 @@ struct ExaCtx {
   double time = 0.0, dtfactor = 0.0;
   int nf_total = 0;
   std::vector<void*> allocs;
+  long long alloc_bytes = 0;  // device bytes held by the context
   // statistics of the last solve
   int last_gmres_iters = 0, last_newton_iters = 0, total_gmres_iters = 0;
   double last_gmres_relerr = 0.0;
@@ -97,6 +98,11 @@ struct ExaCtx {
 int exa_ctx_init(ExaCtx& c, const double* app, long long napp, const double* master, long long nmaster,
                  const double* mesh, long long nmesh, const double* sol, long long nsol, int device);
 void exa_ctx_free(ExaCtx& c);
+int exa_ctx_reset(ExaCtx& c, const double* app, long long napp, const double* sol, long long nsol);
+unsigned long long exa_ctx_key(const double* app, long long napp, const double* master, long long nmaster,
+                               const double* mesh, long long nmesh, const double* sol, long long nsol);
+long long exa_ctx_estimate_bytes(const double* app, long long napp, const double* master, long long nmaster,
+                                 const double* mesh, long long nmesh, int precision);
 
 // model-specific steps (instantiated per model)
 int exa_model_assemble(ExaCtx& c, bool jacobian);

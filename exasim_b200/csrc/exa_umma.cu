@@ -175,7 +175,7 @@ int launch_umma(const UGemm& g, int* flag, cudaStream_t st) {
   constexpr size_t smem = (size_t)UST * (UM * UBK * 4 + NP * UBK * 4) + (UST + 1) * 8 + 16;
   static_assert(smem <= 227 * 1024, "tile exceeds shared memory");
   auto kern = umma_gemm_kernel<TA, TB, TCI, TCO, NP>;
-  EXA_CUDA(cudaFuncSetAttribute((const void*)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  EXA_TRY(exa_allow_smem((const void*)kern, smem));
   EXA_CUDA(cudaFuncSetAttribute((const void*)kern, cudaFuncAttributePreferredSharedMemoryCarveout,
                                 (int)cudaSharedmemCarveoutMaxShared));
   dim3 grid((unsigned)exa_ceil_div(g.M, UM), (unsigned)g.batch, (unsigned)g.batch2);
@@ -466,7 +466,7 @@ int launch_umma3(const UGemmP& g, int* flag, cudaStream_t st) {
   constexpr size_t smem = (size_t)PST * 2 * (16 * 512 + (NP / 8) * 512) + (2 * PST + 1) * 8 + 16;
   static_assert(smem <= 227 * 1024, "tile exceeds shared memory");
   auto kern = umma3_kernel<NP, TCI, TCO>;
-  EXA_CUDA(cudaFuncSetAttribute((const void*)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  EXA_TRY(exa_allow_smem((const void*)kern, smem));
   EXA_CUDA(cudaFuncSetAttribute((const void*)kern, cudaFuncAttributePreferredSharedMemoryCarveout,
                                 (int)cudaSharedmemCarveoutMaxShared));
   dim3 grid((unsigned)exa_ceil_div(g.M, UM), (unsigned)g.batch, (unsigned)g.batch2);

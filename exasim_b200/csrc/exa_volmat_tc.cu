@@ -204,8 +204,7 @@ int exa_k_vol_mat_tc(const ExaDims& P, const double* shapegw, const UPacked& Sp,
     return EXA_ERR_UNSUPPORTED;
   }
   const size_t smem = exa_vol_mat_tc_smem(P);
-  EXA_CUDA(cudaFuncSetAttribute((const void*)vol_mat_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)smem));
+  EXA_TRY(exa_allow_smem((const void*)vol_mat_tc_kernel, smem));
   const int nitems = nb * ((P.ncu * P.nc + VGRP - 1) / VGRP);
   int sms = 148;
   int dev = 0;

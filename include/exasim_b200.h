@@ -6,7 +6,8 @@
  * *_dev are CUDA device pointers; every other pointer is host memory owned by the caller.
  * Every function returns 0 on success or an ExaStatus code (1 bad argument,
  * 2 unsupported input, 3 CUDA error, 4 singular block, 5 mesh error, 6 not converged,
- * 7 NaN residual, 8 out of device memory); exa_last_error() describes the last failure.
+ * 7 NaN residual, 8 out of device memory, 9 wait timed out); exa_last_error() describes the
+ * calling thread's last failure.
  * The reference prints and exits instead (backend/Common/common.h:527-555).
  * One host thread per context; calls are synchronous unless noted.
  *
@@ -21,7 +22,7 @@ extern "C" {
 
 typedef struct exa_ctx exa_ctx;
 
-/* Message of the last failed call (thread-unsafe static buffer). */
+/* Message of the calling host thread's last failed call. */
 const char* exa_last_error(void);
 
 /* Build a context from the four input files Exasim's preprocessor writes
@@ -130,8 +131,9 @@ int exa_synchronize(exa_ctx* ctx);
 /* Batched FP64 building blocks on device pointers, enqueued on `stream` (cudaStream_t, may
  * be NULL): C_b = alpha A_b B_b + beta C_b (column-major, batch strides sA, sB, sC) as used for
  * Exasim's PGEMNMStridedBached (backend/Common/pblas.h:695); and the in-place explicit
- * inverse of `batch` n x n blocks `stride` doubles apart (pblas.h:163 Inverse), n <= 160,
- * *info_dev set non-zero on a zero pivot. */
+ * inverse of `batch` n x n blocks `stride` doubles apart (pblas.h:163 Inverse), n <= 320
+ * (above 160 by 2 x 2 blocks with a temporary stream-ordered workspace of n^2 doubles per
+ * block), *info_dev set non-zero on a zero pivot. */
 int exa_dgemm_batched(int M, int N, int K, double alpha, const double* A, long long lda, long long sA,
                       const double* B, long long ldb, long long sB, double beta, double* C, long long ldc,
                       long long sC, int batch, void* stream);
@@ -165,6 +167,40 @@ long long exa_launch_count(void);
  * capture starts.  Nothing needs zeroing beforehand.  Calls whose kernels can overlap (other
  * streams with no ordering, several host threads) race on the shared array: order them. */
 int exa_dnrm2_cols_fixed(const double* X, long long n, long long ldx, int ncols, double* out_dev, void* stream);
+
+/* ---- Serving: continuous batching of independent solves of this library's model ----
+ * No counterpart in the reference, which runs one problem per process.  A server owns
+ * `slots` host threads on one device.  Each submitted request (the four datain blobs, copied
+ * at submit) waits in arrival order until a slot is free and its context fits in
+ * hbm_budget_bytes (estimated from the blobs before it exists, its actual size after); it
+ * then runs on its own context and CUDA stream, so admitted solves overlap on the device.
+ * Steady problems run Newton (exa_newton); time-dependent ones every DIRK step of their app
+ * (exa_dirk).  With reuse_contexts, a finished request's context stays resident, keyed by
+ * master, mesh, sol and app without the physical parameters and tau; a later request with
+ * the same key reuses it after a reset of parameters and initial state, and contexts held
+ * for reuse are evicted least recently used first when memory is needed.  A solve's result
+ * does not depend on what else runs: every reduction is in a fixed order.
+ * precision, inner_tol and rtol are those of exa_set_precision.  Contexts use stream-ordered
+ * allocation, so creating and freeing one does not synchronise the device. */
+typedef struct exa_server exa_server;
+int exa_server_create(int device, long long hbm_budget_bytes, int slots, int reuse_contexts, exa_server** out);
+int exa_server_submit(exa_server* s, const double* app, long long napp, const double* master, long long nmaster,
+                      const double* mesh, long long nmesh, const double* sol, long long nsol, int precision,
+                      double inner_tol, double rtol, long long* id);
+/* Blocks until request `id` has finished (timeout_s < 0: no limit; else EXA_ERR_TIMEOUT) and
+ * gives its result sizes (udg npe*nc*ne, uhat ndofuhat); returns the solve's status. */
+int exa_server_wait(exa_server* s, long long id, double timeout_s, long long* nudg, long long* nuh);
+/* Copies a finished request's udg and uhat (either may be NULL) and info[8] = {queued ms,
+ * run ms (set-up or reset, solve, read-back), latency ms (submit to finish), Newton steps,
+ * GMRES iterations, first and last residual norm, 1 if its context was reused}, then
+ * forgets the request. */
+int exa_server_fetch(exa_server* s, long long id, double* udg, long long nudg, double* uh, long long nuh,
+                     double* info);
+/* out[10] = {queued, running, done, failed, device bytes held, peak bytes held, contexts
+ * created, contexts reused, contexts kept idle, contexts evicted} */
+int exa_server_stats(exa_server* s, long long* out);
+/* Finishes the running solves, drops queued requests and frees every context. */
+void exa_server_destroy(exa_server* s);
 
 #ifdef __cplusplus
 }
