@@ -379,7 +379,7 @@ def run_one_form(s, lib, torch, local, args, world, dist, rank):
 SERVED_WORKLOAD = ("served stream of 2D convection-diffusion HDG solves: kappa log-uniform [1e-3, 1], unit "
                    "velocity of uniform direction, p uniform in {2, 3, 4}, n x n quadrilaterals with n uniform in "
                    "{8..64}, source sin(a pi x) sin(b pi y); plain form: one Newton step, block-Jacobi GMRES(50) "
-                   "to 1e-10; mixed form: FP64 refinement to ||r||/||r0|| <= 1e-8")
+                   "to 1e-11; mixed form: FP64 refinement to ||r||/||r0|| <= 1e-8")
 
 
 def run_served(args, device):

@@ -383,7 +383,14 @@ int exa_ctx_init(ExaCtx& c, const double* app, long long napp, const double* mas
     EXA_TRY(dev_alloc(c, &c.udgprev, ne * n));
     EXA_TRY(dev_alloc(c, &c.utmp, ne * n));
   }
-  EXA_CUDA(cudaMallocHost((void**)&c.pinned, sizeof(double) * (n1 * (n1 + 2) + 64)));
+  // staging for the Hessenberg matrix and Givens vector, then one residual slot per step
+  EXA_CUDA(cudaMallocHost((void**)&c.pinned, sizeof(double) * (n1 * (n1 + 3) + 64)));
+  for (int k = 0; k < 2; ++k) {
+    EXA_CUDA(cudaEventCreateWithFlags(&c.step_ev[k], cudaEventDisableTiming));
+    c.arnoldi_graph[k].assign(c.restart, nullptr);
+    c.arnoldi_launches[k].assign(c.restart, 0);
+    c.arnoldi_seen[k].assign(c.restart, 0);
+  }
   EXA_CUDA(cudaStreamSynchronize(c.st));
   return EXA_OK;
 }
@@ -542,6 +549,13 @@ void exa_ctx_free(ExaCtx& c) {
   c.alloc_bytes = 0;
   if (c.pinned) cudaFreeHost(c.pinned);
   c.pinned = nullptr;
+  for (int k = 0; k < 2; ++k) {
+    for (cudaGraphExec_t g : c.arnoldi_graph[k])
+      if (g) cudaGraphExecDestroy(g);
+    c.arnoldi_graph[k].clear();
+    if (c.step_ev[k]) cudaEventDestroy(c.step_ev[k]);
+    c.step_ev[k] = nullptr;
+  }
   if (c.st) cudaStreamDestroy(c.st);
   c.st = nullptr;
 }

@@ -55,6 +55,10 @@ const char* exa_get_error();
 // Every kernel launch site ends with EXA_LAUNCH_CHECK(), which also counts the launch
 // (exa_launch_count() in the C ABI).
 void exa_count_launch();
+// Launches made by the calling host thread, and an adjustment of both counts: a captured CUDA
+// graph's kernels are counted when the graph is replayed, not when it is captured.
+long long exa_thread_launches();
+void exa_add_launches(long long n);
 
 #define EXA_LAUNCH_CHECK()                                                          \
   do {                                                                              \

@@ -193,8 +193,111 @@ void back_solve(double* y, const double* H, const double* s, int i, int n) {
 
 }  // namespace
 
+namespace {
+
+// The work of Arnoldi step i of a restart cycle, all enqueued on the context stream with
+// no host synchronisation: v_{i+1} = P A v_i orthogonalised against v_0..v_i (MGS or CGS),
+// the Hessenberg column i, the Givens update and the residual estimate |s_{i+1}| / |b|,
+// copied to the pinned slot `rel_pin`.
+int arnoldi_ops(ExaCtx& c, int i, const double* d_nrmb, double* d_relerr, double* rel_pin) {
+  const long long N = c.ndofuhat();
+  const int n1 = c.restart + 1;
+  double* vi = c.V + (long long)i * N;
+  double* vn = c.V + (long long)(i + 1) * N;
+  double* hcol = c.hess + (long long)n1 * i;
+  EXA_TRY(exa_drv_matvec(c, vi, c.w));
+  EXA_TRY(exa_drv_precond(c, c.w, vn));
+  {
+    ExaProfScope ps_ortho(c, EXA_PH_ORTHO);
+    if (c.ortho == 0) {
+      EXA_TRY(exa_dot_partials(vn, c.V, N, c.part_a, c.st));
+      double* pin = c.part_a;
+      double* pout = c.part_b;
+      for (int k = 1; k <= i; ++k) {
+        EXA_TRY(exa_mgs_step(vn, c.V + (long long)(k - 1) * N, c.V + (long long)k * N, pin, pout, hcol + k - 1, N, c.st));
+        std::swap(pin, pout);
+      }
+      EXA_TRY(exa_mgs_step(vn, c.V + (long long)i * N, nullptr, pin, pout, hcol + i, N, c.st));
+      EXA_TRY(exa_mgs_finish(vn, vn, pout, hcol + i + 1, N, c.st));
+    } else {
+      EXA_TRY(exa_cgs(vn, c.V, hcol, c.part_m, N, i + 1, c.st));
+      EXA_TRY(exa_dot_partials(vn, vn, N, c.part_a, c.st));
+      EXA_TRY(exa_mgs_finish(vn, vn, c.part_a, hcol + i + 1, N, c.st));
+    }
+  }
+  EXA_TRY(exa_givens(hcol, c.gs, c.gcs, c.gsn, i, d_nrmb, d_relerr, c.st));
+  EXA_CUDA(cudaMemcpyAsync(rel_pin, d_relerr, sizeof(double), cudaMemcpyDeviceToHost, c.st));
+  return EXA_OK;
+}
+
+// Enqueues Arnoldi step i.  Its first use runs the launches directly; from the second use on
+// the step is one CUDA graph, captured then and replayed after, which replaces some 30
+// launches (the matvec, the preconditioner, one Gram-Schmidt launch per basis vector, the
+// Givens update) by one.  The graph's arguments are fixed per context: the basis column,
+// the Hessenberg column, the residual slot.  Phase profiling records events between the
+// launches, so it runs the launches directly.  A capture that fails leaves the context on
+// direct launches.
+int arnoldi_step(ExaCtx& c, int i, const double* d_nrmb, double* d_relerr, double* rel_pin) {
+  const int pr = c.precision == 1 ? 1 : 0;
+  if (!c.use_graphs || c.prof.on || i >= (int)c.arnoldi_graph[pr].size())
+    return arnoldi_ops(c, i, d_nrmb, d_relerr, rel_pin);
+  cudaGraphExec_t& ex = c.arnoldi_graph[pr][i];
+  if (ex) {
+    EXA_CUDA(cudaGraphLaunch(ex, c.st));
+    exa_add_launches(c.arnoldi_launches[pr][i]);
+    return EXA_OK;
+  }
+  if (!c.arnoldi_seen[pr][i]) {
+    c.arnoldi_seen[pr][i] = 1;
+    return arnoldi_ops(c, i, d_nrmb, d_relerr, rel_pin);
+  }
+  const long long l0 = exa_thread_launches();
+  EXA_CUDA(cudaStreamBeginCapture(c.st, cudaStreamCaptureModeThreadLocal));
+  const int st = arnoldi_ops(c, i, d_nrmb, d_relerr, rel_pin);
+  cudaGraph_t g = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(c.st, &g);
+  const long long nl = exa_thread_launches() - l0;
+  exa_add_launches(-nl);  // counted again at each replay
+  if (st == EXA_OK && e == cudaSuccess && g && cudaGraphInstantiate(&ex, g, 0) == cudaSuccess) {
+    cudaGraphDestroy(g);
+    c.arnoldi_launches[pr][i] = nl;
+    EXA_CUDA(cudaGraphLaunch(ex, c.st));
+    exa_add_launches(nl);
+    return EXA_OK;
+  }
+  if (g) cudaGraphDestroy(g);
+  ex = nullptr;
+  cudaGetLastError();
+  c.use_graphs = 0;
+  return arnoldi_ops(c, i, d_nrmb, d_relerr, rel_pin);
+}
+
+// UpdateSolution (gmres.cpp:132-137) with the first i + 1 basis vectors: y from the
+// Hessenberg back-solve on the host, x += V y on the device.
+int update_solution(ExaCtx& c, int i, std::vector<double>& ybuf) {
+  const long long N = c.ndofuhat();
+  const int n1 = c.restart + 1, nrest = c.restart;
+  double* hh = c.pinned;
+  double* ss = hh + (size_t)n1 * nrest;
+  EXA_CUDA(cudaMemcpyAsync(hh, c.hess, sizeof(double) * n1 * nrest, cudaMemcpyDeviceToHost, c.st));
+  EXA_CUDA(cudaMemcpyAsync(ss, c.gs, sizeof(double) * n1, cudaMemcpyDeviceToHost, c.st));
+  EXA_CUDA(cudaStreamSynchronize(c.st));
+  back_solve(ybuf.data(), hh, ss, i, n1);
+  double* yd = c.part_m;  // device copy of the back-solve result (part_m holds >= restart+1 doubles)
+  EXA_CUDA(cudaMemcpyAsync(yd, ybuf.data(), sizeof(double) * (i + 1), cudaMemcpyHostToDevice, c.st));
+  EXA_TRY(exa_gemv_add(c.x, c.V, yd, N, i + 1, c.st));
+  return EXA_OK;
+}
+
+}  // namespace
+
 // GMRES (gmres.cpp:361-597): restarted, left-preconditioned, MGS (flag 0) or CGS (flag 1).
 // Solves A x = b for the current system; x starts at zero (no reduced basis).
+// The host reads each step's residual estimate one step late: step i + 1 is enqueued before
+// the estimate of step i is read, so the device does not wait for the host between steps.
+// When step i has converged, step i + 1 has run as well; it writes only basis column i + 2,
+// Hessenberg column i + 1 and Givens entries i + 1 and i + 2, none of which the solution
+// update of step i reads, so the result is that of stopping at step i.
 int exa_drv_gmres(ExaCtx& c, int* iters_out, double* relerr_out) {
   const long long N = c.ndofuhat();
   const int nrest = c.restart, maxit = c.gmres_maxit, n1 = nrest + 1;
@@ -214,71 +317,47 @@ int exa_drv_gmres(ExaCtx& c, int* iters_out, double* relerr_out) {
   // device copy of nrmb for the Givens kernel
   double* d_nrmb = c.scal + 14;
   double* d_relerr = c.scal + 13;
+  double* rel_pin = c.pinned + (size_t)n1 * (n1 + 2) + 64;  // one slot per step of a cycle
   c.pinned[0] = nrmb;
   EXA_CUDA(cudaMemcpyAsync(d_nrmb, c.pinned, sizeof(double), cudaMemcpyHostToDevice, c.st));
   std::vector<double> ybuf(n1);
   int j = 0;
   double relerr = 1.0;
-  double* yd = c.part_m;  // device copy of the back-solve result (part_m holds >= restart+1 doubles)
   while (j < maxit) {
     EXA_TRY(exa_scale(c.V, c.r, 1.0 / nrmr, N, c.st));
     std::vector<double> s0(n1, 0.0);
     s0[0] = nrmr;
     std::copy(s0.begin(), s0.end(), c.pinned);
     EXA_CUDA(cudaMemcpyAsync(c.gs, c.pinned, sizeof(double) * n1, cudaMemcpyHostToDevice, c.st));
-    int i = 0;
+    int i = 0, pending = -1;
     for (i = 0; i < nrest && j < maxit; i++, j++) {
-      double* vi = c.V + (long long)i * N;
-      double* vn = c.V + (long long)(i + 1) * N;
-      double* hcol = c.hess + (long long)n1 * i;
-      EXA_TRY(exa_drv_matvec(c, vi, c.w));
-      EXA_TRY(exa_drv_precond(c, c.w, vn));
-      ExaProfScope ps_ortho(c, EXA_PH_ORTHO);
-      if (c.ortho == 0) {
-        EXA_TRY(exa_dot_partials(vn, c.V, N, c.part_a, c.st));
-        double* pin = c.part_a;
-        double* pout = c.part_b;
-        for (int k = 1; k <= i; ++k) {
-          EXA_TRY(exa_mgs_step(vn, c.V + (long long)(k - 1) * N, c.V + (long long)k * N, pin, pout, hcol + k - 1, N, c.st));
-          std::swap(pin, pout);
+      EXA_TRY(arnoldi_step(c, i, d_nrmb, d_relerr, rel_pin + i));
+      EXA_CUDA(cudaEventRecord(c.step_ev[i & 1], c.st));
+      if (pending >= 0) {
+        EXA_CUDA(cudaEventSynchronize(c.step_ev[pending & 1]));
+        relerr = rel_pin[pending];
+        if (relerr < tol) {
+          EXA_TRY(update_solution(c, pending, ybuf));
+          EXA_CUDA(cudaStreamSynchronize(c.st));
+          *iters_out = j;
+          *relerr_out = relerr;
+          return EXA_OK;
         }
-        EXA_TRY(exa_mgs_step(vn, c.V + (long long)i * N, nullptr, pin, pout, hcol + i, N, c.st));
-        EXA_TRY(exa_mgs_finish(vn, vn, pout, hcol + i + 1, N, c.st));
-      } else {
-        EXA_TRY(exa_cgs(vn, c.V, hcol, c.part_m, N, i + 1, c.st));
-        EXA_TRY(exa_dot_partials(vn, vn, N, c.part_a, c.st));
-        EXA_TRY(exa_mgs_finish(vn, vn, c.part_a, hcol + i + 1, N, c.st));
       }
-      EXA_TRY(exa_givens(hcol, c.gs, c.gcs, c.gsn, i, d_nrmb, d_relerr, c.st));
-      EXA_CUDA(cudaMemcpyAsync(c.pinned, d_relerr, sizeof(double), cudaMemcpyDeviceToHost, c.st));
-      EXA_CUDA(cudaStreamSynchronize(c.st));
-      relerr = c.pinned[0];
+      pending = i;
+    }
+    if (pending >= 0) {
+      EXA_CUDA(cudaEventSynchronize(c.step_ev[pending & 1]));
+      relerr = rel_pin[pending];
       if (relerr < tol) {
-        // UpdateSolution (gmres.cpp:132-137)
-        double* hh = c.pinned;
-        double* ss = hh + (size_t)n1 * nrest;
-        EXA_CUDA(cudaMemcpyAsync(hh, c.hess, sizeof(double) * n1 * nrest, cudaMemcpyDeviceToHost, c.st));
-        EXA_CUDA(cudaMemcpyAsync(ss, c.gs, sizeof(double) * n1, cudaMemcpyDeviceToHost, c.st));
+        EXA_TRY(update_solution(c, pending, ybuf));
         EXA_CUDA(cudaStreamSynchronize(c.st));
-        back_solve(ybuf.data(), hh, ss, i, n1);
-        EXA_CUDA(cudaMemcpyAsync(yd, ybuf.data(), sizeof(double) * (i + 1), cudaMemcpyHostToDevice, c.st));
-        EXA_TRY(exa_gemv_add(c.x, c.V, yd, N, i + 1, c.st));
-        EXA_CUDA(cudaStreamSynchronize(c.st));
-        *iters_out = j + 1;
+        *iters_out = j;
         *relerr_out = relerr;
         return EXA_OK;
       }
     }
-    {
-      double* hh = c.pinned;
-      double* ss = hh + (size_t)n1 * nrest;
-      EXA_CUDA(cudaMemcpyAsync(hh, c.hess, sizeof(double) * n1 * nrest, cudaMemcpyDeviceToHost, c.st));
-      EXA_CUDA(cudaMemcpyAsync(ss, c.gs, sizeof(double) * n1, cudaMemcpyDeviceToHost, c.st));
-      EXA_CUDA(cudaStreamSynchronize(c.st));
-      back_solve(ybuf.data(), hh, ss, i - 1, n1);
-      EXA_CUDA(cudaMemcpyAsync(yd, ybuf.data(), sizeof(double) * i, cudaMemcpyHostToDevice, c.st));
-      EXA_TRY(exa_gemv_add(c.x, c.V, yd, N, i, c.st));
-    }
+    EXA_TRY(update_solution(c, i - 1, ybuf));
     // r = P (b - A x)
     EXA_TRY(exa_drv_matvec(c, c.x, c.w));
     EXA_TRY(exa_axpby(c.w, c.b, 1.0, -1.0, N, c.st));

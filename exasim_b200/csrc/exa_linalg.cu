@@ -15,6 +15,9 @@
 #include "exa_common.cuh"
 
 #include <atomic>
+#include <mutex>
+#include <set>
+#include <utility>
 
 static thread_local char g_err[1024] = "";  // per host thread: each context is driven by one thread
 static std::atomic<long long> g_launches{0};
@@ -25,11 +28,30 @@ int exa_allow_smem(const void* fn, size_t bytes) {
     exa_set_error("kernel needs %zu bytes of shared memory, more than %zu", bytes, kMax);
     return EXA_ERR_UNSUPPORTED;
   }
-  if (bytes > 48 * 1024) EXA_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMax));
+  if (bytes <= 48 * 1024) return EXA_OK;
+  // once per device and kernel: later launches (graph captures among them) make no call
+  static std::mutex mu;
+  static std::set<std::pair<int, const void*>> done;
+  int dev = 0;
+  EXA_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> g(mu);
+  if (done.count({dev, fn})) return EXA_OK;
+  EXA_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMax));
+  done.insert({dev, fn});
   return EXA_OK;
 }
 
-void exa_count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+static thread_local long long t_launches = 0;  // this host thread's launches (graph captures count them)
+
+void exa_count_launch() {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  ++t_launches;
+}
+long long exa_thread_launches() { return t_launches; }
+void exa_add_launches(long long n) {
+  g_launches.fetch_add(n, std::memory_order_relaxed);
+  t_launches += n;
+}
 extern "C" long long exa_launch_count(void) { return g_launches.load(); }
 
 void exa_set_error(const char* fmt, ...) {

@@ -58,6 +58,13 @@ struct ExaCtx {
          *gsn = nullptr, *scal = nullptr, *udgprev = nullptr, *utmp = nullptr;
   int* d_flag = nullptr;
   double* pinned = nullptr;  // small host staging buffer
+  // GMRES: each Arnoldi step index i of the restart cycle (and each precision) runs as one
+  // captured CUDA graph from its second use on; none while phase profiling records events
+  std::vector<cudaGraphExec_t> arnoldi_graph[2];
+  std::vector<long long> arnoldi_launches[2];
+  std::vector<unsigned char> arnoldi_seen[2];
+  cudaEvent_t step_ev[2] = {nullptr, nullptr};
+  int use_graphs = 1;
   // state
   double time = 0.0, dtfactor = 0.0;
   int nf_total = 0;

@@ -115,10 +115,10 @@ def with_params(app: np.ndarray, params: Sequence[float]) -> np.ndarray:
 
 class CaseCache:
     """Blobs of the served model's (n, p) meshes, written once per shape.  The GMRES tolerance
-    1e-10 (as the 2D Poisson configuration uses) brings the plain form's one Newton step to a
-    residual ratio below 1e-8."""
+    1e-11 on the preconditioned residual brings the plain form's one Newton step to a true
+    residual ratio below 1e-8 on every request of the stream."""
 
-    def __init__(self, gmres_tol: float = 1e-10):
+    def __init__(self, gmres_tol: float = 1e-11):
         self.tmp = tempfile.TemporaryDirectory()
         self.blobs: Dict[Tuple[int, int], List[np.ndarray]] = {}
         self.gmres_tol = gmres_tol
