@@ -272,11 +272,12 @@ int exa_gemm(const GemmBatch& g, cudaStream_t st) {
 // batched explicit inverse.  Exasim forms the explicit inverse of each element block
 // with getrf + getri (backend/Common/pblas.h:163-260).  Here: Gauss-Jordan exchange
 // steps with partial pivoting (pivot = largest magnitude among the rows not yet used,
-// first on ties), one block per matrix, the matrix held in registers: thread (tx, ty)
-// of a 16 x 32 grid owns rows ty + 32*a and columns tx + 16*b.  Rows are never swapped
-// physically; the pivot order is recorded and undone when the result is written, which
-// gives the same pivots and arithmetic as swapping.  Each exchange at pivot (p, k):
-//   a_pk <- 1/a_pk,  a_pj <- a_pj / a_pk,  a_ik <- -a_ik / a_pk,  a_ij <- a_ij - a_ik a_pj / a_pk.
+// first on ties), the matrix held in registers.  Rows are never swapped physically; the
+// pivot order is recorded and undone when the result is written, which gives the same
+// pivots and arithmetic as swapping.  Each exchange at pivot (p, k), with d = 1/a_pk:
+//   a_pk <- d,  a_pj <- a_pj d,  a_ik <- -a_ik d,  a_ij <- a_ij - a_ik (a_pj d).
+// Both kernels below perform exactly these operations in this order, so they give the
+// same bits for the same matrix.
 // ----------------------------------------------------------------------------------
 namespace {
 constexpr int INV_MAX_N = 160;
@@ -284,54 +285,25 @@ constexpr int INV_MAX_N = 160;
 template <typename T>
 __device__ __forceinline__ T absval(T x) { return x < T(0) ? -x : x; }
 
-// FP32 blocks (mixed-precision form) need half the registers: two CTAs per SM
-template <typename T, int RR, int RC>
-__global__ void __launch_bounds__(512, sizeof(T) == 4 ? 2 : 1)
-    inverse_kernel(T* Aall, int n, long long stride, int* flag) {
-  // double-buffered pivot column / pivot row: step k uses buffer k&1, so one barrier
-  // after publishing the column and one after publishing the row suffice per step
-  __shared__ T colk[2][INV_MAX_N];
-  __shared__ T rowp[2][INV_MAX_N];
-  __shared__ int perm[INV_MAX_N];   // perm[k] = pivot row of step k
-  T* G = Aall + (long long)blockIdx.x * stride;
-  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;   // 16 x 32
+// n <= 32: one warp per matrix, lane r holding row r.  The pivot search is a warp argmax,
+// the pivot row reaches every lane by shuffles.  8 matrices per 256-thread CTA.
+template <typename T>
+__global__ void __launch_bounds__(256) inverse_warp_kernel(T* Aall, int n, long long stride, int batch, int* flag) {
   const int lane = threadIdx.x & 31;
-  T a[RR][RC];
+  const long long mat = (long long)blockIdx.x * 8 + (threadIdx.x >> 5);
+  if (mat >= batch) return;
+  T* G = Aall + mat * stride;
+  T a[32];
 #pragma unroll
-  for (int i = 0; i < RR; ++i)
-#pragma unroll
-    for (int j = 0; j < RC; ++j) {
-      const int r = ty + 32 * i, c = tx + 16 * j;
-      a[i][j] = (r < n && c < n) ? G[r + (long long)n * c] : T(0);
-    }
-  unsigned used = 0u;  // bit q: row lane + 32 q already pivoted (identical in every warp)
+  for (int j = 0; j < 32; ++j) a[j] = (lane < n && j < n) ? G[lane + (long long)n * j] : T(0);
+  bool used = lane >= n;
   bool singular = false;
-  for (int k = 0; k < n; ++k) {
-    const int buf = k & 1;
-    const int kb = k >> 4, kt = k & 15;
-    if (tx == kt) {
+  int mystep = 0, myperm = 0;
 #pragma unroll
-      for (int j = 0; j < RC; ++j)
-        if (j == kb) {
-#pragma unroll
-          for (int i = 0; i < RR; ++i) {
-            const int r = ty + 32 * i;
-            if (r < n) colk[buf][r] = a[i][j];
-          }
-        }
-    }
-    __syncthreads();
-    // every warp finds the pivot (largest |a_rk| over unused rows, first on ties)
-    T best = T(-1);
-    int bi = n;
-#pragma unroll
-    for (int q = 0; q < (INV_MAX_N + 31) / 32; ++q) {
-      const int r = lane + 32 * q;
-      if (r < n && !((used >> q) & 1u)) {
-        const T v = absval(colk[buf][r]);
-        if (v > best) { best = v; bi = r; }
-      }
-    }
+  for (int k = 0; k < 32; ++k) {
+    if (k >= n) break;
+    T best = used ? T(-1) : absval(a[k]);
+    int bi = used ? n : lane;
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) {
       const T ob = __shfl_xor_sync(0xffffffffu, best, off);
@@ -340,59 +312,146 @@ __global__ void __launch_bounds__(512, sizeof(T) == 4 ? 2 : 1)
     }
     if (!(best > T(0)) || bi >= n) {
       singular = true;
-      // continue on the first unused row so the block still terminates
-      bi = n;
-      for (int r = 0; r < n; ++r) {
-        const int owner = r & 31, q = r >> 5;
-        const unsigned u = __shfl_sync(0xffffffffu, used, owner);
-        if (!((u >> q) & 1u)) { bi = r; break; }
-      }
-      if (bi >= n) bi = 0;
+      const unsigned free_rows = __ballot_sync(0xffffffffu, !used);
+      bi = free_rows ? __ffs(free_rows) - 1 : 0;
     }
     const int p = bi;
-    if (lane == (p & 31)) used |= 1u << (p >> 5);
-    const T d = T(1) / colk[buf][p];
-    if (threadIdx.x == 0) perm[k] = p;
-    const int pa = p >> 5, pt = p & 31;
-    if (ty == pt) {
+    const T d = T(1) / __shfl_sync(0xffffffffu, a[k], p);
+    if (lane == p) { used = true; mystep = k; }
+    if (lane == k) myperm = p;
+    const T f = a[k];
 #pragma unroll
-      for (int i = 0; i < RR; ++i)
-        if (i == pa) {
-#pragma unroll
-          for (int j = 0; j < RC; ++j) {
-            const int c = tx + 16 * j;
-            const T v = (c == k) ? d : a[i][j] * d;
-            a[i][j] = v;
-            if (c < n) rowp[buf][c] = v;
-          }
-        }
+    for (int j = 0; j < 32; ++j) {
+      const T rpd = __shfl_sync(0xffffffffu, a[j], p) * d;   // a_pj d
+      if (lane == p) a[j] = (j == k) ? d : rpd;
+      else a[j] = (j == k) ? -f * d : a[j] - f * rpd;
     }
-    __syncthreads();
-    T fv[RR], rv[RC];
+  }
+  if (singular && lane == 0) atomicExch(flag, 1);
+  // entry (r, c) of the tableau is inverse(pos[r], perm[c]); pos[r] = the step of row r
 #pragma unroll
-    for (int i = 0; i < RR; ++i) {
-      const int r = ty + 32 * i;
-      fv[i] = (r < n) ? colk[buf][r] : T(0);
-    }
+  for (int c = 0; c < 32; ++c) {
+    const int pc = __shfl_sync(0xffffffffu, myperm, c);
+    if (c < n && lane < n) G[mystep + (long long)n * pc] = a[c];
+  }
+}
+
+// 32 < n <= 16 RC: a CTA of 16 x TY threads; thread (tx, ty) owns rows ty + TY i (i < RR)
+// and columns tx + 16 j (j < RC).  The pivot loop runs over column blocks kb (unrolled) and
+// columns kt within them, so the register column of the pivot column is known at compile
+// time.  Each step: the owners of column k publish it, every warp finds the pivot, the
+// owners of the pivot row publish it scaled by d, every thread updates its entries.  The
+// column and row buffers alternate between steps, so one barrier after each publication
+// suffices.
+template <typename T, int TY, int RR, int RC>
+__global__ void __launch_bounds__(16 * TY, (sizeof(T) == 4 && TY == 16) ? 2 : 1)
+    inverse_kernel(T* Aall, int n, long long stride, int* flag) {
+  __shared__ T colk[2][INV_MAX_N];
+  __shared__ T rowp[2][INV_MAX_N];
+  __shared__ int perm[INV_MAX_N];   // perm[k] = pivot row of step k
+  __shared__ int pos[INV_MAX_N];
+  T* G = Aall + (long long)blockIdx.x * stride;
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  const int lane = threadIdx.x & 31;
+  T a[RR][RC];
+#pragma unroll
+  for (int i = 0; i < RR; ++i)
 #pragma unroll
     for (int j = 0; j < RC; ++j) {
-      const int c = tx + 16 * j;
-      rv[j] = (c < n) ? rowp[buf][c] : T(0);
+      const int r = ty + TY * i, c = tx + 16 * j;
+      a[i][j] = (r < n && c < n) ? G[r + (long long)n * c] : T(0);
     }
+  unsigned used = 0u;  // bit q: row lane + 32 q already pivoted (identical in every warp)
+  bool singular = false;
+  int step = 0;
 #pragma unroll
-    for (int i = 0; i < RR; ++i) {
-      const int r = ty + 32 * i;
-      if (r == p) continue;
+  for (int kb = 0; kb < RC; ++kb) {
+    for (int kt = 0; kt < 16; ++kt) {
+      const int k = 16 * kb + kt;
+      if (k >= n) break;
+      const int buf = step & 1;
+      ++step;
+      if (tx == kt) {
+#pragma unroll
+        for (int i = 0; i < RR; ++i) {
+          const int r = ty + TY * i;
+          if (r < n) colk[buf][r] = a[i][kb];
+        }
+      }
+      __syncthreads();
+      T best = T(-1);
+      int bi = n;
+#pragma unroll
+      for (int q = 0; q < (TY * RR + 31) / 32; ++q) {
+        const int r = lane + 32 * q;
+        if (r < n && !((used >> q) & 1u)) {
+          const T v = absval(colk[buf][r]);
+          if (v > best) { best = v; bi = r; }
+        }
+      }
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) {
+        const T ob = __shfl_xor_sync(0xffffffffu, best, off);
+        const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
+        if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
+      }
+      if (!(best > T(0)) || bi >= n) {
+        singular = true;
+        // continue on the first unused row so the block still terminates
+        bi = n;
+        for (int r = 0; r < n; ++r) {
+          const unsigned u = __shfl_sync(0xffffffffu, used, r & 31);
+          if (!((u >> (r >> 5)) & 1u)) { bi = r; break; }
+        }
+        if (bi >= n) bi = 0;
+      }
+      const int p = bi;
+      if (lane == (p & 31)) used |= 1u << (p >> 5);
+      const T d = T(1) / colk[buf][p];
+      if (threadIdx.x == 0) perm[k] = p;
+      const int pa = p / TY, pt = p % TY;
+      if (ty == pt) {
+#pragma unroll
+        for (int i = 0; i < RR; ++i)
+          if (i == pa) {
+#pragma unroll
+            for (int j = 0; j < RC; ++j) {
+              const int c = tx + 16 * j;
+              const T v = (j == kb && tx == kt) ? d : a[i][j] * d;
+              a[i][j] = v;
+              if (c < n) rowp[buf][c] = v;
+            }
+          }
+      }
+      __syncthreads();
+      T fv[RR], rv[RC];
+      bool isp[RR];
+#pragma unroll
+      for (int i = 0; i < RR; ++i) {
+        const int r = ty + TY * i;
+        isp[i] = (r == p);
+        fv[i] = (r < n && r != p) ? colk[buf][r] : T(0);
+      }
 #pragma unroll
       for (int j = 0; j < RC; ++j) {
         const int c = tx + 16 * j;
-        a[i][j] = (c == k) ? -fv[i] * d : a[i][j] - fv[i] * rv[j];
+        rv[j] = (c < n) ? rowp[buf][c] : T(0);
       }
+#pragma unroll
+      for (int i = 0; i < RR; ++i)
+#pragma unroll
+        for (int j = 0; j < RC; ++j) {
+          if (j == kb) {
+            // column k: -a_ik d off the pivot row (the pivot row holds d already)
+            if (tx == kt) { if (!isp[i]) a[i][j] = -fv[i] * d; }
+            else a[i][j] = a[i][j] - fv[i] * rv[j];
+          } else {
+            a[i][j] = a[i][j] - fv[i] * rv[j];
+          }
+        }
     }
   }
   if (singular && threadIdx.x == 0) atomicExch(flag, 1);
-  // element (r, c) of the exchanged tableau is inverse(pos[r], perm[c]) with pos = perm^-1
-  __shared__ int pos[INV_MAX_N];
   __syncthreads();
   for (int t = threadIdx.x; t < n; t += blockDim.x) pos[perm[t]] = t;
   __syncthreads();
@@ -400,14 +459,15 @@ __global__ void __launch_bounds__(512, sizeof(T) == 4 ? 2 : 1)
   for (int i = 0; i < RR; ++i)
 #pragma unroll
     for (int j = 0; j < RC; ++j) {
-      const int r = ty + 32 * i, c = tx + 16 * j;
+      const int r = ty + TY * i, c = tx + 16 * j;
       if (r < n && c < n) G[pos[r] + (long long)n * perm[c]] = a[i][j];
     }
 }
 
-template <typename T, int RR, int RC>
+template <typename T, int TY, int RR, int RC>
 int launch_inverse(T* A, int n, long long stride, int batch, int* d_flag, cudaStream_t st) {
-  inverse_kernel<T, RR, RC><<<batch, 512, 0, st>>>(A, n, stride, d_flag);
+  static_assert(TY * RR <= INV_MAX_N + 31 && 16 * RC <= INV_MAX_N, "inverse tile exceeds the buffers");
+  inverse_kernel<T, TY, RR, RC><<<batch, 16 * TY, 0, st>>>(A, n, stride, d_flag);
   EXA_LAUNCH_CHECK();
   return EXA_OK;
 }
@@ -419,15 +479,29 @@ int inverse_dispatch(T* A, int n, long long stride, int batch, int* d_flag, cuda
     exa_set_error("dense inverse of order %d exceeds the register kernel limit %d", n, INV_MAX_N);
     return EXA_ERR_UNSUPPORTED;
   }
-  const int rr = (n + 31) / 32, rc = (n + 15) / 16;
-  // rows per thread 1..5, columns per thread 1..10
-  if (rr <= 1 && rc <= 2) return launch_inverse<T, 1, 2>(A, n, stride, batch, d_flag, st);
-  if (rr <= 1 && rc <= 4) return launch_inverse<T, 1, 4>(A, n, stride, batch, d_flag, st);
-  if (rr <= 2 && rc <= 4) return launch_inverse<T, 2, 4>(A, n, stride, batch, d_flag, st);
-  if (rr <= 2 && rc <= 6) return launch_inverse<T, 2, 6>(A, n, stride, batch, d_flag, st);
-  if (rr <= 3 && rc <= 6) return launch_inverse<T, 3, 6>(A, n, stride, batch, d_flag, st);
-  if (rr <= 4 && rc <= 8) return launch_inverse<T, 4, 8>(A, n, stride, batch, d_flag, st);
-  return launch_inverse<T, 5, 10>(A, n, stride, batch, d_flag, st);
+  if (n <= 32) {
+    for (int b0 = 0; b0 < batch; b0 += 8 * 65535) {
+      const int nb = (batch - b0 < 8 * 65535) ? batch - b0 : 8 * 65535;
+      inverse_warp_kernel<T><<<exa_ceil_div(nb, 8), 256, 0, st>>>(A + (long long)b0 * stride, n, stride, nb, d_flag);
+      EXA_LAUNCH_CHECK();
+    }
+    return EXA_OK;
+  }
+  const int rc = (n + 15) / 16;
+  // FP32 blocks up to 128: 256 threads with 8 x 8 entries each, two CTAs per SM
+  if constexpr (sizeof(T) == 4) {
+    if (n <= 128) {
+      if (rc <= 4) return launch_inverse<T, 16, 4, 4>(A, n, stride, batch, d_flag, st);
+      if (rc <= 6) return launch_inverse<T, 16, 6, 6>(A, n, stride, batch, d_flag, st);
+      return launch_inverse<T, 16, 8, 8>(A, n, stride, batch, d_flag, st);
+    }
+  }
+  const int rr = (n + 31) / 32;
+  if (rr <= 2 && rc <= 4) return launch_inverse<T, 32, 2, 4>(A, n, stride, batch, d_flag, st);
+  if (rr <= 2 && rc <= 6) return launch_inverse<T, 32, 2, 6>(A, n, stride, batch, d_flag, st);
+  if (rr <= 3 && rc <= 6) return launch_inverse<T, 32, 3, 6>(A, n, stride, batch, d_flag, st);
+  if (rr <= 4 && rc <= 8) return launch_inverse<T, 32, 4, 8>(A, n, stride, batch, d_flag, st);
+  return launch_inverse<T, 32, 5, 10>(A, n, stride, batch, d_flag, st);
 }
 }  // namespace
 
