@@ -239,38 +239,46 @@ namespace {
 constexpr int PST = 3;    // stages
 constexpr int PNT = 128;  // threads (4 warps: epilogue lanes 0..127)
 
-// one CTA per batch entry (b1, b2); a warp fills one 8-row x 16-k group (four core
-// matrices, 512 contiguous bytes per part): lane (ki, r8) converts the four k of its row in
-// core ki and stores them as one float4 per part
+// one CTA per (batch entry, row tile): lane l of a warp takes row 32 rb + l of the tile and
+// four consecutive k, so a warp's loads of one k are 32 consecutive rows of a column-major
+// source and its float4 stores fill whole 128-byte rows of four core matrices.  Offsets
+// within the tile follow pack_off with the tile's group count fixed once, without
+// divisions in the loop.
 template <typename TS>
 __global__ void __launch_bounds__(256) pack_kernel(const TS* src, long long rs, long long ks, long long sb,
-                                                   long long sb2, int batch2, UPacked d) {
-  const int nkc = (d.K + PK - 1) / PK, NG = (d.R + 7) / 8;
-  const long long b2 = blockIdx.x % batch2, b1 = blockIdx.x / batch2;
+                                                   long long sb2, int batch2, int ntiles, UPacked d) {
+  const int t = blockIdx.x % ntiles;
+  const long long e = blockIdx.x / ntiles;
+  const long long b2 = e % batch2, b1 = e / batch2;
   const TS* X = src + b1 * sb + b2 * sb2;
-  float* hi = d.hi + b1 * d.sb + b2 * d.sb2;
-  float* lo = d.lo ? d.lo + b1 * d.sb + b2 * d.sb2 : nullptr;
+  const int nkc = (d.K + PK - 1) / PK;
+  const long long tbase = b1 * d.sb + b2 * d.sb2 + (long long)t * (d.TR / 8) * nkc * 128;
+  float* hi = d.hi + tbase;
+  float* lo = d.lo ? d.lo + tbase : nullptr;
+  const int r0 = t * d.TR;
+  const int rows_t = min(d.TR, d.R - r0), ng = (rows_t + 7) / 8;
+  const int nrb = (ng * 8 + 31) / 32, nkq = nkc * 4;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int ki = lane >> 3, r8 = lane & 7;
-  const int npair = NG * nkc;
-  for (int p = warp; p < npair; p += blockDim.x >> 5) {
-    const int G = p / nkc, kc = p - G * nkc;
-    const int row = 8 * G + r8, k0 = PK * kc + 4 * ki;
-    float4 h, l;
-    float* hp = &h.x;
-    float* lp = &l.x;
+  for (int kq = warp; kq < nkq; kq += blockDim.x >> 5) {
+    const int k0 = 4 * kq;
+    const long long ocol = (long long)(kq >> 2) * ng * 128 + (kq & 3) * 32;
+    for (int rb = 0; rb < nrb; ++rb) {
+      const int lr = 32 * rb + lane;
+      if (lr >= ng * 8) break;
+      const int row = r0 + lr;
+      float4 h, l;
+      float* hp = &h.x;
+      float* lp = &l.x;
 #pragma unroll
-    for (int k4 = 0; k4 < 4; ++k4) {
-      const int k = k0 + k4;
-      const double x = (row < d.R && k < d.K) ? (double)X[row * rs + k * ks] : 0.0;
-      split_tf32(x, hp[k4], lp[k4]);
+      for (int k4 = 0; k4 < 4; ++k4) {
+        const int k = k0 + k4;
+        const double x = (row < d.R && k < d.K) ? (double)X[row * rs + k * ks] : 0.0;
+        split_tf32(x, hp[k4], lp[k4]);
+      }
+      const long long o = ocol + (lr >> 3) * 128 + (lr & 7) * 4;
+      *reinterpret_cast<float4*>(hi + o) = h;
+      if (lo) *reinterpret_cast<float4*>(lo + o) = l;
     }
-    // tile t of TR rows: groups of earlier tiles are full, this tile has ng groups
-    const int t = (8 * G) / d.TR, g = G - t * (d.TR / 8);
-    const int rows_t = min(d.TR, d.R - t * d.TR), ng = (rows_t + 7) / 8;
-    const long long o = (long long)t * (d.TR / 8) * nkc * 128 + (long long)kc * ng * 128 + g * 128 + ki * 32 + r8 * 4;
-    *reinterpret_cast<float4*>(hi + o) = h;
-    if (lo) *reinterpret_cast<float4*>(lo + o) = l;
   }
 }
 
@@ -493,15 +501,16 @@ int exa_pack(const void* src, int src_f64, long long rs, long long ks, long long
     exa_set_error("pack: tile height %d is not a multiple of 8", d.TR);
     return EXA_ERR_ARG;
   }
-  if ((long long)batch * batch2 > 0x7fffffffLL) {
+  const int ntiles = (d.R + d.TR - 1) / d.TR;
+  if ((long long)batch * batch2 * ntiles > 0x7fffffffLL) {
     exa_set_error("pack: %d x %d batch entries exceed the grid", batch, batch2);
     return EXA_ERR_ARG;
   }
-  const unsigned grid = (unsigned)((long long)batch * batch2);
+  const unsigned grid = (unsigned)((long long)batch * batch2 * ntiles);
   if (src_f64)
-    pack_kernel<double><<<grid, 256, 0, st>>>((const double*)src, rs, ks, sb, sb2, batch2, d);
+    pack_kernel<double><<<grid, 256, 0, st>>>((const double*)src, rs, ks, sb, sb2, batch2, ntiles, d);
   else
-    pack_kernel<float><<<grid, 256, 0, st>>>((const float*)src, rs, ks, sb, sb2, batch2, d);
+    pack_kernel<float><<<grid, 256, 0, st>>>((const float*)src, rs, ks, sb, sb2, batch2, ntiles, d);
   EXA_LAUNCH_CHECK();
   return EXA_OK;
 }
