@@ -255,7 +255,9 @@ __global__ void face_kernel(AsmArgs A, double* Ru, double* Rh, double* D, double
   const int npe = P.npe, npf = P.npf, ngf = P.ngf, nc = P.nc, ncu = P.ncu, nd = P.nd, ncx = P.ncx;
   const int nfe = P.nfe, ndf = P.ndf, n = P.n, m = P.m;
   const int nqn = npe * nd * ncu;  // columns of B and G
-  double* uhn = sm;                   // npf*ncu
+  double* sW = sm;                    // npf*ngf: shapfgw[:, :, 0]
+  double* sT = sW + npf * ngf;        // ngf*npf: shapfgt[:, :, 0]
+  double* uhn = sT + npf * ngf;       // npf*ncu
   double* un = uhn + npf * ncu;       // npf*nc
   double* uhg = un + npf * nc;        // ngf*ncu
   double* ugq = uhg + ngf * ncu;      // ngf*nc   (u, q)
@@ -269,6 +271,10 @@ __global__ void face_kernel(AsmArgs A, double* Ru, double* Rh, double* D, double
   double* fb_uq = fh_uh + ngf * ncu * ncu;   // ngf*ncu*nc
   double* fb_uh = fb_uq + ngf * ncu * nc;    // ngf*ncu*ncu
   __shared__ int s_ib;
+  for (int t = threadIdx.x; t < npf * ngf; t += blockDim.x) {
+    sW[t] = A.shapfgw[t];
+    sT[t] = A.shapfgt[t];
+  }
 
   const double* U = A.udg + (long long)e * npe * nc;
   double* Rue = Ru + (long long)le * n;
@@ -302,13 +308,13 @@ __global__ void face_kernel(AsmArgs A, double* Ru, double* Rh, double* D, double
     for (int t = threadIdx.x; t < ngf * ncu; t += blockDim.x) {
       const int g = t % ngf, k = t / ngf;
       double s = 0.0;
-      for (int a = 0; a < npf; ++a) s = fma(A.shapfgt[g + ngf * a], uhn[a + npf * k], s);
+      for (int a = 0; a < npf; ++a) s = fma(sT[g + ngf * a], uhn[a + npf * k], s);
       uhg[t] = s;
     }
     for (int t = threadIdx.x; t < ngf * nc; t += blockDim.x) {
       const int g = t % ngf, c = t / ngf;
       double s = 0.0;
-      for (int a = 0; a < npf; ++a) s = fma(A.shapfgt[g + ngf * a], un[a + npf * c], s);
+      for (int a = 0; a < npf; ++a) s = fma(sT[g + ngf * a], un[a + npf * c], s);
       ugq[t] = s;
     }
     __syncthreads();
@@ -368,8 +374,8 @@ __global__ void face_kernel(AsmArgs A, double* Ru, double* Rh, double* D, double
       const int a = t % npf, k = t / npf;
       double s = 0.0, r = 0.0;
       for (int g = 0; g < ngf; ++g) {
-        s = fma(A.shapfgw[a + npf * g], fh[g + ngf * k], s);
-        r = fma(A.shapfgw[a + npf * g], fT[g + ngf * k], r);
+        s = fma(sW[a + npf * g], fh[g + ngf * k], s);
+        r = fma(sW[a + npf * g], fT[g + ngf * k], r);
       }
       Rue[pl[a] + npe * k] -= s;
       Rhe[k + ncu * (a + npf * l)] = -r;
@@ -383,30 +389,51 @@ __global__ void face_kernel(AsmArgs A, double* Ru, double* Rh, double* D, double
       double* Ke = K + (long long)le * m * n;
       double* Ge = G + (long long)le * m * nqn;
       double* He = H + (long long)le * m * m;
-      for (int t = threadIdx.x; t < npf * npf * ncu * nc; t += blockDim.x) {
-        const int a = t % npf, b = (t / npf) % npf, k = (t / (npf * npf)) % ncu, c = t / (npf * npf * ncu);
-        double vq = 0.0, vT = 0.0, vh = 0.0, vTh = 0.0;
-        for (int g = 0; g < ngf; ++g) {
-          const double w = A.shapfgw[a + npf * g] * A.shapfgt[g + ngf * b];
-          vq = fma(w, fh_uq[g + ngf * (k + ncu * c)], vq);
-          vT = fma(w, fT_uq[g + ngf * (k + ncu * c)], vT);
-          if (c < ncu) {
-            vh = fma(w, fh_uh[g + ngf * (k + ncu * c)], vh);
-            vTh = fma(w, fT_uh[g + ngf * (k + ncu * c)], vTh);
+      // one thread per face-node pair (a, b): the weight w_g = shapfgw[a, g] shapfgt[g, b] is
+      // formed once per g and shared by every column q = k + ncu c, taken QC at a time
+      constexpr int QC = 4;
+      const int nq = ncu * nc;
+      for (int ab = threadIdx.x; ab < npf * npf; ab += blockDim.x) {
+        const int a = ab % npf, b = ab / npf;
+        const int pa = pl[a], pb = pl[b];
+        for (int q0 = 0; q0 < nq; q0 += QC) {
+          double vq[QC], vT[QC], vh[QC], vTh[QC];
+#pragma unroll
+          for (int u = 0; u < QC; ++u) vq[u] = vT[u] = vh[u] = vTh[u] = 0.0;
+          for (int g = 0; g < ngf; ++g) {
+            const double w = sW[a + npf * g] * sT[g + ngf * b];
+#pragma unroll
+            for (int u = 0; u < QC; ++u) {
+              const int q = q0 + u;
+              if (q < nq) {
+                vq[u] = fma(w, fh_uq[g + ngf * q], vq[u]);
+                vT[u] = fma(w, fT_uq[g + ngf * q], vT[u]);
+                if (q < ncu * ncu) {
+                  vh[u] = fma(w, fh_uh[g + ngf * q], vh[u]);
+                  vTh[u] = fma(w, fT_uh[g + ngf * q], vTh[u]);
+                }
+              }
+            }
           }
-        }
-        const int row_e = pl[a] + npe * k;           // element row (i,k)
-        const int row_t = k + ncu * (a + npf * l);   // trace row (k, jf)
-        if (c < ncu) {
-          De[row_e + (long long)n * (pl[b] + npe * c)] += vq;
-          Fe[row_e + (long long)n * (c + ncu * (b + npf * l))] = vh;
-          Ke[row_t + (long long)m * (pl[b] + npe * c)] = vT;
-          He[row_t + (long long)m * (c + ncu * (b + npf * l))] = vTh;
-        } else {
-          const int qc = c - ncu, nq = qc % ncu, d = qc / ncu;
-          const long long col = pl[b] + (long long)npe * d + (long long)npe * nd * nq;
-          Be[row_e + (long long)n * col] += vq;
-          Ge[row_t + (long long)m * col] = vT;
+#pragma unroll
+          for (int u = 0; u < QC; ++u) {
+            const int q = q0 + u;
+            if (q >= nq) break;
+            const int k = q % ncu, c = q / ncu;
+            const int row_e = pa + npe * k;             // element row (i,k)
+            const int row_t = k + ncu * (a + npf * l);  // trace row (k, jf)
+            if (c < ncu) {
+              De[row_e + (long long)n * (pb + npe * c)] += vq[u];
+              Fe[row_e + (long long)n * (c + ncu * (b + npf * l))] = vh[u];
+              Ke[row_t + (long long)m * (pb + npe * c)] = vT[u];
+              He[row_t + (long long)m * (c + ncu * (b + npf * l))] = vTh[u];
+            } else {
+              const int qc = c - ncu, nqc = qc % ncu, d = qc / ncu;
+              const long long col = pb + (long long)npe * d + (long long)npe * nd * nqc;
+              Be[row_e + (long long)n * col] += vq[u];
+              Ge[row_t + (long long)m * col] = vT[u];
+            }
+          }
         }
       }
     }
@@ -417,6 +444,7 @@ __global__ void face_kernel(AsmArgs A, double* Ru, double* Rh, double* D, double
 inline size_t face_smem(const ExaDims& P, bool jac) {
   size_t s = (size_t)P.npf * (P.ncu + P.nc) + (size_t)P.ngf * (P.ncu + 2 * P.nc + P.ncu * P.nd + 2 * P.ncu);
   if (jac) s += (size_t)P.ngf * P.ncu * (P.nd * P.nc + 2 * P.nc + 2 * P.ncu);
+  s += 2 * (size_t)P.npf * P.ngf;  // shapfgw, shapfgt
   return s * sizeof(double);
 }
 

@@ -190,31 +190,45 @@ __global__ void __launch_bounds__(256) elem_matvec_kernel(ExaDims P, const int* 
   double* ve = sm;             // [m]
   double* part = sm + P.m;     // [8][m]
   const int e = blockIdx.x, m = P.m, ncu = P.ncu;
-  for (int r = threadIdx.x; r < m; r += blockDim.x) ve[r] = v[r % ncu + ncu * (long long)elemcon[r / ncu + P.ndf * e]];
-  __syncthreads();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const T* Ae = A + (long long)e * m * m;
-  double acc[RI];
-#pragma unroll
-  for (int i = 0; i < RI; ++i) acc[i] = 0.0;
-  int c = warp;
-  // four columns (c, c + 8, c + 16, c + 24) per step: 4 RI independent loads per thread
-  for (; c + 24 < m; c += 32) {
-    T y[4][RI];
+  // four columns (c, c + 8, c + 16, c + 24) per step: 4 RI independent loads per thread; the
+  // next step's columns are loaded while this step's are used, and the first step's before
+  // the gather of the element's trace values
+  auto load4 = [&](int c0, T (&y)[4][RI]) {
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
-      const T* a = Ae + (long long)m * (c + 8 * u);
+      const T* a = Ae + (long long)m * (c0 + 8 * u);
 #pragma unroll
       for (int i = 0; i < RI; ++i) {
         const int r = lane + 32 * i;
         y[u][i] = r < m ? a[r] : T(0);
       }
     }
+  };
+  int c = warp;
+  T y[4][RI];
+  if (c + 24 < m) load4(c, y);
+  for (int r = threadIdx.x; r < m; r += blockDim.x) ve[r] = v[r % ncu + ncu * (long long)elemcon[r / ncu + P.ndf * e]];
+  __syncthreads();
+  double acc[RI];
+#pragma unroll
+  for (int i = 0; i < RI; ++i) acc[i] = 0.0;
+  for (; c + 24 < m; c += 32) {
+    T yn[4][RI];
+    const bool more = c + 56 < m;
+    if (more) load4(c + 32, yn);
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
       const double x = ve[c + 8 * u];
 #pragma unroll
       for (int i = 0; i < RI; ++i) acc[i] = fma((double)y[u][i], x, acc[i]);
+    }
+    if (more) {
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int i = 0; i < RI; ++i) y[u][i] = yn[u][i];
     }
   }
   for (; c < m; c += 8) {
@@ -399,9 +413,13 @@ template <typename T>
 int exa_k_elem_matvec(const ExaDims& P, const int* elemcon, const T* A, const double* v, double* we,
                       cudaStream_t st) {
   const size_t smem = sizeof(double) * (size_t)P.m * 9;
+  // rows per lane: exactly ceil(m / 32) up to 6, so no register holds a row past m
   if (P.m <= 32) elem_matvec_kernel<T, 1><<<P.ne, 256, smem, st>>>(P, elemcon, A, v, we);
   else if (P.m <= 64) elem_matvec_kernel<T, 2><<<P.ne, 256, smem, st>>>(P, elemcon, A, v, we);
+  else if (P.m <= 96) elem_matvec_kernel<T, 3><<<P.ne, 256, smem, st>>>(P, elemcon, A, v, we);
   else if (P.m <= 128) elem_matvec_kernel<T, 4><<<P.ne, 256, smem, st>>>(P, elemcon, A, v, we);
+  else if (P.m <= 160) elem_matvec_kernel<T, 5><<<P.ne, 256, smem, st>>>(P, elemcon, A, v, we);
+  else if (P.m <= 192) elem_matvec_kernel<T, 6><<<P.ne, 256, smem, st>>>(P, elemcon, A, v, we);
   else if (P.m <= 256) elem_matvec_kernel<T, 8><<<P.ne, 256, smem, st>>>(P, elemcon, A, v, we);
   else if (P.m <= 512) elem_matvec_kernel<T, 16><<<P.ne, 256, smem, st>>>(P, elemcon, A, v, we);
   else {
