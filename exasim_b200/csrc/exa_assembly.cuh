@@ -14,6 +14,8 @@
 // sequence, so face contributions accumulate into D, B and Ru without atomics.
 #pragma once
 #include "exa_kernels.cuh"
+#include "exa_tc.cuh"
+#include "exa_umma.cuh"
 
 struct AsmArgs {
   ExaDims P;
@@ -25,6 +27,9 @@ struct AsmArgs {
   double time, dtfactor;
   int tdep, tdfunc, sourcefunc, modelnumber;
   int e0;  // first element of the chunk; per-chunk outputs are indexed from it
+  // mixed form: G goes straight into the packed 3xTF32 operand of the q elimination (one
+  // part per trace component) instead of the FP64 G; unused when Gp.hi is null
+  UPacked Gp;
 };
 
 // ----------------------------------------------------------------------------------
@@ -431,7 +436,16 @@ __global__ void face_kernel(AsmArgs A, double* Ru, double* Rh, double* D, double
               const int qc = c - ncu, nqc = qc % ncu, d = qc / ncu;
               const long long col = pb + (long long)npe * d + (long long)npe * nd * nqc;
               Be[row_e + (long long)n * col] += vq[u];
-              Ge[row_t + (long long)m * col] = vT[u];
+              if (A.Gp.hi) {
+                const long long o = (long long)le * A.Gp.sb + (long long)nqc * A.Gp.sb2 +
+                                    exa_tc::pack_off(row_t, pb + npe * d, m, npe * nd, A.Gp.TR);
+                float h, lo;
+                exa_tc::split_tf32(vT[u], h, lo);
+                A.Gp.hi[o] = h;
+                A.Gp.lo[o] = lo;
+              } else {
+                Ge[row_t + (long long)m * col] = vT[u];
+              }
             }
           }
         }

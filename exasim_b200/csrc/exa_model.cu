@@ -137,7 +137,7 @@ int schur_chunk_mixed(ExaCtx& c, int e0, int nb) {
       // B and G per trace component: row r, k = (l, d) at column l + npe*d + npe*nd*b
       ExaProfScope pp(c, EXA_PH_PACK);
       EXA_TRY(exa_pack(c.wB, 1, 1, n, (long long)n * nqn, (long long)n * kq, nb, ncu, c.wBp, c.st));
-      EXA_TRY(exa_pack(c.wG, 1, 1, m, (long long)m * nqn, (long long)m * kq, nb, ncu, c.wGp, c.st));
+      // G is already packed: the face kernel writes it in this layout in the mixed form
     }
     ExaProfScope ps(c, EXA_PH_QELIM);
     exa_prof_flops(c, EXA_PH_QELIM, 2.0 * nb * ncu * (double)npe * nd * (double)(n + m) * (npe + ndf));
@@ -258,7 +258,17 @@ int exa_model_assemble(ExaCtx& c, bool jacobian) {
         ExaProfScope ps(c, EXA_PH_FACE);
         EXA_CUDA(cudaMemsetAsync(c.wF, 0, sizeof(double) * (size_t)nb * n * m, c.st));
         EXA_CUDA(cudaMemsetAsync(c.wK, 0, sizeof(double) * (size_t)nb * m * n, c.st));
-        if (nqn > 0 && P.ncq > 0) EXA_CUDA(cudaMemsetAsync(c.wG, 0, sizeof(double) * (size_t)nb * m * nqn, c.st));
+        if (nqn > 0 && P.ncq > 0) {
+          if (c.precision == 1 && c.wGp.hi) {
+            // G written packed by the face kernel (its zeros included, as the pack would)
+            A.Gp = c.wGp;
+            const size_t gp = (size_t)nb * c.wGp.sb;
+            EXA_CUDA(cudaMemsetAsync(c.wGp.hi, 0, sizeof(float) * gp, c.st));
+            EXA_CUDA(cudaMemsetAsync(c.wGp.lo, 0, sizeof(float) * gp, c.st));
+          } else {
+            EXA_CUDA(cudaMemsetAsync(c.wG, 0, sizeof(double) * (size_t)nb * m * nqn, c.st));
+          }
+        }
         EXA_CUDA(cudaMemsetAsync(Hc, 0, sizeof(double) * (size_t)nb * m * m, c.st));
         face_kernel<ExaModel, true><<<nb, tpb_f, fs, c.st>>>(A, Ruc, Rhc, c.wD, c.wB, c.wF, c.wK, c.wG, Hc);
         EXA_LAUNCH_CHECK();
