@@ -449,6 +449,10 @@ def run_served(args, device):
 # workload: 4.458 GB for 1000 elements; it scales with the element count (each element's
 # blocks are read once), so per launch and element it is 4.458e9 / 1000 / 4 bytes.
 QELIM_TRAFFIC_PER_ELEMENT_LAUNCH = 4.458e9 / 1000 / 4
+# The same for the mixed form's four 3xTF32 q-elimination launches (umma3_kernel), one ncu
+# capture on the 10^3 mesh: 0.969, 1.152, 1.222 and 1.198 GB read + written, mean 1.135 GB
+# per launch for 1000 elements.
+QELIM_MIXED_TRAFFIC_PER_ELEMENT_LAUNCH = 1.1351e9 / 1000
 
 
 def fp64_gemm_peak(torch):
@@ -507,7 +511,9 @@ def kernel_rooflines(s32, s64, mixed, plain, torch, steps):
                 "bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                 "frac": achieved / peaks["hbm_gbs"], "peak_source": src,
                 "algorithmic_bytes_per_launch": qbytes / 4, "ms_per_launch": ms_launch, "launches": launches,
-                "traffic": None}
+                "traffic": QELIM_MIXED_TRAFFIC_PER_ELEMENT_LAUNCH * ne,
+                "traffic_source": "ncu dram bytes of the four launches on a 10^3 mesh, mean per launch, scaled by "
+                                  "element count"}
     p_ms, p_regions, p_flops = plain["prof"]["qelim"]
     peak64 = fp64_gemm_peak(torch)
     pl = 4 * p_regions
