@@ -104,8 +104,10 @@ def cdsin2d_quad(datain: str, n: int = 16, porder: int = 3, kappa: float = 0.01,
                  a: int = 1, b: int = 1, gmres_tol: float = 1e-8, restart: int = 50, preconditioner: int = 0):
     grid = I.square_quad_grid(n)
     master = I.make_master(2, 1, porder, 2 * porder)
+    # up to 100 restart cycles: strongly convective requests (kappa near 1e-3) need more than
+    # 1000 block-Jacobi GMRES iterations to reach the tolerance
     app = I.PDEApp(nd=2, ncu=1, model="ModelD", preconditioner=preconditioner, NewtonIter=1,
-                   NewtonTol=1e-8, GMRESiter=1000, GMRESrestart=restart, GMREStol=gmres_tol,
+                   NewtonTol=1e-8, GMRESiter=5000, GMRESrestart=restart, GMREStol=gmres_tol,
                    RBdim=0, ppdegree=1, tau=[1.0],
                    physicsparam=[kappa, float(np.cos(theta)), float(np.sin(theta)), float(a), float(b)],
                    externalparam=[0.0, 0.0])
