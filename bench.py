@@ -167,6 +167,20 @@ def cpu_baseline_sample(tmp, full_n):
                       f"{per_solve:.2f} s per solve, scaled by element count"}
 
 
+def max_over_ranks(ms, world, dist, torch, device):
+    """The slowest rank's time: whole-job throughput of independent replicas is the units of all
+    ranks over the time of the slowest (one all-reduce of one number)."""
+    t = torch.tensor([float(ms)], dtype=torch.float64, device=device)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replicas_value(steps_per_rank, world, total_ms):
+    """Whole-job solves/s of `world` replicas that each made `steps_per_rank` solves."""
+    return world * steps_per_rank / (total_ms / 1000.0)
+
+
 def run_reference(args):
     """The reference path's CPU restatement (the reference itself is not built here), one
     DIRK-stage solve on the 4^3 sub-mesh per step, reported scaled to the full mesh."""
@@ -242,10 +256,8 @@ def run_form(s, lib, torch, local, args, world, dist):
     s.profile(False)
     prof = s.profile_read()
     per = [ev[i].elapsed_time(ev[i + 1]) for i in range(args.steps)]
-    total = torch.tensor([ev[0].elapsed_time(ev[args.steps])], dtype=torch.float64, device=f"cuda:{local}")
-    if world > 1:
-        dist.all_reduce(total, op=dist.ReduceOp.MAX)
-    return {"total_ms": float(total.item()), "per": per, "gmres": gmres, "newton": newton, "ratios": ratios,
+    total = max_over_ranks(ev[0].elapsed_time(ev[args.steps]), world, dist, torch, f"cuda:{local}")
+    return {"total_ms": total, "per": per, "gmres": gmres, "newton": newton, "ratios": ratios,
             "launches": launches, "prof": prof, "clocks": clk.summary(), "stream": stream, "stage": stage}
 
 
@@ -303,8 +315,8 @@ def run_ours(args):
             return 0
         plain = run_form(s64, lib, torch, local, args, world, dist)
         mixed = run_form(s32, lib, torch, local, args, world, dist)
-        value = world * args.steps / (mixed["total_ms"] / 1000.0)
-        plain_value = world * args.steps / (plain["total_ms"] / 1000.0)
+        value = replicas_value(args.steps, world, mixed["total_ms"])
+        plain_value = replicas_value(args.steps, world, plain["total_ms"])
 
         # end-to-end: one more stage solve through the C ABI (exa_solve) from pinned host
         # buffers: its start state (saved before an untimed run of the stage) and its source
@@ -323,7 +335,8 @@ def run_ours(args):
             s32.solve(h_udg, h_uh, o_udg, o_uh)
         torch.cuda.synchronize()
         e2e_s = time.perf_counter() - t0
-        e2e = {"value": world * ne2e / e2e_s, "unit": "solves/s", "steps": ne2e,
+        e2e_ms = max_over_ranks(e2e_s * 1000.0, world, dist, torch, f"cuda:{local}")
+        e2e = {"value": replicas_value(ne2e, world, e2e_ms), "unit": "solves/s", "steps": ne2e,
                "h2d_bytes_per_step": 8 * (nu + nh + ns), "d2h_bytes_per_step": 8 * (nu + nh)}
 
         roof = kernel_rooflines(s32, s64, mixed, plain, torch, args.steps)
@@ -371,7 +384,7 @@ def run_one_form(s, lib, torch, local, args, world, dist, rank):
     """One form alone (--form mixed|plain): a partial line without the comparison, for profiling."""
     r = run_form(s, lib, torch, local, args, world, dist)
     if rank == 0:
-        print(json.dumps({"metric": METRIC, "form": args.form, "value": world * args.steps / (r["total_ms"] / 1000.0),
+        print(json.dumps({"metric": METRIC, "form": args.form, "value": replicas_value(args.steps, world, r["total_ms"]),
                           "unit": "solves/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
                           "ms_per_step": r["total_ms"] / args.steps, "config": config(args.n),
                           "gmres_iters_per_solve": float(np.mean(r["gmres"])),
