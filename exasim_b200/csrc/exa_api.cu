@@ -363,6 +363,19 @@ int exa_ctx_init(ExaCtx& c, const double* app, long long napp, const double* mas
   EXA_TRY(dev_alloc(c, &c.wRg, nb * P.nge * (P.nd + 1) * P.ncu * P.nc));
   EXA_TRY(dev_alloc(c, &c.wRu, nb * n));
   if (inv_ws) EXA_TRY(dev_alloc(c, &c.wInv, nb * inv_ws));
+  {
+    // the FP64 element products of the assembly: the fastest GEMM tile of each shape is
+    // measured once per process and device (q elimination, D^-1 F, K D^-1 F)
+    const int kq = P.npe * P.nd, nbt = (int)std::min<size_t>(nb, 512);
+    if (P.ncq > 0) {
+      EXA_TRY(exa_gemm_tune((int)n, P.npe, kq, nbt, c.st));
+      EXA_TRY(exa_gemm_tune((int)n, P.ndf, kq, nbt, c.st));
+      EXA_TRY(exa_gemm_tune((int)m, P.npe, kq, nbt, c.st));
+      EXA_TRY(exa_gemm_tune((int)m, P.ndf, kq, nbt, c.st));
+    }
+    EXA_TRY(exa_gemm_tune((int)n, (int)m, (int)n, nbt, c.st));
+    EXA_TRY(exa_gemm_tune((int)m, (int)m, (int)n, nbt, c.st));
+  }
   EXA_TRY(dev_alloc(c, &c.V, N * (size_t)(c.restart + 1)));
   EXA_TRY(dev_alloc(c, &c.x, N));
   EXA_TRY(dev_alloc(c, &c.r, N));
@@ -968,6 +981,12 @@ extern "C" int exa_gemm_3xtf32_batched(int M, int N, int K, double alpha, const 
     exa_set_error("3xtf32 gemm: %s", cudaGetErrorString(e));
     return EXA_ERR_CUDA;
   }
+  return EXA_OK;
+}
+
+extern "C" int exa_dgemm_tune(int M, int N, int K, int batch, void* stream, int* tile) {
+  EXA_TRY(exa_gemm_tune(M, N, K, batch, (cudaStream_t)stream));
+  if (tile) *tile = exa_gemm_tile_of(M, N, K);
   return EXA_OK;
 }
 

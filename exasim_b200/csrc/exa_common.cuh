@@ -83,6 +83,11 @@ struct GemmBatch {
   int batch, batch2;
 };
 int exa_gemm(const GemmBatch& g, cudaStream_t st);
+// Times the FP64 GEMM's candidate CTA tiles for one shape on scratch blocks and keeps the
+// fastest for this device (an autotuner; exa_gemm uses a padding heuristic for shapes not
+// tuned).  The tile does not change the result.  Not for use inside stream capture.
+int exa_gemm_tune(int M, int N, int K, int batch, cudaStream_t st);
+int exa_gemm_tile_of(int M, int N, int K);  // index of the tile exa_gemm uses for the shape
 
 // In-place explicit inverse of `batch` n x n column-major matrices spaced `stride`
 // doubles apart (Gauss-Jordan with partial pivoting in shared memory).  Sets

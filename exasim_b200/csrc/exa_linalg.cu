@@ -14,7 +14,10 @@
 
 #include "exa_common.cuh"
 
+#include <algorithm>
+#include <array>
 #include <atomic>
+#include <map>
 #include <mutex>
 #include <set>
 #include <utility>
@@ -225,6 +228,40 @@ int launch_dmma(const GemmBatch& g, cudaStream_t st) {
 long long tiles_cost(int M, int N, int bm, int bn) {
   return (long long)((M + bm - 1) / bm) * bm * ((N + bn - 1) / bn) * bn;
 }
+
+// CTA tiles sized to the element blocks: 128 x 64, 128 x 80, 160 x 32 and 160 x 64 cover
+// 125 -> 128 and 150 -> 160 with little padding
+constexpr int kTiles = 4;
+constexpr int kTile[kTiles][2] = {{128, 64}, {128, 80}, {160, 32}, {160, 64}};
+
+int launch_tile(int t, const GemmBatch& g, cudaStream_t st) {
+  switch (t) {
+    case 0: return launch_dmma<4, 4, 4, 2>(g, st);
+    case 1: return launch_dmma<4, 5, 4, 2>(g, st);
+    case 2: return launch_dmma<5, 2, 4, 2>(g, st);
+    default: return launch_dmma<5, 4, 4, 2>(g, st);
+  }
+}
+
+std::mutex g_tune_mu;
+std::map<std::array<int, 4>, int> g_tune;  // (device, M, N, K) -> measured fastest tile
+
+// the measured tile of this shape, else the first three tiles by padded area
+int gemm_tile(int M, int N, int K) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) == cudaSuccess) {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune.find({dev, M, N, K});
+    if (it != g_tune.end()) return it->second;
+  }
+  int best = 0;
+  long long bc = -1;
+  for (int i = 0; i < 3; ++i) {
+    const long long c = tiles_cost(M, N, kTile[i][0], kTile[i][1]);
+    if (bc < 0 || c < bc) { bc = c; best = i; }
+  }
+  return best;
+}
 }  // namespace
 
 int exa_gemm(const GemmBatch& g, cudaStream_t st) {
@@ -251,22 +288,64 @@ int exa_gemm(const GemmBatch& g, cudaStream_t st) {
     EXA_LAUNCH_CHECK();
     return EXA_OK;
   }
-  // CTA tiles sized to the element blocks: 128 x 64, 128 x 80 and 160 x 32 cover
-  // 125 -> 128 and 150 -> 160 with little padding; tiny blocks use 32 x 32 CTAs
   if (g.M <= 40 && g.N <= 40) return launch_dmma<2, 2, 2, 2>(g, st);
-  const int cand[3][2] = {{128, 64}, {128, 80}, {160, 32}};
-  int best = 0;
-  long long bc = -1;
-  for (int i = 0; i < 3; ++i) {
-    const long long c = tiles_cost(g.M, g.N, cand[i][0], cand[i][1]);
-    if (bc < 0 || c < bc) { bc = c; best = i; }
-  }
-  switch (best) {
-    case 0: return launch_dmma<4, 4, 4, 2>(g, st);
-    case 1: return launch_dmma<4, 5, 4, 2>(g, st);
-    default: return launch_dmma<5, 2, 4, 2>(g, st);
-  }
+  return launch_tile(gemm_tile(g.M, g.N, g.K), g, st);
 }
+
+// Measures the candidate tiles of an M x N x K product on `batch` scratch blocks (at most
+// 512) and keeps the fastest for this device and shape; later products of that shape use
+// it.  Every tile accumulates each entry over k in the same order, so the choice changes
+// the time, not the result.  Allocates its scratch stream-ordered on `st` and synchronizes
+// `st`; call it outside stream capture.
+int exa_gemm_tune(int M, int N, int K, int batch, cudaStream_t st) {
+  if (M <= 0 || N <= 1 || K <= 0 || (M <= 40 && N <= 40)) return EXA_OK;
+  int dev = 0;
+  EXA_CUDA(cudaGetDevice(&dev));
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    if (g_tune.count({dev, M, N, K})) return EXA_OK;
+  }
+  const int nb = std::max(1, std::min(batch, 512));
+  const size_t sa = (size_t)M * K, sb = (size_t)K * N, sc = (size_t)M * N;
+  double* buf = nullptr;
+  EXA_CUDA(cudaMallocAsync((void**)&buf, sizeof(double) * (sa + sb + sc) * nb, st));
+  // bytes 0x3f: every double is 4.8e-4, so no product overflows
+  cudaError_t e = cudaMemsetAsync(buf, 0x3f, sizeof(double) * (sa + sb) * nb, st);
+  GemmBatch g{M, N, K, 1.0, 0.0, buf, M, (long long)sa, 0, buf + sa * nb, K, (long long)sb, 0,
+              buf + (sa + sb) * nb, M, (long long)sc, 0, nb, 1};
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (e == cudaSuccess) e = cudaEventCreate(&e0);
+  if (e == cudaSuccess) e = cudaEventCreate(&e1);
+  int best = gemm_tile(M, N, K);
+  float best_ms = -1.0f;
+  for (int t = 0; t < kTiles && e == cudaSuccess; ++t) {
+    if (launch_tile(t, g, st) != EXA_OK) break;  // warm
+    e = cudaEventRecord(e0, st);
+    for (int r = 0; r < 3 && e == cudaSuccess; ++r)
+      if (launch_tile(t, g, st) != EXA_OK) e = cudaErrorUnknown;
+    if (e == cudaSuccess) e = cudaEventRecord(e1, st);
+    if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+    float ms = 0.0f;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+    if (e == cudaSuccess && (best_ms < 0 || ms < best_ms)) {
+      best_ms = ms;
+      best = t;
+    }
+  }
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  cudaFreeAsync(buf, st);
+  if (e != cudaSuccess) {
+    exa_set_error("gemm tuning of %d x %d x %d: %s", M, N, K, cudaGetErrorString(e));
+    return EXA_ERR_CUDA;
+  }
+  EXA_CUDA(cudaStreamSynchronize(st));
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tune[{dev, M, N, K}] = best;
+  return EXA_OK;
+}
+
+int exa_gemm_tile_of(int M, int N, int K) { return gemm_tile(M, N, K); }
 
 // ----------------------------------------------------------------------------------
 // batched explicit inverse.  Exasim forms the explicit inverse of each element block

@@ -138,6 +138,13 @@ int exa_dgemm_batched(int M, int N, int K, double alpha, const double* A, long l
                       const double* B, long long ldb, long long sB, double beta, double* C, long long ldc,
                       long long sC, int batch, void* stream);
 int exa_dinverse_batched(double* A, int n, long long stride, int batch, int* info_dev, void* stream);
+/* No counterpart in the reference.  Times the candidate CTA tiles of exa_dgemm_batched for
+ * one M x N x K shape on `batch` (at most 512) scratch blocks, allocated stream-ordered on
+ * `stream`, and keeps the fastest for this device and shape; *tile (may be NULL) gets its
+ * index.  exa_create tunes the shapes of its element products this way.  Every tile sums
+ * each entry over k in the same order, so the choice changes the time, not the result.
+ * Synchronizes `stream`; not for use inside stream capture. */
+int exa_dgemm_tune(int M, int N, int K, int batch, void* stream, int* tile);
 /* C_b = alpha A_b B_b + beta C_b with FP32 C, the products split as hi*hi + hi*lo + lo*hi over
  * TF32 parts (3xTF32, about FP32 accuracy) on the tcgen05 tensor cores with FP32
  * accumulation: the product the mixed-precision form uses.  A and B are FP64 or FP32,
