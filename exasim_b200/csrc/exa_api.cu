@@ -415,10 +415,6 @@ int exa_ctx_set_precision(ExaCtx& c, int mode) {
     exa_set_error("precision mode %d: 0 (FP64) or 1 (FP32/TF32 elimination with FP64 refinement)", mode);
     return EXA_ERR_ARG;
   }
-  if (mode == 1 && exa_inverse_needs_ws(c.P.n)) {
-    exa_set_error("the FP32 element elimination covers element blocks up to order 160 (this mesh: %d)", c.P.n);
-    return EXA_ERR_UNSUPPORTED;
-  }
   if (mode == 1 && c.H32 == nullptr) {
     const ExaDims& P = c.P;
     const size_t ne = P.ne, n = P.n, m = P.m, nb = c.neb;
@@ -953,8 +949,8 @@ extern "C" int exa_gemm_3xtf32_batched(int M, int N, int K, double alpha, const 
                                        long long sA, const void* B, int b_f64, long long ldb, long long sB,
                                        double beta, float* C, long long ldc, long long sC, int batch, int* flag_dev,
                                        void* stream) {
-  if (M <= 0 || N <= 0 || K <= 0 || batch <= 0 || N > 256) {
-    exa_set_error("3xtf32 gemm: sizes M %d N %d K %d batch %d (N <= 256)", M, N, K, batch);
+  if (M <= 0 || N <= 0 || K <= 0 || batch <= 0 || N > 1024) {
+    exa_set_error("3xtf32 gemm: sizes M %d N %d K %d batch %d (N <= 1024)", M, N, K, batch);
     return EXA_ERR_ARG;
   }
   cudaStream_t st = (cudaStream_t)stream;

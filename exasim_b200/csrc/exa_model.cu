@@ -184,7 +184,9 @@ int schur_chunk_mixed(ExaCtx& c, int e0, int nb) {
   }
   {
     ExaProfScope ps(c, EXA_PH_INVERSE);
-    EXA_TRY(exa_inverse(D32, n, (long long)n * n, nb, c.d_flag, c.st));
+    // blocks above order 160 go blockwise, with the chunk's inverse workspace (n^2 doubles per
+    // element, so room for n^2 floats)
+    EXA_TRY(exa_inverse_ws(D32, n, (long long)n * n, nb, reinterpret_cast<float*>(c.wInv), c.d_flag, c.st));
   }
   {
     ExaProfScope pp(c, EXA_PH_PACK);

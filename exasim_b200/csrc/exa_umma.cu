@@ -302,6 +302,7 @@ __global__ void __launch_bounds__(PNT, 1) umma3_kernel(UGemmP g, int* flag) {
   const int nkc = (g.K + PK - 1) / PK;
   const int rowsA = (g.M - m0) < UM ? (g.M - m0) : UM;
   const int ngA = (rowsA + 7) / 8, ngB = (g.N + 7) / 8;
+  const int ngBt = (g.B.R + 7) / 8;  // groups of all of B's rows: the stride between K chunks
   const uint32_t bytesA = (uint32_t)ngA * 512, bytesB = (uint32_t)ngB * 512;
 
   if (warp == 0) {
@@ -326,8 +327,8 @@ __global__ void __launch_bounds__(PNT, 1) umma3_kernel(UGemmP g, int* flag) {
 
   const float* Ahi = g.A.hi + b1 * g.A.sb + b2 * g.A.sb2 + (long long)tA * 16 * nkc * 128;
   const float* Alo = g.A.lo + b1 * g.A.sb + b2 * g.A.sb2 + (long long)tA * 16 * nkc * 128;
-  const float* Bhi = g.B.hi + b1 * g.B.sb + b2 * g.B.sb2;
-  const float* Blo = g.B.lo + b1 * g.B.sb + b2 * g.B.sb2;
+  const float* Bhi = g.B.hi + b1 * g.B.sb + b2 * g.B.sb2 + (long long)(g.n0 >> 3) * 128;
+  const float* Blo = g.B.lo + b1 * g.B.sb + b2 * g.B.sb2 + (long long)(g.n0 >> 3) * 128;
 
   if (warp == 0 && lane == 0) {
     // producer: chunk kc into stage kc % PST once the MMAs of chunk kc - PST are done
@@ -341,8 +342,8 @@ __global__ void __launch_bounds__(PNT, 1) umma3_kernel(UGemmP g, int* flag) {
       mbar_expect_tx(&full[s], 2 * (bytesA + bytesB));
       bulk_g2s(st, Ahi + (long long)kc * ngA * 128, bytesA, &full[s]);
       bulk_g2s(st + A_B, Alo + (long long)kc * ngA * 128, bytesA, &full[s]);
-      bulk_g2s(st + 2 * A_B, Bhi + (long long)kc * ngB * 128, bytesB, &full[s]);
-      bulk_g2s(st + 2 * A_B + B_B, Blo + (long long)kc * ngB * 128, bytesB, &full[s]);
+      bulk_g2s(st + 2 * A_B, Bhi + (long long)kc * ngBt * 128, bytesB, &full[s]);
+      bulk_g2s(st + 2 * A_B + B_B, Blo + (long long)kc * ngBt * 128, bytesB, &full[s]);
     }
   } else if (warp == 1 && lane == 0) {
     // MMA issuer: hi*hi + hi*lo + lo*hi per K step of 8
@@ -435,7 +436,7 @@ __global__ void __launch_bounds__(PNT, 1) umma3_kernel(UGemmP g, int* flag) {
           // are one float4 (the packed K is zero-padded, so whole quads are written)
 #pragma unroll
           for (int j = 0; j < 16; j += 4) {
-            const int gc = c0 + j + (int)b2 * po.cadd;
+            const int gc = c0 + j + g.n0 + (int)b2 * po.cadd;
             if (c0 + j >= g.N) break;
             const long long off = pbase[o] + (long long)(gc >> 4) * png[o] * 128 + ((gc >> 2) & 3) * 32;
             float4 h, l;
@@ -451,7 +452,7 @@ __global__ void __launch_bounds__(PNT, 1) umma3_kernel(UGemmP g, int* flag) {
           for (int j = 0; j < 16; ++j) {
             const int c = c0 + j;
             if (c >= g.N) break;
-            const int gc = c * po.cmul + (int)b2 * po.cadd;
+            const int gc = (c + g.n0) * po.cmul + (int)b2 * po.cadd;
             const long long off = po.as_b ? pbase[o] + (gc >> 3) * 128 + (gc & 7) * 4
                                            : pbase[o] + (long long)(gc >> 4) * png[o] * 128 + ((gc >> 2) & 3) * 32 + (gc & 3);
             float h, l;
@@ -516,11 +517,25 @@ int exa_pack(const void* src, int src_f64, long long rs, long long ks, long long
 }
 
 int exa_gemm_3xtf32(const UGemmP& g, int* flag, cudaStream_t st) {
+  if (g.N > 256) {
+    // column chunks of 256: B rows, C and Cin columns and packed-output indices shift by n0
+    for (int c0 = 0; c0 < g.N; c0 += 256) {
+      UGemmP h = g;
+      h.N = (g.N - c0) < 256 ? (g.N - c0) : 256;
+      h.n0 = g.n0 + c0;
+      if (h.C) h.C = (char*)h.C + (long long)(h.tco == EXA_T_F64 ? 8 : 4) * h.ldc * c0;
+      if (h.Cin) h.Cin = (const char*)h.Cin + (long long)(h.tci == EXA_T_F64 ? 8 : 4) * h.ldci * c0;
+      EXA_TRY(exa_gemm_3xtf32(h, flag, st));
+    }
+    return EXA_OK;
+  }
   if (g.M <= 0 || g.N <= 0 || g.batch <= 0 || g.batch2 <= 0) return EXA_OK;
   // the kernel locates chunks from M and N, so the packed operands must have exactly those
   // rows; batch strides keep every chunk on a 16-byte boundary for the bulk copies
-  if (g.K <= 0 || g.N > 256 || g.A.K != g.K || g.B.K != g.K || g.A.TR != UM || g.B.TR < g.N || g.A.R != g.M ||
-      g.B.R != g.N || !g.A.lo || !g.B.lo || g.nout < 0 || g.nout > 2 || (g.beta != 0.0 && !g.Cin) ||
+  // B's rows n0 .. n0 + N - 1 are read from one tile of all its rows; chunks start on a group
+  if (g.K <= 0 || g.N > 256 || g.A.K != g.K || g.B.K != g.K || g.A.TR != UM || g.B.TR < g.B.R || g.A.R != g.M ||
+      g.n0 < 0 || (g.n0 & 7) != 0 || g.B.R < g.n0 + g.N ||
+      !g.A.lo || !g.B.lo || g.nout < 0 || g.nout > 2 || (g.beta != 0.0 && !g.Cin) ||
       (g.A.sb | g.A.sb2 | g.B.sb | g.B.sb2) % 4 != 0) {
     exa_set_error("3xtf32 gemm: inconsistent operand description (M %d N %d K %d)", g.M, g.N, g.K);
     return EXA_ERR_ARG;

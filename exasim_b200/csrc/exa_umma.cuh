@@ -64,5 +64,7 @@ struct UGemmP {
   void* C; int tco; long long ldc, sC, sC2;
   UPackOut out[2]; int nout;
   int batch, batch2;
+  int n0;  // first column: the product covers columns n0 .. n0 + N - 1 of B, C and Cin (set by the host for N > 256)
 };
+// N above 256 runs as column chunks of at most 256 (one launch each).
 int exa_gemm_3xtf32(const UGemmP& g, int* flag, cudaStream_t st);

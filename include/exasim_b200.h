@@ -148,7 +148,8 @@ int exa_dgemm_tune(int M, int N, int K, int batch, void* stream, int* tile);
 /* C_b = alpha A_b B_b + beta C_b with FP32 C, the products split as hi*hi + hi*lo + lo*hi over
  * TF32 parts (3xTF32, about FP32 accuracy) on the tcgen05 tensor cores with FP32
  * accumulation: the product the mixed-precision form uses.  A and B are FP64 or FP32,
- * column-major.  N <= 256.  The call packs A and B into temporary device buffers (allocated
+ * column-major.  N <= 1024 (above 256 in column chunks of 256, one launch each).  The call
+ * packs A and B into temporary device buffers (allocated
  * and freed inside) and synchronises the stream.  *flag_dev as for exa_gemm_tf32_batched. */
 int exa_gemm_3xtf32_batched(int M, int N, int K, double alpha, const void* A, int a_f64, long long lda, long long sA,
                             const void* B, int b_f64, long long ldb, long long sB, double beta, float* C, long long ldc,

@@ -119,6 +119,22 @@ def test_euler3d_vortex_blocks(tmp_path, porder, inv_tol):
 
 
 @pytest.mark.parametrize("porder", [2, 3])
+def test_euler3d_mixed_dirk_matches_fp64(tmp_path, porder):
+    """The mixed form on 135 x 135 and 320 x 320 blocks (blocked FP32 inverse, products of
+    more than 256 columns in chunks)."""
+    d = cases.euler3d_vortex_hex(str(tmp_path / "eu"), n=3, porder=porder, nsteps=1)
+    s64 = HDGSolver(d, "euler3d")
+    s64.DIRK(1)
+    s32 = HDGSolver(d, "euler3d")
+    s32.set_precision(1, inner_tol=1e-4, rtol=1e-10)
+    s32.DIRK(1)
+    u, ref = s32.get("udg"), s64.get("udg")
+    assert np.linalg.norm(u - ref) / np.linalg.norm(ref) < 1e-6
+    s64.close()
+    s32.close()
+
+
+@pytest.mark.parametrize("porder", [2, 3])
 def test_euler3d_vortex_dirk(tmp_path, porder):
     d = cases.euler3d_vortex_hex(str(tmp_path / "eu"), n=3, porder=porder, nsteps=1)
     s = HDGSolver(d, "euler3d")

@@ -57,7 +57,8 @@ def test_tf32_gemm_matches_rounded_reference(M, N, K, a64):
 
 
 @pytest.mark.parametrize("M,N,K,a64", [(125, 125, 375, True), (150, 150, 125, False), (125, 150, 375, True),
-                                       (150, 125, 375, True), (10, 12, 20, True), (64, 256, 40, False)])
+                                       (150, 125, 375, True), (10, 12, 20, True), (64, 256, 40, False),
+                                       (150, 480, 320, True), (96, 300, 40, False)])
 def test_3xtf32_gemm_matches_fp64(M, N, K, a64):
     """hi*hi + hi*lo + lo*hi drops the lo*lo term (2^-22 relative) and the tensor cores add the
     products in FP32 without round-to-nearest on every step: within 1e-5 of max |C| at K <= 375
