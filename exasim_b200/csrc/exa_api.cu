@@ -313,6 +313,7 @@ int exa_ctx_init(ExaCtx& c, const double* app, long long napp, const double* mas
     EXA_TRY(dev_alloc(c, &c.d_flag, 4));
     EXA_TRY(exa_k_qmats(P, c.shapegt, c.shapegw, c.shapfgt, c.shapfgw, c.perm, c.elemg, c.faceg, mass, cw, ew, c.st));
     EXA_TRY(exa_inverse(mass, P.npe, (long long)P.npe * P.npe, P.ne, c.d_flag, c.st));
+    c.Minv = mass;  // kept: q recovery applies it to C u - E uhat
     GemmBatch g{};
     g.M = P.npe; g.N = P.npe; g.K = P.npe; g.alpha = 1.0; g.beta = 0.0;
     g.A = mass; g.lda = P.npe; g.sA = (long long)P.npe * P.npe; g.sA2 = 0;

@@ -366,6 +366,81 @@ __global__ void getq_kernel(ExaDims P, const int* elemcon, const double* MC, con
   }
 }
 
+// The same q without MinvC and MinvE: q_d = Minv (C_d u - E_d uhat), with C_d u and E_d uhat
+// by quadrature (the sums that define C and E in qmats_kernel, taken over the Gauss points of
+// u and uhat instead of stored as matrices), so each element reads its 125 KB Minv (p = 4 hex)
+// instead of 825 KB of MinvC and MinvE.  One block per element.
+__global__ void getq_mf_kernel(ExaDims P, const double* shapegt, const double* shapegw, const double* shapfgt,
+                               const double* shapfgw, const int* perm, const int* elemcon, const double* elemg,
+                               const double* faceg, const double* Minv, const double* uh, double* udg) {
+  extern __shared__ double sm[];
+  const int e = blockIdx.x, npe = P.npe, ncu = P.ncu, ndf = P.ndf, nd = P.nd, nc = P.nc;
+  const int nge = P.nge, npf = P.npf, ngf = P.ngf, nfe = P.nfe;
+  double* u = sm;                  // [npe, ncu]
+  double* uhe = u + npe * ncu;     // [ndf, ncu]
+  double* vg = uhe + ndf * ncu;    // [nge, nd (ref r), nd (phys d), ncu]: Xx[g, d, r] u(g)
+  double* w = vg + nge * nd * nd * ncu;  // [npe, ncu, nd]
+  double* hg = w + npe * ncu * nd;       // [ngf, nd, ncu]: n_d fj uhat(g) on one face
+  double* U = udg + (long long)e * npe * nc;
+  const double* eg = elemg + (long long)e * P.elemg_stride();
+  const double* Xx = eg + nge * P.ncx;
+  for (int t = threadIdx.x; t < npe * ncu; t += blockDim.x) u[t] = U[t];
+  for (int t = threadIdx.x; t < ndf * ncu; t += blockDim.x) {
+    const int jf = t % ndf, k = t / ndf;
+    uhe[t] = uh[k + ncu * (long long)elemcon[jf + ndf * e]];
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < nge * ncu; t += blockDim.x) {
+    const int g = t % nge, k = t / nge;
+    double s = 0.0;
+    for (int b = 0; b < npe; ++b) s = fma(shapegt[g + nge * b], u[b + npe * k], s);
+    for (int d = 0; d < nd; ++d)
+      for (int r = 0; r < nd; ++r) vg[g + nge * (r + nd * (d + nd * k))] = Xx[g + nge * (d + nd * r)] * s;
+  }
+  __syncthreads();
+  // C_d u: sum over g and r of shapegw[a, g, 1 + r] vg[g, r, d]
+  for (int t = threadIdx.x; t < npe * ncu * nd; t += blockDim.x) {
+    const int a = t % npe, k = (t / npe) % ncu, d = t / (npe * ncu);
+    double s = 0.0;
+    for (int r = 0; r < nd; ++r) {
+      const double* W = shapegw + a + (long long)npe * nge * (1 + r);
+      const double* v = vg + nge * (r + nd * (d + nd * k));
+      for (int g = 0; g < nge; ++g) s = fma(W[npe * g], v[g], s);
+    }
+    w[t] = s;
+  }
+  __syncthreads();
+  // minus E_d uhat, face by face (faces share corner and edge nodes)
+  for (int l = 0; l < nfe; ++l) {
+    const double* fg = faceg + ((long long)e * nfe + l) * P.faceg_stride();
+    const double* nl = fg + ngf * P.ncx;
+    const double* fj = nl + ngf * nd;
+    for (int t = threadIdx.x; t < ngf * ncu; t += blockDim.x) {
+      const int g = t % ngf, k = t / ngf;
+      double s = 0.0;
+      for (int b = 0; b < npf; ++b) s = fma(shapfgt[g + ngf * b], uhe[b + npf * l + ndf * k], s);
+      for (int d = 0; d < nd; ++d) hg[g + ngf * (d + nd * k)] = nl[g + ngf * d] * fj[g] * s;
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < npf * ncu * nd; t += blockDim.x) {
+      const int a = t % npf, k = (t / npf) % ncu, d = t / (npf * ncu);
+      double s = 0.0;
+      for (int g = 0; g < ngf; ++g) s = fma(shapfgw[a + npf * g], hg[g + ngf * (d + nd * k)], s);
+      w[perm[a + npf * l] + npe * (k + ncu * d)] -= s;
+    }
+    __syncthreads();
+  }
+  // q = Minv w
+  const double* Mi = Minv + (long long)e * npe * npe;
+  for (int t = threadIdx.x; t < npe * ncu * nd; t += blockDim.x) {
+    const int i = t % npe, k = (t / npe) % ncu, d = t / (npe * ncu);
+    const double* wk = w + npe * (k + ncu * d);
+    double s = 0.0;
+    for (int j = 0; j < npe; ++j) s = fma(Mi[i + (long long)npe * j], wk[j], s);
+    U[i + npe * (ncu + k + ncu * d)] = s;
+  }
+}
+
 // uh from the first element of each face (kokkosimpl.h:901-915)
 __global__ void face_nodes_kernel(ExaDims P, const int* f2e, const int* perm, const double* udg, double* uh) {
   const long long N = (long long)P.ncu * P.npf * P.nf;
@@ -472,6 +547,22 @@ int exa_k_getq(const ExaDims& P, const int* elemcon, const double* MC, const dou
                double* udg, cudaStream_t st) {
   size_t smem = sizeof(double) * ((size_t)P.npe * P.ncu + (size_t)P.ndf * P.ncu);
   getq_kernel<<<P.ne, 128, smem, st>>>(P, elemcon, MC, ME, uh, udg);
+  EXA_LAUNCH_CHECK();
+  return EXA_OK;
+}
+
+size_t exa_getq_mf_smem(const ExaDims& P) {
+  return sizeof(double) * ((size_t)P.npe * P.ncu + (size_t)P.ndf * P.ncu + (size_t)P.nge * P.nd * P.nd * P.ncu +
+                           (size_t)P.npe * P.ncu * P.nd + (size_t)P.ngf * P.nd * P.ncu);
+}
+
+int exa_k_getq_mf(const ExaDims& P, const double* shapegt, const double* shapegw, const double* shapfgt,
+                  const double* shapfgw, const int* perm, const int* elemcon, const double* elemg,
+                  const double* faceg, const double* Minv, const double* uh, double* udg, cudaStream_t st) {
+  const size_t smem = exa_getq_mf_smem(P);
+  EXA_TRY(exa_allow_smem((const void*)getq_mf_kernel, smem));
+  getq_mf_kernel<<<P.ne, 128, smem, st>>>(P, shapegt, shapegw, shapfgt, shapfgw, perm, elemcon, elemg, faceg, Minv,
+                                          uh, udg);
   EXA_LAUNCH_CHECK();
   return EXA_OK;
 }

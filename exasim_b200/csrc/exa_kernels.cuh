@@ -61,6 +61,11 @@ int exa_k_bilu_apply(const ExaDims& P, const ExaBiluDev& b, const T* BE, const d
 // y = (float) x
 int exa_k_to_f32(const double* x, float* y, long long n, cudaStream_t st);
 int exa_k_udg_update(const ExaDims& P, double* udg, const double* du, double alpha, cudaStream_t st);
+// q = Minv (C u - E uhat) by quadrature (no MinvC / MinvE reads)
+size_t exa_getq_mf_smem(const ExaDims& P);
+int exa_k_getq_mf(const ExaDims& P, const double* shapegt, const double* shapegw, const double* shapfgt,
+                  const double* shapfgw, const int* perm, const int* elemcon, const double* elemg,
+                  const double* faceg, const double* Minv, const double* uh, double* udg, cudaStream_t st);
 int exa_k_getq(const ExaDims& P, const int* elemcon, const double* MC, const double* ME, const double* uh,
                double* udg, cudaStream_t st);
 int exa_k_face_nodes(const ExaDims& P, const int* f2e, const int* perm, const double* udg, double* uh, cudaStream_t st);

@@ -47,6 +47,7 @@ struct ExaCtx {
   double *xdg = nullptr, *elemg = nullptr, *faceg = nullptr, *uinf = nullptr, *param = nullptr, *tau = nullptr;
   double *udg = nullptr, *uh = nullptr, *sdg = nullptr;
   double *MC = nullptr, *ME = nullptr;
+  double* Minv = nullptr;  // inverse element mass matrices [npe, npe, ne] (q recovery by quadrature)
   double *H = nullptr, *F = nullptr, *Ru = nullptr, *Rh = nullptr, *b = nullptr, *Pc = nullptr;
   // assembly workspace for a chunk of `neb` elements
   int neb = 0;
