@@ -69,6 +69,7 @@ __global__ void vol_points_kernel(AsmArgs A, double* Ru, double* rgJ) {
   for (int t = threadIdx.x; t < nge * nc; t += blockDim.x) {
     const int g = t % nge, c = t / nge;
     double s = 0.0;
+#pragma unroll 8
     for (int j = 0; j < npe; ++j) s = fma(A.shapegt[g + nge * j], un[j + npe * c], s);
     ug[t] = s;
   }
@@ -77,6 +78,7 @@ __global__ void vol_points_kernel(AsmArgs A, double* Ru, double* rgJ) {
     for (int t = threadIdx.x; t < nge * ncu; t += blockDim.x) {
       const int g = t % nge, k = t / nge;
       double s = 0.0;
+#pragma unroll 8
       for (int j = 0; j < npe; ++j) s = fma(A.shapegt[g + nge * j], S[j + npe * k], s);
       sdgg[t] = s;
     }
@@ -146,6 +148,9 @@ __global__ void vol_points_kernel(AsmArgs A, double* Ru, double* rgJ) {
   for (int t = threadIdx.x; t < npe * ncu; t += blockDim.x) {
     const int i = t % npe, k = t / npe;
     double s = 0.0;
+    // unrolled so the weight loads (from L2) are in flight together; one accumulator, so the
+    // sum keeps its order
+#pragma unroll 8
     for (int q = 0; q < K; ++q) s = fma(A.shapegw[i + npe * q], rgR[q + K * k], s);
     Ru[(long long)le * P.n + t] = s;
   }
