@@ -18,6 +18,7 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(PKG, "csrc")
 BUILD = os.path.join(PKG, "_build")
 LIB = os.path.join(PKG, "lib")
+BIN = os.path.join(PKG, "bin")
 MODELS = os.path.join(PKG, "models")
 NVCC = os.environ.get("NVCC", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -32,6 +33,11 @@ def available_models() -> List[str]:
 
 def lib_path(model: str) -> str:
     return os.path.join(LIB, f"libexasim_b200_{model}.so")
+
+
+def exe_path(model: str) -> str:
+    """The model's executable (csrc/exa_main.cpp): datain/ in, the reference's output files out."""
+    return os.path.join(BIN, f"exasim_b200_{model}")
 
 
 def _run(cmd):
@@ -93,6 +99,11 @@ def build(models: Optional[List[str]] = None, jobs: int = 8) -> List[str]:
             if _newer(so, common_objs + [obj]):
                 _run([NVCC] + ARCH + ["-shared", "-o", so] + common_objs + [obj])
             outs.append(so)
+            exe, main = exe_path(mname), os.path.join(CSRC, "exa_main.cpp")
+            if _newer(exe, [so, main] + _headers()):
+                os.makedirs(BIN, exist_ok=True)
+                _run(["g++", "-O2", "-std=c++17", main, "-o", exe, "-L", LIB, f"-l:libexasim_b200_{mname}.so",
+                      "-Wl,-rpath,$ORIGIN/../lib"])
     return outs
 
 

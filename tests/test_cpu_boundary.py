@@ -103,3 +103,16 @@ def test_master_generator_matches_reference_tet_master():
     # face shapes differ by ~5e-8: the preprocessor's simplex basis clamps y to 0.99999999 at the
     # face vertex (text2code/text2code/makemaster.cpp:451-455); the tables here do not
     assert np.abs(m.shapfgt.ravel(order="F") - ref["shapfgt"]).max() < 1e-6
+
+
+def test_executable_reports_usage_and_missing_input(tmp_path):
+    """The executable starts without a GPU far enough to check its arguments and inputs."""
+    import subprocess
+    from exasim_b200 import build as B
+    exe = B.exe_path("poisson2d")
+    assert os.path.exists(exe)
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 1 and "usage" in r.stderr
+    r = subprocess.run([exe, str(tmp_path / "nowhere"), str(tmp_path / "out")], capture_output=True, text=True,
+                       timeout=60)
+    assert r.returncode == 1 and "cannot open" in r.stderr
