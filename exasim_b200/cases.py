@@ -64,12 +64,12 @@ def poisson2d_quad(datain: str, n: int = 16, porder: int = 3, preconditioner: in
 
 def convdiff3d_hex(datain: str, n: int = 16, porder: int = 4, nsteps: int = 20, dt: float = 0.01,
                    preconditioner: int = 0, gmres_tol: float = 1e-8, restart: int = 50, ortho: int = 0,
-                   nstage: int = 3, torder: int = 3, cartgridpart=()):
+                   nstage: int = 3, torder: int = 3, cartgridpart=(), rbdim: int = 0):
     grid = I.cube_hex_grid(n)
     master = I.make_master(3, 1, porder, 2 * porder)
     app = I.PDEApp(nd=3, ncu=1, model="ModelD", preconditioner=preconditioner, NewtonIter=20,
                    NewtonTol=1e-6, GMRESiter=1000, GMRESrestart=restart, GMREStol=gmres_tol, GMRESortho=ortho,
-                   RBdim=0, ppdegree=1, tau=[1.0], torder=torder, nstage=nstage, dt=[dt] * nsteps,
+                   RBdim=rbdim, ppdegree=1, tau=[1.0], torder=torder, nstage=nstage, dt=[dt] * nsteps,
                    physicsparam=[0.01, 1.0, 0.5, 0.25, 0.5, 0.5, 0.5, 0.1], externalparam=[0.0, 0.0])
     exprs = [_on(2, 0.0), _on(2, 1.0), _on(1, 0.0), _on(0, 1.0), _on(1, 1.0), _on(0, 0.0)]
     return write_case(datain, grid, master, app, exprs, [1, 1, 1, 1, 1, 1], cartgridpart)

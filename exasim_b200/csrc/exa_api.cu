@@ -166,7 +166,7 @@ int exa_ctx_init(ExaCtx& c, const double* app, long long napp, const double* mas
   if (P.nco > 0 || P.ncw > 0) { exa_set_error("odg/wdg fields (nco=%d, ncw=%d) are outside the HDG hot path", P.nco, P.ncw); return EXA_ERR_UNSUPPORTED; }
   if (c.wave) { exa_set_error("wave (ModelW) problems are not supported"); return EXA_ERR_UNSUPPORTED; }
   if (coupled > 0) { exa_set_error("coupled interfaces are not supported"); return EXA_ERR_UNSUPPORTED; }
-  if (c.RBdim > 0) { exa_set_error("reduced-basis initial guess (RBdim=%d) is not supported; set RBdim = 0", c.RBdim); return EXA_ERR_UNSUPPORTED; }
+  if (c.RBdim < 0 || c.RBdim > 64) { exa_set_error("reduced-basis dimension %d outside 0..64", c.RBdim); return EXA_ERR_UNSUPPORTED; }
   if (c.ppdegree > 1) { exa_set_error("polynomial preconditioner (ppdegree=%d) is not supported", c.ppdegree); return EXA_ERR_UNSUPPORTED; }
   if (c.preconditioner < 0 || c.preconditioner > 2) { exa_set_error("preconditioner %d: block Jacobi (0), elemental additive Schwarz (1) or block ILU(0) on Cartesian sub-domains (2)", c.preconditioner); return EXA_ERR_UNSUPPORTED; }
   if (c.restart < 1 || c.gmres_maxit < 1) { exa_set_error("GMRES restart/iterations must be positive"); return EXA_ERR_ARG; }
@@ -393,6 +393,11 @@ int exa_ctx_init(ExaCtx& c, const double* app, long long napp, const double* mas
   EXA_TRY(dev_alloc(c, &c.gcs, n1));
   EXA_TRY(dev_alloc(c, &c.gsn, n1));
   EXA_TRY(dev_alloc(c, &c.scal, 16));
+  if (c.RBdim > 0) {
+    EXA_TRY(dev_alloc(c, &c.rbW, N * (size_t)c.RBdim));
+    EXA_TRY(dev_alloc(c, &c.rbU, N * (size_t)c.RBdim));
+    EXA_TRY(dev_alloc(c, &c.rbD, (size_t)c.RBdim * (c.RBdim + 1)));
+  }
   if (c.tdep) {
     EXA_TRY(dev_alloc(c, &c.udgprev, ne * n));
     EXA_TRY(dev_alloc(c, &c.utmp, ne * n));
@@ -492,6 +497,7 @@ int exa_ctx_reset(ExaCtx& c, const double* app, long long napp, const double* so
   c.dtfactor = 0.0;
   c.last_gmres_iters = c.last_newton_iters = c.total_gmres_iters = 0;
   c.last_norm0 = c.last_norm = 0.0;
+  c.rb_cur = c.rb_removed = 0;
   EXA_CUDA(cudaMemsetAsync(c.sdg, 0, sizeof(double) * (size_t)c.P.npe * c.P.ncu * c.P.ne, c.st));
   EXA_TRY(init_solution(c, S));
   EXA_CUDA(cudaStreamSynchronize(c.st));

@@ -275,6 +275,80 @@ int arnoldi_step(ExaCtx& c, int i, const double* d_nrmb, double* d_relerr, doubl
   return arnoldi_ops(c, i, d_nrmb, d_relerr, rel_pin);
 }
 
+// ComputeInitialGuessAndPreconditioner (preconditioner.cpp:133-181): the image of the newest
+// basis vector under the current condensed operator, U_i = A W_i, then c = (U^T U)^-1 U^T b
+// (the small matrix inverted on the host by Gauss-Jordan with partial pivoting, as the
+// reference inverts it with getrf/getri) and x = W c.  A singular U^T U leaves x = 0.
+int rb_initial_guess(ExaCtx& c) {
+  const long long N = c.ndofuhat();
+  const int cur = c.rb_cur;
+  const int i = c.rb_removed > 0 ? c.rb_removed - 1 : cur - 1;
+  EXA_TRY(exa_drv_matvec(c, c.rbW + (long long)i * N, c.rbU + (long long)i * N));
+  int nd = 0;
+  for (int j = 0; j < cur; ++j) {
+    EXA_TRY(exa_dot_partials(c.rbU + (long long)j * N, c.b, N, c.part_a, c.st));
+    EXA_TRY(exa_reduce_partials(c.part_a, c.rbD + nd++, 0, c.st));
+  }
+  for (int j = 0; j < cur; ++j)
+    for (int k = 0; k <= j; ++k) {
+      EXA_TRY(exa_dot_partials(c.rbU + (long long)j * N, c.rbU + (long long)k * N, N, c.part_a, c.st));
+      EXA_TRY(exa_reduce_partials(c.part_a, c.rbD + nd++, 0, c.st));
+    }
+  std::vector<double> d(nd);
+  EXA_CUDA(cudaMemcpyAsync(d.data(), c.rbD, sizeof(double) * nd, cudaMemcpyDeviceToHost, c.st));
+  EXA_CUDA(cudaStreamSynchronize(c.st));
+  // H = U^T U (symmetric), inverted in place
+  std::vector<double> H((size_t)cur * cur), rhs(d.begin(), d.begin() + cur);
+  for (int j = 0, o = cur; j < cur; ++j)
+    for (int k = 0; k <= j; ++k, ++o) H[j + cur * k] = H[k + cur * j] = d[o];
+  std::vector<int> used(cur, 0), perm(cur);
+  for (int k = 0; k < cur; ++k) {
+    int p = -1;
+    double best = 0.0;
+    for (int r = 0; r < cur; ++r)
+      if (!used[r] && std::fabs(H[r + cur * k]) > best) { best = std::fabs(H[r + cur * k]); p = r; }
+    if (p < 0) return EXA_OK;  // singular: zero initial guess
+    used[p] = 1;
+    perm[k] = p;
+    const double dinv = 1.0 / H[p + cur * k];
+    for (int j = 0; j < cur; ++j) H[p + cur * j] = (j == k) ? dinv : H[p + cur * j] * dinv;
+    for (int r = 0; r < cur; ++r) {
+      if (r == p) continue;
+      const double f = H[r + cur * k];
+      for (int j = 0; j < cur; ++j) H[r + cur * j] = (j == k) ? -f * dinv : H[r + cur * j] - f * H[p + cur * j];
+    }
+  }
+  // entry (r, c) of the tableau is inverse(pos[r], perm[c]); coef = inverse * rhs
+  std::vector<int> pos(cur);
+  for (int k = 0; k < cur; ++k) pos[perm[k]] = k;
+  std::vector<double> inv((size_t)cur * cur), coef(cur, 0.0);
+  for (int r = 0; r < cur; ++r)
+    for (int k = 0; k < cur; ++k) inv[pos[r] + cur * perm[k]] = H[r + cur * k];
+  for (int r = 0; r < cur; ++r)
+    for (int k = 0; k < cur; ++k) coef[r] += inv[r + cur * k] * rhs[k];
+  double* cd = c.rbD;  // the dot products are consumed: reuse for the coefficients
+  EXA_CUDA(cudaMemcpyAsync(cd, coef.data(), sizeof(double) * cur, cudaMemcpyHostToDevice, c.st));
+  EXA_TRY(exa_gemv_add(c.x, c.rbW, cd, N, cur, c.st));
+  EXA_CUDA(cudaStreamSynchronize(c.st));  // coef is host memory that goes out of scope
+  return EXA_OK;
+}
+
+// UpdateRB (ptcsolver.cpp:484-500): the Newton update, scaled by its step length, replaces
+// the oldest basis vector
+int rb_update(ExaCtx& c, double alpha) {
+  const long long N = c.ndofuhat();
+  EXA_TRY(exa_scale(c.x, c.x, alpha, N, c.st));
+  double nrm = 0.0;
+  EXA_TRY(exa_drv_norm(c, c.x, N, &nrm));
+  if (nrm > 0.0) {
+    EXA_CUDA(cudaMemcpyAsync(c.rbW + (long long)c.rb_removed * N, c.x, sizeof(double) * N, cudaMemcpyDeviceToDevice,
+                             c.st));
+    if (c.rb_cur < c.RBdim) c.rb_cur += 1;
+    c.rb_removed = (c.rb_removed + 1) % c.RBdim;
+  }
+  return EXA_OK;
+}
+
 // UpdateSolution (gmres.cpp:132-137) with the first i + 1 basis vectors: y from the
 // Hessenberg back-solve on the host, x += V y on the device.
 int update_solution(ExaCtx& c, int i, std::vector<double>& ybuf) {
@@ -312,9 +386,20 @@ int exa_drv_gmres(ExaCtx& c, int* iters_out, double* relerr_out) {
     *relerr_out = 0.0;
     return EXA_OK;
   }
-  nrmr = nrmb;  // x = 0: r = b
+  // initial guess from the reduced basis (LinearSolver, ptcsolver.cpp:374-379); a guess of
+  // norm at most 1e-12 counts as none, as in gmres.cpp:404-421
+  if (c.RBdim > 0 && c.rb_cur > 0) EXA_TRY(rb_initial_guess(c));
+  double scalar = 0.0;
+  if (c.RBdim > 0 && c.rb_cur > 0) EXA_TRY(exa_drv_norm(c, c.x, N, &scalar));
+  if (scalar > 1e-12) {
+    EXA_TRY(exa_drv_matvec(c, c.x, c.w));
+    EXA_TRY(exa_axpby(c.w, c.b, 1.0, -1.0, N, c.st));  // w = b - A x
+    EXA_TRY(exa_drv_norm(c, c.w, N, &nrmr));
+  } else {
+    nrmr = nrmb;  // r = b
+  }
   const double tol = std::min(0.1, c.gmres_tol * (nrmb / nrmr));
-  EXA_TRY(exa_drv_precond(c, c.b, c.r));
+  EXA_TRY(exa_drv_precond(c, scalar > 1e-12 ? c.w : c.b, c.r));
   EXA_TRY(exa_drv_norm(c, c.r, N, &nrmb));
   nrmr = nrmb;
   // device copy of nrmb for the Givens kernel
@@ -418,6 +503,7 @@ int exa_drv_newton(ExaCtx& c, int* iters_out, double* norm_out) {
       EXA_TRY(exa_drv_residual(c, &nrmr));
       if (alpha < 1e-12) break;
     }
+    if (c.RBdim > 0) EXA_TRY(rb_update(c, alpha));
     c.last_newton_iters = it + 1;
     if (std::isnan(nrmr)) {
       exa_set_error("Newton residual is NaN");
@@ -494,6 +580,7 @@ int exa_drv_newton_mixed(ExaCtx& c, int* iters_out, double* norm_out) {
     EXA_TRY(exa_axpby(c.uh, c.x, 1.0, 1.0, N, c.st));
     EXA_TRY(exa_k_dudg(P, c.elemcon, c.F32, c.Ru, c.x, c.du, c.st));
     EXA_TRY(exa_k_udg_update(P, c.udg, c.du, 1.0, c.st));
+    if (c.RBdim > 0) EXA_TRY(rb_update(c, 1.0));
     EXA_TRY(exa_drv_getq(c));
     EXA_TRY(exa_drv_residual(c, &nrmr));
     c.last_newton_iters = it + 1;

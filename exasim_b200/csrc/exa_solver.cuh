@@ -59,6 +59,10 @@ struct ExaCtx {
          *gsn = nullptr, *scal = nullptr, *udgprev = nullptr, *utmp = nullptr;
   int* d_flag = nullptr;
   double* pinned = nullptr;  // small host staging buffer
+  // reduced-basis initial guess of GMRES (RBdim > 0): the last RBdim Newton updates W, their
+  // images U under the condensed operator, a ring position, and the dot products of a guess
+  double *rbW = nullptr, *rbU = nullptr, *rbD = nullptr;
+  int rb_cur = 0, rb_removed = 0;
   // GMRES: each Arnoldi step index i of the restart cycle (and each precision) runs as one
   // captured CUDA graph from its second use on; none while phase profiling records events
   std::vector<cudaGraphExec_t> arnoldi_graph[2];

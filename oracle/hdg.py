@@ -151,6 +151,11 @@ class HDGOracle:
         self.newton_maxit = self.problem[13]
         self.gmres_maxit = self.problem[14]
         self.restart = self.problem[15]
+        # reduced-basis initial guess of GMRES (ptcsolver.cpp:217-236, 374-379;
+        # preconditioner.cpp:133-181): the last RBdim Newton updates
+        self.RBdim = int(self.problem[16]) if self.problem.size > 16 else 0
+        self.rb_W = self.rb_U = None
+        self.rb_cur = self.rb_removed = 0
         self.torder, self.nstage = self.problem[3], self.problem[4]
         self.newton_tol = self.solversparam[0]
         self.gmres_tol = self.solversparam[1]
@@ -712,7 +717,7 @@ class HDGOracle:
             self.assemble()
             b = self.assemble_rhs(self.Rh)
             self.build_precond()
-            x, info = self.gmres(b)
+            x, info = self.gmres(b, self._rb_guess(b))
             self.gmres_log.append(info)
             alpha = 1.0
             u = self.uh + alpha * x
@@ -734,11 +739,42 @@ class HDGOracle:
                     self.get_q(self.udg, self.uh)
                 nrmr, _ = self.residual_norm()
             norms.append(nrmr)
+            if self.RBdim > 0:
+                self._rb_update(alpha * x)
             if self.verbose:
                 print(f"Newton {it + 1}: alpha {alpha} norm {nrmr:.6e} gmres {info}")
             if nrmr < tol:
                 return it + 1, norms
         return maxit, norms
+
+    def _rb_guess(self, b):
+        """ComputeInitialGuessAndPreconditioner (preconditioner.cpp:133-181): U_i = A W_i for the
+        newest basis vector under the current Jacobian, c = (U^T U)^-1 U^T b, x0 = W c; None
+        (zero guess) without a basis or with a singular U^T U."""
+        if self.RBdim <= 0 or self.rb_cur == 0:
+            return None
+        shape = b.shape
+        cur = self.rb_cur
+        i = self.rb_removed - 1 if self.rb_removed > 0 else cur - 1
+        self.rb_U[:, i] = self.matvec(self.rb_W[:, i].reshape(shape, order="F")).ravel(order="F")
+        U, W = self.rb_U[:, :cur], self.rb_W[:, :cur]
+        H = U.T @ U
+        try:
+            c = np.linalg.inv(H) @ (U.T @ b.ravel(order="F"))
+        except np.linalg.LinAlgError:
+            return None
+        return (W @ c).reshape(shape, order="F")
+
+    def _rb_update(self, x):
+        """UpdateRB (ptcsolver.cpp:484-500): the scaled Newton update replaces the oldest vector."""
+        xv = x.ravel(order="F")
+        if self.rb_W is None:
+            self.rb_W = np.zeros((xv.size, self.RBdim))
+            self.rb_U = np.zeros((xv.size, self.RBdim))
+        if np.sqrt(np.dot(xv, xv)) > 0.0:
+            self.rb_W[:, self.rb_removed] = xv
+            self.rb_cur = min(self.rb_cur + 1, self.RBdim)
+            self.rb_removed = (self.rb_removed + 1) % self.RBdim
 
     # --------------------------------------------------------------------- DIRK
     def dirk_solve(self, nsteps=None, on_stage=None):
