@@ -102,3 +102,54 @@ def test_product_ordering_matches_oracle(tmp_path, nd, n, cgp):
     assert nfse == len(row_ptr) - 1, L.exa_last_error()
     assert np.array_equal(rp[:nfse + 1], row_ptr) and np.array_equal(ci[:row_ptr[-1]], col_ind)
     assert np.array_equal(fc[:nse.value * nfse].reshape(nse.value, nfse, order="F"), face)
+
+
+def ilu_pattern_error(fac, orig, row_ptr, col_ind):
+    """Block ILU(0) property, the dense check of the reference's test_block_ilu0.m in
+    substance: with L unit lower (stored L blocks) and U upper (inverted stored diagonal,
+    stored U blocks), (L U)_jk equals the assembled A_jk on every stored block (j, k)."""
+    nfse = len(row_ptr) - 1
+    ncf = fac.shape[-1]
+    n = nfse * ncf
+    L, U, A = np.eye(n), np.zeros((n, n)), np.zeros((n, n))
+    blk = lambda i: slice(i * ncf, (i + 1) * ncf)
+    for i in range(nfse):
+        for t in range(row_ptr[i], row_ptr[i + 1]):
+            j = int(col_ind[t])
+            A[blk(i), blk(j)] = orig[t]
+            if j == i:
+                U[blk(i), blk(i)] = np.linalg.inv(fac[t])
+            elif j > i:
+                U[blk(i), blk(j)] = fac[t]
+            else:
+                L[blk(i), blk(j)] = fac[t]
+    LU = L @ U
+    err = 0.0
+    for i in range(nfse):
+        for t in range(row_ptr[i], row_ptr[i + 1]):
+            j = int(col_ind[t])
+            err = max(err, np.abs(LU[blk(i), blk(j)] - A[blk(i), blk(j)]).max())
+    return err / np.abs(A).max()
+
+
+@pytest.mark.parametrize("nd", [2, 3])
+def test_oracle_block_ilu0_reproduces_the_matrix_on_its_pattern(tmp_path, nd):
+    from exasim_b200 import cases
+    from oracle.bilu0 import BlockILU0
+    from oracle.hdg import HDGOracle
+    from oracle.models import MODELS
+    if nd == 2:
+        d = cases.poisson2d_quad(str(tmp_path / "q"), n=4, porder=1, preconditioner=2, cartgridpart=(2, 4, 4, 2, 2, 0))
+        o = HDGOracle(d, MODELS["poisson2d"]())
+    else:
+        d = cases.convdiff3d_hex(str(tmp_path / "h"), n=2, porder=1, nsteps=1, preconditioner=2,
+                                 cartgridpart=(3, 2, 2, 2, 2, 2, 2, 0))
+        o = HDGOracle(d, MODELS["convdiff3d"]())
+    rng = np.random.default_rng(nd)
+    m = o.ncu * o.npf * o.nfe
+    H = rng.standard_normal((m, m, o.ne)) + 4.0 * m * np.eye(m)[:, :, None]
+    b = BlockILU0(o.cartgridpart, o.f2e, o.elemcon, o.ncu, o.npf, o.nfe)
+    orig = b.assemble(H)
+    fac = b.factor(orig.copy())
+    for r in range(b.nse):
+        assert ilu_pattern_error(fac[r], orig[r], b.row_ptr, b.col_ind) < 1e-12

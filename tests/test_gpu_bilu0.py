@@ -62,6 +62,11 @@ def test_bilu0_blocks_and_apply(tmp_path, nd):
     b = o.bilu
     got = s.get("P").reshape(ncf, ncf, b.nse, len(b.col_ind), order="F")
     assert rel(got, np.transpose(o.P, (2, 3, 0, 1))) < TOL
+    # the device factors reproduce the assembled sub-domain matrix on its block pattern
+    from tests.test_bilu0_ordering import ilu_pattern_error
+    orig = b.assemble(o.H.reshape(o.ncu * o.npf * o.nfe, o.ncu * o.npf * o.nfe, o.ne, order="F"))
+    fac = np.transpose(got, (2, 3, 0, 1))
+    assert max(ilu_pattern_error(fac[r], orig[r], b.row_ptr, b.col_ind) for r in range(b.nse)) < 1e-10
     import torch
     N = s.sizes["ndofuhat"]
     v = np.random.default_rng(5).standard_normal(N)
