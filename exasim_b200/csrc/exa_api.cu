@@ -547,7 +547,11 @@ long long exa_ctx_estimate_bytes(const double* app, long long napp, const double
   per_elem += precond == 1 ? m * m : 0;
   // element chunk workspace (the whole mesh when it fits in 8 GB)
   per_elem += n * n + n * nqn + 2 * n * m + m * nqn + nge * (nd + 1) * ncu * nc + n + (n > 160 ? n * n : 0);
-  double words = ne * per_elem + N * (restart + 6) + (precond == 0 ? ncu * npf * ncu * npf * nf : 0);
+  // preconditioner blocks: block Jacobi one per face; block ILU(0) one per stored block of the
+  // sub-domain face graph, at most the face itself and the other faces of its two elements
+  const double ncf2 = ncu * npf * ncu * npf;
+  const double pblocks = precond == 0 ? ncf2 * nf : (precond == 2 ? ncf2 * nf * (1 + 2 * (nfe - 1)) : 0.0);
+  double words = ne * per_elem + N * (restart + 6) + pblocks;
   if (precision == 1) words *= 1.75;
   return (long long)(8.0 * words) + (16LL << 20);
 }
