@@ -106,7 +106,7 @@ int exa_inverse_ws(float* A, int n, long long stride, int batch, float* ws, int*
 // writes a partial sum and consumers reduce the partial array in a fixed order.
 int exa_vec_blocks();
 int exa_dot_partials(const double* x, const double* y, long long n, double* part, cudaStream_t st);
-int exa_reduce_partials(const double* part, double* out, int take_sqrt, cudaStream_t st);
+int exa_reduce_partials(const double* part, long long n, double* out, int take_sqrt, cudaStream_t st);
 int exa_axpby(double* y, const double* x, double a, double b, long long n, cudaStream_t st);
 int exa_scale(double* y, const double* x, double a, long long n, cudaStream_t st);
 int exa_fill(double* y, double a, long long n, cudaStream_t st);

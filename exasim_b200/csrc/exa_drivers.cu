@@ -73,7 +73,7 @@ ExaProfScope::~ExaProfScope() {
 
 int exa_drv_norm(ExaCtx& c, const double* x, long long n, double* out) {
   EXA_TRY(exa_dot_partials(x, x, n, c.part_a, c.st));
-  EXA_TRY(exa_reduce_partials(c.part_a, c.scal + 15, 1, c.st));
+  EXA_TRY(exa_reduce_partials(c.part_a, n, c.scal + 15, 1, c.st));
   EXA_CUDA(cudaMemcpyAsync(c.pinned, c.scal + 15, sizeof(double), cudaMemcpyDeviceToHost, c.st));
   EXA_CUDA(cudaStreamSynchronize(c.st));
   *out = c.pinned[0];
@@ -287,12 +287,12 @@ int rb_initial_guess(ExaCtx& c) {
   int nd = 0;
   for (int j = 0; j < cur; ++j) {
     EXA_TRY(exa_dot_partials(c.rbU + (long long)j * N, c.b, N, c.part_a, c.st));
-    EXA_TRY(exa_reduce_partials(c.part_a, c.rbD + nd++, 0, c.st));
+    EXA_TRY(exa_reduce_partials(c.part_a, N, c.rbD + nd++, 0, c.st));
   }
   for (int j = 0; j < cur; ++j)
     for (int k = 0; k <= j; ++k) {
       EXA_TRY(exa_dot_partials(c.rbU + (long long)j * N, c.rbU + (long long)k * N, N, c.part_a, c.st));
-      EXA_TRY(exa_reduce_partials(c.part_a, c.rbD + nd++, 0, c.st));
+      EXA_TRY(exa_reduce_partials(c.part_a, N, c.rbD + nd++, 0, c.st));
     }
   std::vector<double> d(nd);
   EXA_CUDA(cudaMemcpyAsync(d.data(), c.rbD, sizeof(double) * nd, cudaMemcpyDeviceToHost, c.st));

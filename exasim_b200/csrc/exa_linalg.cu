@@ -766,6 +766,28 @@ __device__ __forceinline__ double block_sum(double v) {
   return s;  // valid in thread 0
 }
 
+// Vectors of n entries run on vec_grid(n) blocks, one entry per thread up to VB blocks:
+// short vectors (a small mesh's trace space) occupy a few SMs instead of the whole GPU,
+// which leaves room for other contexts' kernels (on the served stream this was faster both
+// for one solve at a time and for 16 overlapping solves than a fixed VB blocks, and than
+// four entries per thread).  The count depends on n alone, so every reduction over the
+// same n takes the same partition and order.
+inline int vec_grid(long long n) {
+  const long long b = (n + VT - 1) / VT;
+  return (int)(b < 1 ? 1 : (b > VB ? VB : b));
+}
+
+// every block reduces the first nb partials in the same order (thread-parallel, then fixed tree)
+__device__ __forceinline__ double sum_partials_n(const double* part, int nb) {
+  __shared__ double tot_n;
+  double v = 0.0;
+  for (int i = threadIdx.x; i < nb; i += VT) v += part[i];
+  double s = block_sum(v);
+  if (threadIdx.x == 0) tot_n = s;
+  __syncthreads();
+  return tot_n;
+}
+
 // every block reduces the VB partials in the same order (thread-parallel, then fixed tree)
 __device__ __forceinline__ double sum_partials(const double* part) {
   __shared__ double tot;
@@ -779,13 +801,14 @@ __device__ __forceinline__ double sum_partials(const double* part) {
 
 __global__ void __launch_bounds__(VT) dot_kernel(const double* x, const double* y, long long n, double* part) {
   double v = 0.0;
-  for (long long i = blockIdx.x * (long long)VT + threadIdx.x; i < n; i += (long long)VB * VT) v = fma(x[i], y[i], v);
+  for (long long i = blockIdx.x * (long long)VT + threadIdx.x; i < n; i += (long long)gridDim.x * VT)
+    v = fma(x[i], y[i], v);
   double s = block_sum(v);
   if (threadIdx.x == 0) part[blockIdx.x] = s;
 }
 
-__global__ void __launch_bounds__(VT) reduce_kernel(const double* part, double* out, int take_sqrt) {
-  double s = sum_partials(part);
+__global__ void __launch_bounds__(VT) reduce_kernel(const double* part, int nb, double* out, int take_sqrt) {
+  double s = sum_partials_n(part, nb);
   if (threadIdx.x == 0) *out = take_sqrt ? sqrt(s) : s;
 }
 
@@ -807,10 +830,10 @@ __global__ void fill_kernel(double* y, double a, long long n) {
 __global__ void __launch_bounds__(VT) mgs_step_kernel(double* w, const double* vprev, const double* vnext,
                                                       const double* part_in, double* part_out, double* h_out,
                                                       long long n) {
-  const double h = sum_partials(part_in);
+  const double h = sum_partials_n(part_in, gridDim.x);
   if (blockIdx.x == 0 && threadIdx.x == 0) *h_out = h;
   double v = 0.0;
-  for (long long i = blockIdx.x * (long long)VT + threadIdx.x; i < n; i += (long long)VB * VT) {
+  for (long long i = blockIdx.x * (long long)VT + threadIdx.x; i < n; i += (long long)gridDim.x * VT) {
     double wi = w[i] - h * vprev[i];
     w[i] = wi;
     v = fma(wi, vnext ? vnext[i] : wi, v);
@@ -821,10 +844,10 @@ __global__ void __launch_bounds__(VT) mgs_step_kernel(double* w, const double* v
 
 __global__ void __launch_bounds__(VT) mgs_finish_kernel(double* vout, const double* w, const double* part_in,
                                                         double* h_out, long long n) {
-  const double h = sqrt(sum_partials(part_in));
+  const double h = sqrt(sum_partials_n(part_in, gridDim.x));
   if (blockIdx.x == 0 && threadIdx.x == 0) *h_out = h;
   const double r = 1.0 / h;
-  for (long long i = blockIdx.x * (long long)VT + threadIdx.x; i < n; i += (long long)VB * VT) vout[i] = w[i] * r;
+  for (long long i = blockIdx.x * (long long)VT + threadIdx.x; i < n; i += (long long)gridDim.x * VT) vout[i] = w[i] * r;
 }
 
 // cpuApplyGivensRotation (backend/Common/cpuimpl.h:167-196) on the device
@@ -867,16 +890,16 @@ __global__ void gemv_add_kernel(double* x, const double* V, const double* y, lon
 __global__ void __launch_bounds__(VT) multi_dot_kernel(const double* w, const double* V, long long n, int k, double* part) {
   for (int j = 0; j < k; ++j) {
     double v = 0.0;
-    for (long long i = blockIdx.x * (long long)VT + threadIdx.x; i < n; i += (long long)VB * VT)
+    for (long long i = blockIdx.x * (long long)VT + threadIdx.x; i < n; i += (long long)gridDim.x * VT)
       v = fma(V[i + n * j], w[i], v);
     double s = block_sum(v);
     if (threadIdx.x == 0) part[j * VB + blockIdx.x] = s;
   }
 }
 
-__global__ void __launch_bounds__(VT) multi_reduce_kernel(const double* part, double* h, int k) {
+__global__ void __launch_bounds__(VT) multi_reduce_kernel(const double* part, double* h, int k, int nb) {
   for (int j = 0; j < k; ++j) {
-    double s = sum_partials(part + j * VB);
+    double s = sum_partials_n(part + j * VB, nb);
     if (threadIdx.x == 0) h[j] = s;
     __syncthreads();
   }
@@ -894,47 +917,47 @@ __global__ void gemv_sub_kernel(double* w, const double* V, const double* h, lon
 int exa_vec_blocks() { return VB; }
 
 int exa_dot_partials(const double* x, const double* y, long long n, double* part, cudaStream_t st) {
-  dot_kernel<<<VB, VT, 0, st>>>(x, y, n, part);
+  dot_kernel<<<vec_grid(n), VT, 0, st>>>(x, y, n, part);
   EXA_LAUNCH_CHECK();
   return EXA_OK;
 }
 
-int exa_reduce_partials(const double* part, double* out, int take_sqrt, cudaStream_t st) {
-  reduce_kernel<<<1, VT, 0, st>>>(part, out, take_sqrt);
+int exa_reduce_partials(const double* part, long long n, double* out, int take_sqrt, cudaStream_t st) {
+  reduce_kernel<<<1, VT, 0, st>>>(part, vec_grid(n), out, take_sqrt);
   EXA_LAUNCH_CHECK();
   return EXA_OK;
 }
 
 int exa_axpby(double* y, const double* x, double a, double b, long long n, cudaStream_t st) {
   if (n <= 0) return EXA_OK;
-  axpby_kernel<<<VB, VT, 0, st>>>(y, x, a, b, n);
+  axpby_kernel<<<vec_grid(n), VT, 0, st>>>(y, x, a, b, n);
   EXA_LAUNCH_CHECK();
   return EXA_OK;
 }
 
 int exa_scale(double* y, const double* x, double a, long long n, cudaStream_t st) {
   if (n <= 0) return EXA_OK;
-  scale_kernel<<<VB, VT, 0, st>>>(y, x, a, n);
+  scale_kernel<<<vec_grid(n), VT, 0, st>>>(y, x, a, n);
   EXA_LAUNCH_CHECK();
   return EXA_OK;
 }
 
 int exa_fill(double* y, double a, long long n, cudaStream_t st) {
   if (n <= 0) return EXA_OK;
-  fill_kernel<<<VB, VT, 0, st>>>(y, a, n);
+  fill_kernel<<<vec_grid(n), VT, 0, st>>>(y, a, n);
   EXA_LAUNCH_CHECK();
   return EXA_OK;
 }
 
 int exa_mgs_step(double* w, const double* vprev, const double* vnext, const double* part_in,
                  double* part_out, double* h_out, long long n, cudaStream_t st) {
-  mgs_step_kernel<<<VB, VT, 0, st>>>(w, vprev, vnext, part_in, part_out, h_out, n);
+  mgs_step_kernel<<<vec_grid(n), VT, 0, st>>>(w, vprev, vnext, part_in, part_out, h_out, n);
   EXA_LAUNCH_CHECK();
   return EXA_OK;
 }
 
 int exa_mgs_finish(double* v, const double* w, const double* part_in, double* h_out, long long n, cudaStream_t st) {
-  mgs_finish_kernel<<<VB, VT, 0, st>>>(v, w, part_in, h_out, n);
+  mgs_finish_kernel<<<vec_grid(n), VT, 0, st>>>(v, w, part_in, h_out, n);
   EXA_LAUNCH_CHECK();
   return EXA_OK;
 }
@@ -948,17 +971,18 @@ int exa_givens(double* hcol, double* s, double* cs, double* sn, int i, const dou
 
 int exa_gemv_add(double* x, const double* V, const double* y, long long n, int k, cudaStream_t st) {
   if (k <= 0) return EXA_OK;
-  gemv_add_kernel<<<VB, VT, 0, st>>>(x, V, y, n, k);
+  gemv_add_kernel<<<vec_grid(n), VT, 0, st>>>(x, V, y, n, k);
   EXA_LAUNCH_CHECK();
   return EXA_OK;
 }
 
 int exa_cgs(double* w, const double* V, double* hcol, double* part, long long n, int k, cudaStream_t st) {
-  multi_dot_kernel<<<VB, VT, 0, st>>>(w, V, n, k, part);
+  const int nb = vec_grid(n);
+  multi_dot_kernel<<<nb, VT, 0, st>>>(w, V, n, k, part);
   EXA_LAUNCH_CHECK();
-  multi_reduce_kernel<<<1, VT, 0, st>>>(part, hcol, k);
+  multi_reduce_kernel<<<1, VT, 0, st>>>(part, hcol, k, nb);
   EXA_LAUNCH_CHECK();
-  gemv_sub_kernel<<<VB, VT, 0, st>>>(w, V, hcol, n, k);
+  gemv_sub_kernel<<<nb, VT, 0, st>>>(w, V, hcol, n, k);
   EXA_LAUNCH_CHECK();
   return EXA_OK;
 }
