@@ -56,18 +56,19 @@ def test_tf32_gemm_matches_rounded_reference(M, N, K, a64):
         assert np.array_equal(got[b, :, M:], C0[b, :, M:].astype(np.float64))
 
 
-@pytest.mark.parametrize("M,N,K,a64", [(125, 125, 375, True), (150, 150, 125, False), (125, 150, 375, True),
-                                       (150, 125, 375, True), (10, 12, 20, True), (64, 256, 40, False),
-                                       (150, 480, 320, True), (96, 300, 40, False)])
-def test_3xtf32_gemm_matches_fp64(M, N, K, a64):
+@pytest.mark.parametrize("M,N,K,a64,nb", [(125, 125, 375, True, 29), (150, 150, 125, False, 29),
+                                          (125, 150, 375, True, 29), (150, 125, 375, True, 29), (10, 12, 20, True, 29),
+                                          (64, 256, 40, False, 29), (150, 480, 320, True, 29), (96, 300, 40, False, 29),
+                                          (125, 125, 100, True, 700), (150, 150, 60, False, 400),
+                                          (64, 256, 40, False, 640)])
+def test_3xtf32_gemm_matches_fp64(M, N, K, a64, nb):
     """hi*hi + hi*lo + lo*hi drops the lo*lo term (2^-22 relative) and the tensor cores add the
     products in FP32 without round-to-nearest on every step: within 1e-5 of max |C| at K <= 375
-    (1xTF32 is about 1e-3 there)."""
+    (1xTF32 is about 1e-3 there).  Batches of 400 and more as well as 29."""
     import torch
     B.build(["poisson2d"])
     L = load_library("poisson2d")
     rng = np.random.default_rng(M * 7 + N * 3 + K)
-    nb = 29
     lda, ldb, ldc = M + 1, K + 3, M + 2
     A = rng.standard_normal((nb, K, lda))
     Bm = rng.standard_normal((nb, N, ldb))
