@@ -45,11 +45,13 @@ def parse():
     ap.add_argument("--n", type=int, default=CFG_N, help="elements per cube edge")
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--form", default="both", choices=["both", "mixed", "plain", "served"],
+    ap.add_argument("--form", default="both", choices=["both", "mixed", "plain", "served", "euler"],
                     help="time both forms (default) or one; one form prints a partial line, for profiling")
     ap.add_argument("--serve-requests", type=int, default=200,
                     help="requests per configuration of the served-stream leg (0 skips it)")
     ap.add_argument("--serve-slots", type=int, default=16)
+    ap.add_argument("--euler-n", type=int, default=32, help="elements per cube edge of the 3D Euler leg")
+    ap.add_argument("--euler-steps", type=int, default=4, help="timed stage solves per form of the 3D Euler leg (0 skips it)")
     return ap.parse_args()
 
 
@@ -217,12 +219,17 @@ MIXED = {"inner_tol": 1e-4, "rtol": 1e-8}
 # the served stream's small 2D solves: a looser inner GMRES tolerance per refinement step
 # takes fewer iterations in all (restarts lose less of the Krylov space)
 MIXED_SERVED = {"inner_tol": 1e-3, "rtol": 1e-8}
+# 3D Euler is nonlinear: the refinement steps reuse one assembly (a chord iteration), whose rate
+# and not the inner tolerance bounds each step, so a loose inner solve saves Krylov iterations
+MIXED_EULER = {"inner_tol": 1e-2, "rtol": 1e-8}
 
 
-def run_form(s, lib, torch, local, args, world, dist):
-    """W warm-up and K timed DIRK-stage solves of one solver on its own stream."""
+def run_form(s, lib, torch, local, args, world, dist, ndt=20, S=3, steps=None, warmup=None):
+    """W warm-up and K timed DIRK-stage solves of one solver on its own stream, through ndt
+    time steps of S stages (wrapping around)."""
     stream = torch.cuda.ExternalStream(s.stream(), device=local)
-    ndt, S = 20, 3
+    steps = args.steps if steps is None else steps
+    warmup = args.warmup if warmup is None else warmup
     k = [0]
 
     def stage():
@@ -231,12 +238,12 @@ def run_form(s, lib, torch, local, args, world, dist):
         k[0] += 1
         return its
 
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         stage()
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
-    ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(steps + 1)]
     gmres, newton, ratios = [], [], []
     s.profile(True)  # per-phase CUDA events on the solver's stream, read after the timed region
     l0 = lib.exa_launch_count()
@@ -244,7 +251,7 @@ def run_form(s, lib, torch, local, args, world, dist):
         torch.cuda.synchronize()
         torch.cuda.profiler.start()  # a profiler started with --profile-from-start off sees the timed region only
         ev[0].record(stream)
-        for i in range(args.steps):
+        for i in range(steps):
             newton.append(stage())
             gmres.append(s.stats()["gmres_total"])
             r0, r1 = s.last_residual()
@@ -255,8 +262,8 @@ def run_form(s, lib, torch, local, args, world, dist):
     launches = lib.exa_launch_count() - l0
     s.profile(False)
     prof = s.profile_read()
-    per = [ev[i].elapsed_time(ev[i + 1]) for i in range(args.steps)]
-    total = max_over_ranks(ev[0].elapsed_time(ev[args.steps]), world, dist, torch, f"cuda:{local}")
+    per = [ev[i].elapsed_time(ev[i + 1]) for i in range(steps)]
+    total = max_over_ranks(ev[0].elapsed_time(ev[steps]), world, dist, torch, f"cuda:{local}")
     return {"total_ms": total, "per": per, "gmres": gmres, "newton": newton, "ratios": ratios,
             "launches": launches, "prof": prof, "clocks": clk.summary(), "stream": stream, "stage": stage}
 
@@ -295,6 +302,15 @@ def run_ours(args):
         s64 = HDGSolver(d, "convdiff3d", device=local)
         s32 = HDGSolver(d, "convdiff3d", device=local)
         s32.set_precision(1, **MIXED)
+        if args.form == "euler":
+            s64.close()
+            s32.close()
+            if rank == 0:
+                print(json.dumps({"metric": METRIC, "form": "euler", "euler3d": run_euler(args, local, tmp)}), flush=True)
+            if world > 1:
+                dist.barrier()
+                dist.destroy_process_group()
+            return 0
         if args.form == "served":
             served = run_served(args, local)
             if rank == 0:
@@ -368,6 +384,8 @@ def run_ours(args):
             out.update(roof)
             if args.serve_requests > 0 and world == 1:
                 out["served"] = run_served(args, local)
+            if args.euler_steps > 0 and world == 1:
+                out["euler3d"] = run_euler(args, local, tmp)
             if not args.no_cpu_baseline and world == 1:
                 out["cpu_baseline"] = {k: v for k, v in cpu_baseline_sample(tmp, args.n).items()
                                        if k != "per_solve_s_sample"}
@@ -390,6 +408,47 @@ def run_one_form(s, lib, torch, local, args, world, dist, rank):
                           "gmres_iters_per_solve": float(np.mean(r["gmres"])),
                           "residual_ratio_max": max(r["ratios"]), "gpu_launches": int(r["launches"]),
                           "clocks": r["clocks"], "phases": phases_of(r["prof"], args.steps)}), flush=True)
+
+
+def run_euler(args, local, tmp):
+    """The 3D Euler leg: the isentropic-vortex configuration (p = 3 hexahedra of a periodic
+    cube, 5 conserved variables, strength 5, Mach 0.5, DIRK(2,2) dt = 0.05) on args.euler_n^3
+    elements.  Its element blocks are 320 x 320 and its condensed blocks 480 x 480, and there is
+    no q, so the elimination is the block inverse and the Schur products: compute-bound, where
+    the plain form runs FP64 DMMA and the mixed form 3xTF32 tcgen05.  Both forms solve the same
+    stages from the same start (W warm-up, then the timed ones); the mixed solution is compared
+    with the FP64 one after the last stage."""
+    import torch
+    from exasim_b200 import HDGSolver, load_library, build as B, cases
+    B.build(["euler3d"])
+    lib = load_library("euler3d")
+    n = args.euler_n
+    d = os.path.join(tmp, "euler_datain")
+    cases.euler3d_vortex_hex(d, n=n, porder=3, nsteps=5, dt=0.05)
+    forms = {}
+    sol = {}
+    for name, prec in (("plain_fp64", 0), ("mixed", 1)):
+        s = HDGSolver(d, "euler3d", device=local)
+        if prec:
+            s.set_precision(1, **MIXED_EULER)
+        r = run_form(s, lib, torch, local, args, 1, None, ndt=5, S=2, steps=args.euler_steps)
+        st = args.euler_steps
+        forms[name] = {"value": st / (r["total_ms"] * 1e-3), "unit": "solves/s", "ms_per_step": r["total_ms"] / st,
+                       "latency_ms": {"p50": float(np.percentile(r["per"], 50)),
+                                      "p99": float(np.percentile(r["per"], 99))},
+                       "newton_steps_per_solve": float(np.mean(r["newton"])),
+                       "gmres_iters_per_solve": float(np.mean(r["gmres"])),
+                       "residual_ratio_max": max(r["ratios"]), "gpu_launches": int(r["launches"]),
+                       "clocks": r["clocks"], "phases": phases_of(r["prof"], st)}
+        sol[name] = s.get("udg")
+        s.close()
+    u, ref = sol["mixed"], sol["plain_fp64"]
+    return {"workload": f"3D Euler HDG p=3, periodic {n}^3 hexahedra ({n ** 3} elements, 320 x 320 element "
+                        "blocks), isentropic vortex strength 5, Mach 0.5, DIRK(2,2) dt=0.05, block-Jacobi GMRES",
+            "elements": n ** 3, "steps": args.euler_steps, "warmup": args.warmup,
+            "mixed": forms["mixed"], "plain_fp64": forms["plain_fp64"],
+            "speedup_vs_plain_fp64": forms["mixed"]["value"] / forms["plain_fp64"]["value"],
+            "mixed_vs_fp64_rel_l2": float(np.linalg.norm(u - ref) / np.linalg.norm(ref))}
 
 
 SERVED_WORKLOAD = ("served stream of 2D convection-diffusion HDG solves: kappa log-uniform [1e-3, 1], unit "

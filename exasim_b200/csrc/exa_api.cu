@@ -336,7 +336,8 @@ int exa_ctx_init(ExaCtx& c, const double* app, long long napp, const double* mas
   }
 
   // condensed system and workspace
-  const size_t n = P.n, m = P.m, nqn = (size_t)P.npe * P.nd * P.ncu;
+  // B and G (the q columns) exist only for models with q
+  const size_t n = P.n, m = P.m, nqn = P.ncq > 0 ? (size_t)P.npe * P.nd * P.ncu : 0;
   EXA_TRY(dev_alloc(c, &c.H, ne * m * m));
   EXA_TRY(dev_alloc(c, &c.F, ne * n * m));
   EXA_TRY(dev_alloc(c, &c.Ru, ne * n));
@@ -414,13 +415,68 @@ int exa_ctx_init(ExaCtx& c, const double* app, long long napp, const double* mas
   return EXA_OK;
 }
 
+namespace {
+// Frees one allocation of the context (stream-ordered) and takes it off its list.
+void dev_release(ExaCtx& c, void* p, size_t bytes) {
+  if (!p) return;
+  for (size_t i = 0; i < c.allocs.size(); ++i)
+    if (c.allocs[i] == p) {
+      c.allocs.erase(c.allocs.begin() + (long long)i);
+      c.alloc_bytes -= (long long)bytes;
+      break;
+    }
+  cudaFreeAsync(p, c.st);
+}
+
+size_t precond_blocks(const ExaCtx& c) {
+  const ExaDims& P = c.P;
+  const size_t ncf = (size_t)P.ncu * P.npf;
+  if (c.preconditioner == 0) return ncf * ncf * P.nf;
+  if (c.preconditioner == 2) return ncf * ncf * c.bilu.nse * c.bilu.nnz;
+  return (size_t)P.ne * P.m * P.m;
+}
+
+// The FP64 condensed blocks for all elements (full) or the mixed form's staging only: H for
+// one element chunk, no F and no FP64 preconditioner blocks.  At 32^3 hexahedra of 3D Euler
+// (p = 3) the full set is 105 GB, which the mixed form cannot hold beside its FP32 copies.
+// The plain form's captured GMRES steps name the freed arrays, so they are dropped.
+int fp64_blocks(ExaCtx& c, bool full) {
+  if (full == c.fp64_full) return EXA_OK;
+  const ExaDims& P = c.P;
+  const size_t ne = P.ne, n = P.n, m = P.m, nb = c.neb;
+  EXA_CUDA(cudaStreamSynchronize(c.st));
+  for (cudaGraphExec_t& g : c.arnoldi_graph[0]) {
+    if (g) cudaGraphExecDestroy(g);
+    g = nullptr;
+  }
+  std::fill(c.arnoldi_seen[0].begin(), c.arnoldi_seen[0].end(), 0);
+  dev_release(c, c.H, sizeof(double) * (full ? nb : ne) * m * m);
+  c.H = nullptr;
+  if (full) {
+    EXA_TRY(dev_alloc(c, &c.H, ne * m * m));
+    EXA_TRY(dev_alloc(c, &c.F, ne * n * m));
+    EXA_TRY(dev_alloc(c, &c.Pc, precond_blocks(c)));
+  } else {
+    dev_release(c, c.F, sizeof(double) * ne * n * m);
+    dev_release(c, c.Pc, sizeof(double) * precond_blocks(c));
+    c.F = nullptr;
+    c.Pc = nullptr;
+    EXA_TRY(dev_alloc(c, &c.H, nb * m * m));
+  }
+  c.fp64_full = full;
+  return EXA_OK;
+}
+}  // namespace
+
 // Switch between the plain FP64 form (0) and the mixed-precision form (1).  The FP32
-// arrays of the mixed form are allocated on the first switch to it and kept afterwards.
+// arrays of the mixed form are allocated on the first switch to it and kept afterwards;
+// the FP64 blocks that the new form does not read are freed (fp64_blocks).
 int exa_ctx_set_precision(ExaCtx& c, int mode) {
   if (mode != 0 && mode != 1) {
     exa_set_error("precision mode %d: 0 (FP64) or 1 (FP32/TF32 elimination with FP64 refinement)", mode);
     return EXA_ERR_ARG;
   }
+  if (mode == 1) EXA_TRY(fp64_blocks(c, false));
   if (mode == 1 && c.H32 == nullptr) {
     const ExaDims& P = c.P;
     const size_t ne = P.ne, n = P.n, m = P.m, nb = c.neb;
@@ -469,6 +525,7 @@ int exa_ctx_set_precision(ExaCtx& c, int mode) {
     c.d_uflag = c.d_flag + 1;
     EXA_CUDA(cudaStreamSynchronize(c.st));
   }
+  if (mode == 0) EXA_TRY(fp64_blocks(c, true));
   c.precision = mode;
   return EXA_OK;
 }
@@ -601,14 +658,14 @@ bool field(ExaCtx& c, const char* name, FieldRef& f) {
   const std::string s(name ? name : "");
   if (s == "udg") f = {c.udg, (long long)P.npe * P.nc * ne};
   else if (s == "uh") f = {c.uh, N};
-  else if (s == "H") f = {c.H, m * m * ne};
-  else if (s == "F") f = {c.F, n * m * ne};
+  else if (s == "H" && c.fp64_full) f = {c.H, m * m * ne};
+  else if (s == "F" && c.fp64_full) f = {c.F, n * m * ne};
   else if (s == "Ru") f = {c.Ru, n * ne};
   else if (s == "Rh") f = {c.Rh, m * ne};
   else if (s == "b") f = {c.b, N};
   else if (s == "x") f = {c.x, N};
   else if (s == "sdg") f = {c.sdg, n * ne};
-  else if (s == "P")
+  else if (s == "P" && c.fp64_full)
     f = {c.Pc, c.preconditioner == 0   ? (long long)P.ncu * P.npf * P.ncu * P.npf * P.nf
                : c.preconditioner == 2 ? (long long)P.ncu * P.npf * P.ncu * P.npf * c.bilu.nse * c.bilu.nnz
                                        : m * m * ne};

@@ -530,9 +530,16 @@ int exa_drv_newton(ExaCtx& c, int* iters_out, double* norm_out) {
 int exa_drv_condense_mixed(ExaCtx& c) {
   const ExaDims& P = c.P;
   const int n = P.n, m = P.m;
-  EXA_CUDA(cudaMemcpyAsync(c.wRu, c.Ru, sizeof(double) * (size_t)n * P.ne, cudaMemcpyDeviceToDevice, c.st));
-  EXA_TRY(exa_k_gemv32(n, n, P.ne, 1.0, c.Dinv32, (long long)n * n, c.wRu, n, 0.0, c.Ru, n, c.st));
-  EXA_TRY(exa_k_gemv32(m, n, P.ne, -1.0, c.K32, (long long)m * n, c.Ru, n, 1.0, c.Rh, m, c.st));
+  // in element chunks of the assembly's workspace (c.wRu holds neb element vectors)
+  for (int e0 = 0; e0 < P.ne; e0 += c.neb) {
+    const int nb = std::min(c.neb, P.ne - e0);
+    double* Ruc = c.Ru + (long long)e0 * n;
+    EXA_CUDA(cudaMemcpyAsync(c.wRu, Ruc, sizeof(double) * (size_t)n * nb, cudaMemcpyDeviceToDevice, c.st));
+    EXA_TRY(exa_k_gemv32(n, n, nb, 1.0, c.Dinv32 + (long long)e0 * n * n, (long long)n * n, c.wRu, n, 0.0, Ruc, n,
+                         c.st));
+    EXA_TRY(exa_k_gemv32(m, n, nb, -1.0, c.K32 + (long long)e0 * m * n, (long long)m * n, Ruc, n, 1.0,
+                         c.Rh + (long long)e0 * m, m, c.st));
+  }
   return exa_k_scatter(P, c.f2e, c.elemcon, c.Rh, c.b, c.st);
 }
 

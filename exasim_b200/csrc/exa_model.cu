@@ -124,7 +124,7 @@ int schur_chunk_mixed(ExaCtx& c, int e0, int nb) {
   float* K32 = c.K32 + (long long)e0 * m * n;
   float* H32 = c.H32 + (long long)e0 * m * m;
   float* F32 = c.F32 + (long long)e0 * n * m;
-  const double* Hc = c.H + (long long)e0 * m * m;
+  const double* Hc = c.fp64_full ? c.H + (long long)e0 * m * m : c.H;  // per-chunk staging in the mixed form
   auto at = [](UPacked u, long long e) {  // operand of element e of the set
     u.hi += e * u.sb;
     u.lo += e * u.sb;
@@ -255,7 +255,7 @@ int exa_model_assemble(ExaCtx& c, bool jacobian) {
           EXA_LAUNCH_CHECK();
         }
       }
-      double* Hc = c.H + (long long)e0 * m * m;
+      double* Hc = c.fp64_full ? c.H + (long long)e0 * m * m : c.H;
       {
         ExaProfScope ps(c, EXA_PH_FACE);
         EXA_CUDA(cudaMemsetAsync(c.wF, 0, sizeof(double) * (size_t)nb * n * m, c.st));

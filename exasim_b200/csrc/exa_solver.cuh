@@ -88,6 +88,9 @@ struct ExaCtx {
   // the residual, the Newton update and GMRES stay FP64 and iterate the FP32 solve to the
   // FP64 residual tolerance.
   int precision = 0;              // 0 plain FP64, 1 mixed
+  // FP64 H, F (D^-1 F) and preconditioner blocks held for all elements (the plain form); the
+  // mixed form holds neither F nor the FP64 preconditioner, and H for one element chunk only
+  bool fp64_full = true;
   double mixed_inner_tol = 1e-4;  // GMRES tolerance of each refinement step
   double mixed_rtol = 0.0;        // target residual ratio of a mixed solve (0: GMRES tolerance)
   int mixed_maxit = 30;           // refinement steps per mixed solve

@@ -236,7 +236,8 @@ int exa_gemm_tf32(const UGemm& g, int* flag, cudaStream_t st) {
 // ==================================================================================
 namespace {
 
-constexpr int PST = 3;    // stages
+// shared-memory ring: 3 stages for N tiles up to 160 (two CTAs per SM); 2 stages for 256,
+// so that two CTAs still share an SM and one's epilogue overlaps the other's main loop
 constexpr int PNT = 128;  // threads (4 warps: epilogue lanes 0..127)
 
 // one CTA per (batch entry, row tile): lane l of a warp takes row 32 rb + l of the tile and
@@ -282,7 +283,7 @@ __global__ void __launch_bounds__(256) pack_kernel(const TS* src, long long rs, 
   }
 }
 
-template <int NP, typename TCI, typename TCO>
+template <int NP, int PST, typename TCI, typename TCO>
 __global__ void __launch_bounds__(PNT, 1) umma3_kernel(UGemmP g, int* flag) {
   static_assert(NP % 16 == 0 && NP >= 16 && NP <= 256, "N tile");
   constexpr int A_B = 16 * 512, B_B = (NP / 8) * 512;     // one part (hi or lo) per stage
@@ -470,11 +471,11 @@ __global__ void __launch_bounds__(PNT, 1) umma3_kernel(UGemmP g, int* flag) {
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TCOLS) : "memory");
 }
 
-template <int NP, typename TCI, typename TCO>
+template <int NP, int PST, typename TCI, typename TCO>
 int launch_umma3(const UGemmP& g, int* flag, cudaStream_t st) {
   constexpr size_t smem = (size_t)PST * 2 * (16 * 512 + (NP / 8) * 512) + (2 * PST + 1) * 8 + 16;
   static_assert(smem <= 227 * 1024, "tile exceeds shared memory");
-  auto kern = umma3_kernel<NP, TCI, TCO>;
+  auto kern = umma3_kernel<NP, PST, TCI, TCO>;
   EXA_TRY(exa_allow_smem((const void*)kern, smem));
   EXA_CUDA(cudaFuncSetAttribute((const void*)kern, cudaFuncAttributePreferredSharedMemoryCarveout,
                                 (int)cudaSharedmemCarveoutMaxShared));
@@ -486,9 +487,9 @@ int launch_umma3(const UGemmP& g, int* flag, cudaStream_t st) {
 
 template <typename TCI, typename TCO>
 int umma3_np(const UGemmP& g, int* flag, cudaStream_t st) {
-  if (g.N <= 128) return launch_umma3<128, TCI, TCO>(g, flag, st);
-  if (g.N <= 160) return launch_umma3<160, TCI, TCO>(g, flag, st);
-  return launch_umma3<256, TCI, TCO>(g, flag, st);
+  if (g.N <= 128) return launch_umma3<128, 3, TCI, TCO>(g, flag, st);
+  if (g.N <= 160) return launch_umma3<160, 3, TCI, TCO>(g, flag, st);
+  return launch_umma3<256, 2, TCI, TCO>(g, flag, st);
 }
 
 }  // namespace
