@@ -71,6 +71,7 @@ def load_library(model: str) -> ctypes.CDLL:
         "exa_launch_count": ([], LL),
         "exa_dgemm_batched": ([I, I, I, D, P, LL, LL, P, LL, LL, D, P, LL, LL, I, P], I),
         "exa_dinverse_batched": ([P, I, LL, I, P, P], I),
+        "exa_sinverse_batched": ([P, I, LL, I, P, P], I),
         "exa_dgemm_tune": ([I, I, I, I, P, PI], I),
         "exa_dnrm2_cols_fixed": ([P, LL, LL, I, P, P], I),
         "exa_gemm_tf32_batched": ([I, I, I, D, P, I, LL, LL, P, I, LL, LL, D, P, I, LL, LL, I, P, P], I),

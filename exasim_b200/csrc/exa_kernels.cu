@@ -312,20 +312,111 @@ __global__ void bj_apply_kernel(ExaDims P, const T* BE, const double* x, double*
   }
 }
 
-// du_e = Ru_e + DinvF_e gather(x) (matvec.cpp:219-238); udg(:, 0:ncu, e) += alpha du_e
-template <typename T>
-__global__ void dudg_kernel(ExaDims P, const int* elemcon, const T* DinvF, const double* Ru, const double* x,
-                            double* du) {
-  extern __shared__ double ve[];
-  const int e = blockIdx.x, m = P.m, n = P.n, ncu = P.ncu;
-  for (int r = threadIdx.x; r < m; r += blockDim.x) ve[r] = x[r % ncu + ncu * (long long)elemcon[r / ncu + P.ndf * e]];
+// y_e = alpha A_e x_e + beta y0_e for a batch of column-major M x K blocks A_e (leading
+// dimension M, batch stride sA; y0 may alias y).  x_e is read at x + e sx, or, with elemcon,
+// gathered from a trace vector: x_e[k] = x[k % ncu + ncu elemcon[k / ncu + ndf e]].  The
+// scheme of elem_matvec_kernel: 8 warps split the columns four at a time with the next four
+// loaded ahead, lane l keeps rows l + 32 i (i < RI) in registers, and a row's 8 partial sums
+// meet in shared memory in a fixed order.  Serves du = Ru + D^-1 F x (hdgGetDUDG,
+// matvec.cpp:219-238) and the mixed form's Ru <- D^-1 Ru, Rh <- Rh - K Ru.
+template <typename T, int RI>
+__global__ void __launch_bounds__(256) bgemv_kernel(int M, int K, const T* A, long long sA, const double* x,
+                                                    long long sx, const int* elemcon, int ndf, int ncu,
+                                                    double alpha, double beta, const double* y0, double* y,
+                                                    long long sy) {
+  extern __shared__ double sm[];
+  double* xe = sm;         // [K]
+  double* part = sm + K;   // [8][M]
+  const long long e = blockIdx.x;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const T* Ae = A + e * sA;
+  auto load4 = [&](int c0, T (&v)[4][RI]) {
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const T* a = Ae + (long long)M * (c0 + 8 * u);
+#pragma unroll
+      for (int i = 0; i < RI; ++i) {
+        const int r = lane + 32 * i;
+        v[u][i] = r < M ? a[r] : T(0);
+      }
+    }
+  };
+  int c = warp;
+  T a[4][RI];
+  if (c + 24 < K) load4(c, a);
+  for (int k = threadIdx.x; k < K; k += blockDim.x)
+    xe[k] = elemcon ? x[k % ncu + ncu * (long long)elemcon[k / ncu + (long long)ndf * e]] : x[e * sx + k];
   __syncthreads();
-  const T* A = DinvF + (long long)e * n * m;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    double s = 0.0;
-    for (int c = 0; c < m; ++c) s = fma((double)A[i + (long long)n * c], ve[c], s);
-    du[(long long)e * n + i] = Ru[(long long)e * n + i] + s;
+  double acc[RI];
+#pragma unroll
+  for (int i = 0; i < RI; ++i) acc[i] = 0.0;
+  for (; c + 24 < K; c += 32) {
+    T an[4][RI];
+    const bool more = c + 56 < K;
+    if (more) load4(c + 32, an);
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const double xv = xe[c + 8 * u];
+#pragma unroll
+      for (int i = 0; i < RI; ++i) acc[i] = fma((double)a[u][i], xv, acc[i]);
+    }
+    if (more) {
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int i = 0; i < RI; ++i) a[u][i] = an[u][i];
+    }
   }
+  for (; c < K; c += 8) {
+    const T* a0 = Ae + (long long)M * c;
+    const double xv = xe[c];
+#pragma unroll
+    for (int i = 0; i < RI; ++i) {
+      const int r = lane + 32 * i;
+      if (r < M) acc[i] = fma((double)a0[r], xv, acc[i]);
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < RI; ++i) {
+    const int r = lane + 32 * i;
+    if (r < M) part[warp * M + r] = acc[i];
+  }
+  __syncthreads();
+  for (int r = threadIdx.x; r < M; r += blockDim.x) {
+    double s = 0.0;
+#pragma unroll
+    for (int w = 0; w < 8; ++w) s += part[w * M + r];
+    const double prev = beta != 0.0 ? y0[e * sy + r] : 0.0;
+    y[e * sy + r] = alpha * s + beta * prev;
+  }
+}
+
+template <typename T>
+int launch_bgemv(int M, int K, int batch, const T* A, long long sA, const double* x, long long sx,
+                 const int* elemcon, int ndf, int ncu, double alpha, double beta, const double* y0, double* y,
+                 long long sy, cudaStream_t st) {
+  if (batch <= 0 || M <= 0) return EXA_OK;
+  if (M > 512 || K > 512) {
+    exa_set_error("batched gemv: blocks of %d x %d exceed 512 x 512", M, K);
+    return EXA_ERR_UNSUPPORTED;
+  }
+  const size_t smem = sizeof(double) * ((size_t)(K > 0 ? K : 1) + 8 * (size_t)M);
+  const int ri = (M + 31) / 32;
+#define EXA_BGEMV(R)                                                                                          \
+  bgemv_kernel<T, R><<<batch, 256, smem, st>>>(M, K, A, sA, x, sx, elemcon, ndf, ncu, alpha, beta, y0, y, sy)
+  if (ri <= 1) EXA_BGEMV(1);
+  else if (ri <= 2) EXA_BGEMV(2);
+  else if (ri <= 3) EXA_BGEMV(3);
+  else if (ri <= 4) EXA_BGEMV(4);
+  else if (ri <= 5) EXA_BGEMV(5);
+  else if (ri <= 6) EXA_BGEMV(6);
+  else if (ri <= 8) EXA_BGEMV(8);
+  else if (ri <= 10) EXA_BGEMV(10);
+  else if (ri <= 12) EXA_BGEMV(12);
+  else EXA_BGEMV(16);
+#undef EXA_BGEMV
+  EXA_LAUNCH_CHECK();
+  return EXA_OK;
 }
 
 __global__ void udg_update_kernel(ExaDims P, double* udg, const double* du, double alpha) {
@@ -532,9 +623,9 @@ int exa_k_bj_apply(const ExaDims& P, const T* BE, const double* x, double* y, cu
 template <typename T>
 int exa_k_dudg(const ExaDims& P, const int* elemcon, const T* DinvF, const double* Ru, const double* x,
                double* du, cudaStream_t st) {
-  dudg_kernel<<<P.ne, 128, P.m * sizeof(double), st>>>(P, elemcon, DinvF, Ru, x, du);
-  EXA_LAUNCH_CHECK();
-  return EXA_OK;
+  // du_e = Ru_e + DinvF_e gather(x)
+  return launch_bgemv<T>(P.n, P.m, P.ne, DinvF, (long long)P.n * P.m, x, 0, elemcon, P.ndf, P.ncu, 1.0, 1.0, Ru, du,
+                         P.n, st);
 }
 
 int exa_k_udg_update(const ExaDims& P, double* udg, const double* du, double alpha, cudaStream_t st) {
@@ -574,21 +665,6 @@ int exa_k_face_nodes(const ExaDims& P, const int* f2e, const int* perm, const do
 }
 
 namespace {
-__global__ void gemv32_kernel(int M, int K, double alpha, const float* A, long long sA, const double* x,
-                              long long sx, double beta, double* y, long long sy) {
-  extern __shared__ double xs[];
-  const long long e = blockIdx.x;
-  for (int k = threadIdx.x; k < K; k += blockDim.x) xs[k] = x[e * sx + k];
-  __syncthreads();
-  const float* Ae = A + e * sA;
-  for (int r = threadIdx.x; r < M; r += blockDim.x) {
-    double s = 0.0;
-    for (int k = 0; k < K; ++k) s = fma((double)Ae[r + (long long)M * k], xs[k], s);
-    double* yr = y + e * sy + r;
-    *yr = (beta == 0.0) ? alpha * s : alpha * s + beta * *yr;
-  }
-}
-
 __global__ void to_f32_kernel(const double* x, float* y, long long n) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
     y[i] = (float)x[i];
@@ -597,11 +673,7 @@ __global__ void to_f32_kernel(const double* x, float* y, long long n) {
 
 int exa_k_gemv32(int M, int K, int batch, double alpha, const float* A, long long sA, const double* x, long long sx,
                  double beta, double* y, long long sy, cudaStream_t st) {
-  if (batch <= 0 || M <= 0) return EXA_OK;
-  const int th = M <= 64 ? 64 : (M <= 128 ? 128 : 256);
-  gemv32_kernel<<<batch, th, sizeof(double) * (size_t)(K > 0 ? K : 1), st>>>(M, K, alpha, A, sA, x, sx, beta, y, sy);
-  EXA_LAUNCH_CHECK();
-  return EXA_OK;
+  return launch_bgemv<float>(M, K, batch, A, sA, x, sx, nullptr, 0, 1, alpha, beta, y, y, sy, st);
 }
 
 int exa_k_to_f32(const double* x, float* y, long long n, cudaStream_t st) {

@@ -13,6 +13,7 @@
 #include <cmath>
 
 #include "exa_common.cuh"
+#include "exa_umma.cuh"
 
 #include <algorithm>
 #include <array>
@@ -731,6 +732,113 @@ int inverse_ws(T* A, int n, long long stride, int batch, T* ws, int* d_flag, cud
   return inverse_blocked<T>(A, n, stride, batch, ws, d_flag, st);
 }
 }  // namespace
+
+// ----------------------------------------------------------------------------------
+// The same 2 x 2 block inverse for FP32 blocks with the five products on the tcgen05
+// 3xTF32 GEMM (the mixed-precision form).  With X = A11^-1 and Y = S^-1:
+//   W1 = X A12, S = A22 - A21 W1, W3 = A21 X,
+//   A12 <- -W1 Y, A11 <- X - A12 W3, A21 <- -Y W3, A22 <- Y.
+// W1 and W3 exist only packed: the products that make them write their packed copies
+// (A and B operand layouts) from the epilogue.  The packed operands live in pk: seven
+// slots of hi and lo parts, per matrix; X as A and A12 as B are dead once W1 exists, and
+// W1 as B once S does, so Y (A and B) and the new A12 (A) take their slots.
+// ----------------------------------------------------------------------------------
+namespace {
+long long inv_tc_slot(int n) {
+  const int n1 = (n + 1) / 2;
+  return exa_pack_size(n1, n1);  // every operand has at most n1 rows and n1 k
+}
+}  // namespace
+
+long long exa_inverse_tc32_pk(int n) { return n > INV_MAX_N ? 14 * inv_tc_slot(n) : 0; }
+
+int exa_inverse_tc32(float* A, int n, long long stride, int batch, float* ws, float* pk, int* d_flag, int* uflag,
+                     cudaStream_t st) {
+  if (n <= INV_MAX_N || batch <= 0) return inverse_dispatch<float>(A, n, stride, batch, d_flag, st);
+  if (n > 2 * INV_MAX_N) {
+    exa_set_error("dense inverse of order %d exceeds the blocked kernel limit %d", n, 2 * INV_MAX_N);
+    return EXA_ERR_UNSUPPORTED;
+  }
+  if (!ws || !pk) {
+    exa_set_error("tensor-core inverse of order %d needs workspaces", n);
+    return EXA_ERR_ARG;
+  }
+  const int n1 = (n + 1) / 2, n2 = n - n1;
+  const long long sw = (long long)n * n, S = inv_tc_slot(n), spk = exa_inverse_tc32_pk(n);
+  float* W0 = ws;                       // n1 x n1: A11, then X
+  float* W2 = W0 + (long long)n1 * n1;  // n2 x n2: S, then Y
+  float* A11 = A;
+  float* A21 = A + n1;
+  float* A12 = A + (long long)n * n1;
+  float* A22 = A + n1 + (long long)n * n1;
+  // slot k: hi at pk + 2kS, lo at pk + (2k+1)S, per matrix stride spk
+  auto op = [&](int k, int R, int K, bool as_b) {
+    UPacked u{};
+    u.hi = pk + 2LL * k * S;
+    u.lo = u.hi + S;
+    u.sb = spk;
+    u.sb2 = 0;
+    u.R = R;
+    u.K = K;
+    u.TR = as_b ? (R + 15) / 16 * 16 : 128;  // a B operand is one tile of all its rows
+    return u;
+  };
+  const UPacked Xa = op(0, n1, n1, false), A12b = op(1, n2, n1, true), W1b = op(2, n2, n1, true);
+  const UPacked Xb = op(3, n1, n1, true), A21a = op(4, n2, n1, false), W1a = op(5, n1, n2, false);
+  const UPacked W3b = op(6, n1, n2, true);
+  const UPacked Ya = op(0, n2, n2, false), Yb = op(1, n2, n2, true), A12a = op(2, n1, n2, false);
+  auto gemm = [&](int M, int N, int K, double alpha, const UPacked& Aop, const UPacked& Bop, double beta,
+                  const float* Cin, long long ldci, long long sci, float* C, long long ldc, long long sc,
+                  std::initializer_list<UPackOut> outs) {
+    UGemmP g{};
+    g.M = M; g.N = N; g.K = K; g.alpha = alpha; g.beta = beta;
+    g.A = Aop; g.B = Bop;
+    g.Cin = Cin; g.tci = EXA_T_F32; g.ldci = ldci; g.sCi = sci;
+    g.C = C; g.tco = EXA_T_F32; g.ldc = ldc; g.sC = sc;
+    g.nout = 0;
+    for (const UPackOut& o : outs) g.out[g.nout++] = o;
+    g.batch = batch; g.batch2 = 1;
+    return exa_gemm_3xtf32(g, uflag, st);
+  };
+  // the packs write every entry of an operand, padding included; the products' packed
+  // outputs write only the rows and k of the product, so where halves are not multiples of
+  // 16 the slots they write are cleared first (a slot may hold another shape's entries)
+  const bool padded = (n1 % 16) != 0 || (n2 % 16) != 0;
+  auto clear = [&](int k) -> cudaError_t {
+    if (!padded) return cudaSuccess;
+    return cudaMemset2DAsync(pk + 2LL * k * S, sizeof(float) * (size_t)spk, 0, sizeof(float) * 2 * (size_t)S,
+                             (size_t)batch, st);
+  };
+  EXA_TRY(subcopy<float>(W0, n1, sw, A11, n, stride, n1, n1, batch, st));
+  EXA_TRY(inverse_dispatch<float>(W0, n1, sw, batch, d_flag, st));
+  EXA_TRY(exa_pack(W0, 0, 1, n1, sw, 0, batch, 1, Xa, st));
+  EXA_TRY(exa_pack(W0, 0, n1, 1, sw, 0, batch, 1, Xb, st));
+  EXA_TRY(exa_pack(A12, 0, n, 1, stride, 0, batch, 1, A12b, st));
+  EXA_TRY(exa_pack(A21, 0, 1, n, stride, 0, batch, 1, A21a, st));
+  // W1 = X A12 (packed as A and as B only)
+  EXA_CUDA(clear(2));
+  EXA_CUDA(clear(5));
+  EXA_TRY(gemm(n1, n2, n1, 1.0, Xa, A12b, 0.0, nullptr, 0, 0, nullptr, 0, 0,
+               {UPackOut{W1a, 0, 1, 0}, UPackOut{W1b, 1, 1, 0}}));
+  // S = A22 - A21 W1, in place
+  EXA_TRY(gemm(n2, n2, n1, -1.0, A21a, W1b, 1.0, A22, n, stride, A22, n, stride, {}));
+  EXA_TRY(subcopy<float>(W2, n2, sw, A22, n, stride, n2, n2, batch, st));
+  EXA_TRY(inverse_dispatch<float>(W2, n2, sw, batch, d_flag, st));
+  EXA_TRY(exa_pack(W2, 0, 1, n2, sw, 0, batch, 1, Ya, st));
+  EXA_TRY(exa_pack(W2, 0, n2, 1, sw, 0, batch, 1, Yb, st));
+  // W3 = A21 X (packed as B only)
+  EXA_CUDA(clear(6));
+  EXA_TRY(gemm(n2, n1, n1, 1.0, A21a, Xb, 0.0, nullptr, 0, 0, nullptr, 0, 0, {UPackOut{W3b, 1, 1, 0}}));
+  // A12 = -W1 Y (and packed as A)
+  EXA_CUDA(clear(2));
+  EXA_TRY(gemm(n1, n2, n2, -1.0, W1a, Yb, 0.0, nullptr, 0, 0, A12, n, stride, {UPackOut{A12a, 0, 1, 0}}));
+  // A11 = X - A12 W3
+  EXA_TRY(gemm(n1, n1, n2, -1.0, A12a, W3b, 1.0, W0, n1, sw, A11, n, stride, {}));
+  // A21 = -Y W3
+  EXA_TRY(gemm(n2, n1, n2, -1.0, Ya, W3b, 0.0, nullptr, 0, 0, A21, n, stride, {}));
+  EXA_TRY(subcopy<float>(A22, n, stride, W2, n2, sw, n2, n2, batch, st));
+  return EXA_OK;
+}
 
 int exa_inverse_max_n() { return 2 * INV_MAX_N; }
 int exa_inverse_needs_ws(int n) { return n > INV_MAX_N; }

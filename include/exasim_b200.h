@@ -138,6 +138,11 @@ int exa_dgemm_batched(int M, int N, int K, double alpha, const double* A, long l
                       const double* B, long long ldb, long long sB, double beta, double* C, long long ldc,
                       long long sC, int batch, void* stream);
 int exa_dinverse_batched(double* A, int n, long long stride, int batch, int* info_dev, void* stream);
+/* FP32 counterpart of exa_dinverse_batched, the mixed-precision form's element inverse
+ * (an FP32 restatement of pblas.h:163 Inverse; the reference has FP64 only).  Above order 160
+ * the 2 x 2 block products run on the tcgen05 3xTF32 GEMM, with a temporary stream-ordered
+ * workspace.  *info_dev is set to 1 on a zero pivot and to 2 if a tensor-core wait ran out. */
+int exa_sinverse_batched(float* A, int n, long long stride, int batch, int* info_dev, void* stream);
 /* No counterpart in the reference.  Times the candidate CTA tiles of exa_dgemm_batched for
  * one M x N x K shape on `batch` (at most 512) scratch blocks, allocated stream-ordered on
  * `stream`, and keeps the fastest for this device and shape; *tile (may be NULL) gets its

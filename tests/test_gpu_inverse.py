@@ -40,6 +40,31 @@ def test_inverse_matches_lapack(lib, n):
     assert err < 1e-12, err
 
 
+@pytest.mark.parametrize("n", [25, 125, 160, 170, 201, 250, 320])
+def test_fp32_inverse_matches_lapack(lib, n):
+    """exa_sinverse_batched, the mixed form's FP32 inverse: register kernels up to 160, the
+    blocked form with 3xTF32 tensor-core products above (201 and 250 have halves that are
+    not multiples of 16, so the packed operands carry padding).  FP32 rounding of the input
+    and of the elimination: within 2e-5 of max |inverse| at cond ~ 1e2."""
+    import torch
+    rng = np.random.default_rng(1000 + n)
+    batch = 37
+    A = (rng.standard_normal((batch, n, n)) + np.eye(n) * (2.0 * np.sqrt(n))).astype(np.float32)
+    dev = torch.tensor(np.ascontiguousarray(np.transpose(A, (0, 2, 1))).ravel(), dtype=torch.float32, device="cuda")
+    flag = torch.zeros(1, dtype=torch.int32, device="cuda")
+    for _ in range(2):  # the second call reuses the stream-ordered workspace memory
+        d = dev.clone()
+        st = lib.exa_sinverse_batched(ctypes.c_void_p(d.data_ptr()), n, n * n, batch,
+                                      ctypes.c_void_p(flag.data_ptr()), None)
+        assert st == 0, lib.exa_last_error().decode()
+        torch.cuda.synchronize()
+        assert int(flag.item()) == 0
+        got = np.transpose(d.cpu().numpy().reshape(batch, n, n), (0, 2, 1)).astype(np.float64)
+        ref = np.linalg.inv(A.astype(np.float64))
+        err = np.abs(got - ref).max() / np.abs(ref).max()
+        assert err < 2e-5, err
+
+
 @pytest.mark.parametrize("n", [8, 125])
 def test_singular_block_sets_flag(lib, n):
     import torch
