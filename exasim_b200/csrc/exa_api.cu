@@ -516,7 +516,10 @@ int exa_ctx_set_precision(ExaCtx& c, int mode) {
     EXA_TRY(dev_alloc(c, &c.F32, ne * n * m));
     EXA_TRY(dev_alloc(c, &c.K32, ne * m * n));
     EXA_TRY(dev_alloc(c, &c.Dinv32, ne * n * n));
-    if (exa_inverse_needs_ws((int)n)) EXA_TRY(dev_alloc(c, &c.wInvPk, nb * (size_t)exa_inverse_tc32_pk((int)n)));
+    if (exa_inverse_tc32_pk((int)n) > 0) {
+      EXA_TRY(dev_alloc(c, &c.wInv32, nb * (size_t)exa_inverse_tc32_ws((int)n)));
+      EXA_TRY(dev_alloc(c, &c.wInvPk, nb * (size_t)exa_inverse_tc32_pk((int)n)));
+    }
     if (c.preconditioner == 0)
       EXA_TRY(dev_alloc(c, &c.Pc32, (size_t)P.ncu * P.npf * P.ncu * P.npf * P.nf));
     else if (c.preconditioner == 2)
@@ -1056,14 +1059,14 @@ extern "C" int exa_dgemm_tune(int M, int N, int K, int batch, void* stream, int*
 }
 
 extern "C" int exa_sinverse_batched(float* A, int n, long long stride, int batch, int* info_dev, void* stream) {
-  if (!exa_inverse_needs_ws(n) || batch <= 0) return exa_inverse(A, n, stride, batch, info_dev, (cudaStream_t)stream);
+  if (exa_inverse_tc32_pk(n) == 0 || batch <= 0) return exa_inverse(A, n, stride, batch, info_dev, (cudaStream_t)stream);
   if (n > exa_inverse_max_n()) {
     exa_set_error("dense inverse of order %d exceeds %d", n, exa_inverse_max_n());
     return EXA_ERR_UNSUPPORTED;
   }
-  // n^2 floats of blocks and the packed operands per matrix, freed after the stream drains
+  // the blocks of every level and the packed operands per matrix, freed after the stream drains
   cudaStream_t st = (cudaStream_t)stream;
-  const size_t nblk = ((size_t)n * n * batch + 63) / 64 * 64;  // packed operands start 256-byte aligned
+  const size_t nblk = ((size_t)exa_inverse_tc32_ws(n) * batch + 63) / 64 * 64;  // packed operands start 256-byte aligned
   float* ws = nullptr;
   EXA_CUDA(cudaMallocAsync((void**)&ws, sizeof(float) * (nblk + (size_t)exa_inverse_tc32_pk(n) * batch), st));
   const int s = exa_inverse_tc32(A, n, stride, batch, ws, ws + nblk, info_dev, info_dev, st);

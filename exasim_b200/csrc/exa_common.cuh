@@ -101,9 +101,11 @@ int exa_inverse_max_n();
 int exa_inverse_needs_ws(int n);
 int exa_inverse_ws(double* A, int n, long long stride, int batch, double* ws, int* d_flag, cudaStream_t st);
 int exa_inverse_ws(float* A, int n, long long stride, int batch, float* ws, int* d_flag, cudaStream_t st);
-// FP32 blocks of order up to exa_inverse_max_n() with the blocked form's products on the
-// tcgen05 3xTF32 GEMM: ws holds n^2 floats and pk exa_inverse_tc32_pk(n) floats per matrix;
-// *uflag reports a tensor-core wait that ran out.
+// FP32 blocks of order up to exa_inverse_max_n(): above the register kernel's limit by the
+// blocked form applied recursively, its products on the tcgen05 3xTF32 GEMM.  ws holds
+// exa_inverse_tc32_ws(n) floats and pk exa_inverse_tc32_pk(n) floats per matrix (both 0 for
+// orders the register kernel takes whole); *uflag reports a tensor-core wait that ran out.
+long long exa_inverse_tc32_ws(int n);
 long long exa_inverse_tc32_pk(int n);
 int exa_inverse_tc32(float* A, int n, long long stride, int batch, float* ws, float* pk, int* d_flag, int* uflag,
                      cudaStream_t st);

@@ -178,82 +178,6 @@ __global__ void scatter_kernel(ExaDims P, const int* f2e, const int* elemcon, co
   }
 }
 
-// we_e = A_e * gather(v), A_e = H (matvec) or the additive-Schwarz inverse blocks
-// we_e = A_e ve_e per element, ve_e gathered from v through elemcon.  8 warps split the
-// columns (warp w takes c = w, w + 8, ...); lane l keeps the partial sums of rows
-// l + 32 i (i < RI) in registers, so every column is one coalesced load per 32 rows and
-// each thread has RI x 4 independent loads in flight; the 8 partials meet in shared memory.
-template <typename T, int RI>
-__global__ void __launch_bounds__(256) elem_matvec_kernel(ExaDims P, const int* elemcon, const T* A, const double* v,
-                                                          double* we) {
-  extern __shared__ double sm[];
-  double* ve = sm;             // [m]
-  double* part = sm + P.m;     // [8][m]
-  const int e = blockIdx.x, m = P.m, ncu = P.ncu;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const T* Ae = A + (long long)e * m * m;
-  // four columns (c, c + 8, c + 16, c + 24) per step: 4 RI independent loads per thread; the
-  // next step's columns are loaded while this step's are used, and the first step's before
-  // the gather of the element's trace values
-  auto load4 = [&](int c0, T (&y)[4][RI]) {
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      const T* a = Ae + (long long)m * (c0 + 8 * u);
-#pragma unroll
-      for (int i = 0; i < RI; ++i) {
-        const int r = lane + 32 * i;
-        y[u][i] = r < m ? a[r] : T(0);
-      }
-    }
-  };
-  int c = warp;
-  T y[4][RI];
-  if (c + 24 < m) load4(c, y);
-  for (int r = threadIdx.x; r < m; r += blockDim.x) ve[r] = v[r % ncu + ncu * (long long)elemcon[r / ncu + P.ndf * e]];
-  __syncthreads();
-  double acc[RI];
-#pragma unroll
-  for (int i = 0; i < RI; ++i) acc[i] = 0.0;
-  for (; c + 24 < m; c += 32) {
-    T yn[4][RI];
-    const bool more = c + 56 < m;
-    if (more) load4(c + 32, yn);
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      const double x = ve[c + 8 * u];
-#pragma unroll
-      for (int i = 0; i < RI; ++i) acc[i] = fma((double)y[u][i], x, acc[i]);
-    }
-    if (more) {
-#pragma unroll
-      for (int u = 0; u < 4; ++u)
-#pragma unroll
-        for (int i = 0; i < RI; ++i) y[u][i] = yn[u][i];
-    }
-  }
-  for (; c < m; c += 8) {
-    const T* a0 = Ae + (long long)m * c;
-    const double x0 = ve[c];
-#pragma unroll
-    for (int i = 0; i < RI; ++i) {
-      const int r = lane + 32 * i;
-      if (r < m) acc[i] = fma((double)a0[r], x0, acc[i]);
-    }
-  }
-#pragma unroll
-  for (int i = 0; i < RI; ++i) {
-    const int r = lane + 32 * i;
-    if (r < m) part[warp * m + r] = acc[i];
-  }
-  __syncthreads();
-  for (int r = threadIdx.x; r < m; r += blockDim.x) {
-    double s = 0.0;
-#pragma unroll
-    for (int w = 0; w < 8; ++w) s += part[w * m + r];
-    we[(long long)e * m + r] = s;
-  }
-}
-
 template <typename T>
 __global__ void bj_build_kernel(ExaDims P, const int* f2e, const int* elemcon, const T* H, T* BE) {
   const int ncu = P.ncu, npf = P.npf, ncf = ncu * npf, m = P.m;
@@ -314,57 +238,75 @@ __global__ void bj_apply_kernel(ExaDims P, const T* BE, const double* x, double*
 
 // y_e = alpha A_e x_e + beta y0_e for a batch of column-major M x K blocks A_e (leading
 // dimension M, batch stride sA; y0 may alias y).  x_e is read at x + e sx, or, with elemcon,
-// gathered from a trace vector: x_e[k] = x[k % ncu + ncu elemcon[k / ncu + ndf e]].  The
-// scheme of elem_matvec_kernel: 8 warps split the columns four at a time with the next four
-// loaded ahead, lane l keeps rows l + 32 i (i < RI) in registers, and a row's 8 partial sums
-// meet in shared memory in a fixed order.  Serves du = Ru + D^-1 F x (hdgGetDUDG,
-// matvec.cpp:219-238) and the mixed form's Ru <- D^-1 Ru, Rh <- Rh - K Ru.
-template <typename T, int RI>
+// gathered from a trace vector: x_e[k] = x[k % ncu + ncu elemcon[k / ncu + ndf e]].  One
+// CTA per block: 8 warps split the columns (warp w takes c = w, w + 8, ...), CU at a time
+// with the next CU loaded ahead (CU = 2 where 4 would not fit the registers); lane l keeps the partial sums of rows V l + 32 V i + v
+// (i < RI, v < V) in registers, so each column is one coalesced load per 32 V rows (V = 2:
+// pairs of floats, as many bytes per load as FP64); the 8 partial sums of a row meet in
+// shared memory in a fixed order.  Serves the condensed matvec w_e = H_e gather(v)
+// (hdgMatVec, matvec.cpp:240-389) and the additive-Schwarz apply, du = Ru + D^-1 F x
+// (hdgGetDUDG, matvec.cpp:219-238) and the mixed form's Ru <- D^-1 Ru, Rh <- Rh - K Ru.
+template <typename T, int RI, int V, int CU>
 __global__ void __launch_bounds__(256) bgemv_kernel(int M, int K, const T* A, long long sA, const double* x,
                                                     long long sx, const int* elemcon, int ndf, int ncu,
                                                     double alpha, double beta, const double* y0, double* y,
                                                     long long sy) {
+  static_assert(V == 1 || (V == 2 && sizeof(T) == 4), "pairs of floats only");
   extern __shared__ double sm[];
   double* xe = sm;         // [K]
   double* part = sm + K;   // [8][M]
   const long long e = blockIdx.x;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const T* Ae = A + e * sA;
-  auto load4 = [&](int c0, T (&v)[4][RI]) {
+  // rows V (lane + 32 i) .. + V - 1 of column c0 + 8 u; with V = 2, M is even, so a pair is
+  // either inside the block or past it, and 8-byte aligned
+  auto loadc = [&](int c0, T (&v)[CU][RI][V]) {
 #pragma unroll
-    for (int u = 0; u < 4; ++u) {
+    for (int u = 0; u < CU; ++u) {
       const T* a = Ae + (long long)M * (c0 + 8 * u);
 #pragma unroll
       for (int i = 0; i < RI; ++i) {
-        const int r = lane + 32 * i;
-        v[u][i] = r < M ? a[r] : T(0);
+        const int r = V * (lane + 32 * i);
+        if constexpr (V == 2) {
+          const float2 t = r < M ? *reinterpret_cast<const float2*>(a + r) : make_float2(0.f, 0.f);
+          v[u][i][0] = t.x;
+          v[u][i][1] = t.y;
+        } else {
+          v[u][i][0] = r < M ? a[r] : T(0);
+        }
       }
     }
   };
   int c = warp;
-  T a[4][RI];
-  if (c + 24 < K) load4(c, a);
+  T a[CU][RI][V];
+  if (c + 8 * (CU - 1) < K) loadc(c, a);
   for (int k = threadIdx.x; k < K; k += blockDim.x)
     xe[k] = elemcon ? x[k % ncu + ncu * (long long)elemcon[k / ncu + (long long)ndf * e]] : x[e * sx + k];
   __syncthreads();
-  double acc[RI];
+  double acc[RI][V];
 #pragma unroll
-  for (int i = 0; i < RI; ++i) acc[i] = 0.0;
-  for (; c + 24 < K; c += 32) {
-    T an[4][RI];
-    const bool more = c + 56 < K;
-    if (more) load4(c + 32, an);
+  for (int i = 0; i < RI; ++i)
 #pragma unroll
-    for (int u = 0; u < 4; ++u) {
+    for (int w = 0; w < V; ++w) acc[i][w] = 0.0;
+  for (; c + 8 * (CU - 1) < K; c += 8 * CU) {
+    T an[CU][RI][V];
+    const bool more = c + 8 * CU + 8 * (CU - 1) < K;
+    if (more) loadc(c + 8 * CU, an);
+#pragma unroll
+    for (int u = 0; u < CU; ++u) {
       const double xv = xe[c + 8 * u];
 #pragma unroll
-      for (int i = 0; i < RI; ++i) acc[i] = fma((double)a[u][i], xv, acc[i]);
+      for (int i = 0; i < RI; ++i)
+#pragma unroll
+        for (int w = 0; w < V; ++w) acc[i][w] = fma((double)a[u][i][w], xv, acc[i][w]);
     }
     if (more) {
 #pragma unroll
-      for (int u = 0; u < 4; ++u)
+      for (int u = 0; u < CU; ++u)
 #pragma unroll
-        for (int i = 0; i < RI; ++i) a[u][i] = an[u][i];
+        for (int i = 0; i < RI; ++i)
+#pragma unroll
+          for (int w = 0; w < V; ++w) a[u][i][w] = an[u][i][w];
     }
   }
   for (; c < K; c += 8) {
@@ -372,15 +314,20 @@ __global__ void __launch_bounds__(256) bgemv_kernel(int M, int K, const T* A, lo
     const double xv = xe[c];
 #pragma unroll
     for (int i = 0; i < RI; ++i) {
-      const int r = lane + 32 * i;
-      if (r < M) acc[i] = fma((double)a0[r], xv, acc[i]);
+      const int r = V * (lane + 32 * i);
+      if (r < M) {
+#pragma unroll
+        for (int w = 0; w < V; ++w) acc[i][w] = fma((double)a0[r + w], xv, acc[i][w]);
+      }
     }
   }
 #pragma unroll
-  for (int i = 0; i < RI; ++i) {
-    const int r = lane + 32 * i;
-    if (r < M) part[warp * M + r] = acc[i];
-  }
+  for (int i = 0; i < RI; ++i)
+#pragma unroll
+    for (int w = 0; w < V; ++w) {
+      const int r = V * (lane + 32 * i) + w;
+      if (r < M) part[warp * M + r] = acc[i][w];
+    }
   __syncthreads();
   for (int r = threadIdx.x; r < M; r += blockDim.x) {
     double s = 0.0;
@@ -401,19 +348,34 @@ int launch_bgemv(int M, int K, int batch, const T* A, long long sA, const double
     return EXA_ERR_UNSUPPORTED;
   }
   const size_t smem = sizeof(double) * ((size_t)(K > 0 ? K : 1) + 8 * (size_t)M);
-  const int ri = (M + 31) / 32;
-#define EXA_BGEMV(R)                                                                                          \
-  bgemv_kernel<T, R><<<batch, 256, smem, st>>>(M, K, A, sA, x, sx, elemcon, ndf, ncu, alpha, beta, y0, y, sy)
-  if (ri <= 1) EXA_BGEMV(1);
-  else if (ri <= 2) EXA_BGEMV(2);
-  else if (ri <= 3) EXA_BGEMV(3);
-  else if (ri <= 4) EXA_BGEMV(4);
-  else if (ri <= 5) EXA_BGEMV(5);
-  else if (ri <= 6) EXA_BGEMV(6);
-  else if (ri <= 8) EXA_BGEMV(8);
-  else if (ri <= 10) EXA_BGEMV(10);
-  else if (ri <= 12) EXA_BGEMV(12);
-  else EXA_BGEMV(16);
+#define EXA_BGEMV(R, V)                                                                                     \
+  bgemv_kernel<T, R, V, (sizeof(T) == 8 && R > 12) ? 2 : 4>                                                   \
+      <<<batch, 256, smem, st>>>(M, K, A, sA, x, sx, elemcon, ndf, ncu, alpha, beta, y0, y, sy)
+  if (sizeof(T) == 4 && M % 2 == 0) {
+    if constexpr (sizeof(T) == 4) {
+      // pairs of rows per lane: ceil(M / 64) pairs
+      const int ri = (M + 63) / 64;
+      if (ri <= 1) EXA_BGEMV(1, 2);
+      else if (ri <= 2) EXA_BGEMV(2, 2);
+      else if (ri <= 3) EXA_BGEMV(3, 2);
+      else if (ri <= 4) EXA_BGEMV(4, 2);
+      else if (ri <= 5) EXA_BGEMV(5, 2);
+      else if (ri <= 6) EXA_BGEMV(6, 2);
+      else EXA_BGEMV(8, 2);
+    }
+  } else {
+    const int ri = (M + 31) / 32;
+    if (ri <= 1) EXA_BGEMV(1, 1);
+    else if (ri <= 2) EXA_BGEMV(2, 1);
+    else if (ri <= 3) EXA_BGEMV(3, 1);
+    else if (ri <= 4) EXA_BGEMV(4, 1);
+    else if (ri <= 5) EXA_BGEMV(5, 1);
+    else if (ri <= 6) EXA_BGEMV(6, 1);
+    else if (ri <= 8) EXA_BGEMV(8, 1);
+    else if (ri <= 10) EXA_BGEMV(10, 1);
+    else if (ri <= 12) EXA_BGEMV(12, 1);
+    else EXA_BGEMV(16, 1);
+  }
 #undef EXA_BGEMV
   EXA_LAUNCH_CHECK();
   return EXA_OK;
@@ -578,22 +540,9 @@ int exa_k_scatter(const ExaDims& P, const int* f2e, const int* elemcon, const do
 template <typename T>
 int exa_k_elem_matvec(const ExaDims& P, const int* elemcon, const T* A, const double* v, double* we,
                       cudaStream_t st) {
-  const size_t smem = sizeof(double) * (size_t)P.m * 9;
-  // rows per lane: exactly ceil(m / 32) up to 6, so no register holds a row past m
-  if (P.m <= 32) elem_matvec_kernel<T, 1><<<P.ne, 256, smem, st>>>(P, elemcon, A, v, we);
-  else if (P.m <= 64) elem_matvec_kernel<T, 2><<<P.ne, 256, smem, st>>>(P, elemcon, A, v, we);
-  else if (P.m <= 96) elem_matvec_kernel<T, 3><<<P.ne, 256, smem, st>>>(P, elemcon, A, v, we);
-  else if (P.m <= 128) elem_matvec_kernel<T, 4><<<P.ne, 256, smem, st>>>(P, elemcon, A, v, we);
-  else if (P.m <= 160) elem_matvec_kernel<T, 5><<<P.ne, 256, smem, st>>>(P, elemcon, A, v, we);
-  else if (P.m <= 192) elem_matvec_kernel<T, 6><<<P.ne, 256, smem, st>>>(P, elemcon, A, v, we);
-  else if (P.m <= 256) elem_matvec_kernel<T, 8><<<P.ne, 256, smem, st>>>(P, elemcon, A, v, we);
-  else if (P.m <= 512) elem_matvec_kernel<T, 16><<<P.ne, 256, smem, st>>>(P, elemcon, A, v, we);
-  else {
-    exa_set_error("matvec: trace block of %d rows exceeds 512", P.m);
-    return EXA_ERR_UNSUPPORTED;
-  }
-  EXA_LAUNCH_CHECK();
-  return EXA_OK;
+  // we_e = A_e gather(v): A_e = H (matvec) or the additive-Schwarz inverse blocks
+  return launch_bgemv<T>(P.m, P.m, P.ne, A, (long long)P.m * P.m, v, 0, elemcon, P.ndf, P.ncu, 1.0, 0.0, nullptr, we,
+                         P.m, st);
 }
 
 template <typename T>

@@ -735,48 +735,60 @@ int inverse_ws(T* A, int n, long long stride, int batch, T* ws, int* d_flag, cud
 
 // ----------------------------------------------------------------------------------
 // The same 2 x 2 block inverse for FP32 blocks with the five products on the tcgen05
-// 3xTF32 GEMM (the mixed-precision form).  With X = A11^-1 and Y = S^-1:
+// 3xTF32 GEMM (the mixed-precision form), for orders above the register kernel's limit,
+// applied recursively: the two diagonal inverses are themselves blocked until their order
+// is at most INV_TC_LEAF, where the register kernel takes over.  At order 320 (3D Euler,
+// p = 3) leaves of 80 (two levels) took 134 ms per solve of 32^3 elements against 161 ms
+// for leaves of 160 and 168 ms for leaves of 40; at 125 the register kernel alone beat one
+// level with leaves of 63 (2.6 against 2.8 ms for 4096 blocks).  With
+// X = A11^-1 and Y = S^-1:
 //   W1 = X A12, S = A22 - A21 W1, W3 = A21 X,
 //   A12 <- -W1 Y, A11 <- X - A12 W3, A21 <- -Y W3, A22 <- Y.
 // W1 and W3 exist only packed: the products that make them write their packed copies
-// (A and B operand layouts) from the epilogue.  The packed operands live in pk: seven
-// slots of hi and lo parts, per matrix; X as A and A12 as B are dead once W1 exists, and
-// W1 as B once S does, so Y (A and B) and the new A12 (A) take their slots.
+// (A and B operand layouts) from the epilogue.  Per level the packed operands take seven
+// slots of hi and lo parts per matrix; X as A and A12 as B are dead once W1 exists, and
+// W1 as B once S does, so Y (A and B) and the new A12 (A) take their slots.  Per matrix,
+// level L keeps X and Y (n1^2 + n2^2 floats) and its slots in ws and pk after those of the
+// levels above it; the two inner inversions of a level run one after the other and share
+// the next level's space.
 // ----------------------------------------------------------------------------------
 namespace {
+constexpr int INV_TC_LEAF = 96;
+
 long long inv_tc_slot(int n) {
   const int n1 = (n + 1) / 2;
-  return exa_pack_size(n1, n1);  // every operand has at most n1 rows and n1 k
+  return exa_pack_size(n1, n1);  // every operand of a level has at most n1 rows and n1 k
 }
-}  // namespace
 
-long long exa_inverse_tc32_pk(int n) { return n > INV_MAX_N ? 14 * inv_tc_slot(n) : 0; }
+long long inv_tc_ws(int n) {
+  if (n <= INV_TC_LEAF) return 0;
+  const long long n1 = (n + 1) / 2, n2 = n - n1;
+  return n1 * n1 + n2 * n2 + inv_tc_ws((int)n1);
+}
 
-int exa_inverse_tc32(float* A, int n, long long stride, int batch, float* ws, float* pk, int* d_flag, int* uflag,
-                     cudaStream_t st) {
-  if (n <= INV_MAX_N || batch <= 0) return inverse_dispatch<float>(A, n, stride, batch, d_flag, st);
-  if (n > 2 * INV_MAX_N) {
-    exa_set_error("dense inverse of order %d exceeds the blocked kernel limit %d", n, 2 * INV_MAX_N);
-    return EXA_ERR_UNSUPPORTED;
-  }
-  if (!ws || !pk) {
-    exa_set_error("tensor-core inverse of order %d needs workspaces", n);
-    return EXA_ERR_ARG;
-  }
+long long inv_tc_pk(int n) { return n <= INV_TC_LEAF ? 0 : 14 * inv_tc_slot(n) + inv_tc_pk((n + 1) / 2); }
+
+// A: batch n x n blocks (leading dimension n) `stride` floats apart; ws and pk: this level's
+// part of the workspaces, wstride and pstride floats per matrix
+int inverse_tc32_level(float* A, int n, long long stride, int batch, float* ws, long long wstride, float* pk,
+                       long long pstride, int* d_flag, int* uflag, cudaStream_t st) {
+  if (n <= INV_TC_LEAF) return inverse_dispatch<float>(A, n, stride, batch, d_flag, st);
   const int n1 = (n + 1) / 2, n2 = n - n1;
-  const long long sw = (long long)n * n, S = inv_tc_slot(n), spk = exa_inverse_tc32_pk(n);
+  const long long S = inv_tc_slot(n);
   float* W0 = ws;                       // n1 x n1: A11, then X
   float* W2 = W0 + (long long)n1 * n1;  // n2 x n2: S, then Y
+  float* wsi = W2 + (long long)n2 * n2;  // the inner levels
+  float* pki = pk + 14 * S;
   float* A11 = A;
   float* A21 = A + n1;
   float* A12 = A + (long long)n * n1;
   float* A22 = A + n1 + (long long)n * n1;
-  // slot k: hi at pk + 2kS, lo at pk + (2k+1)S, per matrix stride spk
+  // slot k: hi at pk + 2kS, lo at pk + (2k+1)S
   auto op = [&](int k, int R, int K, bool as_b) {
     UPacked u{};
     u.hi = pk + 2LL * k * S;
     u.lo = u.hi + S;
-    u.sb = spk;
+    u.sb = pstride;
     u.sb2 = 0;
     u.R = R;
     u.K = K;
@@ -806,13 +818,13 @@ int exa_inverse_tc32(float* A, int n, long long stride, int batch, float* ws, fl
   const bool padded = (n1 % 16) != 0 || (n2 % 16) != 0;
   auto clear = [&](int k) -> cudaError_t {
     if (!padded) return cudaSuccess;
-    return cudaMemset2DAsync(pk + 2LL * k * S, sizeof(float) * (size_t)spk, 0, sizeof(float) * 2 * (size_t)S,
+    return cudaMemset2DAsync(pk + 2LL * k * S, sizeof(float) * (size_t)pstride, 0, sizeof(float) * 2 * (size_t)S,
                              (size_t)batch, st);
   };
-  EXA_TRY(subcopy<float>(W0, n1, sw, A11, n, stride, n1, n1, batch, st));
-  EXA_TRY(inverse_dispatch<float>(W0, n1, sw, batch, d_flag, st));
-  EXA_TRY(exa_pack(W0, 0, 1, n1, sw, 0, batch, 1, Xa, st));
-  EXA_TRY(exa_pack(W0, 0, n1, 1, sw, 0, batch, 1, Xb, st));
+  EXA_TRY(subcopy<float>(W0, n1, wstride, A11, n, stride, n1, n1, batch, st));
+  EXA_TRY(inverse_tc32_level(W0, n1, wstride, batch, wsi, wstride, pki, pstride, d_flag, uflag, st));
+  EXA_TRY(exa_pack(W0, 0, 1, n1, wstride, 0, batch, 1, Xa, st));
+  EXA_TRY(exa_pack(W0, 0, n1, 1, wstride, 0, batch, 1, Xb, st));
   EXA_TRY(exa_pack(A12, 0, n, 1, stride, 0, batch, 1, A12b, st));
   EXA_TRY(exa_pack(A21, 0, 1, n, stride, 0, batch, 1, A21a, st));
   // W1 = X A12 (packed as A and as B only)
@@ -822,10 +834,10 @@ int exa_inverse_tc32(float* A, int n, long long stride, int batch, float* ws, fl
                {UPackOut{W1a, 0, 1, 0}, UPackOut{W1b, 1, 1, 0}}));
   // S = A22 - A21 W1, in place
   EXA_TRY(gemm(n2, n2, n1, -1.0, A21a, W1b, 1.0, A22, n, stride, A22, n, stride, {}));
-  EXA_TRY(subcopy<float>(W2, n2, sw, A22, n, stride, n2, n2, batch, st));
-  EXA_TRY(inverse_dispatch<float>(W2, n2, sw, batch, d_flag, st));
-  EXA_TRY(exa_pack(W2, 0, 1, n2, sw, 0, batch, 1, Ya, st));
-  EXA_TRY(exa_pack(W2, 0, n2, 1, sw, 0, batch, 1, Yb, st));
+  EXA_TRY(subcopy<float>(W2, n2, wstride, A22, n, stride, n2, n2, batch, st));
+  EXA_TRY(inverse_tc32_level(W2, n2, wstride, batch, wsi, wstride, pki, pstride, d_flag, uflag, st));
+  EXA_TRY(exa_pack(W2, 0, 1, n2, wstride, 0, batch, 1, Ya, st));
+  EXA_TRY(exa_pack(W2, 0, n2, 1, wstride, 0, batch, 1, Yb, st));
   // W3 = A21 X (packed as B only)
   EXA_CUDA(clear(6));
   EXA_TRY(gemm(n2, n1, n1, 1.0, A21a, Xb, 0.0, nullptr, 0, 0, nullptr, 0, 0, {UPackOut{W3b, 1, 1, 0}}));
@@ -833,11 +845,29 @@ int exa_inverse_tc32(float* A, int n, long long stride, int batch, float* ws, fl
   EXA_CUDA(clear(2));
   EXA_TRY(gemm(n1, n2, n2, -1.0, W1a, Yb, 0.0, nullptr, 0, 0, A12, n, stride, {UPackOut{A12a, 0, 1, 0}}));
   // A11 = X - A12 W3
-  EXA_TRY(gemm(n1, n1, n2, -1.0, A12a, W3b, 1.0, W0, n1, sw, A11, n, stride, {}));
+  EXA_TRY(gemm(n1, n1, n2, -1.0, A12a, W3b, 1.0, W0, n1, wstride, A11, n, stride, {}));
   // A21 = -Y W3
   EXA_TRY(gemm(n2, n1, n2, -1.0, Ya, W3b, 0.0, nullptr, 0, 0, A21, n, stride, {}));
-  EXA_TRY(subcopy<float>(A22, n, stride, W2, n2, sw, n2, n2, batch, st));
+  EXA_TRY(subcopy<float>(A22, n, stride, W2, n2, wstride, n2, n2, batch, st));
   return EXA_OK;
+}
+}  // namespace
+
+long long exa_inverse_tc32_ws(int n) { return n <= INV_MAX_N ? 0 : inv_tc_ws(n); }
+long long exa_inverse_tc32_pk(int n) { return n <= INV_MAX_N ? 0 : inv_tc_pk(n); }
+
+int exa_inverse_tc32(float* A, int n, long long stride, int batch, float* ws, float* pk, int* d_flag, int* uflag,
+                     cudaStream_t st) {
+  if (n <= INV_MAX_N || batch <= 0) return inverse_dispatch<float>(A, n, stride, batch, d_flag, st);
+  if (n > 2 * INV_MAX_N) {
+    exa_set_error("dense inverse of order %d exceeds the blocked kernel limit %d", n, 2 * INV_MAX_N);
+    return EXA_ERR_UNSUPPORTED;
+  }
+  if (!ws || !pk) {
+    exa_set_error("tensor-core inverse of order %d needs workspaces", n);
+    return EXA_ERR_ARG;
+  }
+  return inverse_tc32_level(A, n, stride, batch, ws, inv_tc_ws(n), pk, inv_tc_pk(n), d_flag, uflag, st);
 }
 
 int exa_inverse_max_n() { return 2 * INV_MAX_N; }

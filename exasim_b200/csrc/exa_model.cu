@@ -184,11 +184,10 @@ int schur_chunk_mixed(ExaCtx& c, int e0, int nb) {
   }
   {
     ExaProfScope ps(c, EXA_PH_INVERSE);
-    // blocks above order 160 go blockwise, with the chunk's inverse workspace (n^2 doubles per
-    // element, so room for n^2 floats) and the block products on the tensor cores
+    // the recursive blocked form with its products on the tensor cores where the order
+    // exceeds its leaf size, else the register kernel (exa_inverse_ws takes it whole)
     if (c.wInvPk)
-      EXA_TRY(exa_inverse_tc32(D32, n, (long long)n * n, nb, reinterpret_cast<float*>(c.wInv), c.wInvPk, c.d_flag,
-                               c.d_uflag, c.st));
+      EXA_TRY(exa_inverse_tc32(D32, n, (long long)n * n, nb, c.wInv32, c.wInvPk, c.d_flag, c.d_uflag, c.st));
     else
       EXA_TRY(exa_inverse_ws(D32, n, (long long)n * n, nb, reinterpret_cast<float*>(c.wInv), c.d_flag, c.st));
   }

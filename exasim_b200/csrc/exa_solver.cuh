@@ -96,7 +96,8 @@ struct ExaCtx {
   int mixed_maxit = 30;           // refinement steps per mixed solve
   float *H32 = nullptr, *F32 = nullptr, *K32 = nullptr;    // condensed block, D^-1 F, K
   float *Dinv32 = nullptr, *Pc32 = nullptr;
-  float* wInvPk = nullptr;  // packed operands of the tensor-core blocked inverse (orders above 160), per chunk
+  // blocks and packed operands of the recursive tensor-core inverse, per element chunk
+  float *wInv32 = nullptr, *wInvPk = nullptr;
   int* d_uflag = nullptr;         // tensor-core kernel wait flag
   // operands of the 3xTF32 products, packed in the tensor-core layout (hi and lo parts):
   // Minv C, Minv E as B operands (all elements); per element chunk: B and G (A operands of

@@ -43,9 +43,10 @@ def test_inverse_matches_lapack(lib, n):
 @pytest.mark.parametrize("n", [25, 125, 160, 170, 201, 250, 320])
 def test_fp32_inverse_matches_lapack(lib, n):
     """exa_sinverse_batched, the mixed form's FP32 inverse: register kernels up to 160, the
-    blocked form with 3xTF32 tensor-core products above (201 and 250 have halves that are
-    not multiples of 16, so the packed operands carry padding).  FP32 rounding of the input
-    and of the elimination: within 2e-5 of max |inverse| at cond ~ 1e2."""
+    recursive blocked form with 3xTF32 tensor-core products above (one level at 170, two at
+    201, 250 and 320; 170, 201 and 250 have halves that are not multiples of 16, so the
+    packed operands carry padding).  FP32 rounding of the input and of the elimination:
+    within 2e-5 of max |inverse| at cond ~ 1e2."""
     import torch
     rng = np.random.default_rng(1000 + n)
     batch = 37
