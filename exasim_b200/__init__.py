@@ -232,7 +232,7 @@ class HDGSolver:
         return a.value, b.value
 
     PHASES = ("volume", "face", "qelim", "inverse", "schur", "precond_build", "matvec", "precond_apply",
-              "orthogonalize", "getq", "residual", "pack")
+              "orthogonalize", "getq", "residual", "pack", "update")
 
     def profile(self, enable: bool):
         """Start (resetting the totals) or stop the per-phase device timers."""

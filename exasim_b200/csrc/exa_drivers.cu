@@ -482,10 +482,13 @@ int exa_drv_newton(ExaCtx& c, int* iters_out, double* norm_out) {
     c.last_gmres_relerr = ge;
     c.total_gmres_iters += gi;
     double alpha = 1.0;
-    // u += alpha x; uhat = u; du = Ru + DinvF x; udg(u) += alpha du
-    EXA_TRY(exa_axpby(c.uh, c.x, alpha, 1.0, N, c.st));
-    EXA_TRY(exa_k_dudg(P, c.elemcon, c.F, c.Ru, c.x, c.du, c.st));
-    EXA_TRY(exa_k_udg_update(P, c.udg, c.du, alpha, c.st));
+    {
+      // u += alpha x; uhat = u; du = Ru + DinvF x; udg(u) += alpha du
+      ExaProfScope ps(c, EXA_PH_UPDATE);
+      EXA_TRY(exa_axpby(c.uh, c.x, alpha, 1.0, N, c.st));
+      EXA_TRY(exa_k_dudg(P, c.elemcon, c.F, c.Ru, c.x, c.du, c.st));
+      EXA_TRY(exa_k_udg_update(P, c.udg, c.du, alpha, c.st));
+    }
     EXA_TRY(exa_drv_getq(c));
     const double nrm0 = nrmr;
     EXA_TRY(exa_drv_residual(c, &nrmr));
@@ -530,6 +533,7 @@ int exa_drv_newton(ExaCtx& c, int* iters_out, double* norm_out) {
 int exa_drv_condense_mixed(ExaCtx& c) {
   const ExaDims& P = c.P;
   const int n = P.n, m = P.m;
+  ExaProfScope ps(c, EXA_PH_UPDATE);
   // in element chunks of the assembly's workspace (c.wRu holds neb element vectors)
   for (int e0 = 0; e0 < P.ne; e0 += c.neb) {
     const int nb = std::min(c.neb, P.ne - e0);
@@ -584,10 +588,13 @@ int exa_drv_newton_mixed(ExaCtx& c, int* iters_out, double* norm_out) {
     c.last_gmres_iters = gi;
     c.last_gmres_relerr = ge;
     c.total_gmres_iters += gi;
-    EXA_TRY(exa_axpby(c.uh, c.x, 1.0, 1.0, N, c.st));
-    EXA_TRY(exa_k_dudg(P, c.elemcon, c.F32, c.Ru, c.x, c.du, c.st));
-    EXA_TRY(exa_k_udg_update(P, c.udg, c.du, 1.0, c.st));
-    if (c.RBdim > 0) EXA_TRY(rb_update(c, 1.0));
+    {
+      ExaProfScope ps(c, EXA_PH_UPDATE);
+      EXA_TRY(exa_axpby(c.uh, c.x, 1.0, 1.0, N, c.st));
+      EXA_TRY(exa_k_dudg(P, c.elemcon, c.F32, c.Ru, c.x, c.du, c.st));
+      EXA_TRY(exa_k_udg_update(P, c.udg, c.du, 1.0, c.st));
+      if (c.RBdim > 0) EXA_TRY(rb_update(c, 1.0));
+    }
     EXA_TRY(exa_drv_getq(c));
     EXA_TRY(exa_drv_residual(c, &nrmr));
     c.last_newton_iters = it + 1;

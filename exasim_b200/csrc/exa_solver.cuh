@@ -16,7 +16,8 @@
 // pairs recorded on the context stream around each phase, summed when read.
 enum ExaPhase {
   EXA_PH_VOLUME = 0, EXA_PH_FACE, EXA_PH_QELIM, EXA_PH_INVERSE, EXA_PH_SCHUR, EXA_PH_PRECOND_BUILD,
-  EXA_PH_MATVEC, EXA_PH_PRECOND_APPLY, EXA_PH_ORTHO, EXA_PH_GETQ, EXA_PH_RESIDUAL, EXA_PH_PACK, EXA_NPHASE
+  EXA_PH_MATVEC, EXA_PH_PRECOND_APPLY, EXA_PH_ORTHO, EXA_PH_GETQ, EXA_PH_RESIDUAL, EXA_PH_PACK, EXA_PH_UPDATE,
+  EXA_NPHASE
 };
 
 struct ExaProf {

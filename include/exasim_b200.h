@@ -111,9 +111,10 @@ int exa_last_residual(exa_ctx* ctx, double* initial, double* final_norm);
  * Phases: 0 volume assembly, 1 face assembly, 2 q-elimination GEMMs, 3 element inverse,
  * 4 Schur GEMMs, 5 preconditioner build, 6 matvec, 7 preconditioner apply,
  * 8 Gram-Schmidt + Givens, 9 q recovery, 10 residual-only assembly, 11 packing of tensor-core
- * operands (mixed-precision form).
+ * operands (mixed-precision form), 12 Newton update of uhat and u (and, in the mixed form, the
+ * refinement's condensed right-hand side).
  * exa_profile_read fills ms, count (timed regions) and flops (algorithmic FLOPs of the GEMM
- * phases 2 and 4, 0 elsewhere) for the first nphase (<= 12) phases; any may be NULL.  It
+ * phases 2 and 4, 0 elsewhere) for the first nphase (<= 13) phases; any may be NULL.  It
  * synchronises the context stream. */
 int exa_profile(exa_ctx* ctx, int enable);
 int exa_profile_read(exa_ctx* ctx, int nphase, double* ms, long long* count, double* flops);
