@@ -451,16 +451,24 @@ __global__ void getq_mf_kernel(ExaDims P, const double* shapegt, const double* s
       for (int r = 0; r < nd; ++r) vg[g + nge * (r + nd * (d + nd * k))] = Xx[g + nge * (d + nd * r)] * s;
   }
   __syncthreads();
-  // C_d u: sum over g and r of shapegw[a, g, 1 + r] vg[g, r, d]
-  for (int t = threadIdx.x; t < npe * ncu * nd; t += blockDim.x) {
-    const int a = t % npe, k = (t / npe) % ncu, d = t / (npe * ncu);
-    double s = 0.0;
+  // C_d u: sum over g and r of shapegw[a, g, 1 + r] vg[g, r, d]; one thread per (a, k) takes
+  // every d, so each shapegw entry is loaded once for the nd products that use it
+  for (int t = threadIdx.x; t < npe * ncu; t += blockDim.x) {
+    const int a = t % npe, k = t / npe;
+    double s[3] = {0.0, 0.0, 0.0};
     for (int r = 0; r < nd; ++r) {
       const double* W = shapegw + a + (long long)npe * nge * (1 + r);
-      const double* v = vg + nge * (r + nd * (d + nd * k));
-      for (int g = 0; g < nge; ++g) s = fma(W[npe * g], v[g], s);
+      const double* v = vg + nge * (r + nd * nd * k);
+      for (int g = 0; g < nge; ++g) {
+        const double wv = W[npe * g];
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+          if (d < nd) s[d] = fma(wv, v[g + nge * nd * d], s[d]);
+      }
     }
-    w[t] = s;
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+      if (d < nd) w[a + npe * (k + ncu * d)] = s[d];
   }
   __syncthreads();
   // minus E_d uhat, face by face (faces share corner and edge nodes)
@@ -483,14 +491,25 @@ __global__ void getq_mf_kernel(ExaDims P, const double* shapegt, const double* s
     }
     __syncthreads();
   }
-  // q = Minv w
+  // q = Minv w: one thread per row i takes up to 8 of the ncu nd right-hand sides at once,
+  // so each Minv entry is read once per 8 products
   const double* Mi = Minv + (long long)e * npe * npe;
-  for (int t = threadIdx.x; t < npe * ncu * nd; t += blockDim.x) {
-    const int i = t % npe, k = (t / npe) % ncu, d = t / (npe * ncu);
-    const double* wk = w + npe * (k + ncu * d);
-    double s = 0.0;
-    for (int j = 0; j < npe; ++j) s = fma(Mi[i + (long long)npe * j], wk[j], s);
-    U[i + npe * (ncu + k + ncu * d)] = s;
+  const int nq = ncu * nd;
+  for (int q0 = 0; q0 < nq; q0 += 8) {
+    for (int i = threadIdx.x; i < npe; i += blockDim.x) {
+      double s[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) s[q] = 0.0;
+      for (int j = 0; j < npe; ++j) {
+        const double m = Mi[i + (long long)npe * j];
+#pragma unroll
+        for (int q = 0; q < 8; ++q)
+          if (q0 + q < nq) s[q] = fma(m, w[j + npe * (q0 + q)], s[q]);
+      }
+#pragma unroll
+      for (int q = 0; q < 8; ++q)
+        if (q0 + q < nq) U[i + npe * (ncu + q0 + q)] = s[q];
+    }
   }
 }
 
