@@ -351,7 +351,16 @@ int launch_bgemv(int M, int K, int batch, const T* A, long long sA, const double
 #define EXA_BGEMV(R, V)                                                                                     \
   bgemv_kernel<T, R, V, (sizeof(T) == 8 && R > 12) ? 2 : 4>                                                   \
       <<<batch, 256, smem, st>>>(M, K, A, sA, x, sx, elemcon, ndf, ncu, alpha, beta, y0, y, sy)
-  if (sizeof(T) == 4 && M % 2 == 0) {
+  // rows covered per warp with single rows (RI from 1-6, 8, 10, 12, 16) and with pairs (RI from
+  // 1-6, 8): pairs only where they pad no more rows (m = 150: 160 single against 192 paired)
+  auto inst = [](int r, bool pairs) {
+    const int lim[] = {1, 2, 3, 4, 5, 6, 8, 10, 12, 16};
+    for (int v : lim)
+      if (v >= r && (!pairs || v <= 8)) return v;
+    return pairs ? 8 : 16;
+  };
+  const bool pairs = sizeof(T) == 4 && M % 2 == 0 && 64 * inst((M + 63) / 64, true) <= 32 * inst((M + 31) / 32, false);
+  if (pairs) {
     if constexpr (sizeof(T) == 4) {
       // pairs of rows per lane: ceil(M / 64) pairs
       const int ri = (M + 63) / 64;
