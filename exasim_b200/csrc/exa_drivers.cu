@@ -150,7 +150,7 @@ int exa_drv_residual(ExaCtx& c, double* norm) {
 int exa_drv_matvec(ExaCtx& c, const double* v, double* w) {
   ExaProfScope ps(c, EXA_PH_MATVEC);
   if (c.precision == 1)
-    EXA_TRY(exa_k_elem_matvec(c.P, c.elemcon, c.H32, v, c.we, c.st));
+    EXA_TRY(exa_k_elem_matvec(c.P, c.elemcon, c.H32, v, c.we, c.st, c.d_uflag));
   else
     EXA_TRY(exa_k_elem_matvec(c.P, c.elemcon, c.H, v, c.we, c.st));
   EXA_TRY(exa_k_scatter(c.P, c.f2e, c.elemcon, c.we, w, c.st));
@@ -166,7 +166,7 @@ int exa_drv_precond(ExaCtx& c, const double* v, double* w) {
   }
   if (c.precision == 1) {
     if (c.preconditioner == 0) return exa_k_bj_apply(c.P, c.Pc32, v, w, c.st);
-    EXA_TRY(exa_k_elem_matvec(c.P, c.elemcon, c.Pc32, v, c.we, c.st));
+    EXA_TRY(exa_k_elem_matvec(c.P, c.elemcon, c.Pc32, v, c.we, c.st, c.d_uflag));
     return exa_k_scatter(c.P, c.f2e, c.elemcon, c.we, w, c.st);
   }
   if (c.preconditioner == 0) return exa_k_bj_apply(c.P, c.Pc, v, w, c.st);
@@ -375,7 +375,8 @@ int update_solution(ExaCtx& c, int i, std::vector<double>& ybuf) {
 // When step i has converged, step i + 1 has run as well; it writes only basis column i + 2,
 // Hessenberg column i + 1 and Givens entries i + 1 and i + 2, none of which the solution
 // update of step i reads, so the result is that of stopping at step i.
-int exa_drv_gmres(ExaCtx& c, int* iters_out, double* relerr_out) {
+namespace {
+int gmres_body(ExaCtx& c, int* iters_out, double* relerr_out) {
   const long long N = c.ndofuhat();
   const int nrest = c.restart, maxit = c.gmres_maxit, n1 = nrest + 1;
   double nrmb = 0.0, nrmr = 0.0;
@@ -462,6 +463,27 @@ int exa_drv_gmres(ExaCtx& c, int* iters_out, double* relerr_out) {
   *relerr_out = relerr;
   return EXA_OK;  // not converged: the reference warns and continues (gmres.cpp:586-594)
 }
+}  // namespace
+
+// The mixed form's FP32 block products stream through shared memory with bounded waits
+// (d_flag[1] set when one ran out); read after the work that used them.
+int exa_drv_check_uflag(ExaCtx& c) {
+  if (c.precision != 1 || !c.d_uflag) return EXA_OK;
+  int f = 0;
+  EXA_CUDA(cudaMemcpyAsync(c.pinned, c.d_uflag, sizeof(int), cudaMemcpyDeviceToHost, c.st));
+  EXA_CUDA(cudaStreamSynchronize(c.st));
+  std::memcpy(&f, c.pinned, sizeof(int));
+  if (f) {
+    exa_set_error("FP32 block product: a wait inside the kernel ran out");
+    return EXA_ERR_CUDA;
+  }
+  return EXA_OK;
+}
+
+int exa_drv_gmres(ExaCtx& c, int* iters_out, double* relerr_out) {
+  EXA_TRY(gmres_body(c, iters_out, relerr_out));
+  return exa_drv_check_uflag(c);
+}
 
 // NewtonSolver (solution.cpp:125-243)
 int exa_drv_newton(ExaCtx& c, int* iters_out, double* norm_out) {
@@ -540,9 +562,9 @@ int exa_drv_condense_mixed(ExaCtx& c) {
     double* Ruc = c.Ru + (long long)e0 * n;
     EXA_CUDA(cudaMemcpyAsync(c.wRu, Ruc, sizeof(double) * (size_t)n * nb, cudaMemcpyDeviceToDevice, c.st));
     EXA_TRY(exa_k_gemv32(n, n, nb, 1.0, c.Dinv32 + (long long)e0 * n * n, (long long)n * n, c.wRu, n, 0.0, Ruc, n,
-                         c.st));
+                         c.st, c.d_uflag));
     EXA_TRY(exa_k_gemv32(m, n, nb, -1.0, c.K32 + (long long)e0 * m * n, (long long)m * n, Ruc, n, 1.0,
-                         c.Rh + (long long)e0 * m, m, c.st));
+                         c.Rh + (long long)e0 * m, m, c.st, c.d_uflag));
   }
   return exa_k_scatter(P, c.f2e, c.elemcon, c.Rh, c.b, c.st);
 }
@@ -591,7 +613,7 @@ int exa_drv_newton_mixed(ExaCtx& c, int* iters_out, double* norm_out) {
     {
       ExaProfScope ps(c, EXA_PH_UPDATE);
       EXA_TRY(exa_axpby(c.uh, c.x, 1.0, 1.0, N, c.st));
-      EXA_TRY(exa_k_dudg(P, c.elemcon, c.F32, c.Ru, c.x, c.du, c.st));
+      EXA_TRY(exa_k_dudg(P, c.elemcon, c.F32, c.Ru, c.x, c.du, c.st, c.d_uflag));
       EXA_TRY(exa_k_udg_update(P, c.udg, c.du, 1.0, c.st));
       if (c.RBdim > 0) EXA_TRY(rb_update(c, 1.0));
     }
@@ -616,6 +638,7 @@ int exa_drv_newton_mixed(ExaCtx& c, int* iters_out, double* norm_out) {
   *iters_out = std::min(it + 1, c.mixed_maxit);
   *norm_out = nrmr;
   c.last_norm = nrmr;
+  EXA_TRY(exa_drv_check_uflag(c));  // the updates' and condensations' FP32 products
   if (nrmr > rtol * nrm0 && !(nrmr < c.newton_tol)) {
     exa_set_error("mixed-precision refinement stopped at residual ratio %.3e after %d steps", nrmr / nrm0,
                   c.mixed_maxit);

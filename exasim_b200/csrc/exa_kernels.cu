@@ -6,6 +6,8 @@
 // assembly needs no atomics: the first element of a face writes, the second adds,
 // as Exasim's PutElementFaceNodes pair does (backend/Common/kokkosimpl.h:1032-1065).
 #include "exa_kernels.cuh"
+#include "exa_tc.cuh"
+#include "exa_umma.cuh"
 
 namespace {
 
@@ -338,14 +340,153 @@ __global__ void __launch_bounds__(256) bgemv_kernel(int M, int K, const T* A, lo
   }
 }
 
+// The same product for FP32 blocks streamed through shared memory: one CTA per block; a
+// producer warp copies chunks of CW columns (contiguous in the column-major block) into a
+// ring of BG_ST stages with cp.async.bulk, each completing on its stage's mbarrier by
+// transaction count; 8 consumer warps split the rows (lane l of warp w keeps rows
+// w rpw + l + 32 i) and run over every column of each chunk from shared memory, so no
+// partial sums cross warps and the registers hold only the sums.  Two CTAs share an SM, so
+// up to six 32 KB chunks are in flight per SM.  Every wait is bounded: one that runs out sets
+// *flag to EXA_UMMA_TIMEOUT, the CTA skips the rest of its work and, before it exits, waits
+// (bounded) for the copies it issued.
+constexpr int BG_ST = 3, BG_STAGE_BYTES = 32768, BG_CONS = 256;
+
+size_t bgemv_bulk_smem(int K) { return (size_t)BG_ST * BG_STAGE_BYTES + 8 * (size_t)K + 16 * BG_ST + 16; }
+
+template <int RI>
+__global__ void __launch_bounds__(BG_CONS + 32, 2)
+    bgemv_bulk_kernel(int M, int K, int CW, const float* A, long long sA, const double* x, long long sx,
+                      const int* elemcon, int ndf, int ncu, double alpha, double beta, const double* y0, double* y,
+                      long long sy, int* flag) {
+  using namespace exa_tc;
+  extern __shared__ __align__(128) uint8_t bsm[];
+  float* stage = reinterpret_cast<float*>(bsm);
+  double* xe = reinterpret_cast<double*>(bsm + (size_t)BG_ST * BG_STAGE_BYTES);  // [K]
+  uint64_t* full = reinterpret_cast<uint64_t*>(xe + K);
+  uint64_t* empty = full + BG_ST;
+  int* abort_flag = reinterpret_cast<int*>(empty + BG_ST);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const long long e = blockIdx.x;
+  const int nch = (K + CW - 1) / CW;
+  const float* Ae = A + e * sA;
+  if (tid == 0) {
+    for (int s = 0; s < BG_ST; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], BG_CONS / 32);
+    }
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  volatile int* ab = abort_flag;
+  if (warp == BG_CONS / 32) {
+    if (lane == 0) {
+      int issued = 0;
+      for (int q = 0; q < nch; ++q) {
+        const int s = q % BG_ST;
+        if (q >= BG_ST && (*ab || !mbar_wait(&empty[s], (uint32_t)((q / BG_ST - 1) & 1)))) {
+          *ab = 1;
+          break;
+        }
+        const int c0 = q * CW, ncol = min(CW, K - c0);
+        const uint32_t bytes = (uint32_t)M * ncol * 4;
+        mbar_expect_tx(&full[s], bytes);
+        bulk_g2s(stage + (size_t)s * (BG_STAGE_BYTES / 4), Ae + (long long)c0 * M, bytes, &full[s]);
+        issued = q + 1;
+      }
+      // copies still in flight (only after an abort): their stages' latest phases
+      for (int q = max(0, issued - BG_ST); q < issued; ++q) mbar_wait(&full[q % BG_ST], (uint32_t)((q / BG_ST) & 1));
+    }
+  } else {
+    for (int k = tid; k < K; k += BG_CONS)
+      xe[k] = elemcon ? x[k % ncu + ncu * (long long)elemcon[k / ncu + (long long)ndf * e]] : x[e * sx + k];
+    asm volatile("bar.sync 1, %0;" ::"n"(BG_CONS) : "memory");
+    const int rpw = (M + 7) / 8, r0 = warp * rpw, r1 = min(M, r0 + rpw);
+    double acc[RI];
+#pragma unroll
+    for (int i = 0; i < RI; ++i) acc[i] = 0.0;
+    for (int q = 0; q < nch; ++q) {
+      const int s = q % BG_ST;
+      if (!*ab && !mbar_wait(&full[s], (uint32_t)((q / BG_ST) & 1))) *ab = 1;
+      if (!*ab) {
+        const float* S = stage + (size_t)s * (BG_STAGE_BYTES / 4);
+        const int c0 = q * CW, ncol = min(CW, K - c0);
+        for (int cc = 0; cc < ncol; ++cc) {
+          const double xv = xe[c0 + cc];
+          const float* col = S + (size_t)cc * M;
+#pragma unroll
+          for (int i = 0; i < RI; ++i) {
+            const int r = r0 + lane + 32 * i;
+            if (r < r1) acc[i] = fma((double)col[r], xv, acc[i]);
+          }
+        }
+      }
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&empty[s]);
+    }
+    if (!*ab) {
+#pragma unroll
+      for (int i = 0; i < RI; ++i) {
+        const int r = r0 + lane + 32 * i;
+        if (r < r1) {
+          const double prev = beta != 0.0 ? y0[e * sy + r] : 0.0;
+          y[e * sy + r] = alpha * acc[i] + beta * prev;
+        }
+      }
+    }
+  }
+  __syncthreads();
+  if (tid == 0 && *ab) atomicExch(flag, EXA_UMMA_TIMEOUT);
+}
+
+// columns per chunk for the streamed kernel: at most one stage, with every chunk's bytes and
+// start a multiple of 16; 0 where no such split exists (the register kernel serves those)
+int bgemv_bulk_cw(int M, int K, long long sA) {
+  // one CTA per block: the ring only pays where a block fills it several times.  The FP32
+  // matvec of 3D Euler (480 x 480, 0.9 MB) went from 230 to 181 ms per 32^3 solve; that of
+  // the 3D convection-diffusion case (150 x 150, 90 KB) from 1.96 to 2.12 ms per solve, so
+  // blocks under 256 KB keep the register kernel
+  if (M <= 0 || K <= 0 || M > 512 || sA % 4 != 0 || (long long)M * K < 65536) return 0;
+  for (int cw = std::min(K, BG_STAGE_BYTES / (4 * M)); cw >= 1; --cw) {
+    const int rem = K % cw;
+    if ((M * cw) % 4 == 0 && (M * rem) % 4 == 0) return cw;
+  }
+  return 0;
+}
+
+int launch_bgemv_bulk(int M, int K, int cw, int batch, const float* A, long long sA, const double* x, long long sx,
+                      const int* elemcon, int ndf, int ncu, double alpha, double beta, const double* y0, double* y,
+                      long long sy, int* flag, cudaStream_t st) {
+  const size_t smem = bgemv_bulk_smem(K);
+  const int ri = ((M + 7) / 8 + 31) / 32;
+  if (ri <= 1) {
+    EXA_TRY(exa_allow_smem((const void*)bgemv_bulk_kernel<1>, smem));
+    bgemv_bulk_kernel<1><<<batch, BG_CONS + 32, smem, st>>>(M, K, cw, A, sA, x, sx, elemcon, ndf, ncu, alpha, beta,
+                                                            y0, y, sy, flag);
+  } else {
+    EXA_TRY(exa_allow_smem((const void*)bgemv_bulk_kernel<2>, smem));
+    bgemv_bulk_kernel<2><<<batch, BG_CONS + 32, smem, st>>>(M, K, cw, A, sA, x, sx, elemcon, ndf, ncu, alpha, beta,
+                                                            y0, y, sy, flag);
+  }
+  EXA_LAUNCH_CHECK();
+  return EXA_OK;
+}
+
 template <typename T>
 int launch_bgemv(int M, int K, int batch, const T* A, long long sA, const double* x, long long sx,
                  const int* elemcon, int ndf, int ncu, double alpha, double beta, const double* y0, double* y,
-                 long long sy, cudaStream_t st) {
+                 long long sy, cudaStream_t st, int* flag = nullptr) {
   if (batch <= 0 || M <= 0) return EXA_OK;
   if (M > 512 || K > 512) {
     exa_set_error("batched gemv: blocks of %d x %d exceed 512 x 512", M, K);
     return EXA_ERR_UNSUPPORTED;
+  }
+  if constexpr (sizeof(T) == 4) {
+    // FP32 blocks stream through shared memory where a flag for the bounded waits is given,
+    // the blocks start on 16-byte boundaries and a chunking exists
+    const int cw = flag ? bgemv_bulk_cw(M, K, sA) : 0;
+    if (cw > 0 && (reinterpret_cast<uintptr_t>(A) & 15) == 0)
+      return launch_bgemv_bulk(M, K, cw, batch, A, sA, x, sx, elemcon, ndf, ncu, alpha, beta, y0, y, sy, flag, st);
   }
   const size_t smem = sizeof(double) * ((size_t)(K > 0 ? K : 1) + 8 * (size_t)M);
 #define EXA_BGEMV(R, V)                                                                                     \
@@ -567,10 +708,10 @@ int exa_k_scatter(const ExaDims& P, const int* f2e, const int* elemcon, const do
 
 template <typename T>
 int exa_k_elem_matvec(const ExaDims& P, const int* elemcon, const T* A, const double* v, double* we,
-                      cudaStream_t st) {
+                      cudaStream_t st, int* flag) {
   // we_e = A_e gather(v): A_e = H (matvec) or the additive-Schwarz inverse blocks
   return launch_bgemv<T>(P.m, P.m, P.ne, A, (long long)P.m * P.m, v, 0, elemcon, P.ndf, P.ncu, 1.0, 0.0, nullptr, we,
-                         P.m, st);
+                         P.m, st, flag);
 }
 
 template <typename T>
@@ -599,10 +740,10 @@ int exa_k_bj_apply(const ExaDims& P, const T* BE, const double* x, double* y, cu
 
 template <typename T>
 int exa_k_dudg(const ExaDims& P, const int* elemcon, const T* DinvF, const double* Ru, const double* x,
-               double* du, cudaStream_t st) {
+               double* du, cudaStream_t st, int* flag) {
   // du_e = Ru_e + DinvF_e gather(x)
   return launch_bgemv<T>(P.n, P.m, P.ne, DinvF, (long long)P.n * P.m, x, 0, elemcon, P.ndf, P.ncu, 1.0, 1.0, Ru, du,
-                         P.n, st);
+                         P.n, st, flag);
 }
 
 int exa_k_udg_update(const ExaDims& P, double* udg, const double* du, double alpha, cudaStream_t st) {
@@ -649,8 +790,8 @@ __global__ void to_f32_kernel(const double* x, float* y, long long n) {
 }  // namespace
 
 int exa_k_gemv32(int M, int K, int batch, double alpha, const float* A, long long sA, const double* x, long long sx,
-                 double beta, double* y, long long sy, cudaStream_t st) {
-  return launch_bgemv<float>(M, K, batch, A, sA, x, sx, nullptr, 0, 1, alpha, beta, y, y, sy, st);
+                 double beta, double* y, long long sy, cudaStream_t st, int* flag) {
+  return launch_bgemv<float>(M, K, batch, A, sA, x, sx, nullptr, 0, 1, alpha, beta, y, y, sy, st, flag);
 }
 
 int exa_k_to_f32(const double* x, float* y, long long n, cudaStream_t st) {
@@ -662,10 +803,12 @@ int exa_k_to_f32(const double* x, float* y, long long n, cudaStream_t st) {
 
 // block arrays in FP64 (plain form) and FP32 (mixed-precision form)
 #define EXA_INST_BLOCK_KERNELS(T)                                                                              \
-  template int exa_k_elem_matvec<T>(const ExaDims&, const int*, const T*, const double*, double*, cudaStream_t); \
+  template int exa_k_elem_matvec<T>(const ExaDims&, const int*, const T*, const double*, double*, cudaStream_t, \
+                                    int*);                                                                     \
   template int exa_k_bj_build<T>(const ExaDims&, const int*, const int*, const T*, T*, cudaStream_t);           \
   template int exa_k_eas_build<T>(const ExaDims&, const int*, const int*, const T*, T*, cudaStream_t);          \
   template int exa_k_bj_apply<T>(const ExaDims&, const T*, const double*, double*, cudaStream_t);              \
-  template int exa_k_dudg<T>(const ExaDims&, const int*, const T*, const double*, const double*, double*, cudaStream_t);
+  template int exa_k_dudg<T>(const ExaDims&, const int*, const T*, const double*, const double*, double*, cudaStream_t, \
+                             int*);
 EXA_INST_BLOCK_KERNELS(double)
 EXA_INST_BLOCK_KERNELS(float)

@@ -18,9 +18,11 @@ int exa_k_qmats(const ExaDims& P, const double* shapegt, const double* shapegw, 
                 double* cw, double* ew, cudaStream_t st);
 int exa_k_scatter(const ExaDims& P, const int* f2e, const int* elemcon, const double* we, double* w, cudaStream_t st);
 // block kernels, T = double (plain form) or float (mixed-precision form); vectors stay FP64
+// flag (may be null): FP32 blocks given a device flag stream through shared memory by bulk
+// copies with bounded waits; a wait that runs out sets *flag to EXA_UMMA_TIMEOUT
 template <typename T>
 int exa_k_elem_matvec(const ExaDims& P, const int* elemcon, const T* A, const double* v, double* we,
-                      cudaStream_t st);
+                      cudaStream_t st, int* flag = nullptr);
 template <typename T>
 int exa_k_bj_build(const ExaDims& P, const int* f2e, const int* elemcon, const T* H, T* BE, cudaStream_t st);
 template <typename T>
@@ -29,11 +31,11 @@ template <typename T>
 int exa_k_bj_apply(const ExaDims& P, const T* BE, const double* x, double* y, cudaStream_t st);
 template <typename T>
 int exa_k_dudg(const ExaDims& P, const int* elemcon, const T* DinvF, const double* Ru, const double* x,
-               double* du, cudaStream_t st);
+               double* du, cudaStream_t st, int* flag = nullptr);
 // y_e = alpha A_e x_e + beta y_e per element e: A_e FP32 [M, K] column-major sA apart,
 // x_e, y_e FP64 sx, sy apart (FP64 accumulation)
 int exa_k_gemv32(int M, int K, int batch, double alpha, const float* A, long long sA, const double* x, long long sx,
-                 double beta, double* y, long long sy, cudaStream_t st);
+                 double beta, double* y, long long sy, cudaStream_t st, int* flag = nullptr);
 // D and B volume blocks on the tcgen05 tensor cores (3xTF32) for the mixed-precision form,
 // with S = shapegt[:, :, 0] packed as a B operand (rows npe, K nge); npe, nge <= 128.
 struct UPacked;

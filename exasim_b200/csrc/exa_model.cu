@@ -217,8 +217,9 @@ int schur_chunk_mixed(ExaCtx& c, int e0, int nb) {
   // Ru = Dinv Ru; Rh -= K Ru
   double* Ruc = c.Ru + (long long)e0 * n;
   EXA_CUDA(cudaMemcpyAsync(c.wRu, Ruc, sizeof(double) * (size_t)n * nb, cudaMemcpyDeviceToDevice, c.st));
-  EXA_TRY(exa_k_gemv32(n, n, nb, 1.0, D32, (long long)n * n, c.wRu, n, 0.0, Ruc, n, c.st));
-  EXA_TRY(exa_k_gemv32(m, n, nb, -1.0, K32, (long long)m * n, Ruc, n, 1.0, c.Rh + (long long)e0 * m, m, c.st));
+  EXA_TRY(exa_k_gemv32(n, n, nb, 1.0, D32, (long long)n * n, c.wRu, n, 0.0, Ruc, n, c.st, c.d_uflag));
+  EXA_TRY(exa_k_gemv32(m, n, nb, -1.0, K32, (long long)m * n, Ruc, n, 1.0, c.Rh + (long long)e0 * m, m, c.st,
+                       c.d_uflag));
   return EXA_OK;
 }
 
