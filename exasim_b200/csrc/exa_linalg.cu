@@ -40,7 +40,15 @@ int exa_allow_smem(const void* fn, size_t bytes) {
   EXA_CUDA(cudaGetDevice(&dev));
   std::lock_guard<std::mutex> g(mu);
   if (done.count({dev, fn})) return EXA_OK;
-  EXA_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMax));
+  // the kernel's static shared memory counts against the same per-block limit
+  cudaFuncAttributes fa{};
+  EXA_CUDA(cudaFuncGetAttributes(&fa, fn));
+  const size_t cap = kMax > fa.sharedSizeBytes ? kMax - fa.sharedSizeBytes : 0;
+  if (bytes > cap) {
+    exa_set_error("kernel needs %zu bytes of dynamic shared memory, more than %zu", bytes, cap);
+    return EXA_ERR_UNSUPPORTED;
+  }
+  EXA_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cap));
   done.insert({dev, fn});
   return EXA_OK;
 }

@@ -91,3 +91,31 @@ def test_mixed_dirk_steps_match_fp64(cd3):
     assert rel2(s32.get("udg"), s64.get("udg")) < 1e-6
     s64.close()
     s32.close()
+
+
+def test_switching_forms_on_one_context(cd3):
+    """A context that solves in FP64 (capturing its GMRES steps as CUDA graphs), switches to the
+    mixed form (which frees the FP64 blocks it does not read) and back solves each stage as a
+    context that never switched: FP64 stages bit for bit, the mixed stage within 1e-6."""
+    ref = HDGSolver(cd3, "convdiff3d")
+    s = HDGSolver(cd3, "convdiff3d")
+    for j in range(2):  # FP64 stages on both: the second replays captured GMRES steps
+        ref.DIRKStage(0, j)
+        s.DIRKStage(0, j)
+    assert np.array_equal(s.get("udg"), ref.get("udg"))
+    s.set_precision(1, inner_tol=1e-4, rtol=1e-10)
+    ref.DIRKStage(0, 2)
+    s.DIRKStage(0, 2)
+    assert rel2(s.get("udg"), ref.get("udg")) < 1e-6
+    with pytest.raises(Exception):
+        s.get("F")  # D^-1 F in FP64 is not held in the mixed form
+    s.set_precision(0)
+    s.set("udg", ref.get("udg"))
+    s.set("uh", ref.get("uh"))
+    for j in range(3):
+        ref.DIRKStage(1, j)
+        s.DIRKStage(1, j)
+    assert np.array_equal(s.get("udg"), ref.get("udg"))
+    assert np.array_equal(s.get("F"), ref.get("F"))
+    s.close()
+    ref.close()
