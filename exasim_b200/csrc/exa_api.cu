@@ -244,6 +244,9 @@ int exa_ctx_init(ExaCtx& c, const double* app, long long napp, const double* mas
   c.device = device;
   EXA_CUDA(cudaSetDevice(device));
   EXA_CUDA(cudaStreamCreateWithFlags(&c.st, cudaStreamNonBlocking));
+  EXA_CUDA(cudaStreamCreateWithFlags(&c.st2, cudaStreamNonBlocking));
+  EXA_CUDA(cudaEventCreateWithFlags(&c.ev_q, cudaEventDisableTiming));
+  EXA_CUDA(cudaEventCreateWithFlags(&c.ev_inv, cudaEventDisableTiming));
   EXA_TRY(dev_upload(c, &c.shapegt, M.part[1], (size_t)M.nsize[1]));
   EXA_TRY(dev_upload(c, &c.shapegw, M.part[2], (size_t)M.nsize[2]));
   EXA_TRY(dev_upload(c, &c.shapfgt, M.part[3], (size_t)M.nsize[3]));
@@ -637,6 +640,14 @@ void exa_ctx_free(ExaCtx& c) {
     if (c.step_ev[k]) cudaEventDestroy(c.step_ev[k]);
     c.step_ev[k] = nullptr;
   }
+  if (c.st2) {
+    cudaStreamSynchronize(c.st2);
+    cudaStreamDestroy(c.st2);
+  }
+  c.st2 = nullptr;
+  if (c.ev_q) cudaEventDestroy(c.ev_q);
+  if (c.ev_inv) cudaEventDestroy(c.ev_inv);
+  c.ev_q = c.ev_inv = nullptr;
   if (c.st) cudaStreamDestroy(c.st);
   c.st = nullptr;
 }

@@ -33,6 +33,21 @@ int smem_attr(const void* fn, size_t bytes) {
   return EXA_OK;
 }
 
+// The element inverse needs D alone, so once the q-elimination product into D is done it
+// runs on the context's second stream, beside the three products into F, K and H: its pivot
+// loop is latency-bound and the products are HBM- or tensor-bound.  With phase profiling on,
+// everything stays on the context stream, so the phase events time each step alone.
+bool overlap_inverse(const ExaCtx& c) { return c.P.ncq > 0 && c.st2 && !c.prof.on; }
+
+template <class Fn>
+int inverse_beside(ExaCtx& c, Fn&& fn) {
+  EXA_CUDA(cudaEventRecord(c.ev_q, c.st));
+  EXA_CUDA(cudaStreamWaitEvent(c.st2, c.ev_q, 0));
+  EXA_TRY(fn(c.st2));
+  EXA_CUDA(cudaEventRecord(c.ev_inv, c.st2));
+  return EXA_OK;
+}
+
 // Schur condensation of one chunk (uequation.cpp:559-775): q-elimination, D^-1, DinvF,
 // Ru <- D^-1 Ru, H += K DinvF, Rh -= K Ru.
 int schur_chunk(ExaCtx& c, int e0, int nb) {
@@ -40,6 +55,7 @@ int schur_chunk(ExaCtx& c, int e0, int nb) {
   const int n = P.n, m = P.m, npe = P.npe, nd = P.nd, ncu = P.ncu, ndf = P.ndf;
   const long long nqn = (long long)npe * nd * ncu;
   double* Hc = c.H + (long long)e0 * m * m;
+  const bool overlap = overlap_inverse(c);
   if (P.ncq > 0) {
     ExaProfScope ps(c, EXA_PH_QELIM);
     // four GEMMs per trace component with K = npe*nd: (n + m) rows x (npe + ndf) columns in all
@@ -58,6 +74,9 @@ int schur_chunk(ExaCtx& c, int e0, int nb) {
     g.B = MC; g.ldb = kq; g.sB = kq * npe; g.sB2 = 0;
     g.C = c.wD; g.ldc = n; g.sC = (long long)n * n; g.sC2 = (long long)n * npe;
     EXA_TRY(exa_gemm(g, c.st));
+    if (overlap) EXA_TRY(inverse_beside(c, [&](cudaStream_t s) {
+      return exa_inverse_ws(c.wD, n, (long long)n * n, nb, c.wInv, c.d_flag, s);
+    }));
     // F(:, b + ncu*jf) -= sum_(l,d) B(:, l + npe*d + npe*nd*b) MinvE(l, d, jf)
     g.N = ndf; g.alpha = -1.0;
     g.B = ME; g.ldb = kq; g.sB = kq * ndf;
@@ -75,7 +94,9 @@ int schur_chunk(ExaCtx& c, int e0, int nb) {
     g.C = Hc; g.ldc = (long long)m * ncu; g.sC = (long long)m * m; g.sC2 = m;
     EXA_TRY(exa_gemm(g, c.st));
   }
-  {
+  if (overlap) {
+    EXA_CUDA(cudaStreamWaitEvent(c.st, c.ev_inv, 0));
+  } else {
     ExaProfScope ps(c, EXA_PH_INVERSE);
     EXA_TRY(exa_inverse_ws(c.wD, n, (long long)n * n, nb, c.wInv, c.d_flag, c.st));
   }
@@ -125,6 +146,17 @@ int schur_chunk_mixed(ExaCtx& c, int e0, int nb) {
   float* H32 = c.H32 + (long long)e0 * m * m;
   float* F32 = c.F32 + (long long)e0 * n * m;
   const double* Hc = c.fp64_full ? c.H + (long long)e0 * m * m : c.H;  // per-chunk staging in the mixed form
+  const bool overlap = overlap_inverse(c);
+  // D^-1 in FP32 (the recursive blocked form with its products on the tensor cores where
+  // the order exceeds the register kernel's, else the register kernel), then packed
+  auto inverse = [&](cudaStream_t s) -> int {
+    if (c.wInvPk)
+      EXA_TRY(exa_inverse_tc32(D32, n, (long long)n * n, nb, c.wInv32, c.wInvPk, c.d_flag, c.d_uflag, s));
+    else
+      EXA_TRY(exa_inverse_ws(D32, n, (long long)n * n, nb, reinterpret_cast<float*>(c.wInv), c.d_flag, s));
+    return EXA_OK;
+  };
+  auto pack_dinv = [&](cudaStream_t s) { return exa_pack(D32, 0, 1, n, (long long)n * n, 0, nb, 1, c.Dinvp, s); };
   auto at = [](UPacked u, long long e) {  // operand of element e of the set
     u.hi += e * u.sb;
     u.lo += e * u.sb;
@@ -151,6 +183,10 @@ int schur_chunk_mixed(ExaCtx& c, int e0, int nb) {
     u.C = D32; u.ldc = n; u.sC = (long long)n * n; u.sC2 = (long long)n * npe;
     u.nout = 0;
     EXA_TRY(exa_gemm_3xtf32(u, c.d_uflag, c.st));
+    if (overlap) EXA_TRY(inverse_beside(c, [&](cudaStream_t s) {
+      EXA_TRY(inverse(s));
+      return pack_dinv(s);
+    }));
     // F(:, b + ncu*jf) = F - B_b MinvE, packed only (B operand of D^-1 F)
     u.N = ndf; u.alpha = -1.0;
     u.B = at(c.MEp, e0); u.B.sb2 = 0;
@@ -182,18 +218,15 @@ int schur_chunk_mixed(ExaCtx& c, int e0, int nb) {
     EXA_TRY(exa_pack(c.wF, 1, n, 1, (long long)n * m, 0, nb, 1, c.wFp, c.st));
     EXA_TRY(exa_pack(c.wK, 1, 1, m, (long long)m * n, 0, nb, 1, c.Kp, c.st));
   }
-  {
-    ExaProfScope ps(c, EXA_PH_INVERSE);
-    // the recursive blocked form with its products on the tensor cores where the order
-    // exceeds its leaf size, else the register kernel (exa_inverse_ws takes it whole)
-    if (c.wInvPk)
-      EXA_TRY(exa_inverse_tc32(D32, n, (long long)n * n, nb, c.wInv32, c.wInvPk, c.d_flag, c.d_uflag, c.st));
-    else
-      EXA_TRY(exa_inverse_ws(D32, n, (long long)n * n, nb, reinterpret_cast<float*>(c.wInv), c.d_flag, c.st));
-  }
-  {
+  if (overlap) {
+    EXA_CUDA(cudaStreamWaitEvent(c.st, c.ev_inv, 0));
+  } else {
+    {
+      ExaProfScope ps(c, EXA_PH_INVERSE);
+      EXA_TRY(inverse(c.st));
+    }
     ExaProfScope pp(c, EXA_PH_PACK);
-    EXA_TRY(exa_pack(D32, 0, 1, n, (long long)n * n, 0, nb, 1, c.Dinvp, c.st));
+    EXA_TRY(pack_dinv(c.st));
   }
   ExaProfScope ps(c, EXA_PH_SCHUR);
   exa_prof_flops(c, EXA_PH_SCHUR, 2.0 * nb * ((double)n * n * m + (double)n * n + (double)m * m * n + (double)m * n));

@@ -34,6 +34,10 @@ struct ExaCtx {
   ExaDims P{};
   int device = 0;
   cudaStream_t st = nullptr;
+  // second stream of the assembly: the element inverse runs there beside the q-elimination
+  // products that do not need it (ev_q: D ready; ev_inv: D^-1 ready)
+  cudaStream_t st2 = nullptr;
+  cudaEvent_t ev_q = nullptr, ev_inv = nullptr;
   // app flags (app.bin flag/problem/solversparam, setstructs.cpp:45-322)
   int tdep = 0, wave = 0, preconditioner = 0, ortho = 0, tdfunc = 1, sourcefunc = 1, modelnumber = 0;
   int newton_maxit = 20, gmres_maxit = 200, restart = 25, torder = 1, nstage = 1, ppdegree = 0, RBdim = 0;
