@@ -66,6 +66,21 @@ def test_fp32_inverse_matches_lapack(lib, n):
         assert err < 2e-5, err
 
 
+@pytest.mark.parametrize("n", [125, 250])
+def test_fp32_singular_block_sets_flag(lib, n):
+    """A zero pivot column in the block (the leading diagonal block of the blocked form at
+    250) sets the flag in the FP32 inverse as in the FP64 one."""
+    import torch
+    A = np.eye(n, dtype=np.float32)
+    A[3, 3] = 0.0
+    dev = torch.tensor(A.T.ravel(), dtype=torch.float32, device="cuda")
+    flag = torch.zeros(1, dtype=torch.int32, device="cuda")
+    assert lib.exa_sinverse_batched(ctypes.c_void_p(dev.data_ptr()), n, n * n, 1, ctypes.c_void_p(flag.data_ptr()),
+                                    None) == 0
+    torch.cuda.synchronize()
+    assert int(flag.item()) == 1
+
+
 @pytest.mark.parametrize("n", [8, 125])
 def test_singular_block_sets_flag(lib, n):
     import torch
