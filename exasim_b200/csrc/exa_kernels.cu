@@ -242,10 +242,10 @@ __global__ void bj_apply_kernel(ExaDims P, const T* BE, const double* x, double*
 // dimension M, batch stride sA; y0 may alias y).  x_e is read at x + e sx, or, with elemcon,
 // gathered from a trace vector: x_e[k] = x[k % ncu + ncu elemcon[k / ncu + ndf e]].  One
 // CTA per block: 8 warps split the columns (warp w takes c = w, w + 8, ...), CU at a time
-// with the next CU loaded ahead (CU = 2 where 4 would not fit the registers); lane l keeps the partial sums of rows V l + 32 V i + v
-// (i < RI, v < V) in registers, so each column is one coalesced load per 32 V rows (V = 2:
-// pairs of floats, as many bytes per load as FP64); the 8 partial sums of a row meet in
-// shared memory in a fixed order.  Serves the condensed matvec w_e = H_e gather(v)
+// with the next CU loaded ahead (CU = 2 where 4 would not fit the registers); lane l keeps
+// the partial sums of rows V l + 32 V i + v (i < RI, v < V) in registers, so each column is
+// one coalesced load per 32 V rows (V = 2: pairs of floats, as many bytes per load as FP64);
+// the 8 partial sums of a row meet in shared memory in a fixed order.  Serves the condensed matvec w_e = H_e gather(v)
 // (hdgMatVec, matvec.cpp:240-389) and the additive-Schwarz apply, du = Ru + D^-1 F x
 // (hdgGetDUDG, matvec.cpp:219-238) and the mixed form's Ru <- D^-1 Ru, Rh <- Rh - K Ru.
 template <typename T, int RI, int V, int CU>
