@@ -477,11 +477,25 @@ __global__ void __launch_bounds__(16 * TY, (sizeof(T) == 4 && TY == 16) ? 2 : 1)
           if (v > best) { best = v; bi = r; }
         }
       }
-#pragma unroll
-      for (int off = 16; off > 0; off >>= 1) {
-        const T ob = __shfl_xor_sync(0xffffffffu, best, off);
-        const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
-        if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
+      // a non-negative value orders as its bit pattern: the warp's largest |v| by 32-bit
+      // reductions (for FP64 the high word, then the low word among lanes that tie on it),
+      // and the lowest row holding it by one more: the choice of a shuffle tree that keeps
+      // the larger value and, on ties, the lower row
+      if constexpr (sizeof(T) == 4) {
+        const unsigned key = bi < n ? __float_as_uint(best) : 0u;
+        const unsigned mx = __reduce_max_sync(0xffffffffu, key);
+        const unsigned mn = __reduce_min_sync(0xffffffffu, (bi < n && key == mx) ? (unsigned)bi : 0xffffffffu);
+        best = __uint_as_float(mx);
+        bi = mn == 0xffffffffu ? n : (int)mn;
+      } else {
+        const unsigned long long key = bi < n ? (unsigned long long)__double_as_longlong(best) : 0ull;
+        const unsigned khi = (unsigned)(key >> 32), klo = (unsigned)key;
+        const unsigned mhi = __reduce_max_sync(0xffffffffu, khi);
+        const unsigned mlo = __reduce_max_sync(0xffffffffu, khi == mhi ? klo : 0u);
+        const bool top = bi < n && khi == mhi && klo == mlo;
+        const unsigned mn = __reduce_min_sync(0xffffffffu, top ? (unsigned)bi : 0xffffffffu);
+        best = __longlong_as_double((long long)(((unsigned long long)mhi << 32) | mlo));
+        bi = mn == 0xffffffffu ? n : (int)mn;
       }
       if (!(best > T(0)) || bi >= n) {
         singular = true;
