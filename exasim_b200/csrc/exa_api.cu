@@ -447,6 +447,7 @@ int fp64_blocks(ExaCtx& c, bool full) {
   if (full == c.fp64_full) return EXA_OK;
   const ExaDims& P = c.P;
   const size_t ne = P.ne, n = P.n, m = P.m, nb = c.neb;
+  if (c.st2) EXA_CUDA(cudaStreamSynchronize(c.st2));
   EXA_CUDA(cudaStreamSynchronize(c.st));
   for (cudaGraphExec_t& g : c.arnoldi_graph[0]) {
     if (g) cudaGraphExecDestroy(g);
@@ -622,6 +623,8 @@ long long exa_ctx_estimate_bytes(const double* app, long long napp, const double
 
 void exa_ctx_free(ExaCtx& c) {
   if (c.device >= 0) cudaSetDevice(c.device);
+  // the second stream first: after an error it may still use arrays that are freed below
+  if (c.st2) cudaStreamSynchronize(c.st2);
   if (c.st) cudaStreamSynchronize(c.st);
   exa_prof_free(c);
   for (void* p : c.allocs) {
@@ -640,10 +643,7 @@ void exa_ctx_free(ExaCtx& c) {
     if (c.step_ev[k]) cudaEventDestroy(c.step_ev[k]);
     c.step_ev[k] = nullptr;
   }
-  if (c.st2) {
-    cudaStreamSynchronize(c.st2);
-    cudaStreamDestroy(c.st2);
-  }
+  if (c.st2) cudaStreamDestroy(c.st2);
   c.st2 = nullptr;
   if (c.ev_q) cudaEventDestroy(c.ev_q);
   if (c.ev_inv) cudaEventDestroy(c.ev_inv);

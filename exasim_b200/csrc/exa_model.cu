@@ -39,13 +39,30 @@ int smem_attr(const void* fn, size_t bytes) {
 // everything stays on the context stream, so the phase events time each step alone.
 bool overlap_inverse(const ExaCtx& c) { return c.P.ncq > 0 && c.st2 && !c.prof.on; }
 
+// The context stream joins the second stream before any later work, on every path out of a
+// Schur step (an early error return included), so nothing it runs next can overlap it.
+struct InverseJoin {
+  ExaCtx& c;
+  bool pending = false;
+  ~InverseJoin() {
+    if (pending) cudaStreamWaitEvent(c.st, c.ev_inv, 0);
+  }
+  int join() {
+    pending = false;
+    EXA_CUDA(cudaStreamWaitEvent(c.st, c.ev_inv, 0));
+    return EXA_OK;
+  }
+};
+
 template <class Fn>
-int inverse_beside(ExaCtx& c, Fn&& fn) {
+int inverse_beside(ExaCtx& c, InverseJoin& j, Fn&& fn) {
   EXA_CUDA(cudaEventRecord(c.ev_q, c.st));
   EXA_CUDA(cudaStreamWaitEvent(c.st2, c.ev_q, 0));
-  EXA_TRY(fn(c.st2));
+  j.pending = true;
+  const int st = fn(c.st2);
+  // recorded whatever fn returned, so the join covers whatever it enqueued
   EXA_CUDA(cudaEventRecord(c.ev_inv, c.st2));
-  return EXA_OK;
+  return st;
 }
 
 // Schur condensation of one chunk (uequation.cpp:559-775): q-elimination, D^-1, DinvF,
@@ -56,6 +73,7 @@ int schur_chunk(ExaCtx& c, int e0, int nb) {
   const long long nqn = (long long)npe * nd * ncu;
   double* Hc = c.H + (long long)e0 * m * m;
   const bool overlap = overlap_inverse(c);
+  InverseJoin join{c};
   if (P.ncq > 0) {
     ExaProfScope ps(c, EXA_PH_QELIM);
     // four GEMMs per trace component with K = npe*nd: (n + m) rows x (npe + ndf) columns in all
@@ -74,7 +92,7 @@ int schur_chunk(ExaCtx& c, int e0, int nb) {
     g.B = MC; g.ldb = kq; g.sB = kq * npe; g.sB2 = 0;
     g.C = c.wD; g.ldc = n; g.sC = (long long)n * n; g.sC2 = (long long)n * npe;
     EXA_TRY(exa_gemm(g, c.st));
-    if (overlap) EXA_TRY(inverse_beside(c, [&](cudaStream_t s) {
+    if (overlap) EXA_TRY(inverse_beside(c, join, [&](cudaStream_t s) {
       return exa_inverse_ws(c.wD, n, (long long)n * n, nb, c.wInv, c.d_flag, s);
     }));
     // F(:, b + ncu*jf) -= sum_(l,d) B(:, l + npe*d + npe*nd*b) MinvE(l, d, jf)
@@ -95,7 +113,7 @@ int schur_chunk(ExaCtx& c, int e0, int nb) {
     EXA_TRY(exa_gemm(g, c.st));
   }
   if (overlap) {
-    EXA_CUDA(cudaStreamWaitEvent(c.st, c.ev_inv, 0));
+    EXA_TRY(join.join());
   } else {
     ExaProfScope ps(c, EXA_PH_INVERSE);
     EXA_TRY(exa_inverse_ws(c.wD, n, (long long)n * n, nb, c.wInv, c.d_flag, c.st));
@@ -147,6 +165,7 @@ int schur_chunk_mixed(ExaCtx& c, int e0, int nb) {
   float* F32 = c.F32 + (long long)e0 * n * m;
   const double* Hc = c.fp64_full ? c.H + (long long)e0 * m * m : c.H;  // per-chunk staging in the mixed form
   const bool overlap = overlap_inverse(c);
+  InverseJoin join{c};
   // D^-1 in FP32 (the recursive blocked form with its products on the tensor cores where
   // the order exceeds the register kernel's, else the register kernel), then packed
   auto inverse = [&](cudaStream_t s) -> int {
@@ -183,7 +202,7 @@ int schur_chunk_mixed(ExaCtx& c, int e0, int nb) {
     u.C = D32; u.ldc = n; u.sC = (long long)n * n; u.sC2 = (long long)n * npe;
     u.nout = 0;
     EXA_TRY(exa_gemm_3xtf32(u, c.d_uflag, c.st));
-    if (overlap) EXA_TRY(inverse_beside(c, [&](cudaStream_t s) {
+    if (overlap) EXA_TRY(inverse_beside(c, join, [&](cudaStream_t s) {
       EXA_TRY(inverse(s));
       return pack_dinv(s);
     }));
@@ -219,7 +238,7 @@ int schur_chunk_mixed(ExaCtx& c, int e0, int nb) {
     EXA_TRY(exa_pack(c.wK, 1, 1, m, (long long)m * n, 0, nb, 1, c.Kp, c.st));
   }
   if (overlap) {
-    EXA_CUDA(cudaStreamWaitEvent(c.st, c.ev_inv, 0));
+    EXA_TRY(join.join());
   } else {
     {
       ExaProfScope ps(c, EXA_PH_INVERSE);
