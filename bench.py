@@ -7,8 +7,10 @@ dt = 0.01.  One step = one DIRK-stage Newton solve to a residual ratio of 1e-8: 
 update, assembly with static condensation, block-Jacobi GMRES(50), Newton update and
 residual check.  The headline value is the mixed-precision form (3xTF32 tensor-core element
 elimination into FP32 blocks, FP64 residual refinement); the plain FP64 form of the same
-solves is timed in the same run and reported beside it.  Inputs are seeded synthetic data
-with the configuration's shapes.  With --gpus N (torchrun) every rank solves its own
+solves is timed in the same run and reported beside it.  Two more legs follow on one GPU:
+the 3D Euler isentropic-vortex configuration at its full 32^3 size in both forms (`euler3d`,
+where the elimination is compute-bound) and the served stream of 2D convection-diffusion
+requests (`served`).  Inputs are seeded synthetic data with the configurations' shapes.  With --gpus N (torchrun) every rank solves its own
 replica: the path has no data-path collective, so scaling is weak.
 
 Prints one JSON line.  `--impl reference` times the CPU restatement of the reference
