@@ -544,6 +544,7 @@ class HDGOracle:
         Rhv = np.transpose(Rh, (2, 0, 1)).reshape(m, ne, order="F")          # schurVectorRh
         Rhv = Rhv - np.einsum("ike,ke->ie", Km, Ruv)
         self.H, self.Rh, self.DinvF, self.Ru = Hm, Rhv, DinvF, Ruv
+        self.K, self.Dinv = Km, Dinv  # the condensation factors (the mixed refinement reuses them)
         return Hm, Rhv, DinvF, Ruv
 
     def residual(self, udg=None, uh=None):
@@ -746,6 +747,58 @@ class HDGOracle:
             if nrmr < tol:
                 return it + 1, norms
         return maxit, norms
+
+    def newton_mixed(self, inner_tol=1e-4, rtol=1e-8, maxit=30):
+        """The mixed-precision form of the solve (no counterpart in the reference): the
+        condensed blocks H, D^-1 F, K, D^-1 and the preconditioner of one assembly rounded to
+        FP32 (the CUDA path forms them with 3xTF32 tensor-core products, about FP32
+        accuracy), then refinement steps: GMRES on the FP32 operator to inner_tol, the Newton
+        update, the FP64 residual, and its condensation through the FP32 factors, until the
+        residual norm |b| + |Ru| has fallen by rtol or stops falling below the Newton
+        tolerance.  Vectors and accumulation stay FP64.  Returns (steps, norms)."""
+        f32 = lambda a: np.asarray(a, dtype=np.float32).astype(np.float64)
+        if self.ncq > 0:
+            self.get_q(self.udg, self.uh)
+        nrm0, _ = self.residual_norm()
+        norms = [nrm0]
+        if not nrm0 > 0.0:
+            return 0, norms
+        self.assemble()
+        self.H, self.DinvF, self.K, self.Dinv = f32(self.H), f32(self.DinvF), f32(self.K), f32(self.Dinv)
+        # the FP64 residual condensed through the FP32 factors
+        Ru, Rh = self.residual()
+        self.Ru = np.einsum("ike,ke->ie", self.Dinv, Ru)
+        self.Rh = Rh - np.einsum("ike,ke->ie", self.K, self.Ru)
+        self.build_precond()
+        self.P = f32(self.P)
+        gtol, ntol = self.gmres_tol, self.newton_tol
+        self.gmres_log = []
+        prev = nrm0
+        steps = 0
+        for steps in range(1, maxit + 1):
+            b = self.assemble_rhs(self.Rh)
+            self.gmres_tol, self.newton_tol = inner_tol, 0.0
+            try:
+                x, info = self.gmres(b)
+            finally:
+                self.gmres_tol, self.newton_tol = gtol, ntol
+            self.gmres_log.append(info)
+            self.uh = self.uh + x
+            du = self.Ru + np.einsum("ije,je->ie", self.DinvF, self.gather(x))
+            self.udg[:, :self.ncu] += du.reshape(self.npe, self.ncu, self.ne, order="F")
+            if self.ncq > 0:
+                self.get_q(self.udg, self.uh)
+            Ru, Rh = self.residual()
+            nrm = np.linalg.norm(self.assemble_rhs(Rh)) + np.linalg.norm(Ru)
+            norms.append(nrm)
+            if nrm <= rtol * nrm0:
+                break
+            if nrm < ntol and nrm > 0.5 * prev:  # the FP64 round-off floor
+                break
+            prev = nrm
+            self.Ru = np.einsum("ike,ke->ie", self.Dinv, Ru)
+            self.Rh = Rh - np.einsum("ike,ke->ie", self.K, self.Ru)
+        return steps, norms
 
     def _rb_guess(self, b):
         """ComputeInitialGuessAndPreconditioner (preconditioner.cpp:133-181): U_i = A W_i for the
