@@ -101,7 +101,9 @@ int exa_connectivity_host(const int* t, const int* bf, const int* perm, const do
  * and the preconditioner are kept in FP32.  The residual, the Newton update and GMRES stay
  * FP64: each step solves the FP32 system to inner_tol and recomputes the FP64 residual,
  * until the FP64 residual norm has dropped by rtol (0: by the GMRES tolerance of app.bin).
- * The first switch to mode 1 allocates the FP32 arrays. */
+ * The first switch to mode 1 allocates the FP32 arrays.  Mode 1 frees the FP64 "H", "F" and
+ * "P" arrays, which it does not read (their fields are unavailable until a switch back to
+ * mode 0 reallocates them; the next assembly fills them). */
 int exa_set_precision(exa_ctx* ctx, int mode, double inner_tol, double rtol);
 /* Residual norm |b| + |Ru| at the start and at the end of the last Newton solve. */
 int exa_last_residual(exa_ctx* ctx, double* initial, double* final_norm);
