@@ -11,6 +11,7 @@ Exasim datain/ folders (app, master, mesh, sol .bin) by exasim_b200.inputs.
 * ns2d_tgv_quad : 2D compressible Navier-Stokes, Taylor-Green vortex on the periodic [0, 2 pi]^2,
                   p=3 quadrilaterals, Mach 0.1, Re 1600, gamma 1.4, Pr 0.72, DIRK(3,3) dt 0.05,
                   Newton to 1e-8, GMRES(100) with block ILU(0) on 4 x 4-element sub-domains
+                  (periodic=False: the same square with boundary code 1 on every side)
 * euler3d_vortex_hex: 3D Euler (no q), isentropic vortex of strength 5 on the periodic
                   [-5, 5]^3, p=3 hexahedra (320 x 320 element blocks), Mach 0.5, DIRK(2,2)
 * cdsin2d_quad  : one request of the served stream: 2D convection-diffusion on the unit square,
@@ -77,15 +78,19 @@ def convdiff3d_hex(datain: str, n: int = 16, porder: int = 4, nsteps: int = 20, 
 
 def ns2d_tgv_quad(datain: str, n: int = 64, porder: int = 3, nsteps: int = 10, dt: float = 0.05,
                   preconditioner: int = 2, block: int = 4, restart: int = 100, gmres_tol: float = 1e-8,
-                  newton_tol: float = 1e-8, mach: float = 0.1, tau: float = 2.0):
-    grid = I.periodic_square_quad_grid(n, 0.0, 2 * np.pi)
+                  newton_tol: float = 1e-8, mach: float = 0.1, tau: float = 2.0, periodic: bool = True):
+    grid = I.periodic_square_quad_grid(n, 0.0, 2 * np.pi) if periodic else I.square_quad_grid(n, 2 * np.pi)
     master = I.make_master(2, 1, porder, 2 * porder)
     app = I.PDEApp(nd=2, ncu=4, model="ModelD", preconditioner=preconditioner, NewtonIter=20,
                    NewtonTol=newton_tol, GMRESiter=1000, GMRESrestart=restart, GMREStol=gmres_tol,
                    RBdim=0, ppdegree=1, tau=[tau], torder=3, nstage=3, dt=[dt] * nsteps,
                    physicsparam=[1.4, 1600.0, 0.72, mach], externalparam=[0.0, 0.0])
     cgp = (2, n, n, block, block, 0) if preconditioner == 2 else ()
-    return write_case(datain, grid, master, app, [], [], cgp)
+    # periodic: no face carries a boundary code, but the list of boundary conditions still has
+    # one entry, as the preprocessor writes it for a periodic domain (the reader builds
+    # connectivity only when that list is non-empty, backend/Discretization/readbinaryfiles.cpp:
+    # 390-393).  Otherwise every side gets boundary code 1, FbouHdg = f(u, q).n + tau (u - uhat).
+    return write_case(datain, grid, master, app, [lambda x: True], [1], cgp)
 
 
 def euler3d_vortex_hex(datain: str, n: int = 32, porder: int = 3, nsteps: int = 5, dt: float = 0.05,
@@ -97,7 +102,7 @@ def euler3d_vortex_hex(datain: str, n: int = 32, porder: int = 3, nsteps: int = 
                    NewtonTol=newton_tol, GMRESiter=1000, GMRESrestart=restart, GMREStol=gmres_tol,
                    RBdim=0, ppdegree=1, tau=[1.0 + 1.0 / mach], torder=2, nstage=2, dt=[dt] * nsteps,
                    physicsparam=[1.4, mach], externalparam=[0.0, 0.0])
-    return write_case(datain, grid, master, app, [], [])
+    return write_case(datain, grid, master, app, [lambda x: True], [1])
 
 
 def cdsin2d_quad(datain: str, n: int = 16, porder: int = 3, kappa: float = 0.01, theta: float = 0.0,

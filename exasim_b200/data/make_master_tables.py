@@ -63,4 +63,4 @@ def main(src):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/text2code/text2code")
+    main(sys.argv[1] if len(sys.argv) > 1 else os.path.join(os.environ["EXASIM_REF"], "text2code/text2code"))

@@ -1,0 +1,184 @@
+"""Run the reference's own CPU solver on a datain/ folder.
+
+Test infrastructure: tests/, tests/golden/ and bench.py's reference arm use it as the checker
+and as the CPU baseline; the product never imports it.  The solver is cput2cEXASIM, built from
+the reference tree by oracle/build_ref_full.py into oracle/_ref/ (backend/Main/main.cpp with
+-D_TEXT2CODE: it reads the datain/ folder named by a pdeapp.txt, exasim.hpp:281-298, and
+writes dataout/out*.bin).  The model library (libpdemodelserial.so, generated by the
+reference's text2code) is chosen per run through LD_LIBRARY_PATH.
+
+With debugmode = 1 in app.bin (flag 3, readbinaryfiles.cpp) the reference writes the
+intermediate arrays of its first Newton step (uequation.cpp:182-202, 542-556, 683-693,
+764-774; qequation.cpp:155-167, 474-483; matvec.cpp:114-116, 185-187, 235-237, 385-387;
+solution.cpp:140-184) and stops there with status 1, as designed ("stop for debugging").
+"""
+from __future__ import annotations
+
+import os
+import re
+import select
+import subprocess
+import time
+from dataclasses import dataclass, field
+from typing import Dict, List, Optional, Tuple
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF = os.path.join(HERE, "_ref")
+
+# pdeapp.txt keys the reader requires (readpdeapp.cpp); the solver itself takes only the
+# data paths from this file, everything else comes from datain/app.bin
+_PDEAPP = """model = "ModelD";
+modelfile = "pdemodel.txt";
+meshfile = "grid.bin";
+discretization = "hdg";
+platform = "cpu";
+mpiprocs = 1;
+porder = 1;
+pgauss = 2;
+physicsparam = [1];
+tau = [1];
+boundaryconditions = [1];
+boundaryexpressions = ["x > -1e9"];
+datapath = "{datapath}";
+exasimpath = "{exasimpath}";
+"""
+
+
+def solver_path(strict: bool = False) -> str:
+    return os.path.join(REF, "cput2cEXASIM_strict" if strict else "cput2cEXASIM")
+
+
+def model_dir(model: str) -> str:
+    return os.path.join(REF, "models", model)
+
+
+def available(model: str, strict: bool = False) -> bool:
+    return os.path.exists(solver_path(strict)) and os.path.exists(os.path.join(model_dir(model), "libpdemodelserial.so"))
+
+
+def set_app_flag(datain: str, index: int, value: float, part: int = 2) -> None:
+    """Set entry `index` of part `part` of datain/app.bin (part 2 = flag: 3 debugmode,
+    part 3 = problem: 13 NewtonIter, 14 GMRESiter, 15 GMRESrestart, 16 RBdim;
+    part 8 = solversparam: 0 NewtonTol, 1 GMREStol), the layout of readpdeapp.cpp:820-918."""
+    fn = os.path.join(datain, "app.bin")
+    a = np.fromfile(fn, dtype=np.float64)
+    ls = int(a[0])
+    ns = a[1:1 + ls].astype(np.int64)
+    off = 1 + ls + int(ns[:part - 1].sum())
+    assert index < ns[part - 1], (index, ns[part - 1])
+    a[off + index] = value
+    a.tofile(fn)
+
+
+@dataclass
+class RefRun:
+    returncode: int
+    stdout: str
+    lines: List[Tuple[float, str]]        # (host clock when read, line)
+    wall_s: float
+    dataout: str
+    newton: List[Tuple[int, float, float, float]] = field(default_factory=list)  # it, alpha, nrm0, nrm
+    gmres_iters: List[int] = field(default_factory=list)
+    assembly_ms: List[float] = field(default_factory=list)
+    gmres_ms: List[float] = field(default_factory=list)
+    stage_starts: List[Tuple[int, int, float]] = field(default_factory=list)   # step, stage, clock
+    # per Newton solve (one per steady solve or DIRK stage): [Newton steps, GMRES iterations,
+    # host clock at its first residual line, at its last Newton line]
+    solves: List[List[float]] = field(default_factory=list)
+
+    def dump(self, name: str) -> np.ndarray:
+        """An intermediate array of a debugmode run, e.g. 'uEquationElemSchur_H' (raw FP64)."""
+        return np.fromfile(os.path.join(self.dataout, f"out{name}.bin"), dtype=np.float64)
+
+    def dumps(self) -> List[str]:
+        return sorted(f[3:-4] for f in os.listdir(self.dataout)
+                      if f.startswith("out") and f.endswith(".bin") and "_np" not in f)
+
+    def uhat(self) -> np.ndarray:
+        """outuhat_np0.bin: (ncu, npf, nf) header then the snapshots (solution.h:45-117)."""
+        return np.fromfile(os.path.join(self.dataout, "outuhat_np0.bin"), dtype=np.float64)
+
+    def udg(self) -> np.ndarray:
+        return np.fromfile(os.path.join(self.dataout, "outudg_np0.bin"), dtype=np.float64)
+
+
+_RE_NEWTON = re.compile(r"Newton Iteration: (\d+), Alpha: ([-+0-9.eE]+), Original Norm: ([-+0-9.eEnaif]+),\s+Updated Norm: ([-+0-9.eEnaif]+)")
+_RE_GMRES = re.compile(r"GMRES\(\d+\) converges to the tolerance \S+ within\s+(\d+) iterations")
+_RE_GMRES_NC = re.compile(r"GMRES\(\d+\) does not converge to the tolerance \S+ within\s+(\d+) iterations")
+_RE_ASM = re.compile(r"hdgAssembleLinearSystem time: ([0-9.eE+-]+) miliseconds")
+_RE_GT = re.compile(r"^GMRES time: ([0-9.eE+-]+) miliseconds")
+_RE_STAGE = re.compile(r"Timestep :\s+(\d+),\s+Timestage :\s+(\d+)")
+_RE_SOLVE = re.compile(r"Newton Iteration: 0,\s+Residual Norm")
+
+
+def run(datain: str, model: str, workdir: str, strict: bool = False, timeout: Optional[float] = None,
+        threads: int = 1) -> RefRun:
+    """Run the reference solver on `datain` with model `model`; outputs go to workdir/dataout.
+
+    Lines are read as the solver prints them (its stdout is made line-buffered through
+    stdbuf), each stamped with the host clock, so stage and Newton times can be read off
+    without changing the solver."""
+    if not available(model, strict):
+        raise FileNotFoundError(f"reference solver or model {model} not built (oracle/build_ref_full.py)")
+    workdir = os.path.abspath(workdir)
+    os.makedirs(os.path.join(workdir, "dataout"), exist_ok=True)
+    link = os.path.join(workdir, "datain")
+    if os.path.abspath(datain) != link:
+        if os.path.islink(link):
+            os.unlink(link)
+        os.symlink(os.path.abspath(datain), link)
+    with open(os.path.join(workdir, "run.txt"), "w") as fh:
+        fh.write(_PDEAPP.format(datapath=workdir, exasimpath=os.path.join(REF, "Exasim")))
+    env = dict(os.environ)
+    env["LD_LIBRARY_PATH"] = model_dir(model) + (":" + env["LD_LIBRARY_PATH"] if env.get("LD_LIBRARY_PATH") else "")
+    for k in ("OPENBLAS_NUM_THREADS", "OMP_NUM_THREADS"):
+        env[k] = str(threads)
+    cmd = ["stdbuf", "-oL", "-eL", solver_path(strict), "run.txt"]
+    t0 = time.perf_counter()
+    p = subprocess.Popen(cmd, cwd=workdir, env=env, stdout=subprocess.PIPE, stderr=subprocess.STDOUT,
+                         bufsize=0)
+    lines: List[Tuple[float, str]] = []
+    buf = b""
+    fd = p.stdout.fileno()
+    while True:
+        if timeout is not None and time.perf_counter() - t0 > timeout:
+            p.kill()
+            p.wait()
+            raise TimeoutError(f"reference solver exceeded {timeout} s")
+        r, _, _ = select.select([fd], [], [], 0.5)
+        if not r:
+            if p.poll() is not None:
+                break
+            continue
+        chunk = os.read(fd, 65536)
+        if not chunk:
+            break
+        now = time.perf_counter()
+        buf += chunk
+        *done, buf = buf.split(b"\n")
+        lines += [(now, ln.decode(errors="replace")) for ln in done]
+    if buf:
+        lines.append((time.perf_counter(), buf.decode(errors="replace")))
+    rc = p.wait()
+    res = RefRun(rc, "\n".join(l for _, l in lines), lines, time.perf_counter() - t0, os.path.join(workdir, "dataout"))
+    for t, ln in lines:
+        if _RE_SOLVE.search(ln):
+            res.solves.append([0, 0, t, t])
+        elif (m := _RE_NEWTON.search(ln)):
+            res.newton.append((int(m.group(1)), float(m.group(2)), float(m.group(3)), float(m.group(4))))
+            if res.solves:
+                res.solves[-1][0] += 1
+                res.solves[-1][3] = t
+        elif (m := _RE_GMRES.search(ln)) or (m := _RE_GMRES_NC.search(ln)):
+            res.gmres_iters.append(int(m.group(1)))
+            if res.solves:
+                res.solves[-1][1] += int(m.group(1))
+        elif (m := _RE_ASM.search(ln)):
+            res.assembly_ms.append(float(m.group(1)))
+        elif (m := _RE_GT.search(ln.strip())):
+            res.gmres_ms.append(float(m.group(1)))
+        elif (m := _RE_STAGE.search(ln)):
+            res.stage_starts.append((int(m.group(1)), int(m.group(2)), t))
+    return res

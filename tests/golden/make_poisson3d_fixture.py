@@ -9,13 +9,14 @@ master's nodes exactly as the preprocessor's compute_dgnodes does.
 
 The .bin files are stored byte for byte.  Usage:
     python tests/golden/make_poisson3d_fixture.py [/path/to/Exasim/examples/Poisson/poisson3d]
+(default: $EXASIM_REF/examples/Poisson/poisson3d)
 """
 import os
 import sys
 
 import numpy as np
 
-src = sys.argv[1] if len(sys.argv) > 1 else "/root/reference/examples/Poisson/poisson3d"
+src = sys.argv[1] if len(sys.argv) > 1 else os.path.join(os.environ["EXASIM_REF"], "examples/Poisson/poisson3d")
 out = {}
 for name in ("app", "master", "mesh"):
     out[name] = np.fromfile(os.path.join(src, "datain", name + ".bin"), dtype=np.uint8)

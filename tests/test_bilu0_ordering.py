@@ -32,9 +32,10 @@ def cube_f2e(nd, n, tmp):
 
 def ref_lib():
     if not os.path.exists(REFSO):
-        if not os.path.isdir("/root/reference/backend"):
-            pytest.skip("reference tree absent: the reference ordering cannot be built")
-        subprocess.run(["sh", os.path.join(ROOT, "oracle", "build_ref.sh")], check=True)
+        ref = os.environ.get("EXASIM_REF", "")
+        if not os.path.isdir(os.path.join(ref, "backend")):
+            pytest.skip("reference tree absent (EXASIM_REF): the reference ordering cannot be built")
+        subprocess.run(["sh", os.path.join(ROOT, "oracle", "build_ref.sh"), ref], check=True)
     L = ctypes.CDLL(REFSO)
     P = ctypes.c_void_p
     L.ref_partition.argtypes = [ctypes.c_int, P, ctypes.POINTER(P), ctypes.POINTER(ctypes.c_int),
