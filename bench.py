@@ -13,8 +13,10 @@ where the elimination is compute-bound) and the served stream of 2D convection-d
 requests (`served`).  Inputs are seeded synthetic data with the configurations' shapes.  With --gpus N (torchrun) every rank solves its own
 replica: the path has no data-path collective, so scaling is weak.
 
-Prints one JSON line.  `--impl reference` times the CPU restatement of the reference
-path (numpy + LAPACK on the host cores) on a bounded sample of the workload.
+Prints one JSON line.  `--impl reference` times the reference's own CPU solver
+(cput2cEXASIM, built from the reference tree into oracle/_ref by oracle/build_ref_full.py)
+on the same full workload, one process per usable host core; `cpu_baseline` in the GPU line
+is one such process timed on one stage solve beside the GPU legs.
 """
 from __future__ import annotations
 
@@ -185,34 +187,131 @@ def replicas_value(steps_per_rank, world, total_ms):
     return world * steps_per_rank / (total_ms / 1000.0)
 
 
+REF_MODEL = "convdiff3d"
+
+
+def reference_processes(n):
+    """Concurrent reference processes this host can take: one per usable core, each needing
+    about 8 GB of host memory at 16^3 (7.3 GB resident measured), with a fifth of the free
+    memory left over."""
+    try:
+        cores = len(os.sched_getaffinity(0))
+    except AttributeError:
+        cores = os.cpu_count() or 1
+    avail = None
+    try:
+        with open("/proc/meminfo") as fh:
+            for ln in fh:
+                if ln.startswith("MemAvailable:"):
+                    avail = int(ln.split()[1]) * 1024
+    except OSError:
+        pass
+    per = 8e9 * (n / 16.0) ** 3
+    by_mem = int(0.8 * avail / per) if avail else cores
+    return max(1, min(cores, by_mem, 64)), cores, avail
+
+
+def _reference_case(tmp, n, nsteps):
+    from exasim_b200 import cases
+    d = os.path.join(tmp, f"ref_datain_{n}_{nsteps}")
+    cases.convdiff3d_hex(d, n=n, porder=CFG_P, nsteps=nsteps, dt=0.01)
+    return d
+
+
 def run_reference(args):
-    """The reference path's CPU restatement (the reference itself is not built here), one
-    DIRK-stage solve on the 4^3 sub-mesh per step, reported scaled to the full mesh."""
+    """The reference's own CPU solver (cput2cEXASIM from oracle/_ref, built from the reference
+    tree by oracle/build_ref_full.py with its flags -O3 -ffast-math, Kokkos serial, OpenBLAS with
+    one thread) on the full workload: P concurrent processes, one per usable host core (bounded
+    by host memory), each solving one DIRK(3,3) step (three stage Newton solves) of the 16^3 p=4
+    mesh.  Each process's first stage is its warm-up; its second and third are timed from the
+    stage's header line to the last Newton line of its solve.  value = timed solves / (last timed
+    end - first timed start) over all processes."""
+    from oracle import refsolver as R
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
+    if not R.available(REF_MODEL):
+        print(json.dumps({"impl": "reference", "unavailable": "the reference solver is not built "
+                          "(oracle/build_ref_full.py needs the reference tree)"}), flush=True)
+        return 0
+    P, cores, avail = reference_processes(args.n)
     with tempfile.TemporaryDirectory() as tmp:
-        o = _oracle_case(tmp, SAMPLE_N)
-        if args.warmup > 0:
-            _oracle_stage_times(o, 1)
-        steps = max(1, min(args.steps, 45))
-        per = _oracle_stage_times(o, steps)
-        scale = (SAMPLE_N ** 3) / float(args.n ** 3)
-        v = scale * len(per) / sum(per)
-        sample = (f"oracle/hdg.py (numpy + LAPACK, {os.cpu_count()} host threads): {len(per)} DIRK(3,3) stage "
-                  f"Newton solves on the {SAMPLE_N}^3 sub-mesh ({SAMPLE_N ** 3} of {args.n ** 3} elements), "
-                  "solves/s scaled by element count")
-        line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "solves/s", "n_gpus": args.gpus,
-                "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / v,
-                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-                "data": "synthetic (seeded mesh and source of the configuration's shape)", "config": config(args.n),
-                "latency_ms": {"p50": float(np.percentile(per, 50)) * 1000.0 / scale,
-                               "p99": float(np.percentile(per, 99)) * 1000.0 / scale},
-                "cpu_baseline": {"value": v, "unit": "solves/s", "cores": os.cpu_count(), "kind": "port",
-                                 "sample": sample},
-                "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-        print(json.dumps(line), flush=True)
+        d = _reference_case(tmp, args.n, 1)
+        runs = R.run_many(d, REF_MODEL, [os.path.join(tmp, f"p{i}") for i in range(P)], threads=1,
+                          timeout=3000)
+    bad = [r for r in runs if r.returncode != 0 or len(r.solves) < 3]
+    if bad:
+        print(json.dumps({"impl": "reference", "unavailable": f"reference run failed (rc {bad[0].returncode}): "
+                          + bad[0].stdout[-300:].replace(chr(10), " ")}), flush=True)
+        return 0
+    timed, per = [], []
+    for r in runs:
+        for (_, _, t0), sv in list(zip(r.stage_starts, r.solves))[1:3]:
+            timed.append((t0, sv[3]))
+            per.append(sv[3] - t0)
+    span = max(e for _, e in timed) - min(s0 for s0, _ in timed)
+    v = len(timed) / span
+    asm = [a for r in runs for a in r.assembly_ms]
+    gm = [g for r in runs for g in r.gmres_ms]
+    its = [sv[1] for r in runs for sv in r.solves]
+    sample = (f"cput2cEXASIM (the reference's CPU solver, -O3 -ffast-math, Kokkos serial, OpenBLAS 1 thread): "
+              f"{P} concurrent processes on {cores} usable host cores, each one DIRK(3,3) step of the full "
+              f"{args.n}^3 p={CFG_P} mesh; {len(timed)} timed stage solves (stages 2 and 3 of each process)")
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "solves/s", "n_gpus": args.gpus,
+            "steps": len(timed), "warmup": P, "ms_per_step": 1000.0 / v, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded mesh and source of the configuration's shape)", "config": config(args.n),
+            "latency_ms": {"p50": float(np.percentile(per, 50)) * 1000.0,
+                           "p99": float(np.percentile(per, 99)) * 1000.0},
+            "processes": P, "host_cores": cores, "host_mem_available_bytes": avail,
+            "reference_timers_ms": {"assembly_per_newton": float(np.mean(asm)), "gmres_per_newton": float(np.mean(gm))},
+            "gmres_iters_per_solve": float(np.mean(its)),
+            "newton_steps_per_solve": float(np.mean([sv[0] for r in runs for sv in r.solves])),
+            "cpu_baseline": {"value": v, "unit": "solves/s", "cores": P, "kind": "reference", "sample": sample},
+            "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
     return 0
+
+
+class ReferenceBaseline:
+    """The cpu_baseline of the GPU arm: one cput2cEXASIM process (one thread) on the same full
+    workload, started before the GPU legs and stopped after its first DIRK-stage Newton solve,
+    so it runs beside the GPU work on a host core of its own."""
+
+    def __init__(self, tmp, n):
+        self.n = n
+        self.res = None
+        self.err = None
+        self.t = None
+        from oracle import refsolver as R
+        if not R.available(REF_MODEL):
+            return
+        d = _reference_case(tmp, n, 1)
+
+        def go():
+            try:
+                self.res = R.run_many(d, REF_MODEL, [os.path.join(tmp, "cpu_baseline")], threads=1,
+                                      timeout=1800, stop_after_stages=1)[0]
+            except Exception as e:  # noqa: BLE001 - reported in the line instead
+                self.err = repr(e)
+
+        self.t = threading.Thread(target=go, daemon=True)
+        self.t.start()
+
+    def result(self):
+        from oracle import refsolver as R
+        if self.t is None:
+            return None
+        self.t.join()
+        if self.err or self.res is None or not R.stage_times(self.res):
+            return {"unavailable": self.err or "reference run gave no stage time"}
+        sec = R.stage_times(self.res)[0]
+        return {"value": 1.0 / sec, "unit": "solves/s", "cores": 1, "kind": "reference",
+                "sample": f"cput2cEXASIM (the reference's CPU solver, -O3 -ffast-math, one thread), one process: "
+                          f"the first DIRK(3,3) stage Newton solve of the full {self.n}^3 p={CFG_P} mesh, "
+                          f"{sec:.1f} s (assembly {self.res.assembly_ms[0] / 1000:.1f} s, GMRES "
+                          f"{self.res.gmres_ms[0] / 1000:.2f} s, {self.res.solves[0][1]} iterations)",
+                "seconds_per_solve": sec}
 
 
 # mixed-precision form of the timed solve: each refinement step solves the FP32 system to
@@ -305,6 +404,8 @@ def run_ours(args):
         dist.barrier()
     lib = load_library("convdiff3d")
     with tempfile.TemporaryDirectory() as tmp:
+        cpu_ref = ReferenceBaseline(tmp, args.n) if (rank == 0 and world == 1 and not args.no_cpu_baseline
+                                                     and args.form == "both") else None
         d = make_case(tmp, args.n)
         s64 = HDGSolver(d, "convdiff3d", device=local)
         s32 = HDGSolver(d, "convdiff3d", device=local)
@@ -393,9 +494,12 @@ def run_ours(args):
                 out["served"] = run_served(args, local)
             if args.euler_steps > 0 and world == 1:
                 out["euler3d"] = run_euler(args, local, tmp)
-            if not args.no_cpu_baseline and world == 1:
-                out["cpu_baseline"] = {k: v for k, v in cpu_baseline_sample(tmp, args.n).items()
-                                       if k != "per_solve_s_sample"}
+            if cpu_ref is not None:
+                cb = cpu_ref.result()
+                if cb is None or "unavailable" in cb:
+                    # the reference solver is not built here: the oracle port on a sub-mesh
+                    cb = dict(cpu_baseline_sample(tmp, args.n), reference=cb)
+                out["cpu_baseline"] = cb
             print(json.dumps(out), flush=True)
         s64.close()
         s32.close()

@@ -113,13 +113,7 @@ _RE_STAGE = re.compile(r"Timestep :\s+(\d+),\s+Timestage :\s+(\d+)")
 _RE_SOLVE = re.compile(r"Newton Iteration: 0,\s+Residual Norm")
 
 
-def run(datain: str, model: str, workdir: str, strict: bool = False, timeout: Optional[float] = None,
-        threads: int = 1) -> RefRun:
-    """Run the reference solver on `datain` with model `model`; outputs go to workdir/dataout.
-
-    Lines are read as the solver prints them (its stdout is made line-buffered through
-    stdbuf), each stamped with the host clock, so stage and Newton times can be read off
-    without changing the solver."""
+def _start(datain: str, model: str, workdir: str, strict: bool, threads: int) -> subprocess.Popen:
     if not available(model, strict):
         raise FileNotFoundError(f"reference solver or model {model} not built (oracle/build_ref_full.py)")
     workdir = os.path.abspath(workdir)
@@ -136,34 +130,11 @@ def run(datain: str, model: str, workdir: str, strict: bool = False, timeout: Op
     for k in ("OPENBLAS_NUM_THREADS", "OMP_NUM_THREADS"):
         env[k] = str(threads)
     cmd = ["stdbuf", "-oL", "-eL", solver_path(strict), "run.txt"]
-    t0 = time.perf_counter()
-    p = subprocess.Popen(cmd, cwd=workdir, env=env, stdout=subprocess.PIPE, stderr=subprocess.STDOUT,
-                         bufsize=0)
-    lines: List[Tuple[float, str]] = []
-    buf = b""
-    fd = p.stdout.fileno()
-    while True:
-        if timeout is not None and time.perf_counter() - t0 > timeout:
-            p.kill()
-            p.wait()
-            raise TimeoutError(f"reference solver exceeded {timeout} s")
-        r, _, _ = select.select([fd], [], [], 0.5)
-        if not r:
-            if p.poll() is not None:
-                break
-            continue
-        chunk = os.read(fd, 65536)
-        if not chunk:
-            break
-        now = time.perf_counter()
-        buf += chunk
-        *done, buf = buf.split(b"\n")
-        lines += [(now, ln.decode(errors="replace")) for ln in done]
-    if buf:
-        lines.append((time.perf_counter(), buf.decode(errors="replace")))
-    rc = p.wait()
-    res = RefRun(rc, "\n".join(l for _, l in lines), lines, time.perf_counter() - t0, os.path.join(workdir, "dataout"))
-    for t, ln in lines:
+    return subprocess.Popen(cmd, cwd=workdir, env=env, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, bufsize=0)
+
+
+def _parse(res: RefRun) -> RefRun:
+    for t, ln in res.lines:
         if _RE_SOLVE.search(ln):
             res.solves.append([0, 0, t, t])
         elif (m := _RE_NEWTON.search(ln)):
@@ -182,3 +153,73 @@ def run(datain: str, model: str, workdir: str, strict: bool = False, timeout: Op
         elif (m := _RE_STAGE.search(ln)):
             res.stage_starts.append((int(m.group(1)), int(m.group(2)), t))
     return res
+
+
+def run_many(datain: str, model: str, workdirs: List[str], strict: bool = False, timeout: Optional[float] = None,
+             threads: int = 1, stop_after_stages: Optional[int] = None) -> List[RefRun]:
+    """Run one reference process per work folder on the same datain/, concurrently.
+
+    Lines are read as the solvers print them (stdout made line-buffered through stdbuf), each
+    stamped with the host clock, so stage and Newton times can be read off without changing the
+    solver.  With stop_after_stages = k a process is stopped once its (k+1)-th DIRK stage
+    begins, or after its k-th Newton solve has finished its last step when it prints no
+    further stage (the run then counts as complete)."""
+    t0 = time.perf_counter()
+    procs = [_start(datain, model, w, strict, threads) for w in workdirs]
+    lines: List[List[Tuple[float, str]]] = [[] for _ in procs]
+    bufs = [b""] * len(procs)
+    open_fds = {p.stdout.fileno(): i for i, p in enumerate(procs)}
+    stopped = [False] * len(procs)
+    try:
+        while open_fds:
+            if timeout is not None and time.perf_counter() - t0 > timeout:
+                raise TimeoutError(f"reference solver exceeded {timeout} s")
+            r, _, _ = select.select(list(open_fds), [], [], 0.5)
+            for fd in r:
+                i = open_fds[fd]
+                chunk = os.read(fd, 65536)
+                if not chunk:
+                    del open_fds[fd]
+                    continue
+                now = time.perf_counter()
+                bufs[i] += chunk
+                *done, bufs[i] = bufs[i].split(b"\n")
+                lines[i] += [(now, ln.decode(errors="replace")) for ln in done]
+                if stop_after_stages is not None and not stopped[i]:
+                    nst = sum(1 for _, ln in lines[i] if _RE_STAGE.search(ln))
+                    if nst > stop_after_stages:
+                        procs[i].kill()
+                        stopped[i] = True
+            if not r:
+                for fd, i in list(open_fds.items()):
+                    if procs[i].poll() is not None:
+                        del open_fds[fd]
+    finally:
+        for p in procs:
+            if p.poll() is None and timeout is not None and time.perf_counter() - t0 > timeout:
+                p.kill()
+    out = []
+    for i, p in enumerate(procs):
+        rc = p.wait()
+        if bufs[i]:
+            lines[i].append((time.perf_counter(), bufs[i].decode(errors="replace")))
+        res = RefRun(0 if stopped[i] else rc, "\n".join(l for _, l in lines[i]), lines[i],
+                     time.perf_counter() - t0, os.path.join(os.path.abspath(workdirs[i]), "dataout"))
+        out.append(_parse(res))
+    return out
+
+
+def run(datain: str, model: str, workdir: str, strict: bool = False, timeout: Optional[float] = None,
+        threads: int = 1) -> RefRun:
+    """Run the reference solver on `datain` with model `model`; outputs go to workdir/dataout."""
+    return run_many(datain, model, [workdir], strict, timeout, threads)[0]
+
+
+def stage_times(res: RefRun) -> List[float]:
+    """Seconds per DIRK-stage Newton solve: from the stage's header line (exasim.hpp:440-441) to
+    the last Newton step line of the solve that follows it (solution.cpp:216, 235)."""
+    out = []
+    for (_, _, t0), sv in zip(res.stage_starts, res.solves):
+        if sv[0] > 0:
+            out.append(sv[3] - t0)
+    return out

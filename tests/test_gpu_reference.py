@@ -13,7 +13,8 @@ outputs of its normal run.  The CUDA path reads the same datain/ and must reprod
     cancel at a stage's first Newton step, so both solvers round at the mass term's scale);
   * the final solution: |gpu - reference| / |reference| <= the case's solver tolerance
     (GMREStol for the one-step linear cases, NewtonTol for the others), with the same Newton
-    step count per solve and GMRES counts within 2 of the reference's.
+    step count per solve and GMRES counts within 2 of the reference's (counted as Arnoldi steps:
+    the reference prints one fewer per call that converges inside a restart cycle).
 
 The reference was built with its own flags (-O3 -ffast-math); its spread against an IEEE-strict
 build of itself is 4.8e-13 on H and 2.1e-13 on D^-1 F on the 512-triangle case.
@@ -106,7 +107,10 @@ def test_solution_matches_reference(name, tmp_path):
     gmres_last = s.stats()["gmres_total"]
     s.close()
     ref_newton = [int(v) for v in fx["solves"][:, 0]]
-    ref_gmres_last = int(fx["solves"][-1, 1])
+    # the reference reports one iteration fewer per GMRES call than the Arnoldi steps it takes
+    # when it converges inside a restart cycle (gmres.cpp:535-545 returns j before the loop's
+    # j++), so each of the last solve's calls (one per Newton step) adds one to its count
+    ref_gmres_last = int(fx["solves"][-1, 1]) + int(fx["solves"][-1, 0])
     print(name, f"uhat rel {rel:.2e}", f"udg rel {rel_u:.2e}" if rel_u is not None else "",
           "Newton", list(counts), ref_newton, "GMRES (last solve)", gmres_last, ref_gmres_last)
     assert rel < tol, (name, rel, tol)
