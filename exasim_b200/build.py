@@ -2,7 +2,9 @@
 
 For each model source folder under exasim_b200/models/ (Exasim-generated format) the
 model is turned into device functions (exasim_b200.modelc) and compiled together with
-the model-independent kernels for sm_100a.  Usage:  python -m exasim_b200.build [model ...]
+the model-independent kernels for sm_100a.  Any other folder of text2code output (the
+backend/Model/*.cpp files text2code writes for a pdemodel.txt) builds the same way, as is:
+    python -m exasim_b200.build [model ...] [--source NAME=FOLDER ...]
 """
 from __future__ import annotations
 
@@ -71,8 +73,13 @@ def _compile(src: str, obj: str, extra: Optional[List[str]] = None, deps: Option
     return obj
 
 
-def build(models: Optional[List[str]] = None, jobs: int = 8) -> List[str]:
-    models = models or available_models()
+def build(models: Optional[List[str]] = None, jobs: int = 8, sources: Optional[dict] = None) -> List[str]:
+    """Build the libraries (and executables) of `models` (default: every folder under
+    exasim_b200/models/).  `sources` maps further model names to folders of generated model
+    sources, which are compiled unchanged; those names are built too."""
+    sources = dict(sources or {})
+    models = list(models or ([] if sources else available_models()))
+    models += [m for m in sources if m not in models]
     os.makedirs(LIB, exist_ok=True)
     common_objs = [os.path.join(BUILD, "common", os.path.splitext(f)[0] + ".o") for f in COMMON]
     with cf.ThreadPoolExecutor(max_workers=jobs) as ex:
@@ -82,11 +89,11 @@ def build(models: Optional[List[str]] = None, jobs: int = 8) -> List[str]:
             mdir = os.path.join(BUILD, mname)
             os.makedirs(mdir, exist_ok=True)
             hdr = os.path.join(mdir, f"model_{mname}.cuh")
-            srcs = [os.path.join(MODELS, mname, f) for f in os.listdir(os.path.join(MODELS, mname))
-                    if f.endswith(".cpp")]
+            sdir = sources.get(mname, os.path.join(MODELS, mname))
+            srcs = [os.path.join(sdir, f) for f in os.listdir(sdir) if f.endswith(".cpp")]
             if _newer(hdr, srcs + [modelc.__file__]):
                 with open(hdr, "w") as fh:
-                    fh.write(modelc.generate(os.path.join(MODELS, mname), mname))
+                    fh.write(modelc.generate(sdir, mname))
             obj = os.path.join(mdir, "exa_model.o")
             extra = [f'-DEXA_MODEL_HEADER="{hdr}"', f"-DEXA_MODEL_NS=exa_model_{mname}"]
             mfuts[mname] = ex.submit(_compile, os.path.join(CSRC, "exa_model.cu"), obj, extra, [hdr])
@@ -108,5 +115,11 @@ def build(models: Optional[List[str]] = None, jobs: int = 8) -> List[str]:
 
 
 if __name__ == "__main__":
-    for p in build(sys.argv[1:] or None):
+    names = [a for a in sys.argv[1:] if not a.startswith("--source")]
+    srcs = {}
+    for a in sys.argv[1:]:
+        if a.startswith("--source="):
+            k, v = a[len("--source="):].split("=", 1)
+            srcs[k] = os.path.abspath(v)
+    for p in build(names or None, sources=srcs):
         print(p)
