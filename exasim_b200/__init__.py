@@ -69,6 +69,7 @@ def load_library(model: str) -> ctypes.CDLL:
         "exa_dirk_stage": ([P, I, I, PI, PD], I),
         "exa_stream": ([P, ctypes.POINTER(P)], I),
         "exa_launch_count": ([], LL),
+        "exa_debug_umma_wait_polls": ([LL], None),
         "exa_dgemm_batched": ([I, I, I, D, P, LL, LL, P, LL, LL, D, P, LL, LL, I, P], I),
         "exa_dinverse_batched": ([P, I, LL, I, P, P], I),
         "exa_sinverse_batched": ([P, I, LL, I, P, P], I),

@@ -851,6 +851,13 @@ int exa_gmres(exa_ctx* h, int* iters, double* relerr) {
   EXA_TRY(exa_drv_gmres(h->c, &it, &re));
   if (iters) *iters = it;
   if (relerr) *relerr = re;
+  if (!h->c.last_gmres_converged) {
+    // the reference prints a warning with the relative error and goes on (gmres.cpp:586-594);
+    // a standalone call reports it, with the iterations and error filled in
+    exa_set_error("GMRES(%d) does not converge to the tolerance within %d iterations: relative error %.6e",
+                  h->c.restart, it, re);
+    return EXA_ERR_NOTCONV;
+  }
   return EXA_OK;
 }
 
@@ -1062,6 +1069,8 @@ extern "C" int exa_gemm_3xtf32_batched(int M, int N, int K, double alpha, const 
   }
   return EXA_OK;
 }
+
+extern "C" void exa_debug_umma_wait_polls(long long polls) { exa_umma_set_wait_polls(polls); }
 
 extern "C" int exa_dgemm_tune(int M, int N, int K, int batch, void* stream, int* tile) {
   EXA_TRY(exa_gemm_tune(M, N, K, batch, (cudaStream_t)stream));

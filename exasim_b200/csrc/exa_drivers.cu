@@ -382,6 +382,7 @@ int gmres_body(ExaCtx& c, int* iters_out, double* relerr_out) {
   double nrmb = 0.0, nrmr = 0.0;
   EXA_CUDA(cudaMemsetAsync(c.x, 0, sizeof(double) * N, c.st));
   EXA_TRY(exa_drv_norm(c, c.b, N, &nrmb));
+  c.last_gmres_converged = true;
   if (nrmb < c.newton_tol) {
     *iters_out = 0;
     *relerr_out = 0.0;
@@ -461,6 +462,7 @@ int gmres_body(ExaCtx& c, int* iters_out, double* relerr_out) {
   }
   *iters_out = j;
   *relerr_out = relerr;
+  c.last_gmres_converged = false;
   return EXA_OK;  // not converged: the reference warns and continues (gmres.cpp:586-594)
 }
 }  // namespace

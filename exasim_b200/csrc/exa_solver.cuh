@@ -83,6 +83,7 @@ struct ExaCtx {
   // statistics of the last solve
   int last_gmres_iters = 0, last_newton_iters = 0, total_gmres_iters = 0;
   double last_gmres_relerr = 0.0;
+  bool last_gmres_converged = true;  // the last GMRES call reached its tolerance
   long long kernel_launches = 0;
   ExaProf prof;
   // residual norms of the last Newton / refinement solve: at its start and at its end

@@ -35,10 +35,11 @@ __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count));
 }
 
-// true once the phase with the given parity has completed; false after WAIT_LIMIT polls
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+// true once the phase with the given parity has completed; false after `limit` polls
+// (WAIT_LIMIT unless a caller passes another; 0 polls gives false at once)
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, long long limit = WAIT_LIMIT) {
   const uint32_t a = smem_addr(bar);
-  for (long long i = 0; i < WAIT_LIMIT; ++i) {
+  for (long long i = 0; i < limit; ++i) {
     uint32_t done;
     asm volatile(
         "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"

@@ -17,6 +17,7 @@
 // Every wait on an mbarrier is bounded.  A wait that runs out sets *flag (EXA_UMMA_TIMEOUT),
 // waits (bounded again) for the MMAs already issued, frees the tensor memory and returns.
 #include <algorithm>
+#include <atomic>
 #include <cstdint>
 
 #include "exa_common.cuh"
@@ -331,11 +332,14 @@ __global__ void __launch_bounds__(PNT, 1) umma3_kernel(UGemmP g, int* flag) {
   const float* Bhi = g.B.hi + b1 * g.B.sb + b2 * g.B.sb2 + (long long)(g.n0 >> 3) * 128;
   const float* Blo = g.B.lo + b1 * g.B.sb + b2 * g.B.sb2 + (long long)(g.n0 >> 3) * 128;
 
+  const long long polls = g.main_wait_polls >= 0 ? g.main_wait_polls : WAIT_LIMIT;
+  volatile int* ab = abort_flag;
   if (warp == 0 && lane == 0) {
     // producer: chunk kc into stage kc % PST once the MMAs of chunk kc - PST are done
+    int issued = 0;
     for (int kc = 0; kc < nkc; ++kc) {
       const int s = kc % PST;
-      if (kc >= PST && !mbar_wait(&empty[s], (uint32_t)((kc / PST - 1) & 1))) {
+      if (kc >= PST && (*ab || !mbar_wait(&empty[s], (uint32_t)((kc / PST - 1) & 1), polls))) {
         atomicExch(abort_flag, 1);
         break;
       }
@@ -345,12 +349,19 @@ __global__ void __launch_bounds__(PNT, 1) umma3_kernel(UGemmP g, int* flag) {
       bulk_g2s(st + A_B, Alo + (long long)kc * ngA * 128, bytesA, &full[s]);
       bulk_g2s(st + 2 * A_B, Bhi + (long long)kc * ngBt * 128, bytesB, &full[s]);
       bulk_g2s(st + 2 * A_B + B_B, Blo + (long long)kc * ngBt * 128, bytesB, &full[s]);
+      issued = kc + 1;
     }
+    // after an abort, copies may still be in flight into stages nobody consumes: wait (at the
+    // normal limit) for the latest phase of every stage this loop armed, so that no copy lands
+    // in shared memory after the CTA has left.  Those are the stages' newest phases (nothing
+    // re-arms them later), so a completed one reads as complete.
+    if (*ab)
+      for (int q = max(0, issued - PST); q < issued; ++q) mbar_wait(&full[q % PST], (uint32_t)((q / PST) & 1));
   } else if (warp == 1 && lane == 0) {
     // MMA issuer: hi*hi + hi*lo + lo*hi per K step of 8
     for (int kc = 0; kc < nkc; ++kc) {
       const int s = kc % PST;
-      if (!mbar_wait(&full[s], (uint32_t)((kc / PST) & 1))) {
+      if (*ab || !mbar_wait(&full[s], (uint32_t)((kc / PST) & 1), polls)) {
         atomicExch(abort_flag, 1);
         break;
       }
@@ -494,6 +505,13 @@ int umma3_np(const UGemmP& g, int* flag, cudaStream_t st) {
 
 }  // namespace
 
+namespace {
+std::atomic<long long> g_umma_wait_polls{-1};
+}
+
+void exa_umma_set_wait_polls(long long polls) { g_umma_wait_polls.store(polls); }
+long long exa_umma_wait_polls() { return g_umma_wait_polls.load(); }
+
 long long exa_pack_size(int R, int K) { return (long long)((R + 7) / 8) * ((K + PK - 1) / PK) * 128; }
 
 int exa_pack(const void* src, int src_f64, long long rs, long long ks, long long sb, long long sb2, int batch,
@@ -556,9 +574,11 @@ int exa_gemm_3xtf32(const UGemmP& g, int* flag, cudaStream_t st) {
       return EXA_ERR_ARG;
     }
   }
+  UGemmP h = g;
+  h.main_wait_polls = exa_umma_wait_polls();
   const bool ci64 = g.tci == EXA_T_F64, co64 = g.tco == EXA_T_F64;
-  if (ci64 && !co64) return umma3_np<double, float>(g, flag, st);
-  if (!ci64 && !co64) return umma3_np<float, float>(g, flag, st);
+  if (ci64 && !co64) return umma3_np<double, float>(h, flag, st);
+  if (!ci64 && !co64) return umma3_np<float, float>(h, flag, st);
   exa_set_error("3xtf32 gemm: FP64 output is not instantiated");
   return EXA_ERR_UNSUPPORTED;
 }

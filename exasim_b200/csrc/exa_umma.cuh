@@ -65,6 +65,12 @@ struct UGemmP {
   UPackOut out[2]; int nout;
   int batch, batch2;
   int n0;  // first column: the product covers columns n0 .. n0 + N - 1 of B, C and Cin (set by the host for N > 256)
+  long long main_wait_polls;  // polls per main-loop wait; set by exa_gemm_3xtf32 from exa_umma_wait_polls()
 };
+// Polls per wait in the main loops of the 3xTF32 GEMM (negative: the normal limit).  Tests of the
+// timeout path set 0, so every main-loop wait gives up at once; the waits that drain copies and
+// MMAs already in flight keep the normal limit.
+void exa_umma_set_wait_polls(long long polls);
+long long exa_umma_wait_polls();
 // N above 256 runs as column chunks of at most 256 (one launch each).
 int exa_gemm_3xtf32(const UGemmP& g, int* flag, cudaStream_t st);

@@ -69,7 +69,10 @@ int exa_residual(exa_ctx* ctx, double* norm);
 int exa_matvec(exa_ctx* ctx, const double* v_dev, double* w_dev);
 /* w = P v, ApplyPreconditioner (Preconditioning/preconditioner.cpp:273-295); v != w. */
 int exa_precond(exa_ctx* ctx, const double* v_dev, double* w_dev);
-/* Solve A x = b by restarted GMRES (Solver/gmres.cpp:361-597); x is field "x". */
+/* Solve A x = b by restarted GMRES (Solver/gmres.cpp:361-597); x is field "x".  When it stops at
+ * the iteration cap above its tolerance it returns EXA_ERR_NOTCONV (6) with *iters and *relerr
+ * filled in; the reference prints a warning with that error instead (gmres.cpp:586-594).
+ * Inside exa_newton an unconverged GMRES call continues the Newton step, as in the reference. */
 int exa_gmres(exa_ctx* ctx, int* iters, double* relerr);
 /* q from u and uhat, hdgGetQ (qequation.cpp:372-484). */
 int exa_getq(exa_ctx* ctx);
@@ -170,6 +173,14 @@ int exa_gemm_3xtf32_batched(int M, int N, int K, double alpha, const void* A, in
 int exa_gemm_tf32_batched(int M, int N, int K, double alpha, const void* A, int a_f64, long long lda, long long sA,
                           const void* B, int b_f64, long long ldb, long long sB, double beta, void* C, int c_f64,
                           long long ldc, long long sC, int batch, int* flag_dev, void* stream);
+/* No counterpart in the reference: a test hook for the timeout path of the 3xTF32 tensor-core
+ * GEMM (exa_gemm_3xtf32_batched and the mixed form's element products).  Sets the polls of each
+ * main-loop mbarrier wait in that kernel, process-wide (negative restores the normal 2^22).  With
+ * 0 every such wait gives up at once: the kernel waits (at the normal limit) for the bulk copies
+ * and MMAs it already started, frees its tensor memory, sets its flag to 2 and returns, and the
+ * caller sees the flag (status 3 from the mixed-form solvers).  Not for use while another thread
+ * runs the mixed form. */
+void exa_debug_umma_wait_polls(long long polls);
 /* Number of CUDA kernels this library has launched since it was loaded (all contexts). */
 long long exa_launch_count(void);
 /* Euclidean norms of `ncols` device columns of length n, column j at X + j*ldx, written to

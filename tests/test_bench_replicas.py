@@ -48,10 +48,14 @@ def test_reference_arm_runs_on_rank_zero_only(tmp_path):
     r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--gpus", "2",
                         "--steps", "1", "--warmup", "0"], capture_output=True, text=True, env=env, timeout=600)
     assert r.returncode == 0 and r.stdout.strip() == ""
+    # rank 0 alone runs the arm; here on a 4^3 mesh of the same workload, so it takes seconds
     env = dict(os.environ, RANK="0", WORLD_SIZE="1", LOCAL_RANK="0")
     r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "1",
-                        "--warmup", "0"], capture_output=True, text=True, env=env, timeout=600)
+                        "--warmup", "0", "--n", "4"], capture_output=True, text=True, env=env, timeout=600)
     assert r.returncode == 0, r.stderr[-2000:]
     line = json.loads(r.stdout.strip().splitlines()[-1])
-    assert line["impl"] == "reference" and line["value"] > 0 and line["cpu_baseline"]["kind"] == "port"
-    assert line["e2e"]["h2d_bytes_per_step"] == 0
+    assert line["impl"] == "reference"
+    if "unavailable" in line:
+        pytest.skip("the reference solver is not built here: " + line["unavailable"])
+    assert line["value"] > 0 and line["cpu_baseline"]["kind"] == "reference"
+    assert line["steps"] == 2 * line["processes"] and line["e2e"]["h2d_bytes_per_step"] == 0
