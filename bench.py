@@ -54,6 +54,8 @@ def parse():
     ap.add_argument("--serve-requests", type=int, default=200,
                     help="requests per configuration of the served-stream leg (0 skips it)")
     ap.add_argument("--serve-slots", type=int, default=16)
+    ap.add_argument("--serve-rates", default="100,1000",
+                    help="Poisson arrival rates (1/s) of the served leg; the configuration sweeps 10,30,100,300,1000")
     ap.add_argument("--euler-n", type=int, default=32, help="elements per cube edge of the 3D Euler leg")
     ap.add_argument("--euler-steps", type=int, default=4, help="timed stage solves per form of the 3D Euler leg (0 skips it)")
     return ap.parse_args()
@@ -568,6 +570,9 @@ SERVED_WORKLOAD = ("served stream of 2D convection-diffusion HDG solves: kappa l
                    "to 1e-11; mixed form: FP64 refinement to ||r||/||r0|| <= 1e-8")
 
 
+SERVE_BATCH = 64  # job slots of the batched Krylov steps (exa_server_set_batching)
+
+
 def run_served(args, device):
     """The served-stream leg: the same seeded requests solved (a) one at a time in plain FP64,
     (b) by the server with `slots` overlapping solves in plain FP64 and (c) in the mixed form,
@@ -588,14 +593,20 @@ def run_served(args, device):
         res = [srv.wait(i) for i in ids]
         return time.perf_counter() - t0, res
 
-    out = {"workload": SERVED_WORKLOAD, "requests": R, "slots": args.serve_slots, "hbm_budget_bytes": budget}
+    out = {"workload": SERVED_WORKLOAD, "requests": R, "slots": args.serve_slots, "hbm_budget_bytes": budget,
+           "batch_slots": SERVE_BATCH}
     lines = {}
-    for name, slots, precision in (("plain_fp64_one_at_a_time", 1, 0), ("served_plain_fp64", args.serve_slots, 0),
-                                   ("served_mixed", args.serve_slots, 1)):
-        with Server("cdsin2d", device=device, hbm_budget=budget, slots=slots) as srv:
+    for name, slots, precision, batch in (("plain_fp64_one_at_a_time", 1, 0, 0),
+                                          ("served_plain_fp64", args.serve_slots, 0, 0),
+                                          ("served_mixed", args.serve_slots, 1, 0),
+                                          ("served_batched_plain_fp64", args.serve_slots, 0, SERVE_BATCH),
+                                          ("served_batched_mixed", args.serve_slots, 1, SERVE_BATCH)):
+        with Server("cdsin2d", device=device, hbm_budget=budget, slots=slots, batch=batch) as srv:
             saturated(srv, precision)            # warm: every (n, p) context created once
+            b0 = srv.batch_stats()
             wall, res = saturated(srv, precision)
             st = srv.stats()
+            b1 = srv.batch_stats()
         dofs = [r.uh.size for r in res]
         lat = [r.latency_ms for r in res]
         ratio = max((r.residual / r.residual0) if r.residual0 > 0 else 0.0 for r in res)
@@ -603,29 +614,44 @@ def run_served(args, device):
                        "mean_run_ms": float(np.mean([r.run_ms for r in res])),
                        "gmres_iters_per_solve": float(np.mean([r.gmres for r in res])),
                        "residual_ratio_max": ratio, "contexts_reused": st["contexts_reused"],
-                       "peak_bytes_held": st["peak_bytes_held"]}
+                       "peak_bytes_held": st["peak_bytes_held"],
+                       "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))}}
+        if batch:
+            steps = b1["steps"] - b0["steps"]
+            lines[name]["batched"] = {"steps": steps, "launches": b1["launches"] - b0["launches"],
+                                      "gmres_iters_per_step": sum(r.gmres for r in res) / max(steps, 1),
+                                      "matvec_elements_per_warp": b1["matvec_elements_per_warp"]}
     base = lines["plain_fp64_one_at_a_time"]["solves_per_s"]
     for v in lines.values():
         v["speedup_vs_plain_fp64_one_at_a_time"] = v["solves_per_s"] / base
     out.update(lines)
-    rates = {}
-    with Server("cdsin2d", device=device, hbm_budget=budget, slots=args.serve_slots) as srv:
-        saturated(srv, 1)
-        for rate in (100.0, 1000.0):
-            arr = stream_requests(R, rate, seed=7)
-            t0 = time.perf_counter()
-            ids = []
-            for (ta, n, p, prm), b in zip(arr, blobs):
-                dt = t0 + ta - time.perf_counter()
-                if dt > 0:
-                    time.sleep(dt)
-                ids.append(srv.submit(b, precision=1, **MIXED_SERVED))
-            res = [srv.wait(i) for i in ids]
-            wall = time.perf_counter() - t0
-            lat = [r.latency_ms for r in res]
-            rates[f"{rate:g}/s"] = {"solves_per_s": R / wall, "latency_ms": {"p50": float(np.percentile(lat, 50)),
-                                                                            "p99": float(np.percentile(lat, 99))}}
-    out["poisson_arrivals_mixed"] = rates
+    # the like-for-like ratios: both forms served the same way, each request brought to a true
+    # FP64 residual ratio <= 1e-8 (residual_ratio_max above)
+    out["mixed_vs_plain_fp64_same_slots"] = lines["served_mixed"]["solves_per_s"] / lines["served_plain_fp64"]["solves_per_s"]
+    out["mixed_vs_plain_fp64_batched"] = (lines["served_batched_mixed"]["solves_per_s"] /
+                                          lines["served_batched_plain_fp64"]["solves_per_s"])
+    rates_list = [float(r) for r in str(args.serve_rates).split(",") if r.strip()]
+    for name, precision in (("poisson_arrivals_batched_mixed", 1), ("poisson_arrivals_batched_plain_fp64", 0)):
+        rates = {}
+        with Server("cdsin2d", device=device, hbm_budget=budget, slots=args.serve_slots, batch=SERVE_BATCH) as srv:
+            saturated(srv, precision)
+            for rate in rates_list:
+                arr = stream_requests(R, rate, seed=7)
+                t0 = time.perf_counter()
+                ids = []
+                for (ta, n, p, prm), b in zip(arr, blobs):
+                    dt = t0 + ta - time.perf_counter()
+                    if dt > 0:
+                        time.sleep(dt)
+                    ids.append(srv.submit(b, precision=precision, **(MIXED_SERVED if precision else {})))
+                res = [srv.wait(i) for i in ids]
+                wall = time.perf_counter() - t0
+                lat = [r.latency_ms for r in res]
+                dofs = sum(r.uh.size for r in res)
+                rates[f"{rate:g}/s"] = {"solves_per_s": R / wall, "dofs_per_s": dofs / wall,
+                                        "latency_ms": {"p50": float(np.percentile(lat, 50)),
+                                                       "p99": float(np.percentile(lat, 99))}}
+        out[name] = rates
     return out
 
 
@@ -666,16 +692,19 @@ def pack_floats(R, K):
 
 
 def qelim_mixed_bytes(sz):
-    """Algorithmic bytes of the four 3xTF32 q-elimination GEMMs of one assembly: packed A and B
-    (hi and lo parts) read once, FP64 Cin read, FP32 results and packed results written."""
-    n, m, npe, nd, ne = sz["n"], sz["m"], sz["npe"], sz["nd"], sz["ne"]
-    ndf, kq = sz["npf"] * sz["nfe"], sz["npe"] * sz["nd"]
-    a_b, a_g = 8 * pack_floats(n, kq), 8 * pack_floats(m, kq)
-    b_mc, b_me = 8 * pack_floats(npe, kq), 8 * pack_floats(ndf, kq)
-    pk = 8 * pack_floats(m, n)
-    per = ((a_b + b_mc + 8 * n * npe + 4 * n * npe) + (a_b + b_me + 8 * n * ndf + pk) +
-           (a_g + b_mc + 8 * m * npe + 4 * m * npe + pk) + (a_g + b_me + 8 * m * ndf + 4 * m * ndf))
-    return per * ne
+    """Algorithmic bytes of the four q-elimination products of one assembly, per element
+    D += B MinvC, F -= B MinvE, K += G MinvC and H -= G MinvE (K = npe nd per trace component):
+    every product reads its FP32 operands once (A: M x K, B: K x N, unpadded), reads its FP64
+    Cin and writes its FP32 results: D and H plain, F packed (the B operand of D^-1 F), K plain
+    and packed (the A operand of K D^-1 F)."""
+    npe, nd, ne, ncu = sz["npe"], sz["nd"], sz["ne"], sz.get("ncu", 1)
+    ndf = sz["npf"] * sz["nfe"]
+    n, m, kq = npe * ncu, ndf * ncu, npe * nd
+    d = 4 * ncu * n * kq + 4 * kq * npe + 8 * n * npe * ncu + 4 * n * npe * ncu
+    f = 4 * ncu * n * kq + 4 * kq * ndf + 8 * n * ndf * ncu + 4 * n * ndf * ncu
+    k = 4 * ncu * m * kq + 4 * kq * npe + 8 * m * npe * ncu + 8 * m * npe * ncu
+    h = 4 * ncu * m * kq + 4 * kq * ndf + 8 * m * ndf * ncu + 4 * m * ndf * ncu
+    return (d + f + k + h) * ne
 
 
 def kernel_rooflines(s32, s64, mixed, plain, torch, steps):
@@ -693,7 +722,8 @@ def kernel_rooflines(s32, s64, mixed, plain, torch, steps):
     ms_launch = q_ms / max(launches, 1)
     achieved = qbytes / 4 / (ms_launch * 1e-3) / 1e9 if q_ms > 0 else 0.0
     roofline = {"kernel": "umma3_kernel (q-elimination GEMMs D += B MinvC, F -= B MinvE, K += G MinvC, "
-                          "H -= G MinvE; 3xTF32 on tcgen05, operands by cp.async.bulk)",
+                          "H -= G MinvE; 3xTF32 on tcgen05: FP32 operands by cp.async.bulk, split into TF32 "
+                          "hi and lo parts in shared memory)",
                 "bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                 "frac": achieved / peaks["hbm_gbs"], "peak_source": src,
                 "algorithmic_bytes_per_launch": qbytes / 4, "ms_per_launch": ms_launch, "launches": launches,

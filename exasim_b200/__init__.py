@@ -70,6 +70,7 @@ def load_library(model: str) -> ctypes.CDLL:
         "exa_stream": ([P, ctypes.POINTER(P)], I),
         "exa_launch_count": ([], LL),
         "exa_debug_umma_wait_polls": ([LL], None),
+        "exa_poly_ritz": ([P, I, P, P], I),
         "exa_dgemm_batched": ([I, I, I, D, P, LL, LL, P, LL, LL, D, P, LL, LL, I, P], I),
         "exa_dinverse_batched": ([P, I, LL, I, P, P], I),
         "exa_sinverse_batched": ([P, I, LL, I, P, P], I),
@@ -88,6 +89,8 @@ def load_library(model: str) -> ctypes.CDLL:
         "exa_server_fetch": ([P, LL, P, LL, P, LL, PD], I),
         "exa_server_stats": ([P, PLL], I),
         "exa_server_destroy": ([P], None),
+        "exa_server_set_batching": ([P, I], I),
+        "exa_server_batch_stats": ([P, PLL], I),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)

@@ -167,7 +167,11 @@ int exa_ctx_init(ExaCtx& c, const double* app, long long napp, const double* mas
   if (c.wave) { exa_set_error("wave (ModelW) problems are not supported"); return EXA_ERR_UNSUPPORTED; }
   if (coupled > 0) { exa_set_error("coupled interfaces are not supported"); return EXA_ERR_UNSUPPORTED; }
   if (c.RBdim < 0 || c.RBdim > 64) { exa_set_error("reduced-basis dimension %d outside 0..64", c.RBdim); return EXA_ERR_UNSUPPORTED; }
-  if (c.ppdegree > 1) { exa_set_error("polynomial preconditioner (ppdegree=%d) is not supported", c.ppdegree); return EXA_ERR_UNSUPPORTED; }
+  if (c.ppdegree > 1 && c.ppdegree > c.restart) {
+    exa_set_error("polynomial preconditioner of degree %d needs a GMRES restart of at least that (restart %d)",
+                  c.ppdegree, c.restart);
+    return EXA_ERR_UNSUPPORTED;
+  }
   if (c.preconditioner < 0 || c.preconditioner > 2) { exa_set_error("preconditioner %d: block Jacobi (0), elemental additive Schwarz (1) or block ILU(0) on Cartesian sub-domains (2)", c.preconditioner); return EXA_ERR_UNSUPPORTED; }
   if (c.restart < 1 || c.gmres_maxit < 1) { exa_set_error("GMRES restart/iterations must be positive"); return EXA_ERR_ARG; }
 
@@ -397,6 +401,36 @@ int exa_ctx_init(ExaCtx& c, const double* app, long long napp, const double* mas
   EXA_TRY(dev_alloc(c, &c.gcs, n1));
   EXA_TRY(dev_alloc(c, &c.gsn, n1));
   EXA_TRY(dev_alloc(c, &c.scal, 16));
+  if (c.ppdegree > 1) {
+    // start vector of the polynomial's Arnoldi process: seeded normal values on the trace
+    // nodes, normalised (the reference draws rand() normals on the element nodes, averages
+    // them to a continuous field and takes the face values, setsysstruct.cpp:84-203, 338-352;
+    // exa_set_field("randvect") replaces it)
+    EXA_TRY(dev_alloc(c, &c.randvect, N));
+    EXA_TRY(dev_alloc(c, &c.poly_q, N));
+    EXA_TRY(dev_alloc(c, &c.poly_p, N));
+    std::vector<double> rv((size_t)N);
+    unsigned long long st = 0x9E3779B97F4A7C15ull;
+    auto next = [&]() {  // splitmix64, then a uniform in (0, 1)
+      st += 0x9E3779B97F4A7C15ull;
+      unsigned long long z = st;
+      z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+      z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+      z ^= z >> 31;
+      return ((double)(z >> 11) + 0.5) / 9007199254740992.0;
+    };
+    double nrm = 0.0;
+    for (size_t i = 0; i < (size_t)N; i += 2) {  // Box-Muller pairs
+      const double u1 = next(), u2 = next(), rr = std::sqrt(-2.0 * std::log(u1));
+      rv[i] = rr * std::cos(6.283185307179586 * u2);
+      if (i + 1 < (size_t)N) rv[i + 1] = rr * std::sin(6.283185307179586 * u2);
+    }
+    for (double v : rv) nrm += v * v;
+    nrm = std::sqrt(nrm);
+    for (double& v : rv) v /= nrm;
+    EXA_CUDA(cudaMemcpyAsync(c.randvect, rv.data(), sizeof(double) * (size_t)N, cudaMemcpyHostToDevice, c.st));
+    EXA_CUDA(cudaStreamSynchronize(c.st));
+  }
   if (c.RBdim > 0) {
     EXA_TRY(dev_alloc(c, &c.rbW, N * (size_t)c.RBdim));
     EXA_TRY(dev_alloc(c, &c.rbU, N * (size_t)c.RBdim));
@@ -486,36 +520,38 @@ int exa_ctx_set_precision(ExaCtx& c, int mode) {
     const size_t ne = P.ne, n = P.n, m = P.m, nb = c.neb;
     const int kq = P.npe * P.nd;
     // a packed operand for `count` elements with `per` parts each (batch strides sb = per
-    // parts, sb2 = one part)
-    auto packed = [&](UPacked& u, int R, int K, int TR, size_t count, int per) -> int {
+    // parts, sb2 = one part); split: hi and lo TF32 parts in HBM, else FP32 values split by
+    // the GEMM in shared memory
+    auto packed = [&](UPacked& u, int R, int K, int TR, size_t count, int per, bool split) -> int {
       const long long sz = exa_pack_size(R, K);
       u.R = R; u.K = K; u.TR = TR;
       u.sb = sz * per;
       u.sb2 = sz;
       EXA_TRY(dev_alloc(c, &u.hi, (size_t)sz * per * count));
-      EXA_TRY(dev_alloc(c, &u.lo, (size_t)sz * per * count));
+      if (split) EXA_TRY(dev_alloc(c, &u.lo, (size_t)sz * per * count));
+      else u.lo = nullptr;
       return EXA_OK;
     };
     const int r16m = (P.m + 15) / 16 * 16;
     if (P.ncq > 0) {
       // Minv C, Minv E as B operands: row j (column of the product), k = (l, d) stacked
-      EXA_TRY(packed(c.MCp, P.npe, kq, (P.npe + 15) / 16 * 16, ne, 1));
-      EXA_TRY(packed(c.MEp, P.ndf, kq, (P.ndf + 15) / 16 * 16, ne, 1));
+      EXA_TRY(packed(c.MCp, P.npe, kq, (P.npe + 15) / 16 * 16, ne, 1, false));
+      EXA_TRY(packed(c.MEp, P.ndf, kq, (P.ndf + 15) / 16 * 16, ne, 1, false));
       EXA_TRY(exa_pack(c.MC, 1, kq, 1, (long long)kq * P.npe, 0, (int)ne, 1, c.MCp, c.st));
       EXA_TRY(exa_pack(c.ME, 1, kq, 1, (long long)kq * P.ndf, 0, (int)ne, 1, c.MEp, c.st));
       // B and G as A operands, one part per trace component b
-      EXA_TRY(packed(c.wBp, P.n, kq, 128, nb, P.ncu));
-      EXA_TRY(packed(c.wGp, P.m, kq, 128, nb, P.ncu));
+      EXA_TRY(packed(c.wBp, P.n, kq, 128, nb, P.ncu, false));
+      EXA_TRY(packed(c.wGp, P.m, kq, 128, nb, P.ncu, false));
     }
     if (exa_vol_mat_tc_fits(P)) {
       // basis at the Gauss points: row j (node), k = g
-      EXA_TRY(packed(c.Sp, P.npe, P.nge, 128, 1, 1));
+      EXA_TRY(packed(c.Sp, P.npe, P.nge, 128, 1, 1, true));
       EXA_TRY(exa_pack(c.shapegt, 1, P.nge, 1, 0, 0, 1, 1, c.Sp, c.st));
     }
-    EXA_TRY(packed(c.Dinvp, P.n, P.n, 128, nb, 1));
-    EXA_TRY(packed(c.wFp, P.m, P.n, r16m, nb, 1));
-    EXA_TRY(packed(c.Kp, P.m, P.n, 128, nb, 1));
-    EXA_TRY(packed(c.DinvFp, P.m, P.n, r16m, nb, 1));
+    EXA_TRY(packed(c.Dinvp, P.n, P.n, 128, nb, 1, false));
+    EXA_TRY(packed(c.wFp, P.m, P.n, r16m, nb, 1, false));
+    EXA_TRY(packed(c.Kp, P.m, P.n, 128, nb, 1, false));
+    EXA_TRY(packed(c.DinvFp, P.m, P.n, r16m, nb, 1, false));
     EXA_TRY(dev_alloc(c, &c.H32, ne * m * m));
     EXA_TRY(dev_alloc(c, &c.F32, ne * n * m));
     EXA_TRY(dev_alloc(c, &c.K32, ne * m * n));
@@ -680,6 +716,7 @@ bool field(ExaCtx& c, const char* name, FieldRef& f) {
   else if (s == "b") f = {c.b, N};
   else if (s == "x") f = {c.x, N};
   else if (s == "sdg") f = {c.sdg, n * ne};
+  else if (s == "randvect" && c.randvect) f = {c.randvect, N};
   else if (s == "P" && c.fp64_full)
     f = {c.Pc, c.preconditioner == 0   ? (long long)P.ncu * P.npf * P.ncu * P.npf * P.nf
                : c.preconditioner == 2 ? (long long)P.ncu * P.npf * P.ncu * P.npf * c.bilu.nse * c.bilu.nnz

@@ -444,10 +444,14 @@ __global__ void face_kernel(AsmArgs A, double* Ru, double* Rh, double* D, double
               if (A.Gp.hi) {
                 const long long o = (long long)le * A.Gp.sb + (long long)nqc * A.Gp.sb2 +
                                     exa_tc::pack_off(row_t, pb + npe * d, m, npe * nd, A.Gp.TR);
-                float h, lo;
-                exa_tc::split_tf32(vT[u], h, lo);
-                A.Gp.hi[o] = h;
-                A.Gp.lo[o] = lo;
+                if (A.Gp.lo) {
+                  float h, lo;
+                  exa_tc::split_tf32(vT[u], h, lo);
+                  A.Gp.hi[o] = h;
+                  A.Gp.lo[o] = lo;
+                } else {
+                  A.Gp.hi[o] = (float)vT[u];  // FP32 operand, split by the GEMM on chip
+                }
               } else {
                 Ge[row_t + (long long)m * col] = vT[u];
               }

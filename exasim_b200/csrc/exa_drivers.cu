@@ -7,6 +7,7 @@
 #include <cstring>
 #include <vector>
 
+#include "exa_batch.cuh"
 #include "exa_solver.cuh"
 
 // ---- phase profile: a pool of event pairs, summed into per-phase totals when read or full
@@ -183,7 +184,89 @@ int exa_drv_getq(ExaCtx& c) {
   return exa_k_getq(c.P, c.elemcon, c.MC, c.ME, c.uh, c.udg, c.st);
 }
 
+extern "C" int exa_poly_ritz(const double* H, int m, double* sr, double* si);
+
 namespace {
+
+// out = P A x (x may be out): the matvec into c.w, then the preconditioner
+int pa(ExaCtx& c, const double* x, double* out) {
+  EXA_TRY(exa_drv_matvec(c, x, c.w));
+  return exa_drv_precond(c, c.w, out);
+}
+
+// ApplyPoly (backend/Solver/gmres.cpp:319-357): wv <- s(P A) wv, the polynomial whose roots are
+// the Leja-ordered Ritz values (complex pairs through one real quadratic factor); uses c.w,
+// poly_q and poly_p as work.  Nothing to do without a polynomial preconditioner.
+int apply_poly(ExaCtx& c, double* wv) {
+  if (c.ppdegree <= 1) return EXA_OK;
+  const int m = c.ppdegree;
+  const long long N = c.ndofuhat();
+  double *q = c.poly_q, *p = c.poly_p;
+  const std::vector<double>&sr = c.poly_sr, &si = c.poly_si;
+  EXA_CUDA(cudaMemcpyAsync(q, wv, sizeof(double) * N, cudaMemcpyDeviceToDevice, c.st));
+  EXA_CUDA(cudaMemsetAsync(wv, 0, sizeof(double) * N, c.st));
+  int i = 0;
+  while (i < m - 1) {
+    if (si[i] == 0.0) {
+      EXA_TRY(exa_axpby(wv, q, 1.0 / sr[i], 1.0, N, c.st));
+      EXA_TRY(pa(c, q, p));
+      EXA_TRY(exa_axpby(q, p, -1.0 / sr[i], 1.0, N, c.st));
+      i += 1;
+    } else {
+      const double a = sr[i], b = si[i], a2b2 = a * a + b * b;
+      EXA_TRY(pa(c, q, p));
+      EXA_TRY(exa_axpby(p, q, 2.0 * a, -1.0, N, c.st));
+      EXA_TRY(exa_axpby(wv, p, 1.0 / a2b2, 1.0, N, c.st));
+      if (i < m - 2) {
+        EXA_TRY(pa(c, p, p));
+        EXA_TRY(exa_axpby(q, p, -1.0 / a2b2, 1.0, N, c.st));
+      }
+      i += 2;
+    }
+  }
+  if (si[m - 1] == 0.0) EXA_TRY(exa_axpby(wv, q, 1.0 / sr[m - 1], 1.0, N, c.st));
+  return EXA_OK;
+}
+
+// v_j <- v_j orthogonalised against v_0 .. v_{j-1} by modified Gram-Schmidt and normalised,
+// the coefficients into hcol[0 .. j] (MGS, getpoly.cpp:36-45; the pipelined launches of
+// arnoldi_ops)
+int mgs_column(ExaCtx& c, int j, double* hcol) {
+  const long long N = c.ndofuhat();
+  double* vn = c.V + (long long)j * N;
+  EXA_TRY(exa_dot_partials(vn, c.V, N, c.part_a, c.st));
+  double* pin = c.part_a;
+  double* pout = c.part_b;
+  for (int k = 1; k < j; ++k) {
+    EXA_TRY(exa_mgs_step(vn, c.V + (long long)(k - 1) * N, c.V + (long long)k * N, pin, pout, hcol + k - 1, N, c.st));
+    std::swap(pin, pout);
+  }
+  EXA_TRY(exa_mgs_step(vn, c.V + (long long)(j - 1) * N, nullptr, pin, pout, hcol + j - 1, N, c.st));
+  return exa_mgs_finish(vn, vn, pout, hcol + j, N, c.st);
+}
+
+// getPoly (getpoly.cpp:226-247) and the Ritz-value post-processing of GMRES (gmres.cpp:385-398):
+// m = ppdegree Arnoldi steps of P A from randvect (makeH, getpoly.cpp:208-224), then on the
+// host the harmonic Ritz values in Leja order (exa_poly_ritz)
+int poly_setup(ExaCtx& c) {
+  const int m = c.ppdegree, m1 = m + 1, n1 = c.restart + 1;
+  const long long N = c.ndofuhat();
+  double nr = 0.0;
+  EXA_TRY(exa_drv_norm(c, c.randvect, N, &nr));
+  EXA_TRY(exa_scale(c.V, c.randvect, 1.0 / nr, N, c.st));
+  for (int j = 0; j < m; ++j) {
+    EXA_TRY(pa(c, c.V + (long long)j * N, c.V + (long long)(j + 1) * N));
+    EXA_TRY(mgs_column(c, j + 1, c.hess + (long long)n1 * j));
+  }
+  EXA_CUDA(cudaMemcpyAsync(c.pinned, c.hess, sizeof(double) * n1 * m, cudaMemcpyDeviceToHost, c.st));
+  EXA_CUDA(cudaStreamSynchronize(c.st));
+  std::vector<double> H((size_t)m1 * m);
+  for (int j = 0; j < m; ++j)
+    for (int i = 0; i < m1; ++i) H[(size_t)i + (size_t)m1 * j] = c.pinned[(size_t)i + (size_t)n1 * j];
+  c.poly_sr.assign(m, 0.0);
+  c.poly_si.assign(m, 0.0);
+  return exa_poly_ritz(H.data(), m, c.poly_sr.data(), c.poly_si.data());
+}
 
 // cpuBackSolve (backend/Common/cpuimpl.h:198-208)
 void back_solve(double* y, const double* H, const double* s, int i, int n) {
@@ -210,6 +293,7 @@ int arnoldi_ops(ExaCtx& c, int i, const double* d_nrmb, double* d_relerr, double
   double* hcol = c.hess + (long long)n1 * i;
   EXA_TRY(exa_drv_matvec(c, vi, c.w));
   EXA_TRY(exa_drv_precond(c, c.w, vn));
+  EXA_TRY(apply_poly(c, vn));
   {
     ExaProfScope ps_ortho(c, EXA_PH_ORTHO);
     if (c.ortho == 0) {
@@ -242,7 +326,9 @@ int arnoldi_ops(ExaCtx& c, int i, const double* d_nrmb, double* d_relerr, double
 // direct launches.
 int arnoldi_step(ExaCtx& c, int i, const double* d_nrmb, double* d_relerr, double* rel_pin) {
   const int pr = c.precision == 1 ? 1 : 0;
-  if (!c.use_graphs || c.prof.on || i >= (int)c.arnoldi_graph[pr].size())
+  // a polynomial preconditioner's Ritz values are kernel arguments and change with every
+  // GMRES call, so its steps run as direct launches
+  if (!c.use_graphs || c.prof.on || c.ppdegree > 1 || i >= (int)c.arnoldi_graph[pr].size())
     return arnoldi_ops(c, i, d_nrmb, d_relerr, rel_pin);
   cudaGraphExec_t& ex = c.arnoldi_graph[pr][i];
   if (ex) {
@@ -380,6 +466,8 @@ int gmres_body(ExaCtx& c, int* iters_out, double* relerr_out) {
   const long long N = c.ndofuhat();
   const int nrest = c.restart, maxit = c.gmres_maxit, n1 = nrest + 1;
   double nrmb = 0.0, nrmr = 0.0;
+  // the polynomial's Ritz values, from the current operator (gmres.cpp:385-398)
+  if (c.ppdegree > 1) EXA_TRY(poly_setup(c));
   EXA_CUDA(cudaMemsetAsync(c.x, 0, sizeof(double) * N, c.st));
   EXA_TRY(exa_drv_norm(c, c.b, N, &nrmb));
   c.last_gmres_converged = true;
@@ -402,6 +490,7 @@ int gmres_body(ExaCtx& c, int* iters_out, double* relerr_out) {
   }
   const double tol = std::min(0.1, c.gmres_tol * (nrmb / nrmr));
   EXA_TRY(exa_drv_precond(c, scalar > 1e-12 ? c.w : c.b, c.r));
+  EXA_TRY(apply_poly(c, c.r));
   EXA_TRY(exa_drv_norm(c, c.r, N, &nrmb));
   nrmr = nrmb;
   // device copy of nrmb for the Givens kernel
@@ -452,6 +541,7 @@ int gmres_body(ExaCtx& c, int* iters_out, double* relerr_out) {
     EXA_TRY(exa_drv_matvec(c, c.x, c.w));
     EXA_TRY(exa_axpby(c.w, c.b, 1.0, -1.0, N, c.st));
     EXA_TRY(exa_drv_precond(c, c.w, c.r));
+    EXA_TRY(apply_poly(c, c.r));
     EXA_TRY(exa_drv_norm(c, c.r, N, &nrmr));
     relerr = nrmr / nrmb;
     if (relerr < tol) {
@@ -483,8 +573,19 @@ int exa_drv_check_uflag(ExaCtx& c) {
 }
 
 int exa_drv_gmres(ExaCtx& c, int* iters_out, double* relerr_out) {
-  EXA_TRY(gmres_body(c, iters_out, relerr_out));
+  if (c.batcher && exa_batchable(c)) {
+    EXA_TRY(exa_batcher_gmres(c.batcher, c, iters_out, relerr_out));
+  } else {
+    EXA_TRY(gmres_body(c, iters_out, relerr_out));
+  }
   return exa_drv_check_uflag(c);
+}
+
+int exa_drv_gmres_update(ExaCtx& c, int i) {
+  std::vector<double> ybuf(c.restart + 1);
+  EXA_TRY(update_solution(c, i, ybuf));
+  EXA_CUDA(cudaStreamSynchronize(c.st));  // ybuf's host copy is consumed
+  return EXA_OK;
 }
 
 // NewtonSolver (solution.cpp:125-243)

@@ -178,7 +178,7 @@ int schur_chunk_mixed(ExaCtx& c, int e0, int nb) {
   auto pack_dinv = [&](cudaStream_t s) { return exa_pack(D32, 0, 1, n, (long long)n * n, 0, nb, 1, c.Dinvp, s); };
   auto at = [](UPacked u, long long e) {  // operand of element e of the set
     u.hi += e * u.sb;
-    u.lo += e * u.sb;
+    if (u.lo) u.lo += e * u.sb;
     return u;
   };
   UPackOut toF{c.wFp, 1, 1, 0}, toK{c.Kp, 0, 1, 0};
@@ -322,7 +322,7 @@ int exa_model_assemble(ExaCtx& c, bool jacobian) {
             A.Gp = c.wGp;
             const size_t gp = (size_t)nb * c.wGp.sb;
             EXA_CUDA(cudaMemsetAsync(c.wGp.hi, 0, sizeof(float) * gp, c.st));
-            EXA_CUDA(cudaMemsetAsync(c.wGp.lo, 0, sizeof(float) * gp, c.st));
+            if (c.wGp.lo) EXA_CUDA(cudaMemsetAsync(c.wGp.lo, 0, sizeof(float) * gp, c.st));
           } else {
             EXA_CUDA(cudaMemsetAsync(c.wG, 0, sizeof(double) * (size_t)nb * m * nqn, c.st));
           }

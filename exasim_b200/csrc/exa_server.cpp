@@ -21,6 +21,7 @@
 #include <unordered_map>
 #include <vector>
 
+#include "exa_batch.cuh"
 #include "exa_solver.cuh"
 #include "../../include/exasim_b200.h"
 
@@ -72,6 +73,7 @@ struct exa_server {
   int running = 0;
   bool stop = false;
   std::vector<std::thread> workers;
+  ExaBatcher* batcher = nullptr;  // batched GMRES across the running solves (exa_server_set_batching)
 };
 
 namespace {
@@ -168,7 +170,11 @@ void worker(exa_server* s) {
     } else {
       st = exa_ctx_reset(*ctx, r->app.data(), (long long)r->app.size(), r->sol.data(), (long long)r->sol.size());
     }
-    if (st == EXA_OK) st = run_solve(*ctx, *r);
+    if (st == EXA_OK) {
+      ctx->batcher = s->batcher;
+      st = run_solve(*ctx, *r);
+      ctx->batcher = nullptr;
+    }
     std::string msg = st == EXA_OK ? std::string() : std::string(exa_get_error());
     const long long held = ctx->alloc_bytes;
     const bool keep = (st == EXA_OK && s->reuse);
@@ -351,9 +357,38 @@ void exa_server_destroy(exa_server* s) {
   s->cv.notify_all();
   for (auto& t : s->workers) t.join();
   cudaSetDevice(s->device);
+  exa_batcher_destroy(s->batcher);
   for (auto& q : s->idle) free_ctx(q.c);
   s->idle.clear();
   delete s;
+}
+
+int exa_server_set_batching(exa_server* s, int capacity) {
+  if (!s || capacity < 0) {
+    exa_set_error("server batching: null server or negative capacity");
+    return EXA_ERR_ARG;
+  }
+  std::lock_guard<std::mutex> g(s->mu);
+  if (s->running > 0 || !s->queue.empty()) {
+    exa_set_error("server batching: set it before submitting requests");
+    return EXA_ERR_ARG;
+  }
+  if (s->batcher) {
+    exa_batcher_destroy(s->batcher);
+    s->batcher = nullptr;
+  }
+  if (capacity > 0) EXA_TRY(exa_batcher_create(s->device, capacity, &s->batcher));
+  return EXA_OK;
+}
+
+int exa_server_batch_stats(exa_server* s, long long* out) {
+  if (!s || !out) {
+    exa_set_error("server batch stats: null argument");
+    return EXA_ERR_ARG;
+  }
+  out[0] = out[1] = out[2] = out[3] = 0;
+  if (s->batcher) exa_batcher_stats(s->batcher, out);
+  return EXA_OK;
 }
 
 }  // extern "C"

@@ -68,6 +68,11 @@ struct ExaCtx {
   // images U under the condensed operator, a ring position, and the dot products of a guess
   double *rbW = nullptr, *rbU = nullptr, *rbD = nullptr;
   int rb_cur = 0, rb_removed = 0;
+  // polynomial preconditioner (ppdegree > 1, getpoly.cpp / gmres.cpp:91-130): the start vector
+  // of its Arnoldi process, two work vectors, and the Leja-ordered Ritz values (real and
+  // imaginary parts) of the last GMRES call
+  double *randvect = nullptr, *poly_q = nullptr, *poly_p = nullptr;
+  std::vector<double> poly_sr, poly_si;
   // GMRES: each Arnoldi step index i of the restart cycle (and each precision) runs as one
   // captured CUDA graph from its second use on; none while phase profiling records events
   std::vector<cudaGraphExec_t> arnoldi_graph[2];
@@ -114,6 +119,9 @@ struct ExaCtx {
   std::vector<int> cartgridpart;
   ExaBiluDev bilu;
 
+  // batched GMRES (exa_batch.cu): when set, GMRES calls of this context run through the batcher
+  struct ExaBatcher* batcher = nullptr;
+
   long long ndofuhat() const { return (long long)P.ncu * P.npf * P.nf; }
 };
 
@@ -143,6 +151,8 @@ int exa_drv_newton(ExaCtx& c, int* iters, double* norm);
 int exa_drv_dirk(ExaCtx& c, int nsteps, int* newton_iters_out, int max_out);
 int exa_drv_dirk_stage(ExaCtx& c, int istep, int stage, int* its_out, double* norm_out);
 int exa_drv_norm(ExaCtx& c, const double* x, long long n, double* out);
+// x += V y with y from the back-solve of the Hessenberg system of steps 0..i (gmres.cpp:132-137)
+int exa_drv_gmres_update(ExaCtx& c, int i);
 // mixed-precision form (exa_drivers.cu, exa_api.cu)
 int exa_ctx_set_precision(ExaCtx& c, int mode);
 int exa_drv_newton_mixed(ExaCtx& c, int* iters, double* norm);

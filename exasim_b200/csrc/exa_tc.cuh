@@ -83,6 +83,12 @@ __device__ __forceinline__ void split_tf32(double x, float& hi, float& lo) {
   lo = __uint_as_float(to_tf32((float)(x - (double)hi)));
 }
 
+// hi = tf32(x), lo = tf32(x - hi) for an FP32 x: x - hi is exact in FP32
+__device__ __forceinline__ void split_tf32f(float x, float& hi, float& lo) {
+  hi = __uint_as_float(to_tf32(x));
+  lo = __uint_as_float(to_tf32(x - hi));
+}
+
 __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
   asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
                    smem_addr(dst)),

@@ -268,33 +268,46 @@ __global__ void __launch_bounds__(256) pack_kernel(const TS* src, long long rs, 
       const int lr = 32 * rb + lane;
       if (lr >= ng * 8) break;
       const int row = r0 + lr;
-      float4 h, l;
-      float* hp = &h.x;
-      float* lp = &l.x;
+      double x[4];
 #pragma unroll
       for (int k4 = 0; k4 < 4; ++k4) {
         const int k = k0 + k4;
-        const double x = (row < d.R && k < d.K) ? (double)X[row * rs + k * ks] : 0.0;
-        split_tf32(x, hp[k4], lp[k4]);
+        x[k4] = (row < d.R && k < d.K) ? (double)X[row * rs + k * ks] : 0.0;
       }
       const long long o = ocol + (lr >> 3) * 128 + (lr & 7) * 4;
+      if (!lo) {
+        // FP32 operand (the GEMM splits it on chip)
+        *reinterpret_cast<float4*>(hi + o) = make_float4((float)x[0], (float)x[1], (float)x[2], (float)x[3]);
+        continue;
+      }
+      float4 h, l;
+      split_tf32(x[0], h.x, l.x);
+      split_tf32(x[1], h.y, l.y);
+      split_tf32(x[2], h.z, l.z);
+      split_tf32(x[3], h.w, l.w);
       *reinterpret_cast<float4*>(hi + o) = h;
-      if (lo) *reinterpret_cast<float4*>(lo + o) = l;
+      *reinterpret_cast<float4*>(lo + o) = l;
     }
   }
 }
 
-template <int NP, int PST, typename TCI, typename TCO>
+// SPLIT: both operands are stored as plain FP32 in the packed layout (lo == nullptr); the bulk
+// copies land them in the hi slots, and warps 2 and 3 split each landed chunk in shared memory
+// into hi = tf32(x) (in place) and lo = tf32(x - hi) before the MMAs read it.  Otherwise both
+// operands arrive already split (hi and lo parts in HBM).
+template <int NP, int PST, typename TCI, typename TCO, bool SPLIT>
 __global__ void __launch_bounds__(PNT, 1) umma3_kernel(UGemmP g, int* flag) {
   static_assert(NP % 16 == 0 && NP >= 16 && NP <= 256, "N tile");
   constexpr int A_B = 16 * 512, B_B = (NP / 8) * 512;     // one part (hi or lo) per stage
   constexpr int STAGE = 2 * (A_B + B_B);
   constexpr int TCOLS = NP <= 32 ? 32 : (NP <= 64 ? 64 : (NP <= 128 ? 128 : 256));
+  constexpr int NCONV = 64;                                // converter threads (warps 2, 3)
   constexpr uint32_t IDESC = idesc_tf32(UM, NP);
   extern __shared__ __align__(1024) uint8_t psm[];
   uint64_t* full = reinterpret_cast<uint64_t*>(psm + PST * STAGE);
   uint64_t* empty = full + PST;
-  uint64_t* done = empty + PST;
+  uint64_t* conv = empty + PST;                            // SPLIT: chunk split into hi and lo
+  uint64_t* done = conv + PST;
   uint32_t* tslot = reinterpret_cast<uint32_t*>(done + 1);
   int* abort_flag = reinterpret_cast<int*>(tslot + 1);
 
@@ -317,6 +330,7 @@ __global__ void __launch_bounds__(PNT, 1) umma3_kernel(UGemmP g, int* flag) {
     for (int s = 0; s < PST; ++s) {
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], 1);
+      mbar_init(&conv[s], NCONV);
     }
     mbar_init(done, 1);
     *abort_flag = 0;
@@ -328,9 +342,9 @@ __global__ void __launch_bounds__(PNT, 1) umma3_kernel(UGemmP g, int* flag) {
   const uint32_t tmem = *tslot;
 
   const float* Ahi = g.A.hi + b1 * g.A.sb + b2 * g.A.sb2 + (long long)tA * 16 * nkc * 128;
-  const float* Alo = g.A.lo + b1 * g.A.sb + b2 * g.A.sb2 + (long long)tA * 16 * nkc * 128;
   const float* Bhi = g.B.hi + b1 * g.B.sb + b2 * g.B.sb2 + (long long)(g.n0 >> 3) * 128;
-  const float* Blo = g.B.lo + b1 * g.B.sb + b2 * g.B.sb2 + (long long)(g.n0 >> 3) * 128;
+  const float* Alo = SPLIT ? nullptr : g.A.lo + b1 * g.A.sb + b2 * g.A.sb2 + (long long)tA * 16 * nkc * 128;
+  const float* Blo = SPLIT ? nullptr : g.B.lo + b1 * g.B.sb + b2 * g.B.sb2 + (long long)(g.n0 >> 3) * 128;
 
   const long long polls = g.main_wait_polls >= 0 ? g.main_wait_polls : WAIT_LIMIT;
   volatile int* ab = abort_flag;
@@ -344,11 +358,17 @@ __global__ void __launch_bounds__(PNT, 1) umma3_kernel(UGemmP g, int* flag) {
         break;
       }
       uint8_t* st = psm + s * STAGE;
-      mbar_expect_tx(&full[s], 2 * (bytesA + bytesB));
-      bulk_g2s(st, Ahi + (long long)kc * ngA * 128, bytesA, &full[s]);
-      bulk_g2s(st + A_B, Alo + (long long)kc * ngA * 128, bytesA, &full[s]);
-      bulk_g2s(st + 2 * A_B, Bhi + (long long)kc * ngBt * 128, bytesB, &full[s]);
-      bulk_g2s(st + 2 * A_B + B_B, Blo + (long long)kc * ngBt * 128, bytesB, &full[s]);
+      if (SPLIT) {
+        mbar_expect_tx(&full[s], bytesA + bytesB);
+        bulk_g2s(st, Ahi + (long long)kc * ngA * 128, bytesA, &full[s]);
+        bulk_g2s(st + 2 * A_B, Bhi + (long long)kc * ngBt * 128, bytesB, &full[s]);
+      } else {
+        mbar_expect_tx(&full[s], 2 * (bytesA + bytesB));
+        bulk_g2s(st, Ahi + (long long)kc * ngA * 128, bytesA, &full[s]);
+        bulk_g2s(st + A_B, Alo + (long long)kc * ngA * 128, bytesA, &full[s]);
+        bulk_g2s(st + 2 * A_B, Bhi + (long long)kc * ngBt * 128, bytesB, &full[s]);
+        bulk_g2s(st + 2 * A_B + B_B, Blo + (long long)kc * ngBt * 128, bytesB, &full[s]);
+      }
       issued = kc + 1;
     }
     // after an abort, copies may still be in flight into stages nobody consumes: wait (at the
@@ -361,7 +381,7 @@ __global__ void __launch_bounds__(PNT, 1) umma3_kernel(UGemmP g, int* flag) {
     // MMA issuer: hi*hi + hi*lo + lo*hi per K step of 8
     for (int kc = 0; kc < nkc; ++kc) {
       const int s = kc % PST;
-      if (*ab || !mbar_wait(&full[s], (uint32_t)((kc / PST) & 1), polls)) {
+      if (*ab || !mbar_wait(SPLIT ? &conv[s] : &full[s], (uint32_t)((kc / PST) & 1), polls)) {
         atomicExch(abort_flag, 1);
         break;
       }
@@ -378,6 +398,37 @@ __global__ void __launch_bounds__(PNT, 1) umma3_kernel(UGemmP g, int* flag) {
       umma_commit(&empty[s]);
     }
     umma_commit(done);  // tracks every MMA issued above
+  } else if (SPLIT && warp >= 2) {
+    // converters: once chunk kc has landed, split it in place (hi) and into the lo slots,
+    // make the writes visible to the tensor cores' (async) proxy, then arrive on conv[s]
+    const int ct = tid - 64;
+    for (int kc = 0; kc < nkc; ++kc) {
+      const int s = kc % PST;
+      if (*ab || !mbar_wait(&full[s], (uint32_t)((kc / PST) & 1), polls)) {
+        atomicExch(abort_flag, 1);
+        break;
+      }
+      uint8_t* st = psm + s * STAGE;
+      float4* ah = reinterpret_cast<float4*>(st);
+      float4* al = reinterpret_cast<float4*>(st + A_B);
+      float4* bh = reinterpret_cast<float4*>(st + 2 * A_B);
+      float4* bl = reinterpret_cast<float4*>(st + 2 * A_B + B_B);
+      const int na = (int)(bytesA >> 4), nbq = (int)(bytesB >> 4);
+      for (int i = ct; i < na + nbq; i += NCONV) {
+        float4* hp = i < na ? ah + i : bh + (i - na);
+        float4* lp = i < na ? al + i : bl + (i - na);
+        const float4 x = *hp;
+        float4 h, l;
+        split_tf32f(x.x, h.x, l.x);
+        split_tf32f(x.y, h.y, l.y);
+        split_tf32f(x.z, h.z, l.z);
+        split_tf32f(x.w, h.w, l.w);
+        *hp = h;
+        *lp = l;
+      }
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      mbar_arrive(&conv[s]);
+    }
   }
   __syncwarp();
   const bool fin = mbar_wait(done, 0);
@@ -451,6 +502,15 @@ __global__ void __launch_bounds__(PNT, 1) umma3_kernel(UGemmP g, int* flag) {
             const int gc = c0 + j + g.n0 + (int)b2 * po.cadd;
             if (c0 + j >= g.N) break;
             const long long off = pbase[o] + (long long)(gc >> 4) * png[o] * 128 + ((gc >> 2) & 3) * 32;
+            if (!po.p.lo) {
+              // FP32 operand, split by the consumer on chip
+              const float4 v = make_float4(c0 + j + 0 < g.N ? (float)x[j + 0] : 0.0f,
+                                           c0 + j + 1 < g.N ? (float)x[j + 1] : 0.0f,
+                                           c0 + j + 2 < g.N ? (float)x[j + 2] : 0.0f,
+                                           c0 + j + 3 < g.N ? (float)x[j + 3] : 0.0f);
+              *reinterpret_cast<float4*>(po.p.hi + off) = v;
+              continue;
+            }
             float4 h, l;
             split_tf32(c0 + j + 0 < g.N ? x[j + 0] : 0.0, h.x, l.x);
             split_tf32(c0 + j + 1 < g.N ? x[j + 1] : 0.0, h.y, l.y);
@@ -467,6 +527,10 @@ __global__ void __launch_bounds__(PNT, 1) umma3_kernel(UGemmP g, int* flag) {
             const int gc = (c + g.n0) * po.cmul + (int)b2 * po.cadd;
             const long long off = po.as_b ? pbase[o] + (gc >> 3) * 128 + (gc & 7) * 4
                                            : pbase[o] + (long long)(gc >> 4) * png[o] * 128 + ((gc >> 2) & 3) * 32 + (gc & 3);
+            if (!po.p.lo) {
+              po.p.hi[off] = (float)x[j];
+              continue;
+            }
             float h, l;
             split_tf32(x[j], h, l);
             po.p.hi[off] = h;
@@ -482,11 +546,11 @@ __global__ void __launch_bounds__(PNT, 1) umma3_kernel(UGemmP g, int* flag) {
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TCOLS) : "memory");
 }
 
-template <int NP, int PST, typename TCI, typename TCO>
+template <int NP, int PST, typename TCI, typename TCO, bool SPLIT>
 int launch_umma3(const UGemmP& g, int* flag, cudaStream_t st) {
-  constexpr size_t smem = (size_t)PST * 2 * (16 * 512 + (NP / 8) * 512) + (2 * PST + 1) * 8 + 16;
+  constexpr size_t smem = (size_t)PST * 2 * (16 * 512 + (NP / 8) * 512) + (3 * PST + 1) * 8 + 16;
   static_assert(smem <= 227 * 1024, "tile exceeds shared memory");
-  auto kern = umma3_kernel<NP, PST, TCI, TCO>;
+  auto kern = umma3_kernel<NP, PST, TCI, TCO, SPLIT>;
   EXA_TRY(exa_allow_smem((const void*)kern, smem));
   EXA_CUDA(cudaFuncSetAttribute((const void*)kern, cudaFuncAttributePreferredSharedMemoryCarveout,
                                 (int)cudaSharedmemCarveoutMaxShared));
@@ -496,11 +560,11 @@ int launch_umma3(const UGemmP& g, int* flag, cudaStream_t st) {
   return EXA_OK;
 }
 
-template <typename TCI, typename TCO>
+template <typename TCI, typename TCO, bool SPLIT>
 int umma3_np(const UGemmP& g, int* flag, cudaStream_t st) {
-  if (g.N <= 128) return launch_umma3<128, 3, TCI, TCO>(g, flag, st);
-  if (g.N <= 160) return launch_umma3<160, 3, TCI, TCO>(g, flag, st);
-  return launch_umma3<256, 2, TCI, TCO>(g, flag, st);
+  if (g.N <= 128) return launch_umma3<128, 3, TCI, TCO, SPLIT>(g, flag, st);
+  if (g.N <= 160) return launch_umma3<160, 3, TCI, TCO, SPLIT>(g, flag, st);
+  return launch_umma3<256, 2, TCI, TCO, SPLIT>(g, flag, st);
 }
 
 }  // namespace
@@ -554,7 +618,7 @@ int exa_gemm_3xtf32(const UGemmP& g, int* flag, cudaStream_t st) {
   // B's rows n0 .. n0 + N - 1 are read from one tile of all its rows; chunks start on a group
   if (g.K <= 0 || g.N > 256 || g.A.K != g.K || g.B.K != g.K || g.A.TR != UM || g.B.TR < g.B.R || g.A.R != g.M ||
       g.n0 < 0 || (g.n0 & 7) != 0 || g.B.R < g.n0 + g.N ||
-      !g.A.lo || !g.B.lo || g.nout < 0 || g.nout > 2 || (g.beta != 0.0 && !g.Cin) ||
+      (!g.A.lo) != (!g.B.lo) || g.nout < 0 || g.nout > 2 || (g.beta != 0.0 && !g.Cin) ||
       (g.A.sb | g.A.sb2 | g.B.sb | g.B.sb2) % 4 != 0) {
     exa_set_error("3xtf32 gemm: inconsistent operand description (M %d N %d K %d)", g.M, g.N, g.K);
     return EXA_ERR_ARG;
@@ -569,16 +633,16 @@ int exa_gemm_3xtf32(const UGemmP& g, int* flag, cudaStream_t st) {
     // step are written in aligned quads of k
     const bool bad = po.as_b ? (po.p.TR < po.p.R || po.p.K < g.M)
                              : (po.p.TR != UM || po.p.R < g.M);
-    if (bad || po.p.sb % 4 != 0 || !po.p.hi || !po.p.lo) {
+    if (bad || po.p.sb % 4 != 0 || !po.p.hi) {
       exa_set_error("3xtf32 gemm: packed output %d does not fit the product", o);
       return EXA_ERR_ARG;
     }
   }
   UGemmP h = g;
   h.main_wait_polls = exa_umma_wait_polls();
-  const bool ci64 = g.tci == EXA_T_F64, co64 = g.tco == EXA_T_F64;
-  if (ci64 && !co64) return umma3_np<double, float>(h, flag, st);
-  if (!ci64 && !co64) return umma3_np<float, float>(h, flag, st);
+  const bool ci64 = g.tci == EXA_T_F64, co64 = g.tco == EXA_T_F64, split = !g.A.lo;
+  if (ci64 && !co64) return split ? umma3_np<double, float, true>(h, flag, st) : umma3_np<double, float, false>(h, flag, st);
+  if (!ci64 && !co64) return split ? umma3_np<float, float, true>(h, flag, st) : umma3_np<float, float, false>(h, flag, st);
   exa_set_error("3xtf32 gemm: FP64 output is not instantiated");
   return EXA_ERR_UNSUPPORTED;
 }

@@ -31,6 +31,8 @@ int exa_gemm_tf32(const UGemm& g, int* flag, cudaStream_t st);
 //   tile as K chunks of 16, each chunk as ceil(rows/8) groups of 8 rows x 16 k, each
 //   group as 4 core matrices of 8 rows x 4 k (128 bytes).  Rows past R and k past K are
 //   zero.  Floats per batch entry: ceil(R/8) * ceil(K/16) * 128 when TR is a multiple of 8.
+// With lo == nullptr the operand is stored once, as FP32 values in hi, and the 3xTF32 GEMM
+// splits each chunk into hi and lo parts in shared memory (half the bytes in HBM).
 struct UPacked {
   float* hi;
   float* lo;
@@ -53,7 +55,8 @@ struct UPackOut {
   int cmul, cadd;
 };
 
-// Cout = alpha A B + beta Cin with A (R = M, tiles of 128) and B (R = N, one tile) packed;
+// Cout = alpha A B + beta Cin with A (R = M, tiles of 128) and B (R = N, one tile) packed, both
+// split (hi and lo given) or both FP32 (lo null; split on chip); packed outputs in either form;
 // the products hi*hi + hi*lo + lo*hi on the TF32 tensor cores, accumulated in FP32.
 // Plain output C (FP32 or FP64, column-major) and up to two packed outputs, each optional.
 struct UGemmP {

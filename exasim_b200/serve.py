@@ -38,12 +38,21 @@ class Result:
 
 class Server:
     def __init__(self, model: str, device: int = 0, hbm_budget: int = 16 << 30, slots: int = 8,
-                 reuse_contexts: bool = True):
+                 reuse_contexts: bool = True, batch: int = 0):
+        """batch > 0: the running solves' GMRES calls share batched Arnoldi steps (that many job
+        slots; exa_server_set_batching)."""
         self.lib = load_library(model)
         h = ctypes.c_void_p()
         self._check(self.lib.exa_server_create(device, int(hbm_budget), int(slots), int(bool(reuse_contexts)),
                                                ctypes.byref(h)))
         self.h = h
+        if batch > 0:
+            self._check(self.lib.exa_server_set_batching(self.h, int(batch)))
+
+    def batch_stats(self) -> Dict[str, int]:
+        out = (ctypes.c_longlong * 4)()
+        self._check(self.lib.exa_server_batch_stats(self.h, out))
+        return {k: int(v) for k, v in zip(["steps", "launches", "gmres_calls", "matvec_elements_per_warp"], out)}
 
     def _check(self, st: int):
         if st != 0:

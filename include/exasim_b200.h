@@ -40,7 +40,8 @@ void exa_destroy(exa_ctx* ctx);
 int exa_sizes(exa_ctx* ctx, long long* out);
 
 /* Host copies of named device arrays: "udg", "uh", "H", "F" (D^-1 F after assembly),
- * "Ru", "Rh", "b", "x", "sdg", "P" (preconditioner), "MinvC", "MinvE", "elemg", "faceg".
+ * "Ru", "Rh", "b", "x", "sdg", "P" (preconditioner), "MinvC", "MinvE", "elemg", "faceg", and with
+ * a polynomial preconditioner "randvect" (the start vector of its Arnoldi process, length ndofuhat).
  * n must equal the array length.  MinvC and MinvE hold, per element, Minv*C_d and Minv*E_d
  * with the dimension index next to the row index: [npe, nd, npe] and [npe, nd, npf*nfe].
  * "K", "B" and "Dinv" (the FP64 K and B blocks, and D^-1 after an FP64 assembly) exist when the whole
@@ -181,6 +182,13 @@ int exa_gemm_tf32_batched(int M, int N, int K, double alpha, const void* A, int 
  * caller sees the flag (status 3 from the mixed-form solvers).  Not for use while another thread
  * runs the mixed form. */
 void exa_debug_umma_wait_polls(long long polls);
+/* Host part of the polynomial preconditioner (ppdegree > 1 in app.bin): from the Hessenberg matrix
+ * H [(m+1) x m, column-major] of m Arnoldi steps of the preconditioned operator, the harmonic Ritz
+ * values in Leja order, sr[m] + i si[m] (getPoly and its post-processing in GMRES,
+ * backend/Solver/getpoly.cpp:111-173, 226-247, gmres.cpp:385-398; eigenvalues by the Francis QR
+ * iteration where the reference calls LAPACK dgeev).  GMRES applies the polynomial with these
+ * roots after the preconditioner (ApplyPoly, gmres.cpp:319-357).  2 <= m <= 64; no GPU needed. */
+int exa_poly_ritz(const double* H, int m, double* sr, double* si);
 /* Number of CUDA kernels this library has launched since it was loaded (all contexts). */
 long long exa_launch_count(void);
 /* Euclidean norms of `ncols` device columns of length n, column j at X + j*ldx, written to
@@ -228,6 +236,17 @@ int exa_server_fetch(exa_server* s, long long id, double* udg, long long nudg, d
 int exa_server_stats(exa_server* s, long long* out);
 /* Finishes the running solves, drops queued requests and frees every context. */
 void exa_server_destroy(exa_server* s);
+/* No counterpart in the reference.  Batched Krylov steps across the server's solves: with
+ * capacity > 0 (up to 1024 job slots), every GMRES call of a running solve that uses block
+ * Jacobi, MGS and no reduced basis (condensed blocks up to 64 x 64) joins one batch, whose
+ * Arnoldi steps run as one set of launches (a captured CUDA graph per highest step index) for
+ * all of its jobs; calls join and leave at any step.  Each job's reductions have their own
+ * fixed order, so a result does not depend on the other jobs.  Set before the first submit;
+ * 0 turns batching off. */
+int exa_server_set_batching(exa_server* s, int capacity);
+/* out[4] = {batched steps, kernel launches of those steps, GMRES calls served, elements per warp
+ * of the batched matvec chosen by its autotuner} */
+int exa_server_batch_stats(exa_server* s, long long* out);
 
 #ifdef __cplusplus
 }

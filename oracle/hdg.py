@@ -154,6 +154,9 @@ class HDGOracle:
         # reduced-basis initial guess of GMRES (ptcsolver.cpp:217-236, 374-379;
         # preconditioner.cpp:133-181): the last RBdim Newton updates
         self.RBdim = int(self.problem[16]) if self.problem.size > 16 else 0
+        self.ppdegree = int(self.problem[27]) if self.problem.size > 27 else 0
+        self.randvect = None  # start vector of the polynomial's Arnoldi process (ppdegree > 1)
+        self.poly_sr = self.poly_si = None
         self.rb_W = self.rb_U = None
         self.rb_cur = self.rb_removed = 0
         self.torder, self.nstage = self.problem[3], self.problem[4]
@@ -644,7 +647,47 @@ class HDGOracle:
         x = np.zeros(N) if x is None else x.ravel(order="F").copy()
         shape = b.shape
         mv = lambda v: self.matvec(v.reshape(shape, order="F")).ravel(order="F")
-        pc = lambda v: self.apply_precond(v.reshape(shape, order="F")).ravel(order="F")
+        pc0 = lambda v: self.apply_precond(v.reshape(shape, order="F")).ravel(order="F")
+        pc = pc0
+        if self.ppdegree > 1:
+            # getPoly (getpoly.cpp:208-247) with the Ritz post-processing (gmres.cpp:385-398), then
+            # the preconditioner followed by ApplyPoly (gmres.cpp:319-357) wherever P is applied
+            from oracle.poly import poly_ritz
+            m = self.ppdegree
+            Vp = np.zeros((N, m + 1))
+            Hp = np.zeros((m + 1, m))
+            rv = self.randvect.ravel(order="F")
+            Vp[:, 0] = rv / np.sqrt(np.dot(rv, rv))
+            for jj in range(m):
+                w = pc0(mv(Vp[:, jj]))
+                for k in range(jj + 1):
+                    Hp[k, jj] = np.dot(w, Vp[:, k])
+                    w = w - Hp[k, jj] * Vp[:, k]
+                Hp[jj + 1, jj] = np.sqrt(np.dot(w, w))
+                Vp[:, jj + 1] = w / Hp[jj + 1, jj]
+            sr, si = poly_ritz(Hp)
+            self.poly_sr, self.poly_si = sr, si
+
+            def pc(v):
+                w = pc0(v)
+                q = w.copy()
+                w = np.zeros_like(q)
+                i = 0
+                while i < m - 1:
+                    if si[i] == 0:
+                        w = w + q / sr[i]
+                        q = q - pc0(mv(q)) / sr[i]
+                        i += 1
+                    else:
+                        a2b2 = sr[i] ** 2 + si[i] ** 2
+                        p = 2 * sr[i] * q - pc0(mv(q))
+                        w = w + p / a2b2
+                        if i < m - 2:
+                            q = q - pc0(mv(p)) / a2b2
+                        i += 2
+                if si[m - 1] == 0:
+                    w = w + q / sr[m - 1]
+                return w
         nrest, maxit = self.restart, self.gmres_maxit
         n1 = nrest + 1
         nrmb = np.sqrt(np.dot(bv, bv))

@@ -57,6 +57,12 @@ def _explicit_initial_state(datain, model):
     I.write_sol_bin(os.path.join(datain, "sol.bin"), xdg, udg=u, nc=int(app["ndims"][5]), ncu=ncu)
 
 
+def _with_problem(datain, index, value):
+    """Entry `index` of app.bin's problem part (27: ppdegree) set to value."""
+    R.set_app_flag(datain, index, value, part=3)
+    return datain
+
+
 # name -> (model, writer(datain))
 CASES = {
     # the first benchmark configuration at its full size: 512 perturbed p=3 triangles,
@@ -83,6 +89,9 @@ CASES = {
     # own block size)
     "euler3d_hex3_p2": ("euler3d", lambda d: cases.euler3d_vortex_hex(d, n=3, porder=2, nsteps=1)),
     "euler3d_hex3_p3": ("euler3d", lambda d: cases.euler3d_vortex_hex(d, n=3, porder=3, nsteps=1)),
+    # the first configuration with the polynomial preconditioner of degree 3 (ppdegree, GMRES
+    # applies it after block Jacobi)
+    "poisson2d_tri16_p3_poly3": ("poisson2d", lambda d: _with_problem(cases.poisson2d_tri(d, n=16), 27, 3)),
     # one request of the served stream: 8 x 8 quadrilaterals, p=3, kappa 0.05, theta 0.7
     "cdsin2d_quad8_p3": ("cdsin2d", lambda d: cases.cdsin2d_quad(d, n=8, kappa=0.05, theta=0.7, a=2, b=1)),
 }

@@ -7,6 +7,7 @@ key proj_<name>), and the outputs of a normal run (outuhat, outudg, Newton norms
 """
 from __future__ import annotations
 
+import ctypes
 import glob
 import os
 from typing import Dict, Optional, Tuple
@@ -82,3 +83,48 @@ def first_stage_state(datain: str) -> Optional[Tuple[float, float, np.ndarray]]:
     else:
         u = u.reshape(npe, ncu, ne, order="F")
     return t0 + dt[0] * tt[0], d[0] / dt[0], u * (d[0] / dt[0])
+
+
+def reference_randvect(oracle) -> np.ndarray:
+    """The start vector of the reference's polynomial preconditioner, made as it makes it
+    (backend/Solver/setsysstruct.cpp:54-81, 84-203, 338-352): rand_normal draws (the polar
+    Box-Muller method on C's rand(), from its default seed) on the element nodes [npe, ncu, ne],
+    each component averaged over the element nodes that share a point (ArrayDG2CG), the values
+    of each face's first element at its nodes (GetFaceNodes), normalised.  The libc of this
+    process supplies rand(), reseeded with srand(1) first."""
+    libc = ctypes.CDLL("libc.so.6")
+    libc.rand.restype = ctypes.c_int
+    libc.srand(1)
+    rmax = 2147483647.0
+    npe, ncu, ne = oracle.npe, oracle.ncu, oracle.ne
+    n = npe * ncu * ne
+    vals = np.empty(n)
+    cached = None
+    for i in range(n):
+        if cached is not None:
+            vals[i], cached = cached, None
+            continue
+        while True:
+            x = 2.0 * libc.rand() / rmax - 1.0
+            y = 2.0 * libc.rand() / rmax - 1.0
+            r = x * x + y * y
+            if r != 0.0 and r <= 1.0:
+                break
+        d = np.sqrt(-2.0 * np.log(r) / r)
+        vals[i], cached = x * d, y * d
+    u = vals.reshape(npe, ncu, ne, order="F")
+    # points shared by element nodes: the nodes' coordinates, rounded
+    xs = oracle.xdg.transpose(2, 0, 1).reshape(ne * npe, -1)   # row j + npe * e
+    key = np.round(xs / max(np.abs(xs).max(), 1.0) * 1e9).astype(np.int64)
+    _, cg = np.unique(key, axis=0, return_inverse=True)
+    cg = cg.ravel()
+    out = np.empty_like(u)
+    for k in range(ncu):
+        dg = u[:, k, :].ravel(order="F")                   # index j + npe * e
+        sums = np.zeros(cg.max() + 1)
+        cnt = np.zeros(cg.max() + 1)
+        np.add.at(sums, cg, dg)
+        np.add.at(cnt, cg, 1.0)
+        out[:, k, :] = (sums / cnt)[cg].reshape(npe, ne, order="F")
+    uh = oracle.get_face_nodes(out).ravel(order="F")
+    return uh / np.sqrt(np.dot(uh, uh))

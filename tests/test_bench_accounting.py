@@ -24,15 +24,14 @@ def test_packed_operand_size():
 
 
 def test_qelim_bytes_of_the_benchmark_assembly():
-    """Four 3xTF32 products per assembly at 16^3 hexahedra, p = 4: packed A and B (hi and lo)
-    read once, FP64 Cin read, FP32 and packed outputs written.  The bench reports a quarter
-    of this per launch, 4.69 GB."""
-    total = bench.qelim_mixed_bytes(sizes())
-    assert total == 4 * 4694462464
-    per_elem = total / 16 ** 3
-    # D += B MinvC alone: B (hi, lo) 8 * 16*24*128, MinvC 8 * 16*24*128, Cin 8 * 125^2, D 4 * 125^2
-    d_part = 8 * 16 * 24 * 128 * 2 + 8 * 125 * 125 + 4 * 125 * 125
-    assert d_part < per_elem / 3
+    """Four 3xTF32 products per assembly at 16^3 hexahedra, p = 4 (n = 125, m = 150, K = 375):
+    FP32 operands read once, FP64 Cin read, FP32 results written (F packed, K plain and packed)."""
+    per_elem = bench.qelim_mixed_bytes(sizes()) / 16 ** 3
+    d = 4 * (125 * 375 + 375 * 125) + 8 * 125 * 125 + 4 * 125 * 125
+    f = 4 * (125 * 375 + 375 * 150) + 8 * 125 * 150 + 4 * 125 * 150
+    k = 4 * (150 * 375 + 375 * 125) + 8 * 150 * 125 + 8 * 150 * 125
+    h = 4 * (150 * 375 + 375 * 150) + 8 * 150 * 150 + 4 * 150 * 150
+    assert per_elem == d + f + k + h == 2632500
 
 
 def test_phase_table_per_solve():

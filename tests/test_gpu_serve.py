@@ -84,11 +84,12 @@ def test_failed_request_does_not_stop_the_server(cache):
     good = requests(cache, 2, seed=11)
     bad = [b.copy() for b in good[0]]
     bad[0] = with_params(bad[0], [1.0, 0.0, 0.0, 1.0, 1.0])
-    # an app asking for the polynomial preconditioner, which this path refuses
+    # an app asking for a polynomial preconditioner of higher degree than the GMRES restart,
+    # which this path refuses
     ls = int(bad[0][0])
     nsize = bad[0][1:1 + ls].astype(np.int64)
     off = 1 + ls + int(nsize[:2].sum()) + 27
-    bad[0][off] = 2.0
+    bad[0][off] = 1000.0
     with Server(MODEL, slots=2) as srv:
         with pytest.raises(ExaError) as e:
             srv.wait(srv.submit(bad))

@@ -66,3 +66,20 @@ def test_oracle_matches_reference_first_newton_step(name, tmp_path):
     print(name, {k: f"{v:.1e}" for k, v in errs.items()})
     for k, v in errs.items():
         assert v < (INV_TOL if k in ("F", "Ru") else ASM_TOL), (name, k, v)
+
+
+@pytest.mark.parametrize("name", [n for n in RF.names() if "poly" in n])
+def test_oracle_polynomial_preconditioner_matches_reference(name, tmp_path):
+    """GMRES with the polynomial preconditioner (ppdegree > 1), started from the reference's own
+    Arnoldi vector: the same iteration count as the reference (plus one: it reports one fewer per
+    call that converges inside a restart cycle) and the same solution within the GMRES tolerance."""
+    fx = RF.load(name)
+    d = RF.write_datain(fx, str(tmp_path / "datain"))
+    o = HDGOracle(d, MODELS[str(fx["model"])]())
+    assert o.ppdegree > 1
+    o.randvect = RF.reference_randvect(o)
+    its, _ = o.newton()
+    assert [its] == [int(v) for v in fx["solves"][:, 0]]
+    assert [g.iters for g in o.gmres_log] == [int(fx["solves"][0, 1]) + 1]
+    ref = fx["outuhat"][3:]
+    assert np.linalg.norm(o.uh.ravel(order="F") - ref) / np.linalg.norm(ref) < o.gmres_tol
