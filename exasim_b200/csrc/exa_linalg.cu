@@ -904,9 +904,10 @@ int exa_inverse_ws(float* A, int n, long long stride, int batch, float* ws, int*
 }
 
 // ----------------------------------------------------------------------------------
-// vector kernels.  A fixed grid of VB blocks (two per SM) covers every vector with a
-// grid-stride loop; each reduction leaves VB partial sums that the consumer kernel
-// adds up in index order, so results do not depend on scheduling.
+// vector kernels.  A vector of n entries runs on vec_grid(n) blocks (one entry per thread,
+// at most VB = two blocks per SM) with a grid-stride loop; each reduction leaves one partial
+// sum per block, which the consumer kernel adds up in index order, so results do not depend
+// on scheduling.
 // ----------------------------------------------------------------------------------
 namespace {
 constexpr int VB = 296, VT = 256;
@@ -1192,7 +1193,9 @@ __global__ void __launch_bounds__(VT) colnrm_partial_kernel(const double* X, lon
   if (threadIdx.x == 0) part[j * VB + blockIdx.x] = s;
 }
 
-// out[j] = sqrt(sum of column j's VB partials), one block per column
+// out[j] = sqrt(sum of column j's VB partials), one block per column.  The partial kernel runs
+// VB blocks where the context's norm runs vec_grid(n): entry i lands in block (i / VT) mod VB
+// in both, and the blocks past vec_grid(n) hold exact zeros, so both sums give the same bits.
 __global__ void __launch_bounds__(VT) colnrm_finish_kernel(const double* part, double* out) {
   double s = sum_partials(part + blockIdx.x * VB);
   if (threadIdx.x == 0) out[blockIdx.x] = sqrt(s);

@@ -60,8 +60,16 @@ int inverse_beside(ExaCtx& c, InverseJoin& j, Fn&& fn) {
   EXA_CUDA(cudaStreamWaitEvent(c.st2, c.ev_q, 0));
   j.pending = true;
   const int st = fn(c.st2);
-  // recorded whatever fn returned, so the join covers whatever it enqueued
-  EXA_CUDA(cudaEventRecord(c.ev_inv, c.st2));
+  // recorded whatever fn returned, so the join covers whatever it enqueued; if the record
+  // itself fails, the second stream is drained here, so that nothing left on it can outlive
+  // this step (the join would otherwise wait on the previous step's event)
+  const cudaError_t e = cudaEventRecord(c.ev_inv, c.st2);
+  if (e != cudaSuccess) {
+    j.pending = false;
+    cudaStreamSynchronize(c.st2);
+    exa_set_error("cudaEventRecord on the second stream: %s", cudaGetErrorString(e));
+    return EXA_ERR_CUDA;
+  }
   return st;
 }
 

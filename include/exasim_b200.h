@@ -199,7 +199,9 @@ long long exa_launch_count(void);
  * array per device (64 columns x 296 blocks of doubles, 151,552 bytes); ncols > 64 returns
  * EXA_ERR_ARG (1).  The first call on each device, with that device current, looks up the
  * array's address (which can load this library's device code), so make it before any stream
- * capture starts.  Nothing needs zeroing beforehand.  Calls whose kernels can overlap (other
+ * capture starts.  That address is kept for the life of the process and belongs to the device's
+ * primary context: after cudaDeviceReset, or from another driver context on the same device,
+ * calls are not valid.  Nothing needs zeroing beforehand.  Calls whose kernels can overlap (other
  * streams with no ordering, several host threads) race on the shared array: order them. */
 int exa_dnrm2_cols_fixed(const double* X, long long n, long long ldx, int ncols, double* out_dev, void* stream);
 

@@ -60,3 +60,32 @@ def test_fixed_scratch_norms_match_residual_norm(tmp_path):
     assert rc == 1 and "65" in L.exa_last_error().decode()
     assert L.exa_launch_count() == before
     s.close()
+
+
+def test_fixed_scratch_norms_at_its_limits():
+    """The full 64 columns, strided (ldx > n), of a vector long enough that the grid-stride
+    loop runs more than once per block (n > 296 * 256), and n = 0, whose norms are 0; each on
+    two calls in a row."""
+    import torch
+    B.build(["poisson2d"])
+    from exasim_b200 import load_library
+    L = load_library("poisson2d")
+    n, ldx, nc = 200_003, 200_011, 64
+    rng = np.random.default_rng(9)
+    X = torch.tensor(rng.standard_normal((nc, ldx)), dtype=torch.float64, device="cuda")
+    out = torch.full((nc + 1,), -1.0, dtype=torch.float64, device="cuda")
+    ref = np.linalg.norm(X.cpu().numpy()[:, :n], axis=1)
+    for _ in range(2):
+        rc = L.exa_dnrm2_cols_fixed(ctypes.c_void_p(X.data_ptr()), n, ldx, nc, ctypes.c_void_p(out.data_ptr()), None)
+        assert rc == 0, L.exa_last_error().decode()
+        torch.cuda.synchronize()
+        got = out.cpu().numpy()
+        assert np.abs(got[:nc] - ref).max() <= 1e-13 * ref.max()
+        assert got[nc] == -1.0
+    for _ in range(2):
+        out.fill_(-1.0)
+        rc = L.exa_dnrm2_cols_fixed(ctypes.c_void_p(X.data_ptr()), 0, ldx, 3, ctypes.c_void_p(out.data_ptr()), None)
+        assert rc == 0, L.exa_last_error().decode()
+        torch.cuda.synchronize()
+        got = out.cpu().numpy()
+        assert np.all(got[:3] == 0.0) and got[3] == -1.0
