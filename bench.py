@@ -660,10 +660,10 @@ def run_served(args, device):
 # workload: 4.458 GB for 1000 elements; it scales with the element count (each element's
 # blocks are read once), so per launch and element it is 4.458e9 / 1000 / 4 bytes.
 QELIM_TRAFFIC_PER_ELEMENT_LAUNCH = 4.458e9 / 1000 / 4
-# The same for the mixed form's four 3xTF32 q-elimination launches (umma3_kernel), one ncu
-# capture on the 10^3 mesh: 0.969, 1.152, 1.222 and 1.198 GB read + written, mean 1.135 GB
-# per launch for 1000 elements.
-QELIM_MIXED_TRAFFIC_PER_ELEMENT_LAUNCH = 1.1351e9 / 1000
+# The same for the mixed form's four 3xTF32 q-elimination launches (umma3_kernel, FP32
+# operands split on chip), one ncu capture on the 10^3 mesh: 0.564, 0.642, 0.709 and 0.721 GB
+# read + written, mean 0.659 GB per launch for 1000 elements (the algorithmic 0.658).
+QELIM_MIXED_TRAFFIC_PER_ELEMENT_LAUNCH = 0.6590e9 / 1000
 
 
 def fp64_gemm_peak(torch):

@@ -7,6 +7,7 @@
 
 #include "exa_solver.cuh"
 #include "exa_bilu0.h"
+#include "exa_tc.cuh"
 #include "exa_umma.cuh"
 #include "../../include/exasim_b200.h"
 
@@ -518,7 +519,7 @@ int exa_ctx_set_precision(ExaCtx& c, int mode) {
   if (mode == 1 && c.H32 == nullptr) {
     const ExaDims& P = c.P;
     const size_t ne = P.ne, n = P.n, m = P.m, nb = c.neb;
-    const int kq = P.npe * P.nd;
+    const int kq = P.npe * P.nd, kg = exa_tc::qk_group(P.npe), kq4 = kg * P.nd;
     // a packed operand for `count` elements with `per` parts each (batch strides sb = per
     // parts, sb2 = one part); split: hi and lo TF32 parts in HBM, else FP32 values split by
     // the GEMM in shared memory
@@ -534,14 +535,15 @@ int exa_ctx_set_precision(ExaCtx& c, int mode) {
     };
     const int r16m = (P.m + 15) / 16 * 16;
     if (P.ncq > 0) {
-      // Minv C, Minv E as B operands: row j (column of the product), k = (l, d) stacked
-      EXA_TRY(packed(c.MCp, P.npe, kq, (P.npe + 15) / 16 * 16, ne, 1, false));
-      EXA_TRY(packed(c.MEp, P.ndf, kq, (P.ndf + 15) / 16 * 16, ne, 1, false));
-      EXA_TRY(exa_pack(c.MC, 1, kq, 1, (long long)kq * P.npe, 0, (int)ne, 1, c.MCp, c.st));
-      EXA_TRY(exa_pack(c.ME, 1, kq, 1, (long long)kq * P.ndf, 0, (int)ne, 1, c.MEp, c.st));
-      // B and G as A operands, one part per trace component b
-      EXA_TRY(packed(c.wBp, P.n, kq, 128, nb, P.ncu, false));
-      EXA_TRY(packed(c.wGp, P.m, kq, 128, nb, P.ncu, false));
+      // Minv C, Minv E as B operands: row j (column of the product), k = (l, d) at
+      // l + qk_group(npe) d (zeros between the groups)
+      EXA_TRY(packed(c.MCp, P.npe, kq4, (P.npe + 15) / 16 * 16, ne, 1, false));
+      EXA_TRY(packed(c.MEp, P.ndf, kq4, (P.ndf + 15) / 16 * 16, ne, 1, false));
+      EXA_TRY(exa_pack(c.MC, 1, kq, 1, (long long)kq * P.npe, 0, (int)ne, 1, c.MCp, c.st, kg, P.npe));
+      EXA_TRY(exa_pack(c.ME, 1, kq, 1, (long long)kq * P.ndf, 0, (int)ne, 1, c.MEp, c.st, kg, P.npe));
+      // B and G as A operands, one part per trace component b, with the same K
+      EXA_TRY(packed(c.wBp, P.n, kq4, 128, nb, P.ncu, false));
+      EXA_TRY(packed(c.wGp, P.m, kq4, 128, nb, P.ncu, false));
     }
     if (exa_vol_mat_tc_fits(P)) {
       // basis at the Gauss points: row j (node), k = g
@@ -726,7 +728,8 @@ bool field(ExaCtx& c, const char* name, FieldRef& f) {
   else if (s == "elemg") f = {c.elemg, (long long)P.elemg_stride() * ne};
   else if (s == "faceg") f = {c.faceg, (long long)P.faceg_stride() * P.nfe * ne};
   else if (s == "K" && c.neb == P.ne) f = {c.wK, m * n * ne};
-  else if (s == "B" && c.neb == P.ne) f = {c.wB, n * (long long)P.npe * P.nd * P.ncu * ne};
+  else if (s == "B" && c.neb == P.ne && !(c.precision == 1 && c.Sp.hi))  // else B exists only packed in FP32
+    f = {c.wB, n * (long long)P.npe * P.nd * P.ncu * ne};
   else if (s == "Dinv" && c.neb == P.ne) f = {c.wD, n * n * ne};
   else if (s == "H32" && c.H32) f = {nullptr, m * m * ne, c.H32};
   else if (s == "F32" && c.F32) f = {nullptr, n * m * ne, c.F32};

@@ -30,6 +30,9 @@ struct AsmArgs {
   // mixed form: G goes straight into the packed 3xTF32 operand of the q elimination (one
   // part per trace component) instead of the FP64 G; unused when Gp.hi is null
   UPacked Gp;
+  // mixed form with the tensor-core volume kernel: B is packed the same way (written by the
+  // volume kernel, face terms added here) instead of the FP64 B; unused when Bp.hi is null
+  UPacked Bp;
 };
 
 // ----------------------------------------------------------------------------------
@@ -403,6 +406,7 @@ __global__ void face_kernel(AsmArgs A, double* Ru, double* Rh, double* D, double
       // formed once per g and shared by every column q = k + ncu c, taken QC at a time
       constexpr int QC = 4;
       const int nq = ncu * nc;
+      const int qg = exa_tc::qk_group(npe);  // K group of the packed B and G
       for (int ab = threadIdx.x; ab < npf * npf; ab += blockDim.x) {
         const int a = ab % npf, b = ab / npf;
         const int pa = pl[a], pb = pl[b];
@@ -440,10 +444,16 @@ __global__ void face_kernel(AsmArgs A, double* Ru, double* Rh, double* D, double
             } else {
               const int qc = c - ncu, nqc = qc % ncu, d = qc / ncu;
               const long long col = pb + (long long)npe * d + (long long)npe * nd * nqc;
-              Be[row_e + (long long)n * col] += vq[u];
+              if (A.Bp.hi) {
+                float* bp = A.Bp.hi + (long long)le * A.Bp.sb + (long long)nqc * A.Bp.sb2 +
+                            exa_tc::pack_off(row_e, pb + qg * d, n, qg * nd, A.Bp.TR);
+                *bp += (float)vq[u];
+              } else {
+                Be[row_e + (long long)n * col] += vq[u];
+              }
               if (A.Gp.hi) {
                 const long long o = (long long)le * A.Gp.sb + (long long)nqc * A.Gp.sb2 +
-                                    exa_tc::pack_off(row_t, pb + npe * d, m, npe * nd, A.Gp.TR);
+                                    exa_tc::pack_off(row_t, pb + qg * d, m, qg * nd, A.Gp.TR);
                 if (A.Gp.lo) {
                   float h, lo;
                   exa_tc::split_tf32(vT[u], h, lo);

@@ -40,8 +40,10 @@ int exa_k_gemv32(int M, int K, int batch, double alpha, const float* A, long lon
 // with S = shapegt[:, :, 0] packed as a B operand (rows npe, K nge); npe, nge <= 128.
 struct UPacked;
 bool exa_vol_mat_tc_fits(const ExaDims& P);
+// With Bp.hi set, B goes into Bp (the packed FP32 A operand of the q elimination, one part per
+// trace component: row i + npe k, k = j + npe d) instead of B.
 int exa_k_vol_mat_tc(const ExaDims& P, const double* shapegw, const UPacked& Sp, const double* rgJ, double* D,
-                     double* B, int nb, int* flag, cudaStream_t st);
+                     double* B, const UPacked& Bp, int nb, int* flag, cudaStream_t st);
 // Block ILU(0) preconditioner on Cartesian sub-domains (Exasim preconditioner = 2): the
 // schedule built on the host (exa_bilu0.h) in device memory, and the sub-domain results.
 struct ExaBiluDev {

@@ -191,17 +191,19 @@ int schur_chunk_mixed(ExaCtx& c, int e0, int nb) {
   };
   UPackOut toF{c.wFp, 1, 1, 0}, toK{c.Kp, 0, 1, 0};
   if (P.ncq > 0) {
-    const long long kq = (long long)npe * nd;
-    {
-      // B and G per trace component: row r, k = (l, d) at column l + npe*d + npe*nd*b
+    const long long kq = (long long)npe * nd;   // the contraction, and B's columns per component
+    const int kg = exa_tc::qk_group(npe);       // packed K: a group of kg per gradient component
+    if (!c.Sp.hi) {
+      // B per trace component b: row r, packed k = l + kg*d from column l + npe*d + npe*nd*b.
+      // With the tensor-core volume kernel B is already packed (volume and face kernels write
+      // it so), and G always is (the face kernel writes it in this layout in the mixed form)
       ExaProfScope pp(c, EXA_PH_PACK);
-      EXA_TRY(exa_pack(c.wB, 1, 1, n, (long long)n * nqn, (long long)n * kq, nb, ncu, c.wBp, c.st));
-      // G is already packed: the face kernel writes it in this layout in the mixed form
+      EXA_TRY(exa_pack(c.wB, 1, 1, n, (long long)n * nqn, (long long)n * kq, nb, ncu, c.wBp, c.st, kg, npe));
     }
     ExaProfScope ps(c, EXA_PH_QELIM);
     exa_prof_flops(c, EXA_PH_QELIM, 2.0 * nb * ncu * (double)npe * nd * (double)(n + m) * (npe + ndf));
     UGemmP u{};
-    u.batch = nb; u.batch2 = ncu; u.K = (int)kq; u.beta = 1.0;
+    u.batch = nb; u.batch2 = ncu; u.K = kg * nd; u.beta = 1.0;
     u.tci = EXA_T_F64; u.tco = EXA_T_F32;
     // D(:, j + npe*b) = D + B_b MinvC
     u.M = n; u.N = npe; u.alpha = 1.0;
@@ -311,7 +313,15 @@ int exa_model_assemble(ExaCtx& c, bool jacobian) {
         vol_points_kernel<ExaModel, true><<<nb, tpb_v, vs, c.st>>>(A, Ruc, c.wRg);
         EXA_LAUNCH_CHECK();
         if (c.precision == 1 && c.Sp.hi) {
-          EXA_TRY(exa_k_vol_mat_tc(P, c.shapegw, c.Sp, c.wRg, c.wD, c.wB, nb, c.d_uflag, c.st));
+          // B straight into its packed FP32 form (the face kernel adds its terms there too).
+          // The volume kernel assigns every entry of B, so only the layout's padding needs
+          // zeros, and nothing writes there after the zeroing at allocation.
+          UPacked bp{};
+          if (nqn > 0 && P.ncq > 0) {
+            bp = c.wBp;
+            A.Bp = c.wBp;
+          }
+          EXA_TRY(exa_k_vol_mat_tc(P, c.shapegw, c.Sp, c.wRg, c.wD, c.wB, bp, nb, c.d_uflag, c.st));
         } else {
           const int tiles = exa_ceil_div(P.npe, 64);
           dim3 grid(tiles * tiles, nb, P.ncu * P.nc);
@@ -326,11 +336,11 @@ int exa_model_assemble(ExaCtx& c, bool jacobian) {
         EXA_CUDA(cudaMemsetAsync(c.wK, 0, sizeof(double) * (size_t)nb * m * n, c.st));
         if (nqn > 0 && P.ncq > 0) {
           if (c.precision == 1 && c.wGp.hi) {
-            // G written packed by the face kernel (its zeros included, as the pack would)
+            // G written packed by the face kernel.  Each element slot gets the same entries
+            // assigned at every assembly (face l's trace rows against face l's nodes, the same
+            // master-face node lists for every element); the rest of G is structurally zero and
+            // keeps the zeros of the allocation, since nothing else writes there.
             A.Gp = c.wGp;
-            const size_t gp = (size_t)nb * c.wGp.sb;
-            EXA_CUDA(cudaMemsetAsync(c.wGp.hi, 0, sizeof(float) * gp, c.st));
-            if (c.wGp.lo) EXA_CUDA(cudaMemsetAsync(c.wGp.lo, 0, sizeof(float) * gp, c.st));
           } else {
             EXA_CUDA(cudaMemsetAsync(c.wG, 0, sizeof(double) * (size_t)nb * m * nqn, c.st));
           }

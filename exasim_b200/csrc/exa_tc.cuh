@@ -67,6 +67,12 @@ __device__ __forceinline__ void umma_commit(uint64_t* bar) {
 
 constexpr int PK = 16;  // K per chunk of a packed operand
 
+// K index of the q elimination's packed operands (B, G, Minv C, Minv E): node j of gradient
+// component d sits at k = j + qk_group(npe) d.  Groups are rounded up to whole quads of k, so
+// each starts on a 16-byte boundary of a core-matrix row and a writer can store float4s; the
+// padding holds zeros in both operands of a product.
+__host__ __device__ inline int qk_group(int npe) { return (npe + 3) & ~3; }
+
 __host__ __device__ inline long long pack_off(int row, int k, int R, int K, int TR) {
   const int nkc = (K + PK - 1) / PK;
   const int t = row / TR, rl = row - t * TR;

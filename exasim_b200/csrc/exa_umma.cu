@@ -248,7 +248,8 @@ constexpr int PNT = 128;  // threads (4 warps: epilogue lanes 0..127)
 // divisions in the loop.
 template <typename TS>
 __global__ void __launch_bounds__(256) pack_kernel(const TS* src, long long rs, long long ks, long long sb,
-                                                   long long sb2, int batch2, int ntiles, UPacked d) {
+                                                   long long sb2, int batch2, int ntiles, UPacked d, int kgp,
+                                                   int kgs) {
   const int t = blockIdx.x % ntiles;
   const long long e = blockIdx.x / ntiles;
   const long long b2 = e % batch2, b1 = e / batch2;
@@ -272,7 +273,11 @@ __global__ void __launch_bounds__(256) pack_kernel(const TS* src, long long rs, 
 #pragma unroll
       for (int k4 = 0; k4 < 4; ++k4) {
         const int k = k0 + k4;
-        x[k4] = (row < d.R && k < d.K) ? (double)X[row * rs + k * ks] : 0.0;
+        // grouped K: packed k = g kgp + j holds source k = g kgs + j (j < kgs), else zero
+        const int g = kgp ? k / kgp : 0, j = k - g * kgp;
+        const bool kin = k < d.K && (kgp == 0 || j < kgs);
+        const int sk = kgp ? g * kgs + j : k;
+        x[k4] = (row < d.R && kin) ? (double)X[row * rs + (long long)sk * ks] : 0.0;
       }
       const long long o = ocol + (lr >> 3) * 128 + (lr & 7) * 4;
       if (!lo) {
@@ -292,16 +297,26 @@ __global__ void __launch_bounds__(256) pack_kernel(const TS* src, long long rs, 
 }
 
 // SPLIT: both operands are stored as plain FP32 in the packed layout (lo == nullptr); the bulk
-// copies land them in the hi slots, and warps 2 and 3 split each landed chunk in shared memory
+// copies land them in the hi slots, and warps 2..7 split each landed chunk in shared memory
 // into hi = tf32(x) (in place) and lo = tf32(x - hi) before the MMAs read it.  Otherwise both
-// operands arrive already split (hi and lo parts in HBM).
+// operands arrive already split (hi and lo parts in HBM) and the CTA has 4 warps.
+//
+// A stage holds [A hi | B hi | A lo | B lo].  Warp 0 lane 0 issues the bulk copies, warp 1
+// lane 0 the MMAs.  In the epilogue warp w reads tensor-memory lanes 32 (w % 4) .. +31 (rows of
+// the tile) and, with 8 warps, the column half w / 4.
 template <int NP, int PST, typename TCI, typename TCO, bool SPLIT>
-__global__ void __launch_bounds__(PNT, 1) umma3_kernel(UGemmP g, int* flag) {
-  static_assert(NP % 16 == 0 && NP >= 16 && NP <= 256, "N tile");
+__global__ void __launch_bounds__(SPLIT ? 2 * PNT : PNT, 1) umma3_kernel(UGemmP g, int* flag) {
+  static_assert(NP % 32 == 0 && NP >= 32 && NP <= 256, "N tile");
+  constexpr int NT = SPLIT ? 2 * PNT : PNT;
   constexpr int A_B = 16 * 512, B_B = (NP / 8) * 512;     // one part (hi or lo) per stage
-  constexpr int STAGE = 2 * (A_B + B_B);
+  constexpr int HALF = A_B + B_B;
+  constexpr int STAGE = 2 * HALF;
   constexpr int TCOLS = NP <= 32 ? 32 : (NP <= 64 ? 64 : (NP <= 128 ? 128 : 256));
-  constexpr int NCONV = 64;                                // converter threads (warps 2, 3)
+  constexpr int NCONV = NT - 64;                           // converter threads (warps 2..7)
+  constexpr int CA = (A_B / 16 + NCONV - 1) / NCONV;       // float4 of A per converter thread
+  constexpr int CB = (B_B / 16 + NCONV - 1) / NCONV;       // float4 of B per converter thread
+  constexpr int NCOL = NP / (NT / 128);                    // epilogue columns per warp
+  static_assert(NCOL % 16 == 0, "epilogue column split");
   constexpr uint32_t IDESC = idesc_tf32(UM, NP);
   extern __shared__ __align__(1024) uint8_t psm[];
   uint64_t* full = reinterpret_cast<uint64_t*>(psm + PST * STAGE);
@@ -361,13 +376,13 @@ __global__ void __launch_bounds__(PNT, 1) umma3_kernel(UGemmP g, int* flag) {
       if (SPLIT) {
         mbar_expect_tx(&full[s], bytesA + bytesB);
         bulk_g2s(st, Ahi + (long long)kc * ngA * 128, bytesA, &full[s]);
-        bulk_g2s(st + 2 * A_B, Bhi + (long long)kc * ngBt * 128, bytesB, &full[s]);
+        bulk_g2s(st + A_B, Bhi + (long long)kc * ngBt * 128, bytesB, &full[s]);
       } else {
         mbar_expect_tx(&full[s], 2 * (bytesA + bytesB));
         bulk_g2s(st, Ahi + (long long)kc * ngA * 128, bytesA, &full[s]);
-        bulk_g2s(st + A_B, Alo + (long long)kc * ngA * 128, bytesA, &full[s]);
-        bulk_g2s(st + 2 * A_B, Bhi + (long long)kc * ngBt * 128, bytesB, &full[s]);
-        bulk_g2s(st + 2 * A_B + B_B, Blo + (long long)kc * ngBt * 128, bytesB, &full[s]);
+        bulk_g2s(st + HALF, Alo + (long long)kc * ngA * 128, bytesA, &full[s]);
+        bulk_g2s(st + A_B, Bhi + (long long)kc * ngBt * 128, bytesB, &full[s]);
+        bulk_g2s(st + HALF + A_B, Blo + (long long)kc * ngBt * 128, bytesB, &full[s]);
       }
       issued = kc + 1;
     }
@@ -386,8 +401,8 @@ __global__ void __launch_bounds__(PNT, 1) umma3_kernel(UGemmP g, int* flag) {
         break;
       }
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      const uint32_t a_hi = smem_addr(psm + s * STAGE), a_lo = a_hi + A_B;
-      const uint32_t b_hi = a_hi + 2 * A_B, b_lo = b_hi + B_B;
+      const uint32_t a_hi = smem_addr(psm + s * STAGE), b_hi = a_hi + A_B;
+      const uint32_t a_lo = a_hi + HALF, b_lo = b_hi + HALF;
 #pragma unroll
       for (int kk = 0; kk < PK / 8; ++kk) {
         const uint32_t o = kk * 256;
@@ -399,8 +414,10 @@ __global__ void __launch_bounds__(PNT, 1) umma3_kernel(UGemmP g, int* flag) {
     }
     umma_commit(done);  // tracks every MMA issued above
   } else if (SPLIT && warp >= 2) {
-    // converters: once chunk kc has landed, split it in place (hi) and into the lo slots,
-    // make the writes visible to the tensor cores' (async) proxy, then arrive on conv[s]
+    // converters: once chunk kc has landed, split it in place (hi) and into the lo slots, make
+    // the writes visible to the tensor cores' (async) proxy, then arrive on conv[s].  Each
+    // thread loads all its float4 of the chunk before converting any (one shared-memory round
+    // trip per chunk)
     const int ct = tid - 64;
     for (int kc = 0; kc < nkc; ++kc) {
       const int s = kc % PST;
@@ -408,23 +425,27 @@ __global__ void __launch_bounds__(PNT, 1) umma3_kernel(UGemmP g, int* flag) {
         atomicExch(abort_flag, 1);
         break;
       }
-      uint8_t* st = psm + s * STAGE;
-      float4* ah = reinterpret_cast<float4*>(st);
-      float4* al = reinterpret_cast<float4*>(st + A_B);
-      float4* bh = reinterpret_cast<float4*>(st + 2 * A_B);
-      float4* bl = reinterpret_cast<float4*>(st + 2 * A_B + B_B);
+      float4* hp = reinterpret_cast<float4*>(psm + s * STAGE);   // A hi, then B hi at A_B
       const int na = (int)(bytesA >> 4), nbq = (int)(bytesB >> 4);
-      for (int i = ct; i < na + nbq; i += NCONV) {
-        float4* hp = i < na ? ah + i : bh + (i - na);
-        float4* lp = i < na ? al + i : bl + (i - na);
-        const float4 x = *hp;
+      float4 x[CA + CB];
+#pragma unroll
+      for (int u = 0; u < CA; ++u)
+        if (ct + NCONV * u < na) x[u] = hp[ct + NCONV * u];
+#pragma unroll
+      for (int u = 0; u < CB; ++u)
+        if (ct + NCONV * u < nbq) x[CA + u] = hp[A_B / 16 + ct + NCONV * u];
+#pragma unroll
+      for (int u = 0; u < CA + CB; ++u) {
+        const int i = u < CA ? ct + NCONV * u : ct + NCONV * (u - CA);
+        if (i >= (u < CA ? na : nbq)) continue;
+        const int o = u < CA ? i : A_B / 16 + i;
         float4 h, l;
-        split_tf32f(x.x, h.x, l.x);
-        split_tf32f(x.y, h.y, l.y);
-        split_tf32f(x.z, h.z, l.z);
-        split_tf32f(x.w, h.w, l.w);
-        *hp = h;
-        *lp = l;
+        split_tf32f(x[u].x, h.x, l.x);
+        split_tf32f(x[u].y, h.y, l.y);
+        split_tf32f(x[u].z, h.z, l.z);
+        split_tf32f(x[u].w, h.w, l.w);
+        hp[o] = h;
+        hp[o + HALF / 16] = l;
       }
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       mbar_arrive(&conv[s]);
@@ -436,7 +457,8 @@ __global__ void __launch_bounds__(PNT, 1) umma3_kernel(UGemmP g, int* flag) {
   if (!ok && tid == 0) atomicExch(flag, EXA_UMMA_TIMEOUT);
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   if (ok) {
-    const int r = m0 + 32 * warp + lane;
+    const int wq = warp & 3, cpart = warp >> 2;
+    const int r = m0 + 32 * wq + lane;
     const bool rv = r < g.M;
     TCO* C = reinterpret_cast<TCO*>(g.C);
     const TCI* Ci = reinterpret_cast<const TCI*>(g.Cin);
@@ -464,9 +486,10 @@ __global__ void __launch_bounds__(PNT, 1) umma3_kernel(UGemmP g, int* flag) {
       }
     }
 #pragma unroll 1
-    for (int c0 = 0; c0 < NP; c0 += 16) {
+    for (int c0 = cpart * NCOL; c0 < (cpart + 1) * NCOL; c0 += 16) {
+      if (c0 >= g.N) break;  // warp-uniform
       uint32_t v[16];
-      const uint32_t taddr = tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)c0;
+      const uint32_t taddr = tmem + ((uint32_t)(32 * wq) << 16) + (uint32_t)c0;
       asm volatile(
           "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
           "%14, %15}, [%16];"
@@ -550,12 +573,13 @@ template <int NP, int PST, typename TCI, typename TCO, bool SPLIT>
 int launch_umma3(const UGemmP& g, int* flag, cudaStream_t st) {
   constexpr size_t smem = (size_t)PST * 2 * (16 * 512 + (NP / 8) * 512) + (3 * PST + 1) * 8 + 16;
   static_assert(smem <= 227 * 1024, "tile exceeds shared memory");
+  constexpr int NT = SPLIT ? 2 * PNT : PNT;
   auto kern = umma3_kernel<NP, PST, TCI, TCO, SPLIT>;
   EXA_TRY(exa_allow_smem((const void*)kern, smem));
   EXA_CUDA(cudaFuncSetAttribute((const void*)kern, cudaFuncAttributePreferredSharedMemoryCarveout,
                                 (int)cudaSharedmemCarveoutMaxShared));
   dim3 grid((unsigned)exa_ceil_div(g.M, UM), (unsigned)g.batch, (unsigned)g.batch2);
-  kern<<<grid, PNT, smem, st>>>(g, flag);
+  kern<<<grid, NT, smem, st>>>(g, flag);
   EXA_LAUNCH_CHECK();
   return EXA_OK;
 }
@@ -579,8 +603,12 @@ long long exa_umma_wait_polls() { return g_umma_wait_polls.load(); }
 long long exa_pack_size(int R, int K) { return (long long)((R + 7) / 8) * ((K + PK - 1) / PK) * 128; }
 
 int exa_pack(const void* src, int src_f64, long long rs, long long ks, long long sb, long long sb2, int batch,
-             int batch2, const UPacked& d, cudaStream_t st) {
+             int batch2, const UPacked& d, cudaStream_t st, int kgp, int kgs) {
   if (batch <= 0 || batch2 <= 0 || d.R <= 0 || d.K <= 0) return EXA_OK;
+  if (kgp < 0 || kgs < 0 || kgs > kgp || (kgp > 0 && kgs == 0)) {
+    exa_set_error("pack: K groups of %d holding %d source entries", kgp, kgs);
+    return EXA_ERR_ARG;
+  }
   if (d.TR % 8 != 0) {
     exa_set_error("pack: tile height %d is not a multiple of 8", d.TR);
     return EXA_ERR_ARG;
@@ -592,9 +620,9 @@ int exa_pack(const void* src, int src_f64, long long rs, long long ks, long long
   }
   const unsigned grid = (unsigned)((long long)batch * batch2 * ntiles);
   if (src_f64)
-    pack_kernel<double><<<grid, 256, 0, st>>>((const double*)src, rs, ks, sb, sb2, batch2, ntiles, d);
+    pack_kernel<double><<<grid, 256, 0, st>>>((const double*)src, rs, ks, sb, sb2, batch2, ntiles, d, kgp, kgs);
   else
-    pack_kernel<float><<<grid, 256, 0, st>>>((const float*)src, rs, ks, sb, sb2, batch2, ntiles, d);
+    pack_kernel<float><<<grid, 256, 0, st>>>((const float*)src, rs, ks, sb, sb2, batch2, ntiles, d, kgp, kgs);
   EXA_LAUNCH_CHECK();
   return EXA_OK;
 }

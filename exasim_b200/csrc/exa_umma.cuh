@@ -42,8 +42,10 @@ struct UPacked {
 long long exa_pack_size(int R, int K);  // floats per batch entry
 
 // Pack X(r, k) = src[b1 sb + b2 sb2 + r rs + k ks] (FP64 or FP32) for b1 < batch, b2 < batch2.
+// With kgp > 0 the packed K comes in groups of kgp: packed k = g kgp + j holds source
+// k = g kgs + j for j < kgs and zero for kgs <= j < kgp.
 int exa_pack(const void* src, int src_f64, long long rs, long long ks, long long sb, long long sb2, int batch,
-             int batch2, const UPacked& dst, cudaStream_t st);
+             int batch2, const UPacked& dst, cudaStream_t st, int kgp = 0, int kgs = 0);
 
 // Packed-output description for a GEMM epilogue: C(r, c) is also stored as a packed
 // operand of a later GEMM, either as an A operand (row r, k = global column) or as a B

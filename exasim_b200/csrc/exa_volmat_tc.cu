@@ -29,7 +29,7 @@ constexpr int VGRP = 4;    // (k, c) blocks per item: 4 accumulators of 128 colu
 
 __global__ void __launch_bounds__(VTN, 1) vol_mat_tc_kernel(ExaDims P, const double* __restrict__ W, UPacked Sp,
                                                             const double* __restrict__ rgJ, double* D, double* B,
-                                                            int nb, int* flag) {
+                                                            UPacked Bp, int nb, int* flag) {
   const int npe = P.npe, nge = P.nge, nd = P.nd, ncu = P.ncu, nc = P.nc, n = P.n;
   const int nblk = ncu * nc, ngrp = (nblk + VGRP - 1) / VGRP;
   const int nkc = (nge + PK - 1) / PK, ngS = (npe + 7) / 8;
@@ -143,15 +143,22 @@ __global__ void __launch_bounds__(VTN, 1) vol_mat_tc_kernel(ExaDims P, const dou
       const int b = 2 * (warp >> 2) + bb;
       if (b >= nbg) break;  // warp-uniform
       const int kc = b0 + b, k = kc % ncu, c = kc / ncu;
-      double* out;
+      double* out = nullptr;
+      float* outp = nullptr;  // B as the packed FP32 operand of the q elimination (part nq)
       long long col0;
+      int kk0 = 0;
       if (c < ncu) {
         out = D + (long long)e * n * n;
         col0 = (long long)npe * c;
       } else {
         const int qc = c - ncu, nq = qc % ncu, d = qc / ncu;
-        out = B + (long long)e * n * npe * nd * ncu;
         col0 = (long long)npe * d + (long long)npe * nd * nq;
+        if (Bp.hi) {
+          outp = Bp.hi + (long long)e * Bp.sb + (long long)nq * Bp.sb2;
+          kk0 = qk_group(npe) * d;
+        } else {
+          out = B + (long long)e * n * npe * nd * ncu;
+        }
       }
 #pragma unroll 1
       for (int j0 = 0; j0 < 128; j0 += 16) {
@@ -165,10 +172,26 @@ __global__ void __launch_bounds__(VTN, 1) vol_mat_tc_kernel(ExaDims P, const dou
             : "r"(taddr));
         asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
         if (i < npe) {
+          if (outp) {
+            // whole quads of k: the group starts on a quad and the accumulator's columns from
+            // npe to the group's end are zeros (S is zero-padded there)
+            const int row = i + npe * k, t = row / Bp.TR;
+            const int ng = (min(Bp.TR, n - t * Bp.TR) + 7) / 8;
+            float* rp = outp + pack_off(row, 0, n, Bp.K, Bp.TR);
 #pragma unroll
-          for (int jj = 0; jj < 16; ++jj) {
-            const int j = j0 + jj;
-            if (j < npe) out[(i + (long long)npe * k) + (long long)n * (col0 + j)] = -(double)__uint_as_float(v[jj]);
+            for (int jj = 0; jj < 16; jj += 4) {
+              const int j = j0 + jj, kq = kk0 + j;
+              if (j >= qk_group(npe)) break;
+              *reinterpret_cast<float4*>(rp + (long long)(kq >> 4) * ng * 128 + ((kq >> 2) & 3) * 32) =
+                  make_float4(-__uint_as_float(v[jj]), -__uint_as_float(v[jj + 1]), -__uint_as_float(v[jj + 2]),
+                              -__uint_as_float(v[jj + 3]));
+            }
+          } else {
+#pragma unroll
+            for (int jj = 0; jj < 16; ++jj) {
+              const int j = j0 + jj;
+              if (j < npe) out[(i + (long long)npe * k) + (long long)n * (col0 + j)] = -(double)__uint_as_float(v[jj]);
+            }
           }
         }
       }
@@ -198,7 +221,12 @@ bool exa_vol_mat_tc_fits(const ExaDims& P) {
 }
 
 int exa_k_vol_mat_tc(const ExaDims& P, const double* shapegw, const UPacked& Sp, const double* rgJ, double* D,
-                     double* B, int nb, int* flag, cudaStream_t st) {
+                     double* B, const UPacked& Bp, int nb, int* flag, cudaStream_t st) {
+  if (Bp.hi && (Bp.lo || Bp.R != P.n || Bp.K != qk_group(P.npe) * P.nd || Bp.TR % 8 != 0)) {
+    exa_set_error("tensor-core volume kernel: packed B must be FP32 single with %d rows and %d k", P.n,
+                  qk_group(P.npe) * P.nd);
+    return EXA_ERR_ARG;
+  }
   if (!exa_vol_mat_tc_fits(P) || Sp.R != P.npe || Sp.K != P.nge) {
     exa_set_error("tensor-core volume kernel: npe %d, nge %d outside one 128 x 128 tile", P.npe, P.nge);
     return EXA_ERR_UNSUPPORTED;
@@ -210,7 +238,7 @@ int exa_k_vol_mat_tc(const ExaDims& P, const double* shapegw, const UPacked& Sp,
   int dev = 0;
   if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const int grid = nitems < sms ? nitems : sms;
-  vol_mat_tc_kernel<<<grid, VTN, smem, st>>>(P, shapegw, Sp, rgJ, D, B, nb, flag);
+  vol_mat_tc_kernel<<<grid, VTN, smem, st>>>(P, shapegw, Sp, rgJ, D, B, Bp, nb, flag);
   EXA_LAUNCH_CHECK();
   return EXA_OK;
 }
