@@ -54,6 +54,7 @@ def load_library(model: str) -> ctypes.CDLL:
         "exa_field_ptr": ([P, ctypes.c_char_p, ctypes.POINTER(P), PLL], I),
         "exa_get_connectivity": ([P, P, P], I),
         "exa_set_time": ([P, D, D], I),
+        "exa_set_step_time": ([P, D], I),
         "exa_assemble": ([P], I),
         "exa_residual": ([P, PD], I),
         "exa_matvec": ([P, P, P], I),
@@ -171,6 +172,10 @@ class HDGSolver:
 
     def set_time(self, time: float, dtfactor: float):
         self._check(self.lib.exa_set_time(self.h, time, dtfactor))
+
+    def set_step_time(self, time0: float):
+        """Start time of the next DIRK step (a restart at step R: R dt[0])."""
+        self._check(self.lib.exa_set_step_time(self.h, time0))
 
     # ---- the reference's steps
     def hdgAssembleLinearSystem(self):

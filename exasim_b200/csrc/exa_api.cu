@@ -322,6 +322,9 @@ int exa_ctx_init(ExaCtx& c, const double* app, long long napp, const double* mas
     EXA_TRY(exa_k_qmats(P, c.shapegt, c.shapegw, c.shapfgt, c.shapfgw, c.perm, c.elemg, c.faceg, mass, cw, ew, c.st));
     EXA_TRY(exa_inverse(mass, P.npe, (long long)P.npe * P.npe, P.ne, c.d_flag, c.st));
     c.Minv = mass;  // kept: q recovery applies it to C u - E uhat
+    EXA_TRY(dev_alloc(c, &c.wq_ug, ne * P.nge * P.ncu));
+    EXA_TRY(dev_alloc(c, &c.wq_v, ne * P.nge * P.nd * P.nd * P.ncu));
+    EXA_TRY(dev_alloc(c, &c.wq_w, ne * P.npe * P.nd * P.ncu));
     GemmBatch g{};
     g.M = P.npe; g.N = P.npe; g.K = P.npe; g.alpha = 1.0; g.beta = 0.0;
     g.A = mass; g.lda = P.npe; g.sA = (long long)P.npe * P.npe; g.sA2 = 0;
@@ -372,6 +375,9 @@ int exa_ctx_init(ExaCtx& c, const double* app, long long napp, const double* mas
   EXA_TRY(dev_alloc(c, &c.wG, std::max<size_t>(1, nb * m * nqn)));
   EXA_TRY(dev_alloc(c, &c.wRg, nb * P.nge * (P.nd + 1) * P.ncu * P.nc));
   EXA_TRY(dev_alloc(c, &c.wRu, nb * n));
+  EXA_TRY(dev_alloc(c, &c.wUG, nb * P.nge * P.nc));
+  EXA_TRY(dev_alloc(c, &c.wSG, nb * P.nge * P.ncu));
+  EXA_TRY(dev_alloc(c, &c.wRG, nb * P.nge * (P.nd + 1) * P.ncu));
   if (inv_ws) EXA_TRY(dev_alloc(c, &c.wInv, nb * inv_ws));
   {
     // the FP64 element products of the assembly: the fastest GEMM tile of each shape is
@@ -549,6 +555,9 @@ int exa_ctx_set_precision(ExaCtx& c, int mode) {
       // basis at the Gauss points: row j (node), k = g
       EXA_TRY(packed(c.Sp, P.npe, P.nge, 128, 1, 1, true));
       EXA_TRY(exa_pack(c.shapegt, 1, P.nge, 1, 0, 0, 1, 1, c.Sp, c.st));
+      const long long nw = (long long)P.npe * P.nge * (P.nd + 1);
+      EXA_TRY(dev_alloc(c, &c.shapegw32, (size_t)nw));
+      EXA_TRY(exa_k_to_f32(c.shapegw, c.shapegw32, nw, c.st));
     }
     EXA_TRY(packed(c.Dinvp, P.n, P.n, 128, nb, 1, false));
     EXA_TRY(packed(c.wFp, P.m, P.n, r16m, nb, 1, false));
@@ -647,9 +656,12 @@ long long exa_ctx_estimate_bytes(const double* app, long long napp, const double
   const double nqn = ncq > 0 ? npe * nd * ncu : 0;
   double per_elem = m * m + n * m + n + m + npe * nc + npe * ncu + nge * (nd + nd * nd + 1) + nfe * ngf * (2 * nd + 1) +
                     (ncq > 0 ? npe * npe * nd + npe * ndf * nd + npe * npe * (2 + nd) + npe * ndf * nd : 0) + m + n;
+  // q recovery workspace (Gauss-point u, its geometric products, C u)
+  per_elem += ncq > 0 ? nge * ncu * (1 + nd * nd) + npe * nd * ncu : 0;
   per_elem += precond == 1 ? m * m : 0;
   // element chunk workspace (the whole mesh when it fits in 8 GB)
   per_elem += n * n + n * nqn + 2 * n * m + m * nqn + nge * (nd + 1) * ncu * nc + n + (n > 160 ? n * n : 0);
+  per_elem += nge * (nc + ncu + (nd + 1) * ncu);  // Gauss-point values and Ru integrand of a chunk
   // preconditioner blocks: block Jacobi one per face; block ILU(0) one per stored block of the
   // sub-domain face graph, at most the face itself and the other faces of its two elements
   const double ncf2 = ncu * npf * ncu * npf;
@@ -851,6 +863,17 @@ int exa_set_time(exa_ctx* h, double time, double dtfactor) {
   EXA_TRY(guard(h));
   h->c.time = time;
   h->c.dtfactor = dtfactor;
+  return EXA_OK;
+}
+
+int exa_set_step_time(exa_ctx* h, double time0) {
+  EXA_TRY(guard(h));
+  if (!std::isfinite(time0)) {
+    exa_set_error("set_step_time: time %g is not finite", time0);
+    return EXA_ERR_ARG;
+  }
+  h->c.time0 = time0;
+  h->c.time = time0;
   return EXA_OK;
 }
 

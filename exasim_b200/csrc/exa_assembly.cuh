@@ -33,6 +33,12 @@ struct AsmArgs {
   // mixed form with the tensor-core volume kernel: B is packed the same way (written by the
   // volume kernel, face terms added here) instead of the FP64 B; unused when Bp.hi is null
   UPacked Bp;
+  // Gauss-point values computed for the whole chunk by GEMMs (null: per element here): udg at
+  // the Gauss points [nge, nc] and the stage source sdg at them [nge, ncu] per chunk element
+  const double *ugpre, *sgpre;
+  // when set, the volume kernel leaves its Ru integrand [nge, nd + 1, ncu] per chunk element
+  // here and the contraction with shapegw runs as one GEMM over the chunk
+  double* rgout;
 };
 
 // ----------------------------------------------------------------------------------
@@ -60,7 +66,8 @@ __global__ void vol_points_kernel(AsmArgs A, double* Ru, double* rgJ) {
   const double* Xx = eg + nge * ncx;
   const double* jac = Xx + nge * nd * nd;
   const double* U = A.udg + (long long)e * npe * nc;
-  for (int t = threadIdx.x; t < npe * nc; t += blockDim.x) un[t] = U[t];
+  if (!A.ugpre)
+    for (int t = threadIdx.x; t < npe * nc; t += blockDim.x) un[t] = U[t];
   for (int t = threadIdx.x; t < nge * ncx; t += blockDim.x) xg[t] = eg[t];
   for (int t = threadIdx.x; t < nge * ncu * nd; t += blockDim.x) fg[t] = 0.0;
   for (int t = threadIdx.x; t < nge * ncu; t += blockDim.x) sg[t] = 0.0;
@@ -69,21 +76,31 @@ __global__ void vol_points_kernel(AsmArgs A, double* Ru, double* rgJ) {
     for (int t = threadIdx.x; t < nge * ncu * nd * nc; t += blockDim.x) fJ[t] = 0.0;
   }
   __syncthreads();
-  for (int t = threadIdx.x; t < nge * nc; t += blockDim.x) {
-    const int g = t % nge, c = t / nge;
-    double s = 0.0;
-#pragma unroll 8
-    for (int j = 0; j < npe; ++j) s = fma(A.shapegt[g + nge * j], un[j + npe * c], s);
-    ug[t] = s;
-  }
-  if (A.tdep) {
-    const double* S = A.sdg + (long long)e * npe * ncu;
-    for (int t = threadIdx.x; t < nge * ncu; t += blockDim.x) {
-      const int g = t % nge, k = t / nge;
+  if (A.ugpre) {
+    const double* ugp = A.ugpre + (long long)le * nge * nc;
+    for (int t = threadIdx.x; t < nge * nc; t += blockDim.x) ug[t] = ugp[t];
+  } else {
+    for (int t = threadIdx.x; t < nge * nc; t += blockDim.x) {
+      const int g = t % nge, c = t / nge;
       double s = 0.0;
 #pragma unroll 8
-      for (int j = 0; j < npe; ++j) s = fma(A.shapegt[g + nge * j], S[j + npe * k], s);
-      sdgg[t] = s;
+      for (int j = 0; j < npe; ++j) s = fma(A.shapegt[g + nge * j], un[j + npe * c], s);
+      ug[t] = s;
+    }
+  }
+  if (A.tdep) {
+    if (A.sgpre) {
+      const double* sgp = A.sgpre + (long long)le * nge * ncu;
+      for (int t = threadIdx.x; t < nge * ncu; t += blockDim.x) sdgg[t] = sgp[t];
+    } else {
+      const double* S = A.sdg + (long long)e * npe * ncu;
+      for (int t = threadIdx.x; t < nge * ncu; t += blockDim.x) {
+        const int g = t % nge, k = t / nge;
+        double s = 0.0;
+#pragma unroll 8
+        for (int j = 0; j < npe; ++j) s = fma(A.shapegt[g + nge * j], S[j + npe * k], s);
+        sdgg[t] = s;
+      }
     }
   }
   __syncthreads();
@@ -146,8 +163,13 @@ __global__ void vol_points_kernel(AsmArgs A, double* Ru, double* rgJ) {
     }
   }
   __syncthreads();
-  // Ru(i,k) = sum_{g,d} shapegw[i,g,d] rgR[g,d,k]
   const int K = nge * (nd + 1);
+  if (A.rgout) {
+    double* o = A.rgout + (long long)le * K * ncu;
+    for (int t = threadIdx.x; t < K * ncu; t += blockDim.x) o[t] = rgR[t];
+    return;
+  }
+  // Ru(i,k) = sum_{g,d} shapegw[i,g,d] rgR[g,d,k]
   for (int t = threadIdx.x; t < npe * ncu; t += blockDim.x) {
     const int i = t % npe, k = t / npe;
     double s = 0.0;

@@ -573,9 +573,13 @@ __global__ void getq_kernel(ExaDims P, const int* elemcon, const double* MC, con
 // by quadrature (the sums that define C and E in qmats_kernel, taken over the Gauss points of
 // u and uhat instead of stored as matrices), so each element reads its 125 KB Minv (p = 4 hex)
 // instead of 825 KB of MinvC and MinvE.  One block per element.
+//
+// With wpre set, C_d u comes from there (w of element e at wpre + e npe ncu nd, computed for all
+// elements by two GEMMs, exa_k_getq_gemm) and the block does the face terms and Minv only.
 __global__ void getq_mf_kernel(ExaDims P, const double* shapegt, const double* shapegw, const double* shapfgt,
                                const double* shapfgw, const int* perm, const int* elemcon, const double* elemg,
-                               const double* faceg, const double* Minv, const double* uh, double* udg) {
+                               const double* faceg, const double* Minv, const double* uh, double* udg,
+                               const double* wpre) {
   extern __shared__ double sm[];
   const int e = blockIdx.x, npe = P.npe, ncu = P.ncu, ndf = P.ndf, nd = P.nd, nc = P.nc;
   const int nge = P.nge, npf = P.npf, ngf = P.ngf, nfe = P.nfe;
@@ -593,34 +597,40 @@ __global__ void getq_mf_kernel(ExaDims P, const double* shapegt, const double* s
     uhe[t] = uh[k + ncu * (long long)elemcon[jf + ndf * e]];
   }
   __syncthreads();
-  for (int t = threadIdx.x; t < nge * ncu; t += blockDim.x) {
-    const int g = t % nge, k = t / nge;
-    double s = 0.0;
-    for (int b = 0; b < npe; ++b) s = fma(shapegt[g + nge * b], u[b + npe * k], s);
-    for (int d = 0; d < nd; ++d)
-      for (int r = 0; r < nd; ++r) vg[g + nge * (r + nd * (d + nd * k))] = Xx[g + nge * (d + nd * r)] * s;
-  }
-  __syncthreads();
-  // C_d u: sum over g and r of shapegw[a, g, 1 + r] vg[g, r, d]; one thread per (a, k) takes
-  // every d, so each shapegw entry is loaded once for the nd products that use it
-  for (int t = threadIdx.x; t < npe * ncu; t += blockDim.x) {
-    const int a = t % npe, k = t / npe;
-    double s[3] = {0.0, 0.0, 0.0};
-    for (int r = 0; r < nd; ++r) {
-      const double* W = shapegw + a + (long long)npe * nge * (1 + r);
-      const double* v = vg + nge * (r + nd * nd * k);
-      for (int g = 0; g < nge; ++g) {
-        const double wv = W[npe * g];
-#pragma unroll
-        for (int d = 0; d < 3; ++d)
-          if (d < nd) s[d] = fma(wv, v[g + nge * nd * d], s[d]);
-      }
+  if (wpre) {
+    const double* we = wpre + (long long)e * npe * ncu * nd;
+    for (int t = threadIdx.x; t < npe * ncu * nd; t += blockDim.x) w[t] = we[t];
+    __syncthreads();
+  } else {
+    for (int t = threadIdx.x; t < nge * ncu; t += blockDim.x) {
+      const int g = t % nge, k = t / nge;
+      double s = 0.0;
+      for (int b = 0; b < npe; ++b) s = fma(shapegt[g + nge * b], u[b + npe * k], s);
+      for (int d = 0; d < nd; ++d)
+        for (int r = 0; r < nd; ++r) vg[g + nge * (r + nd * (d + nd * k))] = Xx[g + nge * (d + nd * r)] * s;
     }
+    __syncthreads();
+    // C_d u: sum over g and r of shapegw[a, g, 1 + r] vg[g, r, d]; one thread per (a, k) takes
+    // every d, so each shapegw entry is loaded once for the nd products that use it
+    for (int t = threadIdx.x; t < npe * ncu; t += blockDim.x) {
+      const int a = t % npe, k = t / npe;
+      double s[3] = {0.0, 0.0, 0.0};
+      for (int r = 0; r < nd; ++r) {
+        const double* W = shapegw + a + (long long)npe * nge * (1 + r);
+        const double* v = vg + nge * (r + nd * nd * k);
+        for (int g = 0; g < nge; ++g) {
+          const double wv = W[npe * g];
 #pragma unroll
-    for (int d = 0; d < 3; ++d)
-      if (d < nd) w[a + npe * (k + ncu * d)] = s[d];
+          for (int d = 0; d < 3; ++d)
+            if (d < nd) s[d] = fma(wv, v[g + nge * nd * d], s[d]);
+        }
+      }
+#pragma unroll
+      for (int d = 0; d < 3; ++d)
+        if (d < nd) w[a + npe * (k + ncu * d)] = s[d];
+    }
+    __syncthreads();
   }
-  __syncthreads();
   // minus E_d uhat, face by face (faces share corner and edge nodes)
   for (int l = 0; l < nfe; ++l) {
     const double* fg = faceg + ((long long)e * nfe + l) * P.faceg_stride();
@@ -660,6 +670,26 @@ __global__ void getq_mf_kernel(ExaDims P, const double* shapegt, const double* s
       for (int q = 0; q < 8; ++q)
         if (q0 + q < nq) U[i + npe * (ncu + q0 + q)] = s[q];
     }
+  }
+}
+
+// V[g + nge r, k + ncu (d + nd e)] = Xx_e[g, d, r] UG[g + nge (e + ne k)]: the Gauss-point
+// values of u_k times the geometric factors, the right operand of C_d u for all elements
+__global__ void getq_v_kernel(ExaDims P, const double* elemg, const double* UG, double* V) {
+  const int nge = P.nge, nd = P.nd, ncu = P.ncu;
+  const long long ne = P.ne, K = (long long)nge * nd;
+  const long long total = K * nd * ncu * ne;
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+       idx += (long long)gridDim.x * blockDim.x) {
+    const long long col = idx / K;
+    const int row = (int)(idx - col * K);
+    const int g = row % nge, r = row / nge;
+    const int k = (int)(col % ncu);
+    const long long de = col / ncu;
+    const int d = (int)(de % nd);
+    const long long e = de / nd;
+    const double* Xx = elemg + e * P.elemg_stride() + (long long)nge * P.ncx;
+    V[idx] = Xx[g + nge * (d + nd * r)] * UG[g + nge * (e + ne * k)];
   }
 }
 
@@ -767,13 +797,38 @@ size_t exa_getq_mf_smem(const ExaDims& P) {
 
 int exa_k_getq_mf(const ExaDims& P, const double* shapegt, const double* shapegw, const double* shapfgt,
                   const double* shapfgw, const int* perm, const int* elemcon, const double* elemg,
-                  const double* faceg, const double* Minv, const double* uh, double* udg, cudaStream_t st) {
+                  const double* faceg, const double* Minv, const double* uh, double* udg, cudaStream_t st,
+                  const double* wpre) {
   const size_t smem = exa_getq_mf_smem(P);
   EXA_TRY(exa_allow_smem((const void*)getq_mf_kernel, smem));
   getq_mf_kernel<<<P.ne, 128, smem, st>>>(P, shapegt, shapegw, shapfgt, shapfgw, perm, elemcon, elemg, faceg, Minv,
-                                          uh, udg);
+                                          uh, udg, wpre);
   EXA_LAUNCH_CHECK();
   return EXA_OK;
+}
+
+int exa_k_getq_gemm(const ExaDims& P, const double* shapegt, const double* shapegw, const double* elemg,
+                    const double* udg, double* UG, double* V, double* W, cudaStream_t st) {
+  if (P.ne <= 0 || P.ncq == 0) return EXA_OK;
+  GemmBatch g{};
+  // UG[:, e + ne k] = shapegt (nge x npe) u_k of element e
+  g.M = P.nge; g.N = P.ne; g.K = P.npe; g.alpha = 1.0; g.beta = 0.0;
+  g.A = shapegt; g.lda = P.nge;
+  g.B = udg; g.ldb = (long long)P.npe * P.nc; g.sB = P.npe;
+  g.C = UG; g.ldc = P.nge; g.sC = (long long)P.nge * P.ne;
+  g.batch = P.ncu; g.batch2 = 1;
+  EXA_TRY(exa_gemm(g, st));
+  const long long nv = (long long)P.nge * P.nd * P.nd * P.ncu * P.ne;
+  getq_v_kernel<<<grid_for(nv), 256, 0, st>>>(P, elemg, UG, V);
+  EXA_LAUNCH_CHECK();
+  // W[:, k + ncu (d + nd e)] = shapegw[:, :, 1..nd] (npe x nge nd) V: C_d u of every element
+  GemmBatch h{};
+  h.M = P.npe; h.N = P.ncu * P.nd * P.ne; h.K = P.nge * P.nd; h.alpha = 1.0; h.beta = 0.0;
+  h.A = shapegw + (long long)P.npe * P.nge; h.lda = P.npe;
+  h.B = V; h.ldb = (long long)P.nge * P.nd;
+  h.C = W; h.ldc = P.npe;
+  h.batch = 1; h.batch2 = 1;
+  return exa_gemm(h, st);
 }
 
 int exa_k_face_nodes(const ExaDims& P, const int* f2e, const int* perm, const double* udg, double* uh, cudaStream_t st) {

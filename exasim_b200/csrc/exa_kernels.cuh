@@ -37,12 +37,13 @@ int exa_k_dudg(const ExaDims& P, const int* elemcon, const T* DinvF, const doubl
 int exa_k_gemv32(int M, int K, int batch, double alpha, const float* A, long long sA, const double* x, long long sx,
                  double beta, double* y, long long sy, cudaStream_t st, int* flag = nullptr);
 // D and B volume blocks on the tcgen05 tensor cores (3xTF32) for the mixed-precision form,
-// with S = shapegt[:, :, 0] packed as a B operand (rows npe, K nge); npe, nge <= 128.
+// with S = shapegt[:, :, 0] packed as a B operand (rows npe, K nge) and shapegw32 = shapegw in
+// FP32; npe, nge <= 128.
 struct UPacked;
 bool exa_vol_mat_tc_fits(const ExaDims& P);
 // With Bp.hi set, B goes into Bp (the packed FP32 A operand of the q elimination, one part per
-// trace component: row i + npe k, k = j + npe d) instead of B.
-int exa_k_vol_mat_tc(const ExaDims& P, const double* shapegw, const UPacked& Sp, const double* rgJ, double* D,
+// trace component: row i + npe k, k = j + qk_group(npe) d) instead of B.
+int exa_k_vol_mat_tc(const ExaDims& P, const float* shapegw32, const UPacked& Sp, const double* rgJ, double* D,
                      double* B, const UPacked& Bp, int nb, int* flag, cudaStream_t st);
 // Block ILU(0) preconditioner on Cartesian sub-domains (Exasim preconditioner = 2): the
 // schedule built on the host (exa_bilu0.h) in device memory, and the sub-domain results.
@@ -65,11 +66,19 @@ int exa_k_bilu_apply(const ExaDims& P, const ExaBiluDev& b, const T* BE, const d
 // y = (float) x
 int exa_k_to_f32(const double* x, float* y, long long n, cudaStream_t st);
 int exa_k_udg_update(const ExaDims& P, double* udg, const double* du, double alpha, cudaStream_t st);
-// q = Minv (C u - E uhat) by quadrature (no MinvC / MinvE reads)
+// q = Minv (C u - E uhat) by quadrature (no MinvC / MinvE reads).  With wpre, C u is taken
+// from there (exa_k_getq_gemm) instead of computed per element.
 size_t exa_getq_mf_smem(const ExaDims& P);
 int exa_k_getq_mf(const ExaDims& P, const double* shapegt, const double* shapegw, const double* shapfgt,
                   const double* shapfgw, const int* perm, const int* elemcon, const double* elemg,
-                  const double* faceg, const double* Minv, const double* uh, double* udg, cudaStream_t st);
+                  const double* faceg, const double* Minv, const double* uh, double* udg, cudaStream_t st,
+                  const double* wpre = nullptr);
+// C_d u of every element as two FP64 tensor-core GEMMs whose left operands (shapegt, shapegw)
+// all elements share: UG = shapegt u (nge x ncu ne), V = Xx (.) UG (nge nd x ncu nd ne), W =
+// shapegw[:, :, 1..nd] V (npe x ncu nd ne, element e's block at W + e npe ncu nd, laid out as
+// the per-element w of exa_k_getq_mf).  UG, V and W are caller workspace of those sizes.
+int exa_k_getq_gemm(const ExaDims& P, const double* shapegt, const double* shapegw, const double* elemg,
+                    const double* udg, double* UG, double* V, double* W, cudaStream_t st);
 int exa_k_getq(const ExaDims& P, const int* elemcon, const double* MC, const double* ME, const double* uh,
                double* udg, cudaStream_t st);
 int exa_k_face_nodes(const ExaDims& P, const int* f2e, const int* perm, const double* udg, double* uh, cudaStream_t st);

@@ -1,7 +1,7 @@
 // exasim_b200_<model>: the solver as an executable, in place of the reference's
 // cput2cEXASIM / gput2cEXASIM for an HDG problem (backend/Main/main.cpp, Main/exasim.hpp).
 //
-//   exasim_b200_<model> <datain dir> <output prefix> [device]
+//   exasim_b200_<model> <datain dir> <output prefix> [restart] [device] [--checkpoint]
 //
 // reads <datain dir>/{app,master,mesh,sol}.bin as text2code writes them, solves through the
 // library's C ABI (steady: Newton; time dependent: every DIRK step of app.bin), and writes
@@ -11,7 +11,16 @@
 // u alone with saveSolOpt 0) and of uhat per saved step.  Steady problems save once; time-
 // dependent ones after every saveSolFreq-th step.  With the reference's default prefix
 // "dataout/out" the files are dataout/outudg_np0.bin and dataout/outuhat_np0.bin.
+//
+// Restart (time-dependent problems; exasim.hpp:338-348, 387-393, 413-420): restart R > 0, from
+// the argument or app.bin's timestepOffset (problem[19]), starts the step loop at time R dt[0]
+// from the state in <output prefix>udg_t<R>_np0.bin and <output prefix>_uhat_t<R>_np0.bin,
+// raw float64 arrays as ReadSolutions reads them (solution.cpp:804-828): u alone (npe ncu ne
+// words, inserted into udg) with saveSolOpt 0, else all of udg; then uhat.  --checkpoint
+// writes those two files, numbered by step + R, at every saved step, so a later run can
+// restart from any of them.
 // Exit status 0, or 1 with the library's message on stderr.
+#include <algorithm>
 #include <cstdio>
 #include <cstdlib>
 #include <fstream>
@@ -64,18 +73,38 @@ struct Output {
     const double h[3] = {a0, a1, a2};
     f.write(reinterpret_cast<const char*>(h), sizeof(h));
   }
+  void open_raw(const std::string& fn) {
+    f.open(fn, std::ios::binary);
+    if (!f) {
+      std::fprintf(stderr, "cannot write %s\n", fn.c_str());
+      std::exit(1);
+    }
+  }
   void write(const std::vector<double>& v) { f.write(reinterpret_cast<const char*>(v.data()), (std::streamsize)(v.size() * sizeof(double))); }
 };
 
 }  // namespace
 
 int main(int argc, char** argv) {
-  if (argc < 3) {
-    std::fprintf(stderr, "usage: %s <datain dir> <output prefix> [device]\n", argv[0]);
+  std::vector<std::string> pos;
+  bool checkpoint = false;
+  for (int i = 1; i < argc; ++i) {
+    const std::string a = argv[i];
+    if (a == "--checkpoint") checkpoint = true;
+    else pos.push_back(a);
+  }
+  if (pos.size() < 2) {
+    std::fprintf(stderr, "usage: %s <datain dir> <output prefix> [restart] [device] [--checkpoint]\n", argv[0]);
     return 1;
   }
-  const std::string din = std::string(argv[1]) + "/", prefix = argv[2];
-  const int device = argc > 3 ? std::atoi(argv[3]) : 0;
+  const std::string din = pos[0] + "/", prefix = pos[1];
+  char* end = nullptr;
+  const long rarg = pos.size() > 2 ? std::strtol(pos[2].c_str(), &end, 10) : 0;
+  if (pos.size() > 2 && (end == pos[2].c_str() || *end != '\0' || rarg < 0)) {
+    std::fprintf(stderr, "invalid restart value: %s\n", pos[2].c_str());
+    return 1;
+  }
+  const int device = pos.size() > 3 ? std::atoi(pos[3].c_str()) : 0;
   const std::vector<double> app = read_words(din + "app.bin"), master = read_words(din + "master.bin"),
                             mesh = read_words(din + "mesh.bin"), sol = read_words(din + "sol.bin");
   exa_ctx* ctx = nullptr;
@@ -92,31 +121,68 @@ int main(int argc, char** argv) {
   const int freq = prob.size() > 17 && prob[17] > 0 ? (int)prob[17] : 1;
   const int opt = prob.size() > 18 ? (int)prob[18] : 1;
   const long long ncs = opt == 0 ? ncu : nc;  // fields saved per node
+  const int offset = prob.size() > 19 ? (int)prob[19] : 0;
+  const int restart = offset > 0 ? offset : (int)rarg;  // the reference's precedence (exasim.hpp:387-388)
+  std::vector<double> udg((size_t)(npe * nc * ne)), uh((size_t)nuh);
+  if (restart > 0) {
+    if (!tdep || dt.empty()) {
+      std::fprintf(stderr, "restart %d: app.bin is not time dependent\n", restart);
+      return 1;
+    }
+    const std::string fu = prefix + "udg_t" + std::to_string(restart) + "_np0.bin";
+    const std::string fh = prefix + "_uhat_t" + std::to_string(restart) + "_np0.bin";
+    const std::vector<double> ru = read_words(fu), rh = read_words(fh);
+    const size_t nu = (size_t)(npe * ncs * ne);
+    if (ru.size() < nu || rh.size() < (size_t)nuh) {
+      std::fprintf(stderr, "restart %d: %s holds %zu words (needs %zu), %s %zu (needs %lld)\n", restart, fu.c_str(),
+                   ru.size(), nu, fh.c_str(), rh.size(), nuh);
+      return 1;
+    }
+    check(exa_get_field(ctx, "udg", udg.data(), (long long)udg.size()), "exa_get_field udg");
+    if (ncs == nc) {
+      std::copy(ru.begin(), ru.begin() + (long long)nu, udg.begin());
+    } else {
+      for (long long e = 0; e < ne; ++e)
+        for (long long k = 0; k < ncu; ++k)
+          for (long long i = 0; i < npe; ++i) udg[i + npe * (k + nc * e)] = ru[i + npe * (k + ncu * e)];
+    }
+    check(exa_set_field(ctx, "udg", udg.data(), (long long)udg.size()), "exa_set_field udg");
+    check(exa_set_field(ctx, "uh", rh.data(), nuh), "exa_set_field uh");
+    check(exa_set_step_time(ctx, restart * dt[0]), "exa_set_step_time");
+    std::printf("restart at step %d, time %g\n", restart, restart * dt[0]);
+  }
 
   Output oudg, ouh;
   oudg.open(prefix + "udg_np0.bin", (double)npe, (double)ncs, (double)ne);
   ouh.open(prefix + "uhat_np0.bin", (double)ncu, (double)npf, (double)nf);
-  std::vector<double> udg((size_t)(npe * nc * ne)), uh((size_t)nuh);
-  auto save = [&]() {
+  auto save = [&](int step) {
     check(exa_get_field(ctx, "udg", udg.data(), (long long)udg.size()), "exa_get_field udg");
     check(exa_get_field(ctx, "uh", uh.data(), (long long)uh.size()), "exa_get_field uh");
-    if (ncs == nc) {
-      oudg.write(udg);
-    } else {
-      std::vector<double> u((size_t)(npe * ncu * ne));
+    std::vector<double> u;
+    if (ncs != nc) {
+      u.resize((size_t)(npe * ncu * ne));
       for (long long e = 0; e < ne; ++e)
         for (long long k = 0; k < ncu; ++k)
           for (long long i = 0; i < npe; ++i) u[i + npe * (k + ncu * e)] = udg[i + npe * (k + nc * e)];
-      oudg.write(u);
     }
+    const std::vector<double>& us = ncs == nc ? udg : u;
+    oudg.write(us);
     ouh.write(uh);
+    if (checkpoint && step > 0) {
+      // the restart files of this step, raw (solution.cpp:804-828 reads them so)
+      Output cu, ch;
+      cu.open_raw(prefix + "udg_t" + std::to_string(step) + "_np0.bin");
+      cu.write(us);
+      ch.open_raw(prefix + "_uhat_t" + std::to_string(step) + "_np0.bin");
+      ch.write(uh);
+    }
   };
   if (!tdep) {
     int its = 0;
     double nrm = 0.0;
     check(exa_newton(ctx, &its, &nrm), "exa_newton");
     std::printf("Newton: %d steps, residual norm %.6e\n", its, nrm);
-    save();
+    save(0);
   } else {
     for (int istep = 0; istep < (int)dt.size(); ++istep) {
       for (int j = 0; j < nstage; ++j) {
@@ -124,8 +190,8 @@ int main(int argc, char** argv) {
         double nrm = 0.0;
         check(exa_dirk_stage(ctx, istep, j, &its, &nrm), "exa_dirk_stage");
       }
-      std::printf("step %d done\n", istep + 1);
-      if ((istep + 1) % freq == 0) save();
+      std::printf("step %d done\n", istep + 1 + restart);
+      if ((istep + 1) % freq == 0) save(istep + 1 + restart);
     }
   }
   exa_destroy(ctx);

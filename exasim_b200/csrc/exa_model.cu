@@ -287,6 +287,44 @@ int schur_chunk_mixed(ExaCtx& c, int e0, int nb) {
 
 }  // namespace
 
+namespace {
+
+// udg (and the stage source) at the Gauss points of elements e0 .. e0 + nb - 1 by GEMMs with the
+// shared basis shapegt: the volume kernel then reads them instead of forming them per element
+int volume_gauss_values(ExaCtx& c, AsmArgs& A, int e0, int nb) {
+  const ExaDims& P = c.P;
+  GemmBatch g{};
+  g.M = P.nge; g.K = P.npe; g.alpha = 1.0; g.beta = 0.0;
+  g.A = c.shapegt; g.lda = P.nge;
+  g.B = c.udg + (long long)e0 * P.npe * P.nc; g.ldb = P.npe; g.N = P.nc * nb;
+  g.C = c.wUG; g.ldc = P.nge;
+  g.batch = 1; g.batch2 = 1;
+  EXA_TRY(exa_gemm(g, c.st));
+  A.ugpre = c.wUG;
+  if (c.tdep) {
+    g.B = c.sdg + (long long)e0 * P.npe * P.ncu; g.N = P.ncu * nb;
+    g.C = c.wSG;
+    EXA_TRY(exa_gemm(g, c.st));
+    A.sgpre = c.wSG;
+  }
+  A.rgout = c.wRG;
+  return EXA_OK;
+}
+
+// Ru of the chunk = shapegw (npe x nge (nd + 1)) times the volume kernel's integrands
+int volume_residual_gemm(ExaCtx& c, double* Ruc, int nb) {
+  const ExaDims& P = c.P;
+  GemmBatch g{};
+  g.M = P.npe; g.K = P.nge * (P.nd + 1); g.N = P.ncu * nb; g.alpha = 1.0; g.beta = 0.0;
+  g.A = c.shapegw; g.lda = P.npe;
+  g.B = c.wRG; g.ldb = (long long)P.nge * (P.nd + 1);
+  g.C = Ruc; g.ldc = P.npe;
+  g.batch = 1; g.batch2 = 1;
+  return exa_gemm(g, c.st);
+}
+
+}  // namespace
+
 int exa_model_assemble(ExaCtx& c, bool jacobian) {
   const ExaDims& P = c.P;
   const int n = P.n, m = P.m;
@@ -310,8 +348,10 @@ int exa_model_assemble(ExaCtx& c, bool jacobian) {
     if (jacobian) {
       {
         ExaProfScope ps(c, EXA_PH_VOLUME);
+        if (c.wRG) EXA_TRY(volume_gauss_values(c, A, e0, nb));
         vol_points_kernel<ExaModel, true><<<nb, tpb_v, vs, c.st>>>(A, Ruc, c.wRg);
         EXA_LAUNCH_CHECK();
+        if (c.wRG) EXA_TRY(volume_residual_gemm(c, Ruc, nb));
         if (c.precision == 1 && c.Sp.hi) {
           // B straight into its packed FP32 form (the face kernel adds its terms there too).
           // The volume kernel assigns every entry of B, so only the layout's padding needs
@@ -321,7 +361,7 @@ int exa_model_assemble(ExaCtx& c, bool jacobian) {
             bp = c.wBp;
             A.Bp = c.wBp;
           }
-          EXA_TRY(exa_k_vol_mat_tc(P, c.shapegw, c.Sp, c.wRg, c.wD, c.wB, bp, nb, c.d_uflag, c.st));
+          EXA_TRY(exa_k_vol_mat_tc(P, c.shapegw32, c.Sp, c.wRg, c.wD, c.wB, bp, nb, c.d_uflag, c.st));
         } else {
           const int tiles = exa_ceil_div(P.npe, 64);
           dim3 grid(tiles * tiles, nb, P.ncu * P.nc);
@@ -352,8 +392,10 @@ int exa_model_assemble(ExaCtx& c, bool jacobian) {
       EXA_TRY(c.precision == 1 ? schur_chunk_mixed(c, e0, nb) : schur_chunk(c, e0, nb));
     } else {
       ExaProfScope ps(c, EXA_PH_RESIDUAL);
+      if (c.wRG) EXA_TRY(volume_gauss_values(c, A, e0, nb));
       vol_points_kernel<ExaModel, false><<<nb, tpb_v, vs, c.st>>>(A, Ruc, nullptr);
       EXA_LAUNCH_CHECK();
+      if (c.wRG) EXA_TRY(volume_residual_gemm(c, Ruc, nb));
       face_kernel<ExaModel, false><<<nb, tpb_f, fs, c.st>>>(A, Ruc, Rhc, nullptr, nullptr, nullptr, nullptr, nullptr,
                                                            nullptr);
       EXA_LAUNCH_CHECK();

@@ -53,10 +53,14 @@ struct ExaCtx {
   double *udg = nullptr, *uh = nullptr, *sdg = nullptr;
   double *MC = nullptr, *ME = nullptr;
   double* Minv = nullptr;  // inverse element mass matrices [npe, npe, ne] (q recovery by quadrature)
+  // q recovery workspace: Gauss-point u, its geometric products and C_d u for all elements
+  double *wq_ug = nullptr, *wq_v = nullptr, *wq_w = nullptr;
   double *H = nullptr, *F = nullptr, *Ru = nullptr, *Rh = nullptr, *b = nullptr, *Pc = nullptr;
   // assembly workspace for a chunk of `neb` elements
   int neb = 0;
   double *wD = nullptr, *wB = nullptr, *wF = nullptr, *wK = nullptr, *wG = nullptr, *wRg = nullptr, *wRu = nullptr;
+  // per chunk: udg and sdg at the Gauss points and the Ru integrand (the volume kernel's GEMMs)
+  double *wUG = nullptr, *wSG = nullptr, *wRG = nullptr;
   double* wInv = nullptr;  // blocked-inverse workspace (n^2 per element) when n exceeds the register kernel
   // Krylov / Newton workspace
   double *V = nullptr, *x = nullptr, *r = nullptr, *w = nullptr, *we = nullptr, *du = nullptr;
@@ -115,6 +119,7 @@ struct ExaCtx {
   // the q elimination), D^-1 (A), F (B of D^-1 F), K (A) and D^-1 F (B of K D^-1 F)
   UPacked MCp{}, MEp{}, wBp{}, wGp{}, Dinvp{}, wFp{}, Kp{}, DinvFp{};
   UPacked Sp{};  // shapegt[:, :, 0] as the B operand of the tensor-core volume kernel
+  float* shapegw32 = nullptr;  // shapegw in FP32, the weights of that kernel's T tiles
   // block ILU(0) on Cartesian sub-domains (preconditioner 2): blocks in Pc / Pc32
   std::vector<int> cartgridpart;
   ExaBiluDev bilu;

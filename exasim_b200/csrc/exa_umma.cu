@@ -296,44 +296,146 @@ __global__ void __launch_bounds__(256) pack_kernel(const TS* src, long long rs, 
   }
 }
 
+// Epilogue helpers shared by the 3xTF32 kernels.  epi_rowbase: the row-dependent parts of the
+// packed outputs' offsets for row r of batch entry b1.  epi_write16: the 16 results x of row r,
+// columns c0 .. c0 + 15 of the product, into the plain output C (already offset to the batch
+// entry) and the packed outputs.
+__device__ __forceinline__ void epi_rowbase(const UGemmP& g, long long b1, int r, long long (&pbase)[2],
+                                            int (&png)[2]) {
+#pragma unroll
+  for (int o = 0; o < 2; ++o) {
+    pbase[o] = 0;
+    png[o] = 0;
+    if (o >= g.nout) break;
+    const UPackOut& po = g.out[o];
+    if (po.as_b) {
+      // row = global column, k = r: one tile of ng groups
+      png[o] = (po.p.R + 7) / 8;
+      pbase[o] = b1 * po.p.sb + (long long)(r >> 4) * png[o] * 128 + ((r >> 2) & 3) * 32 + (r & 3);
+    } else {
+      // row = r in tile t, k = global column
+      const int t = r / po.p.TR, rl = r - t * po.p.TR;
+      const int rows_t = min(po.p.TR, po.p.R - t * po.p.TR);
+      const int nkc = (po.p.K + PK - 1) / PK;
+      png[o] = (rows_t + 7) / 8;
+      pbase[o] = b1 * po.p.sb + (long long)t * (po.p.TR / 8) * nkc * 128 + (rl >> 3) * 128 + (rl & 7) * 4;
+    }
+  }
+}
+
+template <typename TCO>
+__device__ __forceinline__ void epi_write16(const UGemmP& g, TCO* C, long long b2, int r, int c0, const double (&x)[16],
+                                            const long long (&pbase)[2], const int (&png)[2]) {
+  if (C) {
+#pragma unroll
+    for (int j = 0; j < 16; ++j)
+      if (c0 + j < g.N) C[r + g.ldc * (c0 + j)] = (TCO)x[j];
+  }
+#pragma unroll
+  for (int o = 0; o < 2; ++o) {
+    if (o >= g.nout) break;
+    const UPackOut& po = g.out[o];
+    if (!po.as_b && po.cmul == 1 && (po.cadd & 3) == 0) {
+      // A operand, consecutive columns are consecutive k: 4 k of a core-matrix row are one
+      // float4 (the packed K is zero-padded, so whole quads are written)
+#pragma unroll
+      for (int j = 0; j < 16; j += 4) {
+        const int gc = c0 + j + g.n0 + (int)b2 * po.cadd;
+        if (c0 + j >= g.N) break;
+        const long long off = pbase[o] + (long long)(gc >> 4) * png[o] * 128 + ((gc >> 2) & 3) * 32;
+        if (!po.p.lo) {
+          // FP32 operand, split by the consumer on chip
+          const float4 v = make_float4(c0 + j + 0 < g.N ? (float)x[j + 0] : 0.0f,
+                                       c0 + j + 1 < g.N ? (float)x[j + 1] : 0.0f,
+                                       c0 + j + 2 < g.N ? (float)x[j + 2] : 0.0f,
+                                       c0 + j + 3 < g.N ? (float)x[j + 3] : 0.0f);
+          *reinterpret_cast<float4*>(po.p.hi + off) = v;
+          continue;
+        }
+        float4 h, l;
+        split_tf32(c0 + j + 0 < g.N ? x[j + 0] : 0.0, h.x, l.x);
+        split_tf32(c0 + j + 1 < g.N ? x[j + 1] : 0.0, h.y, l.y);
+        split_tf32(c0 + j + 2 < g.N ? x[j + 2] : 0.0, h.z, l.z);
+        split_tf32(c0 + j + 3 < g.N ? x[j + 3] : 0.0, h.w, l.w);
+        *reinterpret_cast<float4*>(po.p.hi + off) = h;
+        *reinterpret_cast<float4*>(po.p.lo + off) = l;
+      }
+    } else {
+#pragma unroll
+      for (int j = 0; j < 16; ++j) {
+        const int c = c0 + j;
+        if (c >= g.N) break;
+        const int gc = (c + g.n0) * po.cmul + (int)b2 * po.cadd;
+        const long long off = po.as_b ? pbase[o] + (gc >> 3) * 128 + (gc & 7) * 4
+                                       : pbase[o] + (long long)(gc >> 4) * png[o] * 128 + ((gc >> 2) & 3) * 32 + (gc & 3);
+        if (!po.p.lo) {
+          po.p.hi[off] = (float)x[j];
+          continue;
+        }
+        float h, l;
+        split_tf32(x[j], h, l);
+        po.p.hi[off] = h;
+        po.p.lo[off] = l;
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+      "%14, %15}, [%16];"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]),
+        "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+      : "r"(taddr));
+}
+
 // SPLIT: both operands are stored as plain FP32 in the packed layout (lo == nullptr); the bulk
 // copies land them in the hi slots, and warps 2..7 split each landed chunk in shared memory
 // into hi = tf32(x) (in place) and lo = tf32(x - hi) before the MMAs read it.  Otherwise both
 // operands arrive already split (hi and lo parts in HBM) and the CTA has 4 warps.
 //
-// A stage holds [A hi | B hi | A lo | B lo].  Warp 0 lane 0 issues the bulk copies, warp 1
-// lane 0 the MMAs.  In the epilogue warp w reads tensor-memory lanes 32 (w % 4) .. +31 (rows of
-// the tile) and, with 8 warps, the column half w / 4.
-template <int NP, int PST, typename TCI, typename TCO, bool SPLIT>
+// RT = 2 (SPLIT only, 128 < M <= 256, NP <= 128): one CTA takes both 128-row tiles of A, so each
+// K chunk of B is loaded and split once for both; tile t accumulates in tensor-memory columns
+// t NP.  The second tile's slot holds only its row groups; its MMA reads 128 rows from there,
+// and the rows past M, which come from the following bytes of the stage, are never read back.
+//
+// A stage holds [A tile 0 | A tile 1 | B] hi, then the same lo.  Warp 0 lane 0 issues the bulk
+// copies, warp 1 lane 0 the MMAs.  In the epilogue warp w reads tensor-memory lanes 32 (w % 4)
+// .. +31 (rows of a tile) and, with 8 warps, the column half w / 4.
+template <int NP, int PST, typename TCI, typename TCO, bool SPLIT, int RT>
 __global__ void __launch_bounds__(SPLIT ? 2 * PNT : PNT, 1) umma3_kernel(UGemmP g, int* flag) {
   static_assert(NP % 32 == 0 && NP >= 32 && NP <= 256, "N tile");
+  static_assert(RT == 1 || (RT == 2 && SPLIT && NP <= 128), "row tiles per CTA");
   constexpr int NT = SPLIT ? 2 * PNT : PNT;
-  constexpr int A_B = 16 * 512, B_B = (NP / 8) * 512;     // one part (hi or lo) per stage
-  constexpr int HALF = A_B + B_B;
-  constexpr int STAGE = 2 * HALF;
-  constexpr int TCOLS = NP <= 32 ? 32 : (NP <= 64 ? 64 : (NP <= 128 ? 128 : 256));
+  constexpr int A_B = 16 * 512, B_B = (NP / 8) * 512;     // one part (hi or lo) of a full A tile, of B
+  constexpr int TCOLS = RT * NP <= 32 ? 32 : (RT * NP <= 64 ? 64 : (RT * NP <= 128 ? 128 : (RT * NP <= 256 ? 256 : 512)));
   constexpr int NCONV = NT - 64;                           // converter threads (warps 2..7)
-  constexpr int CA = (A_B / 16 + NCONV - 1) / NCONV;       // float4 of A per converter thread
+  constexpr int CA = (RT * A_B / 16 + NCONV - 1) / NCONV;  // float4 of A per converter thread
   constexpr int CB = (B_B / 16 + NCONV - 1) / NCONV;       // float4 of B per converter thread
   constexpr int NCOL = NP / (NT / 128);                    // epilogue columns per warp
   static_assert(NCOL % 16 == 0, "epilogue column split");
   constexpr uint32_t IDESC = idesc_tf32(UM, NP);
   extern __shared__ __align__(1024) uint8_t psm[];
+
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const long long b1 = blockIdx.y, b2 = blockIdx.z;
+  const int tA = blockIdx.x, m0 = tA * UM * RT;
+  const int nkc = (g.K + PK - 1) / PK;
+  // rows of each tile, their 8-row groups, and the stage layout (bytes)
+  const int rows0 = min(UM, g.M - m0), rows1 = RT == 2 ? g.M - m0 - UM : 0;
+  const int ngA0 = (rows0 + 7) / 8, ngA1 = (rows1 + 7) / 8;
+  const int ngB = (g.N + 7) / 8;
+  const int ngBt = (g.B.R + 7) / 8;  // groups of all of B's rows: the stride between K chunks
+  const uint32_t bytesA0 = (uint32_t)ngA0 * 512, bytesA1 = (uint32_t)ngA1 * 512, bytesB = (uint32_t)ngB * 512;
+  const uint32_t boff = RT == 2 ? A_B + bytesA1 : A_B;    // B's offset in a part
+  const uint32_t HALF = boff + B_B, STAGE = 2 * HALF;
   uint64_t* full = reinterpret_cast<uint64_t*>(psm + PST * STAGE);
   uint64_t* empty = full + PST;
   uint64_t* conv = empty + PST;                            // SPLIT: chunk split into hi and lo
   uint64_t* done = conv + PST;
   uint32_t* tslot = reinterpret_cast<uint32_t*>(done + 1);
   int* abort_flag = reinterpret_cast<int*>(tslot + 1);
-
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const long long b1 = blockIdx.y, b2 = blockIdx.z;
-  const int tA = blockIdx.x, m0 = tA * UM;
-  const int nkc = (g.K + PK - 1) / PK;
-  const int rowsA = (g.M - m0) < UM ? (g.M - m0) : UM;
-  const int ngA = (rowsA + 7) / 8, ngB = (g.N + 7) / 8;
-  const int ngBt = (g.B.R + 7) / 8;  // groups of all of B's rows: the stride between K chunks
-  const uint32_t bytesA = (uint32_t)ngA * 512, bytesB = (uint32_t)ngB * 512;
 
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(tslot)),
@@ -356,9 +458,11 @@ __global__ void __launch_bounds__(SPLIT ? 2 * PNT : PNT, 1) umma3_kernel(UGemmP 
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = *tslot;
 
-  const float* Ahi = g.A.hi + b1 * g.A.sb + b2 * g.A.sb2 + (long long)tA * 16 * nkc * 128;
+  // A tile t of this CTA starts (tA RT + t) tiles into the batch entry's A
+  const long long abase = b1 * g.A.sb + b2 * g.A.sb2 + (long long)tA * RT * 16 * nkc * 128;
+  const float* Ahi = g.A.hi + abase;
   const float* Bhi = g.B.hi + b1 * g.B.sb + b2 * g.B.sb2 + (long long)(g.n0 >> 3) * 128;
-  const float* Alo = SPLIT ? nullptr : g.A.lo + b1 * g.A.sb + b2 * g.A.sb2 + (long long)tA * 16 * nkc * 128;
+  const float* Alo = SPLIT ? nullptr : g.A.lo + abase;
   const float* Blo = SPLIT ? nullptr : g.B.lo + b1 * g.B.sb + b2 * g.B.sb2 + (long long)(g.n0 >> 3) * 128;
 
   const long long polls = g.main_wait_polls >= 0 ? g.main_wait_polls : WAIT_LIMIT;
@@ -374,15 +478,16 @@ __global__ void __launch_bounds__(SPLIT ? 2 * PNT : PNT, 1) umma3_kernel(UGemmP 
       }
       uint8_t* st = psm + s * STAGE;
       if (SPLIT) {
-        mbar_expect_tx(&full[s], bytesA + bytesB);
-        bulk_g2s(st, Ahi + (long long)kc * ngA * 128, bytesA, &full[s]);
-        bulk_g2s(st + A_B, Bhi + (long long)kc * ngBt * 128, bytesB, &full[s]);
+        mbar_expect_tx(&full[s], bytesA0 + bytesA1 + bytesB);
+        bulk_g2s(st, Ahi + (long long)kc * ngA0 * 128, bytesA0, &full[s]);
+        if (RT == 2) bulk_g2s(st + A_B, Ahi + (long long)16 * nkc * 128 + (long long)kc * ngA1 * 128, bytesA1, &full[s]);
+        bulk_g2s(st + boff, Bhi + (long long)kc * ngBt * 128, bytesB, &full[s]);
       } else {
-        mbar_expect_tx(&full[s], 2 * (bytesA + bytesB));
-        bulk_g2s(st, Ahi + (long long)kc * ngA * 128, bytesA, &full[s]);
-        bulk_g2s(st + HALF, Alo + (long long)kc * ngA * 128, bytesA, &full[s]);
-        bulk_g2s(st + A_B, Bhi + (long long)kc * ngBt * 128, bytesB, &full[s]);
-        bulk_g2s(st + HALF + A_B, Blo + (long long)kc * ngBt * 128, bytesB, &full[s]);
+        mbar_expect_tx(&full[s], 2 * (bytesA0 + bytesB));
+        bulk_g2s(st, Ahi + (long long)kc * ngA0 * 128, bytesA0, &full[s]);
+        bulk_g2s(st + HALF, Alo + (long long)kc * ngA0 * 128, bytesA0, &full[s]);
+        bulk_g2s(st + boff, Bhi + (long long)kc * ngBt * 128, bytesB, &full[s]);
+        bulk_g2s(st + HALF + boff, Blo + (long long)kc * ngBt * 128, bytesB, &full[s]);
       }
       issued = kc + 1;
     }
@@ -393,7 +498,7 @@ __global__ void __launch_bounds__(SPLIT ? 2 * PNT : PNT, 1) umma3_kernel(UGemmP 
     if (*ab)
       for (int q = max(0, issued - PST); q < issued; ++q) mbar_wait(&full[q % PST], (uint32_t)((q / PST) & 1));
   } else if (warp == 1 && lane == 0) {
-    // MMA issuer: hi*hi + hi*lo + lo*hi per K step of 8
+    // MMA issuer: hi*hi + hi*lo + lo*hi per K step of 8 and row tile
     for (int kc = 0; kc < nkc; ++kc) {
       const int s = kc % PST;
       if (*ab || !mbar_wait(SPLIT ? &conv[s] : &full[s], (uint32_t)((kc / PST) & 1), polls)) {
@@ -401,14 +506,21 @@ __global__ void __launch_bounds__(SPLIT ? 2 * PNT : PNT, 1) umma3_kernel(UGemmP 
         break;
       }
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      const uint32_t a_hi = smem_addr(psm + s * STAGE), b_hi = a_hi + A_B;
+      const uint32_t a_hi = smem_addr(psm + s * STAGE), b_hi = a_hi + boff;
       const uint32_t a_lo = a_hi + HALF, b_lo = b_hi + HALF;
 #pragma unroll
       for (int kk = 0; kk < PK / 8; ++kk) {
         const uint32_t o = kk * 256;
-        umma_tf32(tmem, sdesc(a_hi + o, 128, 512), sdesc(b_hi + o, 128, 512), IDESC, (kc > 0 || kk > 0) ? 1u : 0u);
-        umma_tf32(tmem, sdesc(a_hi + o, 128, 512), sdesc(b_lo + o, 128, 512), IDESC, 1u);
-        umma_tf32(tmem, sdesc(a_lo + o, 128, 512), sdesc(b_hi + o, 128, 512), IDESC, 1u);
+        const uint32_t acc_in = (kc > 0 || kk > 0) ? 1u : 0u;
+#pragma unroll
+        for (int t = 0; t < RT; ++t) {
+          // tile 1's groups are ngA1 long per chunk: its k-step offset is the same 256 bytes
+          const uint32_t ta = (uint32_t)(t * A_B);
+          const uint32_t acc = tmem + (uint32_t)(t * NP);
+          umma_tf32(acc, sdesc(a_hi + ta + o, 128, 512), sdesc(b_hi + o, 128, 512), IDESC, acc_in);
+          umma_tf32(acc, sdesc(a_hi + ta + o, 128, 512), sdesc(b_lo + o, 128, 512), IDESC, 1u);
+          umma_tf32(acc, sdesc(a_lo + ta + o, 128, 512), sdesc(b_hi + o, 128, 512), IDESC, 1u);
+        }
       }
       umma_commit(&empty[s]);
     }
@@ -419,26 +531,26 @@ __global__ void __launch_bounds__(SPLIT ? 2 * PNT : PNT, 1) umma3_kernel(UGemmP 
     // thread loads all its float4 of the chunk before converting any (one shared-memory round
     // trip per chunk)
     const int ct = tid - 64;
+    const int na = (int)((bytesA0 + bytesA1) >> 4), nbq = (int)(bytesB >> 4);  // A tiles are adjacent
     for (int kc = 0; kc < nkc; ++kc) {
       const int s = kc % PST;
       if (*ab || !mbar_wait(&full[s], (uint32_t)((kc / PST) & 1), polls)) {
         atomicExch(abort_flag, 1);
         break;
       }
-      float4* hp = reinterpret_cast<float4*>(psm + s * STAGE);   // A hi, then B hi at A_B
-      const int na = (int)(bytesA >> 4), nbq = (int)(bytesB >> 4);
+      float4* hp = reinterpret_cast<float4*>(psm + s * STAGE);   // A hi, then B hi at boff
       float4 x[CA + CB];
 #pragma unroll
       for (int u = 0; u < CA; ++u)
         if (ct + NCONV * u < na) x[u] = hp[ct + NCONV * u];
 #pragma unroll
       for (int u = 0; u < CB; ++u)
-        if (ct + NCONV * u < nbq) x[CA + u] = hp[A_B / 16 + ct + NCONV * u];
+        if (ct + NCONV * u < nbq) x[CA + u] = hp[boff / 16 + ct + NCONV * u];
 #pragma unroll
       for (int u = 0; u < CA + CB; ++u) {
         const int i = u < CA ? ct + NCONV * u : ct + NCONV * (u - CA);
         if (i >= (u < CA ? na : nbq)) continue;
-        const int o = u < CA ? i : A_B / 16 + i;
+        const int o = u < CA ? i : (int)(boff / 16) + i;
         float4 h, l;
         split_tf32f(x[u].x, h.x, l.x);
         split_tf32f(x[u].y, h.y, l.y);
@@ -456,111 +568,36 @@ __global__ void __launch_bounds__(SPLIT ? 2 * PNT : PNT, 1) umma3_kernel(UGemmP 
   const bool ok = __syncthreads_and(fin && *abort_flag == 0);
   if (!ok && tid == 0) atomicExch(flag, EXA_UMMA_TIMEOUT);
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-  if (ok) {
-    const int wq = warp & 3, cpart = warp >> 2;
-    const int r = m0 + 32 * wq + lane;
+  const int wq = warp & 3, cpart = warp >> 2;
+#pragma unroll 1
+  for (int t = 0; ok && t < RT; ++t) {
+    if (m0 + UM * t + 32 * wq >= g.M) continue;  // no row of this warp in tile t (warp-uniform)
+    const int r = m0 + UM * t + 32 * wq + lane;
     const bool rv = r < g.M;
     TCO* C = reinterpret_cast<TCO*>(g.C);
     const TCI* Ci = reinterpret_cast<const TCI*>(g.Cin);
     if (C) C += b1 * g.sC + b2 * g.sC2;
     if (Ci) Ci += b1 * g.sCi + b2 * g.sCi2;
     const bool use_cin = g.beta != 0.0;
-    // per-thread parts of the packed offsets (row r fixed; columns vary)
-    long long pbase[2] = {0, 0};
-    int png[2] = {0, 0};
-#pragma unroll
-    for (int o = 0; o < 2; ++o) {
-      if (o >= g.nout) break;
-      const UPackOut& po = g.out[o];
-      if (po.as_b) {
-        // row = global column, k = r: one tile of ng groups
-        png[o] = (po.p.R + 7) / 8;
-        pbase[o] = b1 * po.p.sb + (long long)(r >> 4) * png[o] * 128 + ((r >> 2) & 3) * 32 + (r & 3);
-      } else {
-        // row = r in tile t, k = global column
-        const int t = r / po.p.TR, rl = r - t * po.p.TR;
-        const int rows_t = min(po.p.TR, po.p.R - t * po.p.TR);
-        const int nkc = (po.p.K + PK - 1) / PK;
-        png[o] = (rows_t + 7) / 8;
-        pbase[o] = b1 * po.p.sb + (long long)t * (po.p.TR / 8) * nkc * 128 + (rl >> 3) * 128 + (rl & 7) * 4;
-      }
-    }
+    long long pbase[2];
+    int png[2];
+    epi_rowbase(g, b1, r, pbase, png);
 #pragma unroll 1
     for (int c0 = cpart * NCOL; c0 < (cpart + 1) * NCOL; c0 += 16) {
       if (c0 >= g.N) break;  // warp-uniform
       uint32_t v[16];
-      const uint32_t taddr = tmem + ((uint32_t)(32 * wq) << 16) + (uint32_t)c0;
-      asm volatile(
-          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
-          "%14, %15}, [%16];"
-          : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
-            "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
-          : "r"(taddr));
+      tmem_ld16(tmem + ((uint32_t)(32 * wq) << 16) + (uint32_t)(t * NP + c0), v);
       // Cin of the 16 columns first: independent loads in flight together
-      double cin[16];
+      double x[16];
 #pragma unroll
       for (int j = 0; j < 16; ++j) {
         const int c = c0 + j;
-        cin[j] = (use_cin && rv && c < g.N) ? (double)Ci[r + g.ldci * c] : 0.0;
+        x[j] = (use_cin && rv && c < g.N) ? (double)Ci[r + g.ldci * c] : 0.0;
       }
       asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-      double x[16];
 #pragma unroll
-      for (int j = 0; j < 16; ++j) x[j] = g.alpha * (double)__uint_as_float(v[j]) + g.beta * cin[j];
-      if (!rv) continue;
-      if (C) {
-#pragma unroll
-        for (int j = 0; j < 16; ++j)
-          if (c0 + j < g.N) C[r + g.ldc * (c0 + j)] = (TCO)x[j];
-      }
-#pragma unroll
-      for (int o = 0; o < 2; ++o) {
-        if (o >= g.nout) break;
-        const UPackOut& po = g.out[o];
-        if (!po.as_b && po.cmul == 1 && (po.cadd & 3) == 0) {
-          // A operand, consecutive columns are consecutive k: 4 k of a core-matrix row
-          // are one float4 (the packed K is zero-padded, so whole quads are written)
-#pragma unroll
-          for (int j = 0; j < 16; j += 4) {
-            const int gc = c0 + j + g.n0 + (int)b2 * po.cadd;
-            if (c0 + j >= g.N) break;
-            const long long off = pbase[o] + (long long)(gc >> 4) * png[o] * 128 + ((gc >> 2) & 3) * 32;
-            if (!po.p.lo) {
-              // FP32 operand, split by the consumer on chip
-              const float4 v = make_float4(c0 + j + 0 < g.N ? (float)x[j + 0] : 0.0f,
-                                           c0 + j + 1 < g.N ? (float)x[j + 1] : 0.0f,
-                                           c0 + j + 2 < g.N ? (float)x[j + 2] : 0.0f,
-                                           c0 + j + 3 < g.N ? (float)x[j + 3] : 0.0f);
-              *reinterpret_cast<float4*>(po.p.hi + off) = v;
-              continue;
-            }
-            float4 h, l;
-            split_tf32(c0 + j + 0 < g.N ? x[j + 0] : 0.0, h.x, l.x);
-            split_tf32(c0 + j + 1 < g.N ? x[j + 1] : 0.0, h.y, l.y);
-            split_tf32(c0 + j + 2 < g.N ? x[j + 2] : 0.0, h.z, l.z);
-            split_tf32(c0 + j + 3 < g.N ? x[j + 3] : 0.0, h.w, l.w);
-            *reinterpret_cast<float4*>(po.p.hi + off) = h;
-            *reinterpret_cast<float4*>(po.p.lo + off) = l;
-          }
-        } else {
-#pragma unroll
-          for (int j = 0; j < 16; ++j) {
-            const int c = c0 + j;
-            if (c >= g.N) break;
-            const int gc = (c + g.n0) * po.cmul + (int)b2 * po.cadd;
-            const long long off = po.as_b ? pbase[o] + (gc >> 3) * 128 + (gc & 7) * 4
-                                           : pbase[o] + (long long)(gc >> 4) * png[o] * 128 + ((gc >> 2) & 3) * 32 + (gc & 3);
-            if (!po.p.lo) {
-              po.p.hi[off] = (float)x[j];
-              continue;
-            }
-            float h, l;
-            split_tf32(x[j], h, l);
-            po.p.hi[off] = h;
-            po.p.lo[off] = l;
-          }
-        }
-      }
+      for (int j = 0; j < 16; ++j) x[j] = g.alpha * (double)__uint_as_float(v[j]) + g.beta * x[j];
+      if (rv) epi_write16<TCO>(g, C, b2, r, c0, x, pbase, png);
     }
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -569,16 +606,20 @@ __global__ void __launch_bounds__(SPLIT ? 2 * PNT : PNT, 1) umma3_kernel(UGemmP 
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TCOLS) : "memory");
 }
 
-template <int NP, int PST, typename TCI, typename TCO, bool SPLIT>
+template <int NP, int PST, typename TCI, typename TCO, bool SPLIT, int RT = 1>
 int launch_umma3(const UGemmP& g, int* flag, cudaStream_t st) {
-  constexpr size_t smem = (size_t)PST * 2 * (16 * 512 + (NP / 8) * 512) + (3 * PST + 1) * 8 + 16;
-  static_assert(smem <= 227 * 1024, "tile exceeds shared memory");
+  // a stage: full A tile(s) (the second of RT = 2 only as many row groups as it has) and B,
+  // hi and lo parts
+  constexpr size_t smax = (size_t)PST * 2 * (RT * 16 * 512 + (NP / 8) * 512) + (3 * PST + 1) * 8 + 16;
+  static_assert(smax <= 227 * 1024, "tile exceeds shared memory");
+  const size_t a1 = RT == 2 ? (size_t)((g.M - UM + 7) / 8) * 512 : 0;
+  const size_t smem = (size_t)PST * 2 * (16 * 512 + a1 + (NP / 8) * 512) + (3 * PST + 1) * 8 + 16;
   constexpr int NT = SPLIT ? 2 * PNT : PNT;
-  auto kern = umma3_kernel<NP, PST, TCI, TCO, SPLIT>;
+  auto kern = umma3_kernel<NP, PST, TCI, TCO, SPLIT, RT>;
   EXA_TRY(exa_allow_smem((const void*)kern, smem));
   EXA_CUDA(cudaFuncSetAttribute((const void*)kern, cudaFuncAttributePreferredSharedMemoryCarveout,
                                 (int)cudaSharedmemCarveoutMaxShared));
-  dim3 grid((unsigned)exa_ceil_div(g.M, UM), (unsigned)g.batch, (unsigned)g.batch2);
+  dim3 grid((unsigned)exa_ceil_div(g.M, UM * RT), (unsigned)g.batch, (unsigned)g.batch2);
   kern<<<grid, NT, smem, st>>>(g, flag);
   EXA_LAUNCH_CHECK();
   return EXA_OK;
@@ -586,6 +627,9 @@ int launch_umma3(const UGemmP& g, int* flag, cudaStream_t st) {
 
 template <typename TCI, typename TCO, bool SPLIT>
 int umma3_np(const UGemmP& g, int* flag, cudaStream_t st) {
+  // two row tiles of up to 256 rows in one CTA, so B is loaded and split once for both
+  if constexpr (SPLIT)
+    if (g.N <= 128 && g.M > UM && g.M <= 2 * UM) return launch_umma3<128, 3, TCI, TCO, SPLIT, 2>(g, flag, st);
   if (g.N <= 128) return launch_umma3<128, 3, TCI, TCO, SPLIT>(g, flag, st);
   if (g.N <= 160) return launch_umma3<160, 3, TCI, TCO, SPLIT>(g, flag, st);
   return launch_umma3<256, 2, TCI, TCO, SPLIT>(g, flag, st);

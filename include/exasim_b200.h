@@ -59,6 +59,10 @@ int exa_get_connectivity(exa_ctx* ctx, int* f2e, int* elemcon);
 /* Current time and DIRK factor d_jj/dt used by time-dependent assembly (UpdateSourceDIRK,
  * backend/Solution/updatesource.cpp:32-50). */
 int exa_set_time(exa_ctx* ctx, double time, double dtfactor);
+/* The time at the start of the next DIRK step (exa_dirk_stage step 0 starts from it; each
+ * completed step adds its dt).  A restart at step R sets it to R dt[0], as the reference does
+ * with its restart argument or timestepOffset (backend/Main/exasim.hpp:387-393, 425). */
+int exa_set_step_time(exa_ctx* ctx, double time0);
 
 /* hdgAssembleLinearSystem (backend/Discretization/discretization.cpp:483-573): element
  * residuals and Jacobians (uequation.cpp:45-557), static condensation (:559-775),

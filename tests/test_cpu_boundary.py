@@ -116,3 +116,8 @@ def test_executable_reports_usage_and_missing_input(tmp_path):
     r = subprocess.run([exe, str(tmp_path / "nowhere"), str(tmp_path / "out")], capture_output=True, text=True,
                        timeout=60)
     assert r.returncode == 1 and "cannot open" in r.stderr
+    # the restart argument must be a non-negative step number (exasim.hpp:341-347 refuses others)
+    for bad in ("x", "-1", "2a"):
+        r = subprocess.run([exe, str(tmp_path / "nowhere"), str(tmp_path / "out"), bad], capture_output=True,
+                           text=True, timeout=60)
+        assert r.returncode == 1 and "invalid restart value" in r.stderr, (bad, r.stderr)

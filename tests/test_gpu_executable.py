@@ -2,7 +2,11 @@
 reference's datain/ folder in, its dataout files out.  On the reference's Poisson3D example
 the written outuhat_np0.bin must carry the reference's header and match its golden trace
 solution to the tolerance of the library-level golden test (1e-10 relative); for a DIRK run
-the last udg snapshot must equal the library's own DIRK result bit for bit."""
+the last udg snapshot must equal the library's own DIRK result bit for bit; and a run restarted
+from a step's checkpoint files (ReadSolutions, backend/Solution/solution.cpp:804-828, with the
+restart argument of backend/Main/exasim.hpp:338-348, 387-393) must end in the same state, bit
+for bit, as the uninterrupted run."""
+import shutil
 import os
 import subprocess
 
@@ -20,8 +24,8 @@ def built():
     B.build(["poisson3d", "convdiff3d"])
 
 
-def run(model, datain, prefix):
-    r = subprocess.run([B.exe_path(model), datain, prefix], capture_output=True, text=True, timeout=900)
+def run(model, datain, prefix, *extra):
+    r = subprocess.run([B.exe_path(model), datain, prefix, *extra], capture_output=True, text=True, timeout=900)
     assert r.returncode == 0, r.stderr
     return r
 
@@ -52,3 +56,34 @@ def test_executable_dirk_snapshots(tmp_path):
     s.DIRK(2)
     assert np.array_equal(snaps[-1], s.get("udg"))
     s.close()
+
+
+def test_executable_restart_matches_uninterrupted_run(tmp_path):
+    # four DIRK steps in one run, checkpointing every saved step
+    da = cases.convdiff3d_hex(str(tmp_path / "a"), n=2, porder=2, nsteps=4)
+    oa = str(tmp_path / "oa")
+    run("convdiff3d", da, oa, "--checkpoint")
+    udg = np.fromfile(oa + "udg_np0.bin")
+    npe, nc, ne = (int(v) for v in udg[:3])
+    full = udg[3:].reshape(-1, npe * nc * ne)
+    uha = np.fromfile(oa + "uhat_np0.bin")[3:].reshape(4, -1)
+    for k in range(1, 5):
+        c = np.fromfile(oa + f"udg_t{k}_np0.bin")
+        assert np.array_equal(c, full[k - 1])       # saveSolOpt 1: all of udg, raw
+        assert np.array_equal(np.fromfile(oa + f"_uhat_t{k}_np0.bin"), uha[k - 1])
+    # the same problem restarted at step 2 for the remaining two steps
+    db = cases.convdiff3d_hex(str(tmp_path / "b"), n=2, porder=2, nsteps=2)
+    ob = str(tmp_path / "ob")
+    shutil.copy(oa + "udg_t2_np0.bin", ob + "udg_t2_np0.bin")
+    shutil.copy(oa + "_uhat_t2_np0.bin", ob + "_uhat_t2_np0.bin")
+    r = run("convdiff3d", db, ob, "2", "0", "--checkpoint")
+    assert "restart at step 2" in r.stdout
+    rest = np.fromfile(ob + "udg_np0.bin")[3:].reshape(-1, npe * nc * ne)
+    assert rest.shape[0] == 2
+    assert np.array_equal(rest[-1], full[-1])
+    assert np.array_equal(np.fromfile(ob + "uhat_np0.bin")[3:].reshape(2, -1)[-1], uha[-1])
+    assert os.path.exists(ob + "udg_t4_np0.bin")     # numbered by step + restart
+    # a missing checkpoint is an error, not a fresh start
+    r = subprocess.run([B.exe_path("convdiff3d"), db, str(tmp_path / "none"), "3"], capture_output=True, text=True,
+                       timeout=300)
+    assert r.returncode == 1 and "cannot open" in r.stderr
