@@ -566,6 +566,133 @@ __global__ void __launch_bounds__(16 * TY, (sizeof(T) == 4 && TY == 16) ? 2 : 1)
     }
 }
 
+// 32 < n <= 128, FP32: columns by warp.  Warp w owns columns w + NW j (j < CW) of every row,
+// lane l rows l + 32 i (i < RL), so column k = NW jk + w lies in one warp: the pivot search is a
+// warp argmax on registers, and the pivot row reaches each warp's lanes by shuffles from the
+// lane that holds it.  Per step the column's warp publishes the column, the pivot row index and
+// its reciprocal in shared memory (two buffers, alternating), and one barrier separates that
+// from the update.  The arithmetic per entry is the same as in inverse_kernel (a_pj d for the
+// pivot row, d and -a_ik d in column k, a_ij - a_ik (a_pj d) elsewhere) with the same pivot
+// choice, so both give the same bits.
+template <int NW, int CW, int RL>
+__global__ void __launch_bounds__(32 * NW, 2) inverse_wcol_kernel(float* Aall, int n, long long stride, int* flag) {
+  __shared__ float colb[2][32 * RL];
+  __shared__ int sp[2];
+  __shared__ float sd[2];
+  __shared__ int perm[32 * RL];
+  __shared__ int pos[32 * RL];
+  float* G = Aall + (long long)blockIdx.x * stride;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  float a[RL][CW];
+#pragma unroll
+  for (int i = 0; i < RL; ++i)
+#pragma unroll
+    for (int j = 0; j < CW; ++j) {
+      const int r = lane + 32 * i, c = warp + NW * j;
+      a[i][j] = (r < n && c < n) ? G[r + (long long)n * c] : 0.0f;
+    }
+  unsigned used = 0u;  // bit i: row lane + 32 i already pivoted (the same in every warp)
+  bool singular = false;
+  int step = 0;
+#pragma unroll
+  for (int jk = 0; jk < CW; ++jk) {
+    for (int wk = 0; wk < NW; ++wk) {
+      const int k = NW * jk + wk;
+      if (k >= n) break;
+      const int buf = step & 1;
+      ++step;
+      if (warp == wk) {
+        // the pivot: largest |a_rk| over the rows not yet pivoted, lowest row on ties
+        float best = -1.0f;
+        int bi = n;
+#pragma unroll
+        for (int i = 0; i < RL; ++i) {
+          const int r = lane + 32 * i;
+          if (r < n && !((used >> i) & 1u)) {
+            const float v = fabsf(a[i][jk]);
+            if (v > best) { best = v; bi = r; }
+          }
+        }
+        const unsigned key = bi < n ? __float_as_uint(best) : 0u;
+        const unsigned mx = __reduce_max_sync(0xffffffffu, key);
+        const unsigned mn = __reduce_min_sync(0xffffffffu, (bi < n && key == mx) ? (unsigned)bi : 0xffffffffu);
+        best = __uint_as_float(mx);
+        bi = mn == 0xffffffffu ? n : (int)mn;
+        if (!(best > 0.0f) || bi >= n) {
+          singular = true;
+          // continue on the first unused row so the block still terminates
+          bi = n;
+          for (int r = 0; r < n; ++r) {
+            const unsigned u = __shfl_sync(0xffffffffu, used, r & 31);
+            if (!((u >> (r >> 5)) & 1u)) { bi = r; break; }
+          }
+          if (bi >= n) bi = 0;
+        }
+        const int pi = bi >> 5;
+        float own = a[0][jk];
+#pragma unroll
+        for (int i = 1; i < RL; ++i)
+          if (i == pi) own = a[i][jk];
+        const float apk = __shfl_sync(0xffffffffu, own, bi & 31);
+#pragma unroll
+        for (int i = 0; i < RL; ++i) colb[buf][lane + 32 * i] = a[i][jk];
+        if (lane == 0) {
+          sp[buf] = bi;
+          sd[buf] = 1.0f / apk;
+          perm[k] = bi;
+        }
+      }
+      __syncthreads();
+      const int p = sp[buf];
+      const float d = sd[buf];
+      const int pl = p & 31, pi = p >> 5;
+      if (lane == pl) used |= 1u << pi;
+      float f[RL];
+#pragma unroll
+      for (int i = 0; i < RL; ++i) f[i] = (lane + 32 * i == p) ? 0.0f : colb[buf][lane + 32 * i];
+      // this warp's part of the pivot row, scaled: r_j = a_pj d
+      float r[CW];
+#pragma unroll
+      for (int j = 0; j < CW; ++j) {
+        float own = a[0][j];
+#pragma unroll
+        for (int i = 1; i < RL; ++i)
+          if (i == pi) own = a[i][j];
+        r[j] = __shfl_sync(0xffffffffu, own, pl) * d;
+      }
+      // rows other than p (f_p = 0 leaves row p as it is), then row p and column k
+#pragma unroll
+      for (int i = 0; i < RL; ++i)
+#pragma unroll
+        for (int j = 0; j < CW; ++j) a[i][j] = a[i][j] - f[i] * r[j];
+      if (warp == wk) {
+#pragma unroll
+        for (int i = 0; i < RL; ++i) a[i][jk] = -f[i] * d;
+      }
+      if (lane == pl) {
+#pragma unroll
+        for (int i = 0; i < RL; ++i)
+          if (i == pi) {
+#pragma unroll
+            for (int j = 0; j < CW; ++j) a[i][j] = r[j];
+            if (warp == wk) a[i][jk] = d;
+          }
+      }
+    }
+  }
+  if (singular && lane == 0) atomicExch(flag, 1);
+  __syncthreads();
+  for (int t = threadIdx.x; t < n; t += blockDim.x) pos[perm[t]] = t;
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < RL; ++i)
+#pragma unroll
+    for (int j = 0; j < CW; ++j) {
+      const int r = lane + 32 * i, c = warp + NW * j;
+      if (r < n && c < n) G[pos[r] + (long long)n * perm[c]] = a[i][j];
+    }
+}
+
 template <typename T, int TY, int RR, int RC>
 int launch_inverse(T* A, int n, long long stride, int batch, int* d_flag, cudaStream_t st) {
   static_assert(TY * RR <= INV_MAX_N + 31 && 16 * RC <= INV_MAX_N, "inverse tile exceeds the buffers");
@@ -593,9 +720,14 @@ int inverse_dispatch(T* A, int n, long long stride, int batch, int* d_flag, cuda
   // FP32 blocks up to 128: 256 threads with 8 x 8 entries each, two CTAs per SM
   if constexpr (sizeof(T) == 4) {
     if (n <= 128) {
-      if (rc <= 4) return launch_inverse<T, 16, 4, 4>(A, n, stride, batch, d_flag, st);
-      if (rc <= 6) return launch_inverse<T, 16, 6, 6>(A, n, stride, batch, d_flag, st);
-      return launch_inverse<T, 16, 8, 8>(A, n, stride, batch, d_flag, st);
+      // columns by warp: 4 warps of 16 columns up to 64, 8 warps up to 128
+      if (n <= 64) {
+        inverse_wcol_kernel<4, 16, 2><<<batch, 128, 0, st>>>(A, n, stride, d_flag);
+      } else {
+        inverse_wcol_kernel<8, 16, 4><<<batch, 256, 0, st>>>(A, n, stride, d_flag);
+      }
+      EXA_LAUNCH_CHECK();
+      return EXA_OK;
     }
   }
   const int rr = (n + 31) / 32;
