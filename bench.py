@@ -491,6 +491,7 @@ def run_ours(args):
                                   "phases": phases_of(plain["prof"], plain["prof_steps"]),
                                   "roofline": roof.pop("plain_roofline")},
                    "phases": phases_of(mixed["prof"], mixed["prof_steps"])}
+            out["autotuned"] = autotuned(s32)
             out.update(roof)
             if args.serve_requests > 0 and world == 1:
                 out["served"] = run_served(args, local)
@@ -576,8 +577,10 @@ SERVE_BATCH = 64  # job slots of the batched Krylov steps (exa_server_set_batchi
 def run_served(args, device):
     """The served-stream leg: the same seeded requests solved (a) one at a time in plain FP64,
     (b) by the server with `slots` overlapping solves in plain FP64 and (c) in the mixed form,
-    each on warm (resident) contexts; then the mixed server under Poisson arrivals at 100/s and
-    1000/s for p50/p99 latency.  Times are host wall-clock from submit to result."""
+    then (d, e) both forms with batched Krylov steps, each after a warm-up pass that creates the
+    resident context of every (mesh, order) pair once; then the batched servers of both forms
+    under Poisson arrivals at the rates of --serve-rates for p50/p99 latency.  Times are host
+    wall-clock from submit to result."""
     from exasim_b200 import build as B
     from exasim_b200.serve import CaseCache, Server, stream_requests, with_params
     B.build(["cdsin2d"])
@@ -587,11 +590,19 @@ def run_served(args, device):
     blobs = [[with_params(cache.get(n, p)[0], prm)] + cache.get(n, p)[1:] for _, n, p, prm in reqs]
     budget = 48 << 30
 
-    def saturated(srv, precision):
+    def saturated(srv, precision, which=None):
         t0 = time.perf_counter()
-        ids = [srv.submit(b, precision=precision, **(MIXED_SERVED if precision else {})) for b in blobs]
+        sel = blobs if which is None else [blobs[i] for i in which]
+        ids = [srv.submit(b, precision=precision, **(MIXED_SERVED if precision else {})) for b in sel]
         res = [srv.wait(i) for i in ids]
         return time.perf_counter() - t0, res
+
+    # the warm-up pass: one request of each (mesh, order) pair, so that every resident context the
+    # stream can reuse exists (as far as the memory budget holds them) before anything is timed
+    first = {}
+    for i, (_, n, p, _) in enumerate(reqs):
+        first.setdefault((n, p), i)
+    warm = sorted(first.values())
 
     out = {"workload": SERVED_WORKLOAD, "requests": R, "slots": args.serve_slots, "hbm_budget_bytes": budget,
            "batch_slots": SERVE_BATCH}
@@ -602,7 +613,7 @@ def run_served(args, device):
                                           ("served_batched_plain_fp64", args.serve_slots, 0, SERVE_BATCH),
                                           ("served_batched_mixed", args.serve_slots, 1, SERVE_BATCH)):
         with Server("cdsin2d", device=device, hbm_budget=budget, slots=slots, batch=batch) as srv:
-            saturated(srv, precision)            # warm: every (n, p) context created once
+            saturated(srv, precision, warm)      # warm: every (n, p) context created once
             b0 = srv.batch_stats()
             wall, res = saturated(srv, precision)
             st = srv.stats()
@@ -634,7 +645,7 @@ def run_served(args, device):
     for name, precision in (("poisson_arrivals_batched_mixed", 1), ("poisson_arrivals_batched_plain_fp64", 0)):
         rates = {}
         with Server("cdsin2d", device=device, hbm_budget=budget, slots=args.serve_slots, batch=SERVE_BATCH) as srv:
-            saturated(srv, precision)
+            saturated(srv, precision, warm)
             for rate in rates_list:
                 arr = stream_requests(R, rate, seed=7)
                 t0 = time.perf_counter()
@@ -705,6 +716,27 @@ def qelim_mixed_bytes(sz):
     k = 4 * ncu * m * kq + 4 * kq * npe + 8 * m * npe * ncu + 8 * m * npe * ncu
     h = 4 * ncu * m * kq + 4 * kq * ndf + 8 * m * ndf * ncu + 4 * m * ndf * ncu
     return (d + f + k + h) * ne
+
+
+def autotuned(s):
+    """The shapes the project's autotuners chose for this workload (timed on scratch blocks
+    when the contexts were created): the element inverse of order n in FP32 and FP64 (shape
+    0-3 of the column-by-warp Gauss-Jordan) and the FP64 DMMA tile of each q-elimination and
+    Schur product (exa_dgemm_tune's index into its tiles)."""
+    import ctypes
+    L, sz = s.lib, s.sizes
+    n, m, npe, ndf, nd = sz["n"], sz["m"], sz["npe"], sz["npf"] * sz["nfe"], sz["nd"]
+    out = {}
+    for fp64 in (0, 1):
+        v = ctypes.c_int(-1)
+        L.exa_inverse_autotune(n, fp64, sz["ne"], None, ctypes.byref(v))
+        out[f"inverse_n{n}_{'fp64' if fp64 else 'fp32'}_shape"] = v.value
+    for M, N, K in ((n, npe, npe * nd), (n, ndf, npe * nd), (m, npe, npe * nd), (m, ndf, npe * nd), (n, m, n),
+                    (m, m, n)):
+        t = ctypes.c_int(-1)
+        L.exa_dgemm_tune(M, N, K, min(sz["ne"], 512), None, ctypes.byref(t))
+        out[f"dgemm_{M}x{N}x{K}_tile"] = t.value
+    return out
 
 
 def kernel_rooflines(s32, s64, mixed, plain, torch, steps):

@@ -76,6 +76,7 @@ def load_library(model: str) -> ctypes.CDLL:
         "exa_dinverse_batched": ([P, I, LL, I, P, P], I),
         "exa_sinverse_batched": ([P, I, LL, I, P, P], I),
         "exa_dgemm_tune": ([I, I, I, I, P, PI], I),
+        "exa_inverse_autotune": ([I, I, I, P, PI], I),
         "exa_dnrm2_cols_fixed": ([P, LL, LL, I, P, P], I),
         "exa_gemm_tf32_batched": ([I, I, I, D, P, I, LL, LL, P, I, LL, LL, D, P, I, LL, LL, I, P, P], I),
         "exa_gemm_3xtf32_batched": ([I, I, I, D, P, I, LL, LL, P, I, LL, LL, D, P, LL, LL, I, P, P], I),

@@ -320,6 +320,7 @@ int exa_ctx_init(ExaCtx& c, const double* app, long long napp, const double* mas
     EXA_TRY(dev_alloc(c, &c.ME, ne * P.npe * P.ndf * P.nd));
     EXA_TRY(dev_alloc(c, &c.d_flag, 4));
     EXA_TRY(exa_k_qmats(P, c.shapegt, c.shapegw, c.shapfgt, c.shapfgw, c.perm, c.elemg, c.faceg, mass, cw, ew, c.st));
+    EXA_TRY(exa_inverse_tune(P.npe, (int)std::min<size_t>(ne, 4096), 1, c.st));
     EXA_TRY(exa_inverse(mass, P.npe, (long long)P.npe * P.npe, P.ne, c.d_flag, c.st));
     c.Minv = mass;  // kept: q recovery applies it to C u - E uhat
     EXA_TRY(dev_alloc(c, &c.wq_ug, ne * P.nge * P.ncu));
@@ -391,6 +392,8 @@ int exa_ctx_init(ExaCtx& c, const double* app, long long napp, const double* mas
     }
     EXA_TRY(exa_gemm_tune((int)n, (int)m, (int)n, nbt, c.st));
     EXA_TRY(exa_gemm_tune((int)m, (int)m, (int)n, nbt, c.st));
+    // and the element inverse (FP64 D of the plain form)
+    EXA_TRY(exa_inverse_tune((int)n, (int)std::min<size_t>(nb, 4096), 1, c.st));
   }
   EXA_TRY(dev_alloc(c, &c.V, N * (size_t)(c.restart + 1)));
   EXA_TRY(dev_alloc(c, &c.x, N));
@@ -521,7 +524,17 @@ int exa_ctx_set_precision(ExaCtx& c, int mode) {
     exa_set_error("precision mode %d: 0 (FP64) or 1 (FP32/TF32 elimination with FP64 refinement)", mode);
     return EXA_ERR_ARG;
   }
-  if (mode == 1) EXA_TRY(fp64_blocks(c, false));
+  if (mode == 1) {
+    EXA_TRY(fp64_blocks(c, false));
+    // the mixed assembly writes only the face blocks of the chunk arrays F, K and H (its
+    // products read them): their other entries must be zero, which a plain assembly may
+    // have overwritten
+    const ExaDims& P = c.P;
+    const size_t nb = c.neb, n = P.n, m = P.m;
+    EXA_CUDA(cudaMemsetAsync(c.wF, 0, sizeof(double) * nb * n * m, c.st));
+    EXA_CUDA(cudaMemsetAsync(c.wK, 0, sizeof(double) * nb * m * n, c.st));
+    EXA_CUDA(cudaMemsetAsync(c.H, 0, sizeof(double) * nb * m * m, c.st));
+  }
   if (mode == 1 && c.H32 == nullptr) {
     const ExaDims& P = c.P;
     const size_t ne = P.ne, n = P.n, m = P.m, nb = c.neb;
@@ -567,6 +580,7 @@ int exa_ctx_set_precision(ExaCtx& c, int mode) {
     EXA_TRY(dev_alloc(c, &c.F32, ne * n * m));
     EXA_TRY(dev_alloc(c, &c.K32, ne * m * n));
     EXA_TRY(dev_alloc(c, &c.Dinv32, ne * n * n));
+    EXA_TRY(exa_inverse_tune((int)n, (int)std::min<size_t>(nb, 4096), 0, c.st));
     if (exa_inverse_tc32_pk((int)n) > 0) {
       EXA_TRY(dev_alloc(c, &c.wInv32, nb * (size_t)exa_inverse_tc32_ws((int)n)));
       EXA_TRY(dev_alloc(c, &c.wInvPk, nb * (size_t)exa_inverse_tc32_pk((int)n)));
@@ -1138,6 +1152,12 @@ extern "C" void exa_debug_umma_wait_polls(long long polls) { exa_umma_set_wait_p
 extern "C" int exa_dgemm_tune(int M, int N, int K, int batch, void* stream, int* tile) {
   EXA_TRY(exa_gemm_tune(M, N, K, batch, (cudaStream_t)stream));
   if (tile) *tile = exa_gemm_tile_of(M, N, K);
+  return EXA_OK;
+}
+
+extern "C" int exa_inverse_autotune(int n, int fp64, int batch, void* stream, int* variant) {
+  EXA_TRY(exa_inverse_tune(n, batch, fp64, (cudaStream_t)stream));
+  if (variant) *variant = exa_inverse_variant_of(n, fp64);
   return EXA_OK;
 }
 

@@ -87,6 +87,12 @@ int exa_gemm(const GemmBatch& g, cudaStream_t st);
 // fastest for this device (an autotuner; exa_gemm uses a padding heuristic for shapes not
 // tuned).  The tile does not change the result.  Not for use inside stream capture.
 int exa_gemm_tune(int M, int N, int K, int batch, cudaStream_t st);
+// The same for the dense element inverse of order 32 < n <= 128: times the column-by-warp
+// shapes on up to 4096 scratch blocks (the default shape stays if they do not fit) and keeps
+// the fastest for this device, order and type (all shapes give the same bits).  Synchronizes
+// st; call it outside stream capture.
+int exa_inverse_tune(int n, int batch, int fp64, cudaStream_t st);
+int exa_inverse_variant_of(int n, int fp64);  // the shape exa_inverse uses for order n (-1: not tuned here)
 int exa_gemm_tile_of(int M, int N, int K);  // index of the tile exa_gemm uses for the shape
 
 // In-place explicit inverse of `batch` n x n column-major matrices spaced `stride`

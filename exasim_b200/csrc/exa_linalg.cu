@@ -566,30 +566,53 @@ __global__ void __launch_bounds__(16 * TY, (sizeof(T) == 4 && TY == 16) ? 2 : 1)
     }
 }
 
-// 32 < n <= 128, FP32: columns by warp.  Warp w owns columns w + NW j (j < CW) of every row,
-// lane l rows l + 32 i (i < RL), so column k = NW jk + w lies in one warp: the pivot search is a
-// warp argmax on registers, and the pivot row reaches each warp's lanes by shuffles from the
-// lane that holds it.  Per step the column's warp publishes the column, the pivot row index and
-// its reciprocal in shared memory (two buffers, alternating), and one barrier separates that
-// from the update.  The arithmetic per entry is the same as in inverse_kernel (a_pj d for the
-// pivot row, d and -a_ik d in column k, a_ij - a_ik (a_pj d) elsewhere) with the same pivot
-// choice, so both give the same bits.
-template <int NW, int CW, int RL>
-__global__ void __launch_bounds__(32 * NW, 2) inverse_wcol_kernel(float* Aall, int n, long long stride, int* flag) {
-  __shared__ float colb[2][32 * RL];
+// 32 < n <= 128: columns by warp.  Warp w owns columns w + NW j (j < CW) of every row, lane l
+// rows l + 32 i (i < RL), so column k = NW jk + w lies in one warp: the pivot search is a warp
+// argmax on registers, and the pivot row reaches each warp's lanes by shuffles from the lane
+// that holds it.  Per step the column's warp publishes the column, the pivot row index and its
+// reciprocal in shared memory (two buffers, alternating), and one barrier separates that from
+// the update.  The arithmetic per entry is the same as in inverse_kernel (a_pj d for the pivot
+// row, d and -a_ik d in column k, a_ij - a_ik (a_pj d) elsewhere) with the same pivot choice, so
+// every shape (NW, CW, RL) and inverse_kernel give the same bits.
+template <typename T>
+__device__ __forceinline__ void warp_argmax(T best, int bi, int n, T& mbest, int& mbi) {
+  // a non-negative value orders as its bit pattern: the warp's largest |v|, and the lowest
+  // row holding it (for FP64 the high word, then the low word among lanes that tie on it)
+  if constexpr (sizeof(T) == 4) {
+    const unsigned key = bi < n ? __float_as_uint(best) : 0u;
+    const unsigned mx = __reduce_max_sync(0xffffffffu, key);
+    const unsigned mn = __reduce_min_sync(0xffffffffu, (bi < n && key == mx) ? (unsigned)bi : 0xffffffffu);
+    mbest = __uint_as_float(mx);
+    mbi = mn == 0xffffffffu ? n : (int)mn;
+  } else {
+    const unsigned long long key = bi < n ? (unsigned long long)__double_as_longlong(best) : 0ull;
+    const unsigned khi = (unsigned)(key >> 32), klo = (unsigned)key;
+    const unsigned mhi = __reduce_max_sync(0xffffffffu, khi);
+    const unsigned mlo = __reduce_max_sync(0xffffffffu, khi == mhi ? klo : 0u);
+    const bool top = bi < n && khi == mhi && klo == mlo;
+    const unsigned mn = __reduce_min_sync(0xffffffffu, top ? (unsigned)bi : 0xffffffffu);
+    mbest = __longlong_as_double((long long)(((unsigned long long)mhi << 32) | mlo));
+    mbi = mn == 0xffffffffu ? n : (int)mn;
+  }
+}
+
+template <typename T, int NW, int CW, int RL>
+__global__ void __launch_bounds__(32 * NW, sizeof(T) == 4 ? 2 : 1)
+    inverse_wcol_kernel(T* Aall, int n, long long stride, int* flag) {
+  __shared__ T colb[2][32 * RL];
   __shared__ int sp[2];
-  __shared__ float sd[2];
+  __shared__ T sd[2];
   __shared__ int perm[32 * RL];
   __shared__ int pos[32 * RL];
-  float* G = Aall + (long long)blockIdx.x * stride;
+  T* G = Aall + (long long)blockIdx.x * stride;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  float a[RL][CW];
+  T a[RL][CW];
 #pragma unroll
   for (int i = 0; i < RL; ++i)
 #pragma unroll
     for (int j = 0; j < CW; ++j) {
       const int r = lane + 32 * i, c = warp + NW * j;
-      a[i][j] = (r < n && c < n) ? G[r + (long long)n * c] : 0.0f;
+      a[i][j] = (r < n && c < n) ? G[r + (long long)n * c] : T(0);
     }
   unsigned used = 0u;  // bit i: row lane + 32 i already pivoted (the same in every warp)
   bool singular = false;
@@ -603,22 +626,24 @@ __global__ void __launch_bounds__(32 * NW, 2) inverse_wcol_kernel(float* Aall, i
       ++step;
       if (warp == wk) {
         // the pivot: largest |a_rk| over the rows not yet pivoted, lowest row on ties
-        float best = -1.0f;
+        T best = T(-1);
         int bi = n;
 #pragma unroll
         for (int i = 0; i < RL; ++i) {
           const int r = lane + 32 * i;
           if (r < n && !((used >> i) & 1u)) {
-            const float v = fabsf(a[i][jk]);
+            const T v = fabs(a[i][jk]);  // fabsf for float: the compare takes |x| as an operand
             if (v > best) { best = v; bi = r; }
           }
         }
-        const unsigned key = bi < n ? __float_as_uint(best) : 0u;
-        const unsigned mx = __reduce_max_sync(0xffffffffu, key);
-        const unsigned mn = __reduce_min_sync(0xffffffffu, (bi < n && key == mx) ? (unsigned)bi : 0xffffffffu);
-        best = __uint_as_float(mx);
-        bi = mn == 0xffffffffu ? n : (int)mn;
-        if (!(best > 0.0f) || bi >= n) {
+        {
+          T mb;
+          int mi;
+          warp_argmax(best, bi, n, mb, mi);
+          best = mb;
+          bi = mi;
+        }
+        if (!(best > T(0)) || bi >= n) {
           singular = true;
           // continue on the first unused row so the block still terminates
           bi = n;
@@ -629,32 +654,32 @@ __global__ void __launch_bounds__(32 * NW, 2) inverse_wcol_kernel(float* Aall, i
           if (bi >= n) bi = 0;
         }
         const int pi = bi >> 5;
-        float own = a[0][jk];
+        T own = a[0][jk];
 #pragma unroll
         for (int i = 1; i < RL; ++i)
           if (i == pi) own = a[i][jk];
-        const float apk = __shfl_sync(0xffffffffu, own, bi & 31);
+        const T apk = __shfl_sync(0xffffffffu, own, bi & 31);
 #pragma unroll
         for (int i = 0; i < RL; ++i) colb[buf][lane + 32 * i] = a[i][jk];
         if (lane == 0) {
           sp[buf] = bi;
-          sd[buf] = 1.0f / apk;
+          sd[buf] = T(1) / apk;
           perm[k] = bi;
         }
       }
       __syncthreads();
       const int p = sp[buf];
-      const float d = sd[buf];
+      const T d = sd[buf];
       const int pl = p & 31, pi = p >> 5;
       if (lane == pl) used |= 1u << pi;
-      float f[RL];
+      T f[RL];
 #pragma unroll
-      for (int i = 0; i < RL; ++i) f[i] = (lane + 32 * i == p) ? 0.0f : colb[buf][lane + 32 * i];
+      for (int i = 0; i < RL; ++i) f[i] = (lane + 32 * i == p) ? T(0) : colb[buf][lane + 32 * i];
       // this warp's part of the pivot row, scaled: r_j = a_pj d
-      float r[CW];
+      T r[CW];
 #pragma unroll
       for (int j = 0; j < CW; ++j) {
-        float own = a[0][j];
+        T own = a[0][j];
 #pragma unroll
         for (int i = 1; i < RL; ++i)
           if (i == pi) own = a[i][j];
@@ -693,6 +718,39 @@ __global__ void __launch_bounds__(32 * NW, 2) inverse_wcol_kernel(float* Aall, i
     }
 }
 
+// The column-by-warp shapes: warps x columns per warp x rows per lane.  Variants 0-1 hold up
+// to 128 rows and columns, 2-3 up to 64.  exa_inverse_tune times them per order and type.
+constexpr int kInvVariants = 4;
+__host__ __device__ constexpr int inv_variant_nmax(int v) { return v < 2 ? 128 : 64; }
+
+template <typename T>
+int launch_wcol(int v, T* A, int n, long long stride, int batch, int* d_flag, cudaStream_t st) {
+  switch (v) {
+    case 0: inverse_wcol_kernel<T, 8, 16, 4><<<batch, 256, 0, st>>>(A, n, stride, d_flag); break;
+    case 1: inverse_wcol_kernel<T, 16, 8, 4><<<batch, 512, 0, st>>>(A, n, stride, d_flag); break;
+    case 2: inverse_wcol_kernel<T, 4, 16, 2><<<batch, 128, 0, st>>>(A, n, stride, d_flag); break;
+    default: inverse_wcol_kernel<T, 8, 8, 2><<<batch, 256, 0, st>>>(A, n, stride, d_flag); break;
+  }
+  EXA_LAUNCH_CHECK();
+  return EXA_OK;
+}
+
+std::mutex g_inv_mu;
+std::map<std::array<int, 3>, int> g_inv_tune;  // (device, n, fp64) -> measured fastest variant
+
+// the measured variant for this order and type, else the default: FP32 8 warps x 16 columns
+// (4 warps up to 64), FP64 16 warps x 8 columns (8 x 8 up to 64)
+int inv_variant(int n, bool fp64) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) == cudaSuccess) {
+    std::lock_guard<std::mutex> lk(g_inv_mu);
+    auto it = g_inv_tune.find({dev, n, fp64 ? 1 : 0});
+    if (it != g_inv_tune.end()) return it->second;
+  }
+  if (fp64) return n <= 64 ? 3 : 1;
+  return n <= 64 ? 2 : 0;
+}
+
 template <typename T, int TY, int RR, int RC>
 int launch_inverse(T* A, int n, long long stride, int batch, int* d_flag, cudaStream_t st) {
   static_assert(TY * RR <= INV_MAX_N + 31 && 16 * RC <= INV_MAX_N, "inverse tile exceeds the buffers");
@@ -718,18 +776,7 @@ int inverse_dispatch(T* A, int n, long long stride, int batch, int* d_flag, cuda
   }
   const int rc = (n + 15) / 16;
   // FP32 blocks up to 128: 256 threads with 8 x 8 entries each, two CTAs per SM
-  if constexpr (sizeof(T) == 4) {
-    if (n <= 128) {
-      // columns by warp: 4 warps of 16 columns up to 64, 8 warps up to 128
-      if (n <= 64) {
-        inverse_wcol_kernel<4, 16, 2><<<batch, 128, 0, st>>>(A, n, stride, d_flag);
-      } else {
-        inverse_wcol_kernel<8, 16, 4><<<batch, 256, 0, st>>>(A, n, stride, d_flag);
-      }
-      EXA_LAUNCH_CHECK();
-      return EXA_OK;
-    }
-  }
+  if (n <= 128) return launch_wcol<T>(inv_variant(n, sizeof(T) == 8), A, n, stride, batch, d_flag, st);
   const int rr = (n + 31) / 32;
   if (rr <= 2 && rc <= 4) return launch_inverse<T, 32, 2, 4>(A, n, stride, batch, d_flag, st);
   if (rr <= 2 && rc <= 6) return launch_inverse<T, 32, 2, 6>(A, n, stride, batch, d_flag, st);
@@ -745,6 +792,81 @@ int exa_inverse(double* A, int n, long long stride, int batch, int* d_flag, cuda
 
 int exa_inverse(float* A, int n, long long stride, int batch, int* d_flag, cudaStream_t st) {
   return inverse_dispatch(A, n, stride, batch, d_flag, st);
+}
+
+namespace {
+// scratch blocks for timing: hashed values uniform in [-1, 1), so partial pivoting permutes
+// the rows as it does on element blocks (and the final store is scattered as there)
+template <typename T>
+__global__ void inv_tune_fill_kernel(T* A, int n, long long total) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    unsigned long long z = (unsigned long long)t * 0x9E3779B97F4A7C15ull + 0x632BE59BD9B4E019ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    z ^= z >> 31;
+    A[t] = T((double)(z >> 11) * (2.0 / 9007199254740992.0) - 1.0);
+  }
+}
+
+template <typename T>
+int inverse_tune(int n, int batch, cudaStream_t st) {
+  int dev = 0;
+  EXA_CUDA(cudaGetDevice(&dev));
+  const std::array<int, 3> key{dev, n, sizeof(T) == 8 ? 1 : 0};
+  {
+    std::lock_guard<std::mutex> lk(g_inv_mu);
+    if (g_inv_tune.count(key)) return EXA_OK;
+  }
+  // as many blocks as the caller inverts (up to 4096): fewer fit in L2 and would time the
+  // shapes on cached data
+  const int nb = std::max(1, std::min(batch, 4096));
+  const long long total = (long long)n * n * nb;
+  T* buf = nullptr;
+  if (cudaMallocAsync((void**)&buf, sizeof(T) * total + 16, st) != cudaSuccess) {
+    cudaGetLastError();  // no room for scratch: keep the default shape
+    return EXA_OK;
+  }
+  int* flag = reinterpret_cast<int*>(buf + total);  // the timing runs' own singular flag
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  cudaError_t e = cudaEventCreate(&e0);
+  if (e == cudaSuccess) e = cudaEventCreate(&e1);
+  int best = inv_variant(n, sizeof(T) == 8);
+  float best_ms = -1.0f;
+  for (int v = 0; v < kInvVariants && e == cudaSuccess; ++v) {
+    if (n > inv_variant_nmax(v)) continue;
+    inv_tune_fill_kernel<T><<<1024, 256, 0, st>>>(buf, n, total);
+    if (launch_wcol<T>(v, buf, n, (long long)n * n, nb, flag, st) != EXA_OK) break;  // warm
+    e = cudaEventRecord(e0, st);
+    for (int r = 0; r < 3 && e == cudaSuccess; ++r)
+      if (launch_wcol<T>(v, buf, n, (long long)n * n, nb, flag, st) != EXA_OK) e = cudaErrorUnknown;
+    if (e == cudaSuccess) e = cudaEventRecord(e1, st);
+    if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+    float ms = 0.0f;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+    if (e == cudaSuccess && (best_ms < 0 || ms < best_ms)) {
+      best_ms = ms;
+      best = v;
+    }
+  }
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  cudaFreeAsync(buf, st);
+  if (e != cudaSuccess) {
+    exa_set_error("inverse tuning of order %d: %s", n, cudaGetErrorString(e));
+    return EXA_ERR_CUDA;
+  }
+  std::lock_guard<std::mutex> lk(g_inv_mu);
+  g_inv_tune[key] = best;
+  return EXA_OK;
+}
+}  // namespace
+
+int exa_inverse_variant_of(int n, int fp64) { return n > 32 && n <= 128 ? inv_variant(n, fp64 != 0) : -1; }
+
+int exa_inverse_tune(int n, int batch, int fp64, cudaStream_t st) {
+  if (n <= 32 || n > 128 || batch <= 0) return EXA_OK;
+  return fp64 ? inverse_tune<double>(n, batch, st) : inverse_tune<float>(n, batch, st);
 }
 
 // ----------------------------------------------------------------------------------

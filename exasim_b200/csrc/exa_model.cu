@@ -372,8 +372,16 @@ int exa_model_assemble(ExaCtx& c, bool jacobian) {
       double* Hc = c.fp64_full ? c.H + (long long)e0 * m * m : c.H;
       {
         ExaProfScope ps(c, EXA_PH_FACE);
-        EXA_CUDA(cudaMemsetAsync(c.wF, 0, sizeof(double) * (size_t)nb * n * m, c.st));
-        EXA_CUDA(cudaMemsetAsync(c.wK, 0, sizeof(double) * (size_t)nb * m * n, c.st));
+        // F, K and H of the chunk: the face kernel assigns their face blocks, at the same
+        // positions at every assembly (face l's rows or columns, the same master-face node
+        // lists for every element); the rest is structurally zero.  The plain form's products
+        // overwrite these arrays, so it zeroes them each time; in the mixed form the products
+        // only read them, and the zeros of the switch to that form (exa_ctx_set_precision) stay.
+        const bool zero_blocks = c.precision != 1;
+        if (zero_blocks) {
+          EXA_CUDA(cudaMemsetAsync(c.wF, 0, sizeof(double) * (size_t)nb * n * m, c.st));
+          EXA_CUDA(cudaMemsetAsync(c.wK, 0, sizeof(double) * (size_t)nb * m * n, c.st));
+        }
         if (nqn > 0 && P.ncq > 0) {
           if (c.precision == 1 && c.wGp.hi) {
             // G written packed by the face kernel.  Each element slot gets the same entries
@@ -385,7 +393,7 @@ int exa_model_assemble(ExaCtx& c, bool jacobian) {
             EXA_CUDA(cudaMemsetAsync(c.wG, 0, sizeof(double) * (size_t)nb * m * nqn, c.st));
           }
         }
-        EXA_CUDA(cudaMemsetAsync(Hc, 0, sizeof(double) * (size_t)nb * m * m, c.st));
+        if (zero_blocks) EXA_CUDA(cudaMemsetAsync(Hc, 0, sizeof(double) * (size_t)nb * m * m, c.st));
         face_kernel<ExaModel, true><<<nb, tpb_f, fs, c.st>>>(A, Ruc, Rhc, c.wD, c.wB, c.wF, c.wK, c.wG, Hc);
         EXA_LAUNCH_CHECK();
       }

@@ -161,6 +161,13 @@ int exa_sinverse_batched(float* A, int n, long long stride, int batch, int* info
  * each entry over k in the same order, so the choice changes the time, not the result.
  * Synchronizes `stream`; not for use inside stream capture. */
 int exa_dgemm_tune(int M, int N, int K, int batch, void* stream, int* tile);
+/* The same autotuner for the batched element inverse of order 32 < n <= 128 (FP64 when fp64 is
+ * nonzero, else FP32): times the column-by-warp Gauss-Jordan shapes on min(batch, 4096)
+ * scratch blocks (once per process, device, order and type; later calls return at once) and
+ * keeps the fastest; *variant (optional) receives the shape used for order n (0-3; -1 outside
+ * 33..128).  Every shape gives the same bits.  Synchronizes `stream`; not inside stream capture.
+ * exa_create and exa_set_precision tune the orders they invert. */
+int exa_inverse_autotune(int n, int fp64, int batch, void* stream, int* variant);
 /* C_b = alpha A_b B_b + beta C_b with FP32 C, the products split as hi*hi + hi*lo + lo*hi over
  * TF32 parts (3xTF32, about FP32 accuracy) on the tcgen05 tensor cores with FP32
  * accumulation: the product the mixed-precision form uses.  A and B are FP64 or FP32,

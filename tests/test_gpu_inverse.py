@@ -92,3 +92,45 @@ def test_singular_block_sets_flag(lib, n):
                                     None) == 0
     torch.cuda.synchronize()
     assert int(flag.item()) == 1
+
+
+@pytest.mark.parametrize("fp64", [0, 1])
+def test_every_tuned_shape_gives_the_same_bits(lib, fp64):
+    """exa_inverse_autotune picks one of the column-by-warp shapes per order; whatever it
+    picks, the inverse is the same to the bit, because every shape performs the same
+    operations with the same pivots.  The same blocks of orders 96 and 125 are inverted with
+    the untuned default shape and again after tuning: the results must be identical.  (In a
+    session where an earlier test already tuned the order, both runs use the tuned shape and
+    the check holds trivially.)"""
+    import torch
+    dt, inv = (torch.float64, lib.exa_dinverse_batched) if fp64 else (torch.float32, lib.exa_sinverse_batched)
+    for n in (96, 125):
+        rng = np.random.default_rng(100 + n)
+        batch = 300
+        # diagonally weighted (cond ~ 1e2), then the rows shuffled, so partial pivoting has to
+        # find the permutation
+        A = rng.standard_normal((batch, n, n)) + np.eye(n) * (2.0 * np.sqrt(n))
+        A = np.stack([a[rng.permutation(n)] for a in A])
+        host = np.ascontiguousarray(np.transpose(A, (0, 2, 1))).ravel()
+        outs = []
+        for tune in (False, True):
+            if tune:
+                v = ctypes.c_int(-2)
+                assert lib.exa_inverse_autotune(n, fp64, batch, None, ctypes.byref(v)) == 0, lib.exa_last_error().decode()
+                assert 0 <= v.value <= 3
+                w = ctypes.c_int(-2)
+                assert lib.exa_inverse_autotune(n, fp64, batch, None, ctypes.byref(w)) == 0
+                assert w.value == v.value                       # kept after the first call
+            dev = torch.tensor(host, dtype=dt, device="cuda")
+            flag = torch.zeros(1, dtype=torch.int32, device="cuda")
+            st = inv(ctypes.c_void_p(dev.data_ptr()), n, n * n, batch, ctypes.c_void_p(flag.data_ptr()), None)
+            assert st == 0, lib.exa_last_error().decode()
+            torch.cuda.synchronize()
+            outs.append(dev.cpu().numpy())
+        assert np.array_equal(outs[0], outs[1])
+        ref = np.linalg.inv(A)
+        got = np.transpose(outs[1].reshape(batch, n, n), (0, 2, 1))
+        tol = 1e-12 if fp64 else 1e-4
+        assert np.abs(got - ref).max() / np.abs(ref).max() < tol
+    v = ctypes.c_int(-2)
+    assert lib.exa_inverse_autotune(200, fp64, 8, None, ctypes.byref(v)) == 0 and v.value == -1
