@@ -379,6 +379,12 @@ int exa_ctx_init(ExaCtx& c, const double* app, long long napp, const double* mas
   EXA_TRY(dev_alloc(c, &c.wUG, nb * P.nge * P.nc));
   EXA_TRY(dev_alloc(c, &c.wSG, nb * P.nge * P.ncu));
   EXA_TRY(dev_alloc(c, &c.wRG, nb * P.nge * (P.nd + 1) * P.ncu));
+  {
+    // T factors of the FP64 volume products: at most 512 MB, the chunk taken in parts
+    const size_t per = (size_t)P.npe * P.nge * P.ncu * P.nc;
+    c.wT_elems = (int)std::max<size_t>(1, std::min<size_t>(nb, (512u << 20) / (8 * per)));
+    EXA_TRY(dev_alloc(c, &c.wT, (size_t)c.wT_elems * per));
+  }
   if (inv_ws) EXA_TRY(dev_alloc(c, &c.wInv, nb * inv_ws));
   {
     // the FP64 element products of the assembly: the fastest GEMM tile of each shape is
@@ -392,6 +398,7 @@ int exa_ctx_init(ExaCtx& c, const double* app, long long napp, const double* mas
     }
     EXA_TRY(exa_gemm_tune((int)n, (int)m, (int)n, nbt, c.st));
     EXA_TRY(exa_gemm_tune((int)m, (int)m, (int)n, nbt, c.st));
+    EXA_TRY(exa_gemm_tune(P.npe, P.npe, P.nge, nbt, c.st));  // the FP64 volume products
     // and the element inverse (FP64 D of the plain form)
     EXA_TRY(exa_inverse_tune((int)n, (int)std::min<size_t>(nb, 4096), 1, c.st));
   }
@@ -680,7 +687,9 @@ long long exa_ctx_estimate_bytes(const double* app, long long napp, const double
   // sub-domain face graph, at most the face itself and the other faces of its two elements
   const double ncf2 = ncu * npf * ncu * npf;
   const double pblocks = precond == 0 ? ncf2 * nf : (precond == 2 ? ncf2 * nf * (1 + 2 * (nfe - 1)) : 0.0);
-  double words = ne * per_elem + N * (restart + 6) + pblocks;
+  // volume-product T factors: at most 512 MB
+  const double wt = std::min(ne * npe * nge * ncu * nc, (double)(64 << 20));
+  double words = ne * per_elem + N * (restart + 6) + pblocks + wt;
   if (precision == 1) words *= 1.75;
   return (long long)(8.0 * words) + (16LL << 20);
 }

@@ -271,6 +271,26 @@ __global__ void __launch_bounds__(256) vol_mat_kernel(ExaDims P, const double* s
   }
 }
 
+// The left factors of the same products for elements le0 .. le0 + nbs - 1 of the chunk, for the
+// FP64 DMMA GEMM: T[i, g] = -sum_d shapegw[i, g, d] rgJ[g, d, k, c], npe x nge column-major, block
+// (k, c) of element le at T + ((le - le0) ncu nc + k + ncu c) npe nge.  Consecutive threads take
+// consecutive i: the weight loads are coalesced and the rgJ loads shared by the warp.
+__global__ void vol_t_kernel(ExaDims P, const double* __restrict__ shapegw, const double* __restrict__ rgJ, int le0,
+                             int nbs, double* __restrict__ T) {
+  const int npe = P.npe, nge = P.nge, nd = P.nd, nblk = P.ncu * P.nc;
+  const long long blk = (long long)npe * nge;
+  const long long total = blk * nblk * nbs;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    const long long bq = t / blk;  // (element, block) pair
+    const int r = (int)(t - bq * blk), i = r % npe, g = r / npe;
+    const double* R = rgJ + (long long)(le0 + bq / nblk) * nge * (nd + 1) * nblk + (long long)nge * (nd + 1) * (bq % nblk);
+    double v = 0.0;
+    for (int d = 0; d <= nd; ++d) v = fma(shapegw[i + (long long)npe * (g + (long long)nge * d)], R[g + nge * d], v);
+    T[t] = -v;
+  }
+}
+
 // ----------------------------------------------------------------------------------
 // faces.  Per element face l (processed in order by the whole block):
 //   uhat, (u, q) at the face nodes (elemcon / perm), then at the face points;

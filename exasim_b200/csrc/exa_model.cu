@@ -311,6 +311,40 @@ int volume_gauss_values(ExaCtx& c, AsmArgs& A, int e0, int nb) {
   return EXA_OK;
 }
 
+// The FP64 volume blocks D and B of the chunk on the DMMA tensor cores: for each field c, the
+// products T_(k,c) shapegt[:, :, 0] of all (element, k) pairs in one batched GEMM, written into
+// the columns of D (c < ncu) or B, elements in parts of c.wT_elems (vol_mat_kernel's sums).
+int volume_blocks_gemm(ExaCtx& c, int nb) {
+  const ExaDims& P = c.P;
+  const int npe = P.npe, nge = P.nge, ncu = P.ncu, nd = P.nd, n = P.n, nblk = P.ncu * P.nc;
+  const long long nqn = (long long)npe * nd * ncu, blk = (long long)npe * nge;
+  for (int le0 = 0; le0 < nb; le0 += c.wT_elems) {
+    const int nbs = std::min(c.wT_elems, nb - le0);
+    const long long tot = blk * nblk * nbs;
+    vol_t_kernel<<<(unsigned)std::min<long long>((tot + 255) / 256, 8192), 256, 0, c.st>>>(P, c.shapegw, c.wRg, le0,
+                                                                                         nbs, c.wT);
+    EXA_LAUNCH_CHECK();
+    for (int cc = 0; cc < P.nc; ++cc) {
+      GemmBatch g{};
+      g.M = npe; g.N = npe; g.K = nge; g.alpha = 1.0; g.beta = 0.0;
+      g.A = c.wT + (long long)ncu * cc * blk; g.lda = npe; g.sA = nblk * blk; g.sA2 = blk;
+      g.B = c.shapegt; g.ldb = nge;
+      if (cc < ncu) {
+        g.C = c.wD + (long long)le0 * n * n + (long long)n * npe * cc;
+        g.ldc = n; g.sC = (long long)n * n;
+      } else {
+        const int qc = cc - ncu, nq = qc % ncu, d = qc / ncu;
+        g.C = c.wB + (long long)le0 * n * nqn + (long long)n * ((long long)npe * d + (long long)npe * nd * nq);
+        g.ldc = n; g.sC = (long long)n * nqn;
+      }
+      g.sC2 = npe;  // trace component k: rows npe k
+      g.batch = nbs; g.batch2 = ncu;
+      EXA_TRY(exa_gemm(g, c.st));
+    }
+  }
+  return EXA_OK;
+}
+
 // Ru of the chunk = shapegw (npe x nge (nd + 1)) times the volume kernel's integrands
 int volume_residual_gemm(ExaCtx& c, double* Ruc, int nb) {
   const ExaDims& P = c.P;
@@ -362,6 +396,8 @@ int exa_model_assemble(ExaCtx& c, bool jacobian) {
             A.Bp = c.wBp;
           }
           EXA_TRY(exa_k_vol_mat_tc(P, c.shapegw32, c.Sp, c.wRg, c.wD, c.wB, bp, nb, c.d_uflag, c.st));
+        } else if (c.wT) {
+          EXA_TRY(volume_blocks_gemm(c, nb));
         } else {
           const int tiles = exa_ceil_div(P.npe, 64);
           dim3 grid(tiles * tiles, nb, P.ncu * P.nc);

@@ -61,6 +61,10 @@ struct ExaCtx {
   double *wD = nullptr, *wB = nullptr, *wF = nullptr, *wK = nullptr, *wG = nullptr, *wRg = nullptr, *wRu = nullptr;
   // per chunk: udg and sdg at the Gauss points and the Ru integrand (the volume kernel's GEMMs)
   double *wUG = nullptr, *wSG = nullptr, *wRG = nullptr;
+  // the volume blocks' left factors T = -(shapegw . rgJ) of up to wT_elems elements, for the
+  // FP64 volume products on the DMMA tensor cores
+  double* wT = nullptr;
+  int wT_elems = 0;
   double* wInv = nullptr;  // blocked-inverse workspace (n^2 per element) when n exceeds the register kernel
   // Krylov / Newton workspace
   double *V = nullptr, *x = nullptr, *r = nullptr, *w = nullptr, *we = nullptr, *du = nullptr;
