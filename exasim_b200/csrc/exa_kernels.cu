@@ -5,6 +5,10 @@
 // Every kernel maps one element (or one face) to one block, so the element-to-face
 // assembly needs no atomics: the first element of a face writes, the second adds,
 // as Exasim's PutElementFaceNodes pair does (backend/Common/kokkosimpl.h:1032-1065).
+#include <map>
+#include <mutex>
+#include <tuple>
+
 #include "exa_kernels.cuh"
 #include "exa_tc.cuh"
 #include "exa_umma.cuh"
@@ -240,29 +244,33 @@ __global__ void bj_apply_kernel(ExaDims P, const T* BE, const double* x, double*
 
 // y_e = alpha A_e x_e + beta y0_e for a batch of column-major M x K blocks A_e (leading
 // dimension M, batch stride sA; y0 may alias y).  x_e is read at x + e sx, or, with elemcon,
-// gathered from a trace vector: x_e[k] = x[k % ncu + ncu elemcon[k / ncu + ndf e]].  One
-// CTA per block: 8 warps split the columns (warp w takes c = w, w + 8, ...), CU at a time
-// with the next CU loaded ahead (CU = 2 where 4 would not fit the registers); lane l keeps
-// the partial sums of rows V l + 32 V i + v (i < RI, v < V) in registers, so each column is
-// one coalesced load per 32 V rows (V = 2: pairs of floats, as many bytes per load as FP64);
-// the 8 partial sums of a row meet in shared memory in a fixed order.  Serves the condensed matvec w_e = H_e gather(v)
-// (hdgMatVec, matvec.cpp:240-389) and the additive-Schwarz apply, du = Ru + D^-1 F x
-// (hdgGetDUDG, matvec.cpp:219-238) and the mixed form's Ru <- D^-1 Ru, Rh <- Rh - K Ru.
+// gathered from a trace vector: x_e[k] = x[k % ncu + ncu elemcon[k / ncu + ndf e]].
+// Persistent: CTA b takes blocks b, b + gridDim.x, ...  Per block, 8 warps split the columns
+// (warp w takes c = w, w + 8, ...), CU at a time with the next CU loaded ahead (CU = 2 where 4
+// would not fit the registers); lane l keeps the partial sums of rows V l + 32 V i + v
+// (i < RI, v < V) in registers, so each column is one coalesced load per 32 V rows (V = 2:
+// pairs of floats, as many bytes per load as FP64); the 8 partial sums of a row meet in shared
+// memory in a fixed order.  The first columns of the CTA's next block and its gathered x
+// (the other of two buffers) are loaded before the partial sums of the current one are
+// reduced, so their latency overlaps that step.  Serves the condensed matvec
+// w_e = H_e gather(v) (hdgMatVec, matvec.cpp:240-389) and the additive-Schwarz apply,
+// du = Ru + D^-1 F x (hdgGetDUDG, matvec.cpp:219-238) and the mixed form's Ru <- D^-1 Ru,
+// Rh <- Rh - K Ru.
 template <typename T, int RI, int V, int CU>
-__global__ void __launch_bounds__(256) bgemv_kernel(int M, int K, const T* A, long long sA, const double* x,
-                                                    long long sx, const int* elemcon, int ndf, int ncu,
-                                                    double alpha, double beta, const double* y0, double* y,
+__global__ void __launch_bounds__(256) bgemv_kernel(int M, int K, int batch, const T* A, long long sA,
+                                                    const double* x, long long sx, const int* elemcon, int ndf,
+                                                    int ncu, double alpha, double beta, const double* y0, double* y,
                                                     long long sy) {
   static_assert(V == 1 || (V == 2 && sizeof(T) == 4), "pairs of floats only");
   extern __shared__ double sm[];
-  double* xe = sm;         // [K]
-  double* part = sm + K;   // [8][M]
-  const long long e = blockIdx.x;
+  double* xb = sm;             // [2][K]
+  double* part = sm + 2 * K;   // [8][M]
+  long long e = blockIdx.x;
+  if (e >= batch) return;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const T* Ae = A + e * sA;
   // rows V (lane + 32 i) .. + V - 1 of column c0 + 8 u; with V = 2, M is even, so a pair is
   // either inside the block or past it, and 8-byte aligned
-  auto loadc = [&](int c0, T (&v)[CU][RI][V]) {
+  auto loadc = [&](const T* Ae, int c0, T (&v)[CU][RI][V]) {
 #pragma unroll
     for (int u = 0; u < CU; ++u) {
       const T* a = Ae + (long long)M * (c0 + 8 * u);
@@ -279,64 +287,83 @@ __global__ void __launch_bounds__(256) bgemv_kernel(int M, int K, const T* A, lo
       }
     }
   };
-  int c = warp;
+  auto gather = [&](long long eb, double* xe) {
+    for (int k = threadIdx.x; k < K; k += blockDim.x)
+      xe[k] = elemcon ? x[k % ncu + ncu * (long long)elemcon[k / ncu + (long long)ndf * eb]] : x[eb * sx + k];
+  };
+  int buf = 0;
   T a[CU][RI][V];
-  if (c + 8 * (CU - 1) < K) loadc(c, a);
-  for (int k = threadIdx.x; k < K; k += blockDim.x)
-    xe[k] = elemcon ? x[k % ncu + ncu * (long long)elemcon[k / ncu + (long long)ndf * e]] : x[e * sx + k];
+  if (warp + 8 * (CU - 1) < K) loadc(A + e * sA, warp, a);
+  gather(e, xb);
   __syncthreads();
-  double acc[RI][V];
+  for (;;) {
+    const T* Ae = A + e * sA;
+    const double* xe = xb + buf * K;
+    double acc[RI][V];
 #pragma unroll
-  for (int i = 0; i < RI; ++i)
+    for (int i = 0; i < RI; ++i)
 #pragma unroll
-    for (int w = 0; w < V; ++w) acc[i][w] = 0.0;
-  for (; c + 8 * (CU - 1) < K; c += 8 * CU) {
-    T an[CU][RI][V];
-    const bool more = c + 8 * CU + 8 * (CU - 1) < K;
-    if (more) loadc(c + 8 * CU, an);
+      for (int w = 0; w < V; ++w) acc[i][w] = 0.0;
+    int c = warp;
+    for (; c + 8 * (CU - 1) < K; c += 8 * CU) {
+      T an[CU][RI][V];
+      const bool more = c + 8 * CU + 8 * (CU - 1) < K;
+      if (more) loadc(Ae, c + 8 * CU, an);
 #pragma unroll
-    for (int u = 0; u < CU; ++u) {
-      const double xv = xe[c + 8 * u];
-#pragma unroll
-      for (int i = 0; i < RI; ++i)
-#pragma unroll
-        for (int w = 0; w < V; ++w) acc[i][w] = fma((double)a[u][i][w], xv, acc[i][w]);
-    }
-    if (more) {
-#pragma unroll
-      for (int u = 0; u < CU; ++u)
+      for (int u = 0; u < CU; ++u) {
+        const double xv = xe[c + 8 * u];
 #pragma unroll
         for (int i = 0; i < RI; ++i)
 #pragma unroll
-          for (int w = 0; w < V; ++w) a[u][i][w] = an[u][i][w];
-    }
-  }
-  for (; c < K; c += 8) {
-    const T* a0 = Ae + (long long)M * c;
-    const double xv = xe[c];
+          for (int w = 0; w < V; ++w) acc[i][w] = fma((double)a[u][i][w], xv, acc[i][w]);
+      }
+      if (more) {
 #pragma unroll
-    for (int i = 0; i < RI; ++i) {
-      const int r = V * (lane + 32 * i);
-      if (r < M) {
+        for (int u = 0; u < CU; ++u)
 #pragma unroll
-        for (int w = 0; w < V; ++w) acc[i][w] = fma((double)a0[r + w], xv, acc[i][w]);
+          for (int i = 0; i < RI; ++i)
+#pragma unroll
+            for (int w = 0; w < V; ++w) a[u][i][w] = an[u][i][w];
       }
     }
-  }
+    for (; c < K; c += 8) {
+      const T* a0 = Ae + (long long)M * c;
+      const double xv = xe[c];
 #pragma unroll
-  for (int i = 0; i < RI; ++i)
+      for (int i = 0; i < RI; ++i) {
+        const int r = V * (lane + 32 * i);
+        if (r < M) {
 #pragma unroll
-    for (int w = 0; w < V; ++w) {
-      const int r = V * (lane + 32 * i) + w;
-      if (r < M) part[warp * M + r] = acc[i][w];
+          for (int w = 0; w < V; ++w) acc[i][w] = fma((double)a0[r + w], xv, acc[i][w]);
+        }
+      }
     }
-  __syncthreads();
-  for (int r = threadIdx.x; r < M; r += blockDim.x) {
-    double s = 0.0;
+    // the next block's first columns and x, in flight while this block's sums are reduced
+    const long long en = e + gridDim.x;
+    const bool next = en < batch;
+    if (next) {
+      if (warp + 8 * (CU - 1) < K) loadc(A + en * sA, warp, a);
+      gather(en, xb + (buf ^ 1) * K);
+    }
 #pragma unroll
-    for (int w = 0; w < 8; ++w) s += part[w * M + r];
-    const double prev = beta != 0.0 ? y0[e * sy + r] : 0.0;
-    y[e * sy + r] = alpha * s + beta * prev;
+    for (int i = 0; i < RI; ++i)
+#pragma unroll
+      for (int w = 0; w < V; ++w) {
+        const int r = V * (lane + 32 * i) + w;
+        if (r < M) part[warp * M + r] = acc[i][w];
+      }
+    __syncthreads();
+    for (int r = threadIdx.x; r < M; r += blockDim.x) {
+      double s = 0.0;
+#pragma unroll
+      for (int w = 0; w < 8; ++w) s += part[w * M + r];
+      const double prev = beta != 0.0 ? y0[e * sy + r] : 0.0;
+      y[e * sy + r] = alpha * s + beta * prev;
+    }
+    __syncthreads();  // part is rewritten and the other x buffer read next
+    if (!next) break;
+    e = en;
+    buf ^= 1;
   }
 }
 
@@ -472,6 +499,31 @@ int launch_bgemv_bulk(int M, int K, int cw, int batch, const float* A, long long
   return EXA_OK;
 }
 
+// CTAs of a persistent batched-gemv launch: the blocks per SM that the instance's registers
+// and shared memory allow (cached per instance, device and shared-memory size) times the SMs
+int bgemv_grid(const void* kern, size_t smem, int batch) {
+  static std::mutex mu;
+  static std::map<std::tuple<const void*, int, size_t>, int> cache;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return batch;
+  int per = 0;
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = cache.find({kern, dev, smem});
+    if (it != cache.end()) per = it->second;
+  }
+  if (per == 0) {
+    int sms = 0, occ = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, 256, smem) != cudaSuccess || occ <= 0 || sms <= 0)
+      return batch;  // one CTA per block
+    per = occ * sms;
+    std::lock_guard<std::mutex> lk(mu);
+    cache[{kern, dev, smem}] = per;
+  }
+  return batch < per ? batch : per;
+}
+
 template <typename T>
 int launch_bgemv(int M, int K, int batch, const T* A, long long sA, const double* x, long long sx,
                  const int* elemcon, int ndf, int ncu, double alpha, double beta, const double* y0, double* y,
@@ -488,10 +540,15 @@ int launch_bgemv(int M, int K, int batch, const T* A, long long sA, const double
     if (cw > 0 && (reinterpret_cast<uintptr_t>(A) & 15) == 0)
       return launch_bgemv_bulk(M, K, cw, batch, A, sA, x, sx, elemcon, ndf, ncu, alpha, beta, y0, y, sy, flag, st);
   }
-  const size_t smem = sizeof(double) * ((size_t)(K > 0 ? K : 1) + 8 * (size_t)M);
+  const size_t smem = sizeof(double) * (2 * (size_t)(K > 0 ? K : 1) + 8 * (size_t)M);
+  // persistent: as many CTAs as fit on the device at once (the occupancy of the instance, taken
+  // once per instance and device), at most one per block
 #define EXA_BGEMV(R, V)                                                                                     \
-  bgemv_kernel<T, R, V, (sizeof(T) == 8 && R > 12) ? 2 : 4>                                                   \
-      <<<batch, 256, smem, st>>>(M, K, A, sA, x, sx, elemcon, ndf, ncu, alpha, beta, y0, y, sy)
+  do {                                                                                                      \
+    auto kern = bgemv_kernel<T, R, V, (sizeof(T) == 8 && R > 12) ? 2 : 4>;                                    \
+    const int g = bgemv_grid((const void*)kern, smem, batch);                                               \
+    kern<<<g, 256, smem, st>>>(M, K, batch, A, sA, x, sx, elemcon, ndf, ncu, alpha, beta, y0, y, sy);      \
+  } while (0)
   // rows covered per warp with single rows (RI from 1-6, 8, 10, 12, 16) and with pairs (RI from
   // 1-6, 8): pairs only where they pad no more rows (m = 150: 160 single against 192 paired)
   auto inst = [](int r, bool pairs) {

@@ -1,7 +1,7 @@
 // exasim_b200_<model>: the solver as an executable, in place of the reference's
 // cput2cEXASIM / gput2cEXASIM for an HDG problem (backend/Main/main.cpp, Main/exasim.hpp).
 //
-//   exasim_b200_<model> <datain dir> <output prefix> [restart] [device] [--checkpoint]
+//   exasim_b200_<model> <datain dir> <output prefix> [restart] [device] [--checkpoint] [--vtu]
 //
 // reads <datain dir>/{app,master,mesh,sol}.bin as text2code writes them, solves through the
 // library's C ABI (steady: Newton; time dependent: every DIRK step of app.bin), and writes
@@ -19,6 +19,11 @@
 // words, inserted into udg) with saveSolOpt 0, else all of udg; then uhat.  --checkpoint
 // writes those two files, numbered by step + R, at every saved step, so a later run can
 // restart from any of them.
+//
+// --vtu writes each saved snapshot for visualization as well (exa_vtu.h): <output prefix>vis.vtu
+// for a steady problem; <output prefix>vis_<step>.vtu per saved step and <output prefix>vis.pvd,
+// the time series, for a time-dependent one (the reference's SaveParaview names,
+// solution.cpp:861-880).
 // Exit status 0, or 1 with the library's message on stderr.
 #include <algorithm>
 #include <cstdio>
@@ -28,6 +33,7 @@
 #include <vector>
 
 #include "../../include/exasim_b200.h"
+#include "exa_vtu.h"
 
 namespace {
 
@@ -87,14 +93,15 @@ struct Output {
 
 int main(int argc, char** argv) {
   std::vector<std::string> pos;
-  bool checkpoint = false;
+  bool checkpoint = false, vtu = false;
   for (int i = 1; i < argc; ++i) {
     const std::string a = argv[i];
     if (a == "--checkpoint") checkpoint = true;
+    else if (a == "--vtu") vtu = true;
     else pos.push_back(a);
   }
   if (pos.size() < 2) {
-    std::fprintf(stderr, "usage: %s <datain dir> <output prefix> [restart] [device] [--checkpoint]\n", argv[0]);
+    std::fprintf(stderr, "usage: %s <datain dir> <output prefix> [restart] [device] [--checkpoint] [--vtu]\n", argv[0]);
     return 1;
   }
   const std::string din = pos[0] + "/", prefix = pos[1];
@@ -155,6 +162,23 @@ int main(int argc, char** argv) {
   Output oudg, ouh;
   oudg.open(prefix + "udg_np0.bin", (double)npe, (double)ncs, (double)ne);
   ouh.open(prefix + "uhat_np0.bin", (double)ncu, (double)npf, (double)nf);
+  // visualization: the master element's lattice and the nodes' coordinates
+  const std::vector<double> mnd = part(master, 0), xpe = part(master, 9), xdg = part(sol, 1);
+  const int vnd = mnd.size() > 5 ? (int)mnd[0] : 0, vet = mnd.size() > 5 ? (int)mnd[1] : 0;
+  const int vp = mnd.size() > 5 ? (int)mnd[3] : 0;
+  const int ncx = npe * ne > 0 ? (int)(xdg.size() / (size_t)(npe * ne)) : 0;
+  std::vector<std::string> vis_files;
+  std::vector<double> vis_times;
+  double tnow = 0.0;  // the time of the state being saved (time-dependent runs)
+  auto visualize = [&](int step) {
+    const std::string name = tdep ? "vis_" + std::to_string(step) + ".vtu" : "vis.vtu";
+    if (!exa_vtu::write(prefix + name, vnd, vet, vp, (int)npe, xpe.data(), ne, ncx, xdg.data(), (int)nc, udg.data())) {
+      std::fprintf(stderr, "cannot write %s%s\n", prefix.c_str(), name.c_str());
+      std::exit(1);
+    }
+    vis_files.push_back(name);
+    vis_times.push_back(tnow);
+  };
   auto save = [&](int step) {
     check(exa_get_field(ctx, "udg", udg.data(), (long long)udg.size()), "exa_get_field udg");
     check(exa_get_field(ctx, "uh", uh.data(), (long long)uh.size()), "exa_get_field uh");
@@ -168,6 +192,7 @@ int main(int argc, char** argv) {
     const std::vector<double>& us = ncs == nc ? udg : u;
     oudg.write(us);
     ouh.write(uh);
+    if (vtu) visualize(step);
     if (checkpoint && step > 0) {
       // the restart files of this step, raw (solution.cpp:804-828 reads them so)
       Output cu, ch;
@@ -184,14 +209,22 @@ int main(int argc, char** argv) {
     std::printf("Newton: %d steps, residual norm %.6e\n", its, nrm);
     save(0);
   } else {
+    // the start time: app.bin's factor[0] (time), or R dt[0] on a restart (exasim.hpp:390-393)
+    const std::vector<double> factor = part(app, 5);
+    tnow = restart > 0 ? restart * dt[0] : (factor.empty() ? 0.0 : factor[0]);
     for (int istep = 0; istep < (int)dt.size(); ++istep) {
       for (int j = 0; j < nstage; ++j) {
         int its = 0;
         double nrm = 0.0;
         check(exa_dirk_stage(ctx, istep, j, &its, &nrm), "exa_dirk_stage");
       }
+      tnow += dt[istep];
       std::printf("step %d done\n", istep + 1 + restart);
       if ((istep + 1) % freq == 0) save(istep + 1 + restart);
+    }
+    if (vtu && !exa_vtu::write_pvd(prefix + "vis.pvd", vis_files, vis_times)) {
+      std::fprintf(stderr, "cannot write %svis.pvd\n", prefix.c_str());
+      return 1;
     }
   }
   exa_destroy(ctx);

@@ -5,7 +5,8 @@ solution to the tolerance of the library-level golden test (1e-10 relative); for
 the last udg snapshot must equal the library's own DIRK result bit for bit; and a run restarted
 from a step's checkpoint files (ReadSolutions, backend/Solution/solution.cpp:804-828, with the
 restart argument of backend/Main/exasim.hpp:338-348, 387-393) must end in the same state, bit
-for bit, as the uninterrupted run."""
+for bit, as the uninterrupted run; with --vtu, each saved step's VTK file holds that step's
+udg and the .pvd series their times."""
 import shutil
 import os
 import subprocess
@@ -87,3 +88,22 @@ def test_executable_restart_matches_uninterrupted_run(tmp_path):
     r = subprocess.run([B.exe_path("convdiff3d"), db, str(tmp_path / "none"), "3"], capture_output=True, text=True,
                        timeout=300)
     assert r.returncode == 1 and "cannot open" in r.stderr
+
+
+def test_executable_writes_vtu_snapshots(tmp_path):
+    from tests.test_cpu_vtu import read_vtu
+    d = cases.convdiff3d_hex(str(tmp_path / "cd"), n=2, porder=2, nsteps=2, dt=0.01)
+    out = str(tmp_path / "o")
+    run("convdiff3d", d, out, "--vtu")
+    udg = np.fromfile(out + "udg_np0.bin")
+    npe, nc, ne = (int(v) for v in udg[:3])
+    snaps = udg[3:].reshape(-1, npe * nc * ne)
+    for k in (1, 2):
+        npts, ncell, a = read_vtu(out + f"vis_{k}.vtu")
+        assert npts == npe * ne and ncell == 8 * ne       # p^3 hexahedra per element
+        u = snaps[k - 1].reshape(npe, nc, ne, order="F")
+        for q in range(nc):
+            assert np.array_equal(a[f"udg{q}"], u[:, q, :].ravel(order="F").astype(np.float32))
+    pvd = open(out + "vis.pvd").read()
+    times = [float(t) for t in __import__("re").findall(r'timestep="([^"]+)"', pvd)]
+    assert times == pytest.approx([0.01, 0.02]) and "vis_1.vtu" in pvd and "vis_2.vtu" in pvd
