@@ -541,12 +541,15 @@ int launch_bgemv(int M, int K, int batch, const T* A, long long sA, const double
       return launch_bgemv_bulk(M, K, cw, batch, A, sA, x, sx, elemcon, ndf, ncu, alpha, beta, y0, y, sy, flag, st);
   }
   const size_t smem = sizeof(double) * (2 * (size_t)(K > 0 ? K : 1) + 8 * (size_t)M);
-  // persistent: as many CTAs as fit on the device at once (the occupancy of the instance, taken
-  // once per instance and device), at most one per block
+  // FP64 blocks persistent: as many CTAs as fit on the device at once (the occupancy of the
+  // instance, taken once per instance and device).  FP32 blocks one CTA per block: their
+  // blocks are half the bytes, and the last round of a persistent launch (blocks / CTAs is not
+  // whole) idled more than the overlap of the next block's loads saved (0.104 against 0.096 ms
+  // per matvec of the benchmark workload, against 0.140 and 0.145 ms for the FP64 blocks)
 #define EXA_BGEMV(R, V)                                                                                     \
   do {                                                                                                      \
     auto kern = bgemv_kernel<T, R, V, (sizeof(T) == 8 && R > 12) ? 2 : 4>;                                    \
-    const int g = bgemv_grid((const void*)kern, smem, batch);                                               \
+    const int g = sizeof(T) == 8 ? bgemv_grid((const void*)kern, smem, batch) : batch;                      \
     kern<<<g, 256, smem, st>>>(M, K, batch, A, sA, x, sx, elemcon, ndf, ncu, alpha, beta, y0, y, sy);      \
   } while (0)
   // rows covered per warp with single rows (RI from 1-6, 8, 10, 12, 16) and with pairs (RI from
