@@ -325,10 +325,50 @@ __global__ void face_kernel(AsmArgs A, double* Ru, double* Rh, double* D, double
   double* fh_uh = fh_uq + ngf * ncu * nc;    // ngf*ncu*ncu
   double* fb_uq = fh_uh + ngf * ncu * ncu;   // ngf*ncu*nc
   double* fb_uh = fb_uq + ngf * ncu * nc;    // ngf*ncu*ncu
+  // JAC: index tables of the block placement, filled once per element (no divisions per entry):
+  // column q = k + ncu c of the derivatives as k | c << 8 | (c - ncu) % ncu << 16 | (c - ncu) / ncu
+  // << 24; the row parts of the packed offsets of B (rows of Ru) and G (trace rows), with the
+  // row groups of their tiles
+  int* qtab = reinterpret_cast<int*>(fb_uh + ngf * ncu * ncu);  // ncu*nc
+  int* brow = qtab + ncu * nc;  // n: row part, then n: groups of the row's tile
+  int* grow = brow + 2 * n;     // m, m
+  // JAC in the mixed form (packed G given): the pair products in FP32, from FP32 copies of the
+  // face weights (once per element) and of each face's flux derivatives
+  const bool f32 = JAC && A.Gp.hi != nullptr;
+  float* sW32 = reinterpret_cast<float*>(grow + 2 * m);  // npf*ngf
+  float* sT32 = sW32 + npf * ngf;                        // ngf*npf
+  float* fq32 = sT32 + npf * ngf;                        // ngf*ncu*nc: fh_uq
+  float* fTq32 = fq32 + ngf * ncu * nc;                  // ngf*ncu*nc: trace-row u-q derivatives
+  float* fh32 = fTq32 + ngf * ncu * nc;                  // ngf*ncu*ncu: fh_uh
+  float* fTh32 = fh32 + ngf * ncu * ncu;                 // ngf*ncu*ncu: trace-row uhat derivatives
   __shared__ int s_ib;
   for (int t = threadIdx.x; t < npf * ngf; t += blockDim.x) {
     sW[t] = A.shapfgw[t];
     sT[t] = A.shapfgt[t];
+  }
+  if (f32)
+    for (int t = threadIdx.x; t < npf * ngf; t += blockDim.x) {
+      sW32[t] = (float)A.shapfgw[t];
+      sT32[t] = (float)A.shapfgt[t];
+    }
+  if (JAC) {
+    for (int q = threadIdx.x; q < ncu * nc; q += blockDim.x) {
+      const int k = q % ncu, c = q / ncu;
+      const int qc = c < ncu ? 0 : c - ncu;
+      qtab[q] = k | (c << 8) | ((qc % ncu) << 16) | ((qc / ncu) << 24);
+    }
+    auto rowpart = [](int row, int R, int K, int TR, int& ng) {
+      const int nkc = (K + exa_tc::PK - 1) / exa_tc::PK;
+      const int t = row / TR, rl = row - t * TR;
+      const int rows_t = (R - t * TR) < TR ? (R - t * TR) : TR;
+      ng = (rows_t + 7) / 8;
+      return t * (TR / 8) * nkc * 128 + (rl >> 3) * 128 + (rl & 7) * 4;
+    };
+    const int qg = exa_tc::qk_group(npe);
+    if (A.Bp.hi)
+      for (int r = threadIdx.x; r < n; r += blockDim.x) brow[r] = rowpart(r, n, qg * nd, A.Bp.TR, brow[n + r]);
+    if (A.Gp.hi)
+      for (int r = threadIdx.x; r < m; r += blockDim.x) grow[r] = rowpart(r, m, qg * nd, A.Gp.TR, grow[m + r]);
   }
 
   const double* U = A.udg + (long long)e * npe * nc;
@@ -449,67 +489,90 @@ __global__ void face_kernel(AsmArgs A, double* Ru, double* Rh, double* D, double
       constexpr int QC = 4;
       const int nq = ncu * nc;
       const int qg = exa_tc::qk_group(npe);  // K group of the packed B and G
-      for (int ab = threadIdx.x; ab < npf * npf; ab += blockDim.x) {
-        const int a = ab % npf, b = ab / npf;
-        const int pa = pl[a], pb = pl[b];
-        for (int q0 = 0; q0 < nq; q0 += QC) {
-          double vq[QC], vT[QC], vh[QC], vTh[QC];
-#pragma unroll
-          for (int u = 0; u < QC; ++u) vq[u] = vT[u] = vh[u] = vTh[u] = 0.0;
-          for (int g = 0; g < ngf; ++g) {
-            const double w = sW[a + npf * g] * sT[g + ngf * b];
-#pragma unroll
-            for (int u = 0; u < QC; ++u) {
-              const int q = q0 + u;
-              if (q < nq) {
-                vq[u] = fma(w, fh_uq[g + ngf * q], vq[u]);
-                vT[u] = fma(w, fT_uq[g + ngf * q], vT[u]);
-                if (q < ncu * ncu) {
-                  vh[u] = fma(w, fh_uh[g + ngf * q], vh[u]);
-                  vTh[u] = fma(w, fT_uh[g + ngf * q], vTh[u]);
+      // the pair products of the face, in TA (FP64, or FP32 in the mixed form)
+      auto pairs = [&](auto zero, const auto* W, const auto* Tt, const auto* fq, const auto* fTq, const auto* fh,
+                       const auto* fTh) {
+        using TA = decltype(zero);
+        for (int ab = threadIdx.x; ab < npf * npf; ab += blockDim.x) {
+          const int a = ab % npf, b = ab / npf;
+          const int pa = pl[a], pb = pl[b];
+          for (int q0 = 0; q0 < nq; q0 += QC) {
+            TA vq[QC], vT[QC], vh[QC], vTh[QC];
+  #pragma unroll
+            for (int u = 0; u < QC; ++u) vq[u] = vT[u] = vh[u] = vTh[u] = TA(0);
+            for (int g = 0; g < ngf; ++g) {
+              const TA w = W[a + npf * g] * Tt[g + ngf * b];
+  #pragma unroll
+              for (int u = 0; u < QC; ++u) {
+                const int q = q0 + u;
+                if (q < nq) {
+                  vq[u] = fma(w, fq[g + ngf * q], vq[u]);
+                  vT[u] = fma(w, fTq[g + ngf * q], vT[u]);
+                  if (q < ncu * ncu) {
+                    vh[u] = fma(w, fh[g + ngf * q], vh[u]);
+                    vTh[u] = fma(w, fTh[g + ngf * q], vTh[u]);
+                  }
                 }
               }
             }
-          }
-#pragma unroll
-          for (int u = 0; u < QC; ++u) {
-            const int q = q0 + u;
-            if (q >= nq) break;
-            const int k = q % ncu, c = q / ncu;
-            const int row_e = pa + npe * k;             // element row (i,k)
-            const int row_t = k + ncu * (a + npf * l);  // trace row (k, jf)
-            if (c < ncu) {
-              De[row_e + (long long)n * (pb + npe * c)] += vq[u];
-              Fe[row_e + (long long)n * (c + ncu * (b + npf * l))] = vh[u];
-              Ke[row_t + (long long)m * (pb + npe * c)] = vT[u];
-              He[row_t + (long long)m * (c + ncu * (b + npf * l))] = vTh[u];
-            } else {
-              const int qc = c - ncu, nqc = qc % ncu, d = qc / ncu;
-              const long long col = pb + (long long)npe * d + (long long)npe * nd * nqc;
-              if (A.Bp.hi) {
-                float* bp = A.Bp.hi + (long long)le * A.Bp.sb + (long long)nqc * A.Bp.sb2 +
-                            exa_tc::pack_off(row_e, pb + qg * d, n, qg * nd, A.Bp.TR);
-                *bp += (float)vq[u];
+  #pragma unroll
+            for (int u = 0; u < QC; ++u) {
+              const int q = q0 + u;
+              if (q >= nq) break;
+              const int qd = qtab[q];
+              const int k = qd & 255, c = (qd >> 8) & 255;
+              const int row_e = pa + npe * k;             // element row (i,k)
+              const int row_t = k + ncu * (a + npf * l);  // trace row (k, jf)
+              if (c < ncu) {
+                De[row_e + (long long)n * (pb + npe * c)] += vq[u];
+                Fe[row_e + (long long)n * (c + ncu * (b + npf * l))] = vh[u];
+                Ke[row_t + (long long)m * (pb + npe * c)] = vT[u];
+                He[row_t + (long long)m * (c + ncu * (b + npf * l))] = vTh[u];
               } else {
-                Be[row_e + (long long)n * col] += vq[u];
-              }
-              if (A.Gp.hi) {
-                const long long o = (long long)le * A.Gp.sb + (long long)nqc * A.Gp.sb2 +
-                                    exa_tc::pack_off(row_t, pb + qg * d, m, qg * nd, A.Gp.TR);
-                if (A.Gp.lo) {
-                  float h, lo;
-                  exa_tc::split_tf32(vT[u], h, lo);
-                  A.Gp.hi[o] = h;
-                  A.Gp.lo[o] = lo;
+                const int nqc = (qd >> 16) & 255, d = qd >> 24;
+                const long long col = pb + (long long)npe * d + (long long)npe * nd * nqc;
+                // packed column part of k = pb + qg d for a row of ng groups (pack_off's k terms)
+                const int kk = pb + qg * d;
+                auto colpart = [kk](int ng) { return (kk >> 4) * ng * 128 + ((kk >> 2) & 3) * 32 + (kk & 3); };
+                if (A.Bp.hi) {
+                  float* bp = A.Bp.hi + (long long)le * A.Bp.sb + (long long)nqc * A.Bp.sb2 + brow[row_e] +
+                              colpart(brow[n + row_e]);
+                  *bp += (float)vq[u];
                 } else {
-                  A.Gp.hi[o] = (float)vT[u];  // FP32 operand, split by the GEMM on chip
+                  Be[row_e + (long long)n * col] += vq[u];
                 }
-              } else {
-                Ge[row_t + (long long)m * col] = vT[u];
+                if (A.Gp.hi) {
+                  const long long o = (long long)le * A.Gp.sb + (long long)nqc * A.Gp.sb2 + grow[row_t] +
+                                      colpart(grow[m + row_t]);
+                  if (A.Gp.lo) {
+                    float h, lo;
+                    exa_tc::split_tf32(vT[u], h, lo);
+                    A.Gp.hi[o] = h;
+                    A.Gp.lo[o] = lo;
+                  } else {
+                    A.Gp.hi[o] = (float)vT[u];  // FP32 operand, split by the GEMM on chip
+                  }
+                } else {
+                  Ge[row_t + (long long)m * col] = vT[u];
+                }
               }
             }
           }
         }
+      };
+      if (f32) {
+        for (int t = threadIdx.x; t < ngf * ncu * nc; t += blockDim.x) {
+          fq32[t] = (float)fh_uq[t];
+          fTq32[t] = (float)fT_uq[t];
+        }
+        for (int t = threadIdx.x; t < ngf * ncu * ncu; t += blockDim.x) {
+          fh32[t] = (float)fh_uh[t];
+          fTh32[t] = (float)fT_uh[t];
+        }
+        __syncthreads();
+        pairs(0.0f, sW32, sT32, fq32, fTq32, fh32, fTh32);
+      } else {
+        pairs(0.0, sW, sT, fh_uq, fT_uq, fh_uh, fT_uh);
       }
     }
     __syncthreads();
@@ -520,7 +583,11 @@ inline size_t face_smem(const ExaDims& P, bool jac) {
   size_t s = (size_t)P.npf * (P.ncu + P.nc) + (size_t)P.ngf * (P.ncu + 2 * P.nc + P.ncu * P.nd + 2 * P.ncu);
   if (jac) s += (size_t)P.ngf * P.ncu * (P.nd * P.nc + 2 * P.nc + 2 * P.ncu);
   s += 2 * (size_t)P.npf * P.ngf;  // shapfgw, shapfgt
-  return s * sizeof(double);
+  // the JAC index tables (ints): derivative columns, packed row parts of B and G; then the
+  // FP32 copies of the mixed form's pair products (floats)
+  const size_t ti = jac ? (size_t)P.ncu * P.nc + 2 * (size_t)P.n + 2 * (size_t)P.m : 0;
+  const size_t tf = jac ? 2 * (size_t)P.npf * P.ngf + 2 * (size_t)P.ngf * P.ncu * (P.nc + P.ncu) : 0;
+  return s * sizeof(double) + ti * sizeof(int) + tf * sizeof(float);
 }
 
 // Binds a generated model namespace to the argument roles the kernels use

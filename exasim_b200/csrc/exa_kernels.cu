@@ -244,8 +244,108 @@ __global__ void bj_apply_kernel(ExaDims P, const T* BE, const double* x, double*
 
 // y_e = alpha A_e x_e + beta y0_e for a batch of column-major M x K blocks A_e (leading
 // dimension M, batch stride sA; y0 may alias y).  x_e is read at x + e sx, or, with elemcon,
-// gathered from a trace vector: x_e[k] = x[k % ncu + ncu elemcon[k / ncu + ndf e]].
-// Persistent: CTA b takes blocks b, b + gridDim.x, ...  Per block, 8 warps split the columns
+// gathered from a trace vector: x_e[k] = x[k % ncu + ncu elemcon[k / ncu + ndf e]].  One
+// CTA per block: 8 warps split the columns (warp w takes c = w, w + 8, ...), CU at a time
+// with the next CU loaded ahead (CU = 2 where 4 would not fit the registers); lane l keeps
+// the partial sums of rows V l + 32 V i + v (i < RI, v < V) in registers, so each column is
+// one coalesced load per 32 V rows (V = 2: pairs of floats, as many bytes per load as FP64);
+// the 8 partial sums of a row meet in shared memory in a fixed order.  Serves the condensed matvec w_e = H_e gather(v)
+// (hdgMatVec, matvec.cpp:240-389) and the additive-Schwarz apply, du = Ru + D^-1 F x
+// (hdgGetDUDG, matvec.cpp:219-238) and the mixed form's Ru <- D^-1 Ru, Rh <- Rh - K Ru.
+template <typename T, int RI, int V, int CU>
+__global__ void __launch_bounds__(256) bgemv_kernel(int M, int K, const T* A, long long sA, const double* x,
+                                                    long long sx, const int* elemcon, int ndf, int ncu,
+                                                    double alpha, double beta, const double* y0, double* y,
+                                                    long long sy) {
+  static_assert(V == 1 || (V == 2 && sizeof(T) == 4), "pairs of floats only");
+  extern __shared__ double sm[];
+  double* xe = sm;         // [K]
+  double* part = sm + K;   // [8][M]
+  const long long e = blockIdx.x;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const T* Ae = A + e * sA;
+  // rows V (lane + 32 i) .. + V - 1 of column c0 + 8 u; with V = 2, M is even, so a pair is
+  // either inside the block or past it, and 8-byte aligned
+  auto loadc = [&](int c0, T (&v)[CU][RI][V]) {
+#pragma unroll
+    for (int u = 0; u < CU; ++u) {
+      const T* a = Ae + (long long)M * (c0 + 8 * u);
+#pragma unroll
+      for (int i = 0; i < RI; ++i) {
+        const int r = V * (lane + 32 * i);
+        if constexpr (V == 2) {
+          const float2 t = r < M ? *reinterpret_cast<const float2*>(a + r) : make_float2(0.f, 0.f);
+          v[u][i][0] = t.x;
+          v[u][i][1] = t.y;
+        } else {
+          v[u][i][0] = r < M ? a[r] : T(0);
+        }
+      }
+    }
+  };
+  int c = warp;
+  T a[CU][RI][V];
+  if (c + 8 * (CU - 1) < K) loadc(c, a);
+  for (int k = threadIdx.x; k < K; k += blockDim.x)
+    xe[k] = elemcon ? x[k % ncu + ncu * (long long)elemcon[k / ncu + (long long)ndf * e]] : x[e * sx + k];
+  __syncthreads();
+  double acc[RI][V];
+#pragma unroll
+  for (int i = 0; i < RI; ++i)
+#pragma unroll
+    for (int w = 0; w < V; ++w) acc[i][w] = 0.0;
+  for (; c + 8 * (CU - 1) < K; c += 8 * CU) {
+    T an[CU][RI][V];
+    const bool more = c + 8 * CU + 8 * (CU - 1) < K;
+    if (more) loadc(c + 8 * CU, an);
+#pragma unroll
+    for (int u = 0; u < CU; ++u) {
+      const double xv = xe[c + 8 * u];
+#pragma unroll
+      for (int i = 0; i < RI; ++i)
+#pragma unroll
+        for (int w = 0; w < V; ++w) acc[i][w] = fma((double)a[u][i][w], xv, acc[i][w]);
+    }
+    if (more) {
+#pragma unroll
+      for (int u = 0; u < CU; ++u)
+#pragma unroll
+        for (int i = 0; i < RI; ++i)
+#pragma unroll
+          for (int w = 0; w < V; ++w) a[u][i][w] = an[u][i][w];
+    }
+  }
+  for (; c < K; c += 8) {
+    const T* a0 = Ae + (long long)M * c;
+    const double xv = xe[c];
+#pragma unroll
+    for (int i = 0; i < RI; ++i) {
+      const int r = V * (lane + 32 * i);
+      if (r < M) {
+#pragma unroll
+        for (int w = 0; w < V; ++w) acc[i][w] = fma((double)a0[r + w], xv, acc[i][w]);
+      }
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < RI; ++i)
+#pragma unroll
+    for (int w = 0; w < V; ++w) {
+      const int r = V * (lane + 32 * i) + w;
+      if (r < M) part[warp * M + r] = acc[i][w];
+    }
+  __syncthreads();
+  for (int r = threadIdx.x; r < M; r += blockDim.x) {
+    double s = 0.0;
+#pragma unroll
+    for (int w = 0; w < 8; ++w) s += part[w * M + r];
+    const double prev = beta != 0.0 ? y0[e * sy + r] : 0.0;
+    y[e * sy + r] = alpha * s + beta * prev;
+  }
+}
+
+// The same product, persistent (for FP64 blocks): CTA b takes blocks b, b + gridDim.x, ...
+// Per block, 8 warps split the columns
 // (warp w takes c = w, w + 8, ...), CU at a time with the next CU loaded ahead (CU = 2 where 4
 // would not fit the registers); lane l keeps the partial sums of rows V l + 32 V i + v
 // (i < RI, v < V) in registers, so each column is one coalesced load per 32 V rows (V = 2:
@@ -257,7 +357,7 @@ __global__ void bj_apply_kernel(ExaDims P, const T* BE, const double* x, double*
 // du = Ru + D^-1 F x (hdgGetDUDG, matvec.cpp:219-238) and the mixed form's Ru <- D^-1 Ru,
 // Rh <- Rh - K Ru.
 template <typename T, int RI, int V, int CU>
-__global__ void __launch_bounds__(256) bgemv_kernel(int M, int K, int batch, const T* A, long long sA,
+__global__ void __launch_bounds__(256) bgemv_pers_kernel(int M, int K, int batch, const T* A, long long sA,
                                                     const double* x, long long sx, const int* elemcon, int ndf,
                                                     int ncu, double alpha, double beta, const double* y0, double* y,
                                                     long long sy) {
@@ -541,16 +641,22 @@ int launch_bgemv(int M, int K, int batch, const T* A, long long sA, const double
       return launch_bgemv_bulk(M, K, cw, batch, A, sA, x, sx, elemcon, ndf, ncu, alpha, beta, y0, y, sy, flag, st);
   }
   const size_t smem = sizeof(double) * (2 * (size_t)(K > 0 ? K : 1) + 8 * (size_t)M);
-  // FP64 blocks persistent: as many CTAs as fit on the device at once (the occupancy of the
-  // instance, taken once per instance and device).  FP32 blocks one CTA per block: their
-  // blocks are half the bytes, and the last round of a persistent launch (blocks / CTAs is not
-  // whole) idled more than the overlap of the next block's loads saved (0.104 against 0.096 ms
-  // per matvec of the benchmark workload, against 0.140 and 0.145 ms for the FP64 blocks)
+  const size_t smem1 = sizeof(double) * ((size_t)(K > 0 ? K : 1) + 8 * (size_t)M);
+  // FP64 blocks persistent (bgemv_pers_kernel): as many CTAs as fit on the device at once (the
+  // occupancy of the instance, taken once per instance and device).  FP32 blocks one CTA per
+  // block (bgemv_kernel): their blocks are half the bytes, and the persistent form was slower
+  // for them (0.104 against 0.096 ms per matvec of the benchmark workload; 0.140 against 0.145
+  // ms for its FP64 blocks)
 #define EXA_BGEMV(R, V)                                                                                     \
   do {                                                                                                      \
-    auto kern = bgemv_kernel<T, R, V, (sizeof(T) == 8 && R > 12) ? 2 : 4>;                                    \
-    const int g = sizeof(T) == 8 ? bgemv_grid((const void*)kern, smem, batch) : batch;                      \
-    kern<<<g, 256, smem, st>>>(M, K, batch, A, sA, x, sx, elemcon, ndf, ncu, alpha, beta, y0, y, sy);      \
+    if constexpr (sizeof(T) == 8) {                                                                         \
+      auto kern = bgemv_pers_kernel<T, R, V, (R > 12) ? 2 : 4>;                                               \
+      const int g = bgemv_grid((const void*)kern, smem, batch);                                             \
+      kern<<<g, 256, smem, st>>>(M, K, batch, A, sA, x, sx, elemcon, ndf, ncu, alpha, beta, y0, y, sy);    \
+    } else {                                                                                                \
+      bgemv_kernel<T, R, V, 4><<<batch, 256, smem1, st>>>(M, K, A, sA, x, sx, elemcon, ndf, ncu, alpha, beta, \
+                                                          y0, y, sy);                                         \
+    }                                                                                                       \
   } while (0)
   // rows covered per warp with single rows (RI from 1-6, 8, 10, 12, 16) and with pairs (RI from
   // 1-6, 8): pairs only where they pad no more rows (m = 150: 160 single against 192 paired)
