@@ -604,6 +604,8 @@ __global__ void __launch_bounds__(32 * NW, sizeof(T) == 4 ? 2 : 1)
   __shared__ T sd[2];
   __shared__ int perm[32 * RL];
   __shared__ int pos[32 * RL];
+  __shared__ __align__(16) T rowb[NW][CW];  // each warp's part of the pivot row
+  static_assert((CW * sizeof(T)) % 16 == 0, "pivot-row copies in 16-byte vectors");
   T* G = Aall + (long long)blockIdx.x * stride;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   T a[RL][CW];
@@ -675,15 +677,36 @@ __global__ void __launch_bounds__(32 * NW, sizeof(T) == 4 ? 2 : 1)
       T f[RL];
 #pragma unroll
       for (int i = 0; i < RL; ++i) f[i] = (lane + 32 * i == p) ? T(0) : colb[buf][lane + 32 * i];
-      // this warp's part of the pivot row, scaled: r_j = a_pj d
+      // this warp's part of the pivot row, scaled: r_j = a_pj d.  The lane that holds row p
+      // stores it (one branch of RL, taken by one lane), the warp reads it back as broadcasts
+      if (lane == pl) {
+#pragma unroll
+        for (int i = 0; i < RL; ++i)
+          if (i == pi) {
+#pragma unroll
+            for (int j = 0; j < CW; j += 16 / (int)sizeof(T)) {
+              if constexpr (sizeof(T) == 4)
+                *reinterpret_cast<float4*>(&rowb[warp][j]) = make_float4(a[i][j], a[i][j + 1], a[i][j + 2], a[i][j + 3]);
+              else
+                *reinterpret_cast<double2*>(&rowb[warp][j]) = make_double2(a[i][j], a[i][j + 1]);
+            }
+          }
+      }
+      __syncwarp();
       T r[CW];
 #pragma unroll
-      for (int j = 0; j < CW; ++j) {
-        T own = a[0][j];
-#pragma unroll
-        for (int i = 1; i < RL; ++i)
-          if (i == pi) own = a[i][j];
-        r[j] = __shfl_sync(0xffffffffu, own, pl) * d;
+      for (int j = 0; j < CW; j += 16 / (int)sizeof(T)) {
+        if constexpr (sizeof(T) == 4) {
+          const float4 v = *reinterpret_cast<const float4*>(&rowb[warp][j]);
+          r[j] = v.x * d;
+          r[j + 1] = v.y * d;
+          r[j + 2] = v.z * d;
+          r[j + 3] = v.w * d;
+        } else {
+          const double2 v = *reinterpret_cast<const double2*>(&rowb[warp][j]);
+          r[j] = v.x * d;
+          r[j + 1] = v.y * d;
+        }
       }
       // rows other than p (f_p = 0 leaves row p as it is), then row p and column k
 #pragma unroll
