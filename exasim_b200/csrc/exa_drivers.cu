@@ -178,7 +178,7 @@ int exa_drv_precond(ExaCtx& c, const double* v, double* w) {
 int exa_drv_getq(ExaCtx& c) {
   if (c.P.ncq == 0) return EXA_OK;
   ExaProfScope ps(c, EXA_PH_GETQ);
-  if (c.Minv && exa_getq_mf_smem(c.P) <= 227 * 1024) {
+  if (c.Minv && exa_getq_mf_smem(c.P, c.wq_w != nullptr) <= 227 * 1024) {
     if (c.wq_w) EXA_TRY(exa_k_getq_gemm(c.P, c.shapegt, c.shapegw, c.elemg, c.udg, c.wq_ug, c.wq_v, c.wq_w, c.st));
     return exa_k_getq_mf(c.P, c.shapegt, c.shapegw, c.shapfgt, c.shapfgw, c.perm, c.elemcon, c.elemg, c.faceg, c.Minv,
                          c.uh, c.udg, c.st, c.wq_w);

@@ -742,6 +742,16 @@ __global__ void getq_kernel(ExaDims P, const int* elemcon, const double* MC, con
 //
 // With wpre set, C_d u comes from there (w of element e at wpre + e npe ncu nd, computed for all
 // elements by two GEMMs, exa_k_getq_gemm) and the block does the face terms and Minv only.
+//
+// The face terms of all faces are formed at once; each element node then subtracts the terms
+// of the faces it lies on in increasing face order, the order of a face-by-face update.
+__host__ __device__ inline size_t getq_mf_doubles(const ExaDims& P, bool wpre) {
+  const size_t own = (size_t)P.ndf * P.ncu + (size_t)P.npe * P.ncu * P.nd + (size_t)P.ngf * P.nd * P.ncu * P.nfe +
+                     (size_t)P.ndf * P.ncu * P.nd;
+  return own + (wpre ? 0 : (size_t)P.npe * P.ncu + (size_t)P.nge * P.nd * P.nd * P.ncu);
+}
+__host__ __device__ inline size_t getq_mf_ints(const ExaDims& P) { return (size_t)P.ndf + (size_t)P.npe * (P.nfe + 1); }
+
 __global__ void getq_mf_kernel(ExaDims P, const double* shapegt, const double* shapegw, const double* shapfgt,
                                const double* shapfgw, const int* perm, const int* elemcon, const double* elemg,
                                const double* faceg, const double* Minv, const double* uh, double* udg,
@@ -749,25 +759,36 @@ __global__ void getq_mf_kernel(ExaDims P, const double* shapegt, const double* s
   extern __shared__ double sm[];
   const int e = blockIdx.x, npe = P.npe, ncu = P.ncu, ndf = P.ndf, nd = P.nd, nc = P.nc;
   const int nge = P.nge, npf = P.npf, ngf = P.ngf, nfe = P.nfe;
-  double* u = sm;                  // [npe, ncu]
-  double* uhe = u + npe * ncu;     // [ndf, ncu]
-  double* vg = uhe + ndf * ncu;    // [nge, nd (ref r), nd (phys d), ncu]: Xx[g, d, r] u(g)
-  double* w = vg + nge * nd * nd * ncu;  // [npe, ncu, nd]
-  double* hg = w + npe * ncu * nd;       // [ngf, nd, ncu]: n_d fj uhat(g) on one face
+  double* uhe = sm;                      // [ndf, ncu]
+  double* w = uhe + ndf * ncu;           // [npe, ncu, nd]
+  double* hg = w + npe * ncu * nd;       // [ngf, nd, ncu, nfe]: n_d fj uhat(g) on every face
+  double* hs = hg + ngf * nd * ncu * nfe;  // [ndf, ncu, nd]: E_d uhat of each face node
+  double* u = hs + ndf * ncu * nd;       // [npe, ncu]                      (without wpre)
+  double* vg = u + npe * ncu;            // [nge, nd (ref r), nd (phys d), ncu]: Xx[g, d, r] u(g)
+  int* sperm = reinterpret_cast<int*>(sm + getq_mf_doubles(P, wpre != nullptr));  // [ndf]
+  int* ntab = sperm + ndf;               // [npe, 1 + nfe]: count, then face-node slots a + npf l
   double* U = udg + (long long)e * npe * nc;
   const double* eg = elemg + (long long)e * P.elemg_stride();
   const double* Xx = eg + nge * P.ncx;
-  for (int t = threadIdx.x; t < npe * ncu; t += blockDim.x) u[t] = U[t];
   for (int t = threadIdx.x; t < ndf * ncu; t += blockDim.x) {
     const int jf = t % ndf, k = t / ndf;
     uhe[t] = uh[k + ncu * (long long)elemcon[jf + ndf * e]];
   }
-  __syncthreads();
+  for (int t = threadIdx.x; t < ndf; t += blockDim.x) sperm[t] = perm[t];
   if (wpre) {
     const double* we = wpre + (long long)e * npe * ncu * nd;
     for (int t = threadIdx.x; t < npe * ncu * nd; t += blockDim.x) w[t] = we[t];
-    __syncthreads();
   } else {
+    for (int t = threadIdx.x; t < npe * ncu; t += blockDim.x) u[t] = U[t];
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < npe; i += blockDim.x) {
+    int n = 0;
+    for (int t = 0; t < ndf; ++t)
+      if (sperm[t] == i && n < nfe) ntab[i * (1 + nfe) + 1 + n++] = t;
+    ntab[i * (1 + nfe)] = n;
+  }
+  if (!wpre) {
     for (int t = threadIdx.x; t < nge * ncu; t += blockDim.x) {
       const int g = t % nge, k = t / nge;
       double s = 0.0;
@@ -795,47 +816,63 @@ __global__ void getq_mf_kernel(ExaDims P, const double* shapegt, const double* s
       for (int d = 0; d < 3; ++d)
         if (d < nd) w[a + npe * (k + ncu * d)] = s[d];
     }
-    __syncthreads();
   }
-  // minus E_d uhat, face by face (faces share corner and edge nodes)
-  for (int l = 0; l < nfe; ++l) {
+  // E_d uhat: uhat at the Gauss points of every face, then its weighted sums at the face nodes
+  for (int t = threadIdx.x; t < ngf * ncu * nfe; t += blockDim.x) {
+    const int g = t % ngf, k = (t / ngf) % ncu, l = t / (ngf * ncu);
     const double* fg = faceg + ((long long)e * nfe + l) * P.faceg_stride();
     const double* nl = fg + ngf * P.ncx;
     const double* fj = nl + ngf * nd;
-    for (int t = threadIdx.x; t < ngf * ncu; t += blockDim.x) {
-      const int g = t % ngf, k = t / ngf;
-      double s = 0.0;
-      for (int b = 0; b < npf; ++b) s = fma(shapfgt[g + ngf * b], uhe[b + npf * l + ndf * k], s);
-      for (int d = 0; d < nd; ++d) hg[g + ngf * (d + nd * k)] = nl[g + ngf * d] * fj[g] * s;
-    }
-    __syncthreads();
-    for (int t = threadIdx.x; t < npf * ncu * nd; t += blockDim.x) {
-      const int a = t % npf, k = (t / npf) % ncu, d = t / (npf * ncu);
-      double s = 0.0;
-      for (int g = 0; g < ngf; ++g) s = fma(shapfgw[a + npf * g], hg[g + ngf * (d + nd * k)], s);
-      w[perm[a + npf * l] + npe * (k + ncu * d)] -= s;
-    }
-    __syncthreads();
+    double s = 0.0;
+    for (int b = 0; b < npf; ++b) s = fma(shapfgt[g + ngf * b], uhe[b + npf * l + ndf * k], s);
+    for (int d = 0; d < nd; ++d) hg[g + ngf * (d + nd * (k + ncu * l))] = nl[g + ngf * d] * fj[g] * s;
   }
-  // q = Minv w: one thread per row i takes up to 8 of the ncu nd right-hand sides at once,
-  // so each Minv entry is read once per 8 products
+  __syncthreads();
+  for (int t = threadIdx.x; t < npf * ncu * nd * nfe; t += blockDim.x) {
+    const int a = t % npf, k = (t / npf) % ncu, d = (t / (npf * ncu)) % nd, l = t / (npf * ncu * nd);
+    double s = 0.0;
+    for (int g = 0; g < ngf; ++g) s = fma(shapfgw[a + npf * g], hg[g + ngf * (d + nd * (k + ncu * l))], s);
+    hs[a + npf * l + ndf * (k + ncu * d)] = s;
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < npe * ncu * nd; t += blockDim.x) {
+    const int i = t % npe, kd = t / npe;
+    const int* nt = ntab + i * (1 + nfe);
+    double v = w[t];
+    for (int c = 1; c <= nt[0]; ++c) v -= hs[nt[c] + ndf * kd];
+    w[t] = v;
+  }
+  __syncthreads();
+  // q = Minv w: one thread per (row i, group of up to 8 of the ncu nd right-hand sides), so
+  // each Minv entry is read once per 8 products; eight columns of Minv are loaded at a time
   const double* Mi = Minv + (long long)e * npe * npe;
-  const int nq = ncu * nd;
-  for (int q0 = 0; q0 < nq; q0 += 8) {
-    for (int i = threadIdx.x; i < npe; i += blockDim.x) {
-      double s[8];
+  const int nq = ncu * nd, ngrp = (nq + 7) / 8;
+  for (int t = threadIdx.x; t < npe * ngrp; t += blockDim.x) {
+    const int i = t % npe, q0 = 8 * (t / npe);
+    double s[8];
 #pragma unroll
-      for (int q = 0; q < 8; ++q) s[q] = 0.0;
-      for (int j = 0; j < npe; ++j) {
-        const double m = Mi[i + (long long)npe * j];
+    for (int q = 0; q < 8; ++q) s[q] = 0.0;
+    const double* Mr = Mi + i;
+    int j = 0;
+    for (; j + 8 <= npe; j += 8) {
+      double m[8];
+#pragma unroll
+      for (int x = 0; x < 8; ++x) m[x] = __ldcs(Mr + (long long)npe * (j + x));
+#pragma unroll
+      for (int x = 0; x < 8; ++x)
 #pragma unroll
         for (int q = 0; q < 8; ++q)
-          if (q0 + q < nq) s[q] = fma(m, w[j + npe * (q0 + q)], s[q]);
-      }
+          if (q0 + q < nq) s[q] = fma(m[x], w[j + x + npe * (q0 + q)], s[q]);
+    }
+    for (; j < npe; ++j) {
+      const double m = __ldcs(Mr + (long long)npe * j);
 #pragma unroll
       for (int q = 0; q < 8; ++q)
-        if (q0 + q < nq) U[i + npe * (ncu + q0 + q)] = s[q];
+        if (q0 + q < nq) s[q] = fma(m, w[j + npe * (q0 + q)], s[q]);
     }
+#pragma unroll
+    for (int q = 0; q < 8; ++q)
+      if (q0 + q < nq) U[i + npe * (ncu + q0 + q)] = s[q];
   }
 }
 
@@ -956,16 +993,15 @@ int exa_k_getq(const ExaDims& P, const int* elemcon, const double* MC, const dou
   return EXA_OK;
 }
 
-size_t exa_getq_mf_smem(const ExaDims& P) {
-  return sizeof(double) * ((size_t)P.npe * P.ncu + (size_t)P.ndf * P.ncu + (size_t)P.nge * P.nd * P.nd * P.ncu +
-                           (size_t)P.npe * P.ncu * P.nd + (size_t)P.ngf * P.nd * P.ncu);
+size_t exa_getq_mf_smem(const ExaDims& P, bool wpre) {
+  return sizeof(double) * getq_mf_doubles(P, wpre) + sizeof(int) * getq_mf_ints(P);
 }
 
 int exa_k_getq_mf(const ExaDims& P, const double* shapegt, const double* shapegw, const double* shapfgt,
                   const double* shapfgw, const int* perm, const int* elemcon, const double* elemg,
                   const double* faceg, const double* Minv, const double* uh, double* udg, cudaStream_t st,
                   const double* wpre) {
-  const size_t smem = exa_getq_mf_smem(P);
+  const size_t smem = exa_getq_mf_smem(P, wpre != nullptr);
   EXA_TRY(exa_allow_smem((const void*)getq_mf_kernel, smem));
   getq_mf_kernel<<<P.ne, 128, smem, st>>>(P, shapegt, shapegw, shapfgt, shapfgw, perm, elemcon, elemg, faceg, Minv,
                                           uh, udg, wpre);

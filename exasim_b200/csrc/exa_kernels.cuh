@@ -68,7 +68,7 @@ int exa_k_to_f32(const double* x, float* y, long long n, cudaStream_t st);
 int exa_k_udg_update(const ExaDims& P, double* udg, const double* du, double alpha, cudaStream_t st);
 // q = Minv (C u - E uhat) by quadrature (no MinvC / MinvE reads).  With wpre, C u is taken
 // from there (exa_k_getq_gemm) instead of computed per element.
-size_t exa_getq_mf_smem(const ExaDims& P);
+size_t exa_getq_mf_smem(const ExaDims& P, bool wpre);  // shared memory of exa_k_getq_mf (wpre given or not)
 int exa_k_getq_mf(const ExaDims& P, const double* shapegt, const double* shapegw, const double* shapfgt,
                   const double* shapfgw, const int* perm, const int* elemcon, const double* elemg,
                   const double* faceg, const double* Minv, const double* uh, double* udg, cudaStream_t st,
