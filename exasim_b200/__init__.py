@@ -202,6 +202,16 @@ class HDGSolver:
     def hdgGetQ(self):
         self._check(self.lib.exa_getq(self.h))
 
+    def evalResidual(self) -> float:
+        """LDG contexts (problem[0] = 0): R(u) of the current element states into the field
+        "Ru", returning |R| (CDiscretization::evalResidual, discretization.cpp:604-612)."""
+        return self.hdgAssembleResidual()
+
+    def PTCsolver(self):
+        """LDG contexts: the pseudo-transient solve of R(u) = 0 (ptcsolver.cpp:255-330);
+        returns (PTC steps, |R|).  An HDG context runs its Newton solve."""
+        return self.NewtonSolver()
+
     def NewtonSolver(self):
         it, nrm = ctypes.c_int(), ctypes.c_double()
         self._check(self.lib.exa_newton(self.h, ctypes.byref(it), ctypes.byref(nrm)))

@@ -25,7 +25,7 @@ MODELS = os.path.join(PKG, "models")
 NVCC = os.environ.get("NVCC", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"]
-COMMON = ["exa_linalg.cu", "exa_umma.cu", "exa_volmat_tc.cu", "exa_kernels.cu", "exa_drivers.cu", "exa_api.cu", "exa_conn.cpp", "exa_bilu0.cpp", "exa_bilu0_dev.cu", "exa_server.cpp", "exa_batch.cu", "exa_poly.cpp"]
+COMMON = ["exa_linalg.cu", "exa_umma.cu", "exa_volmat_tc.cu", "exa_kernels.cu", "exa_drivers.cu", "exa_api.cu", "exa_conn.cpp", "exa_bilu0.cpp", "exa_bilu0_dev.cu", "exa_server.cpp", "exa_batch.cu", "exa_poly.cpp", "exa_ldg.cu"]
 
 
 def available_models() -> List[str]:

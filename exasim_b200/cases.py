@@ -95,13 +95,21 @@ def ns2d_tgv_quad(datain: str, n: int = 64, porder: int = 3, nsteps: int = 10, d
 
 def euler3d_vortex_hex(datain: str, n: int = 32, porder: int = 3, nsteps: int = 5, dt: float = 0.05,
                        preconditioner: int = 0, restart: int = 50, gmres_tol: float = 1e-8,
-                       newton_tol: float = 1e-8, mach: float = 0.5):
-    grid = I.periodic_cube_hex_grid(n, -5.0, 10.0)
+                       newton_tol: float = 1e-8, mach: float = 0.5, periodic: bool = True, hybrid: int = 1,
+                       precMatrixType: int = 0):
+    """hybrid = 0 selects the LDG discretisation with its pseudo-transient solver; periodic =
+    False closes the cube with boundary code 1 on every side (the model's Ubou / Fbou)."""
+    if periodic:
+        grid = I.periodic_cube_hex_grid(n, -5.0, 10.0)
+    else:
+        grid = I.cube_hex_grid(n, 10.0)
+        grid.p = grid.p - 5.0
     master = I.make_master(3, 1, porder, 2 * porder)
     app = I.PDEApp(nd=3, ncu=5, model="ModelC", preconditioner=preconditioner, NewtonIter=20,
                    NewtonTol=newton_tol, GMRESiter=1000, GMRESrestart=restart, GMREStol=gmres_tol,
                    RBdim=0, ppdegree=1, tau=[1.0 + 1.0 / mach], torder=2, nstage=2, dt=[dt] * nsteps,
-                   physicsparam=[1.4, mach], externalparam=[0.0, 0.0])
+                   physicsparam=[1.4, mach], externalparam=[0.0, 0.0], hybrid=hybrid,
+                   precMatrixType=precMatrixType)
     return write_case(datain, grid, master, app, [lambda x: True], [1])
 
 

@@ -162,7 +162,32 @@ int exa_ctx_init(ExaCtx& c, const double* app, long long napp, const double* mas
   c.gmres_tol = solvers[1];
   c.time0 = (c.tdep == 1 && A.nsize[5] > 0) ? factor[0] : 0.0;
   c.time = c.time0;
-  if (spatial != 1) { exa_set_error("only the HDG discretization (problem[0]=1) is on this path"); return EXA_ERR_UNSUPPORTED; }
+  if (spatial != 0 && spatial != 1) {
+    exa_set_error("discretization problem[0]=%d: LDG (0) or HDG (1)", spatial);
+    return EXA_ERR_UNSUPPORTED;
+  }
+  c.scheme = spatial;
+  c.ntau = (int)A.nsize[8];
+  if (c.scheme == 0) {
+    // LDG with the pseudo-transient solver: models without q, the finite-difference Jacobian
+    // (flag[4], solversparam[2]) and the identity preconditioner (flag[7] = 0)
+    c.matvec_order = (int)flag[4];
+    c.matvec_eps = A.nsize[7] > 2 ? solvers[2] : 1e-3;
+    const int prec_matrix = (int)flag[7];
+    if (P.ncq != 0) {
+      exa_set_error("LDG with q (ncq=%d) is not supported: the reference's GetQ calls RuFace for the q face term",
+                    P.ncq);
+      return EXA_ERR_UNSUPPORTED;
+    }
+    if (c.matvec_order != 1 && c.matvec_order != 2) {
+      exa_set_error("LDG matrix-vector product of order %d: 1 or 2", c.matvec_order);
+      return EXA_ERR_UNSUPPORTED;
+    }
+    if (!(c.matvec_eps > 0.0)) { exa_set_error("LDG finite-difference step %g is not positive", c.matvec_eps); return EXA_ERR_ARG; }
+    if (prec_matrix != 0) { exa_set_error("LDG preconditioner matrix type %d: only the identity (0)", prec_matrix); return EXA_ERR_UNSUPPORTED; }
+    if (c.RBdim > 0) { exa_set_error("LDG with a reduced-basis initial guess (RBdim=%d) is not supported", c.RBdim); return EXA_ERR_UNSUPPORTED; }
+    if (c.ppdegree > 1) { exa_set_error("LDG with a polynomial preconditioner is not supported"); return EXA_ERR_UNSUPPORTED; }
+  }
   if (mpiprocs > 1) { exa_set_error("multi-rank inputs: this solver runs one GPU per mesh"); return EXA_ERR_UNSUPPORTED; }
   if (P.nco > 0 || P.ncw > 0) { exa_set_error("odg/wdg fields (nco=%d, ncw=%d) are outside the HDG hot path", P.nco, P.ncw); return EXA_ERR_UNSUPPORTED; }
   if (c.wave) { exa_set_error("wave (ModelW) problems are not supported"); return EXA_ERR_UNSUPPORTED; }
@@ -303,6 +328,29 @@ int exa_ctx_init(ExaCtx& c, const double* app, long long napp, const double* mas
   EXA_TRY(dev_alloc(c, &c.elemg, ne * P.elemg_stride()));
   EXA_TRY(dev_alloc(c, &c.faceg, ne * P.nfe * P.faceg_stride()));
   EXA_TRY(exa_k_geometry(P, c.shapegt, c.shapfgt, c.perm, c.xdg, c.elemg, c.faceg, c.st));
+  if (c.scheme == 0) {
+    // LDG: both sides' face-node table, the face nodal basis for the boundary's Ubou, and
+    // the residual buffers of the finite-difference Jacobian
+    const bool boundary = conn.nf0 < conn.nf;
+    c.ldg_has_boundary = boundary ? 1 : 0;
+    if (boundary && !exa_model_has_ldg_boundary()) {
+      exa_set_error("LDG on a mesh with boundary faces needs the model's Ubou and Fbou (KokkosUbou, KokkosFbou)");
+      return EXA_ERR_UNSUPPORTED;
+    }
+    if (M.nsize.size() < 8 || M.nsize[7] != (long long)P.npf * P.npf * P.nd) {
+      exa_set_error("master.bin lacks the face nodal basis shapfnt");
+      return EXA_ERR_ARG;
+    }
+    EXA_TRY(dev_upload(c, &c.shapfnt, M.part[7], (size_t)M.nsize[7]));
+    EXA_TRY(dev_alloc(c, &c.ldg_fcon, 2 * (size_t)P.npf * P.nf));
+    EXA_TRY(exa_k_ldg_fcon(P, c.f2e, c.perm, c.elemcon, c.ldg_fcon, c.st));
+    const size_t nl = (size_t)P.npe * P.ncu * ne;
+    EXA_TRY(dev_alloc(c, &c.ldg_R, nl));
+    EXA_TRY(dev_alloc(c, &c.ldg_w, nl));
+    EXA_TRY(dev_alloc(c, &c.ldg_Rw, nl));
+    EXA_TRY(dev_alloc(c, &c.ldg_Rm, nl));
+    EXA_TRY(dev_alloc(c, &c.ldg_Rh, (size_t)P.npf * P.ncu * std::max(1, P.nf)));
+  }
 
   // solution: udg from sol.bin (full or u only) or the model's initial condition; uhat from sol.bin or u
   EXA_TRY(dev_alloc(c, &c.udg, ne * P.npe * P.nc));
@@ -354,7 +402,7 @@ int exa_ctx_init(ExaCtx& c, const double* app, long long napp, const double* mas
   EXA_TRY(dev_alloc(c, &c.F, ne * n * m));
   EXA_TRY(dev_alloc(c, &c.Ru, ne * n));
   EXA_TRY(dev_alloc(c, &c.Rh, ne * m));
-  const size_t N = (size_t)c.ndofuhat();
+  const size_t N = (size_t)std::max(c.ndofuhat(), c.sysN());
   EXA_TRY(dev_alloc(c, &c.b, N));
   if (c.preconditioner == 0)
     EXA_TRY(dev_alloc(c, &c.Pc, (size_t)P.ncu * P.npf * P.ncu * P.npf * P.nf));
@@ -530,6 +578,10 @@ int exa_ctx_set_precision(ExaCtx& c, int mode) {
   if (mode != 0 && mode != 1) {
     exa_set_error("precision mode %d: 0 (FP64) or 1 (FP32/TF32 elimination with FP64 refinement)", mode);
     return EXA_ERR_ARG;
+  }
+  if (mode == 1 && c.scheme == 0) {
+    exa_set_error("the mixed-precision form condenses the HDG system; the LDG path runs in FP64");
+    return EXA_ERR_UNSUPPORTED;
   }
   if (mode == 1) {
     EXA_TRY(fp64_blocks(c, false));
@@ -742,10 +794,11 @@ struct FieldRef {
 
 bool field(ExaCtx& c, const char* name, FieldRef& f) {
   const ExaDims& P = c.P;
-  const long long ne = P.ne, n = P.n, m = P.m, N = c.ndofuhat();
+  const long long ne = P.ne, n = P.n, m = P.m, N = c.sysN();
   const std::string s(name ? name : "");
   if (s == "udg") f = {c.udg, (long long)P.npe * P.nc * ne};
-  else if (s == "uh") f = {c.uh, N};
+  else if (s == "uh") f = {c.uh, c.ndofuhat()};
+  else if (s == "Ru" && c.scheme == 0) f = {c.ldg_R, N};  // the LDG residual of the last exa_residual
   else if (s == "H" && c.fp64_full) f = {c.H, m * m * ne};
   else if (s == "F" && c.fp64_full) f = {c.F, n * m * ne};
   else if (s == "Ru") f = {c.Ru, n * ne};

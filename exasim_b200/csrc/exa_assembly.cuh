@@ -631,4 +631,17 @@ inline size_t face_smem(const ExaDims& P, bool jac) {
                                      int a, int b, int c, int d, int e, int h) {                                \
       NS::HdgFbouonly_pt(i, f, x, uq, v, w, uh, nl, tau, eta, mu, t, mn, ib, N, a, b, c, d, e, h);               \
     }                                                                                                           \
+    /* the LDG boundary functions (KokkosUbou, KokkosFbou); empty when the model has none */                    \
+    static constexpr bool has_ldg_boundary = NS::has_KokkosUbou && NS::has_KokkosFbou;                          \
+    __device__ static void ubou(size_t i, double* f, const double* x, const double* uq, const double* uh,        \
+                                const double* nl, const double* tau, const double* eta, const double* mu,       \
+                                double t, int mn, int ib, int N, int a, int b, int c, int d, int e, int h) {   \
+      NS::KokkosUbou_pt(i, f, x, uq, nullptr, nullptr, uh, nl, tau, eta, mu, t, mn, ib, N, a, b, c, d, e, h);    \
+    }                                                                                                           \
+    __device__ static void fbou_ldg(size_t i, double* f, const double* x, const double* uq, const double* uh,    \
+                                    const double* nl, const double* tau, const double* eta, const double* mu,   \
+                                    double t, int mn, int ib, int N, int a, int b, int c, int d, int e,        \
+                                    int h) {                                                                    \
+      NS::KokkosFbou_pt(i, f, x, uq, nullptr, nullptr, uh, nl, tau, eta, mu, t, mn, ib, N, a, b, c, d, e, h);    \
+    }                                                                                                           \
   };

@@ -136,6 +136,12 @@ int exa_drv_assemble(ExaCtx& c) {
 
 // hdgAssembleResidual: Ru, Rh, b; norm = |b| + |Ru| (solution.cpp:148-157)
 int exa_drv_residual(ExaCtx& c, double* norm) {
+  if (c.scheme == 0) {
+    // LDG: R(u) of the element states (residual.cpp:589-617); norm = |R|
+    EXA_TRY(exa_model_ldg_residual(c, c.udg, c.ldg_R));
+    if (norm) EXA_TRY(exa_drv_norm(c, c.ldg_R, c.sysN(), norm));
+    return EXA_OK;
+  }
   EXA_TRY(exa_model_assemble(c, false));
   EXA_TRY(exa_k_scatter(c.P, c.f2e, c.elemcon, c.Rh, c.b, c.st));
   if (norm) {
@@ -147,9 +153,27 @@ int exa_drv_residual(ExaCtx& c, double* norm) {
   return EXA_OK;
 }
 
+// LDG: w = J(u) v by differences of residuals around the current state u = udg with R(u) in
+// ldg_R (MatVec, matvec.cpp:41-100): (R(u + eps v) - R(u)) / eps, or the central difference
+int ldg_matvec(ExaCtx& c, const double* v, double* w) {
+  const long long N = c.sysN();
+  const double eps = c.matvec_eps;
+  if (c.matvec_order == 1) {
+    EXA_TRY(exa_lincomb(c.ldg_w, 1.0, c.udg, eps, v, N, c.st));
+    EXA_TRY(exa_model_ldg_residual(c, c.ldg_w, c.ldg_Rw));
+    return exa_lincomb(w, 1.0 / eps, c.ldg_Rw, -1.0 / eps, c.ldg_R, N, c.st);
+  }
+  EXA_TRY(exa_lincomb(c.ldg_w, 1.0, c.udg, -eps, v, N, c.st));
+  EXA_TRY(exa_model_ldg_residual(c, c.ldg_w, c.ldg_Rm));
+  EXA_TRY(exa_lincomb(c.ldg_w, 1.0, c.udg, eps, v, N, c.st));
+  EXA_TRY(exa_model_ldg_residual(c, c.ldg_w, c.ldg_Rw));
+  return exa_lincomb(w, 0.5 / eps, c.ldg_Rw, -0.5 / eps, c.ldg_Rm, N, c.st);
+}
+
 // w = A v (hdgMatVec, matvec.cpp:240-389)
 int exa_drv_matvec(ExaCtx& c, const double* v, double* w) {
   ExaProfScope ps(c, EXA_PH_MATVEC);
+  if (c.scheme == 0) return ldg_matvec(c, v, w);
   if (c.precision == 1)
     EXA_TRY(exa_k_elem_matvec(c.P, c.elemcon, c.H32, v, c.we, c.st, c.d_uflag));
   else
@@ -161,6 +185,11 @@ int exa_drv_matvec(ExaCtx& c, const double* v, double* w) {
 // w = P v (ApplyPreconditioner, preconditioner.cpp:273-295); v and w may not alias
 int exa_drv_precond(ExaCtx& c, const double* v, double* w) {
   ExaProfScope ps(c, EXA_PH_PRECOND_APPLY);
+  if (c.scheme == 0) {
+    // LDG with precMatrixType 0: the identity (ApplyMatrix, applymatrix.cpp:87-98)
+    EXA_CUDA(cudaMemcpyAsync(w, v, sizeof(double) * c.sysN(), cudaMemcpyDeviceToDevice, c.st));
+    return EXA_OK;
+  }
   if (c.preconditioner == 2) {
     if (c.precision == 1) return exa_k_bilu_apply(c.P, c.bilu, c.Pc32, v, w, c.st);
     return exa_k_bilu_apply(c.P, c.bilu, c.Pc, v, w, c.st);
@@ -202,7 +231,7 @@ int pa(ExaCtx& c, const double* x, double* out) {
 int apply_poly(ExaCtx& c, double* wv) {
   if (c.ppdegree <= 1) return EXA_OK;
   const int m = c.ppdegree;
-  const long long N = c.ndofuhat();
+  const long long N = c.sysN();
   double *q = c.poly_q, *p = c.poly_p;
   const std::vector<double>&sr = c.poly_sr, &si = c.poly_si;
   EXA_CUDA(cudaMemcpyAsync(q, wv, sizeof(double) * N, cudaMemcpyDeviceToDevice, c.st));
@@ -234,7 +263,7 @@ int apply_poly(ExaCtx& c, double* wv) {
 // the coefficients into hcol[0 .. j] (MGS, getpoly.cpp:36-45; the pipelined launches of
 // arnoldi_ops)
 int mgs_column(ExaCtx& c, int j, double* hcol) {
-  const long long N = c.ndofuhat();
+  const long long N = c.sysN();
   double* vn = c.V + (long long)j * N;
   EXA_TRY(exa_dot_partials(vn, c.V, N, c.part_a, c.st));
   double* pin = c.part_a;
@@ -252,7 +281,7 @@ int mgs_column(ExaCtx& c, int j, double* hcol) {
 // host the harmonic Ritz values in Leja order (exa_poly_ritz)
 int poly_setup(ExaCtx& c) {
   const int m = c.ppdegree, m1 = m + 1, n1 = c.restart + 1;
-  const long long N = c.ndofuhat();
+  const long long N = c.sysN();
   double nr = 0.0;
   EXA_TRY(exa_drv_norm(c, c.randvect, N, &nr));
   EXA_TRY(exa_scale(c.V, c.randvect, 1.0 / nr, N, c.st));
@@ -288,7 +317,7 @@ namespace {
 // the Hessenberg column i, the Givens update and the residual estimate |s_{i+1}| / |b|,
 // copied to the pinned slot `rel_pin`.
 int arnoldi_ops(ExaCtx& c, int i, const double* d_nrmb, double* d_relerr, double* rel_pin) {
-  const long long N = c.ndofuhat();
+  const long long N = c.sysN();
   const int n1 = c.restart + 1;
   double* vi = c.V + (long long)i * N;
   double* vn = c.V + (long long)(i + 1) * N;
@@ -368,7 +397,7 @@ int arnoldi_step(ExaCtx& c, int i, const double* d_nrmb, double* d_relerr, doubl
 // (the small matrix inverted on the host by Gauss-Jordan with partial pivoting, as the
 // reference inverts it with getrf/getri) and x = W c.  A singular U^T U leaves x = 0.
 int rb_initial_guess(ExaCtx& c) {
-  const long long N = c.ndofuhat();
+  const long long N = c.sysN();
   const int cur = c.rb_cur;
   const int i = c.rb_removed > 0 ? c.rb_removed - 1 : cur - 1;
   EXA_TRY(exa_drv_matvec(c, c.rbW + (long long)i * N, c.rbU + (long long)i * N));
@@ -424,7 +453,7 @@ int rb_initial_guess(ExaCtx& c) {
 // UpdateRB (ptcsolver.cpp:484-500): the Newton update, scaled by its step length, replaces
 // the oldest basis vector
 int rb_update(ExaCtx& c, double alpha) {
-  const long long N = c.ndofuhat();
+  const long long N = c.sysN();
   EXA_TRY(exa_scale(c.x, c.x, alpha, N, c.st));
   double nrm = 0.0;
   EXA_TRY(exa_drv_norm(c, c.x, N, &nrm));
@@ -440,7 +469,7 @@ int rb_update(ExaCtx& c, double alpha) {
 // UpdateSolution (gmres.cpp:132-137) with the first i + 1 basis vectors: y from the
 // Hessenberg back-solve on the host, x += V y on the device.
 int update_solution(ExaCtx& c, int i, std::vector<double>& ybuf) {
-  const long long N = c.ndofuhat();
+  const long long N = c.sysN();
   const int n1 = c.restart + 1, nrest = c.restart;
   double* hh = c.pinned;
   double* ss = hh + (size_t)n1 * nrest;
@@ -465,7 +494,7 @@ int update_solution(ExaCtx& c, int i, std::vector<double>& ybuf) {
 // update of step i reads, so the result is that of stopping at step i.
 namespace {
 int gmres_body(ExaCtx& c, int* iters_out, double* relerr_out) {
-  const long long N = c.ndofuhat();
+  const long long N = c.sysN();
   const int nrest = c.restart, maxit = c.gmres_maxit, n1 = nrest + 1;
   double nrmb = 0.0, nrmr = 0.0;
   // the polynomial's Ritz values, from the current operator (gmres.cpp:385-398)
@@ -473,7 +502,9 @@ int gmres_body(ExaCtx& c, int* iters_out, double* relerr_out) {
   EXA_CUDA(cudaMemsetAsync(c.x, 0, sizeof(double) * N, c.st));
   EXA_TRY(exa_drv_norm(c, c.b, N, &nrmb));
   c.last_gmres_converged = true;
-  if (nrmb < c.newton_tol) {
+  // the HDG solve stops at a right-hand side below the Newton tolerance; the LDG GMRES
+  // (gmres.cpp:140-318) has no such test
+  if (c.scheme != 0 && nrmb < c.newton_tol) {
     *iters_out = 0;
     *relerr_out = 0.0;
     return EXA_OK;
@@ -575,7 +606,7 @@ int exa_drv_check_uflag(ExaCtx& c) {
 }
 
 int exa_drv_gmres(ExaCtx& c, int* iters_out, double* relerr_out) {
-  if (c.batcher && exa_batchable(c)) {
+  if (c.batcher && c.scheme != 0 && exa_batchable(c)) {
     EXA_TRY(exa_batcher_gmres(c.batcher, c, iters_out, relerr_out));
   } else {
     EXA_TRY(gmres_body(c, iters_out, relerr_out));
@@ -590,8 +621,55 @@ int exa_drv_gmres_update(ExaCtx& c, int i) {
   return EXA_OK;
 }
 
+// PTCsolver (ptcsolver.cpp:255-330) with LinearSolver (ptcsolver.cpp:53-120) for the LDG
+// discretisation: GMRES on J(u) x = -R(u) from x = 0, u += x, until |R(u)| < the tolerance;
+// a norm above 1e6 or NaN stops it (the reference writes the state and exits there).
+// iters_out counts the PTC steps taken.
+int exa_drv_ptc(ExaCtx& c, int* iters_out, double* norm_out) {
+  const long long N = c.sysN();
+  double nrmr = 0.0;
+  EXA_TRY(exa_model_ldg_residual(c, c.udg, c.ldg_R));
+  EXA_TRY(exa_drv_norm(c, c.ldg_R, N, &nrmr));
+  c.last_norm0 = nrmr;
+  c.total_gmres_iters = 0;
+  int it = 0;
+  for (it = 0; it < c.newton_maxit; ++it) {
+    EXA_TRY(exa_scale(c.b, c.ldg_R, -1.0, N, c.st));  // J x = -R(u)
+    int gi = 0;
+    double ge = 0.0;
+    EXA_TRY(exa_drv_gmres(c, &gi, &ge));
+    c.last_gmres_iters = gi;
+    c.last_gmres_relerr = ge;
+    c.total_gmres_iters += gi;
+    {
+      ExaProfScope ps(c, EXA_PH_UPDATE);
+      EXA_TRY(exa_axpby(c.udg, c.x, 1.0, 1.0, N, c.st));
+    }
+    EXA_TRY(exa_model_ldg_residual(c, c.udg, c.ldg_R));
+    EXA_TRY(exa_drv_norm(c, c.ldg_R, N, &nrmr));
+    c.last_newton_iters = it + 1;
+    if (!(nrmr <= 1.0e6)) {
+      exa_set_error("PTC residual norm %g is above 1e6 or NaN", nrmr);
+      *iters_out = it + 1;
+      *norm_out = nrmr;
+      return std::isnan(nrmr) ? EXA_ERR_NAN : EXA_ERR_NOTCONV;
+    }
+    if (nrmr < c.newton_tol) {
+      *iters_out = it + 1;
+      *norm_out = nrmr;
+      c.last_norm = nrmr;
+      return EXA_OK;
+    }
+  }
+  *iters_out = it;
+  *norm_out = nrmr;
+  c.last_norm = nrmr;
+  return EXA_OK;
+}
+
 // NewtonSolver (solution.cpp:125-243)
 int exa_drv_newton(ExaCtx& c, int* iters_out, double* norm_out) {
+  if (c.scheme == 0) return exa_drv_ptc(c, iters_out, norm_out);
   if (c.precision == 1) return exa_drv_newton_mixed(c, iters_out, norm_out);
   const ExaDims& P = c.P;
   const long long N = c.ndofuhat();

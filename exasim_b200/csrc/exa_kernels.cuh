@@ -82,3 +82,10 @@ int exa_k_getq_gemm(const ExaDims& P, const double* shapegt, const double* shape
 int exa_k_getq(const ExaDims& P, const int* elemcon, const double* MC, const double* ME, const double* uh,
                double* udg, cudaStream_t st);
 int exa_k_face_nodes(const ExaDims& P, const int* f2e, const int* perm, const double* udg, double* uh, cudaStream_t st);
+
+// LDG (exa_ldg.cu): the face-node table of both sides [2, npf, nf]; the element residual from
+// the volume residual Rue and the face residuals Rh [npf, ncu, nf]; out = a x + b y
+int exa_k_ldg_fcon(const ExaDims& P, const int* f2e, const int* perm, const int* elemcon, int* fcon, cudaStream_t st);
+int exa_k_ldg_gather(const ExaDims& P, const int* f2e, const int* perm, const int* elemcon, const double* Rue,
+                     const double* Rh, double* Ru, int tdep, double dtfactor, cudaStream_t st);
+int exa_lincomb(double* out, double a, const double* x, double b, const double* y, long long n, cudaStream_t st);

@@ -1,5 +1,5 @@
 // exasim_b200_<model>: the solver as an executable, in place of the reference's
-// cput2cEXASIM / gput2cEXASIM for an HDG problem (backend/Main/main.cpp, Main/exasim.hpp).
+// cput2cEXASIM / gput2cEXASIM for an HDG or LDG problem (backend/Main/main.cpp, Main/exasim.hpp).
 //
 //   exasim_b200_<model> <datain dir> <output prefix> [restart] [device] [--checkpoint] [--vtu]
 //
@@ -10,7 +10,8 @@
 // float64 words (npe, nc, ne) or (ncu, npf, nf), then one snapshot of udg (all nc fields, or
 // u alone with saveSolOpt 0) and of uhat per saved step.  Steady problems save once; time-
 // dependent ones after every saveSolFreq-th step.  With the reference's default prefix
-// "dataout/out" the files are dataout/outudg_np0.bin and dataout/outuhat_np0.bin.
+// "dataout/out" the files are dataout/outudg_np0.bin and dataout/outuhat_np0.bin.  An LDG
+// problem (problem[0] = 0: pseudo-transient solves of the element states) writes udg only.
 //
 // Restart (time-dependent problems; exasim.hpp:338-348, 387-393, 413-420): restart R > 0, from
 // the argument or app.bin's timestepOffset (problem[19]), starts the step loop at time R dt[0]
@@ -130,6 +131,9 @@ int main(int argc, char** argv) {
   const long long ncs = opt == 0 ? ncu : nc;  // fields saved per node
   const int offset = prob.size() > 19 ? (int)prob[19] : 0;
   const int restart = offset > 0 ? offset : (int)rarg;  // the reference's precedence (exasim.hpp:387-388)
+  // an LDG run (problem[0] = 0) has no trace field: it writes and reads udg only
+  // (solution.cpp:735-760, 824-850 write uhat for HDG alone)
+  const bool ldg = !prob.empty() && prob[0] == 0.0;
   std::vector<double> udg((size_t)(npe * nc * ne)), uh((size_t)nuh);
   if (restart > 0) {
     if (!tdep || dt.empty()) {
@@ -138,9 +142,9 @@ int main(int argc, char** argv) {
     }
     const std::string fu = prefix + "udg_t" + std::to_string(restart) + "_np0.bin";
     const std::string fh = prefix + "_uhat_t" + std::to_string(restart) + "_np0.bin";
-    const std::vector<double> ru = read_words(fu), rh = read_words(fh);
+    const std::vector<double> ru = read_words(fu), rh = ldg ? std::vector<double>() : read_words(fh);
     const size_t nu = (size_t)(npe * ncs * ne);
-    if (ru.size() < nu || rh.size() < (size_t)nuh) {
+    if (ru.size() < nu || (!ldg && rh.size() < (size_t)nuh)) {
       std::fprintf(stderr, "restart %d: %s holds %zu words (needs %zu), %s %zu (needs %lld)\n", restart, fu.c_str(),
                    ru.size(), nu, fh.c_str(), rh.size(), nuh);
       return 1;
@@ -154,14 +158,14 @@ int main(int argc, char** argv) {
           for (long long i = 0; i < npe; ++i) udg[i + npe * (k + nc * e)] = ru[i + npe * (k + ncu * e)];
     }
     check(exa_set_field(ctx, "udg", udg.data(), (long long)udg.size()), "exa_set_field udg");
-    check(exa_set_field(ctx, "uh", rh.data(), nuh), "exa_set_field uh");
+    if (!ldg) check(exa_set_field(ctx, "uh", rh.data(), nuh), "exa_set_field uh");
     check(exa_set_step_time(ctx, restart * dt[0]), "exa_set_step_time");
     std::printf("restart at step %d, time %g\n", restart, restart * dt[0]);
   }
 
   Output oudg, ouh;
   oudg.open(prefix + "udg_np0.bin", (double)npe, (double)ncs, (double)ne);
-  ouh.open(prefix + "uhat_np0.bin", (double)ncu, (double)npf, (double)nf);
+  if (!ldg) ouh.open(prefix + "uhat_np0.bin", (double)ncu, (double)npf, (double)nf);
   // visualization: the master element's lattice and the nodes' coordinates
   const std::vector<double> mnd = part(master, 0), xpe = part(master, 9), xdg = part(sol, 1);
   const int vnd = mnd.size() > 5 ? (int)mnd[0] : 0, vet = mnd.size() > 5 ? (int)mnd[1] : 0;
@@ -191,15 +195,17 @@ int main(int argc, char** argv) {
     }
     const std::vector<double>& us = ncs == nc ? udg : u;
     oudg.write(us);
-    ouh.write(uh);
+    if (!ldg) ouh.write(uh);
     if (vtu) visualize(step);
     if (checkpoint && step > 0) {
       // the restart files of this step, raw (solution.cpp:804-828 reads them so)
       Output cu, ch;
       cu.open_raw(prefix + "udg_t" + std::to_string(step) + "_np0.bin");
       cu.write(us);
-      ch.open_raw(prefix + "_uhat_t" + std::to_string(step) + "_np0.bin");
-      ch.write(uh);
+      if (!ldg) {
+        ch.open_raw(prefix + "_uhat_t" + std::to_string(step) + "_np0.bin");
+        ch.write(uh);
+      }
     }
   };
   if (!tdep) {

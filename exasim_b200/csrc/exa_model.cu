@@ -6,6 +6,7 @@
 #include <vector>
 
 #include "exa_assembly.cuh"
+#include "exa_ldg.cuh"
 #include "exa_solver.cuh"
 #include "exa_umma.cuh"
 #include EXA_MODEL_HEADER
@@ -446,6 +447,50 @@ int exa_model_assemble(ExaCtx& c, bool jacobian) {
     }
   }
   return EXA_OK;
+}
+
+bool exa_model_has_ldg_boundary() { return ExaModel::has_ldg_boundary; }
+
+// The LDG residual of the element states u (the layout of udg: nc = ncu without q): the volume
+// integrals of the HDG residual (RuElem, uresidual.cpp:45-130, is the same quadrature), the
+// face residuals of every face, and their sum into the elements with the sign and scaling of
+// Residual (residual.cpp:589-617).
+int exa_model_ldg_residual(ExaCtx& c, const double* u, double* Ru) {
+  const ExaDims& P = c.P;
+  ExaProfScope ps(c, EXA_PH_RESIDUAL);
+  double* saved = c.udg;
+  c.udg = const_cast<double*>(u);
+  auto body = [&]() -> int {
+    const size_t vs = vol_points_smem<false>(P);
+    EXA_TRY(smem_attr((const void*)vol_points_kernel<ExaModel, false>, vs));
+    const int tpb_v = P.nge <= 64 ? 64 : (P.nge <= 128 ? 128 : 256);
+    for (int e0 = 0; e0 < P.ne; e0 += c.neb) {
+      const int nb = std::min(c.neb, P.ne - e0);
+      AsmArgs A = make_args(c, e0);
+      double* Ruc = c.Ru + (long long)e0 * P.n;
+      if (c.wRG) EXA_TRY(volume_gauss_values(c, A, e0, nb));
+      vol_points_kernel<ExaModel, false><<<nb, tpb_v, vs, c.st>>>(A, Ruc, nullptr);
+      EXA_LAUNCH_CHECK();
+      if (c.wRG) EXA_TRY(volume_residual_gemm(c, Ruc, nb));
+    }
+    LdgArgs L{};
+    L.P = P;
+    L.shapfgt = c.shapfgt; L.shapfgw = c.shapfgw; L.shapfnt = c.shapfnt;
+    L.f2e = c.f2e; L.perm = c.perm; L.bf = c.bf; L.fcon = c.ldg_fcon;
+    L.xdg = c.xdg; L.faceg = c.faceg; L.uinf = c.uinf; L.param = c.param; L.tau = c.tau;
+    L.ntau = c.ntau; L.modelnumber = c.modelnumber; L.time = c.time;
+    L.u = u; L.Rh = c.ldg_Rh;
+    const size_t fs = ldg_face_smem(P);
+    EXA_TRY(smem_attr((const void*)ldg_face_kernel<ExaModel>, fs));
+    if (P.nf > 0) {
+      ldg_face_kernel<ExaModel><<<P.nf, 64, fs, c.st>>>(L);
+      EXA_LAUNCH_CHECK();
+    }
+    return exa_k_ldg_gather(P, c.f2e, c.perm, c.elemcon, c.Ru, c.ldg_Rh, Ru, c.tdep, c.dtfactor, c.st);
+  };
+  const int st = body();
+  c.udg = saved;
+  return st;
 }
 
 // initial u from the model's cpuInitu at the element nodes (readsolstruct, readbinaryfiles.cpp:546-556)

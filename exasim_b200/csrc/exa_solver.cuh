@@ -131,7 +131,21 @@ struct ExaCtx {
   // batched GMRES (exa_batch.cu): when set, GMRES calls of this context run through the batcher
   struct ExaBatcher* batcher = nullptr;
 
+  // LDG discretisation (app.bin problem[0] = 0) and its pseudo-transient solver: the
+  // residual of the element states, its Jacobian by residual differences (flag[4]: one- or
+  // two-sided, solversparam[2]: the step), the identity preconditioner (flag[7] = 0)
+  int scheme = 1;  // 0 LDG, 1 HDG
+  int matvec_order = 1, ntau = 1;
+  double matvec_eps = 1e-3;
+  double* shapfnt = nullptr;  // face nodal basis and its derivatives at the face nodes [npf, npf, nd]
+  int* ldg_fcon = nullptr;    // [2, npf, nf]: e npe + node of face node i on each side (side 1 twice on the boundary)
+  // R(u), a perturbed state, its residual, the face residuals [npf, ncu, nf], R at u - eps v
+  double *ldg_R = nullptr, *ldg_w = nullptr, *ldg_Rw = nullptr, *ldg_Rh = nullptr, *ldg_Rm = nullptr;
+  int ldg_has_boundary = 0;
+
   long long ndofuhat() const { return (long long)P.ncu * P.npf * P.nf; }
+  // unknowns of the linear systems GMRES solves: the trace (HDG) or the element states (LDG)
+  long long sysN() const { return scheme == 0 ? (long long)P.npe * P.ncu * P.ne : ndofuhat(); }
 };
 
 // setup and teardown (exa_api.cu)
@@ -147,6 +161,10 @@ long long exa_ctx_estimate_bytes(const double* app, long long napp, const double
 // model-specific steps (instantiated per model)
 int exa_model_assemble(ExaCtx& c, bool jacobian);
 int exa_model_init_udg(ExaCtx& c, double* host_udg);
+// LDG residual (residual.cpp:589-617) of the element states u [npe, ncu, ne] into Ru
+int exa_model_ldg_residual(ExaCtx& c, const double* u, double* Ru);
+// whether the model carries the LDG boundary functions (Ubou, Fbou)
+bool exa_model_has_ldg_boundary();
 
 // model-independent drivers (exa_drivers.cu)
 int exa_drv_assemble(ExaCtx& c);

@@ -94,6 +94,12 @@ MODEL_FILES = {
     "cpuInitu", "cpuInitq", "cpuInitudg", "cpuInitwdg", "cpuInitodg",
 }
 
+OPTIONAL_BOUNDARY = ("KokkosUbou", "KokkosFbou")
+BOUNDARY_PARAMS = ("dstype* f, const dstype* xdg, const dstype* udg, const dstype* odg, const dstype* wdg, "
+                   "const dstype* uhg, const dstype* nlg, const dstype* tau, const dstype* uinf, "
+                   "const dstype* param, const dstype time, const int modelnumber, const int ib, const int ng, "
+                   "const int nc, const int ncu, const int nd, const int ncx, const int nco, const int ncw")
+
 REQUIRED = ("HdgFlux", "HdgSource", "HdgFbou", "HdgFbouonly", "KokkosFlux", "KokkosSource",
             "KokkosTdfunc", "cpuInitu")
 
@@ -132,6 +138,13 @@ def generate(srcdir: str, model_name: str) -> str:
         if kind == "dispatch":
             body = call.sub(lambda m: f"{m.group(1)}_pt(i, ", body)
         lines.append(f"__device__ __forceinline__ void {n}_pt(const size_t i, {params})\n{{{body}}}")
+    # the LDG boundary functions are optional: a model without them gets empty stand-ins and
+    # a false has_ flag, and the solver refuses LDG on meshes with boundary faces
+    for n in OPTIONAL_BOUNDARY:
+        present = n in funcs and funcs[n][1] == "dispatch"
+        if not present:
+            lines.append(f"__device__ __forceinline__ void {n}_pt(const size_t i, {BOUNDARY_PARAMS}) {{}}")
+        lines.append(f"constexpr bool has_{n} = {'true' if present else 'false'};")
     for n, (params, kind, body) in funcs.items():
         if kind == "host":
             lines.append(f"inline void {n}({params})\n{{{body}}}")

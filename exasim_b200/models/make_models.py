@@ -152,11 +152,12 @@ def _fn_sym(name, sig, tag, loads, outs):
             f"{body}\n\n{_emit(outs)}\n  }});\n}}\n")
 
 
-def write_symbolic_case(name, nd, ncu, modelD, nparam, flux, source, fbou, initu):
+def write_symbolic_case(name, nd, ncu, modelD, nparam, flux, source, fbou, initu, ubou=None):
     """One case folder from sympy callables.
 
     flux(uq, x, mu) -> [[f(m, d) for d] for m]; source(uq, x, mu) -> [s_m]; fbou(uq, x, mu,
-    uhat, n, tau) -> [fb_m] (boundary code 1); initu(x, mu) -> [u_m].  uq holds u then, for
+    uhat, n, tau) -> [fb_m] (boundary code 1); initu(x, mu) -> [u_m]; ubou (optional, same
+    arguments as fbou) -> [uhat_m], with which the LDG boundary files are written too.  uq holds u then, for
     ModelD, q with entry ncu + m + ncu*d = the d-th derivative component of u_m."""
     import sympy as sp
     nc = ncu * (nd + 1) if modelD else ncu
@@ -201,6 +202,17 @@ def write_symbolic_case(name, nd, ncu, modelD, nparam, flux, source, fbou, initu
                               f"    if (ib == 1 )\n        HdgFbou1(f, f_udg, f_wdg, f_uhg, {args});\n}}\n")
     files["HdgFbouonly"] = fb1o + (f"\nvoid HdgFbouonly({DISPATCH.format(J='')}) {{\n"
                                    f"    if (ib == 1 )\n        HdgFbouonly1(f, {args});\n}}\n")
+    if ubou is not None:
+        # the LDG boundary functions: uhat at the boundary face nodes (Ubou) and the boundary
+        # flux (Fbou), boundary code 1
+        lu_b = ubou(uq, x, mu, uh, nl, tau0)
+        files["KokkosUbou"] = (_fn_sym("KokkosUbou1", PTB.format(J=""), "Ubou", lb,
+                                       [(f"f[{m} * N + i]", lu_b[m]) for m in range(ncu)])
+                               + f"\nvoid KokkosUbou({DISPATCH.format(J='')}) {{\n"
+                               f"    if (ib == 1 )\n        KokkosUbou1(f, {args});\n}}\n")
+        files["KokkosFbou"] = (_fn_sym("KokkosFbou1", PTB.format(J=""), "Fbou", lb, bo)
+                               + f"\nvoid KokkosFbou({DISPATCH.format(J='')}) {{\n"
+                               f"    if (ib == 1 )\n        KokkosFbou1(f, {args});\n}}\n")
     U0 = initu(x, mu)
     init_loads = "\n".join(f"    dstype x{k} = x[p+npe*{k}+npe*ncx*e];" for k in range(nd))
     init_loads += "\n" + "\n".join(f"    dstype mu{k} = mu[{k}];" for k in range(nparam))
@@ -311,7 +323,8 @@ def write_symbolic_cases():
         lambda uq, x, mu, uh, nl, t0: _tau_fbou(ns2d_flux(uq, x, mu), uq, uh, nl, t0, 4, 2), tgv2d_initu)
     write_symbolic_case(
         "euler3d", 3, 5, False, 2, euler3d_flux, zero(5),
-        lambda uq, x, mu, uh, nl, t0: _tau_fbou(euler3d_flux(uq, x, mu), uq, uh, nl, t0, 5, 3), vortex3d_initu)
+        lambda uq, x, mu, uh, nl, t0: _tau_fbou(euler3d_flux(uq, x, mu), uq, uh, nl, t0, 5, 3), vortex3d_initu,
+        ubou=lambda uq, x, mu, uh, nl, t0: [uq[m] for m in range(5)])
     write_symbolic_case(
         "cdsin2d", 2, 1, True, 5, cdsin2d_flux, cdsin2d_source,
         lambda uq, x, mu, uh, nl, t0: [t0 * (0 - uh[0])], lambda x, mu: [sp.Integer(0)])

@@ -29,7 +29,14 @@ const char* exa_last_error(void);
  * (datain/app.bin, master.bin, mesh.bin, sol.bin), passed as their float64 words.
  * Replaces CDiscretization's constructor: readInput (backend/Discretization/readbinaryfiles.cpp:625),
  * buildConn for raw element lists (connectivity.cpp:1212), compGeometry (geometry.cpp:87-222),
- * qEquation (qequation.cpp:365) and the HDG allocations (discretization.cpp:245-428). */
+ * qEquation (qequation.cpp:365) and the HDG allocations (discretization.cpp:245-428).
+ * app.bin's problem[0] selects the discretization: 1 HDG, 0 LDG (setstructs.cpp:145).  An LDG
+ * context solves for the element states u (udg without q: models with ncq = 0) with the
+ * pseudo-transient solver: exa_residual, exa_matvec, exa_precond, exa_gmres, exa_newton,
+ * exa_dirk and exa_solve run the LDG forms named at each of them, on vectors of length
+ * npe*ncu*ne.  It refuses (EXA_ERR_UNSUPPORTED) models with q, a preconditioner matrix
+ * other than the identity (flag[7]), a reduced-basis guess, a polynomial preconditioner and
+ * the mixed-precision form, and boundary faces without the model's KokkosUbou/KokkosFbou. */
 int exa_create(const double* app, long long napp, const double* master, long long nmaster,
                const double* mesh, long long nmesh, const double* sol, long long nsol, int device,
                exa_ctx** out);
@@ -68,11 +75,16 @@ int exa_set_step_time(exa_ctx* ctx, double time0);
  * residuals and Jacobians (uequation.cpp:45-557), static condensation (:559-775),
  * RHS b (matvec.cpp:103) and the preconditioner (matvec.cpp:119-217). */
 int exa_assemble(exa_ctx* ctx);
-/* hdgAssembleResidual (discretization.cpp:576-592); *norm = |b| + |Ru| (solution.cpp:148-157). */
+/* hdgAssembleResidual (discretization.cpp:576-592); *norm = |b| + |Ru| (solution.cpp:148-157).
+ * LDG: R(u) of the current udg into field "Ru" (Residual, residual.cpp:589-617: element and
+ * face integrals, uresidual.cpp:45-334), *norm = |R|. */
 int exa_residual(exa_ctx* ctx, double* norm);
-/* w = A v, hdgMatVec (matvec.cpp:240-389); device vectors of length ndofuhat. */
+/* w = A v, hdgMatVec (matvec.cpp:240-389); device vectors of length ndofuhat.
+ * LDG: w = J(u) v by residual differences around the udg and R of the last exa_residual
+ * (MatVec, matvec.cpp:41-100; flag[4] one- or two-sided, solversparam[2] the step). */
 int exa_matvec(exa_ctx* ctx, const double* v_dev, double* w_dev);
-/* w = P v, ApplyPreconditioner (Preconditioning/preconditioner.cpp:273-295); v != w. */
+/* w = P v, ApplyPreconditioner (Preconditioning/preconditioner.cpp:273-295); v != w.
+ * LDG: the identity (precMatrixType 0, preconditioner.cpp:130-137). */
 int exa_precond(exa_ctx* ctx, const double* v_dev, double* w_dev);
 /* Solve A x = b by restarted GMRES (Solver/gmres.cpp:361-597); x is field "x".  When it stops at
  * the iteration cap above its tolerance it returns EXA_ERR_NOTCONV (6) with *iters and *relerr
@@ -81,7 +93,10 @@ int exa_precond(exa_ctx* ctx, const double* v_dev, double* w_dev);
 int exa_gmres(exa_ctx* ctx, int* iters, double* relerr);
 /* q from u and uhat, hdgGetQ (qequation.cpp:372-484). */
 int exa_getq(exa_ctx* ctx);
-/* Damped Newton on the HDG residual, NewtonSolver (Solution/solution.cpp:125-243). */
+/* Damped Newton on the HDG residual, NewtonSolver (Solution/solution.cpp:125-243).
+ * LDG: PTCsolver (Solver/ptcsolver.cpp:255-330): GMRES on J(u) x = -R(u), u += x, until
+ * |R(u)| < NewtonTol; *iters counts the steps, a norm above 1e6 returns EXA_ERR_NOTCONV
+ * (NaN: EXA_ERR_NAN) where the reference writes the state and exits. */
 int exa_newton(exa_ctx* ctx, int* iters, double* norm);
 /* nsteps DIRK steps around Newton (Main/exasim.hpp:413-482); newton_iters[0..max_out) receives
  * the Newton count of each stage. */

@@ -215,6 +215,15 @@ class Euler3D(_PointModel):
                          np.stack([rv, ru * vv, rv * vv + p, rw * vv, rv * h], 1),
                          np.stack([rw, ru * wv, rv * wv, rw * wv + p, rw * h], 1)], axis=2)
 
+    def ubou(self, ib, x, uq, n, tau, param, t):
+        """KokkosUbou of the model: uhat = u on every boundary."""
+        return uq[:, :self.ncu].copy()
+
+    def fbou_ldg(self, ib, x, uq, uh, n, tau, param, t):
+        """KokkosFbou of the model: f(u) . n + tau (u - uhat)."""
+        f = self._flux(uq[:, :self.nc], param)
+        return np.einsum("pkd,pd->pk", f, n) + tau[0] * (uq[:, :self.ncu] - uh)
+
     def initu(self, x, param):
         gam, M = param[0], param[1]
         phi = 5.0

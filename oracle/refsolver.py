@@ -87,6 +87,9 @@ class RefRun:
     # per Newton solve (one per steady solve or DIRK stage): [Newton steps, GMRES iterations,
     # host clock at its first residual line, at its last Newton line]
     solves: List[List[float]] = field(default_factory=list)
+    # LDG runs (PTC solver, ptcsolver.cpp:255-330): per solve, the residual norms it prints (the
+    # initial one, then one per PTC step)
+    ptc: List[List[float]] = field(default_factory=list)
 
     def dump(self, name: str) -> np.ndarray:
         """An intermediate array of a debugmode run, e.g. 'uEquationElemSchur_H' (raw FP64)."""
@@ -111,6 +114,9 @@ _RE_ASM = re.compile(r"hdgAssembleLinearSystem time: ([0-9.eE+-]+) miliseconds")
 _RE_GT = re.compile(r"^GMRES time: ([0-9.eE+-]+) miliseconds")
 _RE_STAGE = re.compile(r"Timestep :\s+(\d+),\s+Timestage :\s+(\d+)")
 _RE_SOLVE = re.compile(r"Newton Iteration: 0,\s+Residual Norm")
+_RE_PTC0 = re.compile(r"PTC Iteration: 0,\s+Solution Norm")
+_RE_PTC = re.compile(r"PTC Iteration: (\d+),\s+Residual Norm: ([-+0-9.eEnaif]+)")
+_RE_LGMRES = re.compile(r"^GMRES converges to the tolerance \S+ within\s+(\d+) iterations")
 
 
 def _start(datain: str, model: str, workdir: str, strict: bool, threads: int) -> subprocess.Popen:
@@ -135,6 +141,22 @@ def _start(datain: str, model: str, workdir: str, strict: bool, threads: int) ->
 
 def _parse(res: RefRun) -> RefRun:
     for t, ln in res.lines:
+        if _RE_PTC0.search(ln):
+            res.ptc.append([])
+            res.solves.append([0, 0, t, t])
+            continue
+        if (m := _RE_PTC.search(ln)):
+            if res.ptc:
+                res.ptc[-1].append(float(m.group(2)))
+                if len(res.ptc[-1]) > 1:
+                    res.solves[-1][0] += 1
+                    res.solves[-1][3] = t
+            continue
+        if (m := _RE_LGMRES.search(ln.strip())):
+            res.gmres_iters.append(int(m.group(1)))
+            if res.solves:
+                res.solves[-1][1] += int(m.group(1))
+            continue
         if _RE_SOLVE.search(ln):
             res.solves.append([0, 0, t, t])
         elif (m := _RE_NEWTON.search(ln)):

@@ -94,6 +94,12 @@ CASES = {
     "poisson2d_tri16_p3_poly3": ("poisson2d", lambda d: _with_problem(cases.poisson2d_tri(d, n=16), 27, 3)),
     # one request of the served stream: 8 x 8 quadrilaterals, p=3, kappa 0.05, theta 0.7
     "cdsin2d_quad8_p3": ("cdsin2d", lambda d: cases.cdsin2d_quad(d, n=8, kappa=0.05, theta=0.7, a=2, b=1)),
+    # the LDG discretisation with the pseudo-transient solver (hybrid = 0): the isentropic
+    # vortex on 3^3 p=2 hexahedra, one DIRK(2,2) step, periodic and closed by the model's
+    # Ubou / Fbou on every side
+    "euler3d_hex3_p2_ldg": ("euler3d", lambda d: cases.euler3d_vortex_hex(d, n=3, porder=2, nsteps=1, hybrid=0)),
+    "euler3d_hex3_p2_ldg_bnd": ("euler3d", lambda d: cases.euler3d_vortex_hex(d, n=3, porder=2, nsteps=1, hybrid=0,
+                                                                             periodic=False)),
 }
 
 # reference dump name -> fixture key, and the block shape used to project it (None: vector)
@@ -127,12 +133,16 @@ def make(name, out_dir=HERE):
         # normal run
         full = R.run(d, model, os.path.join(tmp, "full"))
         assert full.returncode == 0, full.stdout[-2000:]
-        pack["outuhat"] = full.uhat()
+        # an LDG run writes no trace field
+        if os.path.exists(os.path.join(full.dataout, "outuhat_np0.bin")):
+            pack["outuhat"] = full.uhat()
         pack["outudg"] = full.udg()
         pack["newton_norms"] = np.array([[a, b] for _, _, a, b in full.newton]).reshape(-1, 2)
         pack["gmres_iters"] = np.array(full.gmres_iters)
         # per Newton solve (steady solve or DIRK stage): Newton steps and GMRES iterations
         pack["solves"] = np.array([[a, b] for a, b, _, _ in full.solves], dtype=np.int64).reshape(-1, 2)
+        if int(I.read_app_bin(os.path.join(d, "app.bin"))["problem"][0]) == 0:
+            return _finish_ldg(name, model, d, tmp, full, pack, out_dir)
         # debug run: arrays of the first Newton step
         dbg_in = os.path.join(tmp, "dbg_in")
         shutil.copytree(d, dbg_in)
@@ -166,6 +176,27 @@ def make(name, out_dir=HERE):
         print(f"{name}: {os.path.getsize(fn) / 1e6:.2f} MB, Newton {pack['newton_norms'].tolist()}, "
               f"GMRES {pack['gmres_iters'].tolist()}", flush=True)
         return fn
+
+
+def _finish_ldg(name, model, d, tmp, full, pack, out_dir):
+    """An LDG case: the PTC residual norms of each stage, and from a debug run without PTC
+    steps (NewtonIter = 0) the residual of its last evaluation: the second DIRK stage's at
+    the initial state (residual.cpp:613-617 writes it at every evaluation)."""
+    pack["ptc_norms"] = np.array([v for s in full.ptc for v in s])
+    pack["ptc_lengths"] = np.array([len(s) for s in full.ptc])
+    dbg_in = os.path.join(tmp, "dbg_in")
+    shutil.copytree(d, dbg_in)
+    R.set_app_flag(dbg_in, 3, 1)
+    R.set_app_flag(dbg_in, 13, 0, part=3)
+    dbg = R.run(dbg_in, model, os.path.join(tmp, "dbg"))
+    assert dbg.returncode == 0, dbg.stdout[-2000:]
+    pack["Ru_stage2_initial"] = dbg.dump("_Ru")
+    pack["dumped"] = np.array(["Ru_stage2_initial"])
+    fn = os.path.join(out_dir, f"ref_{name}.npz")
+    np.savez_compressed(fn, **pack)
+    print(f"{name}: {os.path.getsize(fn) / 1e6:.2f} MB, PTC {full.ptc}, GMRES {pack['gmres_iters'].tolist()}",
+          flush=True)
+    return fn
 
 
 def _block_shape(size, kind, datain):

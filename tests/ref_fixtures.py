@@ -18,7 +18,17 @@ GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
 
 def names():
-    return sorted(os.path.basename(f)[4:-4] for f in glob.glob(os.path.join(GOLDEN, "ref_*.npz")))
+    """The HDG cases."""
+    return sorted(n for n in _all() if "_ldg" not in n)
+
+
+def ldg_names():
+    """The LDG cases (pseudo-transient solver): PTC norms, outudg and one residual dump."""
+    return sorted(n for n in _all() if "_ldg" in n)
+
+
+def _all():
+    return [os.path.basename(f)[4:-4] for f in glob.glob(os.path.join(GOLDEN, "ref_*.npz"))]
 
 
 def load(name: str) -> Dict[str, np.ndarray]:

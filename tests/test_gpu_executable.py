@@ -107,3 +107,22 @@ def test_executable_writes_vtu_snapshots(tmp_path):
     pvd = open(out + "vis.pvd").read()
     times = [float(t) for t in __import__("re").findall(r'timestep="([^"]+)"', pvd)]
     assert times == pytest.approx([0.01, 0.02]) and "vis_1.vtu" in pvd and "vis_2.vtu" in pvd
+
+
+def test_executable_ldg_matches_reference_outudg(tmp_path):
+    """An LDG datain (problem[0] = 0): the reference's outudg after its DIRK step, and no
+    uhat file (the reference writes the trace field for HDG alone)."""
+    from tests import ref_fixtures as RF
+    B.build(["euler3d"])
+    fx = RF.load("euler3d_hex3_p2_ldg_bnd")
+    d = RF.write_datain(fx, str(tmp_path / "datain"))
+    out = str(tmp_path / "dataout")
+    os.makedirs(out)
+    run("euler3d", d, out + "/out")
+    udg = np.fromfile(out + "/outudg_np0.bin")
+    ref = fx["outudg"]
+    assert np.array_equal(udg[:3], ref[:3])
+    nud = int(np.prod(ref[:3]))
+    a, b = udg[3:].reshape(-1, nud)[-1], ref[3:].reshape(-1, nud)[-1]
+    assert np.linalg.norm(a - b) / np.linalg.norm(b) < 1e-8
+    assert not os.path.exists(out + "/outuhat_np0.bin")
