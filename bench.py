@@ -9,8 +9,9 @@ residual check.  The headline value is the mixed-precision form (3xTF32 tensor-c
 elimination into FP32 blocks, FP64 residual refinement); the plain FP64 form of the same
 solves is timed in the same run and reported beside it.  Two more legs follow on one GPU:
 the 3D Euler isentropic-vortex configuration at its full 32^3 size in both forms (`euler3d`,
-where the elimination is compute-bound) and the served stream of 2D convection-diffusion
-requests (`served`).  Inputs are seeded synthetic data with the configurations' shapes.  With --gpus N (torchrun) every rank solves its own
+where the elimination is compute-bound), the served stream of 2D convection-diffusion
+requests (`served`), and the LDG discretisation with its pseudo-transient solver on the Euler
+vortex (`ldg`: 8^3 beside the reference's own CPU solve of the same stage, and 32^3).  Inputs are seeded synthetic data with the configurations' shapes.  With --gpus N (torchrun) every rank solves its own
 replica: the path has no data-path collective, so scaling is weak.
 
 Prints one JSON line.  `--impl reference` times the reference's own CPU solver
@@ -58,6 +59,7 @@ def parse():
                     help="Poisson arrival rates (1/s) of the served leg; the configuration sweeps 10,30,100,300,1000")
     ap.add_argument("--euler-n", type=int, default=32, help="elements per cube edge of the 3D Euler leg")
     ap.add_argument("--euler-steps", type=int, default=4, help="timed stage solves per form of the 3D Euler leg (0 skips it)")
+    ap.add_argument("--ldg-n", type=int, default=32, help="elements per cube edge of the LDG leg's large case (0 skips the leg)")
     return ap.parse_args()
 
 
@@ -190,6 +192,7 @@ def replicas_value(steps_per_rank, world, total_ms):
 
 
 REF_MODEL = "convdiff3d"
+REF_MODEL_EULER = "euler3d"
 
 
 def reference_processes(n):
@@ -497,6 +500,8 @@ def run_ours(args):
                 out["served"] = run_served(args, local)
             if args.euler_steps > 0 and world == 1:
                 out["euler3d"] = run_euler(args, local, tmp)
+            if args.ldg_n > 0 and world == 1:
+                out["ldg"] = run_ldg(args, local, tmp, with_cpu=rank == 0 and not args.no_cpu_baseline)
             if cpu_ref is not None:
                 cb = cpu_ref.result()
                 if cb is None or "unavailable" in cb:
@@ -563,6 +568,118 @@ def run_euler(args, local, tmp):
             "mixed": forms["mixed"], "plain_fp64": forms["plain_fp64"],
             "speedup_vs_plain_fp64": forms["mixed"]["value"] / forms["plain_fp64"]["value"],
             "mixed_vs_fp64_rel_l2": float(np.linalg.norm(u - ref) / np.linalg.norm(ref))}
+
+
+LDG_SMALL_N = 8
+
+
+def ldg_residual_bytes(sz, nge, ngf):
+    """Algorithmic bytes of one LDG residual evaluation: the states and the stage source read
+    once, the element geometry (Gauss-point coordinates, Xx, jacobian) and the face geometry
+    (coordinates, normal, jacobian) read once, the residual written once."""
+    ne, nf, npe, ncu, nd = sz["ne"], sz["nf"], sz["npe"], sz["ncu"], sz["nd"]
+    return 8 * (3 * npe * ncu * ne + nge * (nd + nd * nd + 1) * ne + ngf * (nd + nd + 1) * nf)
+
+
+def run_ldg(args, local, tmp, with_cpu):
+    """The LDG leg: the reference's other discretisation (problem[0] = 0) on the 3D Euler
+    isentropic vortex, p = 3 hexahedra of a periodic cube, the first DIRK(2,2) stage solved by
+    the pseudo-transient solver (GMRES(50) on finite-difference Jacobian products, identity
+    preconditioner, PTC to 1e-8).  Each timed solve starts from the same initial state.  On
+    LDG_SMALL_N^3 elements the reference's own CPU solver runs the same stage solve (one
+    process, one thread, beside the GPU work); on args.ldg_n^3 the residual evaluation, the
+    products' building block, is timed with CUDA events on the context's stream against its
+    algorithmic bytes."""
+    import torch
+    from exasim_b200 import HDGSolver, build as B, cases
+    from oracle import refsolver as R
+    B.build(["euler3d"])
+    peaks, src = measured_peaks()
+    ref_res, ref_err, th = {}, {}, None
+    ds = os.path.join(tmp, "ldg_small")
+    cases.euler3d_vortex_hex(ds, n=LDG_SMALL_N, porder=3, nsteps=1, hybrid=0)
+    if with_cpu and R.available(REF_MODEL_EULER):
+        def go():
+            try:
+                ref_res["r"] = R.run_many(ds, REF_MODEL_EULER, [os.path.join(tmp, "ldg_ref")], threads=1, timeout=900,
+                                          stop_after_stages=1)[0]
+            except Exception as e:  # noqa: BLE001 - reported in the line instead
+                ref_err["e"] = repr(e)
+        th = threading.Thread(target=go, daemon=True)
+        th.start()
+    out = {"workload": "3D Euler LDG p=3, periodic n^3 hexahedra, isentropic vortex strength 5, Mach 0.5, first "
+                       "DIRK(2,2) stage (dt 0.05) by pseudo-transient continuation to |R| < 1e-8: GMRES(50) to 1e-8 "
+                       "on finite-difference Jacobian products (step 1e-3), identity preconditioner"}
+    for name, n, W, K in (("small", LDG_SMALL_N, 2, 5), ("large", args.ldg_n, 1, 3)):
+        d = ds if name == "small" else os.path.join(tmp, f"ldg_{n}")
+        if name != "small":
+            cases.euler3d_vortex_hex(d, n=n, porder=3, nsteps=1, hybrid=0)
+        s = HDGSolver(d, "euler3d", device=local)
+        stream = torch.cuda.ExternalStream(s.stream())
+        u0 = s.get("udg")
+        ms, its = [], []
+        for k in range(W + K):
+            s.set("udg", u0)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            it, _ = s.DIRKStage(0, 0)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            if k >= W:
+                ms.append(e0.elapsed_time(e1))
+                its.append((it, s.stats()["gmres_total"]))
+        r = {"elements": n ** 3, "unknowns": int(s.sizes["npe"] * s.sizes["ncu"] * s.sizes["ne"]),
+             "ms_per_stage_solve": float(np.mean(ms)), "stage_solves_per_s": 1000.0 / float(np.mean(ms)),
+             "ptc_steps": its[-1][0], "gmres_iters": its[-1][1]}
+        if name == "large":
+            # residual evaluations alone at the stage's time and source
+            s.set("udg", u0)
+            s.DIRKStage(0, 0)
+            for _ in range(3):
+                s.evalResidual()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            reps = 20
+            e0.record(stream)
+            for _ in range(reps):
+                s.evalResidual()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            rms = e0.elapsed_time(e1) / reps
+            nge = s.sizes["nge"]
+            ngf = s.sizes["ngf"]
+            ab = ldg_residual_bytes(s.sizes, nge, ngf)
+            achieved = ab / (rms * 1e-3) / 1e9
+            r["residual_ms"] = rms
+            r["residual_roofline"] = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                                      "frac": achieved / peaks["hbm_gbs"], "peak_source": src,
+                                      "algorithmic_bytes": ab,
+                                      "note": "one residual evaluation with its norm; its kernels pass the "
+                                              "Gauss-point values and face residuals through HBM, so DRAM "
+                                              "traffic exceeds these bytes"}
+            s.profile(True)
+            s.set("udg", u0)
+            s.DIRKStage(0, 0)
+            torch.cuda.synchronize()
+            r["phases"] = phases_of(s.profile_read(), 1)
+            s.profile(False)
+        s.close()
+        out[name] = r
+    if th is not None:
+        th.join()
+        rr = ref_res.get("r")
+        if rr is not None and R.stage_times(rr):
+            sec = R.stage_times(rr)[0]
+            out["small"]["reference_cpu"] = {
+                "ms_per_stage_solve": sec * 1000.0, "cores": 1, "kind": "reference",
+                "sample": f"cput2cEXASIM (-O3 -ffast-math, one thread) with problem[0] = 0 on the same "
+                          f"{LDG_SMALL_N}^3 input, the same first-stage PTC solve ({len(rr.ptc[0]) - 1} PTC steps, "
+                          f"{rr.solves[0][1]} GMRES iterations)"}
+            out["small"]["speedup_vs_reference_cpu"] = sec * 1000.0 / out["small"]["ms_per_stage_solve"]
+        else:
+            out["small"]["reference_cpu"] = {"unavailable": ref_err.get("e", "reference run gave no stage time")}
+    return out
 
 
 SERVED_WORKLOAD = ("served stream of 2D convection-diffusion HDG solves: kappa log-uniform [1e-3, 1], unit "

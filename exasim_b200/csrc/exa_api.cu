@@ -342,6 +342,11 @@ int exa_ctx_init(ExaCtx& c, const double* app, long long napp, const double* mas
       return EXA_ERR_ARG;
     }
     EXA_TRY(dev_upload(c, &c.shapfnt, M.part[7], (size_t)M.nsize[7]));
+    {
+      bool split = true;
+      for (int f = 0; f < conn.nf && split; ++f) split = (conn.f2e[4 * f + 2] >= 0) == (f < conn.nf0);
+      c.ldg_split = split ? 1 : 0;
+    }
     EXA_TRY(dev_alloc(c, &c.ldg_fcon, 2 * (size_t)P.npf * P.nf));
     EXA_TRY(exa_k_ldg_fcon(P, c.f2e, c.perm, c.elemcon, c.ldg_fcon, c.st));
     const size_t nl = (size_t)P.npe * P.ncu * ne;
@@ -395,39 +400,49 @@ int exa_ctx_init(ExaCtx& c, const double* app, long long napp, const double* mas
     EXA_TRY(dev_alloc(c, &c.d_flag, 4));
   }
 
-  // condensed system and workspace
+  // condensed system and workspace (the HDG arrays; an LDG context needs the element
+  // residual, the volume residual's chunk workspace and the Krylov vectors only)
   // B and G (the q columns) exist only for models with q
+  const bool hdg = c.scheme != 0;
   const size_t n = P.n, m = P.m, nqn = P.ncq > 0 ? (size_t)P.npe * P.nd * P.ncu : 0;
-  EXA_TRY(dev_alloc(c, &c.H, ne * m * m));
-  EXA_TRY(dev_alloc(c, &c.F, ne * n * m));
+  if (hdg) {
+    EXA_TRY(dev_alloc(c, &c.H, ne * m * m));
+    EXA_TRY(dev_alloc(c, &c.F, ne * n * m));
+  }
   EXA_TRY(dev_alloc(c, &c.Ru, ne * n));
-  EXA_TRY(dev_alloc(c, &c.Rh, ne * m));
+  if (hdg) EXA_TRY(dev_alloc(c, &c.Rh, ne * m));
   const size_t N = (size_t)std::max(c.ndofuhat(), c.sysN());
   EXA_TRY(dev_alloc(c, &c.b, N));
-  if (c.preconditioner == 0)
+  if (!hdg) {
+  } else if (c.preconditioner == 0) {
     EXA_TRY(dev_alloc(c, &c.Pc, (size_t)P.ncu * P.npf * P.ncu * P.npf * P.nf));
-  else if (c.preconditioner == 2)
+  } else if (c.preconditioner == 2) {
     EXA_TRY(dev_alloc(c, &c.Pc, (size_t)P.ncu * P.npf * P.ncu * P.npf * c.bilu.nse * c.bilu.nnz));
-  else
+  } else {
     EXA_TRY(dev_alloc(c, &c.Pc, ne * m * m));
+  }
   // element chunk: bounded workspace (about 8 GB at most)
-  const size_t inv_ws = exa_inverse_needs_ws((int)n) ? n * n : 0;
-  const size_t per_elem = sizeof(double) * (n * n + n * nqn + n * m + m * n + m * nqn +
-                                            (size_t)P.nge * (P.nd + 1) * P.ncu * P.nc + n + inv_ws);
+  const size_t inv_ws = hdg && exa_inverse_needs_ws((int)n) ? n * n : 0;
+  const size_t vol_ws = (size_t)P.nge * P.nc + (size_t)P.nge * P.ncu + (size_t)P.nge * (P.nd + 1) * P.ncu;
+  const size_t per_elem = hdg ? sizeof(double) * (n * n + n * nqn + n * m + m * n + m * nqn +
+                                                  (size_t)P.nge * (P.nd + 1) * P.ncu * P.nc + n + inv_ws)
+                              : sizeof(double) * (vol_ws + n);
   size_t cap = (size_t)8 << 30;
   c.neb = (int)std::max<size_t>(1, std::min<size_t>(std::min<size_t>(ne, cap / per_elem), 65535));
   const size_t nb = c.neb;
-  EXA_TRY(dev_alloc(c, &c.wD, nb * n * n));
-  EXA_TRY(dev_alloc(c, &c.wB, std::max<size_t>(1, nb * n * nqn)));
-  EXA_TRY(dev_alloc(c, &c.wF, nb * n * m));
-  EXA_TRY(dev_alloc(c, &c.wK, nb * m * n));
-  EXA_TRY(dev_alloc(c, &c.wG, std::max<size_t>(1, nb * m * nqn)));
-  EXA_TRY(dev_alloc(c, &c.wRg, nb * P.nge * (P.nd + 1) * P.ncu * P.nc));
-  EXA_TRY(dev_alloc(c, &c.wRu, nb * n));
+  if (hdg) {
+    EXA_TRY(dev_alloc(c, &c.wD, nb * n * n));
+    EXA_TRY(dev_alloc(c, &c.wB, std::max<size_t>(1, nb * n * nqn)));
+    EXA_TRY(dev_alloc(c, &c.wF, nb * n * m));
+    EXA_TRY(dev_alloc(c, &c.wK, nb * m * n));
+    EXA_TRY(dev_alloc(c, &c.wG, std::max<size_t>(1, nb * m * nqn)));
+    EXA_TRY(dev_alloc(c, &c.wRg, nb * P.nge * (P.nd + 1) * P.ncu * P.nc));
+    EXA_TRY(dev_alloc(c, &c.wRu, nb * n));
+  }
   EXA_TRY(dev_alloc(c, &c.wUG, nb * P.nge * P.nc));
   EXA_TRY(dev_alloc(c, &c.wSG, nb * P.nge * P.ncu));
   EXA_TRY(dev_alloc(c, &c.wRG, nb * P.nge * (P.nd + 1) * P.ncu));
-  {
+  if (hdg) {
     // T factors of the FP64 volume products: at most 512 MB, the chunk taken in parts
     const size_t per = (size_t)P.npe * P.nge * P.ncu * P.nc;
     c.wT_elems = (int)std::max<size_t>(1, std::min<size_t>(nb, (512u << 20) / (8 * per)));
@@ -435,6 +450,13 @@ int exa_ctx_init(ExaCtx& c, const double* app, long long napp, const double* mas
   }
   if (inv_ws) EXA_TRY(dev_alloc(c, &c.wInv, nb * inv_ws));
   {
+    // the chunk-wide GEMMs of the residual: udg and the stage source at the Gauss points, and
+    // the integrand's contraction with shapegw (one product each over the whole chunk)
+    EXA_TRY(exa_gemm_tune(P.nge, P.nc * (int)nb, P.npe, 1, c.st));
+    if (c.tdep) EXA_TRY(exa_gemm_tune(P.nge, P.ncu * (int)nb, P.npe, 1, c.st));
+    EXA_TRY(exa_gemm_tune(P.npe, P.ncu * (int)nb, P.nge * (P.nd + 1), 1, c.st));
+  }
+  if (hdg) {
     // the FP64 element products of the assembly: the fastest GEMM tile of each shape is
     // measured once per process and device (q elimination, D^-1 F, K D^-1 F)
     const int kq = P.npe * P.nd, nbt = (int)std::min<size_t>(nb, 512);
@@ -454,7 +476,7 @@ int exa_ctx_init(ExaCtx& c, const double* app, long long napp, const double* mas
   EXA_TRY(dev_alloc(c, &c.x, N));
   EXA_TRY(dev_alloc(c, &c.r, N));
   EXA_TRY(dev_alloc(c, &c.w, N));
-  EXA_TRY(dev_alloc(c, &c.we, ne * m));
+  if (hdg) EXA_TRY(dev_alloc(c, &c.we, ne * m));
   EXA_TRY(dev_alloc(c, &c.du, ne * n));
   const int VB = exa_vec_blocks();
   EXA_TRY(dev_alloc(c, &c.part_a, VB));
@@ -583,6 +605,7 @@ int exa_ctx_set_precision(ExaCtx& c, int mode) {
     exa_set_error("the mixed-precision form condenses the HDG system; the LDG path runs in FP64");
     return EXA_ERR_UNSUPPORTED;
   }
+  if (c.scheme == 0) return EXA_OK;  // LDG: FP64 already, no condensed arrays
   if (mode == 1) {
     EXA_TRY(fp64_blocks(c, false));
     // the mixed assembly writes only the face blocks of the chunk arrays F, K and H (its
@@ -796,6 +819,9 @@ bool field(ExaCtx& c, const char* name, FieldRef& f) {
   const ExaDims& P = c.P;
   const long long ne = P.ne, n = P.n, m = P.m, N = c.sysN();
   const std::string s(name ? name : "");
+  if (c.scheme == 0 && s != "udg" && s != "uh" && s != "Ru" && s != "b" && s != "x" && s != "sdg" && s != "elemg" &&
+      s != "faceg")
+    return false;  // an LDG context holds no condensed or preconditioner arrays
   if (s == "udg") f = {c.udg, (long long)P.npe * P.nc * ne};
   else if (s == "uh") f = {c.uh, c.ndofuhat()};
   else if (s == "Ru" && c.scheme == 0) f = {c.ldg_R, N};  // the LDG residual of the last exa_residual

@@ -13,6 +13,8 @@
 // One block per element; all of an element's faces are handled by the same block in
 // sequence, so face contributions accumulate into D, B and Ru without atomics.
 #pragma once
+#include <algorithm>
+
 #include "exa_kernels.cuh"
 #include "exa_tc.cuh"
 #include "exa_umma.cuh"
@@ -45,6 +47,84 @@ struct AsmArgs {
 // volume: quadrature-point values, Ru (volume part) and the Jacobian integrands rgJ
 // rgJ per element: [nge, nd+1, ncu, nc]
 // ----------------------------------------------------------------------------------
+// The residual-only volume integrand with the Gauss-point values precomputed (ugpre, sgpre;
+// rgout set): one thread per Gauss point of the chunk, the model evaluated at that point alone
+// (N = 1), so with the dimension and the number of fields fixed at compile time its inputs and
+// outputs stay in registers.  The same arithmetic as vol_points_kernel<Mdl, false> (the model's
+// sums do not depend on N), with no shared memory and no barriers.  For nc <= VP_NC.
+constexpr int VP_NC = 32;
+template <class Mdl, int ND, int NCU>
+__global__ void __launch_bounds__(128) vol_pointwise_kernel(AsmArgs A, int nb) {
+  const ExaDims& P = A.P;
+  const int nge = P.nge, nc = P.nc, ncx = P.ncx;
+  const long long total = (long long)nb * nge;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int g = (int)(t % nge);
+    const long long le = t / nge, e = A.e0 + le;
+    const double* eg = A.elemg + e * P.elemg_stride();
+    const double* Xx = eg + nge * ncx;
+    double x[ND], uq[VP_NC], s[NCU], f[NCU * ND], td[NCU];
+#pragma unroll
+    for (int c = 0; c < ND; ++c) x[c] = eg[g + nge * c];
+#pragma unroll
+    for (int c = 0; c < VP_NC; ++c)
+      if (c < nc) uq[c] = A.ugpre[g + nge * (c + (long long)nc * le)];
+#pragma unroll
+    for (int k = 0; k < NCU; ++k) {
+      s[k] = 0.0;
+      td[k] = 1.0;
+    }
+#pragma unroll
+    for (int q = 0; q < NCU * ND; ++q) f[q] = 0.0;
+    if (!A.tdep || A.sourcefunc == 1)
+      Mdl::source_only(0, s, x, uq, nullptr, nullptr, A.uinf, A.param, A.time, A.modelnumber, 1, nc, NCU, ND, ncx,
+                       P.nco, P.ncw);
+    Mdl::flux_only(0, f, x, uq, nullptr, nullptr, A.uinf, A.param, A.time, A.modelnumber, 1, nc, NCU, ND, ncx, P.nco,
+                   P.ncw);
+    if (A.tdep && A.tdfunc == 1)
+      Mdl::tdfunc(0, td, x, uq, nullptr, nullptr, A.uinf, A.param, A.time, A.modelnumber, 1, nc, NCU, ND, ncx, P.nco,
+                  P.ncw);
+    const double J = Xx[nge * ND * ND + g];
+    double* o = A.rgout + (long long)le * nge * (ND + 1) * NCU;
+#pragma unroll
+    for (int k = 0; k < NCU; ++k) {
+      double sg = s[k];
+      if (A.tdep) {
+        double fv = 1.0 * A.sgpre[g + nge * (k + (long long)NCU * le)] + (-A.dtfactor) * uq[k];
+        if (A.tdfunc == 1) fv = 1.0 * fv * td[k];
+        sg = 1.0 * sg + 1.0 * fv;
+      }
+      o[g + nge * (ND + 1) * k] = sg * J;
+#pragma unroll
+      for (int mm = 0; mm < ND; ++mm) {
+        double v = f[k] * Xx[g + nge * (ND * mm)];
+#pragma unroll
+        for (int j = 1; j < ND; ++j) v += f[k + NCU * j] * Xx[g + nge * (j + ND * mm)];
+        o[g + nge * (1 + mm) + nge * (ND + 1) * k] = v;
+      }
+    }
+  }
+}
+
+// Launches vol_pointwise_kernel for the model's (nd, ncu); false when that pair has no instance
+template <class Mdl>
+bool launch_vol_pointwise(const AsmArgs& A, int nb, cudaStream_t st) {
+  const ExaDims& P = A.P;
+  if (P.nc > VP_NC || !A.ugpre || !A.rgout || (A.tdep && !A.sgpre)) return false;
+  const long long total = (long long)nb * P.nge;
+  const int blocks = (int)std::min<long long>((total + 127) / 128, 1 << 20);
+#define EXA_VP(ND, NCU)                                                   \
+  if (P.nd == ND && P.ncu == NCU) {                                       \
+    vol_pointwise_kernel<Mdl, ND, NCU><<<blocks, 128, 0, st>>>(A, nb);    \
+    return true;                                                          \
+  }
+  EXA_VP(1, 1) EXA_VP(2, 1) EXA_VP(3, 1) EXA_VP(2, 2) EXA_VP(3, 2) EXA_VP(2, 3) EXA_VP(3, 3)
+  EXA_VP(2, 4) EXA_VP(3, 4) EXA_VP(2, 5) EXA_VP(3, 5)
+#undef EXA_VP
+  return false;
+}
+
 template <class Mdl, bool JAC>
 __global__ void vol_points_kernel(AsmArgs A, double* Ru, double* rgJ) {
   extern __shared__ double sm[];

@@ -239,23 +239,26 @@ long long tiles_cost(int M, int N, int bm, int bn) {
 }
 
 // CTA tiles sized to the element blocks: 128 x 64, 128 x 80, 160 x 32 and 160 x 64 cover
-// 125 -> 128 and 150 -> 160 with little padding
-constexpr int kTiles = 4;
-constexpr int kTile[kTiles][2] = {{128, 64}, {128, 80}, {160, 32}, {160, 64}};
+// 125 -> 128 and 150 -> 160 with little padding; 64 x 128 and 64 x 64 fit the chunk-wide
+// products with 64 rows (Gauss points or nodes of a p = 3 hexahedron) and long rows of columns
+constexpr int kTiles = 6;
+constexpr int kTile[kTiles][2] = {{128, 64}, {128, 80}, {160, 32}, {160, 64}, {64, 128}, {64, 64}};
 
 int launch_tile(int t, const GemmBatch& g, cudaStream_t st) {
   switch (t) {
     case 0: return launch_dmma<4, 4, 4, 2>(g, st);
     case 1: return launch_dmma<4, 5, 4, 2>(g, st);
     case 2: return launch_dmma<5, 2, 4, 2>(g, st);
-    default: return launch_dmma<5, 4, 4, 2>(g, st);
+    case 3: return launch_dmma<5, 4, 4, 2>(g, st);
+    case 4: return launch_dmma<2, 8, 4, 2>(g, st);
+    default: return launch_dmma<2, 4, 4, 2>(g, st);
   }
 }
 
 std::mutex g_tune_mu;
 std::map<std::array<int, 4>, int> g_tune;  // (device, M, N, K) -> measured fastest tile
 
-// the measured tile of this shape, else the first three tiles by padded area
+// the measured tile of this shape, else the least padded of 128 x 64, 128 x 80, 160 x 32 and 64 x 128
 int gemm_tile(int M, int N, int K) {
   int dev = 0;
   if (cudaGetDevice(&dev) == cudaSuccess) {
@@ -265,7 +268,7 @@ int gemm_tile(int M, int N, int K) {
   }
   int best = 0;
   long long bc = -1;
-  for (int i = 0; i < 3; ++i) {
+  for (int i : {0, 1, 2, 4}) {
     const long long c = tiles_cost(M, N, kTile[i][0], kTile[i][1]);
     if (bc < 0 || c < bc) { bc = c; best = i; }
   }
@@ -1239,8 +1242,20 @@ __device__ __forceinline__ double sum_partials(const double* part) {
 
 __global__ void __launch_bounds__(VT) dot_kernel(const double* x, const double* y, long long n, double* part) {
   double v = 0.0;
-  for (long long i = blockIdx.x * (long long)VT + threadIdx.x; i < n; i += (long long)gridDim.x * VT)
-    v = fma(x[i], y[i], v);
+  // four strides' loads in flight, summed in the order of one stride at a time
+  const long long stride = (long long)gridDim.x * VT;
+  long long i = blockIdx.x * (long long)VT + threadIdx.x;
+  for (; i + 3 * stride < n; i += 4 * stride) {
+    double a[4], b[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      a[u] = x[i + u * stride];
+      b[u] = y[i + u * stride];
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) v = fma(a[u], b[u], v);
+  }
+  for (; i < n; i += stride) v = fma(x[i], y[i], v);
   double s = block_sum(v);
   if (threadIdx.x == 0) part[blockIdx.x] = s;
 }
@@ -1271,10 +1286,31 @@ __global__ void __launch_bounds__(VT) mgs_step_kernel(double* w, const double* v
   const double h = sum_partials_n(part_in, gridDim.x);
   if (blockIdx.x == 0 && threadIdx.x == 0) *h_out = h;
   double v = 0.0;
-  for (long long i = blockIdx.x * (long long)VT + threadIdx.x; i < n; i += (long long)gridDim.x * VT) {
-    double wi = w[i] - h * vprev[i];
+  // the basis vectors stream through (evict-first loads), so a vector being orthogonalised
+  // that fits in L2 stays there across the steps of its Gram-Schmidt sweep.  Four strides'
+  // loads are issued before their updates (long vectors need the loads in flight); the
+  // products are summed in the same order as one stride at a time.
+  const long long stride = (long long)gridDim.x * VT;
+  long long i = blockIdx.x * (long long)VT + threadIdx.x;
+  for (; i + 3 * stride < n; i += 4 * stride) {
+    double ww[4], p[4], q[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      ww[u] = w[i + u * stride];
+      p[u] = __ldcs(vprev + i + u * stride);
+      q[u] = vnext ? __ldcs(vnext + i + u * stride) : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const double wi = ww[u] - h * p[u];
+      w[i + u * stride] = wi;
+      v = fma(wi, vnext ? q[u] : wi, v);
+    }
+  }
+  for (; i < n; i += stride) {
+    double wi = w[i] - h * __ldcs(vprev + i);
     w[i] = wi;
-    v = fma(wi, vnext ? vnext[i] : wi, v);
+    v = fma(wi, vnext ? __ldcs(vnext + i) : wi, v);
   }
   double s = block_sum(v);
   if (threadIdx.x == 0) part_out[blockIdx.x] = s;
@@ -1285,7 +1321,16 @@ __global__ void __launch_bounds__(VT) mgs_finish_kernel(double* vout, const doub
   const double h = sqrt(sum_partials_n(part_in, gridDim.x));
   if (blockIdx.x == 0 && threadIdx.x == 0) *h_out = h;
   const double r = 1.0 / h;
-  for (long long i = blockIdx.x * (long long)VT + threadIdx.x; i < n; i += (long long)gridDim.x * VT) vout[i] = w[i] * r;
+  const long long stride = (long long)gridDim.x * VT;
+  long long i = blockIdx.x * (long long)VT + threadIdx.x;
+  for (; i + 3 * stride < n; i += 4 * stride) {
+    double a[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) a[u] = w[i + u * stride];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) vout[i + u * stride] = a[u] * r;
+  }
+  for (; i < n; i += stride) vout[i] = w[i] * r;
 }
 
 // cpuApplyGivensRotation (backend/Common/cpuimpl.h:167-196) on the device

@@ -438,7 +438,8 @@ int exa_model_assemble(ExaCtx& c, bool jacobian) {
     } else {
       ExaProfScope ps(c, EXA_PH_RESIDUAL);
       if (c.wRG) EXA_TRY(volume_gauss_values(c, A, e0, nb));
-      vol_points_kernel<ExaModel, false><<<nb, tpb_v, vs, c.st>>>(A, Ruc, nullptr);
+      if (!launch_vol_pointwise<ExaModel>(A, nb, c.st))
+        vol_points_kernel<ExaModel, false><<<nb, tpb_v, vs, c.st>>>(A, Ruc, nullptr);
       EXA_LAUNCH_CHECK();
       if (c.wRG) EXA_TRY(volume_residual_gemm(c, Ruc, nb));
       face_kernel<ExaModel, false><<<nb, tpb_f, fs, c.st>>>(A, Ruc, Rhc, nullptr, nullptr, nullptr, nullptr, nullptr,
@@ -469,7 +470,8 @@ int exa_model_ldg_residual(ExaCtx& c, const double* u, double* Ru) {
       AsmArgs A = make_args(c, e0);
       double* Ruc = c.Ru + (long long)e0 * P.n;
       if (c.wRG) EXA_TRY(volume_gauss_values(c, A, e0, nb));
-      vol_points_kernel<ExaModel, false><<<nb, tpb_v, vs, c.st>>>(A, Ruc, nullptr);
+      if (!launch_vol_pointwise<ExaModel>(A, nb, c.st))
+        vol_points_kernel<ExaModel, false><<<nb, tpb_v, vs, c.st>>>(A, Ruc, nullptr);
       EXA_LAUNCH_CHECK();
       if (c.wRG) EXA_TRY(volume_residual_gemm(c, Ruc, nb));
     }
@@ -482,8 +484,16 @@ int exa_model_ldg_residual(ExaCtx& c, const double* u, double* Ru) {
     L.u = u; L.Rh = c.ldg_Rh;
     const size_t fs = ldg_face_smem(P);
     EXA_TRY(smem_attr((const void*)ldg_face_kernel<ExaModel>, fs));
-    if (P.nf > 0) {
-      ldg_face_kernel<ExaModel><<<P.nf, 64, fs, c.st>>>(L);
+    // interior faces by the pointwise kernel where the model's (nd, ncu) has one, the boundary
+    // faces (and otherwise all) by the general one
+    int fgen = 0;
+    if (c.ldg_split && launch_ldg_face_inner<ExaModel>(L, P.nf0, c.st)) {
+      EXA_LAUNCH_CHECK();
+      fgen = P.nf0;
+    }
+    if (P.nf > fgen) {
+      L.f0 = fgen;
+      ldg_face_kernel<ExaModel><<<P.nf - fgen, 64, fs, c.st>>>(L);
       EXA_LAUNCH_CHECK();
     }
     return exa_k_ldg_gather(P, c.f2e, c.perm, c.elemcon, c.Ru, c.ldg_Rh, Ru, c.tdep, c.dtfactor, c.st);

@@ -142,6 +142,9 @@ struct ExaCtx {
   // R(u), a perturbed state, its residual, the face residuals [npf, ncu, nf], R at u - eps v
   double *ldg_R = nullptr, *ldg_w = nullptr, *ldg_Rw = nullptr, *ldg_Rh = nullptr, *ldg_Rm = nullptr;
   int ldg_has_boundary = 0;
+  // interior faces are faces [0, nf0) and boundary faces the rest (the pointwise interior-face
+  // kernel relies on it)
+  int ldg_split = 0;
 
   long long ndofuhat() const { return (long long)P.ncu * P.npf * P.nf; }
   // unknowns of the linear systems GMRES solves: the trace (HDG) or the element states (LDG)
