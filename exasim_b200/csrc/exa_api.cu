@@ -379,6 +379,12 @@ int exa_ctx_init(ExaCtx& c, const double* app, long long napp, const double* mas
     EXA_TRY(dev_alloc(c, &c.wq_ug, ne * P.nge * P.ncu));
     EXA_TRY(dev_alloc(c, &c.wq_v, ne * P.nge * P.nd * P.nd * P.ncu));
     EXA_TRY(dev_alloc(c, &c.wq_w, ne * P.npe * P.nd * P.ncu));
+    // the two products of q recovery over all elements: u at the Gauss points (one batch entry
+    // per field) and the gradient moments C_d u (large meshes only, as above)
+    if ((long long)ne * P.nge * P.npe >= (1LL << 25)) {
+      EXA_TRY(exa_gemm_tune(P.nge, (int)ne, P.npe, P.ncu, c.st));
+      EXA_TRY(exa_gemm_tune(P.npe, P.ncu * P.nd * (int)ne, P.nge * P.nd, 1, c.st));
+    }
     GemmBatch g{};
     g.M = P.npe; g.N = P.npe; g.K = P.npe; g.alpha = 1.0; g.beta = 0.0;
     g.A = mass; g.lda = P.npe; g.sA = (long long)P.npe * P.npe; g.sA2 = 0;
@@ -449,9 +455,10 @@ int exa_ctx_init(ExaCtx& c, const double* app, long long napp, const double* mas
     EXA_TRY(dev_alloc(c, &c.wT, (size_t)c.wT_elems * per));
   }
   if (inv_ws) EXA_TRY(dev_alloc(c, &c.wInv, nb * inv_ws));
-  {
+  if ((long long)nb * P.nge * P.npe >= (1LL << 25)) {
     // the chunk-wide GEMMs of the residual: udg and the stage source at the Gauss points, and
-    // the integrand's contraction with shapegw (one product each over the whole chunk)
+    // the integrand's contraction with shapegw (one product each over the whole chunk); small
+    // meshes (the served stream's) keep the padding heuristic rather than pay for the timing
     EXA_TRY(exa_gemm_tune(P.nge, P.nc * (int)nb, P.npe, 1, c.st));
     if (c.tdep) EXA_TRY(exa_gemm_tune(P.nge, P.ncu * (int)nb, P.npe, 1, c.st));
     EXA_TRY(exa_gemm_tune(P.npe, P.ncu * (int)nb, P.nge * (P.nd + 1), 1, c.st));
