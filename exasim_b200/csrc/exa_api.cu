@@ -170,7 +170,8 @@ int exa_ctx_init(ExaCtx& c, const double* app, long long napp, const double* mas
   c.ntau = (int)A.nsize[8];
   if (c.scheme == 0) {
     // LDG with the pseudo-transient solver: models without q, the finite-difference Jacobian
-    // (flag[4], solversparam[2]) and the identity preconditioner (flag[7] = 0)
+    // (flag[4], solversparam[2]), the identity preconditioner (flag[7] = 0) and the reduced-basis
+    // initial guess (problem[16])
     c.matvec_order = (int)flag[4];
     c.matvec_eps = A.nsize[7] > 2 ? solvers[2] : 1e-3;
     const int prec_matrix = (int)flag[7];
@@ -185,7 +186,6 @@ int exa_ctx_init(ExaCtx& c, const double* app, long long napp, const double* mas
     }
     if (!(c.matvec_eps > 0.0)) { exa_set_error("LDG finite-difference step %g is not positive", c.matvec_eps); return EXA_ERR_ARG; }
     if (prec_matrix != 0) { exa_set_error("LDG preconditioner matrix type %d: only the identity (0)", prec_matrix); return EXA_ERR_UNSUPPORTED; }
-    if (c.RBdim > 0) { exa_set_error("LDG with a reduced-basis initial guess (RBdim=%d) is not supported", c.RBdim); return EXA_ERR_UNSUPPORTED; }
     if (c.ppdegree > 1) { exa_set_error("LDG with a polynomial preconditioner is not supported"); return EXA_ERR_UNSUPPORTED; }
   }
   if (mpiprocs > 1) { exa_set_error("multi-rank inputs: this solver runs one GPU per mesh"); return EXA_ERR_UNSUPPORTED; }

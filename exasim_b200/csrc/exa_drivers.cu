@@ -499,7 +499,7 @@ int gmres_body(ExaCtx& c, int* iters_out, double* relerr_out) {
   double nrmb = 0.0, nrmr = 0.0;
   // the polynomial's Ritz values, from the current operator (gmres.cpp:385-398)
   if (c.ppdegree > 1) EXA_TRY(poly_setup(c));
-  EXA_CUDA(cudaMemsetAsync(c.x, 0, sizeof(double) * N, c.st));
+  if (!c.gmres_x_preset) EXA_CUDA(cudaMemsetAsync(c.x, 0, sizeof(double) * N, c.st));
   EXA_TRY(exa_drv_norm(c, c.b, N, &nrmb));
   c.last_gmres_converged = true;
   // the HDG solve stops at a right-hand side below the Newton tolerance; the LDG GMRES
@@ -511,9 +511,9 @@ int gmres_body(ExaCtx& c, int* iters_out, double* relerr_out) {
   }
   // initial guess from the reduced basis (LinearSolver, ptcsolver.cpp:374-379); a guess of
   // norm at most 1e-12 counts as none, as in gmres.cpp:404-421
-  if (c.RBdim > 0 && c.rb_cur > 0) EXA_TRY(rb_initial_guess(c));
+  if (!c.gmres_x_preset && c.RBdim > 0 && c.rb_cur > 0) EXA_TRY(rb_initial_guess(c));
   double scalar = 0.0;
-  if (c.RBdim > 0 && c.rb_cur > 0) EXA_TRY(exa_drv_norm(c, c.x, N, &scalar));
+  if (c.gmres_x_preset || (c.RBdim > 0 && c.rb_cur > 0)) EXA_TRY(exa_drv_norm(c, c.x, N, &scalar));
   if (scalar > 1e-12) {
     EXA_TRY(exa_drv_matvec(c, c.x, c.w));
     EXA_TRY(exa_axpby(c.w, c.b, 1.0, -1.0, N, c.st));  // w = b - A x
@@ -635,9 +635,34 @@ int exa_drv_ptc(ExaCtx& c, int* iters_out, double* norm_out) {
   int it = 0;
   for (it = 0; it < c.newton_maxit; ++it) {
     EXA_TRY(exa_scale(c.b, c.ldg_R, -1.0, N, c.st));  // J x = -R(u)
+    // LinearSolver (ptcsolver.cpp:53-97): with a reduced basis, its guess x (the HDG solve's
+    // formula with b = -R gives the reference's x = -W coef) is kept only if R(u + x) is at most
+    // 1.05 |R(u)| (else x = 0 and the basis is emptied); below the tolerance it is the step
+    int status = 0;
+    const bool rb = c.RBdim > 0 && c.rb_cur > 0;
+    if (rb) {
+      const double oldnrm = nrmr;
+      double nv = 0.0;
+      EXA_CUDA(cudaMemsetAsync(c.x, 0, sizeof(double) * N, c.st));
+      EXA_TRY(rb_initial_guess(c));
+      EXA_TRY(exa_lincomb(c.ldg_w, 1.0, c.udg, 1.0, c.x, N, c.st));
+      EXA_TRY(exa_model_ldg_residual(c, c.ldg_w, c.ldg_Rw));
+      EXA_TRY(exa_drv_norm(c, c.ldg_Rw, N, &nv));
+      if (nv > 1.05 * oldnrm) {
+        EXA_TRY(exa_scale(c.x, c.x, 0.0, N, c.st));
+        c.rb_removed = 0;
+        c.rb_cur = 0;
+      }
+      if (nv < c.newton_tol) status = 1;
+    }
     int gi = 0;
     double ge = 0.0;
-    EXA_TRY(exa_drv_gmres(c, &gi, &ge));
+    if (status == 0) {
+      c.gmres_x_preset = rb ? 1 : 0;
+      const int gs = exa_drv_gmres(c, &gi, &ge);
+      c.gmres_x_preset = 0;
+      EXA_TRY(gs);
+    }
     c.last_gmres_iters = gi;
     c.last_gmres_relerr = ge;
     c.total_gmres_iters += gi;
@@ -648,6 +673,7 @@ int exa_drv_ptc(ExaCtx& c, int* iters_out, double* norm_out) {
     EXA_TRY(exa_model_ldg_residual(c, c.udg, c.ldg_R));
     EXA_TRY(exa_drv_norm(c, c.ldg_R, N, &nrmr));
     c.last_newton_iters = it + 1;
+    if (status == 0 && c.RBdim > 0) EXA_TRY(rb_update(c, 1.0));  // UpdateRB (ptcsolver.cpp:207-226)
     if (!(nrmr <= 1.0e6)) {
       exa_set_error("PTC residual norm %g is above 1e6 or NaN", nrmr);
       *iters_out = it + 1;

@@ -145,6 +145,9 @@ struct ExaCtx {
   // interior faces are faces [0, nf0) and boundary faces the rest (the pointwise interior-face
   // kernel relies on it)
   int ldg_split = 0;
+  // set by the PTC solver: GMRES starts from the x it finds (the reduced-basis guess it has
+  // checked) instead of zero, and computes no guess of its own
+  int gmres_x_preset = 0;
 
   long long ndofuhat() const { return (long long)P.ncu * P.npf * P.nf; }
   // unknowns of the linear systems GMRES solves: the trace (HDG) or the element states (LDG)

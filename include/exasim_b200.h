@@ -34,9 +34,10 @@ const char* exa_last_error(void);
  * context solves for the element states u (udg without q: models with ncq = 0) with the
  * pseudo-transient solver: exa_residual, exa_matvec, exa_precond, exa_gmres, exa_newton,
  * exa_dirk and exa_solve run the LDG forms named at each of them, on vectors of length
- * npe*ncu*ne.  It refuses (EXA_ERR_UNSUPPORTED) models with q, a preconditioner matrix
- * other than the identity (flag[7]), a reduced-basis guess, a polynomial preconditioner and
- * the mixed-precision form, and boundary faces without the model's KokkosUbou/KokkosFbou. */
+ * npe*ncu*ne, with the reduced-basis guess of problem[16] as the PTC solver has it.  It
+ * refuses (EXA_ERR_UNSUPPORTED) models with q, a preconditioner matrix other than the
+ * identity (flag[7]), a polynomial preconditioner and the mixed-precision form, and boundary
+ * faces without the model's KokkosUbou/KokkosFbou. */
 int exa_create(const double* app, long long napp, const double* master, long long nmaster,
                const double* mesh, long long nmesh, const double* sol, long long nsol, int device,
                exa_ctx** out);

@@ -17,7 +17,8 @@ The path, for models without q (ncq = 0, the reference's ModelC):
 * The preconditioner: identity (precMatrixType 0) or the element mass inverse per component
   (ApplyMatrix, applymatrix.cpp:66-98; preconditioner.cpp:130-137).
 * GMRES on J x = -R (gmres.cpp:140-318), the PTC loop (ptcsolver.cpp:53-120, 255-330) with
-  RBdim = 0, and the DIRK stages around it (solution.cpp:451-527).
+  its reduced-basis guess (preconditioner.cpp:78-128), and the DIRK stages around it
+  (solution.cpp:451-527).
 
 Models with q are not restated: the reference's GetQ (residual.cpp:74-127) calls RuFace for
 the q face term where qresidual.cpp's RqFace and the GetQ timing label name RqFace, so the
@@ -149,8 +150,8 @@ class LDGOracle(HDGOracle):
             return x.copy()
         return np.einsum("ije,jke->ike", self.Minv, x)
 
-    def gmres_ldg(self, u, b):
-        """GMRES for J x = -b (gmres.cpp:140-318), zero initial guess; returns (x, iterations)."""
+    def gmres_ldg(self, u, b, x0=None):
+        """GMRES for J x = -b (gmres.cpp:140-318) from x0 (zero if None); returns (x, iterations)."""
         shape = b.shape
         N = b.size
         bv = b.ravel(order="F")
@@ -159,9 +160,13 @@ class LDGOracle(HDGOracle):
         nrest, maxit = self.restart, self.gmres_maxit
         n1 = nrest + 1
         nrmb = np.sqrt(np.dot(bv, bv))
-        x = np.zeros(N)
-        r = -1.0 * bv + 0.0 * bv
-        nrmr = nrmb
+        x = np.zeros(N) if x0 is None else x0.ravel(order="F").copy()
+        if np.sqrt(np.dot(x, x)) > 1e-12:
+            r = -1.0 * bv + (-1.0) * mv(x)
+            nrmr = np.sqrt(np.dot(r, r))
+        else:
+            r = -1.0 * bv + 0.0 * bv
+            nrmr = nrmb
         tol = min(0.1, self.gmres_tol * (nrmb / nrmr))
         r = pc(r)
         nrmb = np.sqrt(np.dot(r, r))
@@ -204,8 +209,21 @@ class LDGOracle(HDGOracle):
                 return x.reshape(shape, order="F"), j
         return x.reshape(shape, order="F"), j
 
+    def _rb_guess_ldg(self, u, b):
+        """ComputeInitialGuessAndPreconditioner, LDG form (preconditioner.cpp:78-128): U_i = J W_i
+        for the newest basis vector, coef = (U^T U)^-1 U^T b, x = -W coef."""
+        cur = self.rb_cur
+        i = self.rb_removed - 1 if self.rb_removed > 0 else cur - 1
+        shape = b.shape
+        self.rb_U[:, i] = self.matvec_fd(u, b, self.rb_W[:, i].reshape(shape, order="F")).ravel(order="F")
+        U, W = self.rb_U[:, :cur], self.rb_W[:, :cur]
+        coef = np.linalg.inv(U.T @ U) @ (U.T @ b.ravel(order="F"))
+        return (-(W @ coef)).reshape(shape, order="F")
+
     def ptc(self, maxit=None, tol=None):
-        """PTCsolver (ptcsolver.cpp:255-330) with RBdim = 0; returns (iterations, norms, gmres)."""
+        """PTCsolver (ptcsolver.cpp:255-330) with LinearSolver (:53-120): the reduced-basis guess
+        when RBdim > 0 (kept if R(u + x) <= 1.05 |R(u)|, the step itself below the tolerance),
+        GMRES from it, UpdateRB after GMRES steps; returns (iterations, norms, gmres)."""
         maxit = self.newton_maxit if maxit is None else maxit
         tol = self.newton_tol if tol is None else tol
         ncu = self.ncu
@@ -215,14 +233,31 @@ class LDGOracle(HDGOracle):
         gm = []
         it = 0
         for it in range(maxit):
-            x, nit = self.gmres_ldg(u, r)
-            gm.append(nit)
+            status = 0
+            x0 = None
+            if self.RBdim > 0 and self.rb_cur > 0:
+                oldnrm = norms[-1]
+                x0 = self._rb_guess_ldg(u, r)
+                nv = np.linalg.norm(self.residual_ldg(1.0 * u + 1.0 * x0))
+                if nv > 1.05 * oldnrm:
+                    x0 = 0.0 * x0
+                    self.rb_removed = 0
+                    self.rb_cur = 0
+                if nv < tol:
+                    status = 1
+            if status == 0:
+                x, nit = self.gmres_ldg(u, r, x0)
+                gm.append(nit)
+            else:
+                x = x0
             u = u + 1.0 * x
             r = self.residual_ldg(u)
             nrmr = np.linalg.norm(r)
             norms.append(nrmr)
             if not nrmr <= 1.0e6:
                 raise FloatingPointError("PTC residual above 1e6 or NaN")
+            if status == 0 and self.RBdim > 0:
+                self._rb_update(x)
             if nrmr < tol:
                 break
         self.udg[:, :ncu] = u

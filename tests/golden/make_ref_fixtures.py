@@ -100,6 +100,9 @@ CASES = {
     "euler3d_hex3_p2_ldg": ("euler3d", lambda d: cases.euler3d_vortex_hex(d, n=3, porder=2, nsteps=1, hybrid=0)),
     "euler3d_hex3_p2_ldg_bnd": ("euler3d", lambda d: cases.euler3d_vortex_hex(d, n=3, porder=2, nsteps=1, hybrid=0,
                                                                              periodic=False)),
+    # the same with the reduced-basis initial guess of 5 vectors over two DIRK steps
+    "euler3d_hex3_p2_ldg_rb": ("euler3d", lambda d: _with_problem(
+        cases.euler3d_vortex_hex(d, n=3, porder=2, nsteps=2, hybrid=0), 16, 5)),
 }
 
 # reference dump name -> fixture key, and the block shape used to project it (None: vector)

@@ -1,6 +1,7 @@
 """The LDG oracle (oracle/ldg.py) against the reference's own LDG runs (tests/golden/
 ref_*_ldg*.npz from cput2cEXASIM with problem[0] = 0): the residual of one evaluation at 1e-12,
-one DIRK step of pseudo-transient solves to the PTC tolerance, the residual norms the reference
+the DIRK steps of pseudo-transient solves to the PTC tolerance (with and without the
+reduced-basis guess), the residual norms the reference
 prints, and its GMRES counts."""
 from __future__ import annotations
 
@@ -51,7 +52,7 @@ def test_ldg_residual_matches_reference(name, tmp_path):
 def test_ldg_dirk_step_matches_reference(name, tmp_path):
     fx = RF.load(name)
     o = _oracle(fx, tmp_path)
-    out = o.dirk_solve_ldg(1)
+    out = o.dirk_solve_ldg()
     udg_ref = fx["outudg"]
     nud = int(np.prod(udg_ref[:3]))
     u_ref = udg_ref[3:].reshape(-1, nud)[-1]
