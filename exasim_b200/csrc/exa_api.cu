@@ -170,11 +170,11 @@ int exa_ctx_init(ExaCtx& c, const double* app, long long napp, const double* mas
   c.ntau = (int)A.nsize[8];
   if (c.scheme == 0) {
     // LDG with the pseudo-transient solver: models without q, the finite-difference Jacobian
-    // (flag[4], solversparam[2]), the identity preconditioner (flag[7] = 0) and the reduced-basis
-    // initial guess (problem[16])
+    // (flag[4], solversparam[2]), the identity or mass-inverse preconditioner (flag[7]) and the
+    // reduced-basis initial guess (problem[16])
     c.matvec_order = (int)flag[4];
     c.matvec_eps = A.nsize[7] > 2 ? solvers[2] : 1e-3;
-    const int prec_matrix = (int)flag[7];
+    c.ldg_prec_matrix = (int)flag[7];
     if (P.ncq != 0) {
       exa_set_error("LDG with q (ncq=%d) is not supported: the reference's GetQ calls RuFace for the q face term",
                     P.ncq);
@@ -185,7 +185,6 @@ int exa_ctx_init(ExaCtx& c, const double* app, long long napp, const double* mas
       return EXA_ERR_UNSUPPORTED;
     }
     if (!(c.matvec_eps > 0.0)) { exa_set_error("LDG finite-difference step %g is not positive", c.matvec_eps); return EXA_ERR_ARG; }
-    if (prec_matrix != 0) { exa_set_error("LDG preconditioner matrix type %d: only the identity (0)", prec_matrix); return EXA_ERR_UNSUPPORTED; }
     if (c.ppdegree > 1) { exa_set_error("LDG with a polynomial preconditioner is not supported"); return EXA_ERR_UNSUPPORTED; }
   }
   if (mpiprocs > 1) { exa_set_error("multi-rank inputs: this solver runs one GPU per mesh"); return EXA_ERR_UNSUPPORTED; }
@@ -404,6 +403,18 @@ int exa_ctx_init(ExaCtx& c, const double* app, long long napp, const double* mas
     if (flag_h) { exa_set_error("singular element mass matrix"); return EXA_ERR_SINGULAR; }
   } else {
     EXA_TRY(dev_alloc(c, &c.d_flag, 4));
+  }
+
+  if (c.scheme == 0 && c.ldg_prec_matrix != 0) {
+    // the LDG preconditioner: the inverse element mass matrices, applied per field
+    // (ApplyMassInv, applymatrix.cpp:66-85)
+    EXA_TRY(dev_alloc(c, &c.Minv, ne * P.npe * P.npe));
+    EXA_TRY(exa_k_ldg_mass(P, c.shapegt, c.shapegw, c.elemg, c.Minv, c.st));
+    EXA_TRY(exa_inverse(c.Minv, P.npe, (long long)P.npe * P.npe, P.ne, c.d_flag, c.st));
+    int flag_h = 0;
+    EXA_CUDA(cudaStreamSynchronize(c.st));
+    EXA_CUDA(cudaMemcpy(&flag_h, c.d_flag, sizeof(int), cudaMemcpyDeviceToHost));
+    if (flag_h) { exa_set_error("singular element mass matrix"); return EXA_ERR_SINGULAR; }
   }
 
   // condensed system and workspace (the HDG arrays; an LDG context needs the element

@@ -186,9 +186,20 @@ int exa_drv_matvec(ExaCtx& c, const double* v, double* w) {
 int exa_drv_precond(ExaCtx& c, const double* v, double* w) {
   ExaProfScope ps(c, EXA_PH_PRECOND_APPLY);
   if (c.scheme == 0) {
-    // LDG with precMatrixType 0: the identity (ApplyMatrix, applymatrix.cpp:87-98)
-    EXA_CUDA(cudaMemcpyAsync(w, v, sizeof(double) * c.sysN(), cudaMemcpyDeviceToDevice, c.st));
-    return EXA_OK;
+    // LDG (ApplyMatrix, applymatrix.cpp:66-98): the identity (precMatrixType 0) or the
+    // element mass inverse applied to each field
+    if (c.ldg_prec_matrix == 0) {
+      EXA_CUDA(cudaMemcpyAsync(w, v, sizeof(double) * c.sysN(), cudaMemcpyDeviceToDevice, c.st));
+      return EXA_OK;
+    }
+    const ExaDims& P = c.P;
+    GemmBatch g{};
+    g.M = P.npe; g.N = P.ncu; g.K = P.npe; g.alpha = 1.0; g.beta = 0.0;
+    g.A = c.Minv; g.lda = P.npe; g.sA = (long long)P.npe * P.npe;
+    g.B = v; g.ldb = P.npe; g.sB = (long long)P.npe * P.ncu;
+    g.C = w; g.ldc = P.npe; g.sC = (long long)P.npe * P.ncu;
+    g.batch = P.ne; g.batch2 = 1;
+    return exa_gemm(g, c.st);
   }
   if (c.preconditioner == 2) {
     if (c.precision == 1) return exa_k_bilu_apply(c.P, c.bilu, c.Pc32, v, w, c.st);

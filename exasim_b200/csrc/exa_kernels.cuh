@@ -89,3 +89,6 @@ int exa_k_ldg_fcon(const ExaDims& P, const int* f2e, const int* perm, const int*
 int exa_k_ldg_gather(const ExaDims& P, const int* f2e, const int* perm, const int* elemcon, const double* Rue,
                      const double* Rh, double* Ru, int tdep, double dtfactor, cudaStream_t st);
 int exa_lincomb(double* out, double a, const double* x, double b, const double* y, long long n, cudaStream_t st);
+// the element mass matrices [npe, npe, ne] (the LDG preconditioner inverts them)
+int exa_k_ldg_mass(const ExaDims& P, const double* shapegt, const double* shapegw, const double* elemg, double* mass,
+                   cudaStream_t st);

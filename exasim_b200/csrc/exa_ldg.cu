@@ -64,6 +64,21 @@ __global__ void ldg_gather_kernel(ExaDims P, const int* f2e, const int* perm, co
   }
 }
 
+// The element mass matrices M[a, b] = sum_g shapegw[a, g] shapegt[g, b] jac[g] (the sums of
+// qmats_kernel), for the LDG preconditioner's mass inverse
+__global__ void ldg_mass_kernel(ExaDims P, const double* shapegt, const double* shapegw, const double* elemg,
+                                double* mass) {
+  const int e = blockIdx.x, npe = P.npe, nge = P.nge;
+  const double* jac = elemg + (long long)e * P.elemg_stride() + nge * (P.ncx + P.nd * P.nd);
+  double* M = mass + (long long)e * npe * npe;
+  for (int t = threadIdx.x; t < npe * npe; t += blockDim.x) {
+    const int a = t % npe, b = t / npe;
+    double s = 0.0;
+    for (int g = 0; g < nge; ++g) s += (shapegw[a + npe * g] * shapegt[g + nge * b]) * jac[g];
+    M[t] = s;
+  }
+}
+
 __global__ void lincomb_kernel(double* out, double a, const double* x, double b, const double* y, long long n) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
     out[i] = a * x[i] + b * y[i];
@@ -90,6 +105,14 @@ int exa_k_ldg_gather(const ExaDims& P, const int* f2e, const int* perm, const in
   const size_t smem = sizeof(double) * (size_t)P.npe * P.ncu;
   EXA_TRY(exa_allow_smem((const void*)ldg_gather_kernel, smem));
   ldg_gather_kernel<<<P.ne, 128, smem, st>>>(P, f2e, perm, elemcon, Rue, Rh, Ru, tdep, dtfactor);
+  EXA_LAUNCH_CHECK();
+  return EXA_OK;
+}
+
+int exa_k_ldg_mass(const ExaDims& P, const double* shapegt, const double* shapegw, const double* elemg, double* mass,
+                   cudaStream_t st) {
+  if (P.ne <= 0) return EXA_OK;
+  ldg_mass_kernel<<<P.ne, 128, 0, st>>>(P, shapegt, shapegw, elemg, mass);
   EXA_LAUNCH_CHECK();
   return EXA_OK;
 }

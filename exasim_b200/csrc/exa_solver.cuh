@@ -135,7 +135,7 @@ struct ExaCtx {
   // residual of the element states, its Jacobian by residual differences (flag[4]: one- or
   // two-sided, solversparam[2]: the step), the identity preconditioner (flag[7] = 0)
   int scheme = 1;  // 0 LDG, 1 HDG
-  int matvec_order = 1, ntau = 1;
+  int matvec_order = 1, ntau = 1, ldg_prec_matrix = 0;  // flag[7]: 0 identity, else the element mass inverse
   double matvec_eps = 1e-3;
   double* shapfnt = nullptr;  // face nodal basis and its derivatives at the face nodes [npf, npf, nd]
   int* ldg_fcon = nullptr;    // [2, npf, nf]: e npe + node of face node i on each side (side 1 twice on the boundary)

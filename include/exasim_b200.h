@@ -35,9 +35,8 @@ const char* exa_last_error(void);
  * pseudo-transient solver: exa_residual, exa_matvec, exa_precond, exa_gmres, exa_newton,
  * exa_dirk and exa_solve run the LDG forms named at each of them, on vectors of length
  * npe*ncu*ne, with the reduced-basis guess of problem[16] as the PTC solver has it.  It
- * refuses (EXA_ERR_UNSUPPORTED) models with q, a preconditioner matrix other than the
- * identity (flag[7]), a polynomial preconditioner and the mixed-precision form, and boundary
- * faces without the model's KokkosUbou/KokkosFbou. */
+ * refuses (EXA_ERR_UNSUPPORTED) models with q, a polynomial preconditioner and the
+ * mixed-precision form, and boundary faces without the model's KokkosUbou/KokkosFbou. */
 int exa_create(const double* app, long long napp, const double* master, long long nmaster,
                const double* mesh, long long nmesh, const double* sol, long long nsol, int device,
                exa_ctx** out);
@@ -85,7 +84,8 @@ int exa_residual(exa_ctx* ctx, double* norm);
  * (MatVec, matvec.cpp:41-100; flag[4] one- or two-sided, solversparam[2] the step). */
 int exa_matvec(exa_ctx* ctx, const double* v_dev, double* w_dev);
 /* w = P v, ApplyPreconditioner (Preconditioning/preconditioner.cpp:273-295); v != w.
- * LDG: the identity (precMatrixType 0, preconditioner.cpp:130-137). */
+ * LDG: the identity (precMatrixType 0) or the element mass inverse per field
+ * (preconditioner.cpp:130-137, applymatrix.cpp:66-98). */
 int exa_precond(exa_ctx* ctx, const double* v_dev, double* w_dev);
 /* Solve A x = b by restarted GMRES (Solver/gmres.cpp:361-597); x is field "x".  When it stops at
  * the iteration cap above its tolerance it returns EXA_ERR_NOTCONV (6) with *iters and *relerr

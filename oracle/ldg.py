@@ -15,7 +15,9 @@ The path, for models without q (ncq = 0, the reference's ModelC):
   minus, side 2 plus), then Ru <- -Ru and, time-dependent, Ru <- Ru / dtfactor.
 * The Jacobian-vector product by a finite difference of residuals (MatVec, matvec.cpp:41-100).
 * The preconditioner: identity (precMatrixType 0) or the element mass inverse per component
-  (ApplyMatrix, applymatrix.cpp:66-98; preconditioner.cpp:130-137).
+  (ApplyMatrix, applymatrix.cpp:66-98; preconditioner.cpp:130-137; the element's own inverse
+  mass matrix, which for an affine element equals the reference's master inverse over the
+  element's jacobian up to rounding).
 * GMRES on J x = -R (gmres.cpp:140-318), the PTC loop (ptcsolver.cpp:53-120, 255-330) with
   its reduced-basis guess (preconditioner.cpp:78-128), and the DIRK stages around it
   (solution.cpp:451-527).
@@ -45,7 +47,7 @@ class LDGOracle(HDGOracle):
         self.matvec_tol = float(self.solversparam[2])
         self.ntau = self.tau.size
         if self.prec_matrix != 0:
-            sgds = np.einsum("jgd,gi->jigd", self.shapegw, self.shapegt)
+            sgds = np.einsum("jgd,gi->jigd", self.shapegw, self.shapegt[:, :, 0])
             mass = np.einsum("jig,ge->jie", sgds[:, :, :, 0], self.jac)
             from oracle.hdg import _inverse
             self.Minv = _inverse(mass)
