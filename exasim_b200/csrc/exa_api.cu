@@ -170,8 +170,8 @@ int exa_ctx_init(ExaCtx& c, const double* app, long long napp, const double* mas
   c.ntau = (int)A.nsize[8];
   if (c.scheme == 0) {
     // LDG with the pseudo-transient solver: models without q, the finite-difference Jacobian
-    // (flag[4], solversparam[2]), the identity or mass-inverse preconditioner (flag[7]) and the
-    // reduced-basis initial guess (problem[16])
+    // (flag[4], solversparam[2]), the identity or mass-inverse preconditioner (flag[7]), the
+    // reduced-basis initial guess (problem[16]) and the polynomial preconditioner (problem[27])
     c.matvec_order = (int)flag[4];
     c.matvec_eps = A.nsize[7] > 2 ? solvers[2] : 1e-3;
     c.ldg_prec_matrix = (int)flag[7];
@@ -185,7 +185,6 @@ int exa_ctx_init(ExaCtx& c, const double* app, long long napp, const double* mas
       return EXA_ERR_UNSUPPORTED;
     }
     if (!(c.matvec_eps > 0.0)) { exa_set_error("LDG finite-difference step %g is not positive", c.matvec_eps); return EXA_ERR_ARG; }
-    if (c.ppdegree > 1) { exa_set_error("LDG with a polynomial preconditioner is not supported"); return EXA_ERR_UNSUPPORTED; }
   }
   if (mpiprocs > 1) { exa_set_error("multi-rank inputs: this solver runs one GPU per mesh"); return EXA_ERR_UNSUPPORTED; }
   if (P.nco > 0 || P.ncw > 0) { exa_set_error("odg/wdg fields (nco=%d, ncw=%d) are outside the HDG hot path", P.nco, P.ncw); return EXA_ERR_UNSUPPORTED; }
@@ -514,7 +513,9 @@ int exa_ctx_init(ExaCtx& c, const double* app, long long napp, const double* mas
     EXA_TRY(dev_alloc(c, &c.randvect, N));
     EXA_TRY(dev_alloc(c, &c.poly_q, N));
     EXA_TRY(dev_alloc(c, &c.poly_p, N));
-    std::vector<double> rv((size_t)N);
+    // the system's length (the trace, or the element states of an LDG context)
+    const size_t Nr = (size_t)c.sysN();
+    std::vector<double> rv(Nr);
     unsigned long long st = 0x9E3779B97F4A7C15ull;
     auto next = [&]() {  // splitmix64, then a uniform in (0, 1)
       st += 0x9E3779B97F4A7C15ull;
@@ -525,15 +526,15 @@ int exa_ctx_init(ExaCtx& c, const double* app, long long napp, const double* mas
       return ((double)(z >> 11) + 0.5) / 9007199254740992.0;
     };
     double nrm = 0.0;
-    for (size_t i = 0; i < (size_t)N; i += 2) {  // Box-Muller pairs
+    for (size_t i = 0; i < Nr; i += 2) {  // Box-Muller pairs
       const double u1 = next(), u2 = next(), rr = std::sqrt(-2.0 * std::log(u1));
       rv[i] = rr * std::cos(6.283185307179586 * u2);
-      if (i + 1 < (size_t)N) rv[i + 1] = rr * std::sin(6.283185307179586 * u2);
+      if (i + 1 < Nr) rv[i + 1] = rr * std::sin(6.283185307179586 * u2);
     }
     for (double v : rv) nrm += v * v;
     nrm = std::sqrt(nrm);
     for (double& v : rv) v /= nrm;
-    EXA_CUDA(cudaMemcpyAsync(c.randvect, rv.data(), sizeof(double) * (size_t)N, cudaMemcpyHostToDevice, c.st));
+    EXA_CUDA(cudaMemcpyAsync(c.randvect, rv.data(), sizeof(double) * Nr, cudaMemcpyHostToDevice, c.st));
     EXA_CUDA(cudaStreamSynchronize(c.st));
   }
   if (c.RBdim > 0) {
@@ -838,7 +839,7 @@ bool field(ExaCtx& c, const char* name, FieldRef& f) {
   const long long ne = P.ne, n = P.n, m = P.m, N = c.sysN();
   const std::string s(name ? name : "");
   if (c.scheme == 0 && s != "udg" && s != "uh" && s != "Ru" && s != "b" && s != "x" && s != "sdg" && s != "elemg" &&
-      s != "faceg")
+      s != "faceg" && s != "randvect")
     return false;  // an LDG context holds no condensed or preconditioner arrays
   if (s == "udg") f = {c.udg, (long long)P.npe * P.nc * ne};
   else if (s == "uh") f = {c.uh, c.ndofuhat()};

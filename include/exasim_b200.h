@@ -34,9 +34,9 @@ const char* exa_last_error(void);
  * context solves for the element states u (udg without q: models with ncq = 0) with the
  * pseudo-transient solver: exa_residual, exa_matvec, exa_precond, exa_gmres, exa_newton,
  * exa_dirk and exa_solve run the LDG forms named at each of them, on vectors of length
- * npe*ncu*ne, with the reduced-basis guess of problem[16] as the PTC solver has it.  It
- * refuses (EXA_ERR_UNSUPPORTED) models with q, a polynomial preconditioner and the
- * mixed-precision form, and boundary faces without the model's KokkosUbou/KokkosFbou. */
+ * npe*ncu*ne, with the reduced-basis guess of problem[16] as the PTC solver has it and the
+ * polynomial preconditioner of problem[27].  It refuses (EXA_ERR_UNSUPPORTED) models with q
+ * and the mixed-precision form, and boundary faces without the model's KokkosUbou/KokkosFbou. */
 int exa_create(const double* app, long long napp, const double* master, long long nmaster,
                const double* mesh, long long nmesh, const double* sol, long long nsol, int device,
                exa_ctx** out);
@@ -48,7 +48,8 @@ int exa_sizes(exa_ctx* ctx, long long* out);
 
 /* Host copies of named device arrays: "udg", "uh", "H", "F" (D^-1 F after assembly),
  * "Ru", "Rh", "b", "x", "sdg", "P" (preconditioner), "MinvC", "MinvE", "elemg", "faceg", and with
- * a polynomial preconditioner "randvect" (the start vector of its Arnoldi process, length ndofuhat).
+ * a polynomial preconditioner "randvect" (the start vector of its Arnoldi process, length ndofuhat;
+ * npe*ncu*ne on an LDG context).
  * n must equal the array length.  MinvC and MinvE hold, per element, Minv*C_d and Minv*E_d
  * with the dimension index next to the row index: [npe, nd, npe] and [npe, nd, npf*nfe].
  * "K", "B" and "Dinv" (the FP64 K and B blocks, and D^-1 after an FP64 assembly) exist when the whole

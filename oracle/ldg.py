@@ -19,7 +19,8 @@ The path, for models without q (ncq = 0, the reference's ModelC):
   mass matrix, which for an affine element equals the reference's master inverse over the
   element's jacobian up to rounding).
 * GMRES on J x = -R (gmres.cpp:140-318), the PTC loop (ptcsolver.cpp:53-120, 255-330) with
-  its reduced-basis guess (preconditioner.cpp:78-128), and the DIRK stages around it
+  its reduced-basis guess (preconditioner.cpp:78-128), the polynomial preconditioner of
+  degree ppdegree (getpoly.cpp:176-200, gmres.cpp:90-176), and the DIRK stages around it
   (solution.cpp:451-527).
 
 Models with q are not restated: the reference's GetQ (residual.cpp:74-127) calls RuFace for
@@ -158,7 +159,10 @@ class LDGOracle(HDGOracle):
         N = b.size
         bv = b.ravel(order="F")
         mv = lambda v: self.matvec_fd(u, b, v.reshape(shape, order="F")).ravel(order="F")
-        pc = lambda v: self.precond_ldg(v.reshape(shape, order="F")).ravel(order="F")
+        pc0 = lambda v: self.precond_ldg(v.reshape(shape, order="F")).ravel(order="F")
+        pc = pc0
+        if self.ppdegree > 1:
+            pc = self._poly_precond(mv, pc0, N)
         nrest, maxit = self.restart, self.gmres_maxit
         n1 = nrest + 1
         nrmb = np.sqrt(np.dot(bv, bv))
@@ -221,6 +225,47 @@ class LDGOracle(HDGOracle):
         U, W = self.rb_U[:, :cur], self.rb_W[:, :cur]
         coef = np.linalg.inv(U.T @ U) @ (U.T @ b.ravel(order="F"))
         return (-(W @ coef)).reshape(shape, order="F")
+
+    def _poly_precond(self, mv, pc0, N):
+        """getPoly (getpoly.cpp:176-200: m Arnoldi steps of P J from randvect, the harmonic Ritz
+        values in Leja order, with GMRES's post-processing, gmres.cpp:163-176) and ApplyPoly
+        (gmres.cpp:90-130) after the preconditioner, as the HDG oracle's GMRES applies them."""
+        from oracle.poly import poly_ritz
+        m = self.ppdegree
+        Vp = np.zeros((N, m + 1))
+        Hp = np.zeros((m + 1, m))
+        rv = self.randvect.ravel(order="F")
+        Vp[:, 0] = rv / np.sqrt(np.dot(rv, rv))
+        for jj in range(m):
+            w = pc0(mv(Vp[:, jj]))
+            for k in range(jj + 1):
+                Hp[k, jj] = np.dot(w, Vp[:, k])
+                w = w - Hp[k, jj] * Vp[:, k]
+            Hp[jj + 1, jj] = np.sqrt(np.dot(w, w))
+            Vp[:, jj + 1] = w / Hp[jj + 1, jj]
+        sr, si = poly_ritz(Hp)
+
+        def pc(v):
+            w = pc0(v)
+            q = w.copy()
+            w = np.zeros_like(q)
+            i = 0
+            while i < m - 1:
+                if si[i] == 0:
+                    w = w + q / sr[i]
+                    q = q - pc0(mv(q)) / sr[i]
+                    i += 1
+                else:
+                    a2b2 = sr[i] ** 2 + si[i] ** 2
+                    p = 2 * sr[i] * q - pc0(mv(q))
+                    w = w + p / a2b2
+                    if i < m - 2:
+                        q = q - pc0(mv(p)) / a2b2
+                    i += 2
+            if si[m - 1] == 0:
+                w = w + q / sr[m - 1]
+            return w
+        return pc
 
     def ptc(self, maxit=None, tol=None):
         """PTCsolver (ptcsolver.cpp:255-330) with LinearSolver (:53-120): the reduced-basis guess

@@ -103,6 +103,9 @@ CASES = {
     # the same with the reduced-basis initial guess of 5 vectors over two DIRK steps
     "euler3d_hex3_p2_ldg_rb": ("euler3d", lambda d: _with_problem(
         cases.euler3d_vortex_hex(d, n=3, porder=2, nsteps=2, hybrid=0), 16, 5)),
+    # the periodic case with the polynomial preconditioner of degree 3
+    "euler3d_hex3_p2_ldg_poly3": ("euler3d", lambda d: _with_problem(
+        cases.euler3d_vortex_hex(d, n=3, porder=2, nsteps=1, hybrid=0), 27, 3)),
     # the closed cube with the element mass inverse as the preconditioner (precMatrixType 1)
     "euler3d_hex3_p2_ldg_minv": ("euler3d", lambda d: cases.euler3d_vortex_hex(
         d, n=3, porder=2, nsteps=1, hybrid=0, periodic=False, precMatrixType=1)),

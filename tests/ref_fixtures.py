@@ -95,12 +95,13 @@ def first_stage_state(datain: str) -> Optional[Tuple[float, float, np.ndarray]]:
     return t0 + dt[0] * tt[0], d[0] / dt[0], u * (d[0] / dt[0])
 
 
-def reference_randvect(oracle) -> np.ndarray:
+def reference_randvect(oracle, faces: bool = True) -> np.ndarray:
     """The start vector of the reference's polynomial preconditioner, made as it makes it
     (backend/Solver/setsysstruct.cpp:54-81, 84-203, 338-352): rand_normal draws (the polar
     Box-Muller method on C's rand(), from its default seed) on the element nodes [npe, ncu, ne],
     each component averaged over the element nodes that share a point (ArrayDG2CG), the values
-    of each face's first element at its nodes (GetFaceNodes), normalised.  The libc of this
+    of each face's first element at its nodes (GetFaceNodes; with faces=False, the LDG form, the
+    element-node field itself), normalised.  The libc of this
     process supplies rand(), reseeded with srand(1) first."""
     libc = ctypes.CDLL("libc.so.6")
     libc.rand.restype = ctypes.c_int
@@ -136,5 +137,9 @@ def reference_randvect(oracle) -> np.ndarray:
         np.add.at(sums, cg, dg)
         np.add.at(cnt, cg, 1.0)
         out[:, k, :] = (sums / cnt)[cg].reshape(npe, ne, order="F")
+    if not faces:
+        # the LDG form keeps the element-node field itself (setsysstruct.cpp:338-341)
+        v = out.ravel(order="F")
+        return v / np.sqrt(np.dot(v, v))
     uh = oracle.get_face_nodes(out).ravel(order="F")
     return uh / np.sqrt(np.dot(uh, uh))

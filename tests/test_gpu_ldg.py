@@ -5,8 +5,9 @@ pseudo-transient solves) through the C ABI, against the reference's own LDG runs
   * the residual of one evaluation (the second DIRK stage's at the initial state, the
     reference's debug dump): |gpu - reference| / |reference| <= 1e-12;
   * the residual at a perturbed, non-smooth state against the oracle: the same bound;
-  * the DIRK(2,2) steps of PTC solves (one; two with the reduced-basis guess): the solution
-    within the PTC tolerance of the reference's and the same PTC step count per stage;
+  * the DIRK(2,2) steps of PTC solves (one; two with the reduced-basis guess; the mass-inverse
+    and polynomial preconditioners): the solution within the PTC tolerance of the reference's
+    and the same PTC step count per stage;
   * the configurations the path does not cover are refused with EXA_ERR_UNSUPPORTED.
 
 Each case runs with the model library built from this package's model sources and with one
@@ -85,6 +86,10 @@ def test_ldg_dirk_step_reference(name, source, tmp_path):
     fx = RF.load(name)
     d = RF.write_datain(fx, str(tmp_path / "datain"))
     s = HDGSolver(d, model_library(str(fx["model"]), source))
+    o = LDGOracle(d, MODELS[str(fx["model"])]())
+    if o.ppdegree > 1:
+        # the polynomial's Arnoldi process starts from the reference's own vector
+        s.set("randvect", RF.reference_randvect(o, faces=False))
     nsolves = len(fx["ptc_lengths"])
     its = s.DIRK(nsolves // 2)[:nsolves]  # DIRK(2,2): two stage solves per step
     u = s.get("udg")

@@ -16,7 +16,11 @@ from oracle.models import MODELS
 
 def _oracle(fx, tmp_path):
     d = RF.write_datain(fx, str(tmp_path / "datain"))
-    return LDGOracle(d, MODELS[str(fx["model"])]())
+    o = LDGOracle(d, MODELS[str(fx["model"])]())
+    if o.ppdegree > 1:
+        # the polynomial's Arnoldi process starts from the reference's own vector
+        o.randvect = RF.reference_randvect(o, faces=False)
+    return o
 
 
 def _stage_setup(o, j, u):
