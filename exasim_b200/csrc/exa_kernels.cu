@@ -775,6 +775,14 @@ __global__ void getq_mf_kernel(ExaDims P, const double* shapegt, const double* s
     uhe[t] = uh[k + ncu * (long long)elemcon[jf + ndf * e]];
   }
   for (int t = threadIdx.x; t < ndf; t += blockDim.x) sperm[t] = perm[t];
+  {
+    // the element's Minv is streamed last, after the face terms: ask for it in L2 now, one
+    // 128-byte line per request, so its DRAM reads overlap the face phase
+    const char* mb = reinterpret_cast<const char*>(Minv + (long long)e * npe * npe);
+    const long long bytes = (long long)npe * npe * (long long)sizeof(double);
+    for (long long o = 128LL * threadIdx.x; o < bytes; o += 128LL * blockDim.x)
+      asm volatile("prefetch.global.L2 [%0];" ::"l"(mb + o));
+  }
   if (wpre) {
     const double* we = wpre + (long long)e * npe * ncu * nd;
     for (int t = threadIdx.x; t < npe * ncu * nd; t += blockDim.x) w[t] = we[t];
