@@ -190,7 +190,7 @@ inline size_t ldg_inner_smem(const ExaDims& P) {
 }
 
 template <class Mdl, int ND, int NCU>
-__global__ void __launch_bounds__(128) ldg_face_inner_kernel(LdgArgs A, int nfaces) {
+__global__ void __launch_bounds__(128, 6) ldg_face_inner_kernel(LdgArgs A, int nfaces) {
   extern __shared__ double sm[];
   const ExaDims& P = A.P;
   const int npe = P.npe, npf = P.npf, ngf = P.ngf, nfe = P.nfe, ncx = P.ncx;
