@@ -752,7 +752,7 @@ __host__ __device__ inline size_t getq_mf_doubles(const ExaDims& P, bool wpre) {
 }
 __host__ __device__ inline size_t getq_mf_ints(const ExaDims& P) { return (size_t)P.ndf + (size_t)P.npe * (P.nfe + 1); }
 
-__global__ void getq_mf_kernel(ExaDims P, const double* shapegt, const double* shapegw, const double* shapfgt,
+__global__ void __launch_bounds__(128, 8) getq_mf_kernel(ExaDims P, const double* shapegt, const double* shapegw, const double* shapfgt,
                                const double* shapfgw, const int* perm, const int* elemcon, const double* elemg,
                                const double* faceg, const double* Minv, const double* uh, double* udg,
                                const double* wpre) {
